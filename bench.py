@@ -1,0 +1,428 @@
+"""Benchmark: Coulomb shift+force evaluations per second at 32k atoms (B200).
+
+Workload: 10,923 rigid 3-site waters = 32,769 charges at 1.0 g/cm^3 in a
+68.91 A cubic cell (seeded synthetic input, converted to Bohr).  One step is one
+shift+force evaluation of the reference's fast Ewald method
+(ewald_potential_force with force, src/dftbp/extlibs/fftewald/fft/ewald_fft_3d.f90:36-134):
+parameters re-derived from the charges, real-space pair sum, adjoint NFFT, four
+forward NFFTs (potential and ik force), self term.
+
+Our arm (default):
+  value   plain FP64 form at tol 1e-10 (the reference chain: 280^3 grid, m=12),
+          inputs and outputs resident in HBM, device-timed with CUDA events on
+          the launching stream; L2 flushed between steps (flush not timed).
+  e2e     the same through the C ABI with pinned host buffers: every step copies
+          positions and charges in and potential and force out.
+  mixed   the mixed-precision form (FP32 stencils, FFT and pair terms, FP64
+          accumulation) at tol 1e-7, with its error against the FP64 result.
+  roofline, cpu_baseline, clocks, gpu_launches as the measurement contract asks.
+Reference arm (--impl reference): the CPU restatement of the reference's own
+algorithm (oracle/), all host threads, one full evaluation per step.
+
+Multi-GPU (torchrun): the single cell does not shard; every rank runs its own
+replica ("replicas only"), value = all ranks' evaluations / max-over-ranks time.
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "dftb_fast-ewald_3d_b200")
+ORACLE = os.path.join(ROOT, "oracle")
+for _p in (PKG, ORACLE):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import workloads  # noqa: E402
+
+METRIC = "Coulomb shift+force evals/s at 32k atoms, mixed vs FP64; rel. err vs FP64"
+TOL_FP64 = 1e-10
+TOL_MIXED = 1e-7
+L2_FLUSH_BYTES = 256 << 20
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ---------------------------------------------------------------------------
+# clocks sampler (nvidia-smi during the timed region)
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        loaded = [x for x in sm if smax is None or x > 0.5 * smax] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes per stage launch (one evaluation), for the roofline
+# ---------------------------------------------------------------------------
+def stage_bytes(params, natoms, real_bytes, nc=4):
+    M = params["n_modes"]
+    n = [2 * m for m in M]
+    H = [m - m // 2 for m in M]
+    K1, K2, K3 = H[0] + 1, 2 * H[1] + 1, 2 * H[2] + 1
+    s, c = real_bytes, 2 * real_bytes
+    G = n[0] * n[1] * n[2] * s
+    return {
+        "spread": G,
+        "fft_x_r2c": G + n[1] * n[2] * K1 * c,
+        "fft_y_fwd": n[2] * n[1] * K1 * c + n[2] * K2 * K1 * c,
+        "fft_z_influence": n[2] * K2 * K1 * c * (1 + nc),
+        "fft_y_inv": nc * n[2] * K2 * K1 * c + nc * n[2] * n[1] * K1 * c,
+        "fft_x_c2r": nc * n[2] * n[1] * K1 * c + nc * G,
+        "gather": nc * G + natoms * (8 * 4 + 8 * 4),
+    }
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# reference arm and CPU baseline: the oracle's port of the reference algorithm
+# ---------------------------------------------------------------------------
+def cpu_evals(pos, q, lat, tol, steps, warmup, threads):
+    import oracle
+
+    oracle.build()
+    oracle.set_threads(threads)
+    for _ in range(warmup):
+        oracle.fft_potential_force(pos, q, lat, tol)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        oracle.fft_potential_force(pos, q, lat, tol)
+        times.append(time.perf_counter() - t0)
+    return times
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    pos, q, lat = workloads.c3_water_32k()
+    threads = os.cpu_count() or 1
+    times = cpu_evals(pos, q, lat, TOL_FP64, args.steps, args.warmup, threads)
+    total = sum(times)
+    value = args.steps / total
+    line = {
+        "metric": METRIC, "value": value, "unit": "evals/s", "impl": "reference", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": "water_32769_atoms_68.91A_tol1e-10", "natoms": len(q), "tol": TOL_FP64,
+                   "grid": "280^3", "window_cutoff": 12},
+        "cpu_baseline": {"value": value, "unit": "evals/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full C3 shift+force evaluations (oracle/ C++ "
+                                   f"restatement, OpenMP, project FFT in place of FFTW)"},
+        "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+class Arm:
+    """One precision form on one device: device-resident and end-to-end timing."""
+
+    def __init__(self, eb, torch, device, precision, tol, pos, q, lat):
+        self.eb, self.torch = eb, torch
+        self.tol = tol
+        self.ctx = eb.Context(device, precision)
+        # A dedicated (non-default) stream: the library launches on it and the
+        # CUDA events that time the steps are recorded on it.
+        self.stream = torch.cuda.Stream(device=device)
+        self.ctx.set_stream(self.stream.cuda_stream)
+        dev = f"cuda:{device}"
+        self.n = len(q)
+        self.lat = np.asfortranarray(lat)
+        self.x = torch.tensor(pos, dtype=torch.float64, device=dev).contiguous()
+        self.q = torch.tensor(q, dtype=torch.float64, device=dev).contiguous()
+        self.pot = torch.empty(self.n, dtype=torch.float64, device=dev)
+        self.force = torch.empty((self.n, 3), dtype=torch.float64, device=dev)
+        self.flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+        # pinned host buffers for the end-to-end path (Fortran positions(N,3))
+        self.h_pos = torch.empty((3, self.n), dtype=torch.float64, pin_memory=True).numpy()
+        self.h_pos[:] = np.asarray(pos).T
+        self.h_q = torch.empty(self.n, dtype=torch.float64, pin_memory=True).numpy()
+        self.h_q[:] = q
+        self.h_pot = torch.empty(self.n, dtype=torch.float64, pin_memory=True).numpy()
+        self.h_force = torch.empty((self.n, 3), dtype=torch.float64, pin_memory=True).numpy()
+        torch.cuda.synchronize()
+
+    def step_device(self):
+        self.ctx.potential_force_device(self.x, self.q, self.lat, self.tol, self.pot, self.force)
+
+    def step_e2e(self):
+        L = self.eb.lib()
+        dp = C.POINTER(C.c_double)
+        ov = self.eb.Overrides()
+        rc = L.ewg_potential_force(self.ctx.handle, self.n, self.h_pos.ctypes.data_as(dp),
+                                   self.h_q.ctypes.data_as(dp), self.lat.ctypes.data_as(dp),
+                                   float(self.tol), self.h_pot.ctypes.data_as(dp),
+                                   self.h_force.ctypes.data_as(dp), C.byref(ov))
+        if rc:
+            raise self.eb.EwaldError(rc, self.eb.status_string(rc))
+
+    def time_device(self, steps, warmup, profile=False):
+        torch = self.torch
+        for _ in range(warmup):
+            self.step_device()
+        if profile:
+            self.ctx.stage_times(reset=True)
+            self.ctx.set_profiling(True)
+        launches0 = self.ctx.kernel_launches
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(steps)]
+        torch.cuda.synchronize()
+        for i in range(steps):
+            with torch.cuda.stream(self.stream):
+                self.flush.zero_()  # L2 flush, outside the timed interval
+            evs[i][0].record(self.stream)
+            self.step_device()
+            evs[i][1].record(self.stream)
+        torch.cuda.synchronize()
+        ms = [a.elapsed_time(b) for a, b in evs]
+        launches = self.ctx.kernel_launches - launches0
+        stages = None
+        if profile:
+            stages = self.ctx.stage_times(reset=True)
+            self.ctx.set_profiling(False)
+        return ms, launches, stages
+
+    def time_e2e(self, steps, warmup):
+        for _ in range(warmup):
+            self.step_e2e()
+        self.torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            self.step_e2e()
+        self.torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+
+def run_ours(args):
+    import torch
+
+    import ewald_b200 as eb
+
+    ws, rank, local = dist_env()
+    dist = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    device = local
+    torch.cuda.set_device(device)
+    eb.lib()
+    pos, q, lat = workloads.c3_water_32k()
+
+    fp64 = Arm(eb, torch, device, eb.FP64, TOL_FP64, pos, q, lat)
+    mixed = Arm(eb, torch, device, eb.MIXED, TOL_MIXED, pos, q, lat)
+
+    # accuracy of the mixed form against the FP64 form (same inputs)
+    fp64.step_device()
+    mixed.step_device()
+    torch.cuda.synchronize()
+    p64, f64 = fp64.pot.cpu().numpy(), fp64.force.cpu().numpy()
+    p32, f32 = mixed.pot.cpu().numpy(), mixed.force.cpu().numpy()
+
+    def rel(a, b):
+        return {"max": float(np.abs(a - b).max() / np.abs(b).max()),
+                "rms": float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b ** 2)))}
+
+    err = {"potential": rel(p32, p64), "force": rel(f32, f64)}
+    params64 = fp64.ctx.last_params()
+    params32 = mixed.ctx.last_params()
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    sampler = ClockSampler(device)
+    barrier()
+    sampler.start()
+    ms64, launches64, stages = fp64.time_device(args.steps, args.warmup, profile=True)
+    clocks = sampler.stop()
+    barrier()
+    ms32, launches32, stages32 = mixed.time_device(args.steps, args.warmup, profile=True)
+    barrier()
+    e2e64 = fp64.time_e2e(args.steps, args.warmup)
+    barrier()
+    e2e32 = mixed.time_e2e(args.steps, args.warmup)
+    barrier()
+
+    def maxrank(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    t64 = maxrank(sum(ms64) / 1e3)
+    t32 = maxrank(sum(ms32) / 1e3)
+    te64 = maxrank(e2e64)
+    te32 = maxrank(e2e32)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        times = cpu_evals(pos, q, lat, TOL_FP64, 1, 0, threads)
+        cpu = {"value": 1.0 / times[0], "unit": "evals/s", "cores": threads, "kind": "port",
+               "sample": "1 full 32,769-atom shift+force evaluation at tol 1e-10 (oracle/ C++ "
+                         "restatement of the reference, OpenMP, project FFT in place of FFTW)"}
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    peak, peak_kind = load_peaks()
+    natoms = len(q)
+
+    def roofline(stages_ms, params, real_bytes, steps):
+        sb = stage_bytes(params, natoms, real_bytes)
+        per = {}
+        for name, (ms, _) in stages_ms.items():
+            if ms <= 0:
+                continue
+            dur = ms / steps / 1e3
+            entry = {"ms": ms / steps}
+            if name in sb:
+                entry["gbs"] = sb[name] / dur / 1e9
+                entry["bytes"] = sb[name]
+            per[name] = entry
+        top = max((k for k in per if k in sb), key=lambda k: per[k]["ms"])
+        ach = per[top]["gbs"]
+        return top, per, {"bound": "hbm", "kernel": top, "achieved": ach, "peak": peak,
+                          "unit": "GB/s", "frac": ach / peak, "peak_source": f"{peak_kind} hbm_gbs",
+                          "traffic": None}
+
+    top64, per64, roof64 = roofline(stages, params64, 8, args.steps)
+    top32, per32, roof32 = roofline(stages32, params32, 4, args.steps)
+    h2d = natoms * 3 * 8 + natoms * 8
+    d2h = natoms * 8 + natoms * 3 * 8
+    value = ws * args.steps / t64
+    line = {
+        "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t64 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "water_32769_atoms_68.91A_tol1e-10", "natoms": natoms,
+                   "tol": TOL_FP64, "grid": "x".join(str(2 * m) for m in params64["n_modes"]),
+                   "window_cutoff": params64["window_cutoff"], "alpha": params64["alpha"],
+                   "r_cut_bohr": params64["r_cut"], "parallelism": f"replicas x{ws}",
+                   "l2": "flushed between steps (256 MiB write, untimed); working set > L2"},
+        "e2e": {"value": ws * args.steps / te64, "unit": "evals/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "roofline": roof64,
+        "stages_ms": per64,
+        "mixed": {
+            "value": ws * args.steps / t32, "unit": "evals/s", "tol": TOL_MIXED,
+            "grid": "x".join(str(2 * m) for m in params32["n_modes"]),
+            "window_cutoff": params32["window_cutoff"],
+            "speedup_vs_fp64": (ws * args.steps / t32) / value,
+            "e2e": {"value": ws * args.steps / te32, "unit": "evals/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "rel_err_vs_fp64": err, "roofline": roof32, "stages_ms": per32,
+            "gpu_launches": launches32,
+        },
+        "gpu_launches": launches64,
+        "clocks": clocks,
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

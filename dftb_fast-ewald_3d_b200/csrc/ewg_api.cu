@@ -1,0 +1,973 @@
+// ewg_api.cu -- context, device buffers, plan caches and the C ABI entry points
+// of the B200 Ewald operator (include/ewald_b200.h).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <tuple>
+#include <vector>
+
+#include "ewg_kernels.h"
+
+using namespace ewg;
+
+namespace {
+
+constexpr int kSpreadTileEdge = 16;
+
+// Device buffers owned by a context, grown on demand and reused across calls.
+enum BufId {
+  B_POS, B_Q, B_POT, B_FORCE, B_POT_SR, B_F_SR, B_S4, B_S4S, B_BOXKEY, B_MC, B_MCS, B_FR, B_FRS,
+  B_TILEKEY, B_COUNTS, B_CURSOR, B_BOXSTART, B_TILESTART, B_TMP, B_PERMBOX, B_PERMMESH, B_WTAB,
+  B_QK, B_GRID, B_A1, B_A2, B_B2, B_B1, B_OUT, B_ERR, B_SUMS, B_PARTIAL, B_KVEC, B_SK, B_WK,
+  B_P6, B_O6, B_COORDS, B_COUNT
+};
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+struct FftEntry {
+  FftPlan plan;
+  void* tw64 = nullptr;
+  void* tw32 = nullptr;
+  bool ok = false;
+};
+
+struct TileEntry {
+  TileLists tl;
+  int* dev = nullptr;
+};
+
+struct CorrEntry {
+  double* dev = nullptr;
+};
+
+bool factor_length(int n, FftPlan& plan) {
+  plan.n = n;
+  plan.nstages = 0;
+  int rem = n;
+  auto push = [&](int r) {
+    if (plan.nstages >= kMaxStages) return false;
+    plan.radix[plan.nstages++] = r;
+    rem /= r;
+    return true;
+  };
+  while (rem % 8 == 0)
+    if (!push(8)) return false;
+  while (rem % 4 == 0)
+    if (!push(4)) return false;
+  while (rem % 2 == 0)
+    if (!push(2)) return false;
+  for (int r : {3, 5, 7})
+    while (rem % r == 0)
+      if (!push(r)) return false;
+  for (int r = 11; r <= 31 && rem > 1; r += 2)
+    while (rem % r == 0)
+      if (!push(r)) return false;
+  return rem == 1;
+}
+
+}  // namespace
+
+struct ewg_context {
+  int device = 0;
+  int precision = EWG_PRECISION_FP64;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  DevBuf buf[B_COUNT];
+  std::map<int, FftEntry> ffts;
+  std::map<std::tuple<int, int, int>, TileEntry> tiles;
+  std::map<std::tuple<int, int, int>, CorrEntry> corrs;
+  long long launches = 0;
+  ewg_params last{};
+  // TCoulomb state
+  bool has_lattice = false, has_coords = false, has_charges = false;
+  double lat_cols[9] = {0};
+  int natoms = 0;
+  std::vector<double> coords, dq;
+  long long coords_version = 0, charges_version = 0;
+  // cached geometry of the resident path
+  struct {
+    long long coords_version = -1;
+    int nb[3] = {0, 0, 0};
+    int ng[3] = {0, 0, 0};
+    int m = -1;
+    int mixed = -1;
+  } resident;
+  long long uploaded_charges = -1;
+  StockSetup stock;
+  bool stock_valid = false;
+  int last_ng = 0;
+  Profiler prof;
+
+  ~ewg_context() {
+    if (stream) {
+      cudaSetDevice(device);
+      cudaStreamSynchronize(stream);
+    }
+    for (auto& b : buf)
+      if (b.p) cudaFree(b.p);
+    for (auto& kv : ffts) {
+      cudaFree(kv.second.tw64);
+      cudaFree(kv.second.tw32);
+    }
+    for (auto& kv : tiles) cudaFree(kv.second.dev);
+    for (auto& kv : corrs) cudaFree(kv.second.dev);
+    for (auto& e : prof.ev)
+      if (e) cudaEventDestroy(e);
+    if (own_stream) cudaStreamDestroy(own_stream);
+  }
+};
+
+namespace {
+
+int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return EWG_OK;
+  if (e == cudaErrorMemoryAllocation) return EWG_ERR_OUT_OF_MEMORY;
+  return EWG_ERR_CUDA;
+}
+
+template <class T>
+T* dbuf(ewg_context* c, BufId id, size_t count, int* rc) {
+  DevBuf& b = c->buf[id];
+  const size_t bytes = std::max<size_t>(count * sizeof(T), 256);
+  if (b.cap < bytes) {
+    if (b.p) {
+      cudaStreamSynchronize(c->stream);
+      cudaFree(b.p);
+      b.p = nullptr;
+      b.cap = 0;
+    }
+    const size_t grown = bytes + bytes / 8;
+    if (cudaMalloc(&b.p, grown) != cudaSuccess) {
+      cudaGetLastError();
+      *rc = EWG_ERR_OUT_OF_MEMORY;
+      return nullptr;
+    }
+    b.cap = grown;
+  }
+  return static_cast<T*>(b.p);
+}
+
+int get_fft(ewg_context* c, int n, FftPlan& out) {
+  auto it = c->ffts.find(n);
+  if (it == c->ffts.end()) {
+    FftEntry e;
+    if (n > kMaxFftLength || !factor_length(n, e.plan)) {
+      c->ffts[n] = e;
+      return EWG_ERR_GRID_TOO_LARGE;
+    }
+    std::vector<double> t64(2 * n);
+    std::vector<float> t32(2 * n);
+    const long double pi_l = 3.141592653589793238462643383279502884L;
+    for (int k = 0; k < n; ++k) {
+      const long double ang = 2.0L * pi_l * static_cast<long double>(k) / static_cast<long double>(n);
+      const long double cr = cosl(ang), ci = -sinl(ang);
+      t64[2 * k] = static_cast<double>(cr);
+      t64[2 * k + 1] = static_cast<double>(ci);
+      t32[2 * k] = static_cast<float>(cr);
+      t32[2 * k + 1] = static_cast<float>(ci);
+    }
+    if (cudaMalloc(&e.tw64, sizeof(double) * 2 * n) != cudaSuccess ||
+        cudaMalloc(&e.tw32, sizeof(float) * 2 * n) != cudaSuccess) {
+      cudaGetLastError();
+      return EWG_ERR_OUT_OF_MEMORY;
+    }
+    cudaMemcpy(e.tw64, t64.data(), sizeof(double) * 2 * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(e.tw32, t32.data(), sizeof(float) * 2 * n, cudaMemcpyHostToDevice);
+    e.plan.tw64 = static_cast<const double*>(e.tw64);
+    e.plan.tw32 = static_cast<const float*>(e.tw32);
+    e.ok = true;
+    it = c->ffts.emplace(n, e).first;
+  }
+  if (!it->second.ok) return EWG_ERR_GRID_TOO_LARGE;
+  out = it->second.plan;
+  return EWG_OK;
+}
+
+// Home-tile lists along one axis: target tile t is reachable from home tile h
+// when some lowest point c in h has (c + o) mod n inside t for |o| <= m.
+int get_tiles(ewg_context* c, int n, int m, TileLists& out) {
+  const int T = kSpreadTileEdge;
+  auto key = std::make_tuple(n, m, T);
+  auto it = c->tiles.find(key);
+  if (it == c->tiles.end()) {
+    const int nt = (n + T - 1) / T;
+    std::vector<std::vector<int>> lists(nt);
+    std::vector<char> reach(n);
+    for (int h = 0; h < nt; ++h) {
+      std::fill(reach.begin(), reach.end(), 0);
+      const int lo = h * T, hi = std::min(n, lo + T) - 1;
+      const long span = static_cast<long>(hi - lo) + 2L * m + 1;
+      if (span >= n) {
+        std::fill(reach.begin(), reach.end(), 1);
+      } else {
+        for (long x = lo - m; x <= hi + m; ++x) reach[((x % n) + n) % n] = 1;
+      }
+      for (int t = 0; t < nt; ++t) {
+        const int tl = t * T, th = std::min(n, tl + T);
+        bool any = false;
+        for (int x = tl; x < th && !any; ++x) any = reach[x];
+        if (any) lists[t].push_back(h);
+      }
+    }
+    int maxlen = 1;
+    for (auto& l : lists) maxlen = std::max<int>(maxlen, static_cast<int>(l.size()));
+    std::vector<int> host(nt + static_cast<size_t>(nt) * maxlen, 0);
+    for (int t = 0; t < nt; ++t) {
+      host[t] = static_cast<int>(lists[t].size());
+      for (size_t k = 0; k < lists[t].size(); ++k) host[nt + static_cast<size_t>(t) * maxlen + k] = lists[t][k];
+    }
+    TileEntry e;
+    if (cudaMalloc(&e.dev, sizeof(int) * host.size()) != cudaSuccess) {
+      cudaGetLastError();
+      return EWG_ERR_OUT_OF_MEMORY;
+    }
+    cudaMemcpy(e.dev, host.data(), sizeof(int) * host.size(), cudaMemcpyHostToDevice);
+    e.tl.tile = T;
+    e.tl.ntiles = nt;
+    e.tl.maxlen = maxlen;
+    e.tl.len = e.dev;
+    e.tl.home = e.dev + nt;
+    it = c->tiles.emplace(key, e).first;
+  }
+  out = it->second.tl;
+  return EWG_OK;
+}
+
+// Squared deconvolution factors f(k)^2, f(k) = exp(b (pi k / n)^2)
+// (nfft/nfft.f90:163-189), for k in [-H, H].
+int get_corr(ewg_context* c, int n, int H, int m, const double** out) {
+  auto key = std::make_tuple(n, H, m);
+  auto it = c->corrs.find(key);
+  if (it == c->corrs.end()) {
+    const double b = window_shape(m);
+    std::vector<double> host(2 * H + 1);
+    for (int k = -H; k <= H; ++k) {
+      const double x = kPi * static_cast<double>(k) / static_cast<double>(n);
+      const double f = std::exp(b * (x * x));
+      host[k + H] = f * f;
+    }
+    CorrEntry e;
+    if (cudaMalloc(&e.dev, sizeof(double) * host.size()) != cudaSuccess) {
+      cudaGetLastError();
+      return EWG_ERR_OUT_OF_MEMORY;
+    }
+    cudaMemcpy(e.dev, host.data(), sizeof(double) * host.size(), cudaMemcpyHostToDevice);
+    it = c->corrs.emplace(key, e).first;
+  }
+  *out = it->second.dev;
+  return EWG_OK;
+}
+
+void real_geometry(const Cell& cell, double r_cut, int natoms, RealGeom& g) {
+  for (int d = 0; d < 3; ++d) {
+    int nb = box_count(r_cut, cell.recLen[d]);
+    g.nb[d] = std::max(1, std::min(nb, 1 << 10));
+  }
+  const long cap = std::max<long>(64, 4L * natoms);
+  while (static_cast<long>(g.nb[0]) * g.nb[1] * g.nb[2] > cap) {
+    int d = 0;
+    if (g.nb[1] > g.nb[d]) d = 1;
+    if (g.nb[2] > g.nb[d]) d = 2;
+    g.nb[d] = std::max(1, g.nb[d] / 2);
+  }
+  for (int d = 0; d < 3; ++d) {
+    g.R[d] = std::max(1, static_cast<int>(std::ceil(r_cut * cell.recLen[d] * g.nb[d])));
+    for (int e = 0; e < 3; ++e) {
+      g.lat[d][e] = cell.lat[d][e];
+      g.rec[d][e] = cell.rec[d][e];
+    }
+  }
+}
+
+int mesh_geometry(const Cell& cell, const ewg_params& p, MeshGeom& g) {
+  for (int d = 0; d < 3; ++d) {
+    if (p.n_modes[d] < 2) return EWG_ERR_ARG;
+    g.M[d] = p.n_modes[d];
+    g.n[d] = kOversampling * p.n_modes[d];
+  }
+  if (p.window_cutoff < 0) return EWG_ERR_ARG;
+  // Closed box |k| <= H covering the mode set S = [M/2 - M, M/2 - 1] and -S.
+  int H[3];
+  for (int d = 0; d < 3; ++d) H[d] = g.M[d] - g.M[d] / 2;
+  g.K1 = H[0] + 1;
+  g.K2 = 2 * H[1] + 1;
+  g.K3 = 2 * H[2] + 1;
+  g.m = p.window_cutoff;
+  g.W = 2 * g.m + 1;
+  g.b = window_shape(g.m);
+  g.pref = 1.0 / std::sqrt(kPi * g.b);
+  for (int i = 0; i < 3; ++i)
+    for (int d = 0; d < 3; ++d) g.rec[i][d] = cell.rec[i][d];
+  g.volume = cell.volume;
+  g.alpha = p.alpha;
+  return EWG_OK;
+}
+
+// Shared evaluation of ewald_potential_force on device-resident inputs.
+// pos: element (i, d) at pos[i * sa + d * sd]; q on device; outputs on device.
+int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const double* q,
+             const Cell& cell, const ewg_params& p, bool want_force, double* pot, double* force,
+             bool resident) {
+  int rc = EWG_OK;
+  cudaStream_t st = c->stream;
+  const int mixed = c->precision == EWG_PRECISION_MIXED;
+  const int nc = want_force ? 4 : 1;
+  RealGeom rg;
+  real_geometry(cell, p.r_cut, n, rg);
+  MeshPlan mp;
+  rc = mesh_geometry(cell, p, mp.g);
+  if (rc) return rc;
+  mp.mixed = mixed;
+  mp.prof = &c->prof;
+  mp.tile = kSpreadTileEdge;
+  for (int d = 0; d < 3; ++d) {
+    if ((rc = get_fft(c, mp.g.n[d], mp.fft[d]))) return rc;
+    if ((rc = get_tiles(c, mp.g.n[d], mp.g.m, mp.tl[d]))) return rc;
+    mp.ntiles[d] = mp.tl[d].ntiles;
+    const int H = mp.g.M[d] - mp.g.M[d] / 2;
+    if ((rc = get_corr(c, mp.g.n[d], H, mp.g.m, &mp.corr2[d]))) return rc;
+  }
+  const int nboxes = rg.nb[0] * rg.nb[1] * rg.nb[2];
+  const int ntiles = mp.ntiles[0] * mp.ntiles[1] * mp.ntiles[2];
+  const MeshSizes ms = mesh_sizes(mp.g, mixed, nc, n);
+
+  double4* s4 = dbuf<double4>(c, B_S4, n, &rc);
+  double4* s4s = dbuf<double4>(c, B_S4S, n, &rc);
+  int* boxkey = dbuf<int>(c, B_BOXKEY, n, &rc);
+  int4* mcv = dbuf<int4>(c, B_MC, n, &rc);
+  int4* mcs = dbuf<int4>(c, B_MCS, n, &rc);
+  double4* fr = dbuf<double4>(c, B_FR, n, &rc);
+  double4* frs = dbuf<double4>(c, B_FRS, n, &rc);
+  int* tilekey = dbuf<int>(c, B_TILEKEY, n, &rc);
+  int* counts = dbuf<int>(c, B_COUNTS, std::max(nboxes, ntiles), &rc);
+  int* cursor = dbuf<int>(c, B_CURSOR, std::max(nboxes, ntiles), &rc);
+  int* boxstart = dbuf<int>(c, B_BOXSTART, nboxes + 1, &rc);
+  int* tilestart = dbuf<int>(c, B_TILESTART, ntiles + 1, &rc);
+  int* tmp = dbuf<int>(c, B_TMP, n, &rc);
+  int* permbox = dbuf<int>(c, B_PERMBOX, n, &rc);
+  int* permmesh = dbuf<int>(c, B_PERMMESH, n, &rc);
+  double* pot_sr = dbuf<double>(c, B_POT_SR, n, &rc);
+  double* f_sr = dbuf<double>(c, B_F_SR, 3 * static_cast<size_t>(n), &rc);
+  void* wtab = dbuf<char>(c, B_WTAB, ms.wtab, &rc);
+  void* qk = dbuf<char>(c, B_QK, ms.qk, &rc);
+  void* grid = dbuf<char>(c, B_GRID, ms.grid, &rc);
+  void* A1 = dbuf<char>(c, B_A1, ms.A1, &rc);
+  void* A2 = dbuf<char>(c, B_A2, ms.A2, &rc);
+  void* B2 = dbuf<char>(c, B_B2, ms.B2, &rc);
+  void* B1 = dbuf<char>(c, B_B1, ms.B1, &rc);
+  void* outg = dbuf<char>(c, B_OUT, ms.out, &rc);
+  int* err = dbuf<int>(c, B_ERR, 1, &rc);
+  if (rc) return rc;
+
+  if (!resident) c->resident.coords_version = -1;  // sorted layouts are about to be overwritten
+  const bool reuse = resident && c->resident.coords_version == c->coords_version &&
+                     c->resident.nb[0] == rg.nb[0] && c->resident.nb[1] == rg.nb[1] &&
+                     c->resident.nb[2] == rg.nb[2] && c->resident.ng[0] == mp.g.n[0] &&
+                     c->resident.ng[1] == mp.g.n[1] && c->resident.ng[2] == mp.g.n[2] &&
+                     c->resident.m == mp.g.m && c->resident.mixed == mixed;
+  cudaMemsetAsync(err, 0, sizeof(int), st);
+  prof_mark(mp.prof, st, ST_PREP);
+  if (!reuse) {
+    launch_atom_prep(pos, sa, sd, q, n, cell, rg.nb, mp.g.n, kSpreadTileEdge, mp.ntiles, s4, boxkey,
+                     mcv, fr, tilekey, st);
+    launch_bucket_sort(boxkey, n, nboxes, counts, cursor, boxstart, tmp, permbox, st);
+    launch_permute4(s4, permbox, n, s4s, st);
+    launch_bucket_sort(tilekey, n, ntiles, counts, cursor, tilestart, tmp, permmesh, st);
+    launch_permute_int4(mcv, permmesh, n, mcs, st);
+    launch_permute4(fr, permmesh, n, frs, st);
+    prof_mark(mp.prof, st, ST_WEIGHTS);
+    launch_weights(mp, frs, n, wtab, qk, st);
+    if (resident) {
+      c->resident.coords_version = c->coords_version;
+      for (int d = 0; d < 3; ++d) {
+        c->resident.nb[d] = rg.nb[d];
+        c->resident.ng[d] = mp.g.n[d];
+      }
+      c->resident.m = mp.g.m;
+      c->resident.mixed = mixed;
+    }
+  } else {
+    // Geometry unchanged: refresh only the charges in the sorted layouts.
+    launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, nullptr, 1, nullptr, s4, nullptr, nullptr,
+                     nullptr, nullptr, st);
+    launch_permute4(s4, permbox, n, s4s, st);
+    launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, mp.g.n, kSpreadTileEdge, mp.ntiles, nullptr,
+                     nullptr, mcv, fr, tilekey, st);
+    launch_permute4(fr, permmesh, n, frs, st);
+    prof_mark(mp.prof, st, ST_WEIGHTS);
+    launch_weights(mp, frs, n, wtab, qk, st);
+  }
+  prof_mark(mp.prof, st, ST_REAL);
+  launch_real_space(s4s, permbox, boxstart, n, rg, p.alpha, p.r_cut, mixed, pot_sr, f_sr, err, st);
+  prof_mark(mp.prof, st, ST_SPREAD);
+  launch_spread(mp, mcs, wtab, qk, tilestart, grid, st);
+  launch_forward_and_weight(mp, grid, A1, A2, B2, nc, st);
+  launch_inverse(mp, B2, B1, outg, nc, st);
+  const double self_coef = -2.0 * p.alpha / std::sqrt(kPi);
+  prof_mark(mp.prof, st, ST_GATHER);
+  launch_gather(mp, mcs, wtab, permmesh, outg, nc, n, q, self_coef, pot_sr, f_sr, pot,
+                want_force ? force : nullptr, st);
+  prof_mark(mp.prof, st, -1);
+  int herr = 0;
+  cudaError_t e = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  prof_collect(mp.prof);
+  if (e != cudaSuccess) return cuda_status(e);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e);
+  if (herr) return EWG_ERR_COINCIDENT;
+  c->last = p;
+  return EWG_OK;
+}
+
+struct LaunchScope {
+  ewg_context* c;
+  long long start;
+  explicit LaunchScope(ewg_context* ctx) : c(ctx), start(g_launches) {
+    cudaSetDevice(ctx->device);
+  }
+  ~LaunchScope() { c->launches += g_launches - start; }
+};
+
+int validate_host(int n, const double* pos, const double* q, const double* lat_rows, double tol,
+                  Cell& cell, double& q2) {
+  if (n <= 0) return EWG_ERR_NPARTICLE;
+  if (!pos || !q || !lat_rows) return EWG_ERR_ARG;
+  int rc = check_charges(n, q, &q2);
+  if (rc) return rc;
+  rc = cell_from_rows(lat_rows, cell);
+  if (rc) return rc;
+  if (!(tol > 0.0 && tol < 1.0)) return EWG_ERR_TOL;
+  return EWG_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* ewg_status_string(int s) {
+  switch (s) {
+    case EWG_OK: return "ok";
+    case EWG_ERR_NPARTICLE: return "ewald_fft_3d: nParticle must be positive";
+    case EWG_ERR_ARG: return "ewald_b200: invalid argument";
+    case EWG_ERR_NOT_NEUTRAL: return "ewald_fft_3d: the cell must be charge neutral";
+    case EWG_ERR_TOL: return "ewald_fft_3d: tol must lie in (0,1)";
+    case EWG_ERR_VOLUME: return "ewald_geometry: cell volume too small";
+    case EWG_ERR_ALPHA: return "ewald_fft_3d: alpha must be positive";
+    case EWG_ERR_COINCIDENT: return "ewald_fft_3d: coincident charges";
+    case EWG_ERR_CUTOFF: return "ewald_direct_3d: cutoffs must be positive";
+    case EWG_ERR_ALPHA_SEARCH: return "Failure in determining optimal alpha for Ewaldsum";
+    case EWG_ERR_LATTICE_SEARCH: return "Failure in getMaxGEwald/getMaxREwald";
+    case EWG_ERR_OUT_OF_MEMORY: return "ewald_b200: out of device memory";
+    case EWG_ERR_CUDA: return "ewald_b200: CUDA error";
+    case EWG_ERR_DEVICE_TIMEOUT: return "ewald_b200: device wait timed out";
+    case EWG_ERR_GRID_TOO_LARGE: return "ewald_b200: FFT length not supported (max 4096, radices <= 31)";
+    case EWG_ERR_NO_DEVICE: return "ewald_b200: no CUDA device";
+    case EWG_ERR_STATE: return "ewald_b200: call order (lattice, coords, charges) not satisfied";
+    default: return "ewald_b200: unknown status";
+  }
+}
+
+int ewg_create(ewg_context** out, int device, int precision) {
+  if (!out) return EWG_ERR_ARG;
+  *out = nullptr;
+  if (precision != EWG_PRECISION_FP64 && precision != EWG_PRECISION_MIXED) return EWG_ERR_ARG;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return EWG_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= count) return EWG_ERR_ARG;
+  if (cudaSetDevice(device) != cudaSuccess) return EWG_ERR_CUDA;
+  auto* c = new ewg_context();
+  c->device = device;
+  c->precision = precision;
+  if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return EWG_ERR_CUDA;
+  }
+  c->stream = c->own_stream;
+  int rc = mesh_configure_kernels();
+  if (rc) {
+    delete c;
+    return rc;
+  }
+  *out = c;
+  return EWG_OK;
+}
+
+int ewg_destroy(ewg_context* c) {
+  if (!c) return EWG_ERR_ARG;
+  cudaSetDevice(c->device);
+  delete c;
+  return EWG_OK;
+}
+
+int ewg_set_stream(ewg_context* c, void* stream) {
+  if (!c) return EWG_ERR_ARG;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  c->stream = stream ? static_cast<cudaStream_t>(stream) : c->own_stream;
+  return EWG_OK;
+}
+
+long long ewg_kernel_launches(const ewg_context* c) { return c ? c->launches : 0; }
+
+int ewg_set_profiling(ewg_context* c, int on) {
+  if (!c) return EWG_ERR_ARG;
+  c->prof.on = on != 0;
+  c->prof.n = 0;
+  return EWG_OK;
+}
+
+int ewg_stage_count(void) { return ST_COUNT; }
+
+const char* ewg_stage_name(int s) {
+  static const char* names[ST_COUNT] = {"prep_sort", "real_space", "weights", "spread",
+                                        "fft_x_r2c", "fft_y_fwd", "fft_z_influence",
+                                        "fft_y_inv", "fft_x_c2r", "gather"};
+  return (s >= 0 && s < ST_COUNT) ? names[s] : "unknown";
+}
+
+int ewg_stage_times(const ewg_context* c, double* ms, long long* launches, int n) {
+  if (!c || (!ms && !launches)) return EWG_ERR_ARG;
+  for (int i = 0; i < n && i < ST_COUNT; ++i) {
+    if (ms) ms[i] = c->prof.ms[i];
+    if (launches) launches[i] = c->prof.launches[i];
+  }
+  return EWG_OK;
+}
+
+int ewg_reset_stage_times(ewg_context* c) {
+  if (!c) return EWG_ERR_ARG;
+  for (int i = 0; i < ST_COUNT; ++i) {
+    c->prof.ms[i] = 0.0;
+    c->prof.launches[i] = 0;
+  }
+  c->prof.n = 0;
+  return EWG_OK;
+}
+
+int ewg_last_params(const ewg_context* c, ewg_params* out) {
+  if (!c || !out) return EWG_ERR_ARG;
+  *out = c->last;
+  return EWG_OK;
+}
+
+int ewg_parameters(int n, const double* charges, const double* lat_rows, double tol,
+                   const ewg_overrides* ov, ewg_params* out) {
+  if (n <= 0) return EWG_ERR_NPARTICLE;
+  if (!charges || !lat_rows || !out) return EWG_ERR_ARG;
+  double q2 = 0.0;
+  int rc = check_charges(n, charges, &q2);
+  if (rc) return rc;
+  Cell cell;
+  rc = cell_from_rows(lat_rows, cell);
+  if (rc) return rc;
+  return choose_parameters(cell, q2, n, tol, ov, *out);
+}
+
+int ewg_grid_memory(int n, const double* charges, const double* lat_rows, double tol,
+                    const ewg_overrides* ov, double* gigabytes) {
+  if (n <= 0) return EWG_ERR_NPARTICLE;
+  if (!charges || !lat_rows || !gigabytes) return EWG_ERR_ARG;
+  double q2 = 0.0;
+  for (int i = 0; i < n; ++i) q2 += charges[i] * charges[i];
+  Cell cell;
+  int rc = cell_from_rows(lat_rows, cell);
+  if (rc) return rc;
+  ewg_params p;
+  rc = choose_parameters(cell, q2, n, tol, ov, p);
+  if (rc) return rc;
+  *gigabytes = grid_memory_gigabytes(p);
+  return EWG_OK;
+}
+
+int ewg_device_memory(int n, const double* charges, const double* lat_rows, double tol,
+                      const ewg_overrides* ov, int precision, int with_force, double* bytes) {
+  if (!bytes) return EWG_ERR_ARG;
+  ewg_params p;
+  int rc = ewg_parameters(n, charges, lat_rows, tol, ov, &p);
+  if (rc) return rc;
+  Cell cell;
+  cell_from_rows(lat_rows, cell);
+  MeshGeom g;
+  rc = mesh_geometry(cell, p, g);
+  if (rc) return rc;
+  const MeshSizes s = mesh_sizes(g, precision == EWG_PRECISION_MIXED, with_force ? 4 : 1, n);
+  const double atoms = static_cast<double>(n) * (32 * 4 + 16 * 2 + 4 * 6 + 8 * 6);
+  *bytes = static_cast<double>(s.grid + s.A1 + s.A2 + s.B2 + s.B1 + s.out + s.wtab + s.qk) + atoms;
+  return EWG_OK;
+}
+
+int ewg_potential_force(ewg_context* c, int n, const double* positions, const double* charges,
+                        const double* lat_rows, double tol, double* pot, double* force,
+                        const ewg_overrides* ov) {
+  if (!c) return EWG_ERR_ARG;
+  LaunchScope scope(c);
+  c->uploaded_charges = -1;
+  c->resident.coords_version = -1;
+  Cell cell;
+  double q2 = 0.0;
+  int rc = validate_host(n, positions, charges, lat_rows, tol, cell, q2);
+  if (rc) return rc;
+  if (!pot) return EWG_ERR_ARG;
+  ewg_params p;
+  rc = choose_parameters(cell, q2, n, tol, ov, p);
+  if (rc) return rc;
+  double* dpos = dbuf<double>(c, B_POS, 3 * static_cast<size_t>(n), &rc);
+  double* dq = dbuf<double>(c, B_Q, n, &rc);
+  double* dpot = dbuf<double>(c, B_POT, n, &rc);
+  double* dforce = dbuf<double>(c, B_FORCE, 3 * static_cast<size_t>(n), &rc);
+  if (rc) return rc;
+  cudaMemcpyAsync(dpos, positions, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(dq, charges, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream);
+  rc = evaluate(c, n, dpos, 1, n, dq, cell, p, force != nullptr, dpot, dforce, false);
+  if (rc) return rc;
+  cudaError_t e = cudaMemcpyAsync(pot, dpot, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && force)
+    e = cudaMemcpyAsync(force, dforce, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return cuda_status(e);
+}
+
+int ewg_potential_force_device(ewg_context* c, int n, const double* coords_device,
+                               const double* charges_device, const double* lat_rows, double tol,
+                               double* pot_device, double* force_device, const ewg_overrides* ov) {
+  if (!c) return EWG_ERR_ARG;
+  LaunchScope scope(c);
+  if (n <= 0) return EWG_ERR_NPARTICLE;
+  if (!coords_device || !charges_device || !lat_rows || !pot_device) return EWG_ERR_ARG;
+  int rc = EWG_OK;
+  double* partial = dbuf<double>(c, B_PARTIAL, 3 * 148, &rc);
+  double* sums = dbuf<double>(c, B_SUMS, 4, &rc);
+  if (rc) return rc;
+  launch_charge_sums(charges_device, n, partial, sums, c->stream);
+  double h[3];
+  cudaError_t e = cudaMemcpyAsync(h, sums, sizeof(h), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_status(e);
+  rc = check_sums(n, h[0], h[1]);
+  if (rc) return rc;
+  Cell cell;
+  rc = cell_from_rows(lat_rows, cell);
+  if (rc) return rc;
+  if (!(tol > 0.0 && tol < 1.0)) return EWG_ERR_TOL;
+  ewg_params p;
+  rc = choose_parameters(cell, h[2], n, tol, ov, p);
+  if (rc) return rc;
+  return evaluate(c, n, coords_device, 3, 1, charges_device, cell, p, force_device != nullptr,
+                  pot_device, force_device, false);
+}
+
+int ewg_direct_potential_force(ewg_context* c, int n, const double* positions,
+                               const double* charges, const double* lat_rows, double tol,
+                               double* pot, double* force, const double* alpha_in,
+                               const double* r_cut_in, const double* k_cut_in) {
+  if (!c) return EWG_ERR_ARG;
+  LaunchScope scope(c);
+  c->uploaded_charges = -1;
+  c->resident.coords_version = -1;
+  Cell cell;
+  double q2 = 0.0;
+  int rc = validate_host(n, positions, charges, lat_rows, tol, cell, q2);
+  if (rc) return rc;
+  if (!pot) return EWG_ERR_ARG;
+  const double alpha = alpha_in ? *alpha_in : balanced_splitting(cell, tol);
+  if (!(alpha > 0.0)) return EWG_ERR_ALPHA;
+  double r_cut = 0.0, k_cut = 0.0;
+  if (!(r_cut_in && k_cut_in)) {
+    r_cut = std::sqrt(-std::log(tol)) / alpha;
+    k_cut = 2.0 * alpha * std::sqrt(-std::log(tol));
+  }
+  if (r_cut_in) r_cut = *r_cut_in;
+  if (k_cut_in) k_cut = *k_cut_in;
+  if (!(r_cut > 0.0) || !(k_cut > 0.0)) return EWG_ERR_CUTOFF;
+  // Modes of the direct Fourier sum (direct/ewald_direct_3d.f90:131-147).
+  int nm[3];
+  for (int d = 0; d < 3; ++d) nm[d] = static_cast<int>(std::ceil(k_cut * cell.latLen[d] / (2.0 * kPi))) + 1;
+  std::vector<double> kv, wk;
+  const double kc2 = k_cut * k_cut;
+  for (int mx = -nm[0]; mx <= nm[0]; ++mx)
+    for (int my = -nm[1]; my <= nm[1]; ++my)
+      for (int mz = -nm[2]; mz <= nm[2]; ++mz) {
+        double k[3];
+        for (int d = 0; d < 3; ++d)
+          k[d] = (mx * cell.rec[0][d] + my * cell.rec[1][d] + mz * cell.rec[2][d]) * 2.0 * kPi;
+        const double k2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
+        if (k2 < 1.0e-24 || k2 > kc2) continue;
+        kv.insert(kv.end(), k, k + 3);
+        wk.push_back(4.0 * kPi / cell.volume * std::exp(-k2 / (4.0 * alpha * alpha)) / k2);
+      }
+  const int nk = static_cast<int>(wk.size());
+  RealGeom rg;
+  real_geometry(cell, r_cut, n, rg);
+  const int nboxes = rg.nb[0] * rg.nb[1] * rg.nb[2];
+  double* dpos = dbuf<double>(c, B_POS, 3 * static_cast<size_t>(n), &rc);
+  double* dcoords = dbuf<double>(c, B_COORDS, 3 * static_cast<size_t>(n), &rc);
+  double* dq = dbuf<double>(c, B_Q, n, &rc);
+  double* dpot = dbuf<double>(c, B_POT, n, &rc);
+  double* dforce = dbuf<double>(c, B_FORCE, 3 * static_cast<size_t>(n), &rc);
+  double4* s4 = dbuf<double4>(c, B_S4, n, &rc);
+  double4* s4s = dbuf<double4>(c, B_S4S, n, &rc);
+  int* boxkey = dbuf<int>(c, B_BOXKEY, n, &rc);
+  int* counts = dbuf<int>(c, B_COUNTS, nboxes, &rc);
+  int* cursor = dbuf<int>(c, B_CURSOR, nboxes, &rc);
+  int* boxstart = dbuf<int>(c, B_BOXSTART, nboxes + 1, &rc);
+  int* tmp = dbuf<int>(c, B_TMP, n, &rc);
+  int* permbox = dbuf<int>(c, B_PERMBOX, n, &rc);
+  double* dk = dbuf<double>(c, B_KVEC, 3 * static_cast<size_t>(std::max(nk, 1)), &rc);
+  double* dwk = dbuf<double>(c, B_WK, std::max(nk, 1), &rc);
+  double* dsk = dbuf<double>(c, B_SK, 2 * static_cast<size_t>(std::max(nk, 1)), &rc);
+  int* err = dbuf<int>(c, B_ERR, 1, &rc);
+  if (rc) return rc;
+  cudaStream_t st = c->stream;
+  std::vector<double> xyz(3 * static_cast<size_t>(n));
+  for (int i = 0; i < n; ++i)
+    for (int d = 0; d < 3; ++d) xyz[3 * i + d] = positions[i + static_cast<size_t>(n) * d];
+  cudaMemcpyAsync(dcoords, xyz.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(dq, charges, sizeof(double) * n, cudaMemcpyHostToDevice, st);
+  if (nk) {
+    cudaMemcpyAsync(dk, kv.data(), sizeof(double) * kv.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(dwk, wk.data(), sizeof(double) * nk, cudaMemcpyHostToDevice, st);
+  }
+  cudaMemsetAsync(err, 0, sizeof(int), st);
+  launch_atom_prep(dcoords, 3, 1, dq, n, cell, rg.nb, nullptr, 1, nullptr, s4, boxkey, nullptr,
+                   nullptr, nullptr, st);
+  launch_bucket_sort(boxkey, n, nboxes, counts, cursor, boxstart, tmp, permbox, st);
+  launch_permute4(s4, permbox, n, s4s, st);
+  launch_real_space(s4s, permbox, boxstart, n, rg, alpha, r_cut, 0, dpot, dforce, err, st);
+  launch_structure_factors(dcoords, dq, n, dk, nk, dsk, st);
+  launch_direct_kspace(dcoords, dq, n, dk, dwk, dsk, nk, dpot, dforce, st);
+  int herr = 0;
+  cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(pot, dpot, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
+  if (force) cudaMemcpyAsync(force, dforce, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_status(e);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e);
+  if (herr) return EWG_ERR_COINCIDENT;
+  const double self = -2.0 * alpha / std::sqrt(kPi);
+  for (int i = 0; i < n; ++i) pot[i] += self * charges[i];
+  return EWG_OK;
+}
+
+// ---- TCoulomb surface ------------------------------------------------------
+
+int ewg_set_lattice(ewg_context* c, const double* lat_cols) {
+  if (!c || !lat_cols) return EWG_ERR_ARG;
+  Cell cell;
+  int rc = cell_from_cols(lat_cols, cell);
+  if (rc) return rc;
+  std::memcpy(c->lat_cols, lat_cols, sizeof(c->lat_cols));
+  c->has_lattice = true;
+  c->stock_valid = false;
+  // updateLatVecs clears coordsUpdated_ and chargesUpdated_ (coulomb.F90:617-618).
+  c->has_coords = false;
+  c->has_charges = false;
+  ++c->coords_version;
+  return EWG_OK;
+}
+
+int ewg_set_coords(ewg_context* c, int n, const double* coords) {
+  if (!c || !coords) return EWG_ERR_ARG;
+  if (n <= 0) return EWG_ERR_NPARTICLE;
+  if (!c->has_lattice) return EWG_ERR_STATE;
+  if (c->natoms != n) c->dq.assign(n, 0.0);
+  c->natoms = n;
+  c->coords.assign(coords, coords + 3 * static_cast<size_t>(n));
+  c->has_coords = true;
+  c->has_charges = false;  // coulomb.F90:570-571
+  ++c->coords_version;
+  return EWG_OK;
+}
+
+int ewg_set_charges(ewg_context* c, const double* dq) {
+  if (!c || !dq) return EWG_ERR_ARG;
+  if (!c->has_coords) return EWG_ERR_STATE;
+  c->dq.assign(dq, dq + c->natoms);
+  c->has_charges = true;
+  ++c->charges_version;
+  return EWG_OK;
+}
+
+namespace {
+int coulomb_eval(ewg_context* c, double tol, double* shift, double* force) {
+  if (!c || !shift) return EWG_ERR_ARG;
+  LaunchScope scope(c);
+  if (!c->has_coords || !c->has_charges) return EWG_ERR_STATE;
+  if (!(tol > 0.0 && tol < 1.0)) tol = 1.0e-9;  // coulomb.F90:348-349
+  const int n = c->natoms;
+  double q2 = 0.0;
+  int rc = check_charges(n, c->dq.data(), &q2);
+  if (rc) return rc;
+  Cell cell;
+  rc = cell_from_cols(c->lat_cols, cell);
+  if (rc) return rc;
+  ewg_params p;
+  rc = choose_parameters(cell, q2, n, tol, nullptr, p);
+  if (rc) return rc;
+  double* dcoords = dbuf<double>(c, B_COORDS, 3 * static_cast<size_t>(n), &rc);
+  double* dq = dbuf<double>(c, B_Q, n, &rc);
+  double* dpot = dbuf<double>(c, B_POT, n, &rc);
+  double* dforce = dbuf<double>(c, B_FORCE, 3 * static_cast<size_t>(n), &rc);
+  if (rc) return rc;
+  if (c->resident.coords_version != c->coords_version)
+    cudaMemcpyAsync(dcoords, c->coords.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice,
+                    c->stream);
+  if (c->uploaded_charges != c->charges_version) {
+    cudaMemcpyAsync(dq, c->dq.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->stream);
+    c->uploaded_charges = c->charges_version;
+  }
+  rc = evaluate(c, n, dcoords, 3, 1, dq, cell, p, force != nullptr, dpot, dforce, true);
+  if (rc) {
+    c->resident.coords_version = -1;
+    return rc;
+  }
+  cudaError_t e = cudaMemcpyAsync(shift, dpot, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && force)
+    e = cudaMemcpyAsync(force, dforce, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  return cuda_status(e);
+}
+}  // namespace
+
+int ewg_shift(ewg_context* c, double tol, double* shift) { return coulomb_eval(c, tol, shift, nullptr); }
+
+int ewg_shift_force(ewg_context* c, double tol, double* shift, double* force) {
+  if (!force) return EWG_ERR_ARG;
+  return coulomb_eval(c, tol, shift, force);
+}
+
+int ewg_stress(ewg_context* c, double tol_ewald, double alpha, double* sigma) {
+  if (!c || !sigma) return EWG_ERR_ARG;
+  LaunchScope scope(c);
+  if (!c->has_coords || !c->has_charges) return EWG_ERR_STATE;
+  if (!(tol_ewald > 0.0)) return EWG_ERR_TOL;
+  const int n = c->natoms;
+  Cell cell;
+  int rc = cell_from_cols(c->lat_cols, cell);
+  if (rc) return rc;
+  StockSetup ss;
+  rc = stock_setup(cell, tol_ewald, alpha, ss);
+  if (rc) return rc;
+  c->stock = ss;
+  c->stock_valid = true;
+  const int ng = static_cast<int>(ss.g.size() / 3);
+  c->last_ng = ng;
+  RealGeom rg;
+  real_geometry(cell, ss.max_r, n, rg);
+  const int nboxes = rg.nb[0] * rg.nb[1] * rg.nb[2];
+  double* dcoords = dbuf<double>(c, B_COORDS, 3 * static_cast<size_t>(n), &rc);
+  double* dq = dbuf<double>(c, B_Q, n, &rc);
+  double4* s4 = dbuf<double4>(c, B_S4, n, &rc);
+  double4* s4s = dbuf<double4>(c, B_S4S, n, &rc);
+  int* boxkey = dbuf<int>(c, B_BOXKEY, n, &rc);
+  int* counts = dbuf<int>(c, B_COUNTS, nboxes, &rc);
+  int* cursor = dbuf<int>(c, B_CURSOR, nboxes, &rc);
+  int* boxstart = dbuf<int>(c, B_BOXSTART, nboxes + 1, &rc);
+  int* tmp = dbuf<int>(c, B_TMP, n, &rc);
+  int* permbox = dbuf<int>(c, B_PERMBOX, n, &rc);
+  double* dk = dbuf<double>(c, B_KVEC, 3 * static_cast<size_t>(std::max(ng, 1)), &rc);
+  double* dsk = dbuf<double>(c, B_SK, 2 * static_cast<size_t>(std::max(ng, 1)), &rc);
+  double* p6 = dbuf<double>(c, B_P6, 6 * static_cast<size_t>(std::max(n, ng)), &rc);
+  double* o6 = dbuf<double>(c, B_O6, 12, &rc);
+  int* err = dbuf<int>(c, B_ERR, 1, &rc);
+  if (rc) return rc;
+  cudaStream_t st = c->stream;
+  // The charge buffer may hold a resident copy; refresh unconditionally.
+  cudaMemcpyAsync(dcoords, c->coords.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(dq, c->dq.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st);
+  c->uploaded_charges = c->charges_version;
+  if (ng) cudaMemcpyAsync(dk, ss.g.data(), sizeof(double) * ss.g.size(), cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(err, 0, sizeof(int), st);
+  c->resident.coords_version = -1;  // the sorted layout below is for max_r
+  launch_atom_prep(dcoords, 3, 1, dq, n, cell, rg.nb, nullptr, 1, nullptr, s4, boxkey, nullptr,
+                   nullptr, nullptr, st);
+  launch_bucket_sort(boxkey, n, nboxes, counts, cursor, boxstart, tmp, permbox, st);
+  launch_permute4(s4, permbox, n, s4s, st);
+  launch_real_stress(s4s, boxstart, n, rg, ss.alpha, ss.max_r, p6, o6, err, st);
+  launch_structure_factors(dcoords, dq, n, dk, ng, dsk, st);
+  launch_recip_stress(dk, dsk, ng, ss.alpha, p6, o6 + 6, st);
+  double h[12];
+  int herr = 0;
+  cudaMemcpyAsync(h, o6, sizeof(h), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_status(e);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e);
+  if (herr) return EWG_ERR_COINCIDENT;
+  // sigma = (-(4 pi / V) recip + real) / V   (coulomb.F90:2834, :2861)
+  const double V = cell.volume;
+  const int map[3][3] = {{0, 3, 4}, {3, 1, 5}, {4, 5, 2}};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      const double recip = -h[6 + map[i][j]] * 4.0 * kPi / V;
+      sigma[i + 3 * j] = (recip + h[map[i][j]]) / V;
+    }
+  return EWG_OK;
+}
+
+int ewg_last_stress_setup(const ewg_context* c, double* alpha, double* max_r, double* max_g,
+                          int* n_g) {
+  if (!c || !c->stock_valid) return EWG_ERR_STATE;
+  if (alpha) *alpha = c->stock.alpha;
+  if (max_r) *max_r = c->stock.max_r;
+  if (max_g) *max_g = c->stock.max_g;
+  if (n_g) *n_g = c->last_ng;
+  return EWG_OK;
+}
+
+// ---- batched form ----------------------------------------------------------
+
+int ewg_batch_potential_force(ewg_context* c, int n_cells, const int* offsets, const double* coords,
+                              const double* charges, const double* lat_rows, double tol,
+                              double* pot, double* force, int* cell_status) {
+  if (!c || n_cells < 0 || !offsets || !coords || !charges || !lat_rows || !pot) return EWG_ERR_ARG;
+  LaunchScope scope(c);
+  c->uploaded_charges = -1;
+  c->resident.coords_version = -1;
+  int first = EWG_OK;
+  const int total = offsets[n_cells];
+  int rc = EWG_OK;
+  double* dcoords = dbuf<double>(c, B_COORDS, 3 * static_cast<size_t>(std::max(total, 1)), &rc);
+  double* dq = dbuf<double>(c, B_Q, std::max(total, 1), &rc);
+  double* dpot = dbuf<double>(c, B_POT, std::max(total, 1), &rc);
+  double* dforce = dbuf<double>(c, B_FORCE, 3 * static_cast<size_t>(std::max(total, 1)), &rc);
+  if (rc) return rc;
+  cudaMemcpyAsync(dcoords, coords, sizeof(double) * 3 * total, cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(dq, charges, sizeof(double) * total, cudaMemcpyHostToDevice, c->stream);
+  for (int cidx = 0; cidx < n_cells; ++cidx) {
+    const int a0 = offsets[cidx], na = offsets[cidx + 1] - a0;
+    Cell cell;
+    double q2 = 0.0;
+    int s = check_charges(na, charges + a0, &q2);
+    if (!s) s = cell_from_rows(lat_rows + 9 * static_cast<size_t>(cidx), cell);
+    if (!s && !(tol > 0.0 && tol < 1.0)) s = EWG_ERR_TOL;
+    ewg_params p;
+    if (!s) s = choose_parameters(cell, q2, na, tol, nullptr, p);
+    if (!s)
+      s = evaluate(c, na, dcoords + 3 * static_cast<size_t>(a0), 3, 1, dq + a0, cell, p,
+                   force != nullptr, dpot + a0, dforce + 3 * static_cast<size_t>(a0), false);
+    if (cell_status) cell_status[cidx] = s;
+    if (s && !first) first = s;
+  }
+  cudaError_t e = cudaMemcpyAsync(pot, dpot, sizeof(double) * total, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && force)
+    e = cudaMemcpyAsync(force, dforce, sizeof(double) * 3 * total, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_status(e);
+  return first;
+}
+
+}  // extern "C"

@@ -1,0 +1,261 @@
+// ewg_fft.cuh -- shared-memory Stockham FFT for the mesh transforms.
+//
+// A CTA transforms `nlines` complex lines of length n held in shared memory,
+// ping-ponging between two buffers.  Each pass of radix r and current
+// sub-length p (Stockham autosort, decimation in time) reads the r inputs
+// spaced n/r apart, multiplies input j by w^(j k) with w = exp(sign 2 pi i/(p r))
+// and k = i mod p, does an r-point DFT and writes output j to
+// (i - k) r + k + j p.  After the last pass the data are in natural order.
+// Twiddles come from one table tw[e] = exp(-2 pi i e / n) per length; the
+// inverse direction conjugates them.  Radices 2, 3, 4, 5, 7, 8 are specialised;
+// other odd primes up to 31 use a generic pass.  No normalisation is applied,
+// matching the reference's FFTW usage (nfft/fft_backend.f90:43-58).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "ewg_internal.h"
+
+namespace ewg {
+
+template <typename R>
+struct __align__(2 * sizeof(R)) cx {
+  R x, y;
+};
+
+template <typename R>
+__device__ __forceinline__ cx<R> mk(R x, R y) {
+  cx<R> c;
+  c.x = x;
+  c.y = y;
+  return c;
+}
+template <typename R>
+__device__ __forceinline__ cx<R> add(cx<R> a, cx<R> b) {
+  return mk(a.x + b.x, a.y + b.y);
+}
+template <typename R>
+__device__ __forceinline__ cx<R> sub(cx<R> a, cx<R> b) {
+  return mk(a.x - b.x, a.y - b.y);
+}
+template <typename R>
+__device__ __forceinline__ cx<R> mul(cx<R> a, cx<R> b) {
+  return mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+// multiply by SIGN * i
+template <typename R, int SIGN>
+__device__ __forceinline__ cx<R> mul_si(cx<R> a) {
+  return SIGN > 0 ? mk(-a.y, a.x) : mk(a.y, -a.x);
+}
+template <typename R>
+__device__ __forceinline__ cx<R> scale(cx<R> a, R s) {
+  return mk(a.x * s, a.y * s);
+}
+
+template <typename R>
+__device__ __forceinline__ cx<R> twiddle(const cx<R>* __restrict__ tw, int e, int sign) {
+  cx<R> w = tw[e];
+  if (sign > 0) w.y = -w.y;
+  return w;
+}
+
+// ---- small DFT kernels -----------------------------------------------------
+template <typename R, int SIGN>
+__device__ __forceinline__ void dft2(cx<R>* u) {
+  cx<R> a = u[0], b = u[1];
+  u[0] = add(a, b);
+  u[1] = sub(a, b);
+}
+
+template <typename R, int SIGN>
+__device__ __forceinline__ void dft4(cx<R>& a0, cx<R>& a1, cx<R>& a2, cx<R>& a3) {
+  cx<R> s02 = add(a0, a2), d02 = sub(a0, a2);
+  cx<R> s13 = add(a1, a3), d13 = mul_si<R, SIGN>(sub(a1, a3));
+  a0 = add(s02, s13);
+  a2 = sub(s02, s13);
+  a1 = add(d02, d13);
+  a3 = sub(d02, d13);
+}
+
+template <typename R, int SIGN>
+__device__ __forceinline__ void dft3(cx<R>* u) {
+  const R half = R(0.5);
+  const R s3 = R(0.86602540378443864676);  // sqrt(3)/2
+  cx<R> t1 = add(u[1], u[2]);
+  cx<R> t2 = scale(mul_si<R, SIGN>(sub(u[1], u[2])), s3);
+  cx<R> base = sub(u[0], scale(t1, half));
+  u[0] = add(u[0], t1);
+  u[1] = add(base, t2);
+  u[2] = sub(base, t2);
+}
+
+template <typename R, int SIGN>
+__device__ __forceinline__ void dft8(cx<R>* u) {
+  const R r2 = R(0.70710678118654752440);  // 1/sqrt(2)
+  cx<R> e0 = u[0], e1 = u[2], e2 = u[4], e3 = u[6];
+  cx<R> o0 = u[1], o1 = u[3], o2 = u[5], o3 = u[7];
+  dft4<R, SIGN>(e0, e1, e2, e3);
+  dft4<R, SIGN>(o0, o1, o2, o3);
+  // w = exp(SIGN 2 pi i / 8)
+  cx<R> w1o = scale(add(o1, mul_si<R, SIGN>(o1)), r2);            // (1 + s i)/sqrt2
+  cx<R> w2o = mul_si<R, SIGN>(o2);                                 // s i
+  cx<R> w3o = scale(sub(mul_si<R, SIGN>(o3), o3), r2);            // (-1 + s i)/sqrt2
+  u[0] = add(e0, o0);
+  u[4] = sub(e0, o0);
+  u[1] = add(e1, w1o);
+  u[5] = sub(e1, w1o);
+  u[2] = add(e2, w2o);
+  u[6] = sub(e2, w2o);
+  u[3] = add(e3, w3o);
+  u[7] = sub(e3, w3o);
+}
+
+// Odd radix RR via conjugate-symmetric pairs; cos/sin of 2 pi j / RR are read
+// from the length-n twiddle table (tw[j n / RR] = exp(-2 pi i j / RR)).
+template <typename R, int SIGN, int RR>
+__device__ __forceinline__ void dft_odd(cx<R>* u, const cx<R>* __restrict__ tw, int n) {
+  constexpr int H = (RR - 1) / 2;
+  R c[H + 1], s[H + 1];
+#pragma unroll
+  for (int j = 1; j <= H; ++j) {
+    cx<R> w = tw[j * (n / RR)];
+    c[j] = w.x;
+    s[j] = -w.y;
+  }
+  cx<R> sp[H + 1], sm[H + 1];
+  cx<R> total = u[0];
+#pragma unroll
+  for (int j = 1; j <= H; ++j) {
+    sp[j] = add(u[j], u[RR - j]);
+    sm[j] = sub(u[j], u[RR - j]);
+    total = add(total, sp[j]);
+  }
+  cx<R> out[RR];
+  out[0] = total;
+#pragma unroll
+  for (int k = 1; k < RR; ++k) {
+    cx<R> acc = u[0];
+#pragma unroll
+    for (int j = 1; j <= H; ++j) {
+      const int idx = (j * k) % RR;
+      const R cs = idx <= H ? c[idx] : c[RR - idx];
+      const R sn = idx <= H ? s[idx] : -s[RR - idx];
+      acc.x += sp[j].x * cs - R(SIGN) * sm[j].y * sn;
+      acc.y += sp[j].y * cs + R(SIGN) * sm[j].x * sn;
+    }
+    out[k] = acc;
+  }
+#pragma unroll
+  for (int k = 0; k < RR; ++k) u[k] = out[k];
+}
+
+template <typename R, int SIGN, int RR>
+__device__ __forceinline__ void dft_fixed(cx<R>* u, const cx<R>* __restrict__ tw, int n) {
+  if constexpr (RR == 2) {
+    dft2<R, SIGN>(u);
+  } else if constexpr (RR == 3) {
+    dft3<R, SIGN>(u);
+  } else if constexpr (RR == 4) {
+    dft4<R, SIGN>(u[0], u[1], u[2], u[3]);
+  } else if constexpr (RR == 8) {
+    dft8<R, SIGN>(u);
+  } else {
+    dft_odd<R, SIGN, RR>(u, tw, n);
+  }
+}
+
+// One Stockham pass of a compile-time radix over all lines.
+template <typename R, int SIGN, int RR>
+__device__ __forceinline__ void stockham_pass(const cx<R>* __restrict__ in, cx<R>* __restrict__ out,
+                                              int n, int nlines, int p,
+                                              const cx<R>* __restrict__ tw) {
+  const int nr = n / RR;
+  const int total = nlines * nr;
+  const int step = n / (p * RR);
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int l = t / nr;
+    const int i = t - l * nr;
+    const int k = i % p;
+    const cx<R>* src = in + l * n + i;
+    cx<R> u[RR];
+#pragma unroll
+    for (int j = 0; j < RR; ++j) u[j] = src[j * nr];
+    if (p > 1) {
+#pragma unroll
+      for (int j = 1; j < RR; ++j) u[j] = mul(u[j], twiddle(tw, j * k * step, SIGN));
+    }
+    dft_fixed<R, SIGN, RR>(u, tw, n);
+    cx<R>* dst = out + l * n + (i - k) * RR + k;
+#pragma unroll
+    for (int j = 0; j < RR; ++j) dst[j * p] = u[j];
+  }
+}
+
+// Generic odd prime radix (slow path for lengths the reference's overrides
+// can produce but the parameter chain never does).
+template <typename R, int SIGN>
+__device__ void stockham_pass_generic(const cx<R>* __restrict__ in, cx<R>* __restrict__ out, int n,
+                                      int nlines, int p, int rr, const cx<R>* __restrict__ tw) {
+  const int nr = n / rr;
+  const int total = nlines * nr;
+  const int step = n / (p * rr);
+  const int stride_rr = n / rr;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int l = t / nr;
+    const int i = t - l * nr;
+    const int k = i % p;
+    const cx<R>* src = in + l * n + i;
+    cx<R>* dst = out + l * n + (i - k) * rr + k;
+    for (int s = 0; s < rr; ++s) {
+      cx<R> acc = mk(R(0), R(0));
+      for (int j = 0; j < rr; ++j) {
+        cx<R> v = src[j * nr];
+        if (p > 1 && j > 0) v = mul(v, twiddle(tw, j * k * step, SIGN));
+        const int e = ((j * s) % rr) * stride_rr;
+        acc = add(acc, mul(v, twiddle(tw, e, SIGN)));
+      }
+      dst[s * p] = acc;
+    }
+  }
+}
+
+// Full transform of `nlines` lines of length n in shared memory.  `a` holds
+// the input; `b` is scratch of the same size.  Returns the buffer holding the
+// result.  The caller synchronises before the call; the function returns after
+// a barrier.
+template <typename R, int SIGN>
+__device__ cx<R>* fft_lines(cx<R>* a, cx<R>* b, int n, int nlines, const FftPlan& plan,
+                            const cx<R>* __restrict__ tw) {
+  int p = 1;
+  for (int s = 0; s < plan.nstages; ++s) {
+    const int rr = plan.radix[s];
+    switch (rr) {
+      case 2: stockham_pass<R, SIGN, 2>(a, b, n, nlines, p, tw); break;
+      case 3: stockham_pass<R, SIGN, 3>(a, b, n, nlines, p, tw); break;
+      case 4: stockham_pass<R, SIGN, 4>(a, b, n, nlines, p, tw); break;
+      case 5: stockham_pass<R, SIGN, 5>(a, b, n, nlines, p, tw); break;
+      case 7: stockham_pass<R, SIGN, 7>(a, b, n, nlines, p, tw); break;
+      case 8: stockham_pass<R, SIGN, 8>(a, b, n, nlines, p, tw); break;
+      default: stockham_pass_generic<R, SIGN>(a, b, n, nlines, p, rr, tw); break;
+    }
+    __syncthreads();
+    cx<R>* t = a;
+    a = b;
+    b = t;
+    p *= rr;
+  }
+  return a;
+}
+
+template <typename R>
+__device__ __forceinline__ const cx<R>* plan_twiddles(const FftPlan& plan);
+template <>
+__device__ __forceinline__ const cx<double>* plan_twiddles<double>(const FftPlan& plan) {
+  return reinterpret_cast<const cx<double>*>(plan.tw64);
+}
+template <>
+__device__ __forceinline__ const cx<float>* plan_twiddles<float>(const FftPlan& plan) {
+  return reinterpret_cast<const cx<float>*>(plan.tw32);
+}
+
+}  // namespace ewg

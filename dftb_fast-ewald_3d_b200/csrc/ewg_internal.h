@@ -1,0 +1,108 @@
+// ewg_internal.h -- declarations shared by the host chain, the kernels and the
+// C ABI of the B200 Ewald operator.  Not installed; include/ewald_b200.h is the
+// public interface.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+#include "../../include/ewald_b200.h"
+
+namespace ewg {
+
+// ---------------------------------------------------------------------------
+// Host side: geometry and the reference's parameter chain (ewg_chain.cpp)
+// ---------------------------------------------------------------------------
+
+// TCell3d (common/ewald_geometry.f90:22-44).  lat[i][d] is lattice vector a_i,
+// rec[i][d] the dual vector b_i with b_i . a_j = delta_ij (no factor 2 pi).
+struct Cell {
+  double lat[3][3];
+  double rec[3][3];
+  double volume;
+  double latLen[3];
+  double recLen[3];
+};
+
+// cell_metrics_3d (common/ewald_geometry.f90:65-93) from the Fortran rows layout.
+int cell_from_rows(const double* lat_rows, Cell& cell);
+// The same geometry from DFTB+'s column layout (coulomb.F90 latVecs_(:, i) = a_i).
+int cell_from_cols(const double* lat_cols, Cell& cell);
+
+// check_configuration (common/ewald_validation.f90:26-48) on host charges;
+// also returns sum q^2 for the parameter chain.
+int check_charges(int n, const double* q, double* q2sum);
+// The same test on the three sums (sum q, sum |q|, sum q^2).
+int check_sums(int n, double sum_q, double sum_abs_q);
+
+// choose_parameters (fft/ewald_fft_3d_parameters.f90:52-142).
+int choose_parameters(const Cell& cell, double q2sum, int n, double tol, const ewg_overrides* ov,
+                      ewg_params& p);
+// grid_memory_gigabytes (fft/ewald_fft_3d_parameters.f90:177-229).
+double grid_memory_gigabytes(const ewg_params& p);
+int next_fast_length(int n);      // nfft/fft_backend.f90:73-91
+double window_shape(int m);       // nfft/nfft.f90:82-92
+int box_count(double r_cut, double recLen);  // common/ewald_cell_list.f90:56-73
+
+// Balanced splitting of the direct engine (direct/ewald_direct_3d.f90:319-347).
+double balanced_splitting(const Cell& cell, double tol);
+
+// Stock DFTB+ setup used by invRStress (coulomb.F90:575-620, :2097-2308).
+struct StockSetup {
+  double alpha, max_r, max_g;
+  std::vector<double> g;  // Cartesian half-space reciprocal vectors, 3 per point
+};
+int stock_setup(const Cell& cell, double tol_ewald, double alpha_in, StockSetup& out);
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr int kOversampling = 2;  // nfft/nfft.f90:43
+
+// ---------------------------------------------------------------------------
+// Device side
+// ---------------------------------------------------------------------------
+
+constexpr int kMaxFftLength = 4096;
+constexpr int kMaxStages = 16;
+
+// One FFT length: its radix schedule and a device twiddle table
+// tw[k] = exp(-2 pi i k / n), k in [0, n).
+struct FftPlan {
+  int n = 0;
+  int nstages = 0;
+  int radix[kMaxStages] = {0};
+  const double* tw64 = nullptr;  // interleaved complex, device
+  const float* tw32 = nullptr;   // interleaved complex, device
+};
+
+// Per-axis lists of "home" tiles whose atoms can reach a given target tile of
+// the mesh: home[t * maxlen + k] for k < len[t].
+struct TileLists {
+  int tile = 0;        // tile edge (points)
+  int ntiles = 0;
+  int maxlen = 0;
+  const int* len = nullptr;   // device
+  const int* home = nullptr;  // device
+};
+
+// Everything the mesh kernels need about one evaluation.
+struct MeshGeom {
+  int n[3];        // fine grid = 2 * modes
+  int M[3];        // retained modes
+  int K1, K2, K3;  // compact spectrum extents: M1/2+1, M2+1, M3+1
+  int m;           // window half-width
+  int W;           // 2m+1
+  double b;        // window shape
+  double pref;     // 1/sqrt(pi b)
+  double rec[3][3];
+  double volume, alpha;
+};
+
+struct RealGeom {
+  int nb[3];       // boxes per axis
+  int R[3];        // neighbour box range per axis
+  double lat[3][3];
+  double rec[3][3];
+};
+
+}  // namespace ewg

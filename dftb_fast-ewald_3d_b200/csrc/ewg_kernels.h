@@ -1,0 +1,138 @@
+// ewg_kernels.h -- host-callable launchers of the Ewald kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "ewg_internal.h"
+
+namespace ewg {
+
+// Launch counter shared by every launcher (the context copies it out).
+extern thread_local long long g_launches;
+
+// Stages of one evaluation, for the per-stage device timing.
+enum Stage {
+  ST_PREP, ST_REAL, ST_WEIGHTS, ST_SPREAD, ST_FFT_X_R2C, ST_FFT_Y_FWD, ST_FFT_Z_INFL,
+  ST_FFT_Y_INV, ST_FFT_X_C2R, ST_GATHER, ST_COUNT
+};
+
+// Event marks on one stream; the interval after mark i belongs to tag[i].
+struct Profiler {
+  static constexpr int kMax = 64;
+  bool on = false;
+  int n = 0;
+  cudaEvent_t ev[kMax] = {};
+  int tag[kMax] = {};
+  double ms[ST_COUNT] = {};
+  long long launches[ST_COUNT] = {};
+  long long launch_mark[kMax] = {};
+};
+// Close the running interval and open one for `stage` (-1: none).
+void prof_mark(Profiler* p, cudaStream_t st, int stage);
+// After the stream is synchronised: fold the intervals into ms[] and reset.
+void prof_collect(Profiler* p);
+
+// ---- atoms: fractional coordinates, keys, sorting (ewg_real.cu) ----------
+
+// Per atom: wrapped fractional coordinates s and charge (double4), real-space
+// box key, mesh lowest point and fraction (nfft/nfft.f90:122-159), mesh tile key.
+// positions: element (i, d) at pos[i * sa + d * sd].
+void launch_atom_prep(const double* pos, long sa, long sd, const double* q, int n, const Cell& cell,
+                      const int nb[3], const int ngrid[3], int tile, const int ntiles[3],
+                      double4* s4, int* box_key, int4* mesh_c, double4* mesh_fr, int* tile_key,
+                      cudaStream_t st);
+
+// Stable counting sort by key: perm[k] = atom with the k-th key in (key, index)
+// order; starts[nkeys + 1] are bucket offsets.  Scratch: counts/cursor (nkeys),
+// tmp (n).
+void launch_bucket_sort(const int* key, int n, int nkeys, int* counts, int* cursor, int* starts,
+                        int* tmp, int* perm, cudaStream_t st);
+
+// out[k] = in[perm[k]]
+void launch_permute4(const double4* in, const int* perm, int n, double4* out, cudaStream_t st);
+void launch_permute_int4(const int4* in, const int* perm, int n, int4* out, cudaStream_t st);
+
+// Charge sums for the parameter chain on device-resident charges:
+// out[0] = sum q, out[1] = sum |q|, out[2] = sum q^2 (fixed-order reduction).
+void launch_charge_sums(const double* q, int n, double* partial, double* out, cudaStream_t st);
+
+// Real-space erfc pair sum (fft/ewald_fft_3d_real.f90:81-187 and
+// direct/ewald_direct_3d.f90:192-309) over box-sorted atoms.  Writes pot and
+// force (3,N) by original atom index.  mixed != 0 evaluates the pair terms in
+// FP32 and accumulates in FP64.
+void launch_real_space(const double4* s4_sorted, const int* perm, const int* box_start, int n,
+                       const RealGeom& g, double alpha, double r_cut, int mixed, double* pot,
+                       double* force, int* err, cudaStream_t st);
+
+// Real-space virial of invRStress (coulomb.F90:2836-2905): per-atom partial
+// tensors (6 per atom) then a fixed-order sum into out6.
+void launch_real_stress(const double4* s4_sorted, const int* box_start, int n, const RealGeom& g,
+                        double alpha, double max_r, double* partial6, double* out6, int* err,
+                        cudaStream_t st);
+
+// Structure factors S(k) = sum_j q_j exp(i k . x_j) for a list of Cartesian
+// wave vectors; x(3,N) atom-major Cartesian coordinates.  out: 2 per vector.
+void launch_structure_factors(const double* coords3n, const double* q, int n, const double* kvec,
+                              int nk, double* out, cudaStream_t st);
+
+// Reciprocal stress of invRStress (coulomb.F90:2800-2833) from S(G):
+// per-vector tensors then a fixed-order sum into out6.
+void launch_recip_stress(const double* kvec, const double* sk, int nk, double alpha,
+                         double* partial6, double* out6, cudaStream_t st);
+
+// Direct Fourier sum of the direct engine (direct/ewald_direct_3d.f90:131-174):
+// pot[i] += sum_k w_k Re(S(k) e^{-ik.x_i}), force[i] -= q_i w_k Im(...) k.
+void launch_direct_kspace(const double* coords3n, const double* q, int n, const double* kvec,
+                          const double* wk, const double* sk, int nk, double* pot, double* force,
+                          cudaStream_t st);
+
+// ---- mesh (ewg_mesh.cu) ----------------------------------------------------
+
+// Everything the mesh pipeline needs, resolved on the host.
+struct MeshPlan {
+  MeshGeom g;
+  FftPlan fft[3];
+  TileLists tl[3];
+  int tile;
+  int ntiles[3];
+  int mixed;                      // 0: FP64, 1: FP32 storage/products
+  Profiler* prof = nullptr;
+  const double* corr2[3] = {nullptr, nullptr, nullptr};  // squared deconvolution factors, index k + M/2
+  const double* kvec_unused = nullptr;
+};
+
+// Stencil weights per mesh-sorted atom: wtab[(k*3 + d)*W + o].
+void launch_weights(const MeshPlan& mp, const double4* mesh_fr_sorted, int n, void* wtab,
+                    void* qk, cudaStream_t st);
+
+// Tile-owned deterministic spread (adjoint_nfft_3d step 1, nfft/nfft.f90:253-278).
+void launch_spread(const MeshPlan& mp, const int4* mesh_c_sorted, const void* wtab, const void* qk,
+                   const int* tile_start, void* grid, cudaStream_t st);
+
+// Pruned forward transform of the real grid to the compact spectrum, fused with
+// the influence weights and the first inverse pass: grid -> A1 -> A2 -> B2.
+// nc = 1 (potential) or 4 (potential and three force components).
+void launch_forward_and_weight(const MeshPlan& mp, const void* grid, void* A1, void* A2, void* B2,
+                               int nc, cudaStream_t st);
+
+// Remaining inverse passes B2 -> B1 -> interleaved real grids (nc per point).
+void launch_inverse(const MeshPlan& mp, const void* B2, void* B1, void* out, int nc, cudaStream_t st);
+
+// Gather (forward_nfft_3d step 3, nfft/nfft.f90:380-402) fused with the final
+// assembly (fft/ewald_fft_3d.f90:121-132): pot = sr + lr + self,
+// force = sr + q * lr.
+void launch_gather(const MeshPlan& mp, const int4* mesh_c_sorted, const void* wtab,
+                   const int* mesh_perm, const void* out_grid, int nc, int n, const double* q_orig,
+                   double self_coef, const double* pot_sr, const double* force_sr, double* pot,
+                   double* force, cudaStream_t st);
+
+// Device byte sizes of the mesh buffers.
+struct MeshSizes {
+  size_t grid, A1, A2, B2, B1, out, wtab, qk;
+};
+MeshSizes mesh_sizes(const MeshGeom& g, int mixed, int nc, int natoms);
+
+// Smallest shared-memory layout checks and per-kernel configuration.
+int mesh_configure_kernels();
+
+}  // namespace ewg

@@ -1,0 +1,565 @@
+// ewg_real.cu -- per-atom preparation, the deterministic bucket sort, the
+// real-space erfc pair sum over a linked-cell layout, and the stock stress
+// terms (real-space virial and reciprocal structure-factor sum).
+//
+// Cell list.  Boxes are at least r_cut wide along every dual direction
+// (box_counts_3d, common/ewald_cell_list.f90:56-73).  An atom in box b meets
+// every partner within r_cut among the boxes b - R .. b + R per axis, where
+// R = ceil(r_cut |b_d| nb_d); R = 1 whenever at least one box fits, so the
+// usual case is the reference's 27-box neighbourhood (fft/ewald_fft_3d_real.f90:143-180),
+// and a cell narrower than the cutoff enumerates periodic images the way the
+// direct engine's explicit image sum does (direct/ewald_direct_3d.f90:236-298).
+// Boxes adjacent along x are contiguous in the sorted order, so each (dy, dz)
+// row of neighbour boxes is scanned as at most a few contiguous runs.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "ewg_kernels.h"
+
+namespace ewg {
+
+thread_local long long g_launches = 0;
+
+namespace {
+
+constexpr double kSqrtPi = 1.77245385090551602730;  // sqrt(pi)
+
+__device__ __forceinline__ int floor_div(int a, int n) {
+  return a >= 0 ? a / n : -((-a + n - 1) / n);
+}
+
+// ---------------------------------------------------------------------------
+// Atom preparation.  Fractional coordinates t = b_d . x (fft/ewald_fft_3d_fourier.f90:76-81),
+// wrapped s = t - floor(t) (common/ewald_cell_list.f90:130-136), the box index
+// min(int(s nb), nb - 1) (:78-91), and the mesh stencil origin: lowest grid
+// point floor(s n) and the fraction s n - lowest (nfft/nfft.f90:148-152).
+// ---------------------------------------------------------------------------
+struct PrepArgs {
+  double rec[3][3];
+  int nb[3];
+  int ng[3];
+  int tile;
+  int ntiles[3];
+};
+
+__global__ void k_atom_prep(const double* __restrict__ pos, long sa, long sd,
+                            const double* __restrict__ q, int n, PrepArgs a,
+                            double4* __restrict__ s4, int* __restrict__ box_key,
+                            int4* __restrict__ mesh_c, double4* __restrict__ mesh_fr,
+                            int* __restrict__ tile_key) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double x[3] = {pos[i * sa], pos[i * sa + sd], pos[i * sa + 2 * sd]};
+  double s[3];
+  int bx[3], c[3], tk[3];
+  double fr[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double t = a.rec[d][0] * x[0] + a.rec[d][1] * x[1] + a.rec[d][2] * x[2];
+    s[d] = t - floor(t);
+    if (a.nb[d] > 0) bx[d] = min(static_cast<int>(s[d] * a.nb[d]), a.nb[d] - 1);
+    if (a.ng[d] > 0) {
+      const double scaled = s[d] * a.ng[d];
+      int lowest = static_cast<int>(floor(scaled));
+      fr[d] = scaled - static_cast<double>(lowest);
+      if (lowest >= a.ng[d]) lowest -= a.ng[d];
+      c[d] = lowest;
+      tk[d] = lowest / a.tile;
+    }
+  }
+  const double qi = q[i];
+  if (s4) s4[i] = make_double4(s[0], s[1], s[2], qi);
+  if (box_key) box_key[i] = (bx[2] * a.nb[1] + bx[1]) * a.nb[0] + bx[0];
+  if (mesh_c) {
+    mesh_c[i] = make_int4(c[0], c[1], c[2], 0);
+    mesh_fr[i] = make_double4(fr[0], fr[1], fr[2], qi);
+    tile_key[i] = (tk[2] * a.ntiles[1] + tk[1]) * a.ntiles[0] + tk[0];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Bucket sort.  Counts and offsets are exact integers; the within-bucket order
+// is made deterministic by ranking each atom among its bucket by index.
+// ---------------------------------------------------------------------------
+__global__ void k_count(const int* __restrict__ key, int n, int* __restrict__ counts) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) atomicAdd(&counts[key[i]], 1);
+}
+
+// Exclusive scan of counts into starts[0..nkeys]; one CTA of 1024 threads.
+__global__ void __launch_bounds__(1024) k_scan(const int* __restrict__ counts, int nkeys,
+                                               int* __restrict__ starts) {
+  __shared__ int warp_sums[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int base = 0; base < nkeys; base += 1024) {
+    const int i = base + threadIdx.x;
+    const int v = i < nkeys ? counts[i] : 0;
+    int x = v;
+    for (int off = 1; off < 32; off <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, off);
+      if (lane >= off) x += y;
+    }
+    if (lane == 31) warp_sums[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      int w = warp_sums[lane];
+      for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, w, off);
+        if (lane >= off) w += y;
+      }
+      warp_sums[lane] = w;
+    }
+    __syncthreads();
+    const int incl = x + (wid > 0 ? warp_sums[wid - 1] : 0);
+    if (i < nkeys) starts[i] = carry + incl - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry += incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) starts[nkeys] = carry;
+}
+
+__global__ void k_scatter(const int* __restrict__ key, int n, const int* __restrict__ starts,
+                          int* __restrict__ cursor, int* __restrict__ tmp) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int k = key[i];
+  tmp[starts[k] + atomicAdd(&cursor[k], 1)] = i;
+}
+
+__global__ void k_rank(const int* __restrict__ key, int n, const int* __restrict__ starts,
+                       const int* __restrict__ tmp, int* __restrict__ perm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int k = key[i];
+  const int b = starts[k], e = starts[k + 1];
+  int r = 0;
+  for (int j = b; j < e; ++j) r += tmp[j] < i;
+  perm[b + r] = i;
+}
+
+__global__ void k_permute4(const double4* __restrict__ in, const int* __restrict__ perm, int n,
+                           double4* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) out[k] = in[perm[k]];
+}
+__global__ void k_permute_int4(const int4* __restrict__ in, const int* __restrict__ perm, int n,
+                               int4* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) out[k] = in[perm[k]];
+}
+
+// ---------------------------------------------------------------------------
+// Charge sums: per-CTA partials, then one CTA sums them in order.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  return v;
+}
+
+template <int NV>
+__device__ void block_sum(double* v, double (*sh)[32]) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int j = 0; j < NV; ++j) v[j] = warp_sum(v[j]);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int j = 0; j < NV; ++j) sh[j][wid] = v[j];
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      double x = lane < nw ? sh[j][lane] : 0.0;
+      v[j] = warp_sum(x);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_charge_partial(const double* __restrict__ q, int n,
+                                                        double* __restrict__ partial) {
+  __shared__ double sh[3][32];
+  double v[3] = {0.0, 0.0, 0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double x = q[i];
+    v[0] += x;
+    v[1] += fabs(x);
+    v[2] += x * x;
+  }
+  block_sum<3>(v, sh);
+  if (threadIdx.x == 0)
+    for (int j = 0; j < 3; ++j) partial[3 * blockIdx.x + j] = v[j];
+}
+
+__global__ void __launch_bounds__(256) k_sum_partials(const double* __restrict__ partial, int np,
+                                                      int nv, double* __restrict__ out) {
+  __shared__ double sh[6][32];
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  for (int i = threadIdx.x; i < np; i += blockDim.x)
+    for (int j = 0; j < nv; ++j) v[j] += partial[static_cast<size_t>(nv) * i + j];
+  block_sum<6>(v, sh);
+  if (threadIdx.x == 0)
+    for (int j = 0; j < nv; ++j) out[j] = v[j];
+}
+
+// ---------------------------------------------------------------------------
+// Real-space pair sums.  One warp per (box-sorted) atom i; lanes stride over the
+// candidates of each contiguous run of neighbour boxes.
+// ---------------------------------------------------------------------------
+template <class Pair>
+__device__ __forceinline__ void for_each_candidate(const double4* __restrict__ srt,
+                                                   const int* __restrict__ box_start, int k,
+                                                   const double4& ai, const RealGeom& g,
+                                                   Pair& pair) {
+  const int lane = threadIdx.x & 31;
+  int b[3];
+  const double sv[3] = {ai.x, ai.y, ai.z};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) b[d] = min(static_cast<int>(sv[d] * g.nb[d]), g.nb[d] - 1);
+  for (int dz = -g.R[2]; dz <= g.R[2]; ++dz) {
+    const int bzr = b[2] + dz;
+    const int sz = floor_div(bzr, g.nb[2]);
+    const int wz = bzr - sz * g.nb[2];
+    for (int dy = -g.R[1]; dy <= g.R[1]; ++dy) {
+      const int byr = b[1] + dy;
+      const int sy = floor_div(byr, g.nb[1]);
+      const int wy = byr - sy * g.nb[1];
+      int dx = -g.R[0];
+      while (dx <= g.R[0]) {
+        const int bxr = b[0] + dx;
+        const int sx = floor_div(bxr, g.nb[0]);
+        const int wx = bxr - sx * g.nb[0];
+        const int len = min(g.R[0] - dx + 1, g.nb[0] - wx);
+        const int first = (wz * g.nb[1] + wy) * g.nb[0] + wx;
+        const int j0 = box_start[first], j1 = box_start[first + len];
+        const bool home_image = (sx == 0 && sy == 0 && sz == 0);
+        for (int j = j0 + lane; j < j1; j += 32) {
+          if (home_image && j == k) continue;
+          const double4 aj = srt[j];
+          const double d1 = (ai.x - aj.x) - sx, d2 = (ai.y - aj.y) - sy, d3 = (ai.z - aj.z) - sz;
+          double sep[3];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) sep[c] = d1 * g.lat[0][c] + d2 * g.lat[1][c] + d3 * g.lat[2][c];
+          pair(sep, aj.w);
+        }
+        dx += len;
+      }
+    }
+  }
+}
+
+// Pair term of fft/ewald_fft_3d_real.f90:153-172 (FP64), or its FP32 form.
+template <bool MIXED>
+struct EwaldPair {
+  double alpha, cut2, qi;
+  double pot = 0.0, f[3] = {0.0, 0.0, 0.0};
+  int bad = 0;
+  __device__ __forceinline__ void operator()(const double* sep, double qj) {
+    const double r2 = sep[0] * sep[0] + sep[1] * sep[1] + sep[2] * sep[2];
+    if (r2 < 1.0e-24) {
+      bad = 1;
+      return;
+    }
+    if (r2 > cut2) return;
+    if constexpr (!MIXED) {
+      const double r = sqrt(r2);
+      const double ec = erfc(alpha * r);
+      pot += qj * ec / r;
+      const double ff = qi * qj * (2.0 * alpha / kSqrtPi * exp(-alpha * alpha * r2) + ec / r) / r2;
+      f[0] += ff * sep[0];
+      f[1] += ff * sep[1];
+      f[2] += ff * sep[2];
+    } else {
+      const float r2f = static_cast<float>(r2);
+      const float af = static_cast<float>(alpha);
+      const float rinv = rsqrtf(r2f);
+      const float r = r2f * rinv;
+      const float ec = erfcf(af * r);
+      const float qjf = static_cast<float>(qj);
+      const float pe = qjf * ec * rinv;
+      pot += static_cast<double>(pe);
+      const float ff = static_cast<float>(qi) * qjf *
+                       (2.0f * af * 0.56418958354775628695f * expf(-af * af * r2f) + ec * rinv) *
+                       (rinv * rinv);
+      f[0] += static_cast<double>(ff * static_cast<float>(sep[0]));
+      f[1] += static_cast<double>(ff * static_cast<float>(sep[1]));
+      f[2] += static_cast<double>(ff * static_cast<float>(sep[2]));
+    }
+  }
+};
+
+template <bool MIXED>
+__global__ void __launch_bounds__(256) k_real_space(const double4* __restrict__ srt,
+                                                    const int* __restrict__ perm,
+                                                    const int* __restrict__ box_start, int n,
+                                                    RealGeom g, double alpha, double cut2,
+                                                    double* __restrict__ pot,
+                                                    double* __restrict__ force,
+                                                    int* __restrict__ err) {
+  const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (k >= n) return;
+  const double4 ai = srt[k];
+  EwaldPair<MIXED> pair;
+  pair.alpha = alpha;
+  pair.cut2 = cut2;
+  pair.qi = ai.w;
+  for_each_candidate(srt, box_start, k, ai, g, pair);
+  double v[4] = {pair.pot, pair.f[0], pair.f[1], pair.f[2]};
+#pragma unroll
+  for (int j = 0; j < 4; ++j) v[j] = warp_sum(v[j]);
+  const int bad = __any_sync(0xffffffffu, pair.bad);
+  if (lane == 0) {
+    const int i = perm[k];
+    pot[i] = v[0];
+    force[3 * i] = v[1];
+    force[3 * i + 1] = v[2];
+    force[3 * i + 2] = v[3];
+    if (bad) atomicOr(err, 1);
+  }
+}
+
+// Real-space virial of invRStress with addNeighbourContribsStress
+// (coulomb.F90:2836-2905).  Over the full list with a factor 1/2 (the half
+// list's pairs each appear twice), r (x) f + f (x) r with f = derivRTerm(r) q_i q_j
+// collapses to derivRTerm-scalar * q_i q_j * r (x) r.
+struct StressPair {
+  double alpha, cut2, qi;
+  double s[6] = {0, 0, 0, 0, 0, 0};  // xx, yy, zz, xy, xz, yz
+  int bad = 0;
+  __device__ __forceinline__ void operator()(const double* r, double qj) {
+    const double d2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    if (d2 > cut2) return;
+    if (d2 < 1.0e-24) {
+      bad = 1;
+      return;
+    }
+    const double rr = sqrt(d2);
+    const double fac = alpha * rr;
+    const double dr = (-2.0 / kSqrtPi * exp(-fac * fac) * fac - erfc(fac)) / (rr * rr * rr);
+    const double w = dr * qi * qj;
+    s[0] += w * r[0] * r[0];
+    s[1] += w * r[1] * r[1];
+    s[2] += w * r[2] * r[2];
+    s[3] += w * r[0] * r[1];
+    s[4] += w * r[0] * r[2];
+    s[5] += w * r[1] * r[2];
+  }
+};
+
+__global__ void __launch_bounds__(256) k_real_stress(const double4* __restrict__ srt,
+                                                     const int* __restrict__ box_start, int n,
+                                                     RealGeom g, double alpha, double cut2,
+                                                     double* __restrict__ partial6,
+                                                     int* __restrict__ err) {
+  const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (k >= n) return;
+  const double4 ai = srt[k];
+  StressPair pair;
+  pair.alpha = alpha;
+  pair.cut2 = cut2;
+  pair.qi = ai.w;
+  for_each_candidate(srt, box_start, k, ai, g, pair);
+#pragma unroll
+  for (int j = 0; j < 6; ++j) pair.s[j] = warp_sum(pair.s[j]);
+  const int bad = __any_sync(0xffffffffu, pair.bad);
+  if (lane == 0) {
+#pragma unroll
+    for (int j = 0; j < 6; ++j) partial6[6 * static_cast<size_t>(k) + j] = pair.s[j];
+    if (bad) atomicOr(err, 1);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Structure factors: one CTA per wave vector.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_structure_factors(const double* __restrict__ x,
+                                                           const double* __restrict__ q, int n,
+                                                           const double* __restrict__ kvec,
+                                                           double* __restrict__ out) {
+  __shared__ double sh[2][32];
+  const int v = blockIdx.x;
+  const double kx = kvec[3 * v], ky = kvec[3 * v + 1], kz = kvec[3 * v + 2];
+  double acc[2] = {0.0, 0.0};
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double ph = kx * x[3 * i] + ky * x[3 * i + 1] + kz * x[3 * i + 2];
+    double sn, cs;
+    sincos(ph, &sn, &cs);
+    acc[0] += q[i] * cs;
+    acc[1] += q[i] * sn;
+  }
+  block_sum<2>(acc, sh);
+  if (threadIdx.x == 0) {
+    out[2 * v] = acc[0];
+    out[2 * v + 1] = acc[1];
+  }
+}
+
+// Reciprocal part of invRStress (coulomb.F90:2800-2833) per half-space G: the
+// reference visits +G and -G separately; |S(-G)| = |S(G)| and the tensor is
+// even in G, so both visits are 2 x the +G term.
+__global__ void k_recip_stress(const double* __restrict__ kvec, const double* __restrict__ sk,
+                               int nk, double alpha, double* __restrict__ partial6) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nk) return;
+  const double g[3] = {kvec[3 * v], kvec[3 * v + 1], kvec[3 * v + 2]};
+  const double sr = sk[2 * v], si = sk[2 * v + 1];
+  const double a2 = alpha * alpha;
+  const double g2 = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+  const double im = 2.0 * (sr * sr + si * si) * exp(-g2 / (4.0 * a2)) / g2;
+  const double c = 2.0 * (1.0 / (4.0 * a2) + 1.0 / g2);
+  partial6[6 * v + 0] = (1.0 - c * g[0] * g[0]) * im;
+  partial6[6 * v + 1] = (1.0 - c * g[1] * g[1]) * im;
+  partial6[6 * v + 2] = (1.0 - c * g[2] * g[2]) * im;
+  partial6[6 * v + 3] = -c * g[0] * g[1] * im;
+  partial6[6 * v + 4] = -c * g[0] * g[2] * im;
+  partial6[6 * v + 5] = -c * g[1] * g[2] * im;
+}
+
+// Direct Fourier sum of ewald_direct_3d: thread per atom, loop over modes.
+__global__ void __launch_bounds__(256) k_direct_kspace(const double* __restrict__ x,
+                                                       const double* __restrict__ q, int n,
+                                                       const double* __restrict__ kvec,
+                                                       const double* __restrict__ wk,
+                                                       const double* __restrict__ sk, int nk,
+                                                       double* __restrict__ pot,
+                                                       double* __restrict__ force) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double xi = x[3 * i], yi = x[3 * i + 1], zi = x[3 * i + 2];
+  double p = 0.0, fx = 0.0, fy = 0.0, fz = 0.0;
+  for (int v = 0; v < nk; ++v) {
+    const double kx = kvec[3 * v], ky = kvec[3 * v + 1], kz = kvec[3 * v + 2];
+    double sn, cs;
+    sincos(kx * xi + ky * yi + kz * zi, &sn, &cs);
+    const double sr = sk[2 * v], si = sk[2 * v + 1];
+    const double lr = sr * cs + si * sn;
+    const double li = si * cs - sr * sn;
+    p += wk[v] * lr;
+    const double ff = wk[v] * li;
+    fx -= ff * kx;
+    fy -= ff * ky;
+    fz -= ff * kz;
+  }
+  pot[i] += p;
+  if (force) {
+    force[3 * i] += q[i] * fx;
+    force[3 * i + 1] += q[i] * fy;
+    force[3 * i + 2] += q[i] * fz;
+  }
+}
+
+inline int blocks_for(long n, int threads) { return static_cast<int>((n + threads - 1) / threads); }
+
+}  // namespace
+
+void launch_atom_prep(const double* pos, long sa, long sd, const double* q, int n, const Cell& cell,
+                      const int nb[3], const int ngrid[3], int tile, const int ntiles[3],
+                      double4* s4, int* box_key, int4* mesh_c, double4* mesh_fr, int* tile_key,
+                      cudaStream_t st) {
+  if (n == 0) return;
+  PrepArgs a;
+  for (int i = 0; i < 3; ++i) {
+    for (int d = 0; d < 3; ++d) a.rec[i][d] = cell.rec[i][d];
+    a.nb[i] = nb ? nb[i] : 0;
+    a.ng[i] = ngrid ? ngrid[i] : 0;
+    a.ntiles[i] = ntiles ? ntiles[i] : 0;
+  }
+  a.tile = tile > 0 ? tile : 1;
+  k_atom_prep<<<blocks_for(n, 256), 256, 0, st>>>(pos, sa, sd, q, n, a, s4, box_key, mesh_c,
+                                                  mesh_fr, tile_key);
+  ++g_launches;
+}
+
+void launch_bucket_sort(const int* key, int n, int nkeys, int* counts, int* cursor, int* starts,
+                        int* tmp, int* perm, cudaStream_t st) {
+  cudaMemsetAsync(counts, 0, sizeof(int) * nkeys, st);
+  cudaMemsetAsync(cursor, 0, sizeof(int) * nkeys, st);
+  if (n > 0) {
+    k_count<<<blocks_for(n, 256), 256, 0, st>>>(key, n, counts);
+    ++g_launches;
+  }
+  k_scan<<<1, 1024, 0, st>>>(counts, nkeys, starts);
+  ++g_launches;
+  if (n > 0) {
+    k_scatter<<<blocks_for(n, 256), 256, 0, st>>>(key, n, starts, cursor, tmp);
+    k_rank<<<blocks_for(n, 256), 256, 0, st>>>(key, n, starts, tmp, perm);
+    g_launches += 2;
+  }
+}
+
+void launch_permute4(const double4* in, const int* perm, int n, double4* out, cudaStream_t st) {
+  if (n == 0) return;
+  k_permute4<<<blocks_for(n, 256), 256, 0, st>>>(in, perm, n, out);
+  ++g_launches;
+}
+
+void launch_permute_int4(const int4* in, const int* perm, int n, int4* out, cudaStream_t st) {
+  if (n == 0) return;
+  k_permute_int4<<<blocks_for(n, 256), 256, 0, st>>>(in, perm, n, out);
+  ++g_launches;
+}
+
+void launch_charge_sums(const double* q, int n, double* partial, double* out, cudaStream_t st) {
+  const int blocks = 148;
+  k_charge_partial<<<blocks, 256, 0, st>>>(q, n, partial);
+  k_sum_partials<<<1, 256, 0, st>>>(partial, blocks, 3, out);
+  g_launches += 2;
+}
+
+void launch_real_space(const double4* srt, const int* perm, const int* box_start, int n,
+                       const RealGeom& g, double alpha, double r_cut, int mixed, double* pot,
+                       double* force, int* err, cudaStream_t st) {
+  if (n == 0) return;
+  const int blocks = blocks_for(static_cast<long>(n) * 32, 256);
+  if (mixed)
+    k_real_space<true><<<blocks, 256, 0, st>>>(srt, perm, box_start, n, g, alpha, r_cut * r_cut,
+                                               pot, force, err);
+  else
+    k_real_space<false><<<blocks, 256, 0, st>>>(srt, perm, box_start, n, g, alpha, r_cut * r_cut,
+                                                pot, force, err);
+  ++g_launches;
+}
+
+void launch_real_stress(const double4* srt, const int* box_start, int n, const RealGeom& g,
+                        double alpha, double max_r, double* partial6, double* out6, int* err,
+                        cudaStream_t st) {
+  if (n == 0) return;
+  k_real_stress<<<blocks_for(static_cast<long>(n) * 32, 256), 256, 0, st>>>(
+      srt, box_start, n, g, alpha, max_r * max_r, partial6, err);
+  k_sum_partials<<<1, 256, 0, st>>>(partial6, n, 6, out6);
+  g_launches += 2;
+}
+
+void launch_structure_factors(const double* coords3n, const double* q, int n, const double* kvec,
+                              int nk, double* out, cudaStream_t st) {
+  if (nk == 0) return;
+  k_structure_factors<<<nk, 256, 0, st>>>(coords3n, q, n, kvec, out);
+  ++g_launches;
+}
+
+void launch_recip_stress(const double* kvec, const double* sk, int nk, double alpha,
+                         double* partial6, double* out6, cudaStream_t st) {
+  if (nk > 0) {
+    k_recip_stress<<<blocks_for(nk, 256), 256, 0, st>>>(kvec, sk, nk, alpha, partial6);
+    ++g_launches;
+  }
+  k_sum_partials<<<1, 256, 0, st>>>(partial6, nk, 6, out6);
+  ++g_launches;
+}
+
+void launch_direct_kspace(const double* coords3n, const double* q, int n, const double* kvec,
+                          const double* wk, const double* sk, int nk, double* pot, double* force,
+                          cudaStream_t st) {
+  if (n == 0 || nk == 0) return;
+  k_direct_kspace<<<blocks_for(n, 256), 256, 0, st>>>(coords3n, q, n, kvec, wk, sk, nk, pot, force);
+  ++g_launches;
+}
+
+}  // namespace ewg

@@ -1,0 +1,191 @@
+/*
+ * ewald_b200.h -- C ABI of the B200 (sm_100a) 3D-periodic Ewald operator.
+ *
+ * This library replaces the engine behind DFTB+'s TCoulomb call surface for
+ * three-dimensionally periodic, charge-neutral SCC calculations: the real-space
+ * erfc pair sum over a linked-cell list, the Gaussian-window NFFT reciprocal
+ * sum (spread, FFT, influence weights, gather) and the stock electrostatic
+ * stress.  Every function returns an int status (EWG_OK == 0); see
+ * ewg_status_string().  All pointers are host memory unless a name ends in
+ * _device.  Outputs are overwritten, never accumulated into.
+ *
+ * Array conventions (atomic units: Bohr, e, Hartree):
+ *   positions(N,3)  Fortran column-major, as the reference library takes them:
+ *                   atom i component d at positions[i + N*d].
+ *   coords(3,N)     DFTB+'s own layout: atom i component d at coords[d + 3*i].
+ *   lat_rows(3,3)   Fortran latVecs with one lattice vector per ROW,
+ *                   column-major: a_i component d at lat_rows[i + 3*d].
+ *   lat_cols(3,3)   DFTB+'s latVecs with one lattice vector per COLUMN:
+ *                   a_i component d at lat_cols[d + 3*i].
+ *   force(3,N)      physical force -dU/dx, atom i component d at force[d + 3*i].
+ *
+ * Threading: one context per host thread; a context is not re-entrant.  Each
+ * context owns one CUDA stream and its device buffers; every call completes on
+ * the GPU before it returns.
+ */
+#ifndef EWALD_B200_H
+#define EWALD_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+/* Each replaces an `error stop` of the reference (paths relative to the
+ * reference project); a Fortran adapter maps non-zero codes back to
+ * `error stop ewg_status_string(rc)`. */
+enum {
+  EWG_OK = 0,
+  EWG_ERR_NPARTICLE = 1,    /* common/ewald_validation.f90:34  nParticle <= 0            */
+  EWG_ERR_ARG = 2,          /* NULL pointer, bad precision mode, shape mismatch            */
+  EWG_ERR_NOT_NEUTRAL = 3,  /* common/ewald_validation.f90:43-46  |sum q| > 1e-8 sum|q|   */
+  EWG_ERR_TOL = 4,          /* fft/ewald_fft_3d.f90:97-98  tol outside (0,1)              */
+  EWG_ERR_VOLUME = 5,       /* common/ewald_geometry.f90:78  cell volume <= 1e-18         */
+  EWG_ERR_ALPHA = 6,        /* fft/ewald_fft_3d_parameters.f90:121  alpha <= 0            */
+  EWG_ERR_COINCIDENT = 7,   /* fft/ewald_fft_3d_real.f90:159-160  r^2 < 1e-24             */
+  EWG_ERR_CUTOFF = 8,       /* direct/ewald_direct_3d.f90:117-118  cutoffs <= 0           */
+  EWG_ERR_ALPHA_SEARCH = 9, /* dftb/coulomb.F90:2172-2177  getOptimalAlphaEwald failed    */
+  EWG_ERR_LATTICE_SEARCH = 10, /* dftb/coulomb.F90:2239-2243, :2304-2308 getMaxG/REwald   */
+  EWG_ERR_OUT_OF_MEMORY = 11,
+  EWG_ERR_CUDA = 12,
+  EWG_ERR_DEVICE_TIMEOUT = 13,
+  EWG_ERR_GRID_TOO_LARGE = 14, /* an FFT length beyond the kernels' limit (4096 per axis)  */
+  EWG_ERR_NO_DEVICE = 15,
+  EWG_ERR_STATE = 16        /* call order: dftb/coulomb.F90 @:ASSERT(coordsUpdated_) etc. */
+};
+
+/* ---- precision forms ---------------------------------------------------- */
+enum {
+  EWG_PRECISION_FP64 = 0,  /* plain form: FP64 throughout, parity with the reference  */
+  EWG_PRECISION_MIXED = 1  /* FP32 stencils, FFT and pair terms; FP64 accumulation,
+                              self term, reductions and lattice setup                 */
+};
+
+/* Optional arguments of ewald_potential_force (fft/ewald_fft_3d.f90:36-77):
+ * alpha_in, r_cut_in, k_cut_in, nModes_in, windowCutoff_in.  A member counts
+ * only when its has_ flag is non-zero. */
+typedef struct {
+  int has_alpha, has_r_cut, has_k_cut, has_n_modes, has_window_cutoff;
+  double alpha, r_cut, k_cut;
+  int n_modes, window_cutoff;
+} ewg_overrides;
+
+/* TEwaldParameters3d (fft/ewald_fft_3d_parameters.f90:24-42). */
+typedef struct {
+  double alpha, r_cut, k_cut;
+  int window_cutoff;
+  int n_modes[3];
+} ewg_params;
+
+typedef struct ewg_context ewg_context;
+
+/* ---- context ------------------------------------------------------------ */
+int ewg_create(ewg_context** ctx, int device, int precision);
+int ewg_destroy(ewg_context* ctx);
+const char* ewg_status_string(int status);
+/* Run the context's work on the caller's CUDA stream (a cudaStream_t passed as
+ * void*); NULL returns to the context's own stream.  Calls still complete on
+ * the GPU before they return. */
+int ewg_set_stream(ewg_context* ctx, void* stream);
+/* Number of this library's kernels launched by the context so far. */
+long long ewg_kernel_launches(const ewg_context* ctx);
+/* Parameters the last evaluation on this context used. */
+int ewg_last_params(const ewg_context* ctx, ewg_params* out);
+
+/* ---- per-stage device timing ------------------------------------------- */
+/* With profiling on, every evaluation records CUDA events on the context's
+ * stream around each stage (atom preparation and sorting, real-space sum,
+ * window weights, spread, the five FFT passes, gather) and accumulates their
+ * device durations.  Stage names: ewg_stage_name(i), 0 <= i < ewg_stage_count(). */
+int ewg_set_profiling(ewg_context* ctx, int on);
+int ewg_stage_count(void);
+const char* ewg_stage_name(int stage);
+/* Accumulated milliseconds and launch counts per stage since the last reset. */
+int ewg_stage_times(const ewg_context* ctx, double* ms, long long* launches, int n);
+int ewg_reset_stage_times(ewg_context* ctx);
+
+/* ---- library surface: fft/ewald_fft_3d.f90 ------------------------------ */
+
+/* ewald_potential_force (fft/ewald_fft_3d.f90:36-134).  force may be NULL:
+ * potential-only evaluation with one forward transform instead of four.
+ * ov may be NULL (no overrides). */
+int ewg_potential_force(ewg_context* ctx, int n, const double* positions, const double* charges,
+                        const double* lat_rows, double tol, double* pot, double* force,
+                        const ewg_overrides* ov);
+
+/* ewald_parameters (fft/ewald_fft_3d.f90:142-191); host only. */
+int ewg_parameters(int n, const double* charges, const double* lat_rows, double tol,
+                   const ewg_overrides* ov, ewg_params* out);
+
+/* ewald_grid_memory (fft/ewald_fft_3d.f90:197-244) in the reference's own
+ * accounting (complex fine grid plus two mode arrays, GiB); host only. */
+int ewg_grid_memory(int n, const double* charges, const double* lat_rows, double tol,
+                    const ewg_overrides* ov, double* gigabytes);
+
+/* Device bytes this library would hold for such an evaluation (all buffers of
+ * the chosen precision), so that a caller can gate a size sweep. */
+int ewg_device_memory(int n, const double* charges, const double* lat_rows, double tol,
+                      const ewg_overrides* ov, int precision, int with_force, double* bytes);
+
+/* Same as ewg_potential_force with every array already in device memory:
+ * coords(3,N), charges(N), pot(N), force(3,N) all device pointers; lat_rows on
+ * the host.  The charge sums the parameter chain needs are reduced on the GPU
+ * and read back (24 bytes). */
+int ewg_potential_force_device(ewg_context* ctx, int n, const double* coords_device,
+                               const double* charges_device, const double* lat_rows, double tol,
+                               double* pot_device, double* force_device, const ewg_overrides* ov);
+
+/* ---- library surface: direct/ewald_direct_3d.f90 ------------------------ */
+
+/* ewald_potential_force of the direct O(N^2) engine (direct/ewald_direct_3d.f90:37-182):
+ * balanced splitting (common/ewald_alpha_search.f90:83-181), explicit image sum
+ * and a direct structure-factor sum over the k sphere.  The optional
+ * arguments are NULL when absent. */
+int ewg_direct_potential_force(ewg_context* ctx, int n, const double* positions,
+                               const double* charges, const double* lat_rows, double tol,
+                               double* pot, double* force, const double* alpha_in,
+                               const double* r_cut_in, const double* k_cut_in);
+
+/* ---- TCoulomb surface: src/dftbp/dftb/coulomb.F90 ----------------------- */
+
+/* TCoulomb%updateLatVecs (coulomb.F90:575-620): lattice vectors as columns. */
+int ewg_set_lattice(ewg_context* ctx, const double* lat_cols);
+/* TCoulomb%updateCoords (coulomb.F90:509-572): coords(3,N) of the central cell.
+ * Geometry-only device state (fractional coordinates, cell list, stencil
+ * weights) is rebuilt lazily at the next evaluation and then kept resident. */
+int ewg_set_coords(ewg_context* ctx, int n, const double* coords);
+/* TCoulomb%updateCharges (coulomb.F90:760-781): deltaQAtom(N). */
+int ewg_set_charges(ewg_context* ctx, const double* dq);
+/* fftEwaldShift (coulomb.F90:336-357) inside TCoulomb%updateShifts (:786-880):
+ * shift(N) = per-atom potential.  tol <= 0 or >= 1 selects 1e-9 as the
+ * adapter does (:348-349). */
+int ewg_shift(ewg_context* ctx, double tol, double* shift);
+/* fftEwaldAddGradients (coulomb.F90:361-385): shift(N) and the physical force
+ * F(3,N); the adapter subtracts F from DFTB+'s gradient array. */
+int ewg_shift_force(ewg_context* ctx, double tol, double* shift, double* force);
+/* invRStress (coulomb.F90:2777-2863) with the stock setup of updateLatVecs
+ * (getOptimalAlphaEwald when alpha <= 0, getMaxREwald, getMaxGEwald,
+ * getLatticePoints): sigma(3,3) column-major; TCoulomb%addStress then does
+ * stress -= 0.5*sigma (coulomb.F90:755). */
+int ewg_stress(ewg_context* ctx, double tol_ewald, double alpha, double* sigma);
+/* The splitting parameter, real cutoff, reciprocal cutoff and number of
+ * half-space reciprocal vectors the last ewg_stress call used. */
+int ewg_last_stress_setup(const ewg_context* ctx, double* alpha, double* max_r, double* max_g,
+                          int* n_g);
+
+/* ---- batched form ------------------------------------------------------- */
+
+/* ewald_potential_force on many independent cells in one submission.
+ * Cell c holds atoms [offsets[c], offsets[c+1]); coords(3, total) atom-major,
+ * lat_rows 9 doubles per cell (Fortran rows layout); pot(total), force(3,total).
+ * Each cell gets its own parameters from the reference chain.  Status of
+ * cell c goes to cell_status[c] when cell_status is not NULL; the return value
+ * is the first non-zero cell status. */
+int ewg_batch_potential_force(ewg_context* ctx, int n_cells, const int* offsets,
+                              const double* coords, const double* charges, const double* lat_rows,
+                              double tol, double* pot, double* force, int* cell_status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
