@@ -17,14 +17,14 @@ using namespace ewg;
 
 namespace {
 
-constexpr int kSpreadTileEdge = 16;
+constexpr int kTiles[3] = {kTileX, kTileY, kTileZ};
 
 // Device buffers owned by a context, grown on demand and reused across calls.
 enum BufId {
   B_POS, B_Q, B_POT, B_FORCE, B_POT_SR, B_F_SR, B_S4, B_S4S, B_BOXKEY, B_MC, B_MCS, B_FR, B_FRS,
   B_TILEKEY, B_COUNTS, B_CURSOR, B_BOXSTART, B_TILESTART, B_TMP, B_PERMBOX, B_PERMMESH, B_WTAB,
   B_QK, B_GRID, B_A1, B_A2, B_B2, B_B1, B_OUT, B_ERR, B_SUMS, B_PARTIAL, B_KVEC, B_SK, B_WK,
-  B_P6, B_O6, B_COORDS, B_COUNT
+  B_P6, B_O6, B_COORDS, B_SLOT, B_PART, B_COUNT
 };
 
 struct DevBuf {
@@ -193,8 +193,7 @@ int get_fft(ewg_context* c, int n, FftPlan& out) {
 
 // Home-tile lists along one axis: target tile t is reachable from home tile h
 // when some lowest point c in h has (c + o) mod n inside t for |o| <= m.
-int get_tiles(ewg_context* c, int n, int m, TileLists& out) {
-  const int T = kSpreadTileEdge;
+int get_tiles(ewg_context* c, int n, int m, int T, TileLists& out) {
   auto key = std::make_tuple(n, m, T);
   auto it = c->tiles.find(key);
   if (it == c->tiles.end()) {
@@ -311,6 +310,41 @@ int mesh_geometry(const Cell& cell, const ewg_params& p, MeshGeom& g) {
   return EWG_OK;
 }
 
+// Particle-side tiling: per axis the most tiles one stencil can touch
+// (brute force over start points, so partial last tiles are covered) and the
+// per-atom weight layout.
+void stencil_dims(const MeshGeom& g, const TileLists* tl, StencilDims& sd) {
+  int off = 0;
+  for (int d = 0; d < 3; ++d) {
+    const int n = g.n[d], T = tl[d].tile, nt = tl[d].ntiles;
+    sd.n[d] = n;
+    sd.T[d] = T;
+    sd.ntiles[d] = nt;
+    int most = nt;
+    if (2 * g.m + 1 < n) {
+      // Walk each start point's stencil through the tiles, as the weights kernel does.
+      most = 1;
+      for (int c = 0; c < n; ++c) {
+        const int p0 = ((c - g.m) % n + n) % n;
+        int t = p0 / T, covered = std::min((t + 1) * T, n) - p0, count = 1;
+        while (covered < 2 * g.m + 1) {
+          t = t + 1 == nt ? 0 : t + 1;
+          ++count;
+          covered += std::min((t + 1) * T, n) - t * T;
+        }
+        most = std::max(most, std::min(count, nt));
+      }
+    }
+    sd.S[d] = most;
+    sd.woff[d] = off;
+    off += most * T;
+  }
+  sd.wstride = off;
+  sd.m = g.m;
+  sd.b = g.b;
+  sd.pref = g.pref;
+}
+
 // Shared evaluation of ewald_potential_force on device-resident inputs.
 // pos: element (i, d) at pos[i * sa + d * sd]; q on device; outputs on device.
 int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const double* q,
@@ -327,17 +361,16 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
   if (rc) return rc;
   mp.mixed = mixed;
   mp.prof = &c->prof;
-  mp.tile = kSpreadTileEdge;
   for (int d = 0; d < 3; ++d) {
     if ((rc = get_fft(c, mp.g.n[d], mp.fft[d]))) return rc;
-    if ((rc = get_tiles(c, mp.g.n[d], mp.g.m, mp.tl[d]))) return rc;
-    mp.ntiles[d] = mp.tl[d].ntiles;
+    if ((rc = get_tiles(c, mp.g.n[d], mp.g.m, kTiles[d], mp.tl[d]))) return rc;
     const int H = mp.g.M[d] - mp.g.M[d] / 2;
     if ((rc = get_corr(c, mp.g.n[d], H, mp.g.m, &mp.corr2[d]))) return rc;
   }
+  stencil_dims(mp.g, mp.tl, mp.sd);
   const int nboxes = rg.nb[0] * rg.nb[1] * rg.nb[2];
-  const int ntiles = mp.ntiles[0] * mp.ntiles[1] * mp.ntiles[2];
-  const MeshSizes ms = mesh_sizes(mp.g, mixed, nc, n);
+  const int ntiles = mp.sd.ntiles[0] * mp.sd.ntiles[1] * mp.sd.ntiles[2];
+  const MeshSizes ms = mesh_sizes(mp.g, mp.sd, mixed, nc, n);
 
   double4* s4 = dbuf<double4>(c, B_S4, n, &rc);
   double4* s4s = dbuf<double4>(c, B_S4S, n, &rc);
@@ -364,6 +397,8 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
   void* B2 = dbuf<char>(c, B_B2, ms.B2, &rc);
   void* B1 = dbuf<char>(c, B_B1, ms.B1, &rc);
   void* outg = dbuf<char>(c, B_OUT, ms.out, &rc);
+  int4* slot = dbuf<int4>(c, B_SLOT, n, &rc);
+  double* part = dbuf<double>(c, B_PART, ms.part / 8, &rc);
   int* err = dbuf<int>(c, B_ERR, 1, &rc);
   if (rc) return rc;
 
@@ -376,15 +411,15 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
   cudaMemsetAsync(err, 0, sizeof(int), st);
   prof_mark(mp.prof, st, ST_PREP);
   if (!reuse) {
-    launch_atom_prep(pos, sa, sd, q, n, cell, rg.nb, mp.g.n, kSpreadTileEdge, mp.ntiles, s4, boxkey,
-                     mcv, fr, tilekey, st);
+    launch_atom_prep(pos, sa, sd, q, n, cell, rg.nb, mp.g.n, kTiles, mp.sd.ntiles, s4, boxkey, mcv,
+                     fr, tilekey, st);
     launch_bucket_sort(boxkey, n, nboxes, counts, cursor, boxstart, tmp, permbox, st);
     launch_permute4(s4, permbox, n, s4s, st);
     launch_bucket_sort(tilekey, n, ntiles, counts, cursor, tilestart, tmp, permmesh, st);
     launch_permute_int4(mcv, permmesh, n, mcs, st);
     launch_permute4(fr, permmesh, n, frs, st);
     prof_mark(mp.prof, st, ST_WEIGHTS);
-    launch_weights(mp, frs, n, wtab, qk, st);
+    launch_weights(mp, mcs, frs, n, wtab, qk, slot, st);
     if (resident) {
       c->resident.coords_version = c->coords_version;
       for (int d = 0; d < 3; ++d) {
@@ -396,25 +431,26 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
     }
   } else {
     // Geometry unchanged: refresh only the charges in the sorted layouts.
-    launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, nullptr, 1, nullptr, s4, nullptr, nullptr,
-                     nullptr, nullptr, st);
+    launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, nullptr, nullptr, nullptr, s4, nullptr,
+                     nullptr, nullptr, nullptr, st);
     launch_permute4(s4, permbox, n, s4s, st);
-    launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, mp.g.n, kSpreadTileEdge, mp.ntiles, nullptr,
+    launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, mp.g.n, kTiles, mp.sd.ntiles, nullptr,
                      nullptr, mcv, fr, tilekey, st);
     launch_permute4(fr, permmesh, n, frs, st);
     prof_mark(mp.prof, st, ST_WEIGHTS);
-    launch_weights(mp, frs, n, wtab, qk, st);
+    launch_weights(mp, mcs, frs, n, wtab, qk, slot, st);
   }
   prof_mark(mp.prof, st, ST_REAL);
   launch_real_space(s4s, permbox, boxstart, n, rg, p.alpha, p.r_cut, mixed, pot_sr, f_sr, err, st);
   prof_mark(mp.prof, st, ST_SPREAD);
-  launch_spread(mp, mcs, wtab, qk, tilestart, grid, st);
+  launch_spread(mp, slot, wtab, qk, tilestart, grid, st);
   launch_forward_and_weight(mp, grid, A1, A2, B2, nc, st);
   launch_inverse(mp, B2, B1, outg, nc, st);
   const double self_coef = -2.0 * p.alpha / std::sqrt(kPi);
   prof_mark(mp.prof, st, ST_GATHER);
-  launch_gather(mp, mcs, wtab, permmesh, outg, nc, n, q, self_coef, pot_sr, f_sr, pot,
-                want_force ? force : nullptr, st);
+  launch_gather(mp, slot, wtab, tilestart, outg, nc, part, st);
+  launch_gather_final(mp, slot, permmesh, part, nc, n, q, self_coef, pot_sr, f_sr, pot,
+                      want_force ? force : nullptr, st);
   prof_mark(mp.prof, st, -1);
   int herr = 0;
   cudaError_t e = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st);
@@ -498,6 +534,7 @@ int ewg_create(ewg_context** out, int device, int precision) {
   }
   c->stream = c->own_stream;
   int rc = mesh_configure_kernels();
+  if (!rc) rc = stencil_configure_kernels();
   if (rc) {
     delete c;
     return rc;
@@ -604,9 +641,18 @@ int ewg_device_memory(int n, const double* charges, const double* lat_rows, doub
   MeshGeom g;
   rc = mesh_geometry(cell, p, g);
   if (rc) return rc;
-  const MeshSizes s = mesh_sizes(g, precision == EWG_PRECISION_MIXED, with_force ? 4 : 1, n);
+  TileLists tl[3];
+  for (int d = 0; d < 3; ++d) {
+    tl[d].tile = kTiles[d];
+    tl[d].ntiles = (g.n[d] + kTiles[d] - 1) / kTiles[d];
+  }
+  StencilDims sd;
+  stencil_dims(g, tl, sd);
+  const MeshSizes s = mesh_sizes(g, sd, precision == EWG_PRECISION_MIXED, with_force ? 4 : 1, n);
   const double atoms = static_cast<double>(n) * (32 * 4 + 16 * 2 + 4 * 6 + 8 * 6);
-  *bytes = static_cast<double>(s.grid + s.A1 + s.A2 + s.B2 + s.B1 + s.out + s.wtab + s.qk) + atoms;
+  *bytes = static_cast<double>(s.grid + s.A1 + s.A2 + s.B2 + s.B1 + s.out + s.wtab + s.qk + s.slot +
+                               s.part) +
+           atoms;
   return EWG_OK;
 }
 
@@ -742,7 +788,7 @@ int ewg_direct_potential_force(ewg_context* c, int n, const double* positions,
     cudaMemcpyAsync(dwk, wk.data(), sizeof(double) * nk, cudaMemcpyHostToDevice, st);
   }
   cudaMemsetAsync(err, 0, sizeof(int), st);
-  launch_atom_prep(dcoords, 3, 1, dq, n, cell, rg.nb, nullptr, 1, nullptr, s4, boxkey, nullptr,
+  launch_atom_prep(dcoords, 3, 1, dq, n, cell, rg.nb, nullptr, nullptr, nullptr, s4, boxkey, nullptr,
                    nullptr, nullptr, st);
   launch_bucket_sort(boxkey, n, nboxes, counts, cursor, boxstart, tmp, permbox, st);
   launch_permute4(s4, permbox, n, s4s, st);
@@ -892,7 +938,7 @@ int ewg_stress(ewg_context* c, double tol_ewald, double alpha, double* sigma) {
   if (ng) cudaMemcpyAsync(dk, ss.g.data(), sizeof(double) * ss.g.size(), cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(err, 0, sizeof(int), st);
   c->resident.coords_version = -1;  // the sorted layout below is for max_r
-  launch_atom_prep(dcoords, 3, 1, dq, n, cell, rg.nb, nullptr, 1, nullptr, s4, boxkey, nullptr,
+  launch_atom_prep(dcoords, 3, 1, dq, n, cell, rg.nb, nullptr, nullptr, nullptr, s4, boxkey, nullptr,
                    nullptr, nullptr, st);
   launch_bucket_sort(boxkey, n, nboxes, counts, cursor, boxstart, tmp, permbox, st);
   launch_permute4(s4, permbox, n, s4s, st);

@@ -38,7 +38,7 @@ void prof_collect(Profiler* p);
 // box key, mesh lowest point and fraction (nfft/nfft.f90:122-159), mesh tile key.
 // positions: element (i, d) at pos[i * sa + d * sd].
 void launch_atom_prep(const double* pos, long sa, long sd, const double* q, int n, const Cell& cell,
-                      const int nb[3], const int ngrid[3], int tile, const int ntiles[3],
+                      const int nb[3], const int ngrid[3], const int tile[3], const int ntiles[3],
                       double4* s4, int* box_key, int4* mesh_c, double4* mesh_fr, int* tile_key,
                       cudaStream_t st);
 
@@ -88,25 +88,41 @@ void launch_direct_kspace(const double* coords3n, const double* q, int n, const 
 
 // ---- mesh (ewg_mesh.cu) ----------------------------------------------------
 
+// Tile shape of the spread and gather (points along x, y, z).
+constexpr int kTileX = 8, kTileY = 16, kTileZ = 16;
+
+// Geometry of the particle-side stencil work.
+struct StencilDims {
+  int n[3];        // fine grid
+  int T[3];        // tile edge per axis
+  int ntiles[3];   // tiles per axis
+  int S[3];        // most tiles one stencil touches per axis
+  int woff[3];     // per-atom weight offsets per axis
+  int wstride;     // per-atom weight count: sum S_d T_d
+  int m;           // window half-width
+  double b;        // window shape
+  double pref;     // 1/sqrt(pi b)
+};
+
 // Everything the mesh pipeline needs, resolved on the host.
 struct MeshPlan {
   MeshGeom g;
+  StencilDims sd;
   FftPlan fft[3];
   TileLists tl[3];
-  int tile;
-  int ntiles[3];
   int mixed;                      // 0: FP64, 1: FP32 storage/products
   Profiler* prof = nullptr;
-  const double* corr2[3] = {nullptr, nullptr, nullptr};  // squared deconvolution factors, index k + M/2
-  const double* kvec_unused = nullptr;
+  const double* corr2[3] = {nullptr, nullptr, nullptr};  // squared deconvolution factors, index k + H
 };
 
-// Stencil weights per mesh-sorted atom: wtab[(k*3 + d)*W + o].
-void launch_weights(const MeshPlan& mp, const double4* mesh_fr_sorted, int n, void* wtab,
-                    void* qk, cudaStream_t st);
+// Tiled window weights per mesh-sorted atom (wtab: wstride values per atom),
+// slot origin and count per axis (slot: first | count << 16 in x, y, z), and
+// the charges in mesh order (qk).
+void launch_weights(const MeshPlan& mp, const int4* mesh_c_sorted, const double4* mesh_fr_sorted,
+                    int n, void* wtab, void* qk, int4* slot, cudaStream_t st);
 
 // Tile-owned deterministic spread (adjoint_nfft_3d step 1, nfft/nfft.f90:253-278).
-void launch_spread(const MeshPlan& mp, const int4* mesh_c_sorted, const void* wtab, const void* qk,
+void launch_spread(const MeshPlan& mp, const int4* slot, const void* wtab, const void* qk,
                    const int* tile_start, void* grid, cudaStream_t st);
 
 // Pruned forward transform of the real grid to the compact spectrum, fused with
@@ -118,21 +134,26 @@ void launch_forward_and_weight(const MeshPlan& mp, const void* grid, void* A1, v
 // Remaining inverse passes B2 -> B1 -> interleaved real grids (nc per point).
 void launch_inverse(const MeshPlan& mp, const void* B2, void* B1, void* out, int nc, cudaStream_t st);
 
-// Gather (forward_nfft_3d step 3, nfft/nfft.f90:380-402) fused with the final
-// assembly (fft/ewald_fft_3d.f90:121-132): pot = sr + lr + self,
-// force = sr + q * lr.
-void launch_gather(const MeshPlan& mp, const int4* mesh_c_sorted, const void* wtab,
-                   const int* mesh_perm, const void* out_grid, int nc, int n, const double* q_orig,
-                   double self_coef, const double* pot_sr, const double* force_sr, double* pot,
-                   double* force, cudaStream_t st);
+// Gather (forward_nfft_3d step 3, nfft/nfft.f90:380-402): per-(atom, tile)
+// partial sums of the nc interleaved real grids into part (nslots * nc per atom).
+void launch_gather(const MeshPlan& mp, const int4* slot, const void* wtab, const int* tile_start,
+                   const void* out_grid, int nc, double* part, cudaStream_t st);
+
+// Fixed-order sum of each atom's partials with the final assembly
+// (fft/ewald_fft_3d.f90:121-132): pot = (sr + lr) + self, force = sr + q lr.
+void launch_gather_final(const MeshPlan& mp, const int4* slot, const int* mesh_perm,
+                         const double* part, int nc, int n, const double* q_orig, double self_coef,
+                         const double* pot_sr, const double* force_sr, double* pot, double* force,
+                         cudaStream_t st);
 
 // Device byte sizes of the mesh buffers.
 struct MeshSizes {
-  size_t grid, A1, A2, B2, B1, out, wtab, qk;
+  size_t grid, A1, A2, B2, B1, out, wtab, qk, slot, part;
 };
-MeshSizes mesh_sizes(const MeshGeom& g, int mixed, int nc, int natoms);
+MeshSizes mesh_sizes(const MeshGeom& g, const StencilDims& sd, int mixed, int nc, int natoms);
 
-// Smallest shared-memory layout checks and per-kernel configuration.
+// Shared-memory limits of the FFT and gather kernels (once per device).
 int mesh_configure_kernels();
+int stencil_configure_kernels();
 
 }  // namespace ewg

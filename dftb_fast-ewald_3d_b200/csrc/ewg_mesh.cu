@@ -31,149 +31,12 @@ namespace ewg {
 
 namespace {
 
-constexpr int kSpreadTile = 16;
-constexpr int kSpreadBatch = 32;
 constexpr int kFftThreads = 256;
 constexpr size_t kSmemBudget = 200 * 1024;
 
 __device__ __forceinline__ int pmod(int a, int n) {
   int r = a % n;
   return r < 0 ? r + n : r;
-}
-
-template <typename R>
-__device__ __forceinline__ void accumulate(double& acc, R s, R w) {
-  if constexpr (sizeof(R) == 8) {
-    acc = fma(static_cast<double>(s), static_cast<double>(w), acc);
-  } else {
-    acc += static_cast<double>(s * w);
-  }
-}
-
-// ---------------------------------------------------------------------------
-// Window weights (nfft/nfft.f90:122-159), evaluated in FP64 and stored in R.
-// ---------------------------------------------------------------------------
-template <typename R>
-__global__ void k_weights(const double4* __restrict__ fr, int n, int m, int W, double b,
-                          double pref, R* __restrict__ wtab, R* __restrict__ qk) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  const double4 f = fr[k];
-  const double fx[3] = {f.x, f.y, f.z};
-  R* out = wtab + static_cast<size_t>(k) * 3 * W;
-  for (int d = 0; d < 3; ++d)
-    for (int o = -m; o <= m; ++o) {
-      const double dd = fx[d] - static_cast<double>(o);
-      out[d * W + o + m] = static_cast<R>(pref * exp(-(dd * dd) / b));
-    }
-  qk[k] = static_cast<R>(f.w);
-}
-
-// ---------------------------------------------------------------------------
-// Spread.  A CTA owns a 16^3 tile of the fine grid; thread (py, pz) owns the
-// x-pencil of 16 points at (y0+py, z0+pz) and keeps it in registers.  The atoms
-// that can reach the tile live in a fixed set of home tiles (atoms are bucketed
-// by the tile of their lowest stencil point); batches of them are staged in
-// shared memory as per-tile folded weight vectors and applied as rank-1
-// updates.  Every grid point is written once by its owner: no atomics, no
-// zeroing pass, and a summation order fixed by the sorted atom order.
-// ---------------------------------------------------------------------------
-template <typename R>
-__global__ void __launch_bounds__(256) k_spread(const int4* __restrict__ mc,
-                                                const R* __restrict__ wtab,
-                                                const R* __restrict__ qk,
-                                                const int* __restrict__ tile_start, TileLists lx,
-                                                TileLists ly, TileLists lz, int n1, int n2, int n3,
-                                                int m, int W, R* __restrict__ grid) {
-  constexpr int T = kSpreadTile;
-  constexpr int B = kSpreadBatch;
-  __shared__ R sW[3][B][T];
-  __shared__ int sStart[64];
-  __shared__ int sPrefix[65];
-  __shared__ int sAtom[B];
-
-  const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
-  const int org[3] = {tx * T, ty * T, tz * T};
-  const int ext[3] = {min(T, n1 - org[0]), min(T, n2 - org[1]), min(T, n3 - org[2])};
-  const int nn[3] = {n1, n2, n3};
-  const int py = threadIdx.x % T, pz = threadIdx.x / T;
-
-  double acc[T];
-#pragma unroll
-  for (int x = 0; x < T; ++x) acc[x] = 0.0;
-
-  const int lenx = lx.len[tx], leny = ly.len[ty], lenz = lz.len[tz];
-  const int nh = lenx * leny * lenz;
-  for (int h0 = 0; h0 < nh; h0 += 64) {
-    const int hc = min(64, nh - h0);
-    __syncthreads();
-    if (threadIdx.x < hc) {
-      const int h = h0 + threadIdx.x;
-      const int ix = h % lenx, iy = (h / lenx) % leny, iz = h / (lenx * leny);
-      const int home = (lz.home[tz * lz.maxlen + iz] * ly.ntiles + ly.home[ty * ly.maxlen + iy]) *
-                           lx.ntiles +
-                       lx.home[tx * lx.maxlen + ix];
-      const int s0 = tile_start[home];
-      sStart[threadIdx.x] = s0;
-      sPrefix[threadIdx.x + 1] = tile_start[home + 1] - s0;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      sPrefix[0] = 0;
-      for (int i = 1; i <= hc; ++i) sPrefix[i] += sPrefix[i - 1];
-    }
-    __syncthreads();
-    const int total = sPrefix[hc];
-    for (int b0 = 0; b0 < total; b0 += B) {
-      const int nb = min(B, total - b0);
-      if (threadIdx.x < nb) {
-        const int f = b0 + threadIdx.x;
-        int lo = 0, hi = hc - 1;  // last slot with prefix <= f
-        while (lo < hi) {
-          const int mid = (lo + hi + 1) >> 1;
-          if (sPrefix[mid] <= f)
-            lo = mid;
-          else
-            hi = mid - 1;
-        }
-        sAtom[threadIdx.x] = sStart[lo] + (f - sPrefix[lo]);
-      }
-      __syncthreads();
-      for (int it = threadIdx.x; it < nb * 3 * T; it += blockDim.x) {
-        const int a = it / (3 * T);
-        const int r = it - a * 3 * T;
-        const int d = r / T;
-        const int p = r - d * T;
-        const int k = sAtom[a];
-        R w = R(0);
-        if (p < ext[d]) {
-          const int4 c4 = mc[k];
-          const int c = d == 0 ? c4.x : (d == 1 ? c4.y : c4.z);
-          int o = pmod(org[d] + p - c, nn[d]);
-          while (o > m) o -= nn[d];
-          const R* wk = wtab + (static_cast<size_t>(k) * 3 + d) * W;
-          for (; o >= -m; o -= nn[d]) w += wk[o + m];
-          if (d == 2) w *= qk[k];
-        }
-        sW[d][a][p] = w;
-      }
-      __syncthreads();
-      for (int a = 0; a < nb; ++a) {
-        const R s = sW[1][a][py] * sW[2][a][pz];
-        if (s != R(0)) {
-#pragma unroll
-          for (int x = 0; x < T; ++x) accumulate<R>(acc[x], s, sW[0][a][x]);
-        }
-      }
-      __syncthreads();
-    }
-  }
-  if (py < ext[1] && pz < ext[2]) {
-    R* row = grid + (static_cast<size_t>(org[2] + pz) * n2 + org[1] + py) * n1 + org[0];
-#pragma unroll
-    for (int x = 0; x < T; ++x)
-      if (x < ext[0]) row[x] = static_cast<R>(acc[x]);
-  }
 }
 
 // ---------------------------------------------------------------------------
@@ -423,85 +286,9 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_x_c2r(const cx<R>* __restri
   }
 }
 
-// ---------------------------------------------------------------------------
-// Gather: one warp per atom, lanes along o1, rows (o2, o3) in order.  Sum of
-// w1 (w2 w3) g over the (2m+1)^3 stencil (nfft/nfft.f90:384-401), fused with
-// the final assembly of potential and force.
-// ---------------------------------------------------------------------------
-template <typename R, int NC>
-__global__ void __launch_bounds__(256) k_gather(const int4* __restrict__ mc,
-                                                const R* __restrict__ wtab,
-                                                const int* __restrict__ perm,
-                                                const R* __restrict__ grid, int n1, int n2, int n3,
-                                                int m, int W, int n, const double* __restrict__ q,
-                                                double self_coef, const double* __restrict__ pot_sr,
-                                                const double* __restrict__ f_sr,
-                                                double* __restrict__ pot,
-                                                double* __restrict__ force) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (warp >= n) return;
-  const int4 c = mc[warp];
-  const R* wt = wtab + static_cast<size_t>(warp) * 3 * W;
-  double acc[NC];
-#pragma unroll
-  for (int j = 0; j < NC; ++j) acc[j] = 0.0;
-  const int nlane = (W + 31) / 32;
-  for (int o3 = 0; o3 < W; ++o3) {
-    const int i3 = pmod(c.z + o3 - m, n3);
-    const R w3 = wt[2 * W + o3];
-    for (int o2 = 0; o2 < W; ++o2) {
-      const int i2 = pmod(c.y + o2 - m, n2);
-      const R s = wt[W + o2] * w3;
-      const size_t rowbase = (static_cast<size_t>(i3) * n2 + i2) * n1;
-      for (int li = 0; li < nlane; ++li) {
-        const int o1 = lane + 32 * li;
-        if (o1 < W) {
-          const int i1 = pmod(c.x + o1 - m, n1);
-          const R w = wt[o1] * s;
-          const R* g = grid + (rowbase + i1) * NC;
-#pragma unroll
-          for (int j = 0; j < NC; ++j) accumulate<R>(acc[j], w, g[j]);
-        }
-      }
-    }
-  }
-#pragma unroll
-  for (int j = 0; j < NC; ++j)
-    for (int off = 16; off > 0; off >>= 1) acc[j] += __shfl_down_sync(0xffffffffu, acc[j], off);
-  if (lane == 0) {
-    const int i = perm[warp];
-    const double qi = q[i];
-    pot[i] = (pot_sr[i] + acc[0]) + self_coef * qi;
-    if (NC == 4 && force) {
-#pragma unroll
-      for (int d = 0; d < 3; ++d) force[3 * i + d] = f_sr[3 * i + d] + qi * acc[1 + d];
-    }
-  }
-}
-
 template <typename R>
 size_t cbytes() {
   return sizeof(cx<R>);
-}
-
-template <typename R>
-void weights_impl(const MeshPlan& mp, const double4* fr, int n, void* wtab, void* qk,
-                  cudaStream_t st) {
-  if (n == 0) return;
-  k_weights<R><<<(n + 127) / 128, 128, 0, st>>>(fr, n, mp.g.m, mp.g.W, mp.g.b, mp.g.pref,
-                                                 static_cast<R*>(wtab), static_cast<R*>(qk));
-  ++g_launches;
-}
-
-template <typename R>
-void spread_impl(const MeshPlan& mp, const int4* mc, const void* wtab, const void* qk,
-                 const int* tile_start, void* grid, cudaStream_t st) {
-  dim3 grd(mp.ntiles[0], mp.ntiles[1], mp.ntiles[2]);
-  k_spread<R><<<grd, 256, 0, st>>>(mc, static_cast<const R*>(wtab), static_cast<const R*>(qk),
-                                    tile_start, mp.tl[0], mp.tl[1], mp.tl[2], mp.g.n[0],
-                                    mp.g.n[1], mp.g.n[2], mp.g.m, mp.g.W, static_cast<R*>(grid));
-  ++g_launches;
 }
 
 int lines_for(size_t per_line_bytes, int cap) {
@@ -580,33 +367,13 @@ void inverse_impl(const MeshPlan& mp, const void* B2v, void* B1v, void* out, int
     const int nrows = n2 * n3;
     // All components of a row pair in one CTA when they fit, else one per CTA.
     const int ncg = 2 * static_cast<size_t>(nc) * n1 * cb <= kSmemBudget ? nc : 1;
-    const int P = lines_for(2 * static_cast<size_t>(ncg) * n1 * cb, 4);
+    const int P = lines_for(2 * static_cast<size_t>(ncg) * n1 * cb, ncg == 1 ? 8 : 2);
     const size_t sm = 2 * static_cast<size_t>(P) * ncg * n1 * cb;
     dim3 grd((nrows / 2 + P - 1) / P, nc / ncg);
     k_fft_x_c2r<R><<<grd, kFftThreads, sm, st>>>(B1, static_cast<R*>(out), n1, nrows, g.K1, nc, ncg,
                                                  P, mp.fft[0]);
     ++g_launches;
   }
-}
-
-template <typename R>
-void gather_impl(const MeshPlan& mp, const int4* mc, const void* wtab, const int* perm,
-                 const void* grid, int nc, int n, const double* q, double self_coef,
-                 const double* pot_sr, const double* f_sr, double* pot, double* force,
-                 cudaStream_t st) {
-  if (n == 0) return;
-  const int threads = 256;
-  const int blocks = (n * 32 + threads - 1) / threads;
-  const MeshGeom& g = mp.g;
-  if (nc == 4)
-    k_gather<R, 4><<<blocks, threads, 0, st>>>(mc, static_cast<const R*>(wtab), perm,
-                                               static_cast<const R*>(grid), g.n[0], g.n[1], g.n[2],
-                                               g.m, g.W, n, q, self_coef, pot_sr, f_sr, pot, force);
-  else
-    k_gather<R, 1><<<blocks, threads, 0, st>>>(mc, static_cast<const R*>(wtab), perm,
-                                               static_cast<const R*>(grid), g.n[0], g.n[1], g.n[2],
-                                               g.m, g.W, n, q, self_coef, pot_sr, f_sr, pot, nullptr);
-  ++g_launches;
 }
 
 template <typename... K>
@@ -625,22 +392,6 @@ int mesh_configure_kernels() {
   return cudaGetLastError() == cudaSuccess ? EWG_OK : EWG_ERR_CUDA;
 }
 
-void launch_weights(const MeshPlan& mp, const double4* fr, int n, void* wtab, void* qk,
-                    cudaStream_t st) {
-  if (mp.mixed)
-    weights_impl<float>(mp, fr, n, wtab, qk, st);
-  else
-    weights_impl<double>(mp, fr, n, wtab, qk, st);
-}
-
-void launch_spread(const MeshPlan& mp, const int4* mc, const void* wtab, const void* qk,
-                   const int* tile_start, void* grid, cudaStream_t st) {
-  if (mp.mixed)
-    spread_impl<float>(mp, mc, wtab, qk, tile_start, grid, st);
-  else
-    spread_impl<double>(mp, mc, wtab, qk, tile_start, grid, st);
-}
-
 void launch_forward_and_weight(const MeshPlan& mp, const void* grid, void* A1, void* A2, void* B2,
                                int nc, cudaStream_t st) {
   if (mp.mixed)
@@ -655,17 +406,6 @@ void launch_inverse(const MeshPlan& mp, const void* B2, void* B1, void* out, int
     inverse_impl<float>(mp, B2, B1, out, nc, st);
   else
     inverse_impl<double>(mp, B2, B1, out, nc, st);
-}
-
-void launch_gather(const MeshPlan& mp, const int4* mc, const void* wtab, const int* perm,
-                   const void* grid, int nc, int n, const double* q, double self_coef,
-                   const double* pot_sr, const double* f_sr, double* pot, double* force,
-                   cudaStream_t st) {
-  if (mp.mixed)
-    gather_impl<float>(mp, mc, wtab, perm, grid, nc, n, q, self_coef, pot_sr, f_sr, pot, force, st);
-  else
-    gather_impl<double>(mp, mc, wtab, perm, grid, nc, n, q, self_coef, pot_sr, f_sr, pot, force,
-                        st);
 }
 
 void prof_mark(Profiler* p, cudaStream_t st, int stage) {
@@ -690,7 +430,7 @@ void prof_collect(Profiler* p) {
   p->n = 0;
 }
 
-MeshSizes mesh_sizes(const MeshGeom& g, int mixed, int nc, int natoms) {
+MeshSizes mesh_sizes(const MeshGeom& g, const StencilDims& sd, int mixed, int nc, int natoms) {
   const size_t r = mixed ? 4 : 8, c = 2 * r;
   const size_t n1 = g.n[0], n2 = g.n[1], n3 = g.n[2];
   MeshSizes s;
@@ -700,8 +440,10 @@ MeshSizes mesh_sizes(const MeshGeom& g, int mixed, int nc, int natoms) {
   s.B2 = nc * n3 * g.K2 * g.K1 * c;
   s.B1 = nc * n3 * n2 * g.K1 * c;
   s.out = nc * n1 * n2 * n3 * r;
-  s.wtab = static_cast<size_t>(natoms) * 3 * g.W * r;
+  s.wtab = static_cast<size_t>(natoms) * sd.wstride * r;
   s.qk = static_cast<size_t>(natoms) * r;
+  s.slot = static_cast<size_t>(natoms) * 16;
+  s.part = static_cast<size_t>(natoms) * sd.S[0] * sd.S[1] * sd.S[2] * nc * 8;
   return s;
 }
 

@@ -40,7 +40,7 @@ struct PrepArgs {
   double rec[3][3];
   int nb[3];
   int ng[3];
-  int tile;
+  int tile[3];
   int ntiles[3];
 };
 
@@ -66,7 +66,7 @@ __global__ void k_atom_prep(const double* __restrict__ pos, long sa, long sd,
       fr[d] = scaled - static_cast<double>(lowest);
       if (lowest >= a.ng[d]) lowest -= a.ng[d];
       c[d] = lowest;
-      tk[d] = lowest / a.tile;
+      tk[d] = lowest / a.tile[d];
     }
   }
   const double qi = q[i];
@@ -460,7 +460,7 @@ inline int blocks_for(long n, int threads) { return static_cast<int>((n + thread
 }  // namespace
 
 void launch_atom_prep(const double* pos, long sa, long sd, const double* q, int n, const Cell& cell,
-                      const int nb[3], const int ngrid[3], int tile, const int ntiles[3],
+                      const int nb[3], const int ngrid[3], const int tile[3], const int ntiles[3],
                       double4* s4, int* box_key, int4* mesh_c, double4* mesh_fr, int* tile_key,
                       cudaStream_t st) {
   if (n == 0) return;
@@ -470,8 +470,8 @@ void launch_atom_prep(const double* pos, long sa, long sd, const double* q, int 
     a.nb[i] = nb ? nb[i] : 0;
     a.ng[i] = ngrid ? ngrid[i] : 0;
     a.ntiles[i] = ntiles ? ntiles[i] : 0;
+    a.tile[i] = tile ? tile[i] : 1;
   }
-  a.tile = tile > 0 ? tile : 1;
   k_atom_prep<<<blocks_for(n, 256), 256, 0, st>>>(pos, sa, sd, q, n, a, s4, box_key, mesh_c,
                                                   mesh_fr, tile_key);
   ++g_launches;
