@@ -24,7 +24,7 @@ enum BufId {
   B_POS, B_Q, B_POT, B_FORCE, B_POT_SR, B_F_SR, B_S4, B_S4S, B_BOXKEY, B_MC, B_MCS, B_FR, B_FRS,
   B_TILEKEY, B_COUNTS, B_CURSOR, B_BOXSTART, B_TILESTART, B_TMP, B_PERMBOX, B_PERMMESH, B_WTAB,
   B_QK, B_GRID, B_A1, B_A2, B_B2, B_B1, B_OUT, B_ERR, B_SUMS, B_PARTIAL, B_KVEC, B_SK, B_WK,
-  B_P6, B_O6, B_COORDS, B_SLOT, B_PART, B_COUNT
+  B_P6, B_O6, B_COORDS, B_SLOT, B_PART, B_PAIRTMP, B_PAIRS, B_PAIRSTART, B_COUNT
 };
 
 struct DevBuf {
@@ -37,11 +37,6 @@ struct FftEntry {
   void* tw64 = nullptr;
   void* tw32 = nullptr;
   bool ok = false;
-};
-
-struct TileEntry {
-  TileLists tl;
-  int* dev = nullptr;
 };
 
 struct CorrEntry {
@@ -82,7 +77,6 @@ struct ewg_context {
   cudaStream_t own_stream = nullptr;
   DevBuf buf[B_COUNT];
   std::map<int, FftEntry> ffts;
-  std::map<std::tuple<int, int, int>, TileEntry> tiles;
   std::map<std::tuple<int, int, int>, CorrEntry> corrs;
   long long launches = 0;
   ewg_params last{};
@@ -117,7 +111,6 @@ struct ewg_context {
       cudaFree(kv.second.tw64);
       cudaFree(kv.second.tw32);
     }
-    for (auto& kv : tiles) cudaFree(kv.second.dev);
     for (auto& kv : corrs) cudaFree(kv.second.dev);
     for (auto& e : prof.ev)
       if (e) cudaEventDestroy(e);
@@ -188,55 +181,6 @@ int get_fft(ewg_context* c, int n, FftPlan& out) {
   }
   if (!it->second.ok) return EWG_ERR_GRID_TOO_LARGE;
   out = it->second.plan;
-  return EWG_OK;
-}
-
-// Home-tile lists along one axis: target tile t is reachable from home tile h
-// when some lowest point c in h has (c + o) mod n inside t for |o| <= m.
-int get_tiles(ewg_context* c, int n, int m, int T, TileLists& out) {
-  auto key = std::make_tuple(n, m, T);
-  auto it = c->tiles.find(key);
-  if (it == c->tiles.end()) {
-    const int nt = (n + T - 1) / T;
-    std::vector<std::vector<int>> lists(nt);
-    std::vector<char> reach(n);
-    for (int h = 0; h < nt; ++h) {
-      std::fill(reach.begin(), reach.end(), 0);
-      const int lo = h * T, hi = std::min(n, lo + T) - 1;
-      const long span = static_cast<long>(hi - lo) + 2L * m + 1;
-      if (span >= n) {
-        std::fill(reach.begin(), reach.end(), 1);
-      } else {
-        for (long x = lo - m; x <= hi + m; ++x) reach[((x % n) + n) % n] = 1;
-      }
-      for (int t = 0; t < nt; ++t) {
-        const int tl = t * T, th = std::min(n, tl + T);
-        bool any = false;
-        for (int x = tl; x < th && !any; ++x) any = reach[x];
-        if (any) lists[t].push_back(h);
-      }
-    }
-    int maxlen = 1;
-    for (auto& l : lists) maxlen = std::max<int>(maxlen, static_cast<int>(l.size()));
-    std::vector<int> host(nt + static_cast<size_t>(nt) * maxlen, 0);
-    for (int t = 0; t < nt; ++t) {
-      host[t] = static_cast<int>(lists[t].size());
-      for (size_t k = 0; k < lists[t].size(); ++k) host[nt + static_cast<size_t>(t) * maxlen + k] = lists[t][k];
-    }
-    TileEntry e;
-    if (cudaMalloc(&e.dev, sizeof(int) * host.size()) != cudaSuccess) {
-      cudaGetLastError();
-      return EWG_ERR_OUT_OF_MEMORY;
-    }
-    cudaMemcpy(e.dev, host.data(), sizeof(int) * host.size(), cudaMemcpyHostToDevice);
-    e.tl.tile = T;
-    e.tl.ntiles = nt;
-    e.tl.maxlen = maxlen;
-    e.tl.len = e.dev;
-    e.tl.home = e.dev + nt;
-    it = c->tiles.emplace(key, e).first;
-  }
-  out = it->second.tl;
   return EWG_OK;
 }
 
@@ -313,10 +257,10 @@ int mesh_geometry(const Cell& cell, const ewg_params& p, MeshGeom& g) {
 // Particle-side tiling: per axis the most tiles one stencil can touch
 // (brute force over start points, so partial last tiles are covered) and the
 // per-atom weight layout.
-void stencil_dims(const MeshGeom& g, const TileLists* tl, StencilDims& sd) {
+void stencil_dims(const MeshGeom& g, StencilDims& sd) {
   int off = 0;
   for (int d = 0; d < 3; ++d) {
-    const int n = g.n[d], T = tl[d].tile, nt = tl[d].ntiles;
+    const int n = g.n[d], T = kTiles[d], nt = (n + T - 1) / T;
     sd.n[d] = n;
     sd.T[d] = T;
     sd.ntiles[d] = nt;
@@ -363,11 +307,10 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
   mp.prof = &c->prof;
   for (int d = 0; d < 3; ++d) {
     if ((rc = get_fft(c, mp.g.n[d], mp.fft[d]))) return rc;
-    if ((rc = get_tiles(c, mp.g.n[d], mp.g.m, kTiles[d], mp.tl[d]))) return rc;
     const int H = mp.g.M[d] - mp.g.M[d] / 2;
     if ((rc = get_corr(c, mp.g.n[d], H, mp.g.m, &mp.corr2[d]))) return rc;
   }
-  stencil_dims(mp.g, mp.tl, mp.sd);
+  stencil_dims(mp.g, mp.sd);
   const int nboxes = rg.nb[0] * rg.nb[1] * rg.nb[2];
   const int ntiles = mp.sd.ntiles[0] * mp.sd.ntiles[1] * mp.sd.ntiles[2];
   const MeshSizes ms = mesh_sizes(mp.g, mp.sd, mixed, nc, n);
@@ -399,6 +342,10 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
   void* outg = dbuf<char>(c, B_OUT, ms.out, &rc);
   int4* slot = dbuf<int4>(c, B_SLOT, n, &rc);
   double* part = dbuf<double>(c, B_PART, ms.part / 8, &rc);
+  const int npairs_max = n * mp.sd.S[0] * mp.sd.S[1] * mp.sd.S[2];
+  int4* pairtmp = dbuf<int4>(c, B_PAIRTMP, npairs_max, &rc);
+  int2* pairs = dbuf<int2>(c, B_PAIRS, npairs_max, &rc);
+  int* pairstart = dbuf<int>(c, B_PAIRSTART, ntiles + 1, &rc);
   int* err = dbuf<int>(c, B_ERR, 1, &rc);
   if (rc) return rc;
 
@@ -420,6 +367,7 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
     launch_permute4(fr, permmesh, n, frs, st);
     prof_mark(mp.prof, st, ST_WEIGHTS);
     launch_weights(mp, mcs, frs, n, wtab, qk, slot, st);
+    launch_pair_bins(mp, slot, n, counts, cursor, pairstart, pairtmp, pairs, npairs_max, st);
     if (resident) {
       c->resident.coords_version = c->coords_version;
       for (int d = 0; d < 3; ++d) {
@@ -443,12 +391,12 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
   prof_mark(mp.prof, st, ST_REAL);
   launch_real_space(s4s, permbox, boxstart, n, rg, p.alpha, p.r_cut, mixed, pot_sr, f_sr, err, st);
   prof_mark(mp.prof, st, ST_SPREAD);
-  launch_spread(mp, slot, wtab, qk, tilestart, grid, st);
+  launch_spread(mp, pairstart, pairs, wtab, qk, grid, st);
   launch_forward_and_weight(mp, grid, A1, A2, B2, nc, st);
   launch_inverse(mp, B2, B1, outg, nc, st);
   const double self_coef = -2.0 * p.alpha / std::sqrt(kPi);
   prof_mark(mp.prof, st, ST_GATHER);
-  launch_gather(mp, slot, wtab, tilestart, outg, nc, part, st);
+  launch_gather(mp, pairstart, pairs, wtab, outg, nc, part, st);
   launch_gather_final(mp, slot, permmesh, part, nc, n, q, self_coef, pot_sr, f_sr, pot,
                       want_force ? force : nullptr, st);
   prof_mark(mp.prof, st, -1);
@@ -641,13 +589,8 @@ int ewg_device_memory(int n, const double* charges, const double* lat_rows, doub
   MeshGeom g;
   rc = mesh_geometry(cell, p, g);
   if (rc) return rc;
-  TileLists tl[3];
-  for (int d = 0; d < 3; ++d) {
-    tl[d].tile = kTiles[d];
-    tl[d].ntiles = (g.n[d] + kTiles[d] - 1) / kTiles[d];
-  }
   StencilDims sd;
-  stencil_dims(g, tl, sd);
+  stencil_dims(g, sd);
   const MeshSizes s = mesh_sizes(g, sd, precision == EWG_PRECISION_MIXED, with_force ? 4 : 1, n);
   const double atoms = static_cast<double>(n) * (32 * 4 + 16 * 2 + 4 * 6 + 8 * 6);
   *bytes = static_cast<double>(s.grid + s.A1 + s.A2 + s.B2 + s.B1 + s.out + s.wtab + s.qk + s.slot +

@@ -75,16 +75,6 @@ struct FftPlan {
   const float* tw32 = nullptr;   // interleaved complex, device
 };
 
-// Per-axis lists of "home" tiles whose atoms can reach a given target tile of
-// the mesh: home[t * maxlen + k] for k < len[t].
-struct TileLists {
-  int tile = 0;        // tile edge (points)
-  int ntiles = 0;
-  int maxlen = 0;
-  const int* len = nullptr;   // device
-  const int* home = nullptr;  // device
-};
-
 // Everything the mesh kernels need about one evaluation.
 struct MeshGeom {
   int n[3];        // fine grid = 2 * modes

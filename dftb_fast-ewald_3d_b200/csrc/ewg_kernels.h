@@ -48,6 +48,9 @@ void launch_atom_prep(const double* pos, long sa, long sd, const double* q, int 
 void launch_bucket_sort(const int* key, int n, int nkeys, int* counts, int* cursor, int* starts,
                         int* tmp, int* perm, cudaStream_t st);
 
+// Exclusive scan of counts[0..nkeys) into starts[0..nkeys] (one CTA).
+void launch_scan(const int* counts, int nkeys, int* starts, cudaStream_t st);
+
 // out[k] = in[perm[k]]
 void launch_permute4(const double4* in, const int* perm, int n, double4* out, cudaStream_t st);
 void launch_permute_int4(const int4* in, const int* perm, int n, int4* out, cudaStream_t st);
@@ -89,7 +92,7 @@ void launch_direct_kspace(const double* coords3n, const double* q, int n, const 
 // ---- mesh (ewg_mesh.cu) ----------------------------------------------------
 
 // Tile shape of the spread and gather (points along x, y, z).
-constexpr int kTileX = 8, kTileY = 16, kTileZ = 16;
+constexpr int kTileX = 8, kTileY = 8, kTileZ = 8;
 
 // Geometry of the particle-side stencil work.
 struct StencilDims {
@@ -109,7 +112,6 @@ struct MeshPlan {
   MeshGeom g;
   StencilDims sd;
   FftPlan fft[3];
-  TileLists tl[3];
   int mixed;                      // 0: FP64, 1: FP32 storage/products
   Profiler* prof = nullptr;
   const double* corr2[3] = {nullptr, nullptr, nullptr};  // squared deconvolution factors, index k + H
@@ -121,9 +123,15 @@ struct MeshPlan {
 void launch_weights(const MeshPlan& mp, const int4* mesh_c_sorted, const double4* mesh_fr_sorted,
                     int n, void* wtab, void* qk, int4* slot, cudaStream_t st);
 
+// Bins every (atom, tile) pair by tile, buckets ordered by atom index:
+// pairs[tile_start[t] .. tile_start[t+1]) = (atom, packed slot).  Scratch:
+// counts/cursor (ntiles), tmp (npairs_max); npairs_max = n * S_x * S_y * S_z.
+void launch_pair_bins(const MeshPlan& mp, const int4* slot, int n, int* counts, int* cursor,
+                      int* tile_start, int4* tmp, int2* pairs, int npairs_max, cudaStream_t st);
+
 // Tile-owned deterministic spread (adjoint_nfft_3d step 1, nfft/nfft.f90:253-278).
-void launch_spread(const MeshPlan& mp, const int4* slot, const void* wtab, const void* qk,
-                   const int* tile_start, void* grid, cudaStream_t st);
+void launch_spread(const MeshPlan& mp, const int* tile_start, const int2* pairs, const void* wtab,
+                   const void* qk, void* grid, cudaStream_t st);
 
 // Pruned forward transform of the real grid to the compact spectrum, fused with
 // the influence weights and the first inverse pass: grid -> A1 -> A2 -> B2.
@@ -136,7 +144,7 @@ void launch_inverse(const MeshPlan& mp, const void* B2, void* B1, void* out, int
 
 // Gather (forward_nfft_3d step 3, nfft/nfft.f90:380-402): per-(atom, tile)
 // partial sums of the nc interleaved real grids into part (nslots * nc per atom).
-void launch_gather(const MeshPlan& mp, const int4* slot, const void* wtab, const int* tile_start,
+void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs, const void* wtab,
                    const void* out_grid, int nc, double* part, cudaStream_t st);
 
 // Fixed-order sum of each atom's partials with the final assembly

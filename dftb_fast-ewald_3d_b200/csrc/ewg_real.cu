@@ -494,6 +494,11 @@ void launch_bucket_sort(const int* key, int n, int nkeys, int* counts, int* curs
   }
 }
 
+void launch_scan(const int* counts, int nkeys, int* starts, cudaStream_t st) {
+  k_scan<<<1, 1024, 0, st>>>(counts, nkeys, starts);
+  ++g_launches;
+}
+
 void launch_permute4(const double4* in, const int* perm, int n, double4* out, cudaStream_t st) {
   if (n == 0) return;
   k_permute4<<<blocks_for(n, 256), 256, 0, st>>>(in, perm, n, out);

@@ -1,26 +1,29 @@
 // ewg_stencil.cu -- the particle side of the NFFT: window weights, spread and
 // gather (nfft/nfft.f90:122-159, :253-278, :380-402).
 //
-// Tiling.  The fine grid is cut into tiles of 8 x 16 x 16 points.  A CTA owns
-// one tile; thread (py, pz) owns the x-pencil of 8 points at (y0+py, z0+pz)
-// and keeps it in registers.  Atoms are bucketed by the tile that holds the
-// lowest point of their stencil; the atoms that can reach a tile live in a
-// fixed set of home tiles (per-axis lists, host-built).
+// Tiling.  The fine grid is cut into tiles of 8 x 8 x 8 points.  Along each
+// axis an atom's stencil [c-m, c+m] (mod n) runs through at most S_d
+// consecutive tiles starting at tile f_d; the atom meets every tile of that
+// S_x x S_y x S_z block once ("slots").
 //
-// Weights.  Along each axis an atom's stencil [c-m, c+m] (mod n) touches a run
-// of at most S_d consecutive tiles, starting at tile f_d.  The weights kernel
-// stores, per atom and axis, the window weights already laid out per touched
-// tile (S_d * T_d values, zero outside the stencil and beyond the grid end;
-// points the stencil reaches twice on a small grid carry the sum).  A CTA then
-// copies an atom's three weight vectors for its tile with no index arithmetic.
+// Weights.  Per atom and axis the window weights are stored already laid out
+// per touched tile (S_d * 8 values; zero outside the stencil and beyond the
+// grid end; points a wrapping stencil reaches twice carry the sum).  A kernel
+// then reads an atom's weights for a tile with no index arithmetic.
 //
-// Spread: each thread accumulates q w1 w2 w3 into its pencil, atom by atom in
-// sorted order, and writes it once: no atomics, no zeroing, fixed order.
-// Gather: each thread forms its pencil's contribution to a batch of atoms;
-// a warp reduce-scatter sums the batch over the warp's pencils, the CTA sums its
-// warps in order, and the per-(atom, tile) partial goes to its own slot; a final
-// kernel adds each atom's slots in a fixed order.  Results are bitwise
-// reproducible.
+// Pairs.  Once per geometry, every (atom, tile) pair is binned by tile with a
+// counting sort whose buckets are ordered by atom index, so each tile owns an
+// exact, deterministic list of the atoms that reach it.
+//
+// Spread: a CTA owns a tile; each thread owns an x-pencil of 8 points in
+// registers and adds q w1 w2 w3 atom by atom in list order, then writes it
+// once (no atomics, no zeroing, fixed order).
+// Gather: a CTA stages its tile in shared memory; each warp takes 32 atoms of
+// the tile's list, one per lane, and walks the tile's 512 points in lockstep so
+// every grid value is a shared-memory broadcast; rows none of the warp's atoms
+// reach are skipped.  Each lane writes its atom's partial to the atom's slot for
+// this tile; a final kernel sums each atom's slots in a fixed order.  Results
+// are bitwise reproducible.
 
 #include <cuda_runtime.h>
 
@@ -33,9 +36,9 @@ namespace ewg {
 namespace {
 
 constexpr int TX = kTileX, TY = kTileY, TZ = kTileZ;
-constexpr int kThreads = TY * TZ;  // one thread per x-pencil
-static_assert(kThreads == 256, "tile shape assumes 256 threads");
-constexpr int kWindow = 256;       // candidates tested per compaction window
+constexpr int kPencils = TY * TZ;  // spread: one thread per x-pencil
+constexpr int kGatherThreads = 64;
+constexpr int kSpreadChunk = 64;   // atoms whose weights are staged at once
 
 __device__ __forceinline__ int pmod(int a, int n) {
   int r = a % n;
@@ -108,170 +111,106 @@ __global__ void k_weights_tiled(const int4* __restrict__ mc, const double4* __re
 }
 
 // ---------------------------------------------------------------------------
-// Candidate enumeration shared by spread and gather: the atoms of the home
-// tiles of this tile, filtered to those whose stencil reaches it, compacted in
-// candidate order into sList (atom index) and sSlots (packed slot indices).
+// (atom, tile) pair binning.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void load_home_chunk(const int* __restrict__ tile_start, const TileLists& lx,
-                                                const TileLists& ly, const TileLists& lz, int tx,
-                                                int ty, int tz, int h0, int hc, int* sStart,
-                                                int* sPrefix) {
-  const int lenx = lx.len[tx], leny = ly.len[ty];
-  if (threadIdx.x < hc) {
-    const int h = h0 + threadIdx.x;
-    const int ix = h % lenx, iy = (h / lenx) % leny, iz = h / (lenx * leny);
-    const int home = (lz.home[tz * lz.maxlen + iz] * ly.ntiles + ly.home[ty * ly.maxlen + iy]) *
-                         lx.ntiles +
-                     lx.home[tx * lx.maxlen + ix];
-    const int s0 = tile_start[home];
-    sStart[threadIdx.x] = s0;
-    sPrefix[threadIdx.x + 1] = tile_start[home + 1] - s0;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    sPrefix[0] = 0;
-    for (int i = 1; i <= hc; ++i) sPrefix[i] += sPrefix[i - 1];
-  }
-  __syncthreads();
-}
-
-// Tests candidates [w0, w0 + NT) of the chunk (NT = threads of the CTA);
-// returns the number kept.
-template <int NT = kThreads>
-__device__ __forceinline__ int compact_window(const int4* __restrict__ slot, const StencilDims& sd,
-                                              int tx, int ty, int tz, int w0, int total, int hc,
-                                              const int* sStart, const int* sPrefix, int* sList,
-                                              int* sSlots, int* sWarpCount) {
-  const int f = w0 + threadIdx.x;
-  int k = -1, packed = 0;
-  bool keep = false;
-  if (f < total) {
-    int lo = 0, hi = hc - 1;  // last home slot with prefix <= f (non-empty by construction)
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (sPrefix[mid] <= f)
-        lo = mid;
-      else
-        hi = mid - 1;
-    }
-    k = sStart[lo] + (f - sPrefix[lo]);
-    const int4 si = slot[k];
-    const int t3[3] = {tx, ty, tz};
-    const int s3[3] = {si.x, si.y, si.z};
-    keep = true;
-    int sl[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      sl[d] = pmod(t3[d] - slot_first(s3[d]), sd.ntiles[d]);
-      keep = keep && sl[d] < slot_count(s3[d]);
-    }
-    packed = sl[0] | (sl[1] << 8) | (sl[2] << 16);
-  }
-  const unsigned ballot = __ballot_sync(0xffffffffu, keep);
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  if (lane == 0) sWarpCount[wid] = __popc(ballot);
-  __syncthreads();
-  int base = 0, kept = 0;
-  for (int w = 0; w < NT / 32; ++w) {
-    const int cnt = sWarpCount[w];
-    if (w < wid) base += cnt;
-    kept += cnt;
-  }
-  if (keep) {
-    const int pos = base + __popc(ballot & ((1u << lane) - 1u));
-    sList[pos] = k;
-    sSlots[pos] = packed;
-  }
-  __syncthreads();
-  return kept;
-}
-
-// Copies batch atoms' per-tile weights into sW (layout [axis][a][T]).
-template <typename R, int B>
-__device__ __forceinline__ void fill_batch(const R* __restrict__ wtab, const R* __restrict__ qk,
-                                           const StencilDims& sd, const int* sList,
-                                           const int* sSlots, int b0, int nb, bool scale_q,
-                                           R (*sW1)[TX], R (*sW2)[TY], R (*sW3)[TZ]) {
-  constexpr int per = TX + TY + TZ;
-  for (int it = threadIdx.x; it < nb * per; it += blockDim.x) {
-    const int a = it / per;
-    const int r = it - a * per;
-    const int k = sList[b0 + a];
-    const int ps = sSlots[b0 + a];
-    const R* wk = wtab + static_cast<size_t>(k) * sd.wstride;
-    if (r < TX) {
-      sW1[a][r] = wk[sd.woff[0] + (ps & 0xff) * TX + r];
-    } else if (r < TX + TY) {
-      const int p = r - TX;
-      sW2[a][p] = wk[sd.woff[1] + ((ps >> 8) & 0xff) * TY + p];
-    } else {
-      const int p = r - TX - TY;
-      R w = wk[sd.woff[2] + ((ps >> 16) & 0xff) * TZ + p];
-      if (scale_q) w *= qk[k];
-      sW3[a][p] = w;
+template <class F>
+__device__ __forceinline__ void for_each_tile(const int4& si, const StencilDims& sd, F f) {
+  const int cx = slot_count(si.x), cy = slot_count(si.y), cz = slot_count(si.z);
+  const int fx = slot_first(si.x), fy = slot_first(si.y), fz = slot_first(si.z);
+  for (int sz = 0; sz < cz; ++sz) {
+    const int tz = (fz + sz) % sd.ntiles[2];
+    for (int sy = 0; sy < cy; ++sy) {
+      const int ty = (fy + sy) % sd.ntiles[1];
+      for (int sx = 0; sx < cx; ++sx) {
+        const int tx = (fx + sx) % sd.ntiles[0];
+        f((tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx, sx | (sy << 8) | (sz << 16));
+      }
     }
   }
 }
 
-template <typename R>
-__device__ __forceinline__ void accumulate(double& acc, R s, R w) {
-  if constexpr (sizeof(R) == 8) {
-    acc = fma(static_cast<double>(s), static_cast<double>(w), acc);
-  } else {
-    acc += static_cast<double>(s * w);
-  }
+__global__ void k_pair_count(const int4* __restrict__ slot, int n, StencilDims sd,
+                             int* __restrict__ counts) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  for_each_tile(slot[k], sd, [&](int tile, int) { atomicAdd(&counts[tile], 1); });
+}
+
+__global__ void k_pair_scatter(const int4* __restrict__ slot, int n, StencilDims sd,
+                               const int* __restrict__ starts, int* __restrict__ cursor,
+                               int4* __restrict__ tmp) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  for_each_tile(slot[k], sd, [&](int tile, int packed) {
+    tmp[starts[tile] + atomicAdd(&cursor[tile], 1)] = make_int4(k, packed, tile, 0);
+  });
+}
+
+// Orders each tile's bucket by atom index (atoms are unique within a bucket).
+// Entries past the last written one (npairs below the bound) hold tile = -1.
+__global__ void k_pair_rank(const int4* __restrict__ tmp, int nmax, const int* __restrict__ starts,
+                            int2* __restrict__ pairs) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nmax) return;
+  const int4 v = tmp[e];
+  if (v.z < 0) return;
+  const int b = starts[v.z], end = starts[v.z + 1];
+  int r = 0;
+  for (int j = b; j < end; ++j) r += tmp[j].x < v.x;
+  pairs[b + r] = make_int2(v.x, v.y);
 }
 
 // ---------------------------------------------------------------------------
 // Spread
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void __launch_bounds__(kThreads) k_spread_tiles(
-    const int4* __restrict__ slot, const R* __restrict__ wtab, const R* __restrict__ qk,
-    const int* __restrict__ tile_start, TileLists lx, TileLists ly, TileLists lz, StencilDims sd,
-    R* __restrict__ grid) {
-  constexpr int B = 16;
-  __shared__ R sW1[B][TX];
-  __shared__ R sW2[B][TY];
-  __shared__ R sW3[B][TZ];
-  __shared__ int sStart[64];
-  __shared__ int sPrefix[65];
-  __shared__ int sList[kWindow];
-  __shared__ int sSlots[kWindow];
-  __shared__ int sWarpCount[kThreads / 32];
-
+__global__ void __launch_bounds__(kPencils) k_spread_tiles(const int* __restrict__ tile_start,
+                                                           const int2* __restrict__ pairs,
+                                                           const R* __restrict__ wtab,
+                                                           const R* __restrict__ qk, StencilDims sd,
+                                                           R* __restrict__ grid) {
+  __shared__ R sW1[kSpreadChunk][TX];
+  __shared__ R sW2[kSpreadChunk][TY];
+  __shared__ R sW3[kSpreadChunk][TZ];
   const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
+  const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
   const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
   const int py = threadIdx.x % TY, pz = threadIdx.x / TY;
   double acc[TX];
 #pragma unroll
   for (int x = 0; x < TX; ++x) acc[x] = 0.0;
-
-  const int nh = lx.len[tx] * ly.len[ty] * lz.len[tz];
-  for (int h0 = 0; h0 < nh; h0 += 64) {
-    const int hc = min(64, nh - h0);
+  const int p0 = tile_start[tile], p1 = tile_start[tile + 1];
+  for (int b0 = p0; b0 < p1; b0 += kSpreadChunk) {
+    const int nb = min(kSpreadChunk, p1 - b0);
     __syncthreads();
-    load_home_chunk(tile_start, lx, ly, lz, tx, ty, tz, h0, hc, sStart, sPrefix);
-    const int total = sPrefix[hc];
-    for (int w0 = 0; w0 < total; w0 += kWindow) {
-      const int kept = compact_window(slot, sd, tx, ty, tz, w0, total, hc, sStart, sPrefix, sList,
-                                      sSlots, sWarpCount);
-      for (int b0 = 0; b0 < kept; b0 += B) {
-        const int nb = min(B, kept - b0);
-        fill_batch<R, B>(wtab, qk, sd, sList, sSlots, b0, nb, true, sW1, sW2, sW3);
-        __syncthreads();
-        for (int a = 0; a < nb; ++a) {
-          const R s = sW2[a][py] * sW3[a][pz];
-          if (s != R(0)) {
+    for (int it = threadIdx.x; it < nb * (TX + TY + TZ); it += blockDim.x) {
+      const int a = it / (TX + TY + TZ);
+      const int r = it - a * (TX + TY + TZ);
+      const int2 pr = pairs[b0 + a];
+      const R* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
+      if (r < TX) {
+        sW1[a][r] = wk[sd.woff[0] + (pr.y & 0xff) * TX + r];
+      } else if (r < TX + TY) {
+        sW2[a][r - TX] = wk[sd.woff[1] + ((pr.y >> 8) & 0xff) * TY + (r - TX)];
+      } else {
+        sW3[a][r - TX - TY] = wk[sd.woff[2] + (pr.y >> 16) * TZ + (r - TX - TY)] * qk[pr.x];
+      }
+    }
+    __syncthreads();
+    for (int a = 0; a < nb; ++a) {
+      const R s = sW2[a][py] * sW3[a][pz];
+      if (s != R(0)) {
 #pragma unroll
-            for (int x = 0; x < TX; ++x) accumulate<R>(acc[x], s, sW1[a][x]);
-          }
+        for (int x = 0; x < TX; ++x) {
+          if constexpr (sizeof(R) == 8)
+            acc[x] = fma(static_cast<double>(s), static_cast<double>(sW1[a][x]), acc[x]);
+          else
+            acc[x] += static_cast<double>(s * sW1[a][x]);
         }
-        __syncthreads();
       }
     }
   }
-  const int ey = min(TY, sd.n[1] - y0), ez = min(TZ, sd.n[2] - z0), ex = min(TX, sd.n[0] - x0);
+  const int ex = min(TX, sd.n[0] - x0), ey = min(TY, sd.n[1] - y0), ez = min(TZ, sd.n[2] - z0);
   if (py < ey && pz < ez) {
     R* row = grid + (static_cast<size_t>(z0 + pz) * sd.n[1] + y0 + py) * sd.n[0] + x0;
 #pragma unroll
@@ -281,115 +220,94 @@ __global__ void __launch_bounds__(kThreads) k_spread_tiles(
 }
 
 // ---------------------------------------------------------------------------
-// Gather: per-(atom, tile) partial sums of w1 w2 w3 g over the tile for NC
-// components, one thread per atom.  The tile's grid values sit in shared
-// memory and every lane of a warp reads the same point at the same time (a
-// broadcast), multiplying it by its own atom's weights; rows no lane of the
-// warp reaches are skipped.  Each thread writes its atom's partial to the
-// atom's slot for this tile, so no cross-thread reduction is needed.
+// Gather
 // ---------------------------------------------------------------------------
-constexpr int kGatherThreads = 128;
-
 template <typename R, int NC>
 __global__ void __launch_bounds__(kGatherThreads) k_gather_tiles(
-    const int4* __restrict__ slot, const R* __restrict__ wtab, const int* __restrict__ tile_start,
-    TileLists lx, TileLists ly, TileLists lz, StencilDims sd, const R* __restrict__ grid,
-    double* __restrict__ part) {
-  using V = typename std::conditional<NC == 4, typename std::conditional<sizeof(R) == 8, double4, float4>::type, R>::type;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  V* sG = reinterpret_cast<V*>(smem_raw);  // [TZ][TY][TX]
-  __shared__ int sStart[64];
-  __shared__ int sPrefix[65];
-  __shared__ int sList[kGatherThreads];
-  __shared__ int sSlots[kGatherThreads];
-  __shared__ int sWarpCount[kGatherThreads / 32];
-
+    const int* __restrict__ tile_start, const int2* __restrict__ pairs, const R* __restrict__ wtab,
+    StencilDims sd, const R* __restrict__ grid, double* __restrict__ part) {
+  using V = typename std::conditional<
+      NC == 4, typename std::conditional<sizeof(R) == 8, double4, float4>::type, R>::type;
+  __shared__ V sG[TZ * TY * TX];
   const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
+  const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
   const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
   const int ex = min(TX, sd.n[0] - x0), ey = min(TY, sd.n[1] - y0), ez = min(TZ, sd.n[2] - z0);
-
-  // Stage the tile (zero beyond the grid end).
+  const int p0 = tile_start[tile], p1 = tile_start[tile + 1];
+  if (p0 == p1) return;  // uniform across the CTA: no atom reaches this tile
   for (int t = threadIdx.x; t < TX * TY * TZ; t += blockDim.x) {
     const int x = t % TX, y = (t / TX) % TY, z = t / (TX * TY);
     V v;
     if (x < ex && y < ey && z < ez) {
-      v = reinterpret_cast<const V*>(grid)[(static_cast<size_t>(z0 + z) * sd.n[1] + y0 + y) * sd.n[0] + x0 + x];
+      v = reinterpret_cast<const V*>(grid)[(static_cast<size_t>(z0 + z) * sd.n[1] + y0 + y) * sd.n[0] +
+                                           x0 + x];
     } else {
-      v = V();
-      if constexpr (NC == 1) v = R(0);
+      if constexpr (NC == 4)
+        v = V{R(0), R(0), R(0), R(0)};
+      else
+        v = R(0);
     }
     sG[t] = v;
   }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int nslots = sd.S[0] * sd.S[1] * sd.S[2];
-  const int nh = lx.len[tx] * ly.len[ty] * lz.len[tz];
-  for (int h0 = 0; h0 < nh; h0 += 64) {
-    const int hc = min(64, nh - h0);
-    __syncthreads();
-    load_home_chunk(tile_start, lx, ly, lz, tx, ty, tz, h0, hc, sStart, sPrefix);
-    const int total = sPrefix[hc];
-    for (int w0 = 0; w0 < total; w0 += kGatherThreads) {
-      const int kept = compact_window<kGatherThreads>(slot, sd, tx, ty, tz, w0, total, hc, sStart,
-                                                      sPrefix, sList, sSlots, sWarpCount);
-      const bool active = threadIdx.x < kept;
-      R w1[TX], w2[TY];
-      int k = 0, ps = 0;
-      const R* wk3 = nullptr;  // this atom's z weights for the tile (read through L1)
-      if (active) {
-        k = sList[threadIdx.x];
-        ps = sSlots[threadIdx.x];
-        const R* wk = wtab + static_cast<size_t>(k) * sd.wstride;
+  for (int a0 = p0 + wid * 32; a0 < p1; a0 += kGatherThreads) {
+    const int e = a0 + lane;
+    const bool active = e < p1;
+    R w1[TX], w2[TY], w3[TZ];
+    int2 pr = make_int2(0, 0);
+    if (active) {
+      pr = pairs[e];
+      const R* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
 #pragma unroll
-        for (int x = 0; x < TX; ++x) w1[x] = wk[sd.woff[0] + (ps & 0xff) * TX + x];
+      for (int x = 0; x < TX; ++x) w1[x] = wk[sd.woff[0] + (pr.y & 0xff) * TX + x];
 #pragma unroll
-        for (int y = 0; y < TY; ++y) w2[y] = wk[sd.woff[1] + ((ps >> 8) & 0xff) * TY + y];
-        wk3 = wk + sd.woff[2] + ((ps >> 16) & 0xff) * TZ;
-      } else {
+      for (int y = 0; y < TY; ++y) w2[y] = wk[sd.woff[1] + ((pr.y >> 8) & 0xff) * TY + y];
 #pragma unroll
-        for (int x = 0; x < TX; ++x) w1[x] = R(0);
+      for (int z = 0; z < TZ; ++z) w3[z] = wk[sd.woff[2] + (pr.y >> 16) * TZ + z];
+    } else {
 #pragma unroll
-        for (int y = 0; y < TY; ++y) w2[y] = R(0);
-      }
-      double acc[NC];
+      for (int i = 0; i < TX; ++i) w1[i] = R(0);
 #pragma unroll
-      for (int c = 0; c < NC; ++c) acc[c] = 0.0;
-      // Warps with no atom skip the whole tile (warp-uniform).
-      if (__any_sync(0xffffffffu, active)) {
-        for (int z = 0; z < TZ; ++z) {
-          const R w3 = active ? wk3[z] : R(0);
-          if (!__any_sync(0xffffffffu, w3 != R(0))) continue;
+      for (int i = 0; i < TY; ++i) w2[i] = R(0);
 #pragma unroll
-          for (int y = 0; y < TY; ++y) {
-            const R w23 = w2[y] * w3;
-            if (!__any_sync(0xffffffffu, w23 != R(0))) continue;
-            R rs[NC];
+      for (int i = 0; i < TZ; ++i) w3[i] = R(0);
+    }
+    double acc[NC];
 #pragma unroll
-            for (int c = 0; c < NC; ++c) rs[c] = R(0);
-            const V* row = sG + (z * TY + y) * TX;
+    for (int c = 0; c < NC; ++c) acc[c] = 0.0;
 #pragma unroll
-            for (int x = 0; x < TX; ++x) {
-              const V g = row[x];
-              const R w = w1[x];
-              if constexpr (NC == 4) {
-                rs[0] = fma(w, g.x, rs[0]);
-                rs[1] = fma(w, g.y, rs[1]);
-                rs[2] = fma(w, g.z, rs[2]);
-                rs[3] = fma(w, g.w, rs[3]);
-              } else {
-                rs[0] = fma(w, g, rs[0]);
-              }
-            }
+    for (int z = 0; z < TZ; ++z) {
 #pragma unroll
-            for (int c = 0; c < NC; ++c) acc[c] += static_cast<double>(w23 * rs[c]);
+      for (int y = 0; y < TY; ++y) {
+        const R w23 = w2[y] * w3[z];
+        if (!__any_sync(0xffffffffu, w23 != R(0))) continue;
+        R rs[NC];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) rs[c] = R(0);
+        const V* row = sG + (z * TY + y) * TX;
+#pragma unroll
+        for (int x = 0; x < TX; ++x) {
+          const V g = row[x];
+          if constexpr (NC == 4) {
+            rs[0] = fma(w1[x], g.x, rs[0]);
+            rs[1] = fma(w1[x], g.y, rs[1]);
+            rs[2] = fma(w1[x], g.z, rs[2]);
+            rs[3] = fma(w1[x], g.w, rs[3]);
+          } else {
+            rs[0] = fma(w1[x], g, rs[0]);
           }
         }
-      }
-      if (active) {
-        const int sidx = ((ps >> 16) * sd.S[1] + ((ps >> 8) & 0xff)) * sd.S[0] + (ps & 0xff);
-        double* dst = part + (static_cast<size_t>(k) * nslots + sidx) * NC;
 #pragma unroll
-        for (int c = 0; c < NC; ++c) dst[c] = acc[c];
+        for (int c = 0; c < NC; ++c) acc[c] += static_cast<double>(w23 * rs[c]);
       }
-      __syncthreads();
+    }
+    if (active) {
+      const int sidx = ((pr.y >> 16) * sd.S[1] + ((pr.y >> 8) & 0xff)) * sd.S[0] + (pr.y & 0xff);
+      double* dst = part + (static_cast<size_t>(pr.x) * nslots + sidx) * NC;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) dst[c] = acc[c];
     }
   }
 }
@@ -427,45 +345,64 @@ __global__ void k_gather_final(const int4* __restrict__ slot, const int* __restr
   }
 }
 
+inline int blocks_for(long n, int threads) { return static_cast<int>((n + threads - 1) / threads); }
+
 }  // namespace
 
 void launch_weights(const MeshPlan& mp, const int4* mc, const double4* fr, int n, void* wtab,
                     void* qk, int4* slot, cudaStream_t st) {
   if (n == 0) return;
-  const int threads = 128, blocks = (3 * n + threads - 1) / threads;
   if (mp.mixed)
-    k_weights_tiled<float><<<blocks, threads, 0, st>>>(mc, fr, n, mp.sd, static_cast<float*>(wtab),
-                                                        static_cast<float*>(qk), slot);
+    k_weights_tiled<float><<<blocks_for(3L * n, 128), 128, 0, st>>>(
+        mc, fr, n, mp.sd, static_cast<float*>(wtab), static_cast<float*>(qk), slot);
   else
-    k_weights_tiled<double><<<blocks, threads, 0, st>>>(mc, fr, n, mp.sd, static_cast<double*>(wtab),
-                                                         static_cast<double*>(qk), slot);
+    k_weights_tiled<double><<<blocks_for(3L * n, 128), 128, 0, st>>>(
+        mc, fr, n, mp.sd, static_cast<double*>(wtab), static_cast<double*>(qk), slot);
   ++g_launches;
 }
 
-void launch_spread(const MeshPlan& mp, const int4* slot, const void* wtab, const void* qk,
-                   const int* tile_start, void* grid, cudaStream_t st) {
+void launch_pair_bins(const MeshPlan& mp, const int4* slot, int n, int* counts, int* cursor,
+                      int* tile_start, int4* tmp, int2* pairs, int npairs_max, cudaStream_t st) {
+  const int ntiles = mp.sd.ntiles[0] * mp.sd.ntiles[1] * mp.sd.ntiles[2];
+  cudaMemsetAsync(counts, 0, sizeof(int) * ntiles, st);
+  cudaMemsetAsync(cursor, 0, sizeof(int) * ntiles, st);
+  // Unused tail entries of tmp are marked with tile = -1.
+  cudaMemsetAsync(tmp, 0xff, sizeof(int4) * static_cast<size_t>(npairs_max), st);
+  if (n > 0) {
+    k_pair_count<<<blocks_for(n, 128), 128, 0, st>>>(slot, n, mp.sd, counts);
+    ++g_launches;
+  }
+  launch_scan(counts, ntiles, tile_start, st);
+  if (n > 0) {
+    k_pair_scatter<<<blocks_for(n, 128), 128, 0, st>>>(slot, n, mp.sd, tile_start, cursor, tmp);
+    k_pair_rank<<<blocks_for(npairs_max, 256), 256, 0, st>>>(tmp, npairs_max, tile_start, pairs);
+    g_launches += 2;
+  }
+}
+
+void launch_spread(const MeshPlan& mp, const int* tile_start, const int2* pairs, const void* wtab,
+                   const void* qk, void* grid, cudaStream_t st) {
   dim3 grd(mp.sd.ntiles[0], mp.sd.ntiles[1], mp.sd.ntiles[2]);
   if (mp.mixed)
-    k_spread_tiles<float><<<grd, kThreads, 0, st>>>(slot, static_cast<const float*>(wtab),
-                                                     static_cast<const float*>(qk), tile_start,
-                                                     mp.tl[0], mp.tl[1], mp.tl[2], mp.sd,
+    k_spread_tiles<float><<<grd, kPencils, 0, st>>>(tile_start, pairs,
+                                                     static_cast<const float*>(wtab),
+                                                     static_cast<const float*>(qk), mp.sd,
                                                      static_cast<float*>(grid));
   else
-    k_spread_tiles<double><<<grd, kThreads, 0, st>>>(slot, static_cast<const double*>(wtab),
-                                                      static_cast<const double*>(qk), tile_start,
-                                                      mp.tl[0], mp.tl[1], mp.tl[2], mp.sd,
+    k_spread_tiles<double><<<grd, kPencils, 0, st>>>(tile_start, pairs,
+                                                      static_cast<const double*>(wtab),
+                                                      static_cast<const double*>(qk), mp.sd,
                                                       static_cast<double*>(grid));
   ++g_launches;
 }
 
-void launch_gather(const MeshPlan& mp, const int4* slot, const void* wtab, const int* tile_start,
+void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs, const void* wtab,
                    const void* grid, int nc, double* part, cudaStream_t st) {
   dim3 grd(mp.sd.ntiles[0], mp.sd.ntiles[1], mp.sd.ntiles[2]);
-  const size_t pts = static_cast<size_t>(TX) * TY * TZ;
-#define EWG_GATHER(R, NC)                                                                         \
-  k_gather_tiles<R, NC><<<grd, kGatherThreads, pts * NC * sizeof(R), st>>>(                         \
-      slot, static_cast<const R*>(wtab), tile_start, mp.tl[0], mp.tl[1], mp.tl[2], mp.sd,           \
-      static_cast<const R*>(grid), part)
+#define EWG_GATHER(R, NC)                                                                      \
+  k_gather_tiles<R, NC><<<grd, kGatherThreads, 0, st>>>(tile_start, pairs,                     \
+                                                        static_cast<const R*>(wtab), mp.sd,    \
+                                                        static_cast<const R*>(grid), part)
   if (mp.mixed) {
     if (nc == 4)
       EWG_GATHER(float, 4);
@@ -481,27 +418,19 @@ void launch_gather(const MeshPlan& mp, const int4* slot, const void* wtab, const
   ++g_launches;
 }
 
-int stencil_configure_kernels() {
-  const int bytes = TX * TY * TZ * 4 * 8;
-  cudaFuncSetAttribute(k_gather_tiles<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_gather_tiles<double, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_gather_tiles<float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  cudaFuncSetAttribute(k_gather_tiles<float, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  return cudaGetLastError() == cudaSuccess ? EWG_OK : EWG_ERR_CUDA;
-}
-
 void launch_gather_final(const MeshPlan& mp, const int4* slot, const int* perm, const double* part,
                          int nc, int n, const double* q, double self_coef, const double* pot_sr,
                          const double* f_sr, double* pot, double* force, cudaStream_t st) {
   if (n == 0) return;
-  const int threads = 128, blocks = (n + threads - 1) / threads;
   if (nc == 4)
-    k_gather_final<4><<<blocks, threads, 0, st>>>(slot, perm, part, n, mp.sd, q, self_coef, pot_sr,
-                                                   f_sr, pot, force);
+    k_gather_final<4><<<blocks_for(n, 128), 128, 0, st>>>(slot, perm, part, n, mp.sd, q, self_coef,
+                                                           pot_sr, f_sr, pot, force);
   else
-    k_gather_final<1><<<blocks, threads, 0, st>>>(slot, perm, part, n, mp.sd, q, self_coef, pot_sr,
-                                                   f_sr, pot, nullptr);
+    k_gather_final<1><<<blocks_for(n, 128), 128, 0, st>>>(slot, perm, part, n, mp.sd, q, self_coef,
+                                                           pot_sr, f_sr, pot, nullptr);
   ++g_launches;
 }
+
+int stencil_configure_kernels() { return EWG_OK; }
 
 }  // namespace ewg
