@@ -259,3 +259,98 @@ __device__ __forceinline__ const cx<float>* plan_twiddles<float>(const FftPlan& 
 }
 
 }  // namespace ewg
+
+namespace ewg {
+
+// ---------------------------------------------------------------------------
+// Line-fastest variant: L lines (a power of two) stored element-major with a
+// padded stride LP = L + 1, element e of line l at buf[e * LP + l].  This is
+// the order in which the strided (y, z) passes find their lines in memory
+// (consecutive k1), so loads and stores are coalesced and the shared-memory
+// accesses of a pass are conflict-free.  Threads map to (line, butterfly) with
+// the line fastest; the Stockham indices j = i / p, k = i mod p advance
+// incrementally, with one division per pass.  blockDim.x must be a multiple of L.
+// ---------------------------------------------------------------------------
+template <typename R, int SIGN, int RR, int L>
+__device__ __forceinline__ void stockham_pass_cols(const cx<R>* __restrict__ in,
+                                                   cx<R>* __restrict__ out, int n, int p,
+                                                   const cx<R>* __restrict__ tw) {
+  constexpr int LP = L + 1;
+  const int nr = n / RR;
+  const int step = n / (p * RR);
+  const int line = threadIdx.x & (L - 1);
+  const int istep = blockDim.x / L;
+  int i = threadIdx.x / L;
+  int j = i / p, k = i - j * p;
+  const int dj = istep / p, dk = istep - dj * p;
+  for (; i < nr; i += istep) {
+    const cx<R>* src = in + i * LP + line;
+    cx<R> u[RR];
+#pragma unroll
+    for (int jj = 0; jj < RR; ++jj) u[jj] = src[jj * nr * LP];
+    if (p > 1) {
+#pragma unroll
+      for (int jj = 1; jj < RR; ++jj) u[jj] = mul(u[jj], twiddle(tw, jj * k * step, SIGN));
+    }
+    dft_fixed<R, SIGN, RR>(u, tw, n);
+    cx<R>* dst = out + (j * p * RR + k) * LP + line;
+#pragma unroll
+    for (int jj = 0; jj < RR; ++jj) dst[jj * p * LP] = u[jj];
+    k += dk;
+    j += dj;
+    if (k >= p) {
+      k -= p;
+      ++j;
+    }
+  }
+}
+
+template <typename R, int SIGN, int L>
+__device__ void stockham_pass_cols_generic(const cx<R>* __restrict__ in, cx<R>* __restrict__ out,
+                                           int n, int p, int rr, const cx<R>* __restrict__ tw) {
+  constexpr int LP = L + 1;
+  const int nr = n / rr;
+  const int step = n / (p * rr);
+  const int stride_rr = n / rr;
+  const int line = threadIdx.x & (L - 1);
+  for (int i = threadIdx.x / L; i < nr; i += blockDim.x / L) {
+    const int k = i % p, j = i / p;
+    const cx<R>* src = in + i * LP + line;
+    cx<R>* dst = out + (j * p * rr + k) * LP + line;
+    for (int s = 0; s < rr; ++s) {
+      cx<R> acc = mk(R(0), R(0));
+      for (int jj = 0; jj < rr; ++jj) {
+        cx<R> v = src[jj * nr * LP];
+        if (p > 1 && jj > 0) v = mul(v, twiddle(tw, jj * k * step, SIGN));
+        acc = add(acc, mul(v, twiddle(tw, ((jj * s) % rr) * stride_rr, SIGN)));
+      }
+      dst[s * p * LP] = acc;
+    }
+  }
+}
+
+template <typename R, int SIGN, int L>
+__device__ cx<R>* fft_cols(cx<R>* a, cx<R>* b, int n, const FftPlan& plan,
+                           const cx<R>* __restrict__ tw) {
+  int p = 1;
+  for (int s = 0; s < plan.nstages; ++s) {
+    const int rr = plan.radix[s];
+    switch (rr) {
+      case 2: stockham_pass_cols<R, SIGN, 2, L>(a, b, n, p, tw); break;
+      case 3: stockham_pass_cols<R, SIGN, 3, L>(a, b, n, p, tw); break;
+      case 4: stockham_pass_cols<R, SIGN, 4, L>(a, b, n, p, tw); break;
+      case 5: stockham_pass_cols<R, SIGN, 5, L>(a, b, n, p, tw); break;
+      case 7: stockham_pass_cols<R, SIGN, 7, L>(a, b, n, p, tw); break;
+      case 8: stockham_pass_cols<R, SIGN, 8, L>(a, b, n, p, tw); break;
+      default: stockham_pass_cols_generic<R, SIGN, L>(a, b, n, p, rr, tw); break;
+    }
+    __syncthreads();
+    cx<R>* t = a;
+    a = b;
+    b = t;
+    p *= rr;
+  }
+  return a;
+}
+
+}  // namespace ewg

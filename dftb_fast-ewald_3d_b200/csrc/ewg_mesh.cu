@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 
 #include "ewg_fft.cuh"
 #include "ewg_kernels.h"
@@ -31,7 +32,6 @@ namespace ewg {
 
 namespace {
 
-constexpr int kFftThreads = 256;
 constexpr size_t kSmemBudget = 200 * 1024;
 
 __device__ __forceinline__ int pmod(int a, int n) {
@@ -39,71 +39,80 @@ __device__ __forceinline__ int pmod(int a, int n) {
   return r < 0 ? r + n : r;
 }
 
+// Every pass stages L lines (a power of two, the fastest index) of length n in
+// shared memory as buf[e * (L + 1) + line]; blockDim.x = 32 * L.
+
 // ---------------------------------------------------------------------------
-// x pass, real to complex: two real rows per complex line; keep k1 = 0..K1-1.
+// x pass, real to complex: row pairs (2p, 2p+1) form one complex line; keep
+// k1 = 0..K1-1 of each row.
 // ---------------------------------------------------------------------------
-template <typename R>
-__global__ void __launch_bounds__(kFftThreads) k_fft_x_r2c(const R* __restrict__ grid,
-                                                           cx<R>* __restrict__ A1, int n1,
-                                                           int npairs, int K1, int P,
-                                                           FftPlan plan) {
-  extern __shared__ unsigned char smem_raw[];
+template <typename R, int L>
+__global__ void __launch_bounds__(32 * L) k_fft_x_r2c(const R* __restrict__ grid,
+                                                      cx<R>* __restrict__ A1, int n1, int npairs,
+                                                      int K1, FftPlan plan) {
+  constexpr int LP = L + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
-  cx<R>* b = a + static_cast<size_t>(P) * n1;
-  const int pair0 = blockIdx.x * P;
-  const int np = min(P, npairs - pair0);
-  for (int t = threadIdx.x; t < np * n1; t += blockDim.x) {
-    const int l = t / n1, k = t - l * n1;
-    const size_t r0 = static_cast<size_t>(2 * (pair0 + l)) * n1;
-    a[l * n1 + k] = mk(grid[r0 + k], grid[r0 + n1 + k]);
+  cx<R>* b = a + static_cast<size_t>(n1) * LP;
+  const int pair0 = blockIdx.x * L;
+  for (int x = threadIdx.x; x < n1; x += blockDim.x) {
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+      const int pr = pair0 + l;
+      cx<R> v = mk(R(0), R(0));
+      if (pr < npairs) {
+        const size_t r0 = static_cast<size_t>(2 * pr) * n1;
+        v = mk(grid[r0 + x], grid[r0 + n1 + x]);
+      }
+      a[x * LP + l] = v;
+    }
   }
   __syncthreads();
   const cx<R>* tw = plan_twiddles<R>(plan);
-  cx<R>* res = fft_lines<R, -1>(a, b, n1, np, plan, tw);
+  cx<R>* res = fft_cols<R, -1, L>(a, b, n1, plan, tw);
   const R h = R(0.5);
-  for (int t = threadIdx.x; t < np * K1; t += blockDim.x) {
-    const int l = t / K1, k = t - l * K1;
-    const cx<R> z = res[l * n1 + k];
-    cx<R> zc = res[l * n1 + (k == 0 ? 0 : n1 - k)];
+  for (int t = threadIdx.x; t < K1 * L; t += blockDim.x) {
+    const int l = t % L, k = t / L;  // L is a power of two
+    const int pr = pair0 + l;
+    if (pr >= npairs) continue;
+    const cx<R> z = res[k * LP + l];
+    cx<R> zc = res[(k == 0 ? 0 : n1 - k) * LP + l];
     zc.y = -zc.y;
-    const size_t row = static_cast<size_t>(2 * (pair0 + l));
+    const size_t row = static_cast<size_t>(2 * pr);
     A1[row * K1 + k] = mk(h * (z.x + zc.x), h * (z.y + zc.y));
     A1[(row + 1) * K1 + k] = mk(h * (z.y - zc.y), -h * (z.x - zc.x));
   }
 }
 
 // ---------------------------------------------------------------------------
-// y pass, forward: lines over i2 for (i3, k1-block); keep k2 in [-M2/2, M2/2].
+// y pass, forward: lines over i2 for (i3, k1-block); keep k2 in [-H2, H2].
 // ---------------------------------------------------------------------------
-template <typename R>
-__global__ void __launch_bounds__(kFftThreads) k_fft_y_fwd(const cx<R>* __restrict__ A1,
-                                                           cx<R>* __restrict__ A2, int n2, int K1,
-                                                           int K2, int H2, int TK, FftPlan plan) {
-  extern __shared__ unsigned char smem_raw[];
+template <typename R, int L>
+__global__ void __launch_bounds__(32 * L) k_fft_y_fwd(const cx<R>* __restrict__ A1,
+                                                      cx<R>* __restrict__ A2, int n2, int K1,
+                                                      int K2, int H2, FftPlan plan) {
+  constexpr int LP = L + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
-  cx<R>* b = a + static_cast<size_t>(TK) * n2;
-  const int k0 = blockIdx.x * TK;
+  cx<R>* b = a + static_cast<size_t>(n2) * LP;
+  const int k0 = blockIdx.x * L;
   const int i3 = blockIdx.y;
-  const int tk = min(TK, K1 - k0);
-  for (int t = threadIdx.x; t < n2 * tk; t += blockDim.x) {
-    const int i2 = t / tk, kk = t - i2 * tk;
-    a[kk * n2 + i2] = A1[(static_cast<size_t>(i3) * n2 + i2) * K1 + k0 + kk];
-  }
+  const int kk = threadIdx.x % L;
+  const bool kin = k0 + kk < K1;
+  for (int i2 = threadIdx.x / L; i2 < n2; i2 += blockDim.x / L)
+    a[i2 * LP + kk] = kin ? A1[(static_cast<size_t>(i3) * n2 + i2) * K1 + k0 + kk] : mk(R(0), R(0));
   __syncthreads();
-  cx<R>* res = fft_lines<R, -1>(a, b, n2, tk, plan, plan_twiddles<R>(plan));
-  const int h2 = H2;
-  for (int t = threadIdx.x; t < K2 * tk; t += blockDim.x) {
-    const int k2i = t / tk, kk = t - k2i * tk;
-    const int idx = pmod(k2i - h2, n2);
-    A2[(static_cast<size_t>(i3) * K2 + k2i) * K1 + k0 + kk] = res[kk * n2 + idx];
-  }
+  cx<R>* res = fft_cols<R, -1, L>(a, b, n2, plan, plan_twiddles<R>(plan));
+  if (kin)
+    for (int k2i = threadIdx.x / L; k2i < K2; k2i += blockDim.x / L)
+      A2[(static_cast<size_t>(i3) * K2 + k2i) * K1 + k0 + kk] = res[pmod(k2i - H2, n2) * LP + kk];
 }
 
 // ---------------------------------------------------------------------------
 // z pass forward, influence weights, z pass inverse -- fused per (k2, k1-block).
 // ---------------------------------------------------------------------------
 struct InfluenceArgs {
-  int H[3];          // closed box |k_d| <= H_d
+  int H[3];            // closed box |k_d| <= H_d
   int slo[3], shi[3];  // mode set S_d = [slo_d, shi_d] (nfft/nfft.f90:61-75)
   double rec[3][3];
   double prefactor;    // 4 pi / V
@@ -111,33 +120,34 @@ struct InfluenceArgs {
   const double* corr2[3];
 };
 
-template <typename R>
-__global__ void __launch_bounds__(kFftThreads) k_fft_z_influence(
-    const cx<R>* __restrict__ A2, cx<R>* __restrict__ B2, int n3, int K1, int K2, int K3, int TK,
-    int nc, InfluenceArgs ia, FftPlan plan) {
-  extern __shared__ unsigned char smem_raw[];
+template <typename R, int L>
+__global__ void __launch_bounds__(32 * L) k_fft_z_influence(const cx<R>* __restrict__ A2,
+                                                            cx<R>* __restrict__ B2, int n3, int K1,
+                                                            int K2, int K3, int nc,
+                                                            InfluenceArgs ia, FftPlan plan) {
+  constexpr int LP = L + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
-  cx<R>* b = a + static_cast<size_t>(TK) * n3;
-  cx<R>* q = b + static_cast<size_t>(TK) * n3;  // TK * K3 weighted modes
-  const int k0 = blockIdx.x * TK;
+  cx<R>* b = a + static_cast<size_t>(n3) * LP;
+  cx<R>* q = b + static_cast<size_t>(n3) * LP;  // K3 weighted modes per line
+  const int k0 = blockIdx.x * L;
   const int k2i = blockIdx.y;
-  const int tk = min(TK, K1 - k0);
+  const int kk = threadIdx.x % L;
+  const int rstep = blockDim.x / L;
+  const bool kin = k0 + kk < K1;
   const cx<R>* tw = plan_twiddles<R>(plan);
-  for (int t = threadIdx.x; t < n3 * tk; t += blockDim.x) {
-    const int i3 = t / tk, kk = t - i3 * tk;
-    a[kk * n3 + i3] = A2[(static_cast<size_t>(i3) * K2 + k2i) * K1 + k0 + kk];
-  }
+  for (int i3 = threadIdx.x / L; i3 < n3; i3 += rstep)
+    a[i3 * LP + kk] = kin ? A2[(static_cast<size_t>(i3) * K2 + k2i) * K1 + k0 + kk] : mk(R(0), R(0));
   __syncthreads();
-  cx<R>* res = fft_lines<R, -1>(a, b, n3, tk, plan, tw);
+  cx<R>* res = fft_cols<R, -1, L>(a, b, n3, plan, tw);
   const int h1 = ia.H[0], h2 = ia.H[1], h3 = ia.H[2];
+  const int k1 = k0 + kk;
   const int k2 = k2i - h2;
   const double twoPi = 2.0 * 3.14159265358979323846;
-  for (int t = threadIdx.x; t < K3 * tk; t += blockDim.x) {
-    const int k3i = t / tk, kk = t - k3i * tk;
-    const int k1 = k0 + kk;
+  for (int k3i = threadIdx.x / L; k3i < K3; k3i += rstep) {
     const int k3 = k3i - h3;
     double wt = 0.0;
-    if (!(k1 == 0 && k2 == 0 && k3 == 0)) {
+    if (kin && !(k1 == 0 && k2 == 0 && k3 == 0)) {
       double kv[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
@@ -154,43 +164,43 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_z_influence(
              ia.corr2[1][k2 + h2] * ia.corr2[2][k3 + h3];
       }
     }
-    const cx<R> g = res[kk * n3 + pmod(k3, n3)];
-    q[kk * K3 + k3i] = mk(static_cast<R>(wt * static_cast<double>(g.x)),
+    const cx<R> g = res[pmod(k3, n3) * LP + kk];
+    q[k3i * LP + kk] = mk(static_cast<R>(wt * static_cast<double>(g.x)),
                           static_cast<R>(wt * static_cast<double>(g.y)));
   }
   __syncthreads();
   for (int c = 0; c < nc; ++c) {
-    for (int t = threadIdx.x; t < n3 * tk; t += blockDim.x) {
-      const int kk = t / n3, i3 = t - kk * n3;
-      int k3;
+    R kc1 = R(0), kc2 = R(0), kc3 = R(0);
+    if (c > 0) {
+      kc1 = static_cast<R>(twoPi * ia.rec[0][c - 1]);
+      kc2 = static_cast<R>(twoPi * ia.rec[1][c - 1]);
+      kc3 = static_cast<R>(twoPi * ia.rec[2][c - 1]);
+    }
+    for (int i3 = threadIdx.x / L; i3 < n3; i3 += rstep) {
+      int k3 = 0;
       bool inside = true;
       if (i3 <= h3)
         k3 = i3;
       else if (i3 >= n3 - h3)
         k3 = i3 - n3;
-      else {
-        k3 = 0;
+      else
         inside = false;
-      }
       cx<R> v = mk(R(0), R(0));
       if (inside) {
-        v = q[kk * K3 + k3 + h3];
+        v = q[(k3 + h3) * LP + kk];
         if (c > 0) {
-          const int k1 = k0 + kk;
-          const R kc = static_cast<R>(twoPi * (k1 * ia.rec[0][c - 1] + k2 * ia.rec[1][c - 1] +
-                                               k3 * ia.rec[2][c - 1]));
+          const R kc = static_cast<R>(k1) * kc1 + static_cast<R>(k2) * kc2 + static_cast<R>(k3) * kc3;
           v = mk(kc * v.y, -kc * v.x);  // -i kc v
         }
       }
-      a[kk * n3 + i3] = v;
+      a[i3 * LP + kk] = v;
     }
     __syncthreads();
-    cx<R>* r2 = fft_lines<R, 1>(a, b, n3, tk, plan, tw);
+    cx<R>* r2 = fft_cols<R, 1, L>(a, b, n3, plan, tw);
     cx<R>* dst = B2 + static_cast<size_t>(c) * n3 * K2 * K1;
-    for (int t = threadIdx.x; t < n3 * tk; t += blockDim.x) {
-      const int i3 = t / tk, kk = t - i3 * tk;
-      dst[(static_cast<size_t>(i3) * K2 + k2i) * K1 + k0 + kk] = r2[kk * n3 + i3];
-    }
+    if (kin)
+      for (int i3 = threadIdx.x / L; i3 < n3; i3 += rstep)
+        dst[(static_cast<size_t>(i3) * K2 + k2i) * K1 + k0 + kk] = r2[i3 * LP + kk];
     __syncthreads();
   }
 }
@@ -198,90 +208,106 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_z_influence(
 // ---------------------------------------------------------------------------
 // y pass inverse: zero-padded k2 box -> i2, for (k1-block, i3, component).
 // ---------------------------------------------------------------------------
-template <typename R>
-__global__ void __launch_bounds__(kFftThreads) k_fft_y_inv(const cx<R>* __restrict__ B2,
-                                                           cx<R>* __restrict__ B1, int n2, int n3,
-                                                           int K1, int K2, int H2, int TK,
-                                                           FftPlan plan) {
-  extern __shared__ unsigned char smem_raw[];
+template <typename R, int L>
+__global__ void __launch_bounds__(32 * L) k_fft_y_inv(const cx<R>* __restrict__ B2,
+                                                      cx<R>* __restrict__ B1, int n2, int n3,
+                                                      int K1, int K2, int H2, FftPlan plan) {
+  constexpr int LP = L + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
-  cx<R>* b = a + static_cast<size_t>(TK) * n2;
-  const int k0 = blockIdx.x * TK;
+  cx<R>* b = a + static_cast<size_t>(n2) * LP;
+  const int k0 = blockIdx.x * L;
   const int i3 = blockIdx.y;
   const int c = blockIdx.z;
-  const int tk = min(TK, K1 - k0);
-  const int h2 = H2;
+  const int kk = threadIdx.x % L;
+  const bool kin = k0 + kk < K1;
   const cx<R>* src = B2 + static_cast<size_t>(c) * n3 * K2 * K1;
-  for (int t = threadIdx.x; t < n2 * tk; t += blockDim.x) {
-    const int i2 = t / tk, kk = t - i2 * tk;
+  for (int i2 = threadIdx.x / L; i2 < n2; i2 += blockDim.x / L) {
     int k2 = 0;
-    bool inside = true;
-    if (i2 <= h2)
+    bool inside = kin;
+    if (i2 <= H2)
       k2 = i2;
-    else if (i2 >= n2 - h2)
+    else if (i2 >= n2 - H2)
       k2 = i2 - n2;
     else
       inside = false;
-    a[kk * n2 + i2] =
-        inside ? src[(static_cast<size_t>(i3) * K2 + k2 + h2) * K1 + k0 + kk] : mk(R(0), R(0));
+    a[i2 * LP + kk] =
+        inside ? src[(static_cast<size_t>(i3) * K2 + k2 + H2) * K1 + k0 + kk] : mk(R(0), R(0));
   }
   __syncthreads();
-  cx<R>* res = fft_lines<R, 1>(a, b, n2, tk, plan, plan_twiddles<R>(plan));
+  cx<R>* res = fft_cols<R, 1, L>(a, b, n2, plan, plan_twiddles<R>(plan));
   cx<R>* dst = B1 + static_cast<size_t>(c) * n3 * n2 * K1;
-  for (int t = threadIdx.x; t < n2 * tk; t += blockDim.x) {
-    const int i2 = t / tk, kk = t - i2 * tk;
-    dst[(static_cast<size_t>(i3) * n2 + i2) * K1 + k0 + kk] = res[kk * n2 + i2];
-  }
+  if (kin)
+    for (int i2 = threadIdx.x / L; i2 < n2; i2 += blockDim.x / L)
+      dst[(static_cast<size_t>(i3) * n2 + i2) * K1 + k0 + kk] = res[i2 * LP + kk];
 }
 
 // ---------------------------------------------------------------------------
-// x pass, complex to real, all components of P row pairs; interleaved output.
+// x pass, complex to real.  Lines are (component, row pair): line = cc * NP + l
+// with NP = L / NCG pairs and NCG components per CTA; output interleaved with
+// nc components per grid point.
 // ---------------------------------------------------------------------------
-template <typename R>
-__global__ void __launch_bounds__(kFftThreads) k_fft_x_c2r(const cx<R>* __restrict__ B1,
-                                                           R* __restrict__ out, int n1, int nrows,
-                                                           int K1, int nc, int ncg, int P,
-                                                           FftPlan plan) {
-  // This CTA handles components [c0, c0 + ncg) of P row pairs.
-  extern __shared__ unsigned char smem_raw[];
-  const int pair0 = blockIdx.x * P;
-  const int c0 = blockIdx.y * ncg;
-  const int np = min(P, nrows / 2 - pair0);
-  const int nl = np * ncg;  // line index = cc * np + l
+template <typename R, int L, int NCG>
+__global__ void __launch_bounds__(32 * L) k_fft_x_c2r(const cx<R>* __restrict__ B1,
+                                                      R* __restrict__ out, int n1, int nrows,
+                                                      int K1, int nc, FftPlan plan) {
+  constexpr int LP = L + 1;
+  constexpr int NP = L / NCG;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
-  cx<R>* b = a + static_cast<size_t>(P) * ncg * n1;
-  for (int t = threadIdx.x; t < nl * n1; t += blockDim.x) {
-    const int line = t / n1, k = t - line * n1;
-    const int cc = line / np, l = line - cc * np;
-    const size_t ra = static_cast<size_t>(2 * (pair0 + l));
-    const cx<R>* src = B1 + static_cast<size_t>(c0 + cc) * nrows * K1;
-    cx<R> fa = mk(R(0), R(0)), fb = mk(R(0), R(0));
-    if (k < K1) {
-      fa = src[ra * K1 + k];
-      fb = src[(ra + 1) * K1 + k];
-      if (k == 0) {
-        fa.y = R(0);
-        fb.y = R(0);
+  cx<R>* b = a + static_cast<size_t>(n1) * LP;
+  const int pair0 = blockIdx.x * NP;
+  const int c0 = blockIdx.y * NCG;
+  const int npairs = nrows / 2;
+  for (int x = threadIdx.x; x < n1; x += blockDim.x) {
+    const bool lo = x < K1;
+    const bool hi = x > n1 - K1;
+    const int kx = lo ? x : n1 - x;
+#pragma unroll
+    for (int line = 0; line < L; ++line) {
+      const int cc = line / NP, l = line % NP;
+      const int pr = pair0 + l;
+      cx<R> fa = mk(R(0), R(0)), fb = mk(R(0), R(0));
+      if (pr < npairs && (lo || hi)) {
+        const cx<R>* src = B1 + static_cast<size_t>(c0 + cc) * nrows * K1;
+        const size_t ra = static_cast<size_t>(2 * pr);
+        fa = src[ra * K1 + kx];
+        fb = src[(ra + 1) * K1 + kx];
+        if (x == 0) {
+          fa.y = R(0);
+          fb.y = R(0);
+        } else if (hi) {
+          fa.y = -fa.y;
+          fb.y = -fb.y;
+        }
       }
-    } else if (k > n1 - K1) {
-      fa = src[ra * K1 + (n1 - k)];
-      fb = src[(ra + 1) * K1 + (n1 - k)];
-      fa.y = -fa.y;
-      fb.y = -fb.y;
+      a[x * LP + line] = mk(fa.x - fb.y, fa.y + fb.x);
     }
-    a[line * n1 + k] = mk(fa.x - fb.y, fa.y + fb.x);
   }
   __syncthreads();
-  cx<R>* res = fft_lines<R, 1>(a, b, n1, nl, plan, plan_twiddles<R>(plan));
-  for (int t = threadIdx.x; t < np * n1; t += blockDim.x) {
-    const int l = t / n1, i1 = t - l * n1;
-    const size_t ra = static_cast<size_t>(2 * (pair0 + l));
-    R* oa = out + (ra * n1 + i1) * nc + c0;
-    R* ob = out + ((ra + 1) * n1 + i1) * nc + c0;
-    for (int cc = 0; cc < ncg; ++cc) {
-      const cx<R> z = res[(cc * np + l) * n1 + i1];
-      oa[cc] = z.x;
-      ob[cc] = z.y;
+  cx<R>* res = fft_cols<R, 1, L>(a, b, n1, plan, plan_twiddles<R>(plan));
+  for (int x = threadIdx.x; x < n1; x += blockDim.x) {
+#pragma unroll
+    for (int l = 0; l < NP; ++l) {
+      const int pr = pair0 + l;
+      if (pr >= npairs) continue;
+      const size_t ra = static_cast<size_t>(2 * pr);
+      R* oa = out + (ra * n1 + x) * nc + c0;
+      R* ob = out + ((ra + 1) * n1 + x) * nc + c0;
+      if constexpr (NCG == 4) {
+        using V = typename std::conditional<sizeof(R) == 8, double4, float4>::type;
+        const cx<R> z0 = res[x * LP + 0 * NP + l], z1 = res[x * LP + 1 * NP + l],
+                    z2 = res[x * LP + 2 * NP + l], z3 = res[x * LP + 3 * NP + l];
+        *reinterpret_cast<V*>(oa) = V{z0.x, z1.x, z2.x, z3.x};
+        *reinterpret_cast<V*>(ob) = V{z0.y, z1.y, z2.y, z3.y};
+      } else {
+#pragma unroll
+        for (int cc = 0; cc < NCG; ++cc) {
+          const cx<R> z = res[x * LP + cc * NP + l];
+          oa[cc] = z.x;
+          ob[cc] = z.y;
+        }
+      }
     }
   }
 }
@@ -291,9 +317,11 @@ size_t cbytes() {
   return sizeof(cx<R>);
 }
 
-int lines_for(size_t per_line_bytes, int cap) {
-  size_t l = kSmemBudget / std::max<size_t>(per_line_bytes, 1);
-  return static_cast<int>(std::max<size_t>(1, std::min<size_t>(l, cap)));
+// Lines per CTA: 8 when both ping-pong buffers of the longest line fit in 64 KB
+// (several CTAs per SM), else 4.
+int pick_lines(int n, size_t cb, size_t extra_per_line_elems = 0) {
+  const size_t bytes8 = (2 * static_cast<size_t>(n) + extra_per_line_elems) * 9 * cb;
+  return bytes8 <= 64 * 1024 ? 8 : 4;
 }
 
 template <typename R>
@@ -308,19 +336,27 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
   {  // x, real to complex
     prof_mark(mp.prof, st, ST_FFT_X_R2C);
     const int npairs = n2 * n3 / 2;
-    const int P = lines_for(2 * n1 * cb, 8);
-    const size_t sm = 2 * static_cast<size_t>(P) * n1 * cb;
-    k_fft_x_r2c<R><<<(npairs + P - 1) / P, kFftThreads, sm, st>>>(static_cast<const R*>(grid), A1,
-                                                                    n1, npairs, g.K1, P, mp.fft[0]);
+    const int L = pick_lines(n1, cb);
+    const size_t sm = 2 * static_cast<size_t>(n1) * (L + 1) * cb;
+    const int blocks = (npairs + L - 1) / L;
+    if (L == 8)
+      k_fft_x_r2c<R, 8><<<blocks, 256, sm, st>>>(static_cast<const R*>(grid), A1, n1, npairs, g.K1,
+                                                   mp.fft[0]);
+    else
+      k_fft_x_r2c<R, 4><<<blocks, 128, sm, st>>>(static_cast<const R*>(grid), A1, n1, npairs, g.K1,
+                                                   mp.fft[0]);
     ++g_launches;
   }
   {  // y forward
     prof_mark(mp.prof, st, ST_FFT_Y_FWD);
-    const int TK = lines_for(2 * n2 * cb, 8);
-    const size_t sm = 2 * static_cast<size_t>(TK) * n2 * cb;
-    dim3 grd((g.K1 + TK - 1) / TK, n3);
-    k_fft_y_fwd<R><<<grd, kFftThreads, sm, st>>>(A1, A2, n2, g.K1, g.K2, (g.K2 - 1) / 2, TK,
-                                                 mp.fft[1]);
+    const int L = pick_lines(n2, cb);
+    const size_t sm = 2 * static_cast<size_t>(n2) * (L + 1) * cb;
+    dim3 grd((g.K1 + L - 1) / L, n3);
+    const int H2 = (g.K2 - 1) / 2;
+    if (L == 8)
+      k_fft_y_fwd<R, 8><<<grd, 256, sm, st>>>(A1, A2, n2, g.K1, g.K2, H2, mp.fft[1]);
+    else
+      k_fft_y_fwd<R, 4><<<grd, 128, sm, st>>>(A1, A2, n2, g.K1, g.K2, H2, mp.fft[1]);
     ++g_launches;
   }
   {  // z forward + influence + z inverse
@@ -336,11 +372,13 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
     ia.prefactor = 4.0 * kPi / g.volume;
     ia.inv4a2 = 1.0 / (4.0 * (g.alpha * g.alpha));
     for (int d = 0; d < 3; ++d) ia.corr2[d] = mp.corr2[d];
-    const int TK = lines_for((2 * n3 + g.K3) * cb, 8);
-    const size_t sm = (2 * static_cast<size_t>(TK) * n3 + static_cast<size_t>(TK) * g.K3) * cb;
-    dim3 grd((g.K1 + TK - 1) / TK, g.K2);
-    k_fft_z_influence<R><<<grd, kFftThreads, sm, st>>>(A2, B2, n3, g.K1, g.K2, g.K3, TK, nc, ia,
-                                                        mp.fft[2]);
+    const int L = pick_lines(n3, cb, g.K3);
+    const size_t sm = (2 * static_cast<size_t>(n3) + g.K3) * (L + 1) * cb;
+    dim3 grd((g.K1 + L - 1) / L, g.K2);
+    if (L == 8)
+      k_fft_z_influence<R, 8><<<grd, 256, sm, st>>>(A2, B2, n3, g.K1, g.K2, g.K3, nc, ia, mp.fft[2]);
+    else
+      k_fft_z_influence<R, 4><<<grd, 128, sm, st>>>(A2, B2, n3, g.K1, g.K2, g.K3, nc, ia, mp.fft[2]);
     ++g_launches;
   }
 }
@@ -355,23 +393,36 @@ void inverse_impl(const MeshPlan& mp, const void* B2v, void* B1v, void* out, int
   const size_t cb = cbytes<R>();
   {
     prof_mark(mp.prof, st, ST_FFT_Y_INV);
-    const int TK = lines_for(2 * n2 * cb, 8);
-    const size_t sm = 2 * static_cast<size_t>(TK) * n2 * cb;
-    dim3 grd((g.K1 + TK - 1) / TK, n3, nc);
-    k_fft_y_inv<R><<<grd, kFftThreads, sm, st>>>(B2, B1, n2, n3, g.K1, g.K2, (g.K2 - 1) / 2, TK,
-                                                 mp.fft[1]);
+    const int L = pick_lines(n2, cb);
+    const size_t sm = 2 * static_cast<size_t>(n2) * (L + 1) * cb;
+    dim3 grd((g.K1 + L - 1) / L, n3, nc);
+    const int H2 = (g.K2 - 1) / 2;
+    if (L == 8)
+      k_fft_y_inv<R, 8><<<grd, 256, sm, st>>>(B2, B1, n2, n3, g.K1, g.K2, H2, mp.fft[1]);
+    else
+      k_fft_y_inv<R, 4><<<grd, 128, sm, st>>>(B2, B1, n2, n3, g.K1, g.K2, H2, mp.fft[1]);
     ++g_launches;
   }
   {
     prof_mark(mp.prof, st, ST_FFT_X_C2R);
     const int nrows = n2 * n3;
-    // All components of a row pair in one CTA when they fit, else one per CTA.
-    const int ncg = 2 * static_cast<size_t>(nc) * n1 * cb <= kSmemBudget ? nc : 1;
-    const int P = lines_for(2 * static_cast<size_t>(ncg) * n1 * cb, ncg == 1 ? 8 : 2);
-    const size_t sm = 2 * static_cast<size_t>(P) * ncg * n1 * cb;
-    dim3 grd((nrows / 2 + P - 1) / P, nc / ncg);
-    k_fft_x_c2r<R><<<grd, kFftThreads, sm, st>>>(B1, static_cast<R*>(out), n1, nrows, g.K1, nc, ncg,
-                                                 P, mp.fft[0]);
+    const int L = pick_lines(n1, cb);
+    const size_t sm = 2 * static_cast<size_t>(n1) * (L + 1) * cb;
+    R* o = static_cast<R*>(out);
+    if (nc == 4) {
+      const int NP = L / 4;
+      dim3 grd((nrows / 2 + NP - 1) / NP, 1);
+      if (L == 8)
+        k_fft_x_c2r<R, 8, 4><<<grd, 256, sm, st>>>(B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
+      else
+        k_fft_x_c2r<R, 4, 4><<<grd, 128, sm, st>>>(B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
+    } else {
+      dim3 grd((nrows / 2 + L - 1) / L, 1);
+      if (L == 8)
+        k_fft_x_c2r<R, 8, 1><<<grd, 256, sm, st>>>(B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
+      else
+        k_fft_x_c2r<R, 4, 1><<<grd, 128, sm, st>>>(B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
+    }
     ++g_launches;
   }
 }
@@ -383,12 +434,19 @@ void allow_smem(K... kernels) {
    ...);
 }
 
+template <typename R>
+void allow_all() {
+  allow_smem(k_fft_x_r2c<R, 8>, k_fft_x_r2c<R, 4>, k_fft_y_fwd<R, 8>, k_fft_y_fwd<R, 4>,
+             k_fft_z_influence<R, 8>, k_fft_z_influence<R, 4>, k_fft_y_inv<R, 8>,
+             k_fft_y_inv<R, 4>, k_fft_x_c2r<R, 8, 4>, k_fft_x_c2r<R, 4, 4>, k_fft_x_c2r<R, 8, 1>,
+             k_fft_x_c2r<R, 4, 1>);
+}
+
 }  // namespace
 
 int mesh_configure_kernels() {
-  allow_smem(k_fft_x_r2c<double>, k_fft_y_fwd<double>, k_fft_z_influence<double>,
-             k_fft_y_inv<double>, k_fft_x_c2r<double>, k_fft_x_r2c<float>, k_fft_y_fwd<float>,
-             k_fft_z_influence<float>, k_fft_y_inv<float>, k_fft_x_c2r<float>);
+  allow_all<double>();
+  allow_all<float>();
   return cudaGetLastError() == cudaSuccess ? EWG_OK : EWG_ERR_CUDA;
 }
 
