@@ -1,0 +1,212 @@
+!> Fortran binding of the B200 Ewald operator's C ABI (include/ewald_b200.h).
+!>
+!> This module is what DFTB+ compiles next to src/dftbp/dftb/coulomb.F90 to
+!> reach the GPU engine: bind(C) interfaces in the style of the reference's own
+!> C interop (src/dftbp/common/envcheck.F90:24-38), plus thin wrappers that keep
+!> the reference library's argument order and stop with the library's message
+!> on a non-zero status, as the reference's `error stop` does.
+!>
+!> Arrays are passed in DFTB+'s native layouts: coords(3,N), latVecs(3,3) with
+!> one lattice vector per column, force(3,N).  No transposes are needed.
+module ewald_b200
+  use, intrinsic :: iso_c_binding, only : c_int, c_double, c_ptr, c_null_ptr, c_char, &
+      & c_associated, c_f_pointer, c_long_long
+  implicit none
+  private
+
+  public :: TEwaldGpu, ewaldGpuInit, ewaldGpuFinal
+  public :: ewaldGpuSetLattice, ewaldGpuSetCoords, ewaldGpuSetCharges
+  public :: ewaldGpuShift, ewaldGpuShiftForce, ewaldGpuStress
+  public :: ewaldGpuPotentialForce
+  public :: EWG_PRECISION_FP64, EWG_PRECISION_MIXED
+
+  integer(c_int), parameter :: EWG_PRECISION_FP64 = 0
+  integer(c_int), parameter :: EWG_PRECISION_MIXED = 1
+
+  !> Handle of one device context.
+  type :: TEwaldGpu
+    type(c_ptr) :: ctx = c_null_ptr
+  end type TEwaldGpu
+
+  !> ewg_overrides of the C header (unused members carry has_* = 0).
+  type, bind(C) :: TEwgOverrides
+    integer(c_int) :: has_alpha = 0, has_r_cut = 0, has_k_cut = 0, has_n_modes = 0, &
+        & has_window_cutoff = 0
+    real(c_double) :: alpha = 0.0_c_double, r_cut = 0.0_c_double, k_cut = 0.0_c_double
+    integer(c_int) :: n_modes = 0, window_cutoff = 0
+  end type TEwgOverrides
+
+  interface
+    function ewg_create(ctx, device, precision) bind(C, name="ewg_create") result(rc)
+      import :: c_ptr, c_int
+      type(c_ptr), intent(out) :: ctx
+      integer(c_int), value :: device, precision
+      integer(c_int) :: rc
+    end function ewg_create
+
+    function ewg_destroy(ctx) bind(C, name="ewg_destroy") result(rc)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: ctx
+      integer(c_int) :: rc
+    end function ewg_destroy
+
+    function ewg_status_string(status) bind(C, name="ewg_status_string") result(msg)
+      import :: c_int, c_ptr
+      integer(c_int), value :: status
+      type(c_ptr) :: msg
+    end function ewg_status_string
+
+    function ewg_set_lattice(ctx, latCols) bind(C, name="ewg_set_lattice") result(rc)
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: latCols(3, 3)
+      integer(c_int) :: rc
+    end function ewg_set_lattice
+
+    function ewg_set_coords(ctx, n, coords) bind(C, name="ewg_set_coords") result(rc)
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: n
+      real(c_double), intent(in) :: coords(3, *)
+      integer(c_int) :: rc
+    end function ewg_set_coords
+
+    function ewg_set_charges(ctx, dq) bind(C, name="ewg_set_charges") result(rc)
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: dq(*)
+      integer(c_int) :: rc
+    end function ewg_set_charges
+
+    function ewg_shift(ctx, tol, shift) bind(C, name="ewg_shift") result(rc)
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), value :: tol
+      real(c_double), intent(out) :: shift(*)
+      integer(c_int) :: rc
+    end function ewg_shift
+
+    function ewg_shift_force(ctx, tol, shift, force) bind(C, name="ewg_shift_force") result(rc)
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), value :: tol
+      real(c_double), intent(out) :: shift(*)
+      real(c_double), intent(out) :: force(3, *)
+      integer(c_int) :: rc
+    end function ewg_shift_force
+
+    function ewg_stress(ctx, tolEwald, alpha, sigma) bind(C, name="ewg_stress") result(rc)
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), value :: tolEwald, alpha
+      real(c_double), intent(out) :: sigma(3, 3)
+      integer(c_int) :: rc
+    end function ewg_stress
+
+    function ewg_potential_force(ctx, n, positions, charges, latRows, tol, pot, force, ov) &
+        & bind(C, name="ewg_potential_force") result(rc)
+      import :: c_ptr, c_int, c_double, TEwgOverrides
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: n
+      real(c_double), intent(in) :: positions(n, 3), charges(n), latRows(3, 3)
+      real(c_double), value :: tol
+      real(c_double), intent(out) :: pot(n)
+      real(c_double), intent(out) :: force(3, n)
+      type(TEwgOverrides), intent(in) :: ov
+      integer(c_int) :: rc
+    end function ewg_potential_force
+  end interface
+
+contains
+
+  !> Stop with the library's message, as the reference does on invalid input.
+  subroutine check(rc)
+    integer(c_int), intent(in) :: rc
+    character(kind=c_char), pointer :: msg(:)
+    character(len=128) :: text
+    integer :: i
+    if (rc == 0) return
+    call c_f_pointer(ewg_status_string(rc), msg, [128])
+    text = ""
+    do i = 1, 128
+      if (msg(i) == achar(0)) exit
+      text(i:i) = msg(i)
+    end do
+    error stop trim(text)
+  end subroutine check
+
+  subroutine ewaldGpuInit(this, device, precision)
+    type(TEwaldGpu), intent(out) :: this
+    integer, intent(in), optional :: device, precision
+    integer(c_int) :: dev, prec
+    dev = 0
+    prec = EWG_PRECISION_FP64
+    if (present(device)) dev = device
+    if (present(precision)) prec = precision
+    call check(ewg_create(this%ctx, dev, prec))
+  end subroutine ewaldGpuInit
+
+  subroutine ewaldGpuFinal(this)
+    type(TEwaldGpu), intent(inout) :: this
+    if (c_associated(this%ctx)) call check(ewg_destroy(this%ctx))
+    this%ctx = c_null_ptr
+  end subroutine ewaldGpuFinal
+
+  !> TCoulomb%updateLatVecs (coulomb.F90:575): latVecs(:, i) = a_i.
+  subroutine ewaldGpuSetLattice(this, latVecs)
+    type(TEwaldGpu), intent(in) :: this
+    real(c_double), intent(in) :: latVecs(3, 3)
+    call check(ewg_set_lattice(this%ctx, latVecs))
+  end subroutine ewaldGpuSetLattice
+
+  !> TCoulomb%updateCoords (coulomb.F90:509): coords(3, N) of the central cell.
+  subroutine ewaldGpuSetCoords(this, coords)
+    type(TEwaldGpu), intent(in) :: this
+    real(c_double), intent(in) :: coords(:, :)
+    call check(ewg_set_coords(this%ctx, int(size(coords, 2), c_int), coords))
+  end subroutine ewaldGpuSetCoords
+
+  !> TCoulomb%updateCharges (coulomb.F90:760).
+  subroutine ewaldGpuSetCharges(this, deltaQAtom)
+    type(TEwaldGpu), intent(in) :: this
+    real(c_double), intent(in) :: deltaQAtom(:)
+    call check(ewg_set_charges(this%ctx, deltaQAtom))
+  end subroutine ewaldGpuSetCharges
+
+  !> Replaces the call in fftEwaldShift (coulomb.F90:355).
+  subroutine ewaldGpuShift(this, tol, shift)
+    type(TEwaldGpu), intent(in) :: this
+    real(c_double), intent(in) :: tol
+    real(c_double), intent(out) :: shift(:)
+    call check(ewg_shift(this%ctx, tol, shift))
+  end subroutine ewaldGpuShift
+
+  !> Replaces the call in fftEwaldAddGradients (coulomb.F90:380); force = -dU/dR.
+  subroutine ewaldGpuShiftForce(this, tol, shift, force)
+    type(TEwaldGpu), intent(in) :: this
+    real(c_double), intent(in) :: tol
+    real(c_double), intent(out) :: shift(:), force(:, :)
+    call check(ewg_shift_force(this%ctx, tol, shift, force))
+  end subroutine ewaldGpuShiftForce
+
+  !> Replaces invRStress in TCoulomb%addStress (coulomb.F90:752); the caller
+  !> keeps stress = stress - 0.5 * sigma.
+  subroutine ewaldGpuStress(this, tolEwald, alpha, sigma)
+    type(TEwaldGpu), intent(in) :: this
+    real(c_double), intent(in) :: tolEwald, alpha
+    real(c_double), intent(out) :: sigma(3, 3)
+    call check(ewg_stress(this%ctx, tolEwald, alpha, sigma))
+  end subroutine ewaldGpuStress
+
+  !> Same argument order as ewald_potential_force (fft/ewald_fft_3d.f90:36).
+  subroutine ewaldGpuPotentialForce(this, positions, charges, nParticle, latVecs, tol, pot, force)
+    type(TEwaldGpu), intent(in) :: this
+    real(c_double), intent(in) :: positions(:, :), charges(:), latVecs(3, 3), tol
+    integer, intent(in) :: nParticle
+    real(c_double), intent(out) :: pot(:), force(:, :)
+    type(TEwgOverrides) :: ov
+    call check(ewg_potential_force(this%ctx, int(nParticle, c_int), positions, charges, latVecs, &
+        & tol, pot, force, ov))
+  end subroutine ewaldGpuPotentialForce
+
+end module ewald_b200
