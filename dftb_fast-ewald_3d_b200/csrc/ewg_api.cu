@@ -458,6 +458,8 @@ const char* ewg_status_string(int s) {
     case EWG_ERR_GRID_TOO_LARGE: return "ewald_b200: FFT length not supported (max 4096, radices <= 31)";
     case EWG_ERR_NO_DEVICE: return "ewald_b200: no CUDA device";
     case EWG_ERR_STATE: return "ewald_b200: call order (lattice, coords, charges) not satisfied";
+    case EWG_ERR_SCRATCH_LIMIT:
+      return "ewald_b200: too many atoms, boxes or modes for the fixed 16 MiB scratch";
     default: return "ewald_b200: unknown status";
   }
 }

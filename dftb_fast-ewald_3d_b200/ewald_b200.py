@@ -38,6 +38,7 @@ STATUS = {
     8: "EWG_ERR_CUTOFF", 9: "EWG_ERR_ALPHA_SEARCH", 10: "EWG_ERR_LATTICE_SEARCH",
     11: "EWG_ERR_OUT_OF_MEMORY", 12: "EWG_ERR_CUDA", 13: "EWG_ERR_DEVICE_TIMEOUT",
     14: "EWG_ERR_GRID_TOO_LARGE", 15: "EWG_ERR_NO_DEVICE", 16: "EWG_ERR_STATE",
+    17: "EWG_ERR_SCRATCH_LIMIT",
 }
 
 # Every entry point of include/ewald_b200.h.
@@ -48,6 +49,7 @@ EXPORTED = [
     "ewg_set_coords", "ewg_set_charges", "ewg_shift", "ewg_shift_force", "ewg_stress",
     "ewg_last_stress_setup", "ewg_batch_potential_force", "ewg_set_profiling", "ewg_stage_count",
     "ewg_stage_name", "ewg_stage_times", "ewg_reset_stage_times", "ewg_set_stream",
+    "ewg_direct_potential_force_static",
 ]
 
 

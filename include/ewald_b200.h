@@ -51,7 +51,9 @@ enum {
   EWG_ERR_DEVICE_TIMEOUT = 13,
   EWG_ERR_GRID_TOO_LARGE = 14, /* an FFT length beyond the kernels' limit (4096 per axis)  */
   EWG_ERR_NO_DEVICE = 15,
-  EWG_ERR_STATE = 16        /* call order: dftb/coulomb.F90 @:ASSERT(coordsUpdated_) etc. */
+  EWG_ERR_STATE = 16,       /* call order: dftb/coulomb.F90 @:ASSERT(coordsUpdated_) etc. */
+  EWG_ERR_SCRATCH_LIMIT = 17 /* configuration too large for the fixed scratch of
+                                ewg_direct_potential_force_static                   */
 };
 
 /* ---- precision forms ---------------------------------------------------- */
@@ -145,6 +147,29 @@ int ewg_direct_potential_force(ewg_context* ctx, int n, const double* positions,
                                const double* charges, const double* lat_rows, double tol,
                                double* pot, double* force, const double* alpha_in,
                                const double* r_cut_in, const double* k_cut_in);
+
+/* The direct engine without any allocation.  No counterpart in the reference:
+ * it exists for host codes that cannot allocate device memory once a run is
+ * under way (for instance a program that gives all device memory to its own
+ * pool allocator at start-up, or one that must not risk an allocation failing
+ * or stalling inside an MD or SCC loop).  Same results as
+ * ewg_direct_potential_force, but every array is a device pointer owned by the
+ * caller: coords(3,N), charges(N), pot(N), force(3,N) (force may be NULL);
+ * lat_rows and the optional arguments are host values.  All working memory
+ * comes from one fixed 16 MiB array in device memory that every GPU loading
+ * the library holds until the process exits; configurations that do not fit
+ * (atoms, cell-list boxes and Fourier modes together) return
+ * EWG_ERR_SCRATCH_LIMIT before any kernel runs.  It calls no cudaMalloc,
+ * cudaFree or other allocating routine.  All calls share that array, so calls
+ * that overlap on the GPU race; run them one at a time.  The first call on a
+ * device looks up the array's device address for that device; make that first
+ * call before any stream capture begins.  stream is a cudaStream_t (NULL: the
+ * default stream); the call returns after the work has finished. */
+int ewg_direct_potential_force_static(int n, const double* coords_device,
+                                      const double* charges_device, const double* lat_rows,
+                                      double tol, double* pot_device, double* force_device,
+                                      const double* alpha_in, const double* r_cut_in,
+                                      const double* k_cut_in, void* stream);
 
 /* ---- TCoulomb surface: src/dftbp/dftb/coulomb.F90 ----------------------- */
 
