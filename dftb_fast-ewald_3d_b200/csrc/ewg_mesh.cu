@@ -99,6 +99,7 @@ __global__ void __launch_bounds__(32 * L) k_fft_y_fwd(const cx<R>* __restrict__ 
   const int i3 = blockIdx.y;
   const int kk = threadIdx.x % L;
   const bool kin = k0 + kk < K1;
+#pragma unroll 4
   for (int i2 = threadIdx.x / L; i2 < n2; i2 += blockDim.x / L)
     a[i2 * LP + kk] = kin ? A1[(static_cast<size_t>(i3) * n2 + i2) * K1 + k0 + kk] : mk(R(0), R(0));
   __syncthreads();
@@ -136,6 +137,7 @@ __global__ void __launch_bounds__(32 * L) k_fft_z_influence(const cx<R>* __restr
   const int rstep = blockDim.x / L;
   const bool kin = k0 + kk < K1;
   const cx<R>* tw = plan_twiddles<R>(plan);
+#pragma unroll 4
   for (int i3 = threadIdx.x / L; i3 < n3; i3 += rstep)
     a[i3 * LP + kk] = kin ? A2[(static_cast<size_t>(i3) * K2 + k2i) * K1 + k0 + kk] : mk(R(0), R(0));
   __syncthreads();
@@ -222,6 +224,7 @@ __global__ void __launch_bounds__(32 * L) k_fft_y_inv(const cx<R>* __restrict__ 
   const int kk = threadIdx.x % L;
   const bool kin = k0 + kk < K1;
   const cx<R>* src = B2 + static_cast<size_t>(c) * n3 * K2 * K1;
+#pragma unroll 4
   for (int i2 = threadIdx.x / L; i2 < n2; i2 += blockDim.x / L) {
     int k2 = 0;
     bool inside = kin;

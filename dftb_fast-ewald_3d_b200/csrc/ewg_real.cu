@@ -88,18 +88,26 @@ __global__ void k_count(const int* __restrict__ key, int n, int* __restrict__ co
   if (i < n) atomicAdd(&counts[key[i]], 1);
 }
 
-// Exclusive scan of counts into starts[0..nkeys]; one CTA of 1024 threads.
+// Exclusive scan of counts into starts[0..nkeys]; one CTA of 1024 threads,
+// each scanning 16 consecutive entries per round.
 __global__ void __launch_bounds__(1024) k_scan(const int* __restrict__ counts, int nkeys,
                                                int* __restrict__ starts) {
+  constexpr int kItems = 16;
   __shared__ int warp_sums[32];
   __shared__ int carry;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int base = 0; base < nkeys; base += 1024) {
-    const int i = base + threadIdx.x;
-    const int v = i < nkeys ? counts[i] : 0;
-    int x = v;
+  for (int base = 0; base < nkeys; base += 1024 * kItems) {
+    const int first = base + threadIdx.x * kItems;
+    int v[kItems];
+    int local = 0;
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+      v[j] = first + j < nkeys ? counts[first + j] : 0;
+      local += v[j];
+    }
+    int x = local;
     for (int off = 1; off < 32; off <<= 1) {
       const int y = __shfl_up_sync(0xffffffffu, x, off);
       if (lane >= off) x += y;
@@ -115,10 +123,14 @@ __global__ void __launch_bounds__(1024) k_scan(const int* __restrict__ counts, i
       warp_sums[lane] = w;
     }
     __syncthreads();
-    const int incl = x + (wid > 0 ? warp_sums[wid - 1] : 0);
-    if (i < nkeys) starts[i] = carry + incl - v;
+    int run = carry + x - local + (wid > 0 ? warp_sums[wid - 1] : 0);
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+      if (first + j < nkeys) starts[first + j] = run;
+      run += v[j];
+    }
     __syncthreads();
-    if (threadIdx.x == 1023) carry += incl;
+    if (threadIdx.x == 1023) carry = run;
     __syncthreads();
   }
   if (threadIdx.x == 0) starts[nkeys] = carry;

@@ -37,7 +37,6 @@ namespace {
 
 constexpr int TX = kTileX, TY = kTileY, TZ = kTileZ;
 constexpr int kPencils = TY * TZ;  // spread: one thread per x-pencil
-constexpr int kGatherThreads = 64;
 constexpr int kSpreadChunk = 64;   // atoms whose weights are staged at once
 
 __device__ __forceinline__ int pmod(int a, int n) {
@@ -172,6 +171,8 @@ __global__ void __launch_bounds__(kPencils) k_spread_tiles(const int* __restrict
   __shared__ R sW1[kSpreadChunk][TX];
   __shared__ R sW2[kSpreadChunk][TY];
   __shared__ R sW3[kSpreadChunk][TZ];
+  __shared__ int2 sPair[kSpreadChunk];
+  __shared__ R sQ[kSpreadChunk];
   const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
   const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
   const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
@@ -183,17 +184,26 @@ __global__ void __launch_bounds__(kPencils) k_spread_tiles(const int* __restrict
   for (int b0 = p0; b0 < p1; b0 += kSpreadChunk) {
     const int nb = min(kSpreadChunk, p1 - b0);
     __syncthreads();
+    // Stage the chunk's pairs and charges, then its weights (two dependent
+    // rounds of loads instead of one per weight).
+    if (threadIdx.x < nb) {
+      const int2 pr = pairs[b0 + threadIdx.x];
+      sPair[threadIdx.x] = pr;
+      sQ[threadIdx.x] = qk[pr.x];
+    }
+    __syncthreads();
+#pragma unroll 4
     for (int it = threadIdx.x; it < nb * (TX + TY + TZ); it += blockDim.x) {
       const int a = it / (TX + TY + TZ);
       const int r = it - a * (TX + TY + TZ);
-      const int2 pr = pairs[b0 + a];
+      const int2 pr = sPair[a];
       const R* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
       if (r < TX) {
         sW1[a][r] = wk[sd.woff[0] + (pr.y & 0xff) * TX + r];
       } else if (r < TX + TY) {
         sW2[a][r - TX] = wk[sd.woff[1] + ((pr.y >> 8) & 0xff) * TY + (r - TX)];
       } else {
-        sW3[a][r - TX - TY] = wk[sd.woff[2] + (pr.y >> 16) * TZ + (r - TX - TY)] * qk[pr.x];
+        sW3[a][r - TX - TY] = wk[sd.woff[2] + (pr.y >> 16) * TZ + (r - TX - TY)] * sQ[a];
       }
     }
     __syncthreads();
@@ -220,12 +230,16 @@ __global__ void __launch_bounds__(kPencils) k_spread_tiles(const int* __restrict
 }
 
 // ---------------------------------------------------------------------------
-// Gather
+// Gather.  One warp per CTA; each lane carries A atoms of the tile's list, so
+// every grid value read from shared memory (a broadcast: all lanes read the
+// same point) feeds A atoms.
 // ---------------------------------------------------------------------------
-template <typename R, int NC>
-__global__ void __launch_bounds__(kGatherThreads) k_gather_tiles(
-    const int* __restrict__ tile_start, const int2* __restrict__ pairs, const R* __restrict__ wtab,
-    StencilDims sd, const R* __restrict__ grid, double* __restrict__ part) {
+template <typename R, int NC, int A>
+__global__ void __launch_bounds__(32) k_gather_tiles(const int* __restrict__ tile_start,
+                                                     const int2* __restrict__ pairs,
+                                                     const R* __restrict__ wtab, StencilDims sd,
+                                                     const R* __restrict__ grid,
+                                                     double* __restrict__ part) {
   using V = typename std::conditional<
       NC == 4, typename std::conditional<sizeof(R) == 8, double4, float4>::type, R>::type;
   __shared__ V sG[TZ * TY * TX];
@@ -234,8 +248,9 @@ __global__ void __launch_bounds__(kGatherThreads) k_gather_tiles(
   const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
   const int ex = min(TX, sd.n[0] - x0), ey = min(TY, sd.n[1] - y0), ez = min(TZ, sd.n[2] - z0);
   const int p0 = tile_start[tile], p1 = tile_start[tile + 1];
-  if (p0 == p1) return;  // uniform across the CTA: no atom reaches this tile
-  for (int t = threadIdx.x; t < TX * TY * TZ; t += blockDim.x) {
+  if (p0 == p1) return;  // no atom reaches this tile
+#pragma unroll 4
+  for (int t = threadIdx.x; t < TX * TY * TZ; t += 32) {
     const int x = t % TX, y = (t / TX) % TY, z = t / (TX * TY);
     V v;
     if (x < ex && y < ey && z < ez) {
@@ -249,65 +264,82 @@ __global__ void __launch_bounds__(kGatherThreads) k_gather_tiles(
     }
     sG[t] = v;
   }
-  __syncthreads();
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __syncwarp();
+  const int lane = threadIdx.x;
   const int nslots = sd.S[0] * sd.S[1] * sd.S[2];
-  for (int a0 = p0 + wid * 32; a0 < p1; a0 += kGatherThreads) {
-    const int e = a0 + lane;
-    const bool active = e < p1;
-    R w1[TX], w2[TY], w3[TZ];
-    int2 pr = make_int2(0, 0);
-    if (active) {
-      pr = pairs[e];
-      const R* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
+  for (int a0 = p0; a0 < p1; a0 += 32 * A) {
+    R w1[A][TX], w2[A][TY];
+    const R* wz[A];
+    int2 pr[A];
+    bool act[A];
 #pragma unroll
-      for (int x = 0; x < TX; ++x) w1[x] = wk[sd.woff[0] + (pr.y & 0xff) * TX + x];
+    for (int a = 0; a < A; ++a) {
+      const int e = a0 + a * 32 + lane;
+      act[a] = e < p1;
+      pr[a] = act[a] ? pairs[e] : make_int2(0, 0);
+      const R* wk = wtab + static_cast<size_t>(pr[a].x) * sd.wstride;
 #pragma unroll
-      for (int y = 0; y < TY; ++y) w2[y] = wk[sd.woff[1] + ((pr.y >> 8) & 0xff) * TY + y];
+      for (int x = 0; x < TX; ++x) w1[a][x] = act[a] ? wk[sd.woff[0] + (pr[a].y & 0xff) * TX + x] : R(0);
 #pragma unroll
-      for (int z = 0; z < TZ; ++z) w3[z] = wk[sd.woff[2] + (pr.y >> 16) * TZ + z];
-    } else {
-#pragma unroll
-      for (int i = 0; i < TX; ++i) w1[i] = R(0);
-#pragma unroll
-      for (int i = 0; i < TY; ++i) w2[i] = R(0);
-#pragma unroll
-      for (int i = 0; i < TZ; ++i) w3[i] = R(0);
+      for (int y = 0; y < TY; ++y)
+        w2[a][y] = act[a] ? wk[sd.woff[1] + ((pr[a].y >> 8) & 0xff) * TY + y] : R(0);
+      wz[a] = wk + sd.woff[2] + (pr[a].y >> 16) * TZ;
     }
-    double acc[NC];
+    double acc[A][NC];
 #pragma unroll
-    for (int c = 0; c < NC; ++c) acc[c] = 0.0;
+    for (int a = 0; a < A; ++a)
 #pragma unroll
+      for (int c = 0; c < NC; ++c) acc[a][c] = 0.0;
+#pragma unroll 1
     for (int z = 0; z < TZ; ++z) {
+      R w3[A];
+#pragma unroll
+      for (int a = 0; a < A; ++a) w3[a] = act[a] ? wz[a][z] : R(0);
 #pragma unroll
       for (int y = 0; y < TY; ++y) {
-        const R w23 = w2[y] * w3[z];
-        if (!__any_sync(0xffffffffu, w23 != R(0))) continue;
-        R rs[NC];
+        R w23[A];
+        bool any = false;
 #pragma unroll
-        for (int c = 0; c < NC; ++c) rs[c] = R(0);
+        for (int a = 0; a < A; ++a) {
+          w23[a] = w2[a][y] * w3[a];
+          any = any || (w23[a] != R(0));
+        }
+        if (!__any_sync(0xffffffffu, any)) continue;
+        R rs[A][NC];
+#pragma unroll
+        for (int a = 0; a < A; ++a)
+#pragma unroll
+          for (int c = 0; c < NC; ++c) rs[a][c] = R(0);
         const V* row = sG + (z * TY + y) * TX;
 #pragma unroll
         for (int x = 0; x < TX; ++x) {
           const V g = row[x];
-          if constexpr (NC == 4) {
-            rs[0] = fma(w1[x], g.x, rs[0]);
-            rs[1] = fma(w1[x], g.y, rs[1]);
-            rs[2] = fma(w1[x], g.z, rs[2]);
-            rs[3] = fma(w1[x], g.w, rs[3]);
-          } else {
-            rs[0] = fma(w1[x], g, rs[0]);
+#pragma unroll
+          for (int a = 0; a < A; ++a) {
+            if constexpr (NC == 4) {
+              rs[a][0] = fma(w1[a][x], g.x, rs[a][0]);
+              rs[a][1] = fma(w1[a][x], g.y, rs[a][1]);
+              rs[a][2] = fma(w1[a][x], g.z, rs[a][2]);
+              rs[a][3] = fma(w1[a][x], g.w, rs[a][3]);
+            } else {
+              rs[a][0] = fma(w1[a][x], g, rs[a][0]);
+            }
           }
         }
 #pragma unroll
-        for (int c = 0; c < NC; ++c) acc[c] += static_cast<double>(w23 * rs[c]);
+        for (int a = 0; a < A; ++a)
+#pragma unroll
+          for (int c = 0; c < NC; ++c) acc[a][c] += static_cast<double>(w23[a] * rs[a][c]);
       }
     }
-    if (active) {
-      const int sidx = ((pr.y >> 16) * sd.S[1] + ((pr.y >> 8) & 0xff)) * sd.S[0] + (pr.y & 0xff);
-      double* dst = part + (static_cast<size_t>(pr.x) * nslots + sidx) * NC;
 #pragma unroll
-      for (int c = 0; c < NC; ++c) dst[c] = acc[c];
+    for (int a = 0; a < A; ++a) {
+      if (!act[a]) continue;
+      const int ps = pr[a].y;
+      const int sidx = ((ps >> 16) * sd.S[1] + ((ps >> 8) & 0xff)) * sd.S[0] + (ps & 0xff);
+      double* dst = part + (static_cast<size_t>(pr[a].x) * nslots + sidx) * NC;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) dst[c] = acc[a][c];
     }
   }
 }
@@ -399,10 +431,9 @@ void launch_spread(const MeshPlan& mp, const int* tile_start, const int2* pairs,
 void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs, const void* wtab,
                    const void* grid, int nc, double* part, cudaStream_t st) {
   dim3 grd(mp.sd.ntiles[0], mp.sd.ntiles[1], mp.sd.ntiles[2]);
-#define EWG_GATHER(R, NC)                                                                      \
-  k_gather_tiles<R, NC><<<grd, kGatherThreads, 0, st>>>(tile_start, pairs,                     \
-                                                        static_cast<const R*>(wtab), mp.sd,    \
-                                                        static_cast<const R*>(grid), part)
+#define EWG_GATHER(R, NC)                                                                 \
+  k_gather_tiles<R, NC, 2><<<grd, 32, 0, st>>>(tile_start, pairs, static_cast<const R*>(wtab), \
+                                               mp.sd, static_cast<const R*>(grid), part)
   if (mp.mixed) {
     if (nc == 4)
       EWG_GATHER(float, 4);
