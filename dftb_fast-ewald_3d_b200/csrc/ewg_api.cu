@@ -310,6 +310,7 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
     const int H = mp.g.M[d] - mp.g.M[d] / 2;
     if ((rc = get_corr(c, mp.g.n[d], H, mp.g.m, &mp.corr2[d]))) return rc;
   }
+  if ((rc = mesh_check_lengths(mp.g, mixed))) return rc;
   stencil_dims(mp.g, mp.sd);
   const int nboxes = rg.nb[0] * rg.nb[1] * rg.nb[2];
   const int ntiles = mp.sd.ntiles[0] * mp.sd.ntiles[1] * mp.sd.ntiles[2];
@@ -455,7 +456,7 @@ const char* ewg_status_string(int s) {
     case EWG_ERR_OUT_OF_MEMORY: return "ewald_b200: out of device memory";
     case EWG_ERR_CUDA: return "ewald_b200: CUDA error";
     case EWG_ERR_DEVICE_TIMEOUT: return "ewald_b200: device wait timed out";
-    case EWG_ERR_GRID_TOO_LARGE: return "ewald_b200: FFT length not supported (max 4096, radices <= 31)";
+    case EWG_ERR_GRID_TOO_LARGE: return "ewald_b200: FFT length not supported (max 4096 and radices <= 31; in FP64 about 2500 on the fused z axis)";
     case EWG_ERR_NO_DEVICE: return "ewald_b200: no CUDA device";
     case EWG_ERR_STATE: return "ewald_b200: call order (lattice, coords, charges) not satisfied";
     case EWG_ERR_SCRATCH_LIMIT:

@@ -40,20 +40,23 @@ __device__ __forceinline__ int pmod(int a, int n) {
 }
 
 // Every pass stages L lines (a power of two, the fastest index) of length n in
-// shared memory as buf[e * (L + 1) + line]; blockDim.x = 32 * L.
+// shared memory as buf[e * (L + 1) + line]; blockDim.x = pass_threads(L): 32
+// threads per line, at least 128 per CTA.
+constexpr int pass_threads(int L) { return L >= 4 ? 32 * L : 128; }
 
 // ---------------------------------------------------------------------------
 // x pass, real to complex: row pairs (2p, 2p+1) form one complex line; keep
 // k1 = 0..K1-1 of each row.
 // ---------------------------------------------------------------------------
 template <typename R, int L>
-__global__ void __launch_bounds__(32 * L) k_fft_x_r2c(const R* __restrict__ grid,
+__global__ void __launch_bounds__(pass_threads(L)) k_fft_x_r2c(const R* __restrict__ grid,
                                                       cx<R>* __restrict__ A1, int n1, int npairs,
                                                       int K1, FftPlan plan) {
   constexpr int LP = L + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
   cx<R>* b = a + static_cast<size_t>(n1) * LP;
+  const cx<R>* tw = plan_twiddles<R>(plan);
   const int pair0 = blockIdx.x * L;
   for (int x = threadIdx.x; x < n1; x += blockDim.x) {
 #pragma unroll
@@ -68,7 +71,6 @@ __global__ void __launch_bounds__(32 * L) k_fft_x_r2c(const R* __restrict__ grid
     }
   }
   __syncthreads();
-  const cx<R>* tw = plan_twiddles<R>(plan);
   cx<R>* res = fft_cols<R, -1, L>(a, b, n1, plan, tw);
   const R h = R(0.5);
   for (int t = threadIdx.x; t < K1 * L; t += blockDim.x) {
@@ -88,13 +90,14 @@ __global__ void __launch_bounds__(32 * L) k_fft_x_r2c(const R* __restrict__ grid
 // y pass, forward: lines over i2 for (i3, k1-block); keep k2 in [-H2, H2].
 // ---------------------------------------------------------------------------
 template <typename R, int L>
-__global__ void __launch_bounds__(32 * L) k_fft_y_fwd(const cx<R>* __restrict__ A1,
+__global__ void __launch_bounds__(pass_threads(L)) k_fft_y_fwd(const cx<R>* __restrict__ A1,
                                                       cx<R>* __restrict__ A2, int n2, int K1,
                                                       int K2, int H2, FftPlan plan) {
   constexpr int LP = L + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
   cx<R>* b = a + static_cast<size_t>(n2) * LP;
+  const cx<R>* tw = plan_twiddles<R>(plan);
   const int k0 = blockIdx.x * L;
   const int i3 = blockIdx.y;
   const int kk = threadIdx.x % L;
@@ -103,7 +106,7 @@ __global__ void __launch_bounds__(32 * L) k_fft_y_fwd(const cx<R>* __restrict__ 
   for (int i2 = threadIdx.x / L; i2 < n2; i2 += blockDim.x / L)
     a[i2 * LP + kk] = kin ? A1[(static_cast<size_t>(i3) * n2 + i2) * K1 + k0 + kk] : mk(R(0), R(0));
   __syncthreads();
-  cx<R>* res = fft_cols<R, -1, L>(a, b, n2, plan, plan_twiddles<R>(plan));
+  cx<R>* res = fft_cols<R, -1, L>(a, b, n2, plan, tw);
   if (kin)
     for (int k2i = threadIdx.x / L; k2i < K2; k2i += blockDim.x / L)
       A2[(static_cast<size_t>(i3) * K2 + k2i) * K1 + k0 + kk] = res[pmod(k2i - H2, n2) * LP + kk];
@@ -122,7 +125,7 @@ struct InfluenceArgs {
 };
 
 template <typename R, int L>
-__global__ void __launch_bounds__(32 * L) k_fft_z_influence(const cx<R>* __restrict__ A2,
+__global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(const cx<R>* __restrict__ A2,
                                                             cx<R>* __restrict__ B2, int n3, int K1,
                                                             int K2, int K3, int nc,
                                                             InfluenceArgs ia, FftPlan plan) {
@@ -131,12 +134,12 @@ __global__ void __launch_bounds__(32 * L) k_fft_z_influence(const cx<R>* __restr
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
   cx<R>* b = a + static_cast<size_t>(n3) * LP;
   cx<R>* q = b + static_cast<size_t>(n3) * LP;  // K3 weighted modes per line
+  const cx<R>* tw = plan_twiddles<R>(plan);
   const int k0 = blockIdx.x * L;
   const int k2i = blockIdx.y;
   const int kk = threadIdx.x % L;
   const int rstep = blockDim.x / L;
   const bool kin = k0 + kk < K1;
-  const cx<R>* tw = plan_twiddles<R>(plan);
 #pragma unroll 4
   for (int i3 = threadIdx.x / L; i3 < n3; i3 += rstep)
     a[i3 * LP + kk] = kin ? A2[(static_cast<size_t>(i3) * K2 + k2i) * K1 + k0 + kk] : mk(R(0), R(0));
@@ -211,13 +214,14 @@ __global__ void __launch_bounds__(32 * L) k_fft_z_influence(const cx<R>* __restr
 // y pass inverse: zero-padded k2 box -> i2, for (k1-block, i3, component).
 // ---------------------------------------------------------------------------
 template <typename R, int L>
-__global__ void __launch_bounds__(32 * L) k_fft_y_inv(const cx<R>* __restrict__ B2,
+__global__ void __launch_bounds__(pass_threads(L)) k_fft_y_inv(const cx<R>* __restrict__ B2,
                                                       cx<R>* __restrict__ B1, int n2, int n3,
                                                       int K1, int K2, int H2, FftPlan plan) {
   constexpr int LP = L + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
   cx<R>* b = a + static_cast<size_t>(n2) * LP;
+  const cx<R>* tw = plan_twiddles<R>(plan);
   const int k0 = blockIdx.x * L;
   const int i3 = blockIdx.y;
   const int c = blockIdx.z;
@@ -238,7 +242,7 @@ __global__ void __launch_bounds__(32 * L) k_fft_y_inv(const cx<R>* __restrict__ 
         inside ? src[(static_cast<size_t>(i3) * K2 + k2 + H2) * K1 + k0 + kk] : mk(R(0), R(0));
   }
   __syncthreads();
-  cx<R>* res = fft_cols<R, 1, L>(a, b, n2, plan, plan_twiddles<R>(plan));
+  cx<R>* res = fft_cols<R, 1, L>(a, b, n2, plan, tw);
   cx<R>* dst = B1 + static_cast<size_t>(c) * n3 * n2 * K1;
   if (kin)
     for (int i2 = threadIdx.x / L; i2 < n2; i2 += blockDim.x / L)
@@ -251,7 +255,7 @@ __global__ void __launch_bounds__(32 * L) k_fft_y_inv(const cx<R>* __restrict__ 
 // nc components per grid point.
 // ---------------------------------------------------------------------------
 template <typename R, int L, int NCG>
-__global__ void __launch_bounds__(32 * L) k_fft_x_c2r(const cx<R>* __restrict__ B1,
+__global__ void __launch_bounds__(pass_threads(L)) k_fft_x_c2r(const cx<R>* __restrict__ B1,
                                                       R* __restrict__ out, int n1, int nrows,
                                                       int K1, int nc, FftPlan plan) {
   constexpr int LP = L + 1;
@@ -259,6 +263,7 @@ __global__ void __launch_bounds__(32 * L) k_fft_x_c2r(const cx<R>* __restrict__ 
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
   cx<R>* b = a + static_cast<size_t>(n1) * LP;
+  const cx<R>* tw = plan_twiddles<R>(plan);
   const int pair0 = blockIdx.x * NP;
   const int c0 = blockIdx.y * NCG;
   const int npairs = nrows / 2;
@@ -288,7 +293,7 @@ __global__ void __launch_bounds__(32 * L) k_fft_x_c2r(const cx<R>* __restrict__ 
     }
   }
   __syncthreads();
-  cx<R>* res = fft_cols<R, 1, L>(a, b, n1, plan, plan_twiddles<R>(plan));
+  cx<R>* res = fft_cols<R, 1, L>(a, b, n1, plan, tw);
   for (int x = threadIdx.x; x < n1; x += blockDim.x) {
 #pragma unroll
     for (int l = 0; l < NP; ++l) {
@@ -320,11 +325,30 @@ size_t cbytes() {
   return sizeof(cx<R>);
 }
 
-// Lines per CTA: 8 when both ping-pong buffers of the longest line fit in 64 KB
-// (several CTAs per SM), else 4.
-int pick_lines(int n, size_t cb, size_t extra_per_line_elems = 0) {
-  const size_t bytes8 = (2 * static_cast<size_t>(n) + extra_per_line_elems) * 9 * cb;
-  return bytes8 <= 64 * 1024 ? 8 : 4;
+// Shared bytes of one pass CTA: two ping-pong buffers of L lines plus `extra`
+// elements per line.
+size_t pass_smem(int n, int L, size_t cb, int extra) {
+  return (2 * static_cast<size_t>(n) + extra) * (L + 1) * cb;
+}
+
+// Lines per CTA: 8 when that fits in 64 KB (several CTAs per SM), else the
+// largest of 4, 2, 1 within the per-CTA budget; 0 when even one line does not fit.
+int pick_lines(int n, size_t cb, int extra = 0) {
+  if (pass_smem(n, 8, cb, extra) <= 64 * 1024) return 8;
+  for (int L = 4; L >= 1; L /= 2)
+    if (pass_smem(n, L, cb, extra) <= kSmemBudget) return L;
+  return 0;
+}
+
+// Calls f(std::integral_constant<int, L>) for L in {1, 2, 4, 8}.
+template <typename F>
+void with_lines(int L, F&& f) {
+  switch (L) {
+    case 8: f(std::integral_constant<int, 8>{}); break;
+    case 4: f(std::integral_constant<int, 4>{}); break;
+    case 2: f(std::integral_constant<int, 2>{}); break;
+    default: f(std::integral_constant<int, 1>{}); break;
+  }
 }
 
 template <typename R>
@@ -340,26 +364,25 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
     prof_mark(mp.prof, st, ST_FFT_X_R2C);
     const int npairs = n2 * n3 / 2;
     const int L = pick_lines(n1, cb);
-    const size_t sm = 2 * static_cast<size_t>(n1) * (L + 1) * cb;
+    const size_t sm = pass_smem(n1, L, cb, 0);
     const int blocks = (npairs + L - 1) / L;
-    if (L == 8)
-      k_fft_x_r2c<R, 8><<<blocks, 256, sm, st>>>(static_cast<const R*>(grid), A1, n1, npairs, g.K1,
-                                                   mp.fft[0]);
-    else
-      k_fft_x_r2c<R, 4><<<blocks, 128, sm, st>>>(static_cast<const R*>(grid), A1, n1, npairs, g.K1,
-                                                   mp.fft[0]);
+    with_lines(L, [&](auto lc) {
+      constexpr int LL = decltype(lc)::value;
+      k_fft_x_r2c<R, LL><<<blocks, pass_threads(LL), sm, st>>>(static_cast<const R*>(grid), A1, n1, npairs,
+                                                       g.K1, mp.fft[0]);
+    });
     ++g_launches;
   }
   {  // y forward
     prof_mark(mp.prof, st, ST_FFT_Y_FWD);
     const int L = pick_lines(n2, cb);
-    const size_t sm = 2 * static_cast<size_t>(n2) * (L + 1) * cb;
+    const size_t sm = pass_smem(n2, L, cb, 0);
     dim3 grd((g.K1 + L - 1) / L, n3);
     const int H2 = (g.K2 - 1) / 2;
-    if (L == 8)
-      k_fft_y_fwd<R, 8><<<grd, 256, sm, st>>>(A1, A2, n2, g.K1, g.K2, H2, mp.fft[1]);
-    else
-      k_fft_y_fwd<R, 4><<<grd, 128, sm, st>>>(A1, A2, n2, g.K1, g.K2, H2, mp.fft[1]);
+    with_lines(L, [&](auto lc) {
+      constexpr int LL = decltype(lc)::value;
+      k_fft_y_fwd<R, LL><<<grd, pass_threads(LL), sm, st>>>(A1, A2, n2, g.K1, g.K2, H2, mp.fft[1]);
+    });
     ++g_launches;
   }
   {  // z forward + influence + z inverse
@@ -376,12 +399,13 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
     ia.inv4a2 = 1.0 / (4.0 * (g.alpha * g.alpha));
     for (int d = 0; d < 3; ++d) ia.corr2[d] = mp.corr2[d];
     const int L = pick_lines(n3, cb, g.K3);
-    const size_t sm = (2 * static_cast<size_t>(n3) + g.K3) * (L + 1) * cb;
+    const size_t sm = pass_smem(n3, L, cb, g.K3);
     dim3 grd((g.K1 + L - 1) / L, g.K2);
-    if (L == 8)
-      k_fft_z_influence<R, 8><<<grd, 256, sm, st>>>(A2, B2, n3, g.K1, g.K2, g.K3, nc, ia, mp.fft[2]);
-    else
-      k_fft_z_influence<R, 4><<<grd, 128, sm, st>>>(A2, B2, n3, g.K1, g.K2, g.K3, nc, ia, mp.fft[2]);
+    with_lines(L, [&](auto lc) {
+      constexpr int LL = decltype(lc)::value;
+      k_fft_z_influence<R, LL><<<grd, pass_threads(LL), sm, st>>>(A2, B2, n3, g.K1, g.K2, g.K3, nc, ia,
+                                                         mp.fft[2]);
+    });
     ++g_launches;
   }
 }
@@ -397,34 +421,34 @@ void inverse_impl(const MeshPlan& mp, const void* B2v, void* B1v, void* out, int
   {
     prof_mark(mp.prof, st, ST_FFT_Y_INV);
     const int L = pick_lines(n2, cb);
-    const size_t sm = 2 * static_cast<size_t>(n2) * (L + 1) * cb;
+    const size_t sm = pass_smem(n2, L, cb, 0);
     dim3 grd((g.K1 + L - 1) / L, n3, nc);
     const int H2 = (g.K2 - 1) / 2;
-    if (L == 8)
-      k_fft_y_inv<R, 8><<<grd, 256, sm, st>>>(B2, B1, n2, n3, g.K1, g.K2, H2, mp.fft[1]);
-    else
-      k_fft_y_inv<R, 4><<<grd, 128, sm, st>>>(B2, B1, n2, n3, g.K1, g.K2, H2, mp.fft[1]);
+    with_lines(L, [&](auto lc) {
+      constexpr int LL = decltype(lc)::value;
+      k_fft_y_inv<R, LL><<<grd, pass_threads(LL), sm, st>>>(B2, B1, n2, n3, g.K1, g.K2, H2, mp.fft[1]);
+    });
     ++g_launches;
   }
   {
     prof_mark(mp.prof, st, ST_FFT_X_C2R);
     const int nrows = n2 * n3;
     const int L = pick_lines(n1, cb);
-    const size_t sm = 2 * static_cast<size_t>(n1) * (L + 1) * cb;
+    const size_t sm = pass_smem(n1, L, cb, 0);
     R* o = static_cast<R*>(out);
-    if (nc == 4) {
+    if (nc == 4 && L >= 4) {  // the four components of a row pair in one CTA
       const int NP = L / 4;
       dim3 grd((nrows / 2 + NP - 1) / NP, 1);
       if (L == 8)
-        k_fft_x_c2r<R, 8, 4><<<grd, 256, sm, st>>>(B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
+        k_fft_x_c2r<R, 8, 4><<<grd, pass_threads(8), sm, st>>>(B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
       else
-        k_fft_x_c2r<R, 4, 4><<<grd, 128, sm, st>>>(B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
-    } else {
-      dim3 grd((nrows / 2 + L - 1) / L, 1);
-      if (L == 8)
-        k_fft_x_c2r<R, 8, 1><<<grd, 256, sm, st>>>(B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
-      else
-        k_fft_x_c2r<R, 4, 1><<<grd, 128, sm, st>>>(B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
+        k_fft_x_c2r<R, 4, 4><<<grd, pass_threads(4), sm, st>>>(B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
+    } else {  // one component per CTA row (grid.y = component)
+      dim3 grd((nrows / 2 + L - 1) / L, nc);
+      with_lines(L, [&](auto lc) {
+        constexpr int LL = decltype(lc)::value;
+        k_fft_x_c2r<R, LL, 1><<<grd, pass_threads(LL), sm, st>>>(B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
+      });
     }
     ++g_launches;
   }
@@ -437,15 +461,30 @@ void allow_smem(K... kernels) {
    ...);
 }
 
+template <typename R, int L>
+void allow_lines() {
+  allow_smem(k_fft_x_r2c<R, L>, k_fft_y_fwd<R, L>, k_fft_z_influence<R, L>, k_fft_y_inv<R, L>,
+             k_fft_x_c2r<R, L, 1>);
+}
+
 template <typename R>
 void allow_all() {
-  allow_smem(k_fft_x_r2c<R, 8>, k_fft_x_r2c<R, 4>, k_fft_y_fwd<R, 8>, k_fft_y_fwd<R, 4>,
-             k_fft_z_influence<R, 8>, k_fft_z_influence<R, 4>, k_fft_y_inv<R, 8>,
-             k_fft_y_inv<R, 4>, k_fft_x_c2r<R, 8, 4>, k_fft_x_c2r<R, 4, 4>, k_fft_x_c2r<R, 8, 1>,
-             k_fft_x_c2r<R, 4, 1>);
+  allow_lines<R, 8>();
+  allow_lines<R, 4>();
+  allow_lines<R, 2>();
+  allow_lines<R, 1>();
+  allow_smem(k_fft_x_c2r<R, 8, 4>, k_fft_x_c2r<R, 4, 4>);
 }
 
 }  // namespace
+
+int mesh_check_lengths(const MeshGeom& g, bool mixed) {
+  const size_t cb = mixed ? sizeof(cx<float>) : sizeof(cx<double>);
+  if (pick_lines(g.n[0], cb) == 0 || pick_lines(g.n[1], cb) == 0 ||
+      pick_lines(g.n[2], cb, g.K3) == 0)
+    return EWG_ERR_GRID_TOO_LARGE;
+  return EWG_OK;
+}
 
 int mesh_configure_kernels() {
   allow_all<double>();
