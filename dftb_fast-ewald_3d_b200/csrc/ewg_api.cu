@@ -53,18 +53,20 @@ bool factor_length(int n, FftPlan& plan) {
     rem /= r;
     return true;
   };
+  // Odd radices first: the first pass then writes shared memory without bank
+  // conflicts (see fft_edges).
+  for (int r : {7, 5, 3})
+    while (rem % r == 0)
+      if (!push(r)) return false;
+  for (int r = 11; r <= 31 && rem > 1; r += 2)
+    while (rem % r == 0)
+      if (!push(r)) return false;
   while (rem % 8 == 0)
     if (!push(8)) return false;
   while (rem % 4 == 0)
     if (!push(4)) return false;
   while (rem % 2 == 0)
     if (!push(2)) return false;
-  for (int r : {3, 5, 7})
-    while (rem % r == 0)
-      if (!push(r)) return false;
-  for (int r = 11; r <= 31 && rem > 1; r += 2)
-    while (rem % r == 0)
-      if (!push(r)) return false;
   return rem == 1;
 }
 
@@ -456,7 +458,7 @@ const char* ewg_status_string(int s) {
     case EWG_ERR_OUT_OF_MEMORY: return "ewald_b200: out of device memory";
     case EWG_ERR_CUDA: return "ewald_b200: CUDA error";
     case EWG_ERR_DEVICE_TIMEOUT: return "ewald_b200: device wait timed out";
-    case EWG_ERR_GRID_TOO_LARGE: return "ewald_b200: FFT length not supported (max 4096 and radices <= 31; in FP64 about 2500 on the fused z axis)";
+    case EWG_ERR_GRID_TOO_LARGE: return "ewald_b200: FFT length not supported (max 4096, radices <= 31)";
     case EWG_ERR_NO_DEVICE: return "ewald_b200: no CUDA device";
     case EWG_ERR_STATE: return "ewald_b200: call order (lattice, coords, charges) not satisfied";
     case EWG_ERR_SCRATCH_LIMIT:

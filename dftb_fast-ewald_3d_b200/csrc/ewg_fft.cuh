@@ -1,15 +1,15 @@
 // ewg_fft.cuh -- shared-memory Stockham FFT for the mesh transforms.
 //
-// A CTA transforms `nlines` complex lines of length n held in shared memory,
-// ping-ponging between two buffers.  Each pass of radix r and current
-// sub-length p (Stockham autosort, decimation in time) reads the r inputs
-// spaced n/r apart, multiplies input j by w^(j k) with w = exp(sign 2 pi i/(p r))
-// and k = i mod p, does an r-point DFT and writes output j to
-// (i - k) r + k + j p.  After the last pass the data are in natural order.
-// Twiddles come from one table tw[e] = exp(-2 pi i e / n) per length; the
-// inverse direction conjugates them.  Radices 2, 3, 4, 5, 7, 8 are specialised;
-// other odd primes up to 31 use a generic pass.  No normalisation is applied,
-// matching the reference's FFTW usage (nfft/fft_backend.f90:43-58).
+// A CTA transforms L complex lines of length n, ping-ponging between two
+// shared buffers.  Each pass of radix r and current sub-length p (Stockham
+// autosort, decimation in time) reads the r inputs spaced n/r apart,
+// multiplies input j by w^(j k) with w = exp(sign 2 pi i/(p r)) and k = i mod p,
+// does an r-point DFT and writes output j to (i - k) r + k + j p.  After the
+// last pass the data are in natural order.  Twiddles come from one table
+// tw[e] = exp(-2 pi i e / n) per length; the inverse direction conjugates them.
+// Radices 2, 3, 4, 5, 7, 8 are specialised; other odd primes up to 31 use a
+// generic pass.  No normalisation is applied, matching the reference's FFTW
+// usage (nfft/fft_backend.f90:43-58).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -164,89 +164,6 @@ __device__ __forceinline__ void dft_fixed(cx<R>* u, const cx<R>* __restrict__ tw
   }
 }
 
-// One Stockham pass of a compile-time radix over all lines.
-template <typename R, int SIGN, int RR>
-__device__ __forceinline__ void stockham_pass(const cx<R>* __restrict__ in, cx<R>* __restrict__ out,
-                                              int n, int nlines, int p,
-                                              const cx<R>* __restrict__ tw) {
-  const int nr = n / RR;
-  const int total = nlines * nr;
-  const int step = n / (p * RR);
-  for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    const int l = t / nr;
-    const int i = t - l * nr;
-    const int k = i % p;
-    const cx<R>* src = in + l * n + i;
-    cx<R> u[RR];
-#pragma unroll
-    for (int j = 0; j < RR; ++j) u[j] = src[j * nr];
-    if (p > 1) {
-#pragma unroll
-      for (int j = 1; j < RR; ++j) u[j] = mul(u[j], twiddle(tw, j * k * step, SIGN));
-    }
-    dft_fixed<R, SIGN, RR>(u, tw, n);
-    cx<R>* dst = out + l * n + (i - k) * RR + k;
-#pragma unroll
-    for (int j = 0; j < RR; ++j) dst[j * p] = u[j];
-  }
-}
-
-// Generic odd prime radix (slow path for lengths the reference's overrides
-// can produce but the parameter chain never does).
-template <typename R, int SIGN>
-__device__ void stockham_pass_generic(const cx<R>* __restrict__ in, cx<R>* __restrict__ out, int n,
-                                      int nlines, int p, int rr, const cx<R>* __restrict__ tw) {
-  const int nr = n / rr;
-  const int total = nlines * nr;
-  const int step = n / (p * rr);
-  const int stride_rr = n / rr;
-  for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    const int l = t / nr;
-    const int i = t - l * nr;
-    const int k = i % p;
-    const cx<R>* src = in + l * n + i;
-    cx<R>* dst = out + l * n + (i - k) * rr + k;
-    for (int s = 0; s < rr; ++s) {
-      cx<R> acc = mk(R(0), R(0));
-      for (int j = 0; j < rr; ++j) {
-        cx<R> v = src[j * nr];
-        if (p > 1 && j > 0) v = mul(v, twiddle(tw, j * k * step, SIGN));
-        const int e = ((j * s) % rr) * stride_rr;
-        acc = add(acc, mul(v, twiddle(tw, e, SIGN)));
-      }
-      dst[s * p] = acc;
-    }
-  }
-}
-
-// Full transform of `nlines` lines of length n in shared memory.  `a` holds
-// the input; `b` is scratch of the same size.  Returns the buffer holding the
-// result.  The caller synchronises before the call; the function returns after
-// a barrier.
-template <typename R, int SIGN>
-__device__ cx<R>* fft_lines(cx<R>* a, cx<R>* b, int n, int nlines, const FftPlan& plan,
-                            const cx<R>* __restrict__ tw) {
-  int p = 1;
-  for (int s = 0; s < plan.nstages; ++s) {
-    const int rr = plan.radix[s];
-    switch (rr) {
-      case 2: stockham_pass<R, SIGN, 2>(a, b, n, nlines, p, tw); break;
-      case 3: stockham_pass<R, SIGN, 3>(a, b, n, nlines, p, tw); break;
-      case 4: stockham_pass<R, SIGN, 4>(a, b, n, nlines, p, tw); break;
-      case 5: stockham_pass<R, SIGN, 5>(a, b, n, nlines, p, tw); break;
-      case 7: stockham_pass<R, SIGN, 7>(a, b, n, nlines, p, tw); break;
-      case 8: stockham_pass<R, SIGN, 8>(a, b, n, nlines, p, tw); break;
-      default: stockham_pass_generic<R, SIGN>(a, b, n, nlines, p, rr, tw); break;
-    }
-    __syncthreads();
-    cx<R>* t = a;
-    a = b;
-    b = t;
-    p *= rr;
-  }
-  return a;
-}
-
 template <typename R>
 __device__ __forceinline__ const cx<R>* plan_twiddles(const FftPlan& plan);
 template <>
@@ -263,19 +180,31 @@ __device__ __forceinline__ const cx<float>* plan_twiddles<float>(const FftPlan& 
 namespace ewg {
 
 // ---------------------------------------------------------------------------
-// Line-fastest variant: L lines (a power of two) stored element-major with a
-// padded stride LP = L + 1, element e of line l at buf[e * LP + l].  This is
-// the order in which the strided (y, z) passes find their lines in memory
-// (consecutive k1), so loads and stores are coalesced and the shared-memory
-// accesses of a pass are conflict-free.  Threads map to (line, butterfly) with
-// the line fastest; the Stockham indices j = i / p, k = i mod p advance
-// incrementally, with one division per pass.  blockDim.x must be a multiple of L.
+// Line-fastest transforms with register edges.  A CTA transforms L lines (L a
+// power of two) of length n; element e of line l sits at buf[e * L + l], the
+// order in which the strided mesh axes find their lines in memory (consecutive
+// k1), so global accesses are coalesced across the lines.  Threads map to
+// (line, butterfly) with the line fastest.
+//
+// The first pass takes its inputs straight from a load functor (global memory
+// or another shared buffer) and the last pass hands its outputs to a store
+// functor, so only the passes in between go through the two ping-pong
+// buffers.  With radices ordered odd first (the host factorisation does so),
+// every shared-memory access of a pass is conflict-free for L = 8 and L = 4.
+//
+//   load(line, e)                 -> cx<R>   input element e of line `line`
+//   store(line, e, v, spare)                 output element e; `spare` is a
+//                                            shared buffer of n * L elements
+//                                            that the transform no longer uses
+//
+// The caller synchronises before the call if the buffers (or data the load
+// functor reads from shared memory) were written by other threads; the
+// function ends without a barrier after the last pass.
 // ---------------------------------------------------------------------------
-template <typename R, int SIGN, int RR, int L>
-__device__ __forceinline__ void stockham_pass_cols(const cx<R>* __restrict__ in,
-                                                   cx<R>* __restrict__ out, int n, int p,
-                                                   const cx<R>* __restrict__ tw) {
-  constexpr int LP = L + 1;
+template <typename R, int SIGN, int RR, int L, class Load, class Store>
+__device__ __forceinline__ void edge_pass(const cx<R>* __restrict__ in, cx<R>* __restrict__ out,
+                                          cx<R>* spare, int n, int p, bool first, bool last,
+                                          const cx<R>* __restrict__ tw, Load& load, Store& store) {
   const int nr = n / RR;
   const int step = n / (p * RR);
   const int line = threadIdx.x & (L - 1);
@@ -284,18 +213,29 @@ __device__ __forceinline__ void stockham_pass_cols(const cx<R>* __restrict__ in,
   int j = i / p, k = i - j * p;
   const int dj = istep / p, dk = istep - dj * p;
   for (; i < nr; i += istep) {
-    const cx<R>* src = in + i * LP + line;
     cx<R> u[RR];
+    if (first) {
 #pragma unroll
-    for (int jj = 0; jj < RR; ++jj) u[jj] = src[jj * nr * LP];
-    if (p > 1) {
+      for (int jj = 0; jj < RR; ++jj) u[jj] = load(line, i + jj * nr);
+    } else {
+      const cx<R>* src = in + i * L + line;
 #pragma unroll
-      for (int jj = 1; jj < RR; ++jj) u[jj] = mul(u[jj], twiddle(tw, jj * k * step, SIGN));
+      for (int jj = 0; jj < RR; ++jj) u[jj] = src[jj * nr * L];
+      if (p > 1) {
+#pragma unroll
+        for (int jj = 1; jj < RR; ++jj) u[jj] = mul(u[jj], twiddle(tw, jj * k * step, SIGN));
+      }
     }
     dft_fixed<R, SIGN, RR>(u, tw, n);
-    cx<R>* dst = out + (j * p * RR + k) * LP + line;
+    const int e0 = j * p * RR + k;
+    if (last) {
 #pragma unroll
-    for (int jj = 0; jj < RR; ++jj) dst[jj * p * LP] = u[jj];
+      for (int jj = 0; jj < RR; ++jj) store(line, e0 + jj * p, u[jj], spare);
+    } else {
+      cx<R>* dst = out + e0 * L + line;
+#pragma unroll
+      for (int jj = 0; jj < RR; ++jj) dst[jj * p * L] = u[jj];
+    }
     k += dk;
     j += dj;
     if (k >= p) {
@@ -305,52 +245,61 @@ __device__ __forceinline__ void stockham_pass_cols(const cx<R>* __restrict__ in,
   }
 }
 
-template <typename R, int SIGN, int L>
-__device__ void stockham_pass_cols_generic(const cx<R>* __restrict__ in, cx<R>* __restrict__ out,
-                                           int n, int p, int rr, const cx<R>* __restrict__ tw) {
-  constexpr int LP = L + 1;
+// Generic odd prime radix rr (slow path for lengths that only the reference's
+// overrides can produce).
+template <typename R, int SIGN, int L, class Load, class Store>
+__device__ void edge_pass_generic(const cx<R>* __restrict__ in, cx<R>* __restrict__ out,
+                                  cx<R>* spare, int n, int p, int rr, bool first, bool last,
+                                  const cx<R>* __restrict__ tw, Load& load, Store& store) {
   const int nr = n / rr;
   const int step = n / (p * rr);
-  const int stride_rr = n / rr;
   const int line = threadIdx.x & (L - 1);
   for (int i = threadIdx.x / L; i < nr; i += blockDim.x / L) {
     const int k = i % p, j = i / p;
-    const cx<R>* src = in + i * LP + line;
-    cx<R>* dst = out + (j * p * rr + k) * LP + line;
+    const int e0 = j * p * rr + k;
     for (int s = 0; s < rr; ++s) {
       cx<R> acc = mk(R(0), R(0));
       for (int jj = 0; jj < rr; ++jj) {
-        cx<R> v = src[jj * nr * LP];
-        if (p > 1 && jj > 0) v = mul(v, twiddle(tw, jj * k * step, SIGN));
-        acc = add(acc, mul(v, twiddle(tw, ((jj * s) % rr) * stride_rr, SIGN)));
+        cx<R> v = first ? load(line, i + jj * nr) : in[(i + jj * nr) * L + line];
+        if (!first && p > 1 && jj > 0) v = mul(v, twiddle(tw, jj * k * step, SIGN));
+        acc = add(acc, mul(v, twiddle(tw, ((jj * s) % rr) * nr, SIGN)));
       }
-      dst[s * p * LP] = acc;
+      if (last)
+        store(line, e0 + s * p, acc, spare);
+      else
+        out[(e0 + s * p) * L + line] = acc;
     }
   }
 }
 
-template <typename R, int SIGN, int L>
-__device__ cx<R>* fft_cols(cx<R>* a, cx<R>* b, int n, const FftPlan& plan,
-                           const cx<R>* __restrict__ tw) {
+template <typename R, int SIGN, int L, class Load, class Store>
+__device__ void fft_edges(cx<R>* a, cx<R>* b, int n, const FftPlan& plan,
+                          const cx<R>* __restrict__ tw, Load load, Store store) {
   int p = 1;
-  for (int s = 0; s < plan.nstages; ++s) {
+  cx<R>* src = b;  // unused by the first pass
+  cx<R>* dst = a;
+  const int ns = plan.nstages;
+  for (int s = 0; s < ns; ++s) {
     const int rr = plan.radix[s];
+    const bool first = s == 0, last = s == ns - 1;
+    // Before the last pass, `dst` is the buffer its outputs would have used.
+    cx<R>* spare = dst;
     switch (rr) {
-      case 2: stockham_pass_cols<R, SIGN, 2, L>(a, b, n, p, tw); break;
-      case 3: stockham_pass_cols<R, SIGN, 3, L>(a, b, n, p, tw); break;
-      case 4: stockham_pass_cols<R, SIGN, 4, L>(a, b, n, p, tw); break;
-      case 5: stockham_pass_cols<R, SIGN, 5, L>(a, b, n, p, tw); break;
-      case 7: stockham_pass_cols<R, SIGN, 7, L>(a, b, n, p, tw); break;
-      case 8: stockham_pass_cols<R, SIGN, 8, L>(a, b, n, p, tw); break;
-      default: stockham_pass_cols_generic<R, SIGN, L>(a, b, n, p, rr, tw); break;
+      case 2: edge_pass<R, SIGN, 2, L>(src, dst, spare, n, p, first, last, tw, load, store); break;
+      case 3: edge_pass<R, SIGN, 3, L>(src, dst, spare, n, p, first, last, tw, load, store); break;
+      case 4: edge_pass<R, SIGN, 4, L>(src, dst, spare, n, p, first, last, tw, load, store); break;
+      case 5: edge_pass<R, SIGN, 5, L>(src, dst, spare, n, p, first, last, tw, load, store); break;
+      case 7: edge_pass<R, SIGN, 7, L>(src, dst, spare, n, p, first, last, tw, load, store); break;
+      case 8: edge_pass<R, SIGN, 8, L>(src, dst, spare, n, p, first, last, tw, load, store); break;
+      default:
+        edge_pass_generic<R, SIGN, L>(src, dst, spare, n, p, rr, first, last, tw, load, store);
+        break;
     }
-    __syncthreads();
-    cx<R>* t = a;
-    a = b;
-    b = t;
+    if (!last) __syncthreads();
     p *= rr;
+    src = dst;
+    dst = dst == a ? b : a;
   }
-  return a;
 }
 
 }  // namespace ewg

@@ -162,7 +162,8 @@ MeshSizes mesh_sizes(const MeshGeom& g, const StencilDims& sd, int mixed, int nc
 
 // Shared-memory limits of the FFT and gather kernels (once per device).
 int mesh_configure_kernels();
-// EWG_ERR_GRID_TOO_LARGE when one line of an axis does not fit a pass CTA's shared memory.
+// EWG_ERR_GRID_TOO_LARGE when one line of an axis does not fit a pass CTA's shared
+// memory (a guard: every length up to kMaxFftLength fits in both precisions).
 int mesh_check_lengths(const MeshGeom& g, bool mixed);
 int stencil_configure_kernels();
 

@@ -34,15 +34,17 @@ namespace {
 
 constexpr size_t kSmemBudget = 200 * 1024;
 
-__device__ __forceinline__ int pmod(int a, int n) {
-  int r = a % n;
-  return r < 0 ? r + n : r;
-}
-
-// Every pass stages L lines (a power of two, the fastest index) of length n in
-// shared memory as buf[e * (L + 1) + line]; blockDim.x = pass_threads(L): 32
-// threads per line, at least 128 per CTA.
+// Every pass transforms L lines (a power of two, the fastest index) of length n
+// with fft_edges: two buffers of n * L elements in shared memory, blockDim.x =
+// pass_threads(L): 32 threads per line, at least 128 per CTA.  The first and
+// last radix passes read and write global memory directly.
 constexpr int pass_threads(int L) { return L >= 4 ? 32 * L : 128; }
+
+// The buffer the last pass of `plan` leaves free (its `spare`).
+template <typename R>
+__device__ __forceinline__ cx<R>* spare_buffer(cx<R>* a, cx<R>* b, const FftPlan& plan) {
+  return (plan.nstages & 1) ? a : b;
+}
 
 // ---------------------------------------------------------------------------
 // x pass, real to complex: row pairs (2p, 2p+1) form one complex line; keep
@@ -50,35 +52,30 @@ constexpr int pass_threads(int L) { return L >= 4 ? 32 * L : 128; }
 // ---------------------------------------------------------------------------
 template <typename R, int L>
 __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_r2c(const R* __restrict__ grid,
-                                                      cx<R>* __restrict__ A1, int n1, int npairs,
-                                                      int K1, FftPlan plan) {
-  constexpr int LP = L + 1;
+                                                               cx<R>* __restrict__ A1, int n1,
+                                                               int npairs, int K1, FftPlan plan) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
-  cx<R>* b = a + static_cast<size_t>(n1) * LP;
+  cx<R>* b = a + static_cast<size_t>(n1) * L;
   const cx<R>* tw = plan_twiddles<R>(plan);
   const int pair0 = blockIdx.x * L;
-  for (int x = threadIdx.x; x < n1; x += blockDim.x) {
-#pragma unroll
-    for (int l = 0; l < L; ++l) {
-      const int pr = pair0 + l;
-      cx<R> v = mk(R(0), R(0));
-      if (pr < npairs) {
-        const size_t r0 = static_cast<size_t>(2 * pr) * n1;
-        v = mk(grid[r0 + x], grid[r0 + n1 + x]);
-      }
-      a[x * LP + l] = v;
-    }
-  }
+  auto load = [&](int l, int x) {
+    const int pr = pair0 + l;
+    if (pr >= npairs) return mk(R(0), R(0));
+    const size_t r0 = static_cast<size_t>(2 * pr) * n1;
+    return mk(grid[r0 + x], grid[r0 + n1 + x]);
+  };
+  auto store = [&](int l, int k, cx<R> v, cx<R>* spare) { spare[k * L + l] = v; };
+  fft_edges<R, -1, L>(a, b, n1, plan, tw, load, store);
   __syncthreads();
-  cx<R>* res = fft_cols<R, -1, L>(a, b, n1, plan, tw);
+  const cx<R>* res = spare_buffer(a, b, plan);
   const R h = R(0.5);
   for (int t = threadIdx.x; t < K1 * L; t += blockDim.x) {
     const int l = t % L, k = t / L;  // L is a power of two
     const int pr = pair0 + l;
     if (pr >= npairs) continue;
-    const cx<R> z = res[k * LP + l];
-    cx<R> zc = res[(k == 0 ? 0 : n1 - k) * LP + l];
+    const cx<R> z = res[k * L + l];
+    cx<R> zc = res[(k == 0 ? 0 : n1 - k) * L + l];
     zc.y = -zc.y;
     const size_t row = static_cast<size_t>(2 * pr);
     A1[row * K1 + k] = mk(h * (z.x + zc.x), h * (z.y + zc.y));
@@ -91,25 +88,29 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_r2c(const R* __restri
 // ---------------------------------------------------------------------------
 template <typename R, int L>
 __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_fwd(const cx<R>* __restrict__ A1,
-                                                      cx<R>* __restrict__ A2, int n2, int K1,
-                                                      int K2, int H2, FftPlan plan) {
-  constexpr int LP = L + 1;
+                                                               cx<R>* __restrict__ A2, int n2,
+                                                               int K1, int K2, int H2,
+                                                               FftPlan plan) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
-  cx<R>* b = a + static_cast<size_t>(n2) * LP;
+  cx<R>* b = a + static_cast<size_t>(n2) * L;
   const cx<R>* tw = plan_twiddles<R>(plan);
   const int k0 = blockIdx.x * L;
   const int i3 = blockIdx.y;
-  const int kk = threadIdx.x % L;
-  const bool kin = k0 + kk < K1;
-#pragma unroll 4
-  for (int i2 = threadIdx.x / L; i2 < n2; i2 += blockDim.x / L)
-    a[i2 * LP + kk] = kin ? A1[(static_cast<size_t>(i3) * n2 + i2) * K1 + k0 + kk] : mk(R(0), R(0));
-  __syncthreads();
-  cx<R>* res = fft_cols<R, -1, L>(a, b, n2, plan, tw);
-  if (kin)
-    for (int k2i = threadIdx.x / L; k2i < K2; k2i += blockDim.x / L)
-      A2[(static_cast<size_t>(i3) * K2 + k2i) * K1 + k0 + kk] = res[pmod(k2i - H2, n2) * LP + kk];
+  auto load = [&](int l, int i2) {
+    return k0 + l < K1 ? A1[(static_cast<size_t>(i3) * n2 + i2) * K1 + k0 + l] : mk(R(0), R(0));
+  };
+  auto store = [&](int l, int e, cx<R> v, cx<R>*) {
+    int k2i;
+    if (e <= H2)
+      k2i = e + H2;
+    else if (e >= n2 - H2)
+      k2i = e - n2 + H2;
+    else
+      return;
+    if (k0 + l < K1) A2[(static_cast<size_t>(i3) * K2 + k2i) * K1 + k0 + l] = v;
+  };
+  fft_edges<R, -1, L>(a, b, n2, plan, tw, load, store);
 }
 
 // ---------------------------------------------------------------------------
@@ -125,34 +126,34 @@ struct InfluenceArgs {
 };
 
 template <typename R, int L>
-__global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(const cx<R>* __restrict__ A2,
-                                                            cx<R>* __restrict__ B2, int n3, int K1,
-                                                            int K2, int K3, int nc,
-                                                            InfluenceArgs ia, FftPlan plan) {
-  constexpr int LP = L + 1;
+__global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
+    const cx<R>* __restrict__ A2, cx<R>* __restrict__ B2, int n3, int K1, int K2, int K3, int nc,
+    InfluenceArgs ia, FftPlan plan) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
-  cx<R>* b = a + static_cast<size_t>(n3) * LP;
-  cx<R>* q = b + static_cast<size_t>(n3) * LP;  // K3 weighted modes per line
+  cx<R>* b = a + static_cast<size_t>(n3) * L;
+  cx<R>* q = b + static_cast<size_t>(n3) * L;  // K3 weighted modes per line
   const cx<R>* tw = plan_twiddles<R>(plan);
   const int k0 = blockIdx.x * L;
   const int k2i = blockIdx.y;
-  const int kk = threadIdx.x % L;
-  const int rstep = blockDim.x / L;
-  const bool kin = k0 + kk < K1;
-#pragma unroll 4
-  for (int i3 = threadIdx.x / L; i3 < n3; i3 += rstep)
-    a[i3 * LP + kk] = kin ? A2[(static_cast<size_t>(i3) * K2 + k2i) * K1 + k0 + kk] : mk(R(0), R(0));
-  __syncthreads();
-  cx<R>* res = fft_cols<R, -1, L>(a, b, n3, plan, tw);
   const int h1 = ia.H[0], h2 = ia.H[1], h3 = ia.H[2];
-  const int k1 = k0 + kk;
   const int k2 = k2i - h2;
   const double twoPi = 2.0 * 3.14159265358979323846;
-  for (int k3i = threadIdx.x / L; k3i < K3; k3i += rstep) {
-    const int k3 = k3i - h3;
+  auto load_fwd = [&](int l, int i3) {
+    return k0 + l < K1 ? A2[(static_cast<size_t>(i3) * K2 + k2i) * K1 + k0 + l] : mk(R(0), R(0));
+  };
+  // Weight each mode of the closed box as it leaves the forward transform.
+  auto store_weighted = [&](int l, int e, cx<R> g, cx<R>*) {
+    int k3;
+    if (e <= h3)
+      k3 = e;
+    else if (e >= n3 - h3)
+      k3 = e - n3;
+    else
+      return;
+    const int k1 = k0 + l;
     double wt = 0.0;
-    if (kin && !(k1 == 0 && k2 == 0 && k3 == 0)) {
+    if (k1 < K1 && !(k1 == 0 && k2 == 0 && k3 == 0)) {
       double kv[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c)
@@ -169,10 +170,10 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(const cx<R>
              ia.corr2[1][k2 + h2] * ia.corr2[2][k3 + h3];
       }
     }
-    const cx<R> g = res[pmod(k3, n3) * LP + kk];
-    q[k3i * LP + kk] = mk(static_cast<R>(wt * static_cast<double>(g.x)),
-                          static_cast<R>(wt * static_cast<double>(g.y)));
-  }
+    q[(k3 + h3) * L + l] = mk(static_cast<R>(wt * static_cast<double>(g.x)),
+                              static_cast<R>(wt * static_cast<double>(g.y)));
+  };
+  fft_edges<R, -1, L>(a, b, n3, plan, tw, load_fwd, store_weighted);
   __syncthreads();
   for (int c = 0; c < nc; ++c) {
     R kc1 = R(0), kc2 = R(0), kc3 = R(0);
@@ -181,31 +182,27 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(const cx<R>
       kc2 = static_cast<R>(twoPi * ia.rec[1][c - 1]);
       kc3 = static_cast<R>(twoPi * ia.rec[2][c - 1]);
     }
-    for (int i3 = threadIdx.x / L; i3 < n3; i3 += rstep) {
-      int k3 = 0;
-      bool inside = true;
+    auto load_inv = [&](int l, int i3) {
+      int k3;
       if (i3 <= h3)
         k3 = i3;
       else if (i3 >= n3 - h3)
         k3 = i3 - n3;
       else
-        inside = false;
-      cx<R> v = mk(R(0), R(0));
-      if (inside) {
-        v = q[(k3 + h3) * LP + kk];
-        if (c > 0) {
-          const R kc = static_cast<R>(k1) * kc1 + static_cast<R>(k2) * kc2 + static_cast<R>(k3) * kc3;
-          v = mk(kc * v.y, -kc * v.x);  // -i kc v
-        }
+        return mk(R(0), R(0));
+      cx<R> v = q[(k3 + h3) * L + l];
+      if (c > 0) {
+        const R kc = static_cast<R>(k0 + l) * kc1 + static_cast<R>(k2) * kc2 +
+                     static_cast<R>(k3) * kc3;
+        v = mk(kc * v.y, -kc * v.x);  // -i kc v
       }
-      a[i3 * LP + kk] = v;
-    }
-    __syncthreads();
-    cx<R>* r2 = fft_cols<R, 1, L>(a, b, n3, plan, tw);
+      return v;
+    };
     cx<R>* dst = B2 + static_cast<size_t>(c) * n3 * K2 * K1;
-    if (kin)
-      for (int i3 = threadIdx.x / L; i3 < n3; i3 += rstep)
-        dst[(static_cast<size_t>(i3) * K2 + k2i) * K1 + k0 + kk] = r2[i3 * LP + kk];
+    auto store = [&](int l, int i3, cx<R> v, cx<R>*) {
+      if (k0 + l < K1) dst[(static_cast<size_t>(i3) * K2 + k2i) * K1 + k0 + l] = v;
+    };
+    fft_edges<R, 1, L>(a, b, n3, plan, tw, load_inv, store);
     __syncthreads();
   }
 }
@@ -215,109 +212,83 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(const cx<R>
 // ---------------------------------------------------------------------------
 template <typename R, int L>
 __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_inv(const cx<R>* __restrict__ B2,
-                                                      cx<R>* __restrict__ B1, int n2, int n3,
-                                                      int K1, int K2, int H2, FftPlan plan) {
-  constexpr int LP = L + 1;
+                                                               cx<R>* __restrict__ B1, int n2,
+                                                               int n3, int K1, int K2, int H2,
+                                                               FftPlan plan) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
-  cx<R>* b = a + static_cast<size_t>(n2) * LP;
+  cx<R>* b = a + static_cast<size_t>(n2) * L;
   const cx<R>* tw = plan_twiddles<R>(plan);
   const int k0 = blockIdx.x * L;
   const int i3 = blockIdx.y;
   const int c = blockIdx.z;
-  const int kk = threadIdx.x % L;
-  const bool kin = k0 + kk < K1;
   const cx<R>* src = B2 + static_cast<size_t>(c) * n3 * K2 * K1;
-#pragma unroll 4
-  for (int i2 = threadIdx.x / L; i2 < n2; i2 += blockDim.x / L) {
-    int k2 = 0;
-    bool inside = kin;
+  cx<R>* dst = B1 + static_cast<size_t>(c) * n3 * n2 * K1;
+  auto load = [&](int l, int i2) {
+    int k2;
     if (i2 <= H2)
       k2 = i2;
     else if (i2 >= n2 - H2)
       k2 = i2 - n2;
     else
-      inside = false;
-    a[i2 * LP + kk] =
-        inside ? src[(static_cast<size_t>(i3) * K2 + k2 + H2) * K1 + k0 + kk] : mk(R(0), R(0));
-  }
-  __syncthreads();
-  cx<R>* res = fft_cols<R, 1, L>(a, b, n2, plan, tw);
-  cx<R>* dst = B1 + static_cast<size_t>(c) * n3 * n2 * K1;
-  if (kin)
-    for (int i2 = threadIdx.x / L; i2 < n2; i2 += blockDim.x / L)
-      dst[(static_cast<size_t>(i3) * n2 + i2) * K1 + k0 + kk] = res[i2 * LP + kk];
+      return mk(R(0), R(0));
+    return k0 + l < K1 ? src[(static_cast<size_t>(i3) * K2 + k2 + H2) * K1 + k0 + l]
+                       : mk(R(0), R(0));
+  };
+  auto store = [&](int l, int i2, cx<R> v, cx<R>*) {
+    if (k0 + l < K1) dst[(static_cast<size_t>(i3) * n2 + i2) * K1 + k0 + l] = v;
+  };
+  fft_edges<R, 1, L>(a, b, n2, plan, tw, load, store);
 }
 
 // ---------------------------------------------------------------------------
-// x pass, complex to real.  Lines are (component, row pair): line = cc * NP + l
-// with NP = L / NCG pairs and NCG components per CTA; output interleaved with
-// nc components per grid point.
+// x pass, complex to real.  Lines are (row pair, component) with the component
+// fastest: line = l * NCG + cc, NP = L / NCG pairs and NCG components per CTA,
+// so neighbouring threads write the components of one grid point; output
+// interleaved with nc components per grid point.
 // ---------------------------------------------------------------------------
 template <typename R, int L, int NCG>
 __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_c2r(const cx<R>* __restrict__ B1,
-                                                      R* __restrict__ out, int n1, int nrows,
-                                                      int K1, int nc, FftPlan plan) {
-  constexpr int LP = L + 1;
+                                                               R* __restrict__ out, int n1,
+                                                               int nrows, int K1, int nc,
+                                                               FftPlan plan) {
   constexpr int NP = L / NCG;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
-  cx<R>* b = a + static_cast<size_t>(n1) * LP;
+  cx<R>* b = a + static_cast<size_t>(n1) * L;
   const cx<R>* tw = plan_twiddles<R>(plan);
   const int pair0 = blockIdx.x * NP;
   const int c0 = blockIdx.y * NCG;
   const int npairs = nrows / 2;
-  for (int x = threadIdx.x; x < n1; x += blockDim.x) {
+  auto load = [&](int line, int x) {
+    const int cc = line % NCG, pr = pair0 + line / NCG;
     const bool lo = x < K1;
     const bool hi = x > n1 - K1;
-    const int kx = lo ? x : n1 - x;
-#pragma unroll
-    for (int line = 0; line < L; ++line) {
-      const int cc = line / NP, l = line % NP;
-      const int pr = pair0 + l;
-      cx<R> fa = mk(R(0), R(0)), fb = mk(R(0), R(0));
-      if (pr < npairs && (lo || hi)) {
-        const cx<R>* src = B1 + static_cast<size_t>(c0 + cc) * nrows * K1;
-        const size_t ra = static_cast<size_t>(2 * pr);
-        fa = src[ra * K1 + kx];
-        fb = src[(ra + 1) * K1 + kx];
-        if (x == 0) {
-          fa.y = R(0);
-          fb.y = R(0);
-        } else if (hi) {
-          fa.y = -fa.y;
-          fb.y = -fb.y;
-        }
-      }
-      a[x * LP + line] = mk(fa.x - fb.y, fa.y + fb.x);
-    }
-  }
-  __syncthreads();
-  cx<R>* res = fft_cols<R, 1, L>(a, b, n1, plan, tw);
-  for (int x = threadIdx.x; x < n1; x += blockDim.x) {
-#pragma unroll
-    for (int l = 0; l < NP; ++l) {
-      const int pr = pair0 + l;
-      if (pr >= npairs) continue;
+    cx<R> fa = mk(R(0), R(0)), fb = mk(R(0), R(0));
+    if (pr < npairs && (lo || hi)) {
+      const int kx = lo ? x : n1 - x;
+      const cx<R>* src = B1 + static_cast<size_t>(c0 + cc) * nrows * K1;
       const size_t ra = static_cast<size_t>(2 * pr);
-      R* oa = out + (ra * n1 + x) * nc + c0;
-      R* ob = out + ((ra + 1) * n1 + x) * nc + c0;
-      if constexpr (NCG == 4) {
-        using V = typename std::conditional<sizeof(R) == 8, double4, float4>::type;
-        const cx<R> z0 = res[x * LP + 0 * NP + l], z1 = res[x * LP + 1 * NP + l],
-                    z2 = res[x * LP + 2 * NP + l], z3 = res[x * LP + 3 * NP + l];
-        *reinterpret_cast<V*>(oa) = V{z0.x, z1.x, z2.x, z3.x};
-        *reinterpret_cast<V*>(ob) = V{z0.y, z1.y, z2.y, z3.y};
-      } else {
-#pragma unroll
-        for (int cc = 0; cc < NCG; ++cc) {
-          const cx<R> z = res[x * LP + cc * NP + l];
-          oa[cc] = z.x;
-          ob[cc] = z.y;
-        }
+      fa = src[ra * K1 + kx];
+      fb = src[(ra + 1) * K1 + kx];
+      if (x == 0) {
+        fa.y = R(0);
+        fb.y = R(0);
+      } else if (hi) {
+        fa.y = -fa.y;
+        fb.y = -fb.y;
       }
     }
-  }
+    return mk(fa.x - fb.y, fa.y + fb.x);
+  };
+  auto store = [&](int line, int x, cx<R> v, cx<R>*) {
+    const int cc = line % NCG, pr = pair0 + line / NCG;
+    if (pr >= npairs) return;
+    const size_t ra = static_cast<size_t>(2 * pr);
+    out[(ra * n1 + x) * nc + c0 + cc] = v.x;
+    out[((ra + 1) * n1 + x) * nc + c0 + cc] = v.y;
+  };
+  fft_edges<R, 1, L>(a, b, n1, plan, tw, load, store);
 }
 
 template <typename R>
@@ -328,7 +299,7 @@ size_t cbytes() {
 // Shared bytes of one pass CTA: two ping-pong buffers of L lines plus `extra`
 // elements per line.
 size_t pass_smem(int n, int L, size_t cb, int extra) {
-  return (2 * static_cast<size_t>(n) + extra) * (L + 1) * cb;
+  return (2 * static_cast<size_t>(n) + extra) * L * cb;
 }
 
 // Lines per CTA: 8 when that fits in 64 KB (several CTAs per SM), else the

@@ -18,10 +18,10 @@
 // Spread: a CTA owns a tile; each thread owns an x-pencil of 8 points in
 // registers and adds q w1 w2 w3 atom by atom in list order, then writes it
 // once (no atomics, no zeroing, fixed order).
-// Gather: a CTA stages its tile in shared memory; each warp takes 32 atoms of
-// the tile's list, one per lane, and walks the tile's 512 points in lockstep so
-// every grid value is a shared-memory broadcast; rows none of the warp's atoms
-// reach are skipped.  Each lane writes its atom's partial to the atom's slot for
+// Gather: a one-warp CTA stages its tile in shared memory and takes the tile's
+// list 64 atoms at a time, two per lane; the warp walks the tile's 512 points in
+// lockstep so every grid value is a shared-memory broadcast, and skips the rows
+// none of its atoms reach.  Each lane writes its atom's partial to the atom's slot for
 // this tile; a final kernel sums each atom's slots in a fixed order.  Results
 // are bitwise reproducible.
 

@@ -49,8 +49,7 @@ enum {
   EWG_ERR_OUT_OF_MEMORY = 11,
   EWG_ERR_CUDA = 12,
   EWG_ERR_DEVICE_TIMEOUT = 13,
-  EWG_ERR_GRID_TOO_LARGE = 14, /* an FFT length beyond the kernels' limit: 4096 per axis,
-                                  about 2500 on the z axis in FP64 (one line per CTA)      */
+  EWG_ERR_GRID_TOO_LARGE = 14, /* an FFT length beyond the kernels' limit (4096 per axis)  */
   EWG_ERR_NO_DEVICE = 15,
   EWG_ERR_STATE = 16,       /* call order: dftb/coulomb.F90 @:ASSERT(coordsUpdated_) etc. */
   EWG_ERR_SCRATCH_LIMIT = 17 /* configuration too large for the fixed scratch of

@@ -69,13 +69,13 @@ def elongated_cell(dims_angstrom, n=64, seed=5):
     return pos, q - q.mean(), lat
 
 
-# Cells with one long axis and a 20 Angstrom cutoff give FFT lines of 1344-2688
+# Cells with one long axis and a 20 Angstrom cutoff give FFT lines of 1680-3360
 # points: in FP64 their passes hold 2 or 1 lines per CTA instead of 4 or 8.
 LONG_AXIS_CASES = [
-    ("x2688", (2400.0, 8.0, 8.0)),   # x passes, one line per CTA
+    ("x3360", (3000.0, 8.0, 8.0)),   # x passes, one line per CTA
     ("x2000", (1800.0, 8.0, 8.0)),   # x passes, two lines
-    ("y1344", (8.0, 1200.0, 8.0)),   # y passes, two lines
-    ("z2240", (8.0, 8.0, 2000.0)),   # fused z pass, one line
+    ("y2000", (8.0, 1800.0, 8.0)),   # y passes, two lines
+    ("z2688", (8.0, 8.0, 2400.0)),   # fused z pass, one line
     ("z1680", (8.0, 8.0, 1500.0)),   # fused z pass, two lines
 ]
 
@@ -88,20 +88,6 @@ def test_long_axes_match_oracle(ctx, ctx_mixed, oracle, dims):
     pg, fg = ctx.potential_force(pos, q, lat, 1e-10, r_cut_in=r_cut)
     assert rel_max(pg, po) < TOL_FP64, rel_max(pg, po)
     assert rel_max(fg, fo) < TOL_FP64, rel_max(fg, fo)
-    pm, fm = ctx_mixed.potential_force(pos, q, lat, 1e-10, r_cut_in=r_cut)
-    assert rel_rms(fm, fo) < TOL_MIXED_RMS
-    assert rel_rms(pm, po) < TOL_MIXED_RMS
-
-
-def test_z_line_beyond_fp64_shared_memory(ctx, ctx_mixed, ewald_lib, oracle):
-    """A 2688-point z line does not fit one FP64 pass CTA: the FP64 form refuses it
-    with EWG_ERR_GRID_TOO_LARGE, the mixed form (half the bytes) computes it."""
-    pos, q, lat = elongated_cell((8.0, 8.0, 2400.0))
-    r_cut = 20.0 * W.ANGSTROM_TO_BOHR
-    with pytest.raises(ewald_lib.EwaldError) as ei:
-        ctx.potential_force(pos, q, lat, 1e-10, r_cut_in=r_cut)
-    assert ei.value.code == 14
-    po, fo = oracle.fft_potential_force(pos, q, lat, 1e-10, r_cut=r_cut)
     pm, fm = ctx_mixed.potential_force(pos, q, lat, 1e-10, r_cut_in=r_cut)
     assert rel_rms(fm, fo) < TOL_MIXED_RMS
     assert rel_rms(pm, po) < TOL_MIXED_RMS
