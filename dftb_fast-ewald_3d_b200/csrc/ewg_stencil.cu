@@ -18,10 +18,10 @@
 // Spread: a CTA owns a tile; each thread owns an x-pencil of 8 points in
 // registers and adds q w1 w2 w3 atom by atom in list order, then writes it
 // once (no atomics, no zeroing, fixed order).
-// Gather: a one-warp CTA stages its tile in shared memory and takes the tile's
-// list 64 atoms at a time, two per lane; the warp walks the tile's 512 points in
-// lockstep so every grid value is a shared-memory broadcast, and skips the rows
-// none of its atoms reach.  Each lane writes its atom's partial to the atom's slot for
+// Gather: a CTA of one (FP64) or two (FP32) warps stages its tile in shared
+// memory; each warp takes 64 atoms of the tile's list at a time, two per lane,
+// and walks the tile's 512 points in lockstep so every grid value is a
+// shared-memory broadcast, skipping the rows none of its atoms reach.  Each lane writes its atom's partial to the atom's slot for
 // this tile; a final kernel sums each atom's slots in a fixed order.  Results
 // are bitwise reproducible.
 
@@ -38,6 +38,12 @@ namespace {
 constexpr int TX = kTileX, TY = kTileY, TZ = kTileZ;
 constexpr int kPencils = TY * TZ;  // spread: one thread per x-pencil
 constexpr int kSpreadChunk = 64;   // atoms whose weights are staged at once
+// Gather: atoms per lane and warps sharing one staged tile, per precision.
+template <typename R>
+struct GatherShape {
+  static constexpr int atoms = 2;
+  static constexpr int warps = sizeof(R) == 8 ? 1 : 2;
+};
 
 __device__ __forceinline__ int pmod(int a, int n) {
   int r = a % n;
@@ -234,15 +240,17 @@ __global__ void __launch_bounds__(kPencils) k_spread_tiles(const int* __restrict
 // every grid value read from shared memory (a broadcast: all lanes read the
 // same point) feeds A atoms.
 // ---------------------------------------------------------------------------
-template <typename R, int NC, int A>
-__global__ void __launch_bounds__(32) k_gather_tiles(const int* __restrict__ tile_start,
-                                                     const int2* __restrict__ pairs,
-                                                     const R* __restrict__ wtab, StencilDims sd,
-                                                     const R* __restrict__ grid,
-                                                     double* __restrict__ part) {
+template <typename R, int NC, int A, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) k_gather_tiles(const int* __restrict__ tile_start,
+                                                             const int2* __restrict__ pairs,
+                                                             const R* __restrict__ wtab,
+                                                             StencilDims sd,
+                                                             const R* __restrict__ grid,
+                                                             double* __restrict__ part) {
   using V = typename std::conditional<
       NC == 4, typename std::conditional<sizeof(R) == 8, double4, float4>::type, R>::type;
   __shared__ V sG[TZ * TY * TX];
+  __shared__ R sW3[WARPS][TZ][32 * A];  // z weights, lane fastest
   const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
   const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
   const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
@@ -250,7 +258,7 @@ __global__ void __launch_bounds__(32) k_gather_tiles(const int* __restrict__ til
   const int p0 = tile_start[tile], p1 = tile_start[tile + 1];
   if (p0 == p1) return;  // no atom reaches this tile
 #pragma unroll 4
-  for (int t = threadIdx.x; t < TX * TY * TZ; t += 32) {
+  for (int t = threadIdx.x; t < TX * TY * TZ; t += 32 * WARPS) {
     const int x = t % TX, y = (t / TX) % TY, z = t / (TX * TY);
     V v;
     if (x < ex && y < ey && z < ez) {
@@ -264,12 +272,11 @@ __global__ void __launch_bounds__(32) k_gather_tiles(const int* __restrict__ til
     }
     sG[t] = v;
   }
-  __syncwarp();
-  const int lane = threadIdx.x;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nslots = sd.S[0] * sd.S[1] * sd.S[2];
-  for (int a0 = p0; a0 < p1; a0 += 32 * A) {
+  for (int a0 = p0 + warp * 32 * A; a0 < p1; a0 += WARPS * 32 * A) {
     R w1[A][TX], w2[A][TY];
-    const R* wz[A];
     int2 pr[A];
     bool act[A];
 #pragma unroll
@@ -283,8 +290,11 @@ __global__ void __launch_bounds__(32) k_gather_tiles(const int* __restrict__ til
 #pragma unroll
       for (int y = 0; y < TY; ++y)
         w2[a][y] = act[a] ? wk[sd.woff[1] + ((pr[a].y >> 8) & 0xff) * TY + y] : R(0);
-      wz[a] = wk + sd.woff[2] + (pr[a].y >> 16) * TZ;
+      const R* wz = wk + sd.woff[2] + (pr[a].y >> 16) * TZ;
+#pragma unroll
+      for (int z = 0; z < TZ; ++z) sW3[warp][z][a * 32 + lane] = act[a] ? wz[z] : R(0);
     }
+    __syncwarp();
     double acc[A][NC];
 #pragma unroll
     for (int a = 0; a < A; ++a)
@@ -294,7 +304,7 @@ __global__ void __launch_bounds__(32) k_gather_tiles(const int* __restrict__ til
     for (int z = 0; z < TZ; ++z) {
       R w3[A];
 #pragma unroll
-      for (int a = 0; a < A; ++a) w3[a] = act[a] ? wz[a][z] : R(0);
+      for (int a = 0; a < A; ++a) w3[a] = sW3[warp][z][a * 32 + lane];
 #pragma unroll
       for (int y = 0; y < TY; ++y) {
         R w23[A];
@@ -341,6 +351,7 @@ __global__ void __launch_bounds__(32) k_gather_tiles(const int* __restrict__ til
 #pragma unroll
       for (int c = 0; c < NC; ++c) dst[c] = acc[a][c];
     }
+    __syncwarp();  // sW3 is rewritten by the next iteration
   }
 }
 
@@ -431,9 +442,10 @@ void launch_spread(const MeshPlan& mp, const int* tile_start, const int2* pairs,
 void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs, const void* wtab,
                    const void* grid, int nc, double* part, cudaStream_t st) {
   dim3 grd(mp.sd.ntiles[0], mp.sd.ntiles[1], mp.sd.ntiles[2]);
-#define EWG_GATHER(R, NC)                                                                 \
-  k_gather_tiles<R, NC, 2><<<grd, 32, 0, st>>>(tile_start, pairs, static_cast<const R*>(wtab), \
-                                               mp.sd, static_cast<const R*>(grid), part)
+#define EWG_GATHER(R, NC)                                                               \
+  k_gather_tiles<R, NC, GatherShape<R>::atoms, GatherShape<R>::warps>                      \
+      <<<grd, 32 * GatherShape<R>::warps, 0, st>>>(tile_start, pairs, static_cast<const R*>(wtab), \
+                                                   mp.sd, static_cast<const R*>(grid), part)
   if (mp.mixed) {
     if (nc == 4)
       EWG_GATHER(float, 4);
