@@ -220,14 +220,59 @@ __global__ void __launch_bounds__(256) k_sum_partials(const double* __restrict__
 }
 
 // ---------------------------------------------------------------------------
-// Real-space pair sums.  One warp per (box-sorted) atom i; lanes stride over the
-// candidates of each contiguous run of neighbour boxes.
+// Real-space pair sums.  One warp per (box-sorted) atom i; lanes take the
+// candidates of each contiguous run of neighbour boxes 32 at a time.  Only
+// about one candidate in eight lies inside the cutoff, so the candidates that
+// pass the distance test are first compacted into a per-warp queue in shared
+// memory; the warp evaluates the pair term (erfc, exp) 32 queued pairs at a
+// time with every lane busy.  The queue order, and so the summation order, is
+// fixed by the candidate order: results are bitwise reproducible.
 // ---------------------------------------------------------------------------
+constexpr int kRealThreads = 256;
+constexpr int kQueue = 64;  // per-warp queue: up to 31 carried over + 32 new
+
 template <class Pair>
+struct PairQueue {
+  double4* q;  // this warp's kQueue entries: separation (x, y, z), q_j
+  Pair& pair;
+  double cut2;
+  int count = 0;
+
+  __device__ __forceinline__ PairQueue(double4* qbuf, Pair& p, double c2)
+      : q(qbuf), pair(p), cut2(c2) {}
+
+  // One candidate per lane (valid = false for lanes past the run's end).
+  __device__ __forceinline__ void operator()(const double* sep, double qj, bool valid) {
+    const int lane = threadIdx.x & 31;
+    const double r2 = sep[0] * sep[0] + sep[1] * sep[1] + sep[2] * sep[2];
+    if (valid && r2 < 1.0e-24) pair.bad = 1;  // coincident charges
+    const bool take = valid && r2 >= 1.0e-24 && r2 <= cut2;
+    const unsigned m = __ballot_sync(0xffffffffu, take);
+    if (take) q[count + __popc(m & ((1u << lane) - 1u))] = make_double4(sep[0], sep[1], sep[2], qj);
+    count += __popc(m);
+    if (count >= 32) {
+      __syncwarp();
+      pair.eval(q[lane]);
+      __syncwarp();
+      if (lane < count - 32) q[lane] = q[lane + 32];
+      count -= 32;
+      __syncwarp();
+    }
+  }
+
+  __device__ __forceinline__ void flush() {
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    if (lane < count) pair.eval(q[lane]);
+    count = 0;
+  }
+};
+
+template <class Visit>
 __device__ __forceinline__ void for_each_candidate(const double4* __restrict__ srt,
                                                    const int* __restrict__ box_start, int k,
                                                    const double4& ai, const RealGeom& g,
-                                                   Pair& pair) {
+                                                   Visit& visit) {
   const int lane = threadIdx.x & 31;
   int b[3];
   const double sv[3] = {ai.x, ai.y, ai.z};
@@ -250,14 +295,20 @@ __device__ __forceinline__ void for_each_candidate(const double4* __restrict__ s
         const int first = (wz * g.nb[1] + wy) * g.nb[0] + wx;
         const int j0 = box_start[first], j1 = box_start[first + len];
         const bool home_image = (sx == 0 && sy == 0 && sz == 0);
-        for (int j = j0 + lane; j < j1; j += 32) {
-          if (home_image && j == k) continue;
-          const double4 aj = srt[j];
-          const double d1 = (ai.x - aj.x) - sx, d2 = (ai.y - aj.y) - sy, d3 = (ai.z - aj.z) - sz;
-          double sep[3];
+        for (int jb = j0; jb < j1; jb += 32) {
+          const int j = jb + lane;
+          const bool valid = j < j1 && !(home_image && j == k);
+          double sep[3] = {0.0, 0.0, 0.0};
+          double qj = 0.0;
+          if (valid) {
+            const double4 aj = srt[j];
+            const double d1 = (ai.x - aj.x) - sx, d2 = (ai.y - aj.y) - sy, d3 = (ai.z - aj.z) - sz;
 #pragma unroll
-          for (int c = 0; c < 3; ++c) sep[c] = d1 * g.lat[0][c] + d2 * g.lat[1][c] + d3 * g.lat[2][c];
-          pair(sep, aj.w);
+            for (int c = 0; c < 3; ++c)
+              sep[c] = d1 * g.lat[0][c] + d2 * g.lat[1][c] + d3 * g.lat[2][c];
+            qj = aj.w;
+          }
+          visit(sep, qj, valid);
         }
         dx += len;
       }
@@ -265,27 +316,24 @@ __device__ __forceinline__ void for_each_candidate(const double4* __restrict__ s
   }
 }
 
-// Pair term of fft/ewald_fft_3d_real.f90:153-172 (FP64), or its FP32 form.
+// Pair term of fft/ewald_fft_3d_real.f90:153-172 (FP64), or its FP32 form, for
+// a separation inside the cutoff.
 template <bool MIXED>
 struct EwaldPair {
-  double alpha, cut2, qi;
+  double alpha, qi;
   double pot = 0.0, f[3] = {0.0, 0.0, 0.0};
   int bad = 0;
-  __device__ __forceinline__ void operator()(const double* sep, double qj) {
-    const double r2 = sep[0] * sep[0] + sep[1] * sep[1] + sep[2] * sep[2];
-    if (r2 < 1.0e-24) {
-      bad = 1;
-      return;
-    }
-    if (r2 > cut2) return;
+  __device__ __forceinline__ void eval(const double4& e) {
+    const double r2 = e.x * e.x + e.y * e.y + e.z * e.z;
+    const double qj = e.w;
     if constexpr (!MIXED) {
       const double r = sqrt(r2);
       const double ec = erfc(alpha * r);
       pot += qj * ec / r;
       const double ff = qi * qj * (2.0 * alpha / kSqrtPi * exp(-alpha * alpha * r2) + ec / r) / r2;
-      f[0] += ff * sep[0];
-      f[1] += ff * sep[1];
-      f[2] += ff * sep[2];
+      f[0] += ff * e.x;
+      f[1] += ff * e.y;
+      f[2] += ff * e.z;
     } else {
       const float r2f = static_cast<float>(r2);
       const float af = static_cast<float>(alpha);
@@ -298,30 +346,32 @@ struct EwaldPair {
       const float ff = static_cast<float>(qi) * qjf *
                        (2.0f * af * 0.56418958354775628695f * expf(-af * af * r2f) + ec * rinv) *
                        (rinv * rinv);
-      f[0] += static_cast<double>(ff * static_cast<float>(sep[0]));
-      f[1] += static_cast<double>(ff * static_cast<float>(sep[1]));
-      f[2] += static_cast<double>(ff * static_cast<float>(sep[2]));
+      f[0] += static_cast<double>(ff * static_cast<float>(e.x));
+      f[1] += static_cast<double>(ff * static_cast<float>(e.y));
+      f[2] += static_cast<double>(ff * static_cast<float>(e.z));
     }
   }
 };
 
 template <bool MIXED>
-__global__ void __launch_bounds__(256) k_real_space(const double4* __restrict__ srt,
-                                                    const int* __restrict__ perm,
-                                                    const int* __restrict__ box_start, int n,
-                                                    RealGeom g, double alpha, double cut2,
-                                                    double* __restrict__ pot,
-                                                    double* __restrict__ force,
-                                                    int* __restrict__ err) {
+__global__ void __launch_bounds__(kRealThreads) k_real_space(const double4* __restrict__ srt,
+                                                             const int* __restrict__ perm,
+                                                             const int* __restrict__ box_start,
+                                                             int n, RealGeom g, double alpha,
+                                                             double cut2, double* __restrict__ pot,
+                                                             double* __restrict__ force,
+                                                             int* __restrict__ err) {
+  __shared__ double4 queue[kRealThreads / 32][kQueue];
   const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (k >= n) return;
   const double4 ai = srt[k];
   EwaldPair<MIXED> pair;
   pair.alpha = alpha;
-  pair.cut2 = cut2;
   pair.qi = ai.w;
-  for_each_candidate(srt, box_start, k, ai, g, pair);
+  PairQueue<EwaldPair<MIXED>> pq(queue[threadIdx.x >> 5], pair, cut2);
+  for_each_candidate(srt, box_start, k, ai, g, pq);
+  pq.flush();
   double v[4] = {pair.pot, pair.f[0], pair.f[1], pair.f[2]};
 #pragma unroll
   for (int j = 0; j < 4; ++j) v[j] = warp_sum(v[j]);
@@ -341,43 +391,41 @@ __global__ void __launch_bounds__(256) k_real_space(const double4* __restrict__ 
 // list's pairs each appear twice), r (x) f + f (x) r with f = derivRTerm(r) q_i q_j
 // collapses to derivRTerm-scalar * q_i q_j * r (x) r.
 struct StressPair {
-  double alpha, cut2, qi;
+  double alpha, qi;
   double s[6] = {0, 0, 0, 0, 0, 0};  // xx, yy, zz, xy, xz, yz
   int bad = 0;
-  __device__ __forceinline__ void operator()(const double* r, double qj) {
-    const double d2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
-    if (d2 > cut2) return;
-    if (d2 < 1.0e-24) {
-      bad = 1;
-      return;
-    }
+  __device__ __forceinline__ void eval(const double4& e) {
+    const double d2 = e.x * e.x + e.y * e.y + e.z * e.z;
     const double rr = sqrt(d2);
     const double fac = alpha * rr;
     const double dr = (-2.0 / kSqrtPi * exp(-fac * fac) * fac - erfc(fac)) / (rr * rr * rr);
-    const double w = dr * qi * qj;
-    s[0] += w * r[0] * r[0];
-    s[1] += w * r[1] * r[1];
-    s[2] += w * r[2] * r[2];
-    s[3] += w * r[0] * r[1];
-    s[4] += w * r[0] * r[2];
-    s[5] += w * r[1] * r[2];
+    const double w = dr * qi * e.w;
+    s[0] += w * e.x * e.x;
+    s[1] += w * e.y * e.y;
+    s[2] += w * e.z * e.z;
+    s[3] += w * e.x * e.y;
+    s[4] += w * e.x * e.z;
+    s[5] += w * e.y * e.z;
   }
 };
 
-__global__ void __launch_bounds__(256) k_real_stress(const double4* __restrict__ srt,
-                                                     const int* __restrict__ box_start, int n,
-                                                     RealGeom g, double alpha, double cut2,
-                                                     double* __restrict__ partial6,
-                                                     int* __restrict__ err) {
+__global__ void __launch_bounds__(kRealThreads) k_real_stress(const double4* __restrict__ srt,
+                                                              const int* __restrict__ box_start,
+                                                              int n, RealGeom g, double alpha,
+                                                              double cut2,
+                                                              double* __restrict__ partial6,
+                                                              int* __restrict__ err) {
+  __shared__ double4 queue[kRealThreads / 32][kQueue];
   const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (k >= n) return;
   const double4 ai = srt[k];
   StressPair pair;
   pair.alpha = alpha;
-  pair.cut2 = cut2;
   pair.qi = ai.w;
-  for_each_candidate(srt, box_start, k, ai, g, pair);
+  PairQueue<StressPair> pq(queue[threadIdx.x >> 5], pair, cut2);
+  for_each_candidate(srt, box_start, k, ai, g, pq);
+  pq.flush();
 #pragma unroll
   for (int j = 0; j < 6; ++j) pair.s[j] = warp_sum(pair.s[j]);
   const int bad = __any_sync(0xffffffffu, pair.bad);
@@ -534,13 +582,13 @@ void launch_real_space(const double4* srt, const int* perm, const int* box_start
                        const RealGeom& g, double alpha, double r_cut, int mixed, double* pot,
                        double* force, int* err, cudaStream_t st) {
   if (n == 0) return;
-  const int blocks = blocks_for(static_cast<long>(n) * 32, 256);
+  const int blocks = blocks_for(static_cast<long>(n) * 32, kRealThreads);
   if (mixed)
-    k_real_space<true><<<blocks, 256, 0, st>>>(srt, perm, box_start, n, g, alpha, r_cut * r_cut,
-                                               pot, force, err);
+    k_real_space<true><<<blocks, kRealThreads, 0, st>>>(srt, perm, box_start, n, g, alpha,
+                                                        r_cut * r_cut, pot, force, err);
   else
-    k_real_space<false><<<blocks, 256, 0, st>>>(srt, perm, box_start, n, g, alpha, r_cut * r_cut,
-                                                pot, force, err);
+    k_real_space<false><<<blocks, kRealThreads, 0, st>>>(srt, perm, box_start, n, g, alpha,
+                                                         r_cut * r_cut, pot, force, err);
   ++g_launches;
 }
 
@@ -548,7 +596,7 @@ void launch_real_stress(const double4* srt, const int* box_start, int n, const R
                         double alpha, double max_r, double* partial6, double* out6, int* err,
                         cudaStream_t st) {
   if (n == 0) return;
-  k_real_stress<<<blocks_for(static_cast<long>(n) * 32, 256), 256, 0, st>>>(
+  k_real_stress<<<blocks_for(static_cast<long>(n) * 32, kRealThreads), kRealThreads, 0, st>>>(
       srt, box_start, n, g, alpha, max_r * max_r, partial6, err);
   k_sum_partials<<<1, 256, 0, st>>>(partial6, n, 6, out6);
   g_launches += 2;

@@ -165,6 +165,27 @@ __global__ void k_pair_rank(const int4* __restrict__ tmp, int nmax, const int* _
   pairs[b + r] = make_int2(v.x, v.y);
 }
 
+// Eight consecutive weights (64 B in FP64, 32 B in FP32; every per-tile weight
+// row starts on such a boundary) with vector loads.
+__device__ __forceinline__ void load8(const double* __restrict__ p, double* out) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const double2 v = reinterpret_cast<const double2*>(p)[i];
+    out[2 * i] = v.x;
+    out[2 * i + 1] = v.y;
+  }
+}
+__device__ __forceinline__ void load8(const float* __restrict__ p, float* out) {
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const float4 v = reinterpret_cast<const float4*>(p)[i];
+    out[4 * i] = v.x;
+    out[4 * i + 1] = v.y;
+    out[4 * i + 2] = v.z;
+    out[4 * i + 3] = v.w;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Spread
 // ---------------------------------------------------------------------------
@@ -177,8 +198,6 @@ __global__ void __launch_bounds__(kPencils) k_spread_tiles(const int* __restrict
   __shared__ R sW1[kSpreadChunk][TX];
   __shared__ R sW2[kSpreadChunk][TY];
   __shared__ R sW3[kSpreadChunk][TZ];
-  __shared__ int2 sPair[kSpreadChunk];
-  __shared__ R sQ[kSpreadChunk];
   const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
   const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
   const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
@@ -189,28 +208,24 @@ __global__ void __launch_bounds__(kPencils) k_spread_tiles(const int* __restrict
   const int p0 = tile_start[tile], p1 = tile_start[tile + 1];
   for (int b0 = p0; b0 < p1; b0 += kSpreadChunk) {
     const int nb = min(kSpreadChunk, p1 - b0);
-    __syncthreads();
-    // Stage the chunk's pairs and charges, then its weights (two dependent
-    // rounds of loads instead of one per weight).
+    __syncthreads();  // the previous chunk's weights are no longer read
+    // One thread per atom of the chunk: its pair, charge and the 3 x 8 weights
+    // for this tile, loaded in one round of independent vector loads.
     if (threadIdx.x < nb) {
-      const int2 pr = pairs[b0 + threadIdx.x];
-      sPair[threadIdx.x] = pr;
-      sQ[threadIdx.x] = qk[pr.x];
-    }
-    __syncthreads();
-#pragma unroll 4
-    for (int it = threadIdx.x; it < nb * (TX + TY + TZ); it += blockDim.x) {
-      const int a = it / (TX + TY + TZ);
-      const int r = it - a * (TX + TY + TZ);
-      const int2 pr = sPair[a];
+      const int a = threadIdx.x;
+      const int2 pr = pairs[b0 + a];
       const R* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
-      if (r < TX) {
-        sW1[a][r] = wk[sd.woff[0] + (pr.y & 0xff) * TX + r];
-      } else if (r < TX + TY) {
-        sW2[a][r - TX] = wk[sd.woff[1] + ((pr.y >> 8) & 0xff) * TY + (r - TX)];
-      } else {
-        sW3[a][r - TX - TY] = wk[sd.woff[2] + (pr.y >> 16) * TZ + (r - TX - TY)] * sQ[a];
-      }
+      R t1[TX], t2[TY], t3[TZ];
+      load8(wk + sd.woff[0] + (pr.y & 0xff) * TX, t1);
+      load8(wk + sd.woff[1] + ((pr.y >> 8) & 0xff) * TY, t2);
+      load8(wk + sd.woff[2] + (pr.y >> 16) * TZ, t3);
+      const R qa = qk[pr.x];
+#pragma unroll
+      for (int x = 0; x < TX; ++x) sW1[a][x] = t1[x];
+#pragma unroll
+      for (int y = 0; y < TY; ++y) sW2[a][y] = t2[y];
+#pragma unroll
+      for (int z = 0; z < TZ; ++z) sW3[a][z] = t3[z] * qa;
     }
     __syncthreads();
     for (int a = 0; a < nb; ++a) {
