@@ -251,6 +251,91 @@ __global__ void __launch_bounds__(kPencils) k_spread_tiles(const int* __restrict
 }
 
 // ---------------------------------------------------------------------------
+// FP64 spread on the tensor cores.  For each z-plane of the tile the spread is
+// a sum of rank-one products, G_z[y][x] = sum_a (q_a w3_a(z) w2_a(y)) w1_a(x),
+// i.e. the 8 x 8 matrix product U_z W1 with U_z[y][a] = q_a w3_a(z) w2_a(y) and
+// W1[a][x] = w1_a(x).  One warp owns a tile and accumulates the eight planes
+// with DMMA (mma.sync m8n8k4, FP64 in and out, IEEE fused multiply-adds), four
+// atoms per step, in list order: deterministic, no atomics.
+// Fragment layouts (m8n8k4, .row.col): A[y][k] at lane 4y + k, B[k][x] at lane
+// 4x + k, C[y][x] at lane 4y + x/2 (element x mod 2).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void dmma_m8n8k4(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+constexpr int kSpreadWarpChunk = 32;  // atoms staged per round (one per lane)
+
+__global__ void __launch_bounds__(32) k_spread_tiles_dmma(const int* __restrict__ tile_start,
+                                                          const int2* __restrict__ pairs,
+                                                          const double* __restrict__ wtab,
+                                                          const double* __restrict__ qk,
+                                                          StencilDims sd,
+                                                          double* __restrict__ grid) {
+  __shared__ double sW1[kSpreadWarpChunk][TX];
+  __shared__ double sW2[kSpreadWarpChunk][TY];
+  __shared__ double sW3[kSpreadWarpChunk][TZ];
+  const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
+  const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
+  const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
+  const int lane = threadIdx.x;
+  const int fr = lane >> 2, fk = lane & 3;  // fragment row (y, or x for B) and k
+  double acc[TZ][2];
+#pragma unroll
+  for (int z = 0; z < TZ; ++z) acc[z][0] = acc[z][1] = 0.0;
+  const int p0 = tile_start[tile], p1 = tile_start[tile + 1];
+  for (int b0 = p0; b0 < p1; b0 += kSpreadWarpChunk) {
+    const int nb = min(kSpreadWarpChunk, p1 - b0);
+    __syncwarp();  // the previous chunk's weights are no longer read
+    double t1[TX], t2[TY], t3[TZ];
+    if (lane < nb) {
+      const int2 pr = pairs[b0 + lane];
+      const double* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
+      load8(wk + sd.woff[0] + (pr.y & 0xff) * TX, t1);
+      load8(wk + sd.woff[1] + ((pr.y >> 8) & 0xff) * TY, t2);
+      load8(wk + sd.woff[2] + (pr.y >> 16) * TZ, t3);
+      const double qa = qk[pr.x];
+#pragma unroll
+      for (int z = 0; z < TZ; ++z) t3[z] *= qa;
+    } else {  // padding atoms of the last group of four contribute zero
+#pragma unroll
+      for (int i = 0; i < 8; ++i) t1[i] = t2[i] = t3[i] = 0.0;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      sW1[lane][i] = t1[i];
+      sW2[lane][i] = t2[i];
+      sW3[lane][i] = t3[i];
+    }
+    __syncwarp();
+    for (int k0 = 0; k0 < nb; k0 += 4) {
+      const int a = k0 + fk;
+      const double bw = sW1[a][fr];  // B[k][x = fr]
+      const double w2 = sW2[a][fr];  // A[y = fr][k] = w2 * q w3(z)
+#pragma unroll
+      for (int z = 0; z < TZ; ++z) dmma_m8n8k4(acc[z][0], acc[z][1], w2 * sW3[a][z], bw);
+    }
+  }
+  const int ex = min(TX, sd.n[0] - x0), ey = min(TY, sd.n[1] - y0), ez = min(TZ, sd.n[2] - z0);
+  const int y = fr, x = 2 * fk;
+  if (y < ey) {
+#pragma unroll
+    for (int z = 0; z < TZ; ++z) {
+      if (z >= ez) break;
+      double* row = grid + (static_cast<size_t>(z0 + z) * sd.n[1] + y0 + y) * sd.n[0] + x0 + x;
+      if (x + 1 < ex) {
+        row[0] = acc[z][0];
+        row[1] = acc[z][1];
+      } else if (x < ex) {
+        row[0] = acc[z][0];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Gather.  One warp per CTA; each lane carries A atoms of the tile's list, so
 // every grid value read from shared memory (a broadcast: all lanes read the
 // same point) feeds A atoms.
@@ -447,10 +532,9 @@ void launch_spread(const MeshPlan& mp, const int* tile_start, const int2* pairs,
                                                      static_cast<const float*>(qk), mp.sd,
                                                      static_cast<float*>(grid));
   else
-    k_spread_tiles<double><<<grd, kPencils, 0, st>>>(tile_start, pairs,
-                                                      static_cast<const double*>(wtab),
-                                                      static_cast<const double*>(qk), mp.sd,
-                                                      static_cast<double*>(grid));
+    k_spread_tiles_dmma<<<grd, 32, 0, st>>>(tile_start, pairs, static_cast<const double*>(wtab),
+                                             static_cast<const double*>(qk), mp.sd,
+                                             static_cast<double*>(grid));
   ++g_launches;
 }
 
