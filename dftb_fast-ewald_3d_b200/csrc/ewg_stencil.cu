@@ -165,16 +165,8 @@ __global__ void k_pair_rank(const int4* __restrict__ tmp, int nmax, const int* _
   pairs[b + r] = make_int2(v.x, v.y);
 }
 
-// Eight consecutive weights (64 B in FP64, 32 B in FP32; every per-tile weight
-// row starts on such a boundary) with vector loads.
-__device__ __forceinline__ void load8(const double* __restrict__ p, double* out) {
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const double2 v = reinterpret_cast<const double2*>(p)[i];
-    out[2 * i] = v.x;
-    out[2 * i + 1] = v.y;
-  }
-}
+// Eight consecutive FP32 weights (32 B; every per-tile weight row starts on
+// such a boundary) with vector loads.
 __device__ __forceinline__ void load8(const float* __restrict__ p, float* out) {
 #pragma unroll
   for (int i = 0; i < 2; ++i) {
@@ -254,7 +246,7 @@ __global__ void __launch_bounds__(kPencils) k_spread_tiles(const int* __restrict
 // FP64 spread on the tensor cores.  For each z-plane of the tile the spread is
 // a sum of rank-one products, G_z[y][x] = sum_a (q_a w3_a(z) w2_a(y)) w1_a(x),
 // i.e. the 8 x 8 matrix product U_z W1 with U_z[y][a] = q_a w3_a(z) w2_a(y) and
-// W1[a][x] = w1_a(x).  One warp owns a tile and accumulates the eight planes
+// W1[a][x] = w1_a(x).  A CTA owns a tile and accumulates its eight planes
 // with DMMA (mma.sync m8n8k4, FP64 in and out, IEEE fused multiply-adds), four
 // atoms per step, in list order: deterministic, no atomics.
 // Fragment layouts (m8n8k4, .row.col): A[y][k] at lane 4y + k, B[k][x] at lane
@@ -266,65 +258,78 @@ __device__ __forceinline__ void dmma_m8n8k4(double& c0, double& c1, double a, do
                : "d"(a), "d"(b));
 }
 
-constexpr int kSpreadWarpChunk = 32;  // atoms staged per round (one per lane)
+constexpr int kSpreadAtoms = 64;  // atoms staged per round, one per thread
+constexpr int kWRow = 12;         // doubles per staged weight row: 8 used; the
+                                  // padding makes the fragment reads conflict-free
 
-__global__ void __launch_bounds__(32) k_spread_tiles_dmma(const int* __restrict__ tile_start,
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Two warps per tile, each owning four z-planes; the 64 threads stage up to 64
+// atoms' weight rows with asynchronous 16-byte copies in one round.
+__global__ void __launch_bounds__(64) k_spread_tiles_dmma(const int* __restrict__ tile_start,
                                                           const int2* __restrict__ pairs,
                                                           const double* __restrict__ wtab,
                                                           const double* __restrict__ qk,
                                                           StencilDims sd,
                                                           double* __restrict__ grid) {
-  __shared__ double sW1[kSpreadWarpChunk][TX];
-  __shared__ double sW2[kSpreadWarpChunk][TY];
-  __shared__ double sW3[kSpreadWarpChunk][TZ];
+  __shared__ __align__(16) double sW[3][kSpreadAtoms][kWRow];
+  __shared__ double sQ[kSpreadAtoms];
   const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
   const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
   const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
-  const int lane = threadIdx.x;
+  const int lane = threadIdx.x & 31, zb = (threadIdx.x >> 5) * (TZ / 2);
   const int fr = lane >> 2, fk = lane & 3;  // fragment row (y, or x for B) and k
-  double acc[TZ][2];
+  double acc[TZ / 2][2];
 #pragma unroll
-  for (int z = 0; z < TZ; ++z) acc[z][0] = acc[z][1] = 0.0;
+  for (int z = 0; z < TZ / 2; ++z) acc[z][0] = acc[z][1] = 0.0;
   const int p0 = tile_start[tile], p1 = tile_start[tile + 1];
-  for (int b0 = p0; b0 < p1; b0 += kSpreadWarpChunk) {
-    const int nb = min(kSpreadWarpChunk, p1 - b0);
-    __syncwarp();  // the previous chunk's weights are no longer read
-    double t1[TX], t2[TY], t3[TZ];
-    if (lane < nb) {
-      const int2 pr = pairs[b0 + lane];
+  for (int b0 = p0; b0 < p1; b0 += kSpreadAtoms) {
+    const int nb = min(kSpreadAtoms, p1 - b0);
+    __syncthreads();  // the previous round's weights are no longer read
+    const int a = threadIdx.x;
+    if (a < nb) {
+      const int2 pr = pairs[b0 + a];
       const double* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
-      load8(wk + sd.woff[0] + (pr.y & 0xff) * TX, t1);
-      load8(wk + sd.woff[1] + ((pr.y >> 8) & 0xff) * TY, t2);
-      load8(wk + sd.woff[2] + (pr.y >> 16) * TZ, t3);
-      const double qa = qk[pr.x];
+      const double* src[3] = {wk + sd.woff[0] + (pr.y & 0xff) * TX,
+                              wk + sd.woff[1] + ((pr.y >> 8) & 0xff) * TY,
+                              wk + sd.woff[2] + (pr.y >> 16) * TZ};
 #pragma unroll
-      for (int z = 0; z < TZ; ++z) t3[z] *= qa;
-    } else {  // padding atoms of the last group of four contribute zero
+      for (int d = 0; d < 3; ++d)
 #pragma unroll
-      for (int i = 0; i < 8; ++i) t1[i] = t2[i] = t3[i] = 0.0;
+        for (int j = 0; j < 4; ++j) cp_async16(&sW[d][a][2 * j], src[d] + 2 * j);
+      sQ[a] = qk[pr.x];
+    } else if (a < ((nb + 3) & ~3)) {  // padding atoms of the last group of four
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) sW[d][a][j] = 0.0;
+      sQ[a] = 0.0;
     }
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      sW1[lane][i] = t1[i];
-      sW2[lane][i] = t2[i];
-      sW3[lane][i] = t3[i];
-    }
-    __syncwarp();
+    cp_async_wait_all();
+    __syncthreads();
     for (int k0 = 0; k0 < nb; k0 += 4) {
-      const int a = k0 + fk;
-      const double bw = sW1[a][fr];  // B[k][x = fr]
-      const double w2 = sW2[a][fr];  // A[y = fr][k] = w2 * q w3(z)
+      const int aa = k0 + fk;
+      const double bw = sW[0][aa][fr];            // B[k][x = fr]
+      const double w2q = sW[1][aa][fr] * sQ[aa];  // A[y = fr][k] = q w2(y) w3(z)
 #pragma unroll
-      for (int z = 0; z < TZ; ++z) dmma_m8n8k4(acc[z][0], acc[z][1], w2 * sW3[a][z], bw);
+      for (int z = 0; z < TZ / 2; ++z)
+        dmma_m8n8k4(acc[z][0], acc[z][1], w2q * sW[2][aa][zb + z], bw);
     }
   }
   const int ex = min(TX, sd.n[0] - x0), ey = min(TY, sd.n[1] - y0), ez = min(TZ, sd.n[2] - z0);
   const int y = fr, x = 2 * fk;
   if (y < ey) {
 #pragma unroll
-    for (int z = 0; z < TZ; ++z) {
-      if (z >= ez) break;
-      double* row = grid + (static_cast<size_t>(z0 + z) * sd.n[1] + y0 + y) * sd.n[0] + x0 + x;
+    for (int z = 0; z < TZ / 2; ++z) {
+      if (zb + z >= ez) break;
+      double* row =
+          grid + (static_cast<size_t>(z0 + zb + z) * sd.n[1] + y0 + y) * sd.n[0] + x0 + x;
       if (x + 1 < ex) {
         row[0] = acc[z][0];
         row[1] = acc[z][1];
@@ -532,7 +537,7 @@ void launch_spread(const MeshPlan& mp, const int* tile_start, const int2* pairs,
                                                      static_cast<const float*>(qk), mp.sd,
                                                      static_cast<float*>(grid));
   else
-    k_spread_tiles_dmma<<<grd, 32, 0, st>>>(tile_start, pairs, static_cast<const double*>(wtab),
+    k_spread_tiles_dmma<<<grd, 64, 0, st>>>(tile_start, pairs, static_cast<const double*>(wtab),
                                              static_cast<const double*>(qk), mp.sd,
                                              static_cast<double*>(grid));
   ++g_launches;
