@@ -460,6 +460,147 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles(const int* __restri
   }
 }
 
+// ---------------------------------------------------------------------------
+// FP64 gather on the tensor cores.  With the tile's values G[z][y][x][c] in
+// shared memory, an atom's result is
+//   phi_a,c = sum_z w3_a(z) sum_y w2_a(y) T_a[z][y][c],
+//   T_a[z][y][c] = sum_x w1_a(x) G[z][y][x][c],
+// and T is a matrix product: rows are atoms (M blocks of 8), the contraction
+// runs over x (two k-steps of 4), columns over (z, c, y) (N blocks of the 8 y
+// values of one plane and component).  Each warp takes up to four M blocks of a
+// round of 64 atoms and loops over the tile's N blocks: two DMMAs per
+// (M block, N block), then the lane holding T for (atom, y pair) folds in
+// w2 and w3.  The four lanes of an atom are summed with shuffles in a fixed
+// order at the end.  Partials go to the (atom, slot) array as in the CUDA-core
+// gather; results are deterministic.
+// Tile layout in shared memory: row (z, y) holds 8 points x NC values, padded
+// to kGRow doubles so the B-fragment reads are nearly conflict-free.
+// ---------------------------------------------------------------------------
+template <int NC>
+struct GatherRow {
+  static constexpr int value = NC == 4 ? 34 : 12;  // 16-byte multiples
+};
+constexpr int kGatherAtoms = 64;  // atoms staged per round, one per thread
+constexpr int kGatherMB = 4;      // M blocks of 8 atoms per warp and round
+
+template <int NC>
+__global__ void __launch_bounds__(64) k_gather_tiles_dmma(const int* __restrict__ tile_start,
+                                                          const int2* __restrict__ pairs,
+                                                          const double* __restrict__ wtab,
+                                                          StencilDims sd,
+                                                          const double* __restrict__ grid,
+                                                          double* __restrict__ part) {
+  constexpr int RS = GatherRow<NC>::value;
+  __shared__ __align__(16) double sG[TZ * TY * RS];
+  __shared__ __align__(16) double sW[3][kGatherAtoms][kWRow];
+  __shared__ int2 sPair[kGatherAtoms];
+  const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
+  const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
+  const int p0 = tile_start[tile], p1 = tile_start[tile + 1];
+  if (p0 == p1) return;  // no atom reaches this tile
+  const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
+  const int ex = min(TX, sd.n[0] - x0), ey = min(TY, sd.n[1] - y0), ez = min(TZ, sd.n[2] - z0);
+  // Stage the tile: 16-byte chunks (NC = 4: half a point; NC = 1: two points).
+  constexpr int kChunksPerRow = TX * NC / 2;
+  for (int t = threadIdx.x; t < TZ * TY * kChunksPerRow; t += blockDim.x) {
+    const int row = t / kChunksPerRow, h = t - row * kChunksPerRow;
+    const int z = row / TY, y = row - z * TY;
+    const int x = NC == 4 ? h / 2 : 2 * h;  // first point of the chunk
+    double* dst = sG + row * RS + 2 * h;
+    if (z < ez && y < ey && x < ex) {
+      const double* src = grid + ((static_cast<size_t>(z0 + z) * sd.n[1] + y0 + y) * sd.n[0] + x0) * NC + 2 * h;
+      cp_async16(dst, src);
+    } else {
+      dst[0] = 0.0;
+      dst[1] = 0.0;
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int fr = lane >> 2, fk = lane & 3;
+  const int nslots = sd.S[0] * sd.S[1] * sd.S[2];
+  for (int b0 = p0; b0 < p1; b0 += kGatherAtoms) {
+    const int nb = min(kGatherAtoms, p1 - b0);
+    __syncthreads();  // the previous round's weights are no longer read
+    {
+      const int a = threadIdx.x;
+      if (a < nb) {
+        const int2 pr = pairs[b0 + a];
+        sPair[a] = pr;
+        const double* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
+        const double* src[3] = {wk + sd.woff[0] + (pr.y & 0xff) * TX,
+                                wk + sd.woff[1] + ((pr.y >> 8) & 0xff) * TY,
+                                wk + sd.woff[2] + (pr.y >> 16) * TZ};
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) cp_async16(&sW[d][a][2 * j], src[d] + 2 * j);
+      } else {  // rows past the list: zero weights, results discarded
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+          for (int j = 0; j < 8; ++j) sW[d][a][j] = 0.0;
+      }
+    }
+    cp_async_wait_all();  // also completes the tile copies on the first round
+    __syncthreads();
+    // This warp's M blocks: atoms warp * 32 + mb * 8 + (0..7) of the round.
+    const int abase = warp * (kGatherMB * 8);
+    if (abase >= nb) continue;
+    const int nmb = min(kGatherMB, (nb - abase + 7) / 8);
+    double fa[kGatherMB][2], w2[kGatherMB][2], acc[kGatherMB][NC];
+#pragma unroll
+    for (int mb = 0; mb < kGatherMB; ++mb) {
+      const int am = abase + mb * 8 + fr;  // this lane's atom row
+      fa[mb][0] = sW[0][am][fk];           // A[m][k], k-step 0: x = k
+      fa[mb][1] = sW[0][am][4 + fk];       // k-step 1: x = 4 + k
+      w2[mb][0] = sW[1][am][2 * fk];       // y pair of this lane's C elements
+      w2[mb][1] = sW[1][am][2 * fk + 1];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) acc[mb][c] = 0.0;
+    }
+#pragma unroll 1
+    for (int z = 0; z < TZ; ++z) {
+      double w3[kGatherMB];
+#pragma unroll
+      for (int mb = 0; mb < kGatherMB; ++mb) w3[mb] = sW[2][abase + mb * 8 + fr][z];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        // B[k][n] = G[z][y = n][x = 4 ks + k][c] at lane 4n + k.
+        const double* gz = sG + (z * TY + fr) * RS + c;
+        const double b0v = gz[fk * NC];
+        const double b1v = gz[(4 + fk) * NC];
+#pragma unroll
+        for (int mb = 0; mb < kGatherMB; ++mb) {
+          if (mb < nmb) {
+            double d0 = 0.0, d1 = 0.0;
+            dmma_m8n8k4(d0, d1, fa[mb][0], b0v);
+            dmma_m8n8k4(d0, d1, fa[mb][1], b1v);
+            acc[mb][c] = fma(w3[mb], fma(w2[mb][0], d0, w2[mb][1] * d1), acc[mb][c]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int mb = 0; mb < kGatherMB; ++mb) {
+      if (mb >= nmb) break;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        acc[mb][c] += __shfl_xor_sync(0xffffffffu, acc[mb][c], 1);
+        acc[mb][c] += __shfl_xor_sync(0xffffffffu, acc[mb][c], 2);
+      }
+      const int a = abase + mb * 8 + fr;
+      if (fk == 0 && a < nb) {
+        const int2 pr = sPair[a];
+        const int ps = pr.y;
+        const int sidx = ((ps >> 16) * sd.S[1] + ((ps >> 8) & 0xff)) * sd.S[0] + (ps & 0xff);
+        double* dst = part + (static_cast<size_t>(pr.x) * nslots + sidx) * NC;
+#pragma unroll
+        for (int c = 0; c < NC; ++c) dst[c] = acc[mb][c];
+      }
+    }
+  }
+}
+
 // Final per-atom sum of the slot partials in a fixed order, with the assembly
 // of fft/ewald_fft_3d.f90:121-132: pot = (sr + lr) + self, force = sr + q lr.
 template <int NC>
@@ -557,9 +698,13 @@ void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs,
       EWG_GATHER(float, 1);
   } else {
     if (nc == 4)
-      EWG_GATHER(double, 4);
+      k_gather_tiles_dmma<4><<<grd, 64, 0, st>>>(tile_start, pairs,
+                                                 static_cast<const double*>(wtab), mp.sd,
+                                                 static_cast<const double*>(grid), part);
     else
-      EWG_GATHER(double, 1);
+      k_gather_tiles_dmma<1><<<grd, 64, 0, st>>>(tile_start, pairs,
+                                                 static_cast<const double*>(wtab), mp.sd,
+                                                 static_cast<const double*>(grid), part);
   }
 #undef EWG_GATHER
   ++g_launches;
