@@ -466,12 +466,12 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles(const int* __restri
 //   phi_a,c = sum_z w3_a(z) sum_y w2_a(y) T_a[z][y][c],
 //   T_a[z][y][c] = sum_x w1_a(x) G[z][y][x][c],
 // and T is a matrix product: rows are atoms (M blocks of 8), the contraction
-// runs over x (two k-steps of 4), columns over (z, c, y) (N blocks of the 8 y
-// values of one plane and component).  Each warp takes up to four M blocks of a
-// round of 64 atoms and loops over the tile's N blocks: two DMMAs per
-// (M block, N block), then the lane holding T for (atom, y pair) folds in
-// w2 and w3.  The four lanes of an atom are summed with shuffles in a fixed
-// order at the end.  Partials go to the (atom, slot) array as in the CUDA-core
+// runs over x (two k-steps of 4), columns over (c, y) (N blocks of the 8 y
+// values of one component).  Scaling the A fragment by w3_a(z) lets the DMMA
+// accumulators sum over the planes too.  Each warp takes up to four M blocks of
+// a round of 64 atoms; per plane and component it issues two DMMAs per M block.
+// At the end the lane holding C for (atom, y pair) folds in w2, and the four
+// lanes of an atom are summed with shuffles in a fixed order.  Partials go to the (atom, slot) array as in the CUDA-core
 // gather; results are deterministic.
 // Tile layout in shared memory: row (z, y) holds 8 points x NC values, padded
 // to kGRow doubles so the B-fragment reads are nearly conflict-free.
@@ -547,22 +547,26 @@ __global__ void __launch_bounds__(64) k_gather_tiles_dmma(const int* __restrict_
     const int abase = warp * (kGatherMB * 8);
     if (abase >= nb) continue;
     const int nmb = min(kGatherMB, (nb - abase + 7) / 8);
-    double fa[kGatherMB][2], w2[kGatherMB][2], acc[kGatherMB][NC];
+    double fa[kGatherMB][2], cacc[kGatherMB][NC][2];
 #pragma unroll
     for (int mb = 0; mb < kGatherMB; ++mb) {
       const int am = abase + mb * 8 + fr;  // this lane's atom row
       fa[mb][0] = sW[0][am][fk];           // A[m][k], k-step 0: x = k
       fa[mb][1] = sW[0][am][4 + fk];       // k-step 1: x = 4 + k
-      w2[mb][0] = sW[1][am][2 * fk];       // y pair of this lane's C elements
-      w2[mb][1] = sW[1][am][2 * fk + 1];
 #pragma unroll
-      for (int c = 0; c < NC; ++c) acc[mb][c] = 0.0;
+      for (int c = 0; c < NC; ++c) cacc[mb][c][0] = cacc[mb][c][1] = 0.0;
     }
+    // w3 is folded into the A fragment, so C sums over z as well:
+    // C[m][y] = sum_z sum_x w3_m(z) w1_m(x) G[z][y][x][c].
 #pragma unroll 1
     for (int z = 0; z < TZ; ++z) {
-      double w3[kGatherMB];
+      double a0[kGatherMB], a1[kGatherMB];
 #pragma unroll
-      for (int mb = 0; mb < kGatherMB; ++mb) w3[mb] = sW[2][abase + mb * 8 + fr][z];
+      for (int mb = 0; mb < kGatherMB; ++mb) {
+        const double w3 = sW[2][abase + mb * 8 + fr][z];
+        a0[mb] = fa[mb][0] * w3;
+        a1[mb] = fa[mb][1] * w3;
+      }
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
         // B[k][n] = G[z][y = n][x = 4 ks + k][c] at lane 4n + k.
@@ -572,10 +576,8 @@ __global__ void __launch_bounds__(64) k_gather_tiles_dmma(const int* __restrict_
 #pragma unroll
         for (int mb = 0; mb < kGatherMB; ++mb) {
           if (mb < nmb) {
-            double d0 = 0.0, d1 = 0.0;
-            dmma_m8n8k4(d0, d1, fa[mb][0], b0v);
-            dmma_m8n8k4(d0, d1, fa[mb][1], b1v);
-            acc[mb][c] = fma(w3[mb], fma(w2[mb][0], d0, w2[mb][1] * d1), acc[mb][c]);
+            dmma_m8n8k4(cacc[mb][c][0], cacc[mb][c][1], a0[mb], b0v);
+            dmma_m8n8k4(cacc[mb][c][0], cacc[mb][c][1], a1[mb], b1v);
           }
         }
       }
@@ -583,10 +585,16 @@ __global__ void __launch_bounds__(64) k_gather_tiles_dmma(const int* __restrict_
 #pragma unroll
     for (int mb = 0; mb < kGatherMB; ++mb) {
       if (mb >= nmb) break;
+      // This lane holds C for y = 2 fk and 2 fk + 1: weight them by w2 and sum
+      // the four lanes of the atom.
+      const int am = abase + mb * 8 + fr;
+      const double w20 = sW[1][am][2 * fk], w21 = sW[1][am][2 * fk + 1];
+      double acc[NC];
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
-        acc[mb][c] += __shfl_xor_sync(0xffffffffu, acc[mb][c], 1);
-        acc[mb][c] += __shfl_xor_sync(0xffffffffu, acc[mb][c], 2);
+        acc[c] = fma(w20, cacc[mb][c][0], w21 * cacc[mb][c][1]);
+        acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], 1);
+        acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], 2);
       }
       const int a = abase + mb * 8 + fr;
       if (fk == 0 && a < nb) {
@@ -595,7 +603,7 @@ __global__ void __launch_bounds__(64) k_gather_tiles_dmma(const int* __restrict_
         const int sidx = ((ps >> 16) * sd.S[1] + ((ps >> 8) & 0xff)) * sd.S[0] + (ps & 0xff);
         double* dst = part + (static_cast<size_t>(pr.x) * nslots + sidx) * NC;
 #pragma unroll
-        for (int c = 0; c < NC; ++c) dst[c] = acc[mb][c];
+        for (int c = 0; c < NC; ++c) dst[c] = acc[c];
       }
     }
   }
