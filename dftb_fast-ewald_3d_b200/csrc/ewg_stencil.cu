@@ -258,6 +258,8 @@ __device__ __forceinline__ void dmma_m8n8k4(double& c0, double& c1, double a, do
                : "d"(a), "d"(b));
 }
 
+constexpr int kGatherWarps = 4;   // FP64 gather: warps per tile
+constexpr int kGatherMB = 2;      // FP64 gather: M blocks of 8 atoms per warp and round
 constexpr int kSpreadAtoms = 64;  // atoms staged per round, one per thread
 constexpr int kWRow = 12;         // doubles per staged weight row: 8 used; the
                                   // padding makes the fragment reads conflict-free
@@ -468,8 +470,8 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles(const int* __restri
 // and T is a matrix product: rows are atoms (M blocks of 8), the contraction
 // runs over x (two k-steps of 4), columns over (c, y) (N blocks of the 8 y
 // values of one component).  Scaling the A fragment by w3_a(z) lets the DMMA
-// accumulators sum over the planes too.  Each warp takes up to four M blocks of
-// a round of 64 atoms; per plane and component it issues two DMMAs per M block.
+// accumulators sum over the planes too.  Each warp takes up to MB M blocks of
+// a round of 8 MB WARPS atoms; per plane and component it issues two DMMAs per M block.
 // At the end the lane holding C for (atom, y pair) folds in w2, and the four
 // lanes of an atom are summed with shuffles in a fixed order.  Partials go to the (atom, slot) array as in the CUDA-core
 // gather; results are deterministic.
@@ -480,17 +482,16 @@ template <int NC>
 struct GatherRow {
   static constexpr int value = NC == 4 ? 34 : 12;  // 16-byte multiples
 };
-constexpr int kGatherAtoms = 64;  // atoms staged per round, one per thread
-constexpr int kGatherMB = 4;      // M blocks of 8 atoms per warp and round
-
-template <int NC>
-__global__ void __launch_bounds__(64) k_gather_tiles_dmma(const int* __restrict__ tile_start,
+// WARPS warps per CTA, MB M blocks of 8 atoms per warp and round.
+template <int NC, int WARPS, int MB>
+__global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma(const int* __restrict__ tile_start,
                                                           const int2* __restrict__ pairs,
                                                           const double* __restrict__ wtab,
                                                           StencilDims sd,
                                                           const double* __restrict__ grid,
                                                           double* __restrict__ part) {
   constexpr int RS = GatherRow<NC>::value;
+  constexpr int kGatherAtoms = WARPS * MB * 8;  // atoms staged per round
   __shared__ __align__(16) double sG[TZ * TY * RS];
   __shared__ __align__(16) double sW[3][kGatherAtoms][kWRow];
   __shared__ int2 sPair[kGatherAtoms];
@@ -521,8 +522,7 @@ __global__ void __launch_bounds__(64) k_gather_tiles_dmma(const int* __restrict_
   for (int b0 = p0; b0 < p1; b0 += kGatherAtoms) {
     const int nb = min(kGatherAtoms, p1 - b0);
     __syncthreads();  // the previous round's weights are no longer read
-    {
-      const int a = threadIdx.x;
+    for (int a = threadIdx.x; a < kGatherAtoms; a += blockDim.x) {
       if (a < nb) {
         const int2 pr = pairs[b0 + a];
         sPair[a] = pr;
@@ -544,12 +544,12 @@ __global__ void __launch_bounds__(64) k_gather_tiles_dmma(const int* __restrict_
     cp_async_wait_all();  // also completes the tile copies on the first round
     __syncthreads();
     // This warp's M blocks: atoms warp * 32 + mb * 8 + (0..7) of the round.
-    const int abase = warp * (kGatherMB * 8);
+    const int abase = warp * (MB * 8);
     if (abase >= nb) continue;
-    const int nmb = min(kGatherMB, (nb - abase + 7) / 8);
-    double fa[kGatherMB][2], cacc[kGatherMB][NC][2];
+    const int nmb = min(MB, (nb - abase + 7) / 8);
+    double fa[MB][2], cacc[MB][NC][2];
 #pragma unroll
-    for (int mb = 0; mb < kGatherMB; ++mb) {
+    for (int mb = 0; mb < MB; ++mb) {
       const int am = abase + mb * 8 + fr;  // this lane's atom row
       fa[mb][0] = sW[0][am][fk];           // A[m][k], k-step 0: x = k
       fa[mb][1] = sW[0][am][4 + fk];       // k-step 1: x = 4 + k
@@ -560,9 +560,9 @@ __global__ void __launch_bounds__(64) k_gather_tiles_dmma(const int* __restrict_
     // C[m][y] = sum_z sum_x w3_m(z) w1_m(x) G[z][y][x][c].
 #pragma unroll 1
     for (int z = 0; z < TZ; ++z) {
-      double a0[kGatherMB], a1[kGatherMB];
+      double a0[MB], a1[MB];
 #pragma unroll
-      for (int mb = 0; mb < kGatherMB; ++mb) {
+      for (int mb = 0; mb < MB; ++mb) {
         const double w3 = sW[2][abase + mb * 8 + fr][z];
         a0[mb] = fa[mb][0] * w3;
         a1[mb] = fa[mb][1] * w3;
@@ -574,7 +574,7 @@ __global__ void __launch_bounds__(64) k_gather_tiles_dmma(const int* __restrict_
         const double b0v = gz[fk * NC];
         const double b1v = gz[(4 + fk) * NC];
 #pragma unroll
-        for (int mb = 0; mb < kGatherMB; ++mb) {
+        for (int mb = 0; mb < MB; ++mb) {
           if (mb < nmb) {
             dmma_m8n8k4(cacc[mb][c][0], cacc[mb][c][1], a0[mb], b0v);
             dmma_m8n8k4(cacc[mb][c][0], cacc[mb][c][1], a1[mb], b1v);
@@ -583,7 +583,7 @@ __global__ void __launch_bounds__(64) k_gather_tiles_dmma(const int* __restrict_
       }
     }
 #pragma unroll
-    for (int mb = 0; mb < kGatherMB; ++mb) {
+    for (int mb = 0; mb < MB; ++mb) {
       if (mb >= nmb) break;
       // This lane holds C for y = 2 fk and 2 fk + 1: weight them by w2 and sum
       // the four lanes of the atom.
@@ -706,11 +706,13 @@ void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs,
       EWG_GATHER(float, 1);
   } else {
     if (nc == 4)
-      k_gather_tiles_dmma<4><<<grd, 64, 0, st>>>(tile_start, pairs,
+      k_gather_tiles_dmma<4, kGatherWarps, kGatherMB><<<grd, 32 * kGatherWarps, 0, st>>>(
+          tile_start, pairs,
                                                  static_cast<const double*>(wtab), mp.sd,
                                                  static_cast<const double*>(grid), part);
     else
-      k_gather_tiles_dmma<1><<<grd, 64, 0, st>>>(tile_start, pairs,
+      k_gather_tiles_dmma<1, kGatherWarps, kGatherMB><<<grd, 32 * kGatherWarps, 0, st>>>(
+          tile_start, pairs,
                                                  static_cast<const double*>(wtab), mp.sd,
                                                  static_cast<const double*>(grid), part);
   }
