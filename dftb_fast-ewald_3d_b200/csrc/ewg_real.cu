@@ -88,23 +88,30 @@ __global__ void k_count(const int* __restrict__ key, int n, int* __restrict__ co
   if (i < n) atomicAdd(&counts[key[i]], 1);
 }
 
-// Exclusive scan of counts into starts[0..nkeys]; one CTA of 1024 threads,
-// each scanning 16 consecutive entries per round.
+// Exclusive scan of counts into starts[0..nkeys]; one CTA of 1024 threads.
+// Each round stages 8192 counts in shared memory with coalesced loads, scans 8
+// consecutive entries per thread and writes the starts back coalesced.
 __global__ void __launch_bounds__(1024) k_scan(const int* __restrict__ counts, int nkeys,
                                                int* __restrict__ starts) {
-  constexpr int kItems = 16;
+  constexpr int kItems = 8, kRound = 1024 * kItems;
+  __shared__ int buf[kRound + kRound / 32];  // padded: entry i at i + i / 32
   __shared__ int warp_sums[32];
-  __shared__ int carry;
-  if (threadIdx.x == 0) carry = 0;
-  __syncthreads();
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int base = 0; base < nkeys; base += 1024 * kItems) {
-    const int first = base + threadIdx.x * kItems;
+  __shared__ int carry_s;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  int carry = 0;
+  for (int base = 0; base < nkeys; base += kRound) {
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+      const int e = j * 1024 + tid;
+      buf[e + (e >> 5)] = base + e < nkeys ? counts[base + e] : 0;
+    }
+    __syncthreads();
     int v[kItems];
     int local = 0;
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
-      v[j] = first + j < nkeys ? counts[first + j] : 0;
+      const int e = tid * kItems + j;
+      v[j] = buf[e + (e >> 5)];
       local += v[j];
     }
     int x = local;
@@ -126,14 +133,21 @@ __global__ void __launch_bounds__(1024) k_scan(const int* __restrict__ counts, i
     int run = carry + x - local + (wid > 0 ? warp_sums[wid - 1] : 0);
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
-      if (first + j < nkeys) starts[first + j] = run;
+      const int e = tid * kItems + j;
+      buf[e + (e >> 5)] = run;
       run += v[j];
     }
+    if (tid == 1023) carry_s = run;
     __syncthreads();
-    if (threadIdx.x == 1023) carry = run;
-    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < kItems; ++j) {
+      const int e = j * 1024 + tid;
+      if (base + e < nkeys) starts[base + e] = buf[e + (e >> 5)];
+    }
+    carry = carry_s;
+    __syncthreads();  // buf and warp_sums are rewritten by the next round
   }
-  if (threadIdx.x == 0) starts[nkeys] = carry;
+  if (tid == 0) starts[nkeys] = carry;
 }
 
 __global__ void k_scatter(const int* __restrict__ key, int n, const int* __restrict__ starts,

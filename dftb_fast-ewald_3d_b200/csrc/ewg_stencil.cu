@@ -27,6 +27,7 @@
 
 #include <cuda_runtime.h>
 
+#include <climits>
 #include <type_traits>
 
 #include "ewg_kernels.h"
@@ -134,35 +135,59 @@ __device__ __forceinline__ void for_each_tile(const int4& si, const StencilDims&
   }
 }
 
+// One thread per (atom, slot of the S_x x S_y x S_z block); slots past the
+// atom's own tile counts are skipped.
+__device__ __forceinline__ bool pair_of_thread(const int4* __restrict__ slot, int n,
+                                               const StencilDims& sd, int* tile, int* k,
+                                               int* packed) {
+  const int S = sd.S[0] * sd.S[1] * sd.S[2];
+  const long t = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= static_cast<long>(n) * S) return false;
+  *k = static_cast<int>(t / S);
+  const int s = static_cast<int>(t - static_cast<long>(*k) * S);
+  const int sx = s % sd.S[0], sy = (s / sd.S[0]) % sd.S[1], sz = s / (sd.S[0] * sd.S[1]);
+  const int4 si = slot[*k];
+  if (sx >= slot_count(si.x) || sy >= slot_count(si.y) || sz >= slot_count(si.z)) return false;
+  const int tx = (slot_first(si.x) + sx) % sd.ntiles[0];
+  const int ty = (slot_first(si.y) + sy) % sd.ntiles[1];
+  const int tz = (slot_first(si.z) + sz) % sd.ntiles[2];
+  *tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
+  *packed = sx | (sy << 8) | (sz << 16);
+  return true;
+}
+
 __global__ void k_pair_count(const int4* __restrict__ slot, int n, StencilDims sd,
                              int* __restrict__ counts) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  for_each_tile(slot[k], sd, [&](int tile, int) { atomicAdd(&counts[tile], 1); });
+  int tile, k, packed;
+  if (pair_of_thread(slot, n, sd, &tile, &k, &packed)) atomicAdd(&counts[tile], 1);
 }
 
 __global__ void k_pair_scatter(const int4* __restrict__ slot, int n, StencilDims sd,
                                const int* __restrict__ starts, int* __restrict__ cursor,
-                               int4* __restrict__ tmp) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  for_each_tile(slot[k], sd, [&](int tile, int packed) {
-    tmp[starts[tile] + atomicAdd(&cursor[tile], 1)] = make_int4(k, packed, tile, 0);
-  });
+                               int2* __restrict__ tmp) {
+  int tile, k, packed;
+  if (pair_of_thread(slot, n, sd, &tile, &k, &packed))
+    tmp[starts[tile] + atomicAdd(&cursor[tile], 1)] = make_int2(k, packed);
 }
 
-// Orders each tile's bucket by atom index (atoms are unique within a bucket).
-// Entries past the last written one (npairs below the bound) hold tile = -1.
-__global__ void k_pair_rank(const int4* __restrict__ tmp, int nmax, const int* __restrict__ starts,
+// One thread per entry: orders each tile's bucket by atom index (atoms are
+// unique within a bucket) by counting the bucket's entries with a smaller atom.
+// The entry's tile follows from its atom's slot record and its packed slot.
+__global__ void k_pair_rank(const int2* __restrict__ tmp, const int* __restrict__ starts,
+                            int ntiles, const int4* __restrict__ slot, StencilDims sd,
                             int2* __restrict__ pairs) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= nmax) return;
-  const int4 v = tmp[e];
-  if (v.z < 0) return;
-  const int b = starts[v.z], end = starts[v.z + 1];
+  if (e >= starts[ntiles]) return;
+  const int2 v = tmp[e];
+  const int4 si = slot[v.x];
+  const int tx = (slot_first(si.x) + (v.y & 0xff)) % sd.ntiles[0];
+  const int ty = (slot_first(si.y) + ((v.y >> 8) & 0xff)) % sd.ntiles[1];
+  const int tz = (slot_first(si.z) + (v.y >> 16)) % sd.ntiles[2];
+  const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
+  const int b = starts[tile], end = starts[tile + 1];
   int r = 0;
   for (int j = b; j < end; ++j) r += tmp[j].x < v.x;
-  pairs[b + r] = make_int2(v.x, v.y);
+  pairs[b + r] = v;
 }
 
 // Eight consecutive FP32 weights (32 B; every per-tile weight row starts on
@@ -611,13 +636,16 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma(const int* __r
 
 // Final per-atom sum of the slot partials in a fixed order, with the assembly
 // of fft/ewald_fft_3d.f90:121-132: pot = (sr + lr) + self, force = sr + q lr.
+// One warp per atom: lanes read the atom's slots (contiguous, coalesced), then
+// a shuffle tree sums them (a fixed order: results are reproducible).
 template <int NC>
 __global__ void k_gather_final(const int4* __restrict__ slot, const int* __restrict__ perm,
                                const double* __restrict__ part, int n, StencilDims sd,
                                const double* __restrict__ q, double self_coef,
                                const double* __restrict__ pot_sr, const double* __restrict__ f_sr,
                                double* __restrict__ pot, double* __restrict__ force) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = static_cast<int>((static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
   if (k >= n) return;
   const int4 si = slot[k];
   const int cx = slot_count(si.x), cy = slot_count(si.y), cz = slot_count(si.z);
@@ -626,13 +654,18 @@ __global__ void k_gather_final(const int4* __restrict__ slot, const int* __restr
   double acc[NC];
 #pragma unroll
   for (int c = 0; c < NC; ++c) acc[c] = 0.0;
-  for (int sz = 0; sz < cz; ++sz)
-    for (int sy = 0; sy < cy; ++sy)
-      for (int sx = 0; sx < cx; ++sx) {
-        const double* pp = pk + ((sz * sd.S[1] + sy) * sd.S[0] + sx) * NC;
+  for (int s = lane; s < nslots; s += 32) {
+    const int sx = s % sd.S[0], sy = (s / sd.S[0]) % sd.S[1], sz = s / (sd.S[0] * sd.S[1]);
+    if (sx < cx && sy < cy && sz < cz) {  // slots past the atom's tiles hold no partial
 #pragma unroll
-        for (int c = 0; c < NC; ++c) acc[c] += pp[c];
-      }
+      for (int c = 0; c < NC; ++c) acc[c] += pk[s * NC + c];
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < NC; ++c)
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
+  if (lane != 0) return;
   const int i = perm[k];
   const double qi = q[i];
   pot[i] = (pot_sr[i] + acc[0]) + self_coef * qi;
@@ -661,18 +694,20 @@ void launch_weights(const MeshPlan& mp, const int4* mc, const double4* fr, int n
 void launch_pair_bins(const MeshPlan& mp, const int4* slot, int n, int* counts, int* cursor,
                       int* tile_start, int4* tmp, int2* pairs, int npairs_max, cudaStream_t st) {
   const int ntiles = mp.sd.ntiles[0] * mp.sd.ntiles[1] * mp.sd.ntiles[2];
+  const long nthreads = static_cast<long>(n) * mp.sd.S[0] * mp.sd.S[1] * mp.sd.S[2];
+  int2* t2 = reinterpret_cast<int2*>(tmp);
   cudaMemsetAsync(counts, 0, sizeof(int) * ntiles, st);
   cudaMemsetAsync(cursor, 0, sizeof(int) * ntiles, st);
-  // Unused tail entries of tmp are marked with tile = -1.
-  cudaMemsetAsync(tmp, 0xff, sizeof(int4) * static_cast<size_t>(npairs_max), st);
   if (n > 0) {
-    k_pair_count<<<blocks_for(n, 128), 128, 0, st>>>(slot, n, mp.sd, counts);
+    k_pair_count<<<blocks_for(nthreads, 256), 256, 0, st>>>(slot, n, mp.sd, counts);
     ++g_launches;
   }
   launch_scan(counts, ntiles, tile_start, st);
   if (n > 0) {
-    k_pair_scatter<<<blocks_for(n, 128), 128, 0, st>>>(slot, n, mp.sd, tile_start, cursor, tmp);
-    k_pair_rank<<<blocks_for(npairs_max, 256), 256, 0, st>>>(tmp, npairs_max, tile_start, pairs);
+    k_pair_scatter<<<blocks_for(nthreads, 256), 256, 0, st>>>(slot, n, mp.sd, tile_start, cursor,
+                                                               t2);
+    k_pair_rank<<<blocks_for(npairs_max, 256), 256, 0, st>>>(t2, tile_start, ntiles, slot, mp.sd,
+                                                              pairs);
     g_launches += 2;
   }
 }
@@ -725,11 +760,11 @@ void launch_gather_final(const MeshPlan& mp, const int4* slot, const int* perm, 
                          const double* f_sr, double* pot, double* force, cudaStream_t st) {
   if (n == 0) return;
   if (nc == 4)
-    k_gather_final<4><<<blocks_for(n, 128), 128, 0, st>>>(slot, perm, part, n, mp.sd, q, self_coef,
-                                                           pot_sr, f_sr, pot, force);
+    k_gather_final<4><<<blocks_for(32L * n, 256), 256, 0, st>>>(
+        slot, perm, part, n, mp.sd, q, self_coef, pot_sr, f_sr, pot, force);
   else
-    k_gather_final<1><<<blocks_for(n, 128), 128, 0, st>>>(slot, perm, part, n, mp.sd, q, self_coef,
-                                                           pot_sr, f_sr, pot, nullptr);
+    k_gather_final<1><<<blocks_for(32L * n, 256), 256, 0, st>>>(
+        slot, perm, part, n, mp.sd, q, self_coef, pot_sr, f_sr, pot, nullptr);
   ++g_launches;
 }
 
