@@ -342,9 +342,11 @@ struct EwaldPair {
     const double qj = e.w;
     if constexpr (!MIXED) {
       const double r = sqrt(r2);
-      const double ec = erfc(alpha * r);
-      pot += qj * ec / r;
-      const double ff = qi * qj * (2.0 * alpha / kSqrtPi * exp(-alpha * alpha * r2) + ec / r) / r2;
+      const double rinv = 1.0 / r;
+      const double ecr = erfc(alpha * r) * rinv;  // erfc(alpha r) / r
+      pot += qj * ecr;
+      const double ff =
+          qi * qj * (2.0 * alpha / kSqrtPi * exp(-alpha * alpha * r2) + ecr) * (rinv * rinv);
       f[0] += ff * e.x;
       f[1] += ff * e.y;
       f[2] += ff * e.z;
