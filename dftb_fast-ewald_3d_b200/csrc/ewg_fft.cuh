@@ -110,17 +110,35 @@ __device__ __forceinline__ void dft8(cx<R>* u) {
   u[7] = sub(e3, w3o);
 }
 
-// Odd radix RR via conjugate-symmetric pairs; cos/sin of 2 pi j / RR are read
-// from the length-n twiddle table (tw[j n / RR] = exp(-2 pi i j / RR)).
+// Odd radix RR via conjugate-symmetric pairs; cos/sin of 2 pi j / RR are
+// constants for RR = 5, 7 and read from the length-n twiddle table
+// (tw[j n / RR] = exp(-2 pi i j / RR)) otherwise.
+// cos and sin of 2 pi j / RR for the specialised odd radices (j = 1 .. (RR-1)/2).
+__host__ __device__ constexpr double odd_root_cos(int rr, int j) {
+  return rr == 5 ? (j == 1 ? 0.30901699437494742408 : -0.80901699437494742410)
+                 : (j == 1 ? 0.62348980185873353053
+                           : (j == 2 ? -0.22252093395631440429 : -0.90096886790241912624));
+}
+__host__ __device__ constexpr double odd_root_sin(int rr, int j) {
+  return rr == 5 ? (j == 1 ? 0.95105651629515357212 : 0.58778525229247312917)
+                 : (j == 1 ? 0.78183148246802980871
+                           : (j == 2 ? 0.97492791218182360702 : 0.43388373911755812048));
+}
+
 template <typename R, int SIGN, int RR>
 __device__ __forceinline__ void dft_odd(cx<R>* u, const cx<R>* __restrict__ tw, int n) {
   constexpr int H = (RR - 1) / 2;
   R c[H + 1], s[H + 1];
 #pragma unroll
   for (int j = 1; j <= H; ++j) {
-    cx<R> w = tw[j * (n / RR)];
-    c[j] = w.x;
-    s[j] = -w.y;
+    if constexpr (RR == 5 || RR == 7) {
+      c[j] = static_cast<R>(odd_root_cos(RR, j));
+      s[j] = static_cast<R>(odd_root_sin(RR, j));
+    } else {
+      cx<R> w = tw[j * (n / RR)];
+      c[j] = w.x;
+      s[j] = -w.y;
+    }
   }
   cx<R> sp[H + 1], sm[H + 1];
   cx<R> total = u[0];
@@ -222,8 +240,19 @@ __device__ __forceinline__ void edge_pass(const cx<R>* __restrict__ in, cx<R>* _
 #pragma unroll
       for (int jj = 0; jj < RR; ++jj) u[jj] = src[jj * nr * L];
       if (p > 1) {
+        if constexpr (sizeof(R) == 8) {
+          // FP64: one table read, the other powers by recurrence (error a few ulp).
+          const cx<R> w1 = twiddle(tw, k * step, SIGN);
+          cx<R> w = w1;
 #pragma unroll
-        for (int jj = 1; jj < RR; ++jj) u[jj] = mul(u[jj], twiddle(tw, jj * k * step, SIGN));
+          for (int jj = 1; jj < RR; ++jj) {
+            u[jj] = mul(u[jj], w);
+            if (jj + 1 < RR) w = mul(w, w1);
+          }
+        } else {
+#pragma unroll
+          for (int jj = 1; jj < RR; ++jj) u[jj] = mul(u[jj], twiddle(tw, jj * k * step, SIGN));
+        }
       }
     }
     dft_fixed<R, SIGN, RR>(u, tw, n);
