@@ -59,12 +59,11 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_r2c(const R* __restri
   cx<R>* b = a + static_cast<size_t>(n1) * L;
   const cx<R>* tw = plan_twiddles<R>(plan);
   const int pair0 = blockIdx.x * L;
-  auto load = [&](int l, int x) {
-    const int pr = pair0 + l;
-    if (pr >= npairs) return mk(R(0), R(0));
-    const size_t r0 = static_cast<size_t>(2 * pr) * n1;
-    return mk(grid[r0 + x], grid[r0 + n1 + x]);
-  };
+  // Each thread serves one line (its lane in the group): resolve its rows once.
+  const bool valid = pair0 + static_cast<int>(threadIdx.x & (L - 1)) < npairs;
+  const R* ra = grid + static_cast<size_t>(2 * (pair0 + (threadIdx.x & (L - 1)))) * n1;
+  const R* rb = ra + n1;
+  auto load = [&](int, int x) { return valid ? mk(ra[x], rb[x]) : mk(R(0), R(0)); };
   auto store = [&](int l, int k, cx<R> v, cx<R>* spare) { spare[k * L + l] = v; };
   fft_edges<R, -1, L>(a, b, n1, plan, tw, load, store);
   __syncthreads();
@@ -97,10 +96,12 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_fwd(const cx<R>* __re
   const cx<R>* tw = plan_twiddles<R>(plan);
   const int k0 = blockIdx.x * L;
   const int i3 = blockIdx.y;
-  auto load = [&](int l, int i2) {
-    return k0 + l < K1 ? A1[(static_cast<size_t>(i3) * n2 + i2) * K1 + k0 + l] : mk(R(0), R(0));
-  };
-  auto store = [&](int l, int e, cx<R> v, cx<R>*) {
+  const int kl = k0 + static_cast<int>(threadIdx.x & (L - 1));  // this thread's k1
+  const bool kin = kl < K1;
+  const cx<R>* src = A1 + static_cast<size_t>(i3) * n2 * K1 + kl;
+  cx<R>* dst = A2 + static_cast<size_t>(i3) * K2 * K1 + kl;
+  auto load = [&](int, int i2) { return kin ? src[i2 * K1] : mk(R(0), R(0)); };
+  auto store = [&](int, int e, cx<R> v, cx<R>*) {
     int k2i;
     if (e <= H2)
       k2i = e + H2;
@@ -108,7 +109,7 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_fwd(const cx<R>* __re
       k2i = e - n2 + H2;
     else
       return;
-    if (k0 + l < K1) A2[(static_cast<size_t>(i3) * K2 + k2i) * K1 + k0 + l] = v;
+    if (kin) dst[k2i * K1] = v;
   };
   fft_edges<R, -1, L>(a, b, n2, plan, tw, load, store);
 }
@@ -139,9 +140,11 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
   const int h1 = ia.H[0], h2 = ia.H[1], h3 = ia.H[2];
   const int k2 = k2i - h2;
   const double twoPi = 2.0 * 3.14159265358979323846;
-  auto load_fwd = [&](int l, int i3) {
-    return k0 + l < K1 ? A2[(static_cast<size_t>(i3) * K2 + k2i) * K1 + k0 + l] : mk(R(0), R(0));
-  };
+  const int kl = k0 + static_cast<int>(threadIdx.x & (L - 1));  // this thread's k1
+  const bool kin = kl < K1;
+  const size_t zstride = static_cast<size_t>(K2) * K1;
+  const cx<R>* src = A2 + static_cast<size_t>(k2i) * K1 + kl;
+  auto load_fwd = [&](int, int i3) { return kin ? src[i3 * zstride] : mk(R(0), R(0)); };
   // Weight each mode of the closed box as it leaves the forward transform.
   auto store_weighted = [&](int l, int e, cx<R> g, cx<R>*) {
     int k3;
@@ -198,9 +201,9 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
       }
       return v;
     };
-    cx<R>* dst = B2 + static_cast<size_t>(c) * n3 * K2 * K1;
-    auto store = [&](int l, int i3, cx<R> v, cx<R>*) {
-      if (k0 + l < K1) dst[(static_cast<size_t>(i3) * K2 + k2i) * K1 + k0 + l] = v;
+    cx<R>* dst = B2 + static_cast<size_t>(c) * n3 * zstride + static_cast<size_t>(k2i) * K1 + kl;
+    auto store = [&](int, int i3, cx<R> v, cx<R>*) {
+      if (kin) dst[i3 * zstride] = v;
     };
     fft_edges<R, 1, L>(a, b, n3, plan, tw, load_inv, store);
     __syncthreads();
@@ -222,9 +225,12 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_inv(const cx<R>* __re
   const int k0 = blockIdx.x * L;
   const int i3 = blockIdx.y;
   const int c = blockIdx.z;
-  const cx<R>* src = B2 + static_cast<size_t>(c) * n3 * K2 * K1;
-  cx<R>* dst = B1 + static_cast<size_t>(c) * n3 * n2 * K1;
-  auto load = [&](int l, int i2) {
+  const int kl = k0 + static_cast<int>(threadIdx.x & (L - 1));  // this thread's k1
+  const bool kin = kl < K1;
+  // src points at the k2 = 0 row of this line's (i3, k1) column.
+  const cx<R>* src = B2 + ((static_cast<size_t>(c) * n3 + i3) * K2 + H2) * K1 + kl;
+  cx<R>* dst = B1 + (static_cast<size_t>(c) * n3 + i3) * n2 * K1 + kl;
+  auto load = [&](int, int i2) {
     int k2;
     if (i2 <= H2)
       k2 = i2;
@@ -232,11 +238,10 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_inv(const cx<R>* __re
       k2 = i2 - n2;
     else
       return mk(R(0), R(0));
-    return k0 + l < K1 ? src[(static_cast<size_t>(i3) * K2 + k2 + H2) * K1 + k0 + l]
-                       : mk(R(0), R(0));
+    return kin ? src[k2 * K1] : mk(R(0), R(0));
   };
-  auto store = [&](int l, int i2, cx<R> v, cx<R>*) {
-    if (k0 + l < K1) dst[(static_cast<size_t>(i3) * n2 + i2) * K1 + k0 + l] = v;
+  auto store = [&](int, int i2, cx<R> v, cx<R>*) {
+    if (kin) dst[i2 * K1] = v;
   };
   fft_edges<R, 1, L>(a, b, n2, plan, tw, load, store);
 }
@@ -260,17 +265,22 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_c2r(const cx<R>* __re
   const int pair0 = blockIdx.x * NP;
   const int c0 = blockIdx.y * NCG;
   const int npairs = nrows / 2;
-  auto load = [&](int line, int x) {
-    const int cc = line % NCG, pr = pair0 + line / NCG;
+  // Each thread serves one line: resolve its rows and output columns once.
+  const int line = static_cast<int>(threadIdx.x & (L - 1));
+  const int cc = line % NCG, pr = pair0 + line / NCG;
+  const bool valid = pr < npairs;
+  const cx<R>* sa = B1 + (static_cast<size_t>(c0 + cc) * nrows + 2 * static_cast<size_t>(pr)) * K1;
+  const cx<R>* sb = sa + K1;
+  R* oa = out + 2 * static_cast<size_t>(pr) * n1 * nc + c0 + cc;
+  R* ob = oa + static_cast<size_t>(n1) * nc;
+  auto load = [&](int, int x) {
     const bool lo = x < K1;
     const bool hi = x > n1 - K1;
     cx<R> fa = mk(R(0), R(0)), fb = mk(R(0), R(0));
-    if (pr < npairs && (lo || hi)) {
+    if (valid && (lo || hi)) {
       const int kx = lo ? x : n1 - x;
-      const cx<R>* src = B1 + static_cast<size_t>(c0 + cc) * nrows * K1;
-      const size_t ra = static_cast<size_t>(2 * pr);
-      fa = src[ra * K1 + kx];
-      fb = src[(ra + 1) * K1 + kx];
+      fa = sa[kx];
+      fb = sb[kx];
       if (x == 0) {
         fa.y = R(0);
         fb.y = R(0);
@@ -281,12 +291,10 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_c2r(const cx<R>* __re
     }
     return mk(fa.x - fb.y, fa.y + fb.x);
   };
-  auto store = [&](int line, int x, cx<R> v, cx<R>*) {
-    const int cc = line % NCG, pr = pair0 + line / NCG;
-    if (pr >= npairs) return;
-    const size_t ra = static_cast<size_t>(2 * pr);
-    out[(ra * n1 + x) * nc + c0 + cc] = v.x;
-    out[((ra + 1) * n1 + x) * nc + c0 + cc] = v.y;
+  auto store = [&](int, int x, cx<R> v, cx<R>*) {
+    if (!valid) return;
+    oa[x * nc] = v.x;
+    ob[x * nc] = v.y;
   };
   fft_edges<R, 1, L>(a, b, n1, plan, tw, load, store);
 }
