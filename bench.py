@@ -136,6 +136,21 @@ def stage_bytes(params, natoms, real_bytes, nc=4):
     }
 
 
+def stage_flops(params, natoms, nc=4):
+    """Algorithmic FP64 flops of the tensor-core stages: one multiply-add per
+    stencil point and component (gather: nc components; spread: one)."""
+    w = (2 * params["window_cutoff"] + 1) ** 3
+    return {"spread": 2 * natoms * w, "gather": 2 * natoms * w * nc}
+
+
+# DRAM bytes (read + write) per launch from one ncu capture of the 32,769-atom
+# workload (profiles/c3_water_32k_top_kernels.md), keyed by (real bytes, stage).
+DRAM_TRAFFIC = {
+    (8, "gather"): 746.37e6 + 62.96e6,
+    (8, "fft_x_c2r"): 356.31e6 + 660.39e6,
+}
+
+
 def load_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -289,6 +304,17 @@ def run_ours(args):
     eb.lib()
     pos, q, lat = workloads.c3_water_32k()
 
+    if args.profile_only:
+        # For profiler captures: warm-up + steps evaluations of one form, nothing
+        # timed, no JSON line (numbers taken under a profiler are not results).
+        prec, tol = (eb.FP64, TOL_FP64) if args.profile_only == "fp64" else (eb.MIXED, TOL_MIXED)
+        arm = Arm(eb, torch, device, prec, tol, pos, q, lat)
+        for _ in range(args.warmup + args.steps):
+            arm.step_device()
+        torch.cuda.synchronize()
+        print(f"profile-only: {args.warmup + args.steps} {args.profile_only} evaluations", flush=True)
+        return 0
+
     fp64 = Arm(eb, torch, device, eb.FP64, TOL_FP64, pos, q, lat)
     mixed = Arm(eb, torch, device, eb.MIXED, TOL_MIXED, pos, q, lat)
 
@@ -312,6 +338,7 @@ def run_ours(args):
             dist.barrier()
         torch.cuda.synchronize()
 
+    tensor_peak = fp64.ctx.fp64_mma_peak()
     sampler = ClockSampler(device)
     barrier()
     sampler.start()
@@ -354,25 +381,49 @@ def run_ours(args):
     peak, peak_kind = load_peaks()
     natoms = len(q)
 
-    def roofline(stages_ms, params, real_bytes, steps):
+    def roofline(stages_ms, params, real_bytes, steps, tensor_peak=None):
+        """Per-stage rates; the roofline entry is the stage with the largest time.
+        HBM-type stages (the FFT passes; every stage in the FP32 form) use
+        algorithmic bytes / time against the measured copy bandwidth.  The FP64
+        spread and gather run on the FP64 tensor cores (DMMA): algorithmic FP64
+        flops / time against the FP64 tensor rate measured live on this GPU."""
         sb = stage_bytes(params, natoms, real_bytes)
+        fl = stage_flops(params, natoms) if tensor_peak else {}
         per = {}
         for name, (ms, _) in stages_ms.items():
             if ms <= 0:
                 continue
             dur = ms / steps / 1e3
             entry = {"ms": ms / steps}
-            if name in sb:
+            if name in fl:
+                entry["tflops"] = fl[name] / dur / 1e12
+                entry["flops"] = fl[name]
+            elif name in sb:
                 entry["gbs"] = sb[name] / dur / 1e9
                 entry["bytes"] = sb[name]
             per[name] = entry
-        top = max((k for k in per if k in sb), key=lambda k: per[k]["ms"])
-        ach = per[top]["gbs"]
-        return top, per, {"bound": "hbm", "kernel": top, "achieved": ach, "peak": peak,
-                          "unit": "GB/s", "frac": ach / peak, "peak_source": f"{peak_kind} hbm_gbs",
-                          "traffic": None}
+        top = max((k for k in per if k in sb or k in fl), key=lambda k: per[k]["ms"])
+        traffic = DRAM_TRAFFIC.get((real_bytes, top))
+        if top in fl:
+            ach = per[top]["tflops"]
+            roof = {"bound": "tensor", "kernel": top, "achieved": ach, "peak": tensor_peak,
+                    "unit": "TFLOP/s", "frac": ach / tensor_peak,
+                    "peak_source": "measured live: dense FP64 DMMA m8n8k4 rate (ewg_fp64_mma_peak)",
+                    "traffic": traffic}
+        else:
+            ach = per[top]["gbs"]
+            roof = {"bound": "hbm", "kernel": top, "achieved": ach, "peak": peak, "unit": "GB/s",
+                    "frac": ach / peak, "peak_source": f"{peak_kind} hbm_gbs", "traffic": traffic}
+        return top, per, roof
 
-    top64, per64, roof64 = roofline(stages, params64, 8, args.steps)
+    def whole_eval(params, real_bytes, t_step):
+        """B_force = 19 G + 8 N s bytes per evaluation against the measured HBM rate."""
+        n = [2 * m for m in params["n_modes"]]
+        G = n[0] * n[1] * n[2] * real_bytes
+        b = 19 * G + 8 * natoms * real_bytes
+        return {"bytes": b, "achieved_gbs": b / t_step / 1e9, "frac": b / t_step / 1e9 / peak}
+
+    top64, per64, roof64 = roofline(stages, params64, 8, args.steps, tensor_peak)
     top32, per32, roof32 = roofline(stages32, params32, 4, args.steps)
     h2d = natoms * 3 * 8 + natoms * 8
     d2h = natoms * 8 + natoms * 3 * 8
@@ -389,6 +440,7 @@ def run_ours(args):
         "e2e": {"value": ws * args.steps / te64, "unit": "evals/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "roofline": roof64,
+        "whole_eval_hbm": whole_eval(params64, 8, t64 / args.steps),
         "stages_ms": per64,
         "mixed": {
             "value": ws * args.steps / t32, "unit": "evals/s", "tol": TOL_MIXED,
@@ -397,7 +449,8 @@ def run_ours(args):
             "speedup_vs_fp64": (ws * args.steps / t32) / value,
             "e2e": {"value": ws * args.steps / te32, "unit": "evals/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "rel_err_vs_fp64": err, "roofline": roof32, "stages_ms": per32,
+            "rel_err_vs_fp64": err, "roofline": roof32,
+            "whole_eval_hbm": whole_eval(params32, 4, t32 / args.steps), "stages_ms": per32,
             "gpu_launches": launches32,
         },
         "gpu_launches": launches64,
@@ -416,6 +469,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-only", choices=["fp64", "mixed"], default=None,
+                    help="run warm-up + steps evaluations of one form for a profiler; no timing")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -513,6 +513,15 @@ int ewg_set_stream(ewg_context* c, void* stream) {
 
 long long ewg_kernel_launches(const ewg_context* c) { return c ? c->launches : 0; }
 
+int ewg_fp64_mma_peak(ewg_context* c, double* tflops) {
+  if (!c || !tflops) return EWG_ERR_ARG;
+  cudaSetDevice(c->device);
+  const long long before = g_launches;
+  const int rc = measure_dmma_peak(c->stream, tflops);
+  c->launches += g_launches - before;
+  return rc;
+}
+
 int ewg_set_profiling(ewg_context* c, int on) {
   if (!c) return EWG_ERR_ARG;
   c->prof.on = on != 0;

@@ -162,6 +162,8 @@ MeshSizes mesh_sizes(const MeshGeom& g, const StencilDims& sd, int mixed, int nc
 
 // Shared-memory limits of the FFT and gather kernels (once per device).
 int mesh_configure_kernels();
+// Dense FP64 tensor-core (DMMA m8n8k4) rate of this GPU in TFLOP/s, timed on `st`.
+int measure_dmma_peak(cudaStream_t st, double* tflops);
 // EWG_ERR_GRID_TOO_LARGE when one line of an axis does not fit a pass CTA's shared
 // memory (a guard: every length up to kMaxFftLength fits in both precisions).
 int mesh_check_lengths(const MeshGeom& g, bool mixed);

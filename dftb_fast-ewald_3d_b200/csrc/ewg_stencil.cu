@@ -675,6 +675,24 @@ __global__ void k_gather_final(const int4* __restrict__ slot, const int* __restr
   }
 }
 
+// FP64 tensor-core throughput probe: every warp issues independent DMMAs on
+// register operands (eight accumulator pairs, no memory traffic), so the
+// measured rate is the m8n8k4 FP64 pipe's own.
+__global__ void __launch_bounds__(128) k_dmma_peak(int iters, double seed, double* sink) {
+  double acc[8][2];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) acc[i][0] = acc[i][1] = 0.0;
+  const double a = seed + 1.0e-9 * threadIdx.x, b = 1.0 - seed;
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) dmma_m8n8k4(acc[i][0], acc[i][1], a, b);
+  }
+  double t = 0.0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) t += acc[i][0] + acc[i][1];
+  if (t == -1.0) sink[threadIdx.x] = t;  // never true; keeps the work live
+}
+
 inline int blocks_for(long n, int threads) { return static_cast<int>((n + threads - 1) / threads); }
 
 }  // namespace
@@ -769,5 +787,29 @@ void launch_gather_final(const MeshPlan& mp, const int4* slot, const int* perm, 
 }
 
 int stencil_configure_kernels() { return EWG_OK; }
+
+int measure_dmma_peak(cudaStream_t st, double* tflops) {
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return EWG_ERR_CUDA;
+  const int blocks = 4 * nsm, threads = 128, iters = 4096;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return EWG_ERR_CUDA;
+  k_dmma_peak<<<blocks, threads, 0, st>>>(iters / 8, 0.25, nullptr);  // warm-up
+  cudaEventRecord(e0, st);
+  k_dmma_peak<<<blocks, threads, 0, st>>>(iters, 0.25, nullptr);
+  cudaEventRecord(e1, st);
+  g_launches += 2;
+  float ms = 0.0f;
+  const bool ok = cudaEventSynchronize(e1) == cudaSuccess &&
+                  cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && ms > 0.0f;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (!ok) return EWG_ERR_CUDA;
+  const double mmas = static_cast<double>(blocks) * (threads / 32) * iters * 8;
+  *tflops = mmas * 2.0 * 8 * 8 * 4 / (ms * 1e-3) / 1e12;
+  return EWG_OK;
+}
 
 }  // namespace ewg

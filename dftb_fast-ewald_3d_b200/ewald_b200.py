@@ -49,7 +49,7 @@ EXPORTED = [
     "ewg_set_coords", "ewg_set_charges", "ewg_shift", "ewg_shift_force", "ewg_stress",
     "ewg_last_stress_setup", "ewg_batch_potential_force", "ewg_set_profiling", "ewg_stage_count",
     "ewg_stage_name", "ewg_stage_times", "ewg_reset_stage_times", "ewg_set_stream",
-    "ewg_direct_potential_force_static",
+    "ewg_direct_potential_force_static", "ewg_fp64_mma_peak",
 ]
 
 
@@ -111,6 +111,7 @@ def lib():
     L.ewg_kernel_launches.argtypes = [vp]
     L.ewg_kernel_launches.restype = C.c_longlong
     L.ewg_last_params.argtypes = [vp, C.POINTER(Params)]
+    L.ewg_fp64_mma_peak.argtypes = [vp, dp]
     L.ewg_potential_force.argtypes = [vp, C.c_int, dp, dp, dp, C.c_double, dp, dp, C.POINTER(Overrides)]
     L.ewg_parameters.argtypes = [C.c_int, dp, dp, C.c_double, C.POINTER(Overrides), C.POINTER(Params)]
     L.ewg_grid_memory.argtypes = [C.c_int, dp, dp, C.c_double, C.POINTER(Overrides), dp]
@@ -224,6 +225,12 @@ class Context:
         if reset:
             _check(L.ewg_reset_stage_times(self._h))
         return {L.ewg_stage_name(i).decode(): (float(ms[i]), int(la[i])) for i in range(n)}
+
+    def fp64_mma_peak(self) -> float:
+        """Measured dense FP64 tensor-core rate of this context's GPU, TFLOP/s."""
+        v = C.c_double()
+        _check(lib().ewg_fp64_mma_peak(self._h, C.byref(v)))
+        return float(v.value)
 
     def last_params(self) -> dict:
         p = Params()

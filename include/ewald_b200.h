@@ -93,6 +93,11 @@ int ewg_set_stream(ewg_context* ctx, void* stream);
 long long ewg_kernel_launches(const ewg_context* ctx);
 /* Parameters the last evaluation on this context used. */
 int ewg_last_params(const ewg_context* ctx, ewg_params* out);
+/* Measured dense FP64 tensor-core rate of the context's GPU (DMMA m8n8k4 on
+ * register operands, all SMs, CUDA-event timed), in TFLOP/s: the roofline
+ * denominator of the FP64 spread and gather.  Diagnostic; no counterpart in
+ * the reference. */
+int ewg_fp64_mma_peak(ewg_context* ctx, double* tflops);
 
 /* ---- per-stage device timing ------------------------------------------- */
 /* With profiling on, every evaluation records CUDA events on the context's
