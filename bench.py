@@ -52,6 +52,22 @@ TOL_MIXED = 1e-7
 L2_FLUSH_BYTES = 256 << 20
 
 
+# Single-cell workloads: name -> (generator, label).  C3 is the headline; the
+# others fill the per-configuration table (seeded synthetic inputs, Bohr).
+SINGLE_CELL = {
+    "c3": (lambda: workloads.c3_water_32k(), "water_32769_atoms_68.91A_tol1e-10"),
+    "c1": (lambda: workloads.c1_small_cubic(), "random_64_atoms_12A_cubic_tol1e-10"),
+    "c2": (lambda: workloads.c2_random_4096(), "random_4096_atoms_35A_cubic_tol1e-10"),
+    "c5": (lambda: workloads.c5_rock_salt_216k(), "rock_salt_216000_sites_169.2A_tol1e-10"),
+}
+
+
+def metric_for(name, natoms):
+    if name == "c3":
+        return METRIC
+    return f"Coulomb shift+force evals/s at {natoms} atoms ({name}), mixed vs FP64; rel. err vs FP64"
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -183,20 +199,25 @@ def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
         return 0
-    pos, q, lat = workloads.c3_water_32k()
+    if args.workload not in SINGLE_CELL:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          f"the reference arm times single-cell workloads only, not {args.workload}"}))
+        return 0
+    gen, label = SINGLE_CELL[args.workload]
+    pos, q, lat = gen()
     threads = os.cpu_count() or 1
     times = cpu_evals(pos, q, lat, TOL_FP64, args.steps, args.warmup, threads)
     total = sum(times)
     value = args.steps / total
     line = {
-        "metric": METRIC, "value": value, "unit": "evals/s", "impl": "reference", "n_gpus": ws,
+        "metric": metric_for(args.workload, len(q)), "value": value, "unit": "evals/s",
+        "impl": "reference", "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "water_32769_atoms_68.91A_tol1e-10", "natoms": len(q), "tol": TOL_FP64,
-                   "grid": "280^3", "window_cutoff": 12},
+        "config": {"workload": label, "natoms": len(q), "tol": TOL_FP64},
         "cpu_baseline": {"value": value, "unit": "evals/s", "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} full C3 shift+force evaluations (oracle/ C++ "
+                         "sample": f"{args.steps} full {args.workload} shift+force evaluations (oracle/ C++ "
                                    f"restatement, OpenMP, project FFT in place of FFTW)"},
         "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -286,6 +307,75 @@ class Arm:
         return time.perf_counter() - t0
 
 
+def run_batched(args, eb, torch, device):
+    """C4: 256 independent triclinic cells (50-2000 atoms each) per step through
+    ewg_batch_potential_force from host arrays (copies inside the timed region)."""
+    cells = workloads.c4_batched_cells()
+    natoms = sum(len(c[1]) for c in cells)
+    out = {}
+    for name, prec, tol in (("fp64", eb.FP64, TOL_FP64), ("mixed", eb.MIXED, TOL_MIXED)):
+        ctx = eb.Context(device, prec)
+        for _ in range(args.warmup):
+            ctx.batch_potential_force(cells, tol)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ctx.batch_potential_force(cells, tol)
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / args.steps
+        out[name] = {"value": len(cells) / dt, "ms_per_step": 1e3 * dt,
+                     "launches_per_step": None}
+        ctx.close()
+    line = {"metric": "C4 batched cells: cell shift+force evals/s (256 cells, 50-2000 atoms)",
+            "value": out["fp64"]["value"], "unit": "cells/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": out["fp64"]["ms_per_step"],
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "timing": "host wall clock around the batch call, host arrays in and out",
+            "config": {"workload": "c4_256_triclinic_cells", "natoms_total": natoms,
+                       "tol": TOL_FP64},
+            "mixed": {"value": out["mixed"]["value"], "unit": "cells/s", "tol": TOL_MIXED,
+                      "ms_per_step": out["mixed"]["ms_per_step"]}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_scc(args, eb, torch, device):
+    """C5 SCC: 216,000-site rock salt, geometry fixed, 30 charge updates per step,
+    each followed by a shift (potential) evaluation through the TCoulomb-style
+    resident calls (ewg_set_charges + ewg_shift, host arrays)."""
+    pos, q, lat = workloads.c5_rock_salt_216k()
+    charges = [workloads.c5_charge_update(q, k) for k in range(30)]
+    out = {}
+    for name, prec, tol in (("fp64", eb.FP64, TOL_FP64), ("mixed", eb.MIXED, TOL_MIXED)):
+        ctx = eb.Context(device, prec)
+        ctx.set_lattice(np.asarray(lat).T)
+        ctx.set_coords(np.ascontiguousarray(np.asarray(pos)))
+        for k in range(min(args.warmup, 30)):
+            ctx.set_charges(charges[k])
+            ctx.shift(tol, len(q))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        nev = 0
+        for _ in range(args.steps):
+            for k in range(30):
+                ctx.set_charges(charges[k])
+                ctx.shift(tol, len(q))
+                nev += 1
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        out[name] = {"value": nev / dt, "ms_per_eval": 1e3 * dt / nev}
+        ctx.close()
+    line = {"metric": "C5 SCC: shift evals/s at 216,000 sites, fixed geometry, 30 charge updates",
+            "value": out["fp64"]["value"], "unit": "evals/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 30 * out["fp64"]["ms_per_eval"],
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "timing": "host wall clock around set_charges + shift, host arrays in and out",
+            "config": {"workload": "c5_rock_salt_216000_scc30", "natoms": len(q), "tol": TOL_FP64},
+            "mixed": {"value": out["mixed"]["value"], "unit": "evals/s", "tol": TOL_MIXED}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_ours(args):
     import torch
 
@@ -302,7 +392,12 @@ def run_ours(args):
     device = local
     torch.cuda.set_device(device)
     eb.lib()
-    pos, q, lat = workloads.c3_water_32k()
+    if args.workload == "c4":
+        return run_batched(args, eb, torch, device)
+    if args.workload == "c5_scc":
+        return run_scc(args, eb, torch, device)
+    gen, label = SINGLE_CELL[args.workload]
+    pos, q, lat = gen()
 
     if args.profile_only:
         # For profiler captures: warm-up + steps evaluations of one form, nothing
@@ -369,7 +464,7 @@ def run_ours(args):
         threads = os.cpu_count() or 1
         times = cpu_evals(pos, q, lat, TOL_FP64, 1, 0, threads)
         cpu = {"value": 1.0 / times[0], "unit": "evals/s", "cores": threads, "kind": "port",
-               "sample": "1 full 32,769-atom shift+force evaluation at tol 1e-10 (oracle/ C++ "
+               "sample": f"1 full {len(q)}-atom shift+force evaluation at tol 1e-10 (oracle/ C++ "
                          "restatement of the reference, OpenMP, project FFT in place of FFTW)"}
 
     if dist:
@@ -429,10 +524,11 @@ def run_ours(args):
     d2h = natoms * 8 + natoms * 3 * 8
     value = ws * args.steps / t64
     line = {
-        "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": ws, "steps": args.steps,
+        "metric": metric_for(args.workload, natoms), "value": value, "unit": "evals/s", "n_gpus": ws,
+        "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t64 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "water_32769_atoms_68.91A_tol1e-10", "natoms": natoms,
+        "config": {"workload": label, "natoms": natoms,
                    "tol": TOL_FP64, "grid": "x".join(str(2 * m) for m in params64["n_modes"]),
                    "window_cutoff": params64["window_cutoff"], "alpha": params64["alpha"],
                    "r_cut_bohr": params64["r_cut"], "parallelism": f"replicas x{ws}",
@@ -469,6 +565,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["c3", "c1", "c2", "c5", "c4", "c5_scc"], default="c3",
+                    help="c3 (default, the headline) or another configuration of the table")
     ap.add_argument("--profile-only", choices=["fp64", "mixed"], default=None,
                     help="run warm-up + steps evaluations of one form for a profiler; no timing")
     args = ap.parse_args()

@@ -24,7 +24,7 @@ enum BufId {
   B_POS, B_Q, B_POT, B_FORCE, B_POT_SR, B_F_SR, B_S4, B_S4S, B_BOXKEY, B_MC, B_MCS, B_FR, B_FRS,
   B_TILEKEY, B_COUNTS, B_CURSOR, B_BOXSTART, B_TILESTART, B_TMP, B_PERMBOX, B_PERMMESH, B_WTAB,
   B_QK, B_GRID, B_A1, B_A2, B_B2, B_B1, B_OUT, B_ERR, B_SUMS, B_PARTIAL, B_KVEC, B_SK, B_WK,
-  B_P6, B_O6, B_COORDS, B_SLOT, B_PART, B_PAIRTMP, B_PAIRS, B_PAIRSTART, B_COUNT
+  B_P6, B_O6, B_COORDS, B_SLOT, B_PART, B_PAIRTMP, B_PAIRS, B_PAIRSTART, B_CELLERR, B_COUNT
 };
 
 struct DevBuf {
@@ -293,9 +293,12 @@ void stencil_dims(const MeshGeom& g, StencilDims& sd) {
 
 // Shared evaluation of ewald_potential_force on device-resident inputs.
 // pos: element (i, d) at pos[i * sa + d * sd]; q on device; outputs on device.
+// With err_flag (a zeroed device int) the coincident-charge flag goes there and
+// the call returns without waiting for the GPU (the caller reads the flag
+// later); otherwise the call completes on the GPU before it returns.
 int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const double* q,
              const Cell& cell, const ewg_params& p, bool want_force, double* pot, double* force,
-             bool resident) {
+             bool resident, int* err_flag = nullptr) {
   int rc = EWG_OK;
   cudaStream_t st = c->stream;
   const int mixed = c->precision == EWG_PRECISION_MIXED;
@@ -349,7 +352,7 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
   int4* pairtmp = dbuf<int4>(c, B_PAIRTMP, npairs_max, &rc);
   int2* pairs = dbuf<int2>(c, B_PAIRS, npairs_max, &rc);
   int* pairstart = dbuf<int>(c, B_PAIRSTART, ntiles + 1, &rc);
-  int* err = dbuf<int>(c, B_ERR, 1, &rc);
+  int* err = err_flag ? err_flag : dbuf<int>(c, B_ERR, 1, &rc);
   if (rc) return rc;
 
   if (!resident) c->resident.coords_version = -1;  // sorted layouts are about to be overwritten
@@ -358,7 +361,7 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
                      c->resident.nb[2] == rg.nb[2] && c->resident.ng[0] == mp.g.n[0] &&
                      c->resident.ng[1] == mp.g.n[1] && c->resident.ng[2] == mp.g.n[2] &&
                      c->resident.m == mp.g.m && c->resident.mixed == mixed;
-  cudaMemsetAsync(err, 0, sizeof(int), st);
+  if (!err_flag) cudaMemsetAsync(err, 0, sizeof(int), st);
   prof_mark(mp.prof, st, ST_PREP);
   if (!reuse) {
     launch_atom_prep(pos, sa, sd, q, n, cell, rg.nb, mp.g.n, kTiles, mp.sd.ntiles, s4, boxkey, mcv,
@@ -403,6 +406,12 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
   launch_gather_final(mp, slot, permmesh, part, nc, n, q, self_coef, pot_sr, f_sr, pot,
                       want_force ? force : nullptr, st);
   prof_mark(mp.prof, st, -1);
+  if (err_flag && !c->prof.on) {  // deferred: the caller synchronises and reads the flag
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) return cuda_status(le);
+    c->last = p;
+    return EWG_OK;
+  }
   int herr = 0;
   cudaError_t e = cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -947,9 +956,14 @@ int ewg_batch_potential_force(ewg_context* c, int n_cells, const int* offsets, c
   double* dq = dbuf<double>(c, B_Q, std::max(total, 1), &rc);
   double* dpot = dbuf<double>(c, B_POT, std::max(total, 1), &rc);
   double* dforce = dbuf<double>(c, B_FORCE, 3 * static_cast<size_t>(std::max(total, 1)), &rc);
+  // One coincident-charge flag per cell, read once at the end: the cells'
+  // evaluations are queued back to back on the stream with no host wait.
+  int* cellerr = dbuf<int>(c, B_CELLERR, std::max(n_cells, 1), &rc);
   if (rc) return rc;
+  cudaMemsetAsync(cellerr, 0, sizeof(int) * std::max(n_cells, 1), c->stream);
   cudaMemcpyAsync(dcoords, coords, sizeof(double) * 3 * total, cudaMemcpyHostToDevice, c->stream);
   cudaMemcpyAsync(dq, charges, sizeof(double) * total, cudaMemcpyHostToDevice, c->stream);
+  std::vector<int> status(n_cells, EWG_OK);
   for (int cidx = 0; cidx < n_cells; ++cidx) {
     const int a0 = offsets[cidx], na = offsets[cidx + 1] - a0;
     Cell cell;
@@ -961,15 +975,24 @@ int ewg_batch_potential_force(ewg_context* c, int n_cells, const int* offsets, c
     if (!s) s = choose_parameters(cell, q2, na, tol, nullptr, p);
     if (!s)
       s = evaluate(c, na, dcoords + 3 * static_cast<size_t>(a0), 3, 1, dq + a0, cell, p,
-                   force != nullptr, dpot + a0, dforce + 3 * static_cast<size_t>(a0), false);
-    if (cell_status) cell_status[cidx] = s;
-    if (s && !first) first = s;
+                   force != nullptr, dpot + a0, dforce + 3 * static_cast<size_t>(a0), false,
+                   cellerr + cidx);
+    status[cidx] = s;
   }
+  std::vector<int> herr(std::max(n_cells, 1), 0);
   cudaError_t e = cudaMemcpyAsync(pot, dpot, sizeof(double) * total, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess && force)
     e = cudaMemcpyAsync(force, dforce, sizeof(double) * 3 * total, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(herr.data(), cellerr, sizeof(int) * n_cells, cudaMemcpyDeviceToHost,
+                        c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_status(e);
+  for (int cidx = 0; cidx < n_cells; ++cidx) {
+    if (status[cidx] == EWG_OK && herr[cidx]) status[cidx] = EWG_ERR_COINCIDENT;
+    if (cell_status) cell_status[cidx] = status[cidx];
+    if (status[cidx] && !first) first = status[cidx];
+  }
   return first;
 }
 
