@@ -24,7 +24,8 @@ enum BufId {
   B_POS, B_Q, B_POT, B_FORCE, B_POT_SR, B_F_SR, B_S4, B_S4S, B_BOXKEY, B_MC, B_MCS, B_FR, B_FRS,
   B_TILEKEY, B_COUNTS, B_CURSOR, B_BOXSTART, B_TILESTART, B_TMP, B_PERMBOX, B_PERMMESH, B_WTAB,
   B_QK, B_GRID, B_A1, B_A2, B_B2, B_B1, B_OUT, B_ERR, B_SUMS, B_PARTIAL, B_KVEC, B_SK, B_WK,
-  B_P6, B_O6, B_COORDS, B_SLOT, B_PART, B_PAIRTMP, B_PAIRS, B_PAIRSTART, B_CELLERR, B_COUNT
+  B_P6, B_O6, B_COORDS, B_SLOT, B_PART, B_PAIRTMP, B_PAIRS, B_PAIRSTART, B_CELLERR, B_ZPART,
+  B_COUNT
 };
 
 struct DevBuf {
@@ -298,7 +299,7 @@ void stencil_dims(const MeshGeom& g, StencilDims& sd) {
 // later); otherwise the call completes on the GPU before it returns.
 int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const double* q,
              const Cell& cell, const ewg_params& p, bool want_force, double* pot, double* force,
-             bool resident, int* err_flag = nullptr) {
+             bool resident, int* err_flag = nullptr, double* stress12 = nullptr) {
   int rc = EWG_OK;
   cudaStream_t st = c->stream;
   const int mixed = c->precision == EWG_PRECISION_MIXED;
@@ -396,9 +397,19 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
   }
   prof_mark(mp.prof, st, ST_REAL);
   launch_real_space(s4s, permbox, boxstart, n, rg, p.alpha, p.r_cut, mixed, pot_sr, f_sr, err, st);
+  double* zpart = nullptr;
+  if (stress12) {  // real-space virial over the same pairs, and z-pass partials zeroed
+    const size_t nz = 6 * static_cast<size_t>(mp.g.K1) * mp.g.K2;
+    double* p6 = dbuf<double>(c, B_P6, 6 * static_cast<size_t>(n), &rc);
+    zpart = dbuf<double>(c, B_ZPART, nz, &rc);
+    if (rc) return rc;
+    launch_real_stress(s4s, boxstart, n, rg, p.alpha, p.r_cut, p6, stress12, err, st);
+    cudaMemsetAsync(zpart, 0, sizeof(double) * nz, st);
+  }
   prof_mark(mp.prof, st, ST_SPREAD);
   launch_spread(mp, pairstart, pairs, wtab, qk, grid, st);
-  launch_forward_and_weight(mp, grid, A1, A2, B2, nc, st);
+  launch_forward_and_weight(mp, grid, A1, A2, B2, nc, st, zpart);
+  if (stress12) launch_sum_partials(zpart, mp.g.K1 * mp.g.K2, 6, stress12 + 6, st);
   launch_inverse(mp, B2, B1, outg, nc, st);
   const double self_coef = -2.0 * p.alpha / std::sqrt(kPi);
   prof_mark(mp.prof, st, ST_GATHER);
@@ -651,6 +662,48 @@ int ewg_potential_force(ewg_context* c, int n, const double* positions, const do
     e = cudaMemcpyAsync(force, dforce, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   return cuda_status(e);
+}
+
+int ewg_potential_force_stress(ewg_context* c, int n, const double* positions,
+                               const double* charges, const double* lat_rows, double tol,
+                               double* pot, double* force, double* sigma,
+                               const ewg_overrides* ov) {
+  if (!c) return EWG_ERR_ARG;
+  LaunchScope scope(c);
+  c->uploaded_charges = -1;
+  c->resident.coords_version = -1;
+  Cell cell;
+  double q2 = 0.0;
+  int rc = validate_host(n, positions, charges, lat_rows, tol, cell, q2);
+  if (rc) return rc;
+  if (!pot || !sigma) return EWG_ERR_ARG;
+  ewg_params p;
+  rc = choose_parameters(cell, q2, n, tol, ov, p);
+  if (rc) return rc;
+  double* dpos = dbuf<double>(c, B_POS, 3 * static_cast<size_t>(n), &rc);
+  double* dq = dbuf<double>(c, B_Q, n, &rc);
+  double* dpot = dbuf<double>(c, B_POT, n, &rc);
+  double* dforce = dbuf<double>(c, B_FORCE, 3 * static_cast<size_t>(n), &rc);
+  double* s12 = dbuf<double>(c, B_O6, 12, &rc);
+  if (rc) return rc;
+  cudaMemcpyAsync(dpos, positions, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(dq, charges, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream);
+  rc = evaluate(c, n, dpos, 1, n, dq, cell, p, force != nullptr, dpot, dforce, false, nullptr, s12);
+  if (rc) return rc;
+  double h[12];
+  cudaError_t e = cudaMemcpyAsync(pot, dpot, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && force)
+    e = cudaMemcpyAsync(force, dforce, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h, s12, sizeof(h), cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_status(e);
+  // sigma = (2/V) dE/d eps = (S_real + 2 dE_k/d eps) / V, S_real the full-list
+  // real-space virial sum (the stock invRStress convention, coulomb.F90:2861).
+  const double V = cell.volume;
+  const int map[3][3] = {{0, 3, 4}, {3, 1, 5}, {4, 5, 2}};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) sigma[i + 3 * j] = (h[map[i][j]] + 2.0 * h[6 + map[i][j]]) / V;
+  return EWG_OK;
 }
 
 int ewg_potential_force_device(ewg_context* c, int n, const double* coords_device,

@@ -69,6 +69,8 @@ void launch_real_space(const double4* s4_sorted, const int* perm, const int* box
 
 // Real-space virial of invRStress (coulomb.F90:2836-2905): per-atom partial
 // tensors (6 per atom) then a fixed-order sum into out6.
+// Fixed-order sum of np partial vectors of nv doubles (one CTA).
+void launch_sum_partials(const double* partial, int np, int nv, double* out, cudaStream_t st);
 void launch_real_stress(const double4* s4_sorted, const int* box_start, int n, const RealGeom& g,
                         double alpha, double max_r, double* partial6, double* out6, int* err,
                         cudaStream_t st);
@@ -136,8 +138,10 @@ void launch_spread(const MeshPlan& mp, const int* tile_start, const int2* pairs,
 // Pruned forward transform of the real grid to the compact spectrum, fused with
 // the influence weights and the first inverse pass: grid -> A1 -> A2 -> B2.
 // nc = 1 (potential) or 4 (potential and three force components).
+// stress_part (optional, K1 x K2 x 6 doubles, zeroed): per-CTA partials of the
+// reciprocal strain derivative, accumulated by the z pass.
 void launch_forward_and_weight(const MeshPlan& mp, const void* grid, void* A1, void* A2, void* B2,
-                               int nc, cudaStream_t st);
+                               int nc, cudaStream_t st, double* stress_part = nullptr);
 
 // Remaining inverse passes B2 -> B1 -> interleaved real grids (nc per point).
 void launch_inverse(const MeshPlan& mp, const void* B2, void* B1, void* out, int nc, cudaStream_t st);

@@ -124,6 +124,9 @@ struct InfluenceArgs {
   double prefactor;    // 4 pi / V
   double inv4a2;       // 1 / (4 alpha^2)
   const double* corr2[3];
+  // Optional: per-CTA partial of the reciprocal strain derivative dE_k/d eps
+  // (xx, yy, zz, xy, xz, yz), 6 doubles at (blockIdx.y * gridDim.x + blockIdx.x) * 6.
+  double* stress;
 };
 
 template <typename R, int L>
@@ -145,6 +148,12 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
   const size_t zstride = static_cast<size_t>(K2) * K1;
   const cx<R>* src = A2 + static_cast<size_t>(k2i) * K1 + kl;
   auto load_fwd = [&](int, int i3) { return kin ? src[i3 * zstride] : mk(R(0), R(0)); };
+  // Reciprocal strain derivative of E_k = sum_k 1/2 w(k) |G(k)|^2 (w with the
+  // deconvolution f^2 and the Nyquist factor c(k)): under a homogeneous strain
+  // k -> (1 - eps) k and V -> V (1 + tr eps), so each mode adds
+  // 1/2 w |G|^2 (2 k_a k_b (1/(4 alpha^2) + 1/k^2) - delta_ab); modes with k1 > 0
+  // stand for the pair (k, -k).
+  double sv[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   // Weight each mode of the closed box as it leaves the forward transform.
   auto store_weighted = [&](int l, int e, cx<R> g, cx<R>*) {
     int k3;
@@ -171,6 +180,17 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
         const double cw = 0.5 * (inS + inMinusS);
         wt = cw * ia.prefactor * exp(-kk2 * ia.inv4a2) / kk2 * ia.corr2[0][k1 + h1] *
              ia.corr2[1][k2 + h2] * ia.corr2[2][k3 + h3];
+        if (ia.stress) {
+          const double gx = static_cast<double>(g.x), gy = static_cast<double>(g.y);
+          const double e = (k1 > 0 ? 1.0 : 0.5) * wt * (gx * gx + gy * gy);
+          const double f = 2.0 * (ia.inv4a2 + 1.0 / kk2);
+          sv[0] += e * (f * kv[0] * kv[0] - 1.0);
+          sv[1] += e * (f * kv[1] * kv[1] - 1.0);
+          sv[2] += e * (f * kv[2] * kv[2] - 1.0);
+          sv[3] += e * f * kv[0] * kv[1];
+          sv[4] += e * f * kv[0] * kv[2];
+          sv[5] += e * f * kv[1] * kv[2];
+        }
       }
     }
     q[(k3 + h3) * L + l] = mk(static_cast<R>(wt * static_cast<double>(g.x)),
@@ -178,6 +198,22 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
   };
   fft_edges<R, -1, L>(a, b, n3, plan, tw, load_fwd, store_weighted);
   __syncthreads();
+  if (ia.stress) {  // fixed-order CTA sum: shuffle tree per warp, then warps in order
+    __shared__ double sred[32][6];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) sv[j] += __shfl_xor_sync(0xffffffffu, sv[j], off);
+      if (lane == 0) sred[warp][j] = sv[j];
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+      double t = 0.0;
+      for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t += sred[w][threadIdx.x];
+      ia.stress[(static_cast<size_t>(blockIdx.y) * gridDim.x + blockIdx.x) * 6 + threadIdx.x] = t;
+    }
+  }
   for (int c = 0; c < nc; ++c) {
     R kc1 = R(0), kc2 = R(0), kc3 = R(0);
     if (c > 0) {
@@ -332,7 +368,7 @@ void with_lines(int L, F&& f) {
 
 template <typename R>
 void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, void* B2v, int nc,
-                  cudaStream_t st) {
+                  double* stress_part, cudaStream_t st) {
   const MeshGeom& g = mp.g;
   const int n1 = g.n[0], n2 = g.n[1], n3 = g.n[2];
   cx<R>* A1 = static_cast<cx<R>*>(A1v);
@@ -377,6 +413,7 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
     ia.prefactor = 4.0 * kPi / g.volume;
     ia.inv4a2 = 1.0 / (4.0 * (g.alpha * g.alpha));
     for (int d = 0; d < 3; ++d) ia.corr2[d] = mp.corr2[d];
+    ia.stress = stress_part;
     const int L = pick_lines(n3, cb, g.K3);
     const size_t sm = pass_smem(n3, L, cb, g.K3);
     dim3 grd((g.K1 + L - 1) / L, g.K2);
@@ -472,11 +509,11 @@ int mesh_configure_kernels() {
 }
 
 void launch_forward_and_weight(const MeshPlan& mp, const void* grid, void* A1, void* A2, void* B2,
-                               int nc, cudaStream_t st) {
+                               int nc, cudaStream_t st, double* stress_part) {
   if (mp.mixed)
-    forward_impl<float>(mp, grid, A1, A2, B2, nc, st);
+    forward_impl<float>(mp, grid, A1, A2, B2, nc, stress_part, st);
   else
-    forward_impl<double>(mp, grid, A1, A2, B2, nc, st);
+    forward_impl<double>(mp, grid, A1, A2, B2, nc, stress_part, st);
 }
 
 void launch_inverse(const MeshPlan& mp, const void* B2, void* B1, void* out, int nc,

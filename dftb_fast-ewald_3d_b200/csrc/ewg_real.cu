@@ -618,6 +618,11 @@ void launch_real_stress(const double4* srt, const int* box_start, int n, const R
   g_launches += 2;
 }
 
+void launch_sum_partials(const double* partial, int np, int nv, double* out, cudaStream_t st) {
+  k_sum_partials<<<1, 256, 0, st>>>(partial, np, nv, out);
+  ++g_launches;
+}
+
 void launch_structure_factors(const double* coords3n, const double* q, int n, const double* kvec,
                               int nk, double* out, cudaStream_t st) {
   if (nk == 0) return;

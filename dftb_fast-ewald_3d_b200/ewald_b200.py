@@ -49,7 +49,7 @@ EXPORTED = [
     "ewg_set_coords", "ewg_set_charges", "ewg_shift", "ewg_shift_force", "ewg_stress",
     "ewg_last_stress_setup", "ewg_batch_potential_force", "ewg_set_profiling", "ewg_stage_count",
     "ewg_stage_name", "ewg_stage_times", "ewg_reset_stage_times", "ewg_set_stream",
-    "ewg_direct_potential_force_static", "ewg_fp64_mma_peak",
+    "ewg_direct_potential_force_static", "ewg_fp64_mma_peak", "ewg_potential_force_stress",
 ]
 
 
@@ -113,6 +113,8 @@ def lib():
     L.ewg_last_params.argtypes = [vp, C.POINTER(Params)]
     L.ewg_fp64_mma_peak.argtypes = [vp, dp]
     L.ewg_potential_force.argtypes = [vp, C.c_int, dp, dp, dp, C.c_double, dp, dp, C.POINTER(Overrides)]
+    L.ewg_potential_force_stress.argtypes = [vp, C.c_int, dp, dp, dp, C.c_double, dp, dp, dp,
+                                             C.POINTER(Overrides)]
     L.ewg_parameters.argtypes = [C.c_int, dp, dp, C.c_double, C.POINTER(Overrides), C.POINTER(Params)]
     L.ewg_grid_memory.argtypes = [C.c_int, dp, dp, C.c_double, C.POINTER(Overrides), dp]
     L.ewg_device_memory.argtypes = [C.c_int, dp, dp, C.c_double, C.POINTER(Overrides), C.c_int,
@@ -249,6 +251,21 @@ class Context:
         _check(lib().ewg_potential_force(self._h, n, _dp(pos), _dp(q), _dp(lat), float(tol), _dp(pot),
                                          _dp(force) if want_force else None, C.byref(o)))
         return (pot, force) if want_force else pot
+
+    def potential_force_stress(self, positions, charges, latVecs, tol=1e-10, **ov):
+        """Potential, force and the NFFT-based stress sigma = (2/V) dE/d(strain)
+        (3 x 3, the invRStress convention) of one evaluation."""
+        q = np.ascontiguousarray(charges, dtype=np.float64)
+        n = q.shape[0]
+        pos = _positions_fortran(positions, n)
+        lat = _lat_fortran(latVecs)
+        pot = np.empty(n)
+        force = np.empty((n, 3))
+        sigma = np.empty((3, 3), order="F")
+        o = _overrides(**ov)
+        _check(lib().ewg_potential_force_stress(self._h, n, _dp(pos), _dp(q), _dp(lat), float(tol),
+                                                _dp(pot), _dp(force), _dp(sigma), C.byref(o)))
+        return pot, force, np.array(sigma)
 
     def potential_force_device(self, coords, charges, latVecs, tol, pot, force=None, **ov):
         """All of coords (N,3) atom-major, charges, pot, force (N,3) are CUDA

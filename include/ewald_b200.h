@@ -120,6 +120,20 @@ int ewg_potential_force(ewg_context* ctx, int n, const double* positions, const 
                         const double* lat_rows, double tol, double* pot, double* force,
                         const ewg_overrides* ov);
 
+/* ewald_potential_force plus the stress of the same evaluation, from the same
+ * NFFT spectrum: sigma (3 x 3, column-major, symmetric) = (2/V) dE/d(strain)
+ * with E = 1/2 sum_i q_i pot_i, the quantity invRStress returns
+ * (dftb/coulomb.F90:2777-2863; the caller does stress -= 0.5 sigma).  Real
+ * space: the virial of the erfc pair term over the evaluation's own pairs;
+ * reciprocal space: sum_k 1/2 w(k) |G(k)|^2 (2 k k (1/(4 alpha^2) + 1/k^2) - 1)
+ * over the NFFT modes.  It uses the fast path's alpha and cutoffs, not the stock
+ * engine's.  The reference lists this as its next step for the fast path
+ * (fft3d_readme.md:30); it has no implementation to compare with. */
+int ewg_potential_force_stress(ewg_context* ctx, int n, const double* positions,
+                               const double* charges, const double* lat_rows, double tol,
+                               double* pot, double* force, double* sigma,
+                               const ewg_overrides* ov);
+
 /* ewald_parameters (fft/ewald_fft_3d.f90:142-191); host only. */
 int ewg_parameters(int n, const double* charges, const double* lat_rows, double tol,
                    const ewg_overrides* ov, ewg_params* out);
