@@ -867,8 +867,9 @@ int ewg_set_charges(ewg_context* c, const double* dq) {
 }
 
 namespace {
-int coulomb_eval(ewg_context* c, double tol, double* shift, double* force) {
-  if (!c || !shift) return EWG_ERR_ARG;
+int coulomb_eval(ewg_context* c, double tol, double* shift, double* force,
+                 double* sigma = nullptr) {
+  if (!c || (!shift && !sigma)) return EWG_ERR_ARG;
   LaunchScope scope(c);
   if (!c->has_coords || !c->has_charges) return EWG_ERR_STATE;
   if (!(tol > 0.0 && tol < 1.0)) tol = 1.0e-9;  // coulomb.F90:348-349
@@ -886,6 +887,7 @@ int coulomb_eval(ewg_context* c, double tol, double* shift, double* force) {
   double* dq = dbuf<double>(c, B_Q, n, &rc);
   double* dpot = dbuf<double>(c, B_POT, n, &rc);
   double* dforce = dbuf<double>(c, B_FORCE, 3 * static_cast<size_t>(n), &rc);
+  double* s12 = sigma ? dbuf<double>(c, B_O6, 12, &rc) : nullptr;
   if (rc) return rc;
   if (c->resident.coords_version != c->coords_version)
     cudaMemcpyAsync(dcoords, c->coords.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice,
@@ -894,20 +896,37 @@ int coulomb_eval(ewg_context* c, double tol, double* shift, double* force) {
     cudaMemcpyAsync(dq, c->dq.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->stream);
     c->uploaded_charges = c->charges_version;
   }
-  rc = evaluate(c, n, dcoords, 3, 1, dq, cell, p, force != nullptr, dpot, dforce, true);
+  rc = evaluate(c, n, dcoords, 3, 1, dq, cell, p, force != nullptr, dpot, dforce, true, nullptr,
+                s12);
   if (rc) {
     c->resident.coords_version = -1;
     return rc;
   }
-  cudaError_t e = cudaMemcpyAsync(shift, dpot, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream);
+  double h[12];
+  cudaError_t e = cudaSuccess;
+  if (shift) e = cudaMemcpyAsync(shift, dpot, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess && force)
     e = cudaMemcpyAsync(force, dforce, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess && sigma)
+    e = cudaMemcpyAsync(h, s12, sizeof(h), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-  return cuda_status(e);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (sigma) {  // (2/V) dE/d eps, as in ewg_potential_force_stress
+    const int map[3][3] = {{0, 3, 4}, {3, 1, 5}, {4, 5, 2}};
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        sigma[i + 3 * j] = (h[map[i][j]] + 2.0 * h[6 + map[i][j]]) / cell.volume;
+  }
+  return EWG_OK;
 }
 }  // namespace
 
 int ewg_shift(ewg_context* c, double tol, double* shift) { return coulomb_eval(c, tol, shift, nullptr); }
+
+int ewg_stress_fast(ewg_context* c, double tol, double* sigma) {
+  if (!sigma) return EWG_ERR_ARG;
+  return coulomb_eval(c, tol, nullptr, nullptr, sigma);
+}
 
 int ewg_shift_force(ewg_context* c, double tol, double* shift, double* force) {
   if (!force) return EWG_ERR_ARG;

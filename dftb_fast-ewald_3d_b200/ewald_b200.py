@@ -50,6 +50,7 @@ EXPORTED = [
     "ewg_last_stress_setup", "ewg_batch_potential_force", "ewg_set_profiling", "ewg_stage_count",
     "ewg_stage_name", "ewg_stage_times", "ewg_reset_stage_times", "ewg_set_stream",
     "ewg_direct_potential_force_static", "ewg_fp64_mma_peak", "ewg_potential_force_stress",
+    "ewg_stress_fast",
 ]
 
 
@@ -128,6 +129,7 @@ def lib():
     L.ewg_shift.argtypes = [vp, C.c_double, dp]
     L.ewg_shift_force.argtypes = [vp, C.c_double, dp, dp]
     L.ewg_stress.argtypes = [vp, C.c_double, C.c_double, dp]
+    L.ewg_stress_fast.argtypes = [vp, C.c_double, dp]
     L.ewg_last_stress_setup.argtypes = [vp, dp, dp, dp, ip]
     L.ewg_batch_potential_force.argtypes = [vp, C.c_int, ip, dp, dp, dp, C.c_double, dp, dp, ip]
     L.ewg_set_profiling.argtypes = [vp, C.c_int]
@@ -337,6 +339,12 @@ class Context:
         _check(lib().ewg_shift_force(self._h, float(tol), _dp(out), _dp(f)))
         return out, f
 
+    def stress_fast(self, tol):
+        """NFFT-based stress (2/V) dE/d(strain) of the resident state."""
+        s = np.empty(9)
+        _check(lib().ewg_stress_fast(self._h, float(tol), _dp(s)))
+        return s.reshape(3, 3, order="F")
+
     def stress(self, tol_ewald, alpha=0.0):
         s = np.empty(9)
         _check(lib().ewg_stress(self._h, float(tol_ewald), float(alpha), _dp(s)))
@@ -445,11 +453,14 @@ class TCoulomb:
     outside (0,1) select 1e-9 for the fast engine (coulomb.F90:348-349).
     ``DFTB_EWALD_DIRECT=1`` swaps in the direct engine at
     ``DFTB_EWALD_DIRECT_TOL`` (coulomb.F90:267-317), as the reference adapter does.
+    ``fastStress=True`` (or ``DFTB_EWALD_STRESS_FAST=1``) makes addStress use the
+    NFFT-based stress of the fast engine instead of the stock invRStress.
     """
 
     def __init__(self, nAtom: int, tolEwald: float = 1.0e-9, ewaldAlpha: float = 0.0,
-                 device: int = 0, precision: int = FP64):
+                 device: int = 0, precision: int = FP64, fastStress: bool = False):
         self.nAtom = int(nAtom)
+        self.fastStress = bool(fastStress) or _env_flag("DFTB_EWALD_STRESS_FAST")
         self.tolEwald = float(tolEwald)
         self.alpha = float(ewaldAlpha)
         self.ctx = Context(device, precision)
@@ -542,6 +553,9 @@ class TCoulomb:
         """coulomb.F90:721-757: stress -= 0.5 * invRStress(...)."""
         if not (self.coordsUpdated and self.chargesUpdated):
             raise EwaldError(16, "addStress before updateCoords/updateCharges")
-        sigma = self.ctx.stress(self.tolEwald, self.alpha)
+        if self.fastStress:
+            sigma = self.ctx.stress_fast(self._tol())
+        else:
+            sigma = self.ctx.stress(self.tolEwald, self.alpha)
         stress -= 0.5 * sigma
         return stress

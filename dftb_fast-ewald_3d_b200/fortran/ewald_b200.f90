@@ -16,7 +16,7 @@ module ewald_b200
 
   public :: TEwaldGpu, ewaldGpuInit, ewaldGpuFinal
   public :: ewaldGpuSetLattice, ewaldGpuSetCoords, ewaldGpuSetCharges
-  public :: ewaldGpuShift, ewaldGpuShiftForce, ewaldGpuStress
+  public :: ewaldGpuShift, ewaldGpuShiftForce, ewaldGpuStress, ewaldGpuStressFast
   public :: ewaldGpuPotentialForce
   public :: EWG_PRECISION_FP64, EWG_PRECISION_MIXED
 
@@ -102,6 +102,14 @@ module ewald_b200
       real(c_double), intent(out) :: sigma(3, 3)
       integer(c_int) :: rc
     end function ewg_stress
+
+    function ewg_stress_fast(ctx, tol, sigma) bind(C, name="ewg_stress_fast") result(rc)
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), value :: tol
+      real(c_double), intent(out) :: sigma(3, 3)
+      integer(c_int) :: rc
+    end function ewg_stress_fast
 
     function ewg_potential_force(ctx, n, positions, charges, latRows, tol, pot, force, ov) &
         & bind(C, name="ewg_potential_force") result(rc)
@@ -197,6 +205,15 @@ contains
     real(c_double), intent(out) :: sigma(3, 3)
     call check(ewg_stress(this%ctx, tolEwald, alpha, sigma))
   end subroutine ewaldGpuStress
+
+  !> NFFT-based stress of the fast engine on the resident state; same convention as
+  !> ewaldGpuStress (the caller does stress = stress - 0.5 * sigma).
+  subroutine ewaldGpuStressFast(this, tol, sigma)
+    type(TEwaldGpu), intent(in) :: this
+    real(c_double), intent(in) :: tol
+    real(c_double), intent(out) :: sigma(3, 3)
+    call check(ewg_stress_fast(this%ctx, tol, sigma))
+  end subroutine ewaldGpuStressFast
 
   !> Same argument order as ewald_potential_force (fft/ewald_fft_3d.f90:36).
   subroutine ewaldGpuPotentialForce(this, positions, charges, nParticle, latVecs, tol, pot, force)

@@ -207,6 +207,15 @@ int ewg_shift(ewg_context* ctx, double tol, double* shift);
 /* fftEwaldAddGradients (coulomb.F90:361-385): shift(N) and the physical force
  * F(3,N); the adapter subtracts F from DFTB+'s gradient array. */
 int ewg_shift_force(ewg_context* ctx, double tol, double* shift, double* force);
+/* The NFFT-based stress of ewg_potential_force_stress on the state set by
+ * ewg_set_lattice / ewg_set_coords / ewg_set_charges (the fast path's own alpha
+ * and cutoffs at tolerance tol, <= 0 or >= 1 meaning 1e-9 as in fftEwaldShift):
+ * sigma = (2/V) dE/d(strain), the invRStress convention, so addStress can do
+ * stress -= 0.5 sigma with it instead of the stock engine.  Reuses the resident
+ * geometry like ewg_shift.  No counterpart in the reference (its next step for
+ * the fast path, fft3d_readme.md:30). */
+int ewg_stress_fast(ewg_context* ctx, double tol, double* sigma);
+
 /* invRStress (coulomb.F90:2777-2863) with the stock setup of updateLatVecs
  * (getOptimalAlphaEwald when alpha <= 0, getMaxREwald, getMaxGEwald,
  * getLatticePoints): sigma(3,3) column-major; TCoulomb%addStress then does

@@ -97,3 +97,18 @@ def test_c3_fast_stress_matches_stock_stress(ctx):
     ctx.set_charges(q)
     stock = ctx.stress(1e-10)
     assert rel_max(sigma, stock) < 1e-7, (sigma, stock)
+
+
+def test_tcoulomb_fast_stress_sequence(ewald_lib, ctx):
+    """The resident TCoulomb path (addStress with fastStress) equals the one-shot call."""
+    pos, q, lat = W.c2_random_4096()
+    n = len(q)
+    tc = ewald_lib.TCoulomb(n, tolEwald=1e-10, fastStress=True)
+    tc.updateLatVecs(lat.T)
+    tc.updateCoords(pos.T)
+    tc.updateCharges(q)
+    tc.updateShifts()
+    stress = np.zeros((3, 3))
+    tc.addStress(stress)
+    _, _, sigma = ctx.potential_force_stress(pos, q, lat, 1e-10)
+    assert rel_max(stress, -0.5 * sigma) < 1e-12
