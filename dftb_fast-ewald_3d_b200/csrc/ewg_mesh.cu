@@ -129,7 +129,7 @@ struct InfluenceArgs {
   double* stress;
 };
 
-template <typename R, int L>
+template <typename R, int L, bool STRESS>
 __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
     const cx<R>* __restrict__ A2, cx<R>* __restrict__ B2, int n3, int K1, int K2, int K3, int nc,
     InfluenceArgs ia, FftPlan plan) {
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
         const double cw = 0.5 * (inS + inMinusS);
         wt = cw * ia.prefactor * exp(-kk2 * ia.inv4a2) / kk2 * ia.corr2[0][k1 + h1] *
              ia.corr2[1][k2 + h2] * ia.corr2[2][k3 + h3];
-        if (ia.stress) {
+        if constexpr (STRESS) {
           const double gx = static_cast<double>(g.x), gy = static_cast<double>(g.y);
           const double e = (k1 > 0 ? 1.0 : 0.5) * wt * (gx * gx + gy * gy);
           const double f = 2.0 * (ia.inv4a2 + 1.0 / kk2);
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
   };
   fft_edges<R, -1, L>(a, b, n3, plan, tw, load_fwd, store_weighted);
   __syncthreads();
-  if (ia.stress) {  // fixed-order CTA sum: shuffle tree per warp, then warps in order
+  if constexpr (STRESS) {  // fixed-order CTA sum: shuffle tree per warp, then warps in order
     __shared__ double sred[32][6];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -419,8 +419,12 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
     dim3 grd((g.K1 + L - 1) / L, g.K2);
     with_lines(L, [&](auto lc) {
       constexpr int LL = decltype(lc)::value;
-      k_fft_z_influence<R, LL><<<grd, pass_threads(LL), sm, st>>>(A2, B2, n3, g.K1, g.K2, g.K3, nc, ia,
-                                                         mp.fft[2]);
+      if (stress_part)
+        k_fft_z_influence<R, LL, true><<<grd, pass_threads(LL), sm, st>>>(
+            A2, B2, n3, g.K1, g.K2, g.K3, nc, ia, mp.fft[2]);
+      else
+        k_fft_z_influence<R, LL, false><<<grd, pass_threads(LL), sm, st>>>(
+            A2, B2, n3, g.K1, g.K2, g.K3, nc, ia, mp.fft[2]);
     });
     ++g_launches;
   }
@@ -479,7 +483,8 @@ void allow_smem(K... kernels) {
 
 template <typename R, int L>
 void allow_lines() {
-  allow_smem(k_fft_x_r2c<R, L>, k_fft_y_fwd<R, L>, k_fft_z_influence<R, L>, k_fft_y_inv<R, L>,
+  allow_smem(k_fft_x_r2c<R, L>, k_fft_y_fwd<R, L>, k_fft_z_influence<R, L, false>,
+             k_fft_z_influence<R, L, true>, k_fft_y_inv<R, L>,
              k_fft_x_c2r<R, L, 1>);
 }
 
