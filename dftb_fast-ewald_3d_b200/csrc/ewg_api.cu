@@ -78,6 +78,10 @@ struct ewg_context {
   int precision = EWG_PRECISION_FP64;
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;
+  // Second stream for the real-space sum, which runs beside the mesh pipeline:
+  // forked from `stream` after the atom sort, joined before the final assembly.
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
   DevBuf buf[B_COUNT];
   std::map<int, FftEntry> ffts;
   std::map<std::tuple<int, int, int>, CorrEntry> corrs;
@@ -117,6 +121,9 @@ struct ewg_context {
     for (auto& kv : corrs) cudaFree(kv.second.dev);
     for (auto& e : prof.ev)
       if (e) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    if (join) cudaEventDestroy(join);
+    if (side) cudaStreamDestroy(side);
     if (own_stream) cudaStreamDestroy(own_stream);
   }
 };
@@ -395,17 +402,27 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
     prof_mark(mp.prof, st, ST_WEIGHTS);
     launch_weights(mp, mcs, frs, n, wtab, qk, slot, st);
   }
+  // The real-space sum (FP64 pipe and issue bound) runs on the side stream
+  // beside the mesh pipeline (memory and tensor bound) unless stages are being
+  // timed; it reads only the box-sorted atoms, written above on `st`.
+  const bool concurrent = !c->prof.on;
+  cudaStream_t rs = concurrent ? c->side : st;
+  if (concurrent) {
+    cudaEventRecord(c->fork, st);
+    cudaStreamWaitEvent(rs, c->fork, 0);
+  }
   prof_mark(mp.prof, st, ST_REAL);
-  launch_real_space(s4s, permbox, boxstart, n, rg, p.alpha, p.r_cut, mixed, pot_sr, f_sr, err, st);
+  launch_real_space(s4s, permbox, boxstart, n, rg, p.alpha, p.r_cut, mixed, pot_sr, f_sr, err, rs);
   double* zpart = nullptr;
   if (stress12) {  // real-space virial over the same pairs, and z-pass partials zeroed
     const size_t nz = 6 * static_cast<size_t>(mp.g.K1) * mp.g.K2;
     double* p6 = dbuf<double>(c, B_P6, 6 * static_cast<size_t>(n), &rc);
     zpart = dbuf<double>(c, B_ZPART, nz, &rc);
     if (rc) return rc;
-    launch_real_stress(s4s, boxstart, n, rg, p.alpha, p.r_cut, p6, stress12, err, st);
+    launch_real_stress(s4s, boxstart, n, rg, p.alpha, p.r_cut, p6, stress12, err, rs);
     cudaMemsetAsync(zpart, 0, sizeof(double) * nz, st);
   }
+  if (concurrent) cudaEventRecord(c->join, rs);
   prof_mark(mp.prof, st, ST_SPREAD);
   launch_spread(mp, pairstart, pairs, wtab, qk, grid, st);
   launch_forward_and_weight(mp, grid, A1, A2, B2, nc, st, zpart);
@@ -414,6 +431,7 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
   const double self_coef = -2.0 * p.alpha / std::sqrt(kPi);
   prof_mark(mp.prof, st, ST_GATHER);
   launch_gather(mp, pairstart, pairs, wtab, outg, nc, part, st);
+  if (concurrent) cudaStreamWaitEvent(st, c->join, 0);  // pot_sr, f_sr, err ready
   launch_gather_final(mp, slot, permmesh, part, nc, n, q, self_coef, pot_sr, f_sr, pot,
                       want_force ? force : nullptr, st);
   prof_mark(mp.prof, st, -1);
@@ -501,7 +519,10 @@ int ewg_create(ewg_context** out, int device, int precision) {
   auto* c = new ewg_context();
   c->device = device;
   c->precision = precision;
-  if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming) != cudaSuccess) {
     delete c;
     return EWG_ERR_CUDA;
   }
