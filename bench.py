@@ -237,7 +237,9 @@ class Arm:
         self.ctx = eb.Context(device, precision)
         # A dedicated (non-default) stream: the library launches on it and the
         # CUDA events that time the steps are recorded on it.
-        self.stream = torch.cuda.Stream(device=device)
+        # High priority: the library's real-space side stream (lowest priority)
+        # then fills the gaps between the mesh kernels.
+        self.stream = torch.cuda.Stream(device=device, priority=-1)
         self.ctx.set_stream(self.stream.cuda_stream)
         dev = f"cuda:{device}"
         self.n = len(q)

@@ -519,8 +519,13 @@ int ewg_create(ewg_context** out, int device, int precision) {
   auto* c = new ewg_context();
   c->device = device;
   c->precision = precision;
-  if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess ||
-      cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+  // The mesh pipeline's own stream gets the highest priority and the real-space
+  // side stream the lowest, so the latter's blocks fill the gaps between the
+  // mesh kernels rather than delay them.
+  int least = 0, greatest = 0;
+  cudaDeviceGetStreamPriorityRange(&least, &greatest);
+  if (cudaStreamCreateWithPriority(&c->own_stream, cudaStreamNonBlocking, greatest) != cudaSuccess ||
+      cudaStreamCreateWithPriority(&c->side, cudaStreamNonBlocking, least) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming) != cudaSuccess) {
     delete c;
