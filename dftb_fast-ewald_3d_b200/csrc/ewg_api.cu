@@ -25,7 +25,7 @@ enum BufId {
   B_TILEKEY, B_COUNTS, B_CURSOR, B_BOXSTART, B_TILESTART, B_TMP, B_PERMBOX, B_PERMMESH, B_WTAB,
   B_QK, B_GRID, B_A1, B_A2, B_B2, B_B1, B_OUT, B_ERR, B_SUMS, B_PARTIAL, B_KVEC, B_SK, B_WK,
   B_P6, B_O6, B_COORDS, B_SLOT, B_PART, B_PAIRTMP, B_PAIRS, B_PAIRSTART, B_CELLERR, B_ZPART,
-  B_COUNT
+  B_BCOUNTS, B_BCURSOR, B_BTMP, B_COUNT
 };
 
 struct DevBuf {
@@ -344,6 +344,10 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
   int* tmp = dbuf<int>(c, B_TMP, n, &rc);
   int* permbox = dbuf<int>(c, B_PERMBOX, n, &rc);
   int* permmesh = dbuf<int>(c, B_PERMMESH, n, &rc);
+  // the box sort runs on the side stream: scratch of its own
+  int* bcounts = dbuf<int>(c, B_BCOUNTS, nboxes, &rc);
+  int* bcursor = dbuf<int>(c, B_BCURSOR, nboxes, &rc);
+  int* btmp = dbuf<int>(c, B_BTMP, n, &rc);
   double* pot_sr = dbuf<double>(c, B_POT_SR, n, &rc);
   double* f_sr = dbuf<double>(c, B_F_SR, 3 * static_cast<size_t>(n), &rc);
   void* wtab = dbuf<char>(c, B_WTAB, ms.wtab, &rc);
@@ -370,12 +374,22 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
                      c->resident.ng[1] == mp.g.n[1] && c->resident.ng[2] == mp.g.n[2] &&
                      c->resident.m == mp.g.m && c->resident.mixed == mixed;
   if (!err_flag) cudaMemsetAsync(err, 0, sizeof(int), st);
+  // The real-space branch (box sort, permutation, erfc pair sum; FP64 pipe and
+  // issue bound) runs on the low-priority side stream beside the mesh pipeline
+  // (memory and tensor bound), forked after the atom preparation and joined
+  // before the final assembly.  With stage events on, everything runs in line.
+  const bool concurrent = !c->prof.on;
+  cudaStream_t rs = concurrent ? c->side : st;
   prof_mark(mp.prof, st, ST_PREP);
   if (!reuse) {
     launch_atom_prep(pos, sa, sd, q, n, cell, rg.nb, mp.g.n, kTiles, mp.sd.ntiles, s4, boxkey, mcv,
                      fr, tilekey, st);
-    launch_bucket_sort(boxkey, n, nboxes, counts, cursor, boxstart, tmp, permbox, st);
-    launch_permute4(s4, permbox, n, s4s, st);
+    if (concurrent) {
+      cudaEventRecord(c->fork, st);
+      cudaStreamWaitEvent(rs, c->fork, 0);
+    }
+    launch_bucket_sort(boxkey, n, nboxes, bcounts, bcursor, boxstart, btmp, permbox, rs);
+    launch_permute4(s4, permbox, n, s4s, rs);
     launch_bucket_sort(tilekey, n, ntiles, counts, cursor, tilestart, tmp, permmesh, st);
     launch_permute_int4(mcv, permmesh, n, mcs, st);
     launch_permute4(fr, permmesh, n, frs, st);
@@ -395,21 +409,16 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
     // Geometry unchanged: refresh only the charges in the sorted layouts.
     launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, nullptr, nullptr, nullptr, s4, nullptr,
                      nullptr, nullptr, nullptr, st);
-    launch_permute4(s4, permbox, n, s4s, st);
+    if (concurrent) {
+      cudaEventRecord(c->fork, st);
+      cudaStreamWaitEvent(rs, c->fork, 0);
+    }
+    launch_permute4(s4, permbox, n, s4s, rs);
     launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, mp.g.n, kTiles, mp.sd.ntiles, nullptr,
                      nullptr, mcv, fr, tilekey, st);
     launch_permute4(fr, permmesh, n, frs, st);
     prof_mark(mp.prof, st, ST_WEIGHTS);
     launch_weights(mp, mcs, frs, n, wtab, qk, slot, st);
-  }
-  // The real-space sum (FP64 pipe and issue bound) runs on the side stream
-  // beside the mesh pipeline (memory and tensor bound) unless stages are being
-  // timed; it reads only the box-sorted atoms, written above on `st`.
-  const bool concurrent = !c->prof.on;
-  cudaStream_t rs = concurrent ? c->side : st;
-  if (concurrent) {
-    cudaEventRecord(c->fork, st);
-    cudaStreamWaitEvent(rs, c->fork, 0);
   }
   prof_mark(mp.prof, st, ST_REAL);
   launch_real_space(s4s, permbox, boxstart, n, rg, p.alpha, p.r_cut, mixed, pot_sr, f_sr, err, rs);
