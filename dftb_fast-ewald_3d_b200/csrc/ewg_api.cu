@@ -25,7 +25,8 @@ enum BufId {
   B_TILEKEY, B_COUNTS, B_CURSOR, B_BOXSTART, B_TILESTART, B_TMP, B_PERMBOX, B_PERMMESH, B_WTAB,
   B_QK, B_GRID, B_A1, B_A2, B_B2, B_B1, B_OUT, B_ERR, B_SUMS, B_PARTIAL, B_KVEC, B_SK, B_WK,
   B_P6, B_O6, B_COORDS, B_SLOT, B_PART, B_PAIRTMP, B_PAIRS, B_PAIRSTART, B_CELLERR, B_ZPART,
-  B_BCOUNTS, B_BCURSOR, B_BTMP, B_COUNT
+  B_BCOUNTS, B_BCURSOR, B_BTMP, B_EXT_T, B_EXT_S, B_EXT_SQ, B_EXT_TQ, B_EXT_BLUR, B_EXT_R,
+  B_EXT_G, B_EXT_SF, B_EXT_SF2, B_EXT_OUT, B_EXT_OUT2, B_COUNT
 };
 
 struct DevBuf {
@@ -966,6 +967,158 @@ int ewg_stress_fast(ewg_context* c, double tol, double* sigma) {
 int ewg_shift_force(ewg_context* c, double tol, double* shift, double* force) {
   if (!force) return EWG_ERR_ARG;
   return coulomb_eval(c, tol, shift, force);
+}
+
+namespace {
+// updateLatVecs's stock Ewald setup (coulomb.F90:575-620) for the point-charge
+// routines: alpha (getOptimalAlphaEwald unless given), the half-space G vectors
+// and the cell translations of getCellTranslations (dftb/periodic.F90:227-263):
+// every index triple in [-(r_i + 1), r_i + 1], r_i = floor(maxR |b_i|), the
+// origin first, then the iterator's order (last index fastest).
+int ext_setup(ewg_context* c, const double* lat_cols, double tol_ewald, double alpha_in, Cell& cell,
+              ExtLattice& L) {
+  int rc = cell_from_cols(lat_cols, cell);
+  if (rc) return rc;
+  if (!(tol_ewald > 0.0)) return EWG_ERR_TOL;
+  StockSetup ss;
+  rc = stock_setup(cell, tol_ewald, alpha_in, ss);
+  if (rc) return rc;
+  int rng[3];
+  for (int d = 0; d < 3; ++d) rng[d] = static_cast<int>(std::floor(ss.max_r * cell.recLen[d])) + 1;
+  std::vector<double> R = {0.0, 0.0, 0.0};
+  for (int c1 = -rng[0]; c1 <= rng[0]; ++c1)
+    for (int c2 = -rng[1]; c2 <= rng[1]; ++c2)
+      for (int c3 = -rng[2]; c3 <= rng[2]; ++c3) {
+        if (c1 == 0 && c2 == 0 && c3 == 0) continue;
+        for (int d = 0; d < 3; ++d)
+          R.push_back(c1 * cell.lat[0][d] + c2 * cell.lat[1][d] + c3 * cell.lat[2][d]);
+      }
+  const int nR = static_cast<int>(R.size() / 3), nG = static_cast<int>(ss.g.size() / 3);
+  double* dR = dbuf<double>(c, B_EXT_R, R.size(), &rc);
+  double* dG = dbuf<double>(c, B_EXT_G, std::max<size_t>(ss.g.size(), 3), &rc);
+  double* dsf = dbuf<double>(c, B_EXT_SF, 2 * static_cast<size_t>(std::max(nG, 1)), &rc);
+  if (rc) return rc;
+  cudaMemcpyAsync(dR, R.data(), sizeof(double) * R.size(), cudaMemcpyHostToDevice, c->stream);
+  if (nG)
+    cudaMemcpyAsync(dG, ss.g.data(), sizeof(double) * ss.g.size(), cudaMemcpyHostToDevice,
+                    c->stream);
+  L = ExtLattice{dR, nR, dG, nG, dsf, ss.alpha, cell.volume};
+  return EWG_OK;
+}
+
+// Copies n values (when n > 0 and the host pointer is set) into context buffer b.
+double* upload(ewg_context* c, BufId b, const double* h, size_t n, int* rc) {
+  if (!h || n == 0) return nullptr;
+  double* d = dbuf<double>(c, b, n, rc);
+  if (*rc) return nullptr;
+  cudaMemcpyAsync(d, h, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream);
+  return d;
+}
+
+void structure_factors(const double* coords, const double* q, int n, const ExtLattice& L,
+                       double* out, cudaStream_t st) {
+  if (n > 0 && L.nG > 0)
+    launch_structure_factors(coords, q, n, L.G, L.nG, out, st);
+  else
+    cudaMemsetAsync(out, 0, sizeof(double) * 2 * std::max(L.nG, 1), st);
+}
+
+int finish(ewg_context* c) {
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  return cuda_status(e);
+}
+}  // namespace
+
+int ewg_potential_at(ewg_context* c, int nt, const double* tcoords, int ns, const double* scoords,
+                     const double* scharges, const double* blur, const double* eps_soften,
+                     const double* lat_cols, double tol_ewald, double alpha, double* pot) {
+  if (!c || nt < 0 || ns < 0 || !lat_cols || (nt && (!tcoords || !pot)) ||
+      (ns && (!scoords || !scharges)))
+    return EWG_ERR_ARG;
+  LaunchScope scope(c);
+  Cell cell;
+  ExtLattice L;
+  int rc = ext_setup(c, lat_cols, tol_ewald, alpha, cell, L);
+  if (rc) return rc;
+  if (nt == 0) return finish(c);
+  const double* dt = upload(c, B_EXT_T, tcoords, 3 * static_cast<size_t>(nt), &rc);
+  const double* ds = upload(c, B_EXT_S, scoords, 3 * static_cast<size_t>(ns), &rc);
+  const double* dq = upload(c, B_EXT_SQ, scharges, ns, &rc);
+  const double* db = upload(c, B_EXT_BLUR, blur, ns, &rc);
+  double* dpot = dbuf<double>(c, B_EXT_OUT, nt, &rc);
+  if (rc) return rc;
+  structure_factors(ds, dq, ns, L, const_cast<double*>(L.sf), c->stream);
+  double qsum = 0.0;
+  for (int s = 0; s < ns; ++s) qsum += scharges[s];
+  const double const_term = -kPi / (cell.volume * L.alpha * L.alpha) * qsum;
+  const double eps2 = eps_soften ? (*eps_soften) * (*eps_soften) : 0.0;
+  launch_ext_potential(nt, dt, ns, ds, dq, db, eps2, L, const_term, dpot, c->stream);
+  cudaMemcpyAsync(pot, dpot, sizeof(double) * nt, cudaMemcpyDeviceToHost, c->stream);
+  return finish(c);
+}
+
+int ewg_potential_gradient_at(ewg_context* c, int nt, const double* tcoords, int ns,
+                              const double* scoords, const double* scharges, const double* blur,
+                              const double* lat_cols, double tol_ewald, double alpha,
+                              double* gradient) {
+  if (!c || nt < 0 || ns < 0 || !lat_cols || (nt && (!tcoords || !gradient)) ||
+      (ns && (!scoords || !scharges)))
+    return EWG_ERR_ARG;
+  LaunchScope scope(c);
+  Cell cell;
+  ExtLattice L;
+  int rc = ext_setup(c, lat_cols, tol_ewald, alpha, cell, L);
+  if (rc) return rc;
+  if (nt == 0) return finish(c);
+  const double* dt = upload(c, B_EXT_T, tcoords, 3 * static_cast<size_t>(nt), &rc);
+  const double* ds = upload(c, B_EXT_S, scoords, 3 * static_cast<size_t>(ns), &rc);
+  const double* dq = upload(c, B_EXT_SQ, scharges, ns, &rc);
+  const double* db = upload(c, B_EXT_BLUR, blur, ns, &rc);
+  double* dg = dbuf<double>(c, B_EXT_OUT, 3 * static_cast<size_t>(nt), &rc);
+  if (rc) return rc;
+  structure_factors(ds, dq, ns, L, const_cast<double*>(L.sf), c->stream);
+  cudaMemsetAsync(dg, 0, sizeof(double) * 3 * nt, c->stream);
+  launch_ext_gradient(nt, dt, ns, ds, dq, db, L, nullptr, dg, c->stream);
+  cudaMemcpyAsync(gradient, dg, sizeof(double) * 3 * nt, cudaMemcpyDeviceToHost, c->stream);
+  return finish(c);
+}
+
+int ewg_external_pot_grad(ewg_context* c, int na, const double* acoords, int ne,
+                          const double* ecoords, const double* acharges, const double* echarges,
+                          int ham_deriv, const double* eblur, const double* lat_cols,
+                          double tol_ewald, double alpha, double* agrad, double* egrad) {
+  if (!c || na < 0 || ne < 0 || !lat_cols || (na && (!acoords || !agrad)) ||
+      (ne && (!ecoords || !echarges)) || (!ham_deriv && ((na && !acharges) || (ne && !egrad))))
+    return EWG_ERR_ARG;
+  LaunchScope scope(c);
+  Cell cell;
+  ExtLattice L;
+  int rc = ext_setup(c, lat_cols, tol_ewald, alpha, cell, L);
+  if (rc) return rc;
+  const double* da = upload(c, B_EXT_T, acoords, 3 * static_cast<size_t>(na), &rc);
+  const double* de = upload(c, B_EXT_S, ecoords, 3 * static_cast<size_t>(ne), &rc);
+  const double* deq = upload(c, B_EXT_SQ, echarges, ne, &rc);
+  const double* daq = ham_deriv ? nullptr : upload(c, B_EXT_TQ, acharges, na, &rc);
+  const double* db = upload(c, B_EXT_BLUR, eblur, ne, &rc);
+  double* dga = upload(c, B_EXT_OUT, agrad, 3 * static_cast<size_t>(na), &rc);
+  double* dge = ham_deriv ? nullptr : upload(c, B_EXT_OUT2, egrad, 3 * static_cast<size_t>(ne), &rc);
+  if (rc) return rc;
+  // atoms: deriv0 += (ham_deriv ? 1 : q_a) sum_e q_e d(r_a - r_e)
+  structure_factors(de, deq, ne, L, const_cast<double*>(L.sf), c->stream);
+  launch_ext_gradient(na, da, ne, de, deq, db, L, daq, dga, c->stream);
+  if (na) cudaMemcpyAsync(agrad, dga, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, c->stream);
+  if (!ham_deriv && ne) {
+    // external charges: deriv1 -= q_e sum_a q_a d(r_a - r_e)
+    double* dsf2 = dbuf<double>(c, B_EXT_SF2, 2 * static_cast<size_t>(std::max(L.nG, 1)), &rc);
+    if (rc) return rc;
+    ExtLattice L2 = L;
+    L2.sf = dsf2;
+    structure_factors(da, daq, na, L2, dsf2, c->stream);
+    launch_ext_source_gradient(na, da, daq, ne, de, deq, db, L2, dge, c->stream);
+    cudaMemcpyAsync(egrad, dge, sizeof(double) * 3 * ne, cudaMemcpyDeviceToHost, c->stream);
+  }
+  return finish(c);
 }
 
 int ewg_stress(ewg_context* c, double tol_ewald, double alpha, double* sigma) {

@@ -165,6 +165,28 @@ struct MeshSizes {
 MeshSizes mesh_sizes(const MeshGeom& g, const StencilDims& sd, int mixed, int nc, int natoms);
 
 // Shared-memory limits of the FFT and gather kernels (once per device).
+// Stock Ewald lattice sums for potentials and gradients at arbitrary points
+// (ewg_external.cu): cell translations R (origin first), half-space reciprocal
+// vectors G (Cartesian, with 2 pi) and the other group's structure factors
+// sf[2g] = sum q cos(G.r), sf[2g+1] = sum q sin(G.r); all device pointers.
+struct ExtLattice {
+  const double* R;
+  int nR;
+  const double* G;
+  int nG;
+  const double* sf;
+  double alpha, volume;
+};
+void launch_ext_potential(int nt, const double* tc, int ns, const double* sc, const double* sq,
+                          const double* blur, double eps2, const ExtLattice& L, double const_term,
+                          double* pot, cudaStream_t st);
+void launch_ext_gradient(int nt, const double* tc, int ns, const double* sc, const double* sq,
+                         const double* blur, const ExtLattice& L, const double* scale,
+                         double* grad, cudaStream_t st);
+void launch_ext_source_gradient(int nt, const double* tc, const double* tq, int ns,
+                                const double* sc, const double* sq, const double* blur,
+                                const ExtLattice& L, double* grad, cudaStream_t st);
+
 int mesh_configure_kernels();
 // Dense FP64 tensor-core (DMMA m8n8k4) rate of this GPU in TFLOP/s, timed on `st`.
 int measure_dmma_peak(cudaStream_t st, double* tflops);

@@ -50,7 +50,7 @@ EXPORTED = [
     "ewg_last_stress_setup", "ewg_batch_potential_force", "ewg_set_profiling", "ewg_stage_count",
     "ewg_stage_name", "ewg_stage_times", "ewg_reset_stage_times", "ewg_set_stream",
     "ewg_direct_potential_force_static", "ewg_fp64_mma_peak", "ewg_potential_force_stress",
-    "ewg_stress_fast",
+    "ewg_stress_fast", "ewg_potential_at", "ewg_potential_gradient_at", "ewg_external_pot_grad",
 ]
 
 
@@ -130,6 +130,12 @@ def lib():
     L.ewg_shift_force.argtypes = [vp, C.c_double, dp, dp]
     L.ewg_stress.argtypes = [vp, C.c_double, C.c_double, dp]
     L.ewg_stress_fast.argtypes = [vp, C.c_double, dp]
+    L.ewg_potential_at.argtypes = [vp, C.c_int, dp, C.c_int, dp, dp, dp, dp, dp, C.c_double,
+                                   C.c_double, dp]
+    L.ewg_potential_gradient_at.argtypes = [vp, C.c_int, dp, C.c_int, dp, dp, dp, dp, C.c_double,
+                                            C.c_double, dp]
+    L.ewg_external_pot_grad.argtypes = [vp, C.c_int, dp, C.c_int, dp, dp, dp, C.c_int, dp, dp,
+                                        C.c_double, C.c_double, dp, dp]
     L.ewg_last_stress_setup.argtypes = [vp, dp, dp, dp, ip]
     L.ewg_batch_potential_force.argtypes = [vp, C.c_int, ip, dp, dp, dp, C.c_double, dp, dp, ip]
     L.ewg_set_profiling.argtypes = [vp, C.c_int]
@@ -338,6 +344,54 @@ class Context:
         f = np.empty((n, 3))
         _check(lib().ewg_shift_force(self._h, float(tol), _dp(out), _dp(f)))
         return out, f
+
+    # -- potentials and gradients at arbitrary points (stock Ewald) -----------
+    def potential_at(self, targets, sources, charges, lat_cols, tol_ewald=1e-9, alpha=0.0,
+                     blur=None, eps_soften=None):
+        """getPotential (coulomb.F90:3122-3153): (N,3) targets, (M,3) sources."""
+        t = np.ascontiguousarray(targets, dtype=np.float64)
+        x = np.ascontiguousarray(sources, dtype=np.float64)
+        q = np.ascontiguousarray(charges, dtype=np.float64)
+        lat = np.asfortranarray(np.asarray(lat_cols, dtype=np.float64))
+        b = None if blur is None else np.ascontiguousarray(blur, dtype=np.float64)
+        eps = None if eps_soften is None else np.array([float(eps_soften)])
+        out = np.empty(t.shape[0])
+        _check(lib().ewg_potential_at(self._h, t.shape[0], _dp(t), x.shape[0], _dp(x), _dp(q),
+                                      _dp(b) if b is not None else None,
+                                      _dp(eps) if eps is not None else None, _dp(lat),
+                                      float(tol_ewald), float(alpha), _dp(out)))
+        return out
+
+    def potential_gradient_at(self, targets, sources, charges, lat_cols, tol_ewald=1e-9,
+                              alpha=0.0, blur=None):
+        """getPotentialGradient (coulomb.F90:3157-3194): (N,3) gradients."""
+        t = np.ascontiguousarray(targets, dtype=np.float64)
+        x = np.ascontiguousarray(sources, dtype=np.float64)
+        q = np.ascontiguousarray(charges, dtype=np.float64)
+        lat = np.asfortranarray(np.asarray(lat_cols, dtype=np.float64))
+        b = None if blur is None else np.ascontiguousarray(blur, dtype=np.float64)
+        out = np.empty((t.shape[0], 3))
+        _check(lib().ewg_potential_gradient_at(self._h, t.shape[0], _dp(t), x.shape[0], _dp(x),
+                                               _dp(q), _dp(b) if b is not None else None, _dp(lat),
+                                               float(tol_ewald), float(alpha), _dp(out)))
+        return out
+
+    def external_pot_grad(self, atoms, ext, atom_charges, ext_charges, lat_cols, ham_deriv,
+                          atom_grads, ext_grads, tol_ewald=1e-9, alpha=0.0, ext_blur=None):
+        """addExternalPotGrad (coulomb.F90:3198-3248): adds into the (N,3) and
+        (M,3) gradient arrays in place (C-contiguous float64)."""
+        a = np.ascontiguousarray(atoms, dtype=np.float64)
+        e = np.ascontiguousarray(ext, dtype=np.float64)
+        qa = np.ascontiguousarray(atom_charges, dtype=np.float64)
+        qe = np.ascontiguousarray(ext_charges, dtype=np.float64)
+        lat = np.asfortranarray(np.asarray(lat_cols, dtype=np.float64))
+        b = None if ext_blur is None else np.ascontiguousarray(ext_blur, dtype=np.float64)
+        _check(lib().ewg_external_pot_grad(self._h, a.shape[0], _dp(a), e.shape[0], _dp(e),
+                                           _dp(qa), _dp(qe), 1 if ham_deriv else 0,
+                                           _dp(b) if b is not None else None, _dp(lat),
+                                           float(tol_ewald), float(alpha), _dp(atom_grads),
+                                           _dp(ext_grads)))
+        return atom_grads, ext_grads
 
     def stress_fast(self, tol):
         """NFFT-based stress (2/V) dE/d(strain) of the resident state."""

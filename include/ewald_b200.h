@@ -207,6 +207,33 @@ int ewg_shift(ewg_context* ctx, double tol, double* shift);
 /* fftEwaldAddGradients (coulomb.F90:361-385): shift(N) and the physical force
  * F(3,N); the adapter subtracts F from DFTB+'s gradient array. */
 int ewg_shift_force(ewg_context* ctx, double tol, double* shift, double* force);
+/* ---- potentials and gradients at arbitrary points ---------------------- */
+/* TCoulomb%getPotential / getPotentialGradient / addExternalPotGrad
+ * (dftb/coulomb.F90:3122-3248), periodic branch: the stock Ewald sum of
+ * sumInvRPeriodicAsymm (:1340-1418) and addInvRPrimePeriodicAsymm (:1934-2092)
+ * between two point sets, with updateLatVecs's setup (:575-620) for the given
+ * lattice (one vector per column), tolerance and alpha (<= 0 selects
+ * getOptimalAlphaEwald).  Coordinates are (3, n) column-major (atom-major),
+ * gradients likewise.  blur_widths (Gaussian width of each source or external
+ * charge) and eps_soften (a pointer to the softening length) may be NULL. */
+int ewg_potential_at(ewg_context* ctx, int n_targets, const double* target_coords, int n_sources,
+                     const double* source_coords, const double* source_charges,
+                     const double* blur_widths, const double* eps_soften, const double* lat_cols,
+                     double tol_ewald, double alpha, double* potential);
+int ewg_potential_gradient_at(ewg_context* ctx, int n_targets, const double* target_coords,
+                              int n_sources, const double* source_coords,
+                              const double* source_charges, const double* blur_widths,
+                              const double* lat_cols, double tol_ewald, double alpha,
+                              double* gradient);
+/* Adds to atom_grads (and, unless ham_deriv, to ext_grads) like the reference
+ * (intent inout); ham_deriv != 0 gives the Hamiltonian derivative (no atom
+ * charges, ext_grads untouched). */
+int ewg_external_pot_grad(ewg_context* ctx, int n_atoms, const double* atom_coords, int n_ext,
+                          const double* ext_coords, const double* atom_charges,
+                          const double* ext_charges, int ham_deriv, const double* ext_blur_widths,
+                          const double* lat_cols, double tol_ewald, double alpha,
+                          double* atom_grads, double* ext_grads);
+
 /* The NFFT-based stress of ewg_potential_force_stress on the state set by
  * ewg_set_lattice / ewg_set_coords / ewg_set_charges (the fast path's own alpha
  * and cutoffs at tolerance tol, <= 0 or >= 1 meaning 1e-9 as in fftEwaldShift):

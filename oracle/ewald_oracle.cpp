@@ -1096,4 +1096,219 @@ int ewo_stock_stress(int n, const double* coords, const double* dq, const double
   return EWO_OK;
 }
 
+
+}  // extern "C"
+
+// ----------------------------------------------------------------------------
+// Source -> target potentials and gradients with the stock Ewald sum:
+// getPotential / getPotentialGradient / addExternalPotGrad (coulomb.F90:3122-3248)
+// through sumInvRPeriodicAsymm (:1340-1418) and addInvRPrimePeriodicAsymm
+// (:1934-2092), the pair function ewald (:2311-2343) with ewaldReciprocal
+// (:2346-2386), ewaldReal (:2520-2575), derivEwaldReal (:2578-2625) and
+// derivEwaldReciprocal (:2690-2711).  The lattice sums use updateLatVecs's
+// setup (:575-620): the stock alpha, gLatPoints (half space, onlyInside) and the
+// cell translations of getCellTranslations (dftb/periodic.F90:227-263).
+// ----------------------------------------------------------------------------
+namespace {
+
+constexpr double kTolSameDist = 1.0e-5;  // common/accuracy.F90:69
+constexpr double kTolSameDist2 = kTolSameDist * kTolSameDist;
+constexpr double kErfArgLimit = 10.0;    // coulomb.F90:214
+
+struct StockLattice {
+  double alpha, volume;
+  std::vector<double> R;  // Cartesian cell translations, origin first
+  std::vector<double> G;  // Cartesian half-space reciprocal vectors
+};
+
+int stock_lattice(const double* lat_cols, double tol_ewald, double alpha, StockLattice& out) {
+  double a[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int d = 0; d < 3; ++d) a[i][d] = lat_cols[d + 3 * i];
+  double c23[3], c31[3], c12[3];
+  cross(a[1], a[2], c23);
+  cross(a[2], a[0], c31);
+  cross(a[0], a[1], c12);
+  const double det = a[0][0] * c23[0] + a[0][1] * c23[1] + a[0][2] * c23[2];
+  const double volume = std::fabs(det);
+  if (volume <= kMinVolume) return EWO_ERR_VOLUME;
+  double g[3][3];
+  for (int d = 0; d < 3; ++d) {
+    g[0][d] = 2.0 * kPi * c23[d] / det;
+    g[1][d] = 2.0 * kPi * c31[d] / det;
+    g[2][d] = 2.0 * kPi * c12[d] / det;
+  }
+  auto len = [](const double* v) { return std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); };
+  int rc;
+  if (alpha <= 0.0) {
+    const double minG = std::min(len(g[0]), std::min(len(g[1]), len(g[2])));
+    const double minR = std::min(len(a[0]), std::min(len(a[1]), len(a[2])));
+    rc = optimal_alpha(minG, minR, volume, tol_ewald, alpha);
+    if (rc) return rc;
+  }
+  double maxR, maxG;
+  rc = max_extent([&](double x) { return rTerm(x, alpha); }, tol_ewald, maxR);
+  if (rc) return rc;
+  rc = max_extent([&](double x) { return gTerm(x, alpha, volume); }, tol_ewald, maxG);
+  if (rc) return rc;
+  const double invLenG[3] = {len(a[0]) / (2.0 * kPi), len(a[1]) / (2.0 * kPi),
+                             len(a[2]) / (2.0 * kPi)};
+  std::vector<int> gp;
+  lattice_points_half(g, invLenG, maxG, gp);
+  out.G.clear();
+  for (size_t k = 0; k < gp.size(); k += 3)
+    for (int d = 0; d < 3; ++d)
+      out.G.push_back(g[0][d] * gp[k] + g[1][d] * gp[k + 1] + g[2][d] * gp[k + 2]);
+  // getLatticePoints(latVecs, recVecs/(2 pi), maxR, posExtension=1, negExtension=1):
+  // every index triple in [-(r_i + 1), r_i + 1], r_i = floor(maxR |b_i| / (2 pi)),
+  // iterator order (last index fastest), with the origin moved to the front.
+  int rng[3];
+  for (int i = 0; i < 3; ++i) rng[i] = ffloor(maxR * len(g[i]) / (2.0 * kPi)) + 1;
+  out.R.assign({0.0, 0.0, 0.0});
+  for (int c1 = -rng[0]; c1 <= rng[0]; ++c1)
+    for (int c2 = -rng[1]; c2 <= rng[1]; ++c2)
+      for (int c3 = -rng[2]; c3 <= rng[2]; ++c3) {
+        if (c1 == 0 && c2 == 0 && c3 == 0) continue;
+        for (int d = 0; d < 3; ++d) out.R.push_back(a[0][d] * c1 + a[1][d] * c2 + a[2][d] * c3);
+      }
+  out.alpha = alpha;
+  out.volume = volume;
+  return EWO_OK;
+}
+
+// ewald(rr, rVec, gVec, alpha, vol, blurWidth, epsSoften), coulomb.F90:2311-2343
+double ewald_pair(const double* rr, const StockLattice& L, double blur, double eps2) {
+  const double alpha = L.alpha, vol = L.volume;
+  // ewaldReciprocal: factor 2 for the half space
+  double rec = 0.0;
+  const double g2f = -1.0 / (4.0 * alpha * alpha);
+  for (size_t k = 0; k < L.G.size(); k += 3) {
+    const double* G = &L.G[k];
+    const double g2 = G[0] * G[0] + G[1] * G[1] + G[2] * G[2];
+    const double gr = G[0] * rr[0] + G[1] * rr[1] + G[2] * rr[2];
+    rec += std::exp(g2f * g2) / g2 * std::cos(gr);
+  }
+  rec = 2.0 * rec * 4.0 * kPi / vol;
+  // ewaldReal
+  double real = 0.0;
+  for (size_t k = 0; k < L.R.size(); k += 3) {
+    const double x[3] = {rr[0] + L.R[k], rr[1] + L.R[k + 1], rr[2] + L.R[k + 2]};
+    const double absRR = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+    if (absRR < kTolSameDist * kTolSameDist) continue;
+    const double r = std::sqrt(absRR), soft = std::sqrt(absRR + eps2);
+    if (blur > 0.0) {
+      real += (absRR < (kErfArgLimit * blur) * (kErfArgLimit * blur) ? std::erf(r / blur) : 1.0) /
+              soft;
+      real -= std::erf(alpha * r) / soft;
+    } else {
+      real += std::erfc(alpha * r) / soft;
+    }
+  }
+  double e = rec + real - kPi / (vol * alpha * alpha);
+  if (rr[0] * rr[0] + rr[1] * rr[1] + rr[2] * rr[2] < kTolSameDist2) e -= 2.0 * alpha / std::sqrt(kPi);
+  return e;
+}
+
+// derivEwaldReal + derivEwaldReciprocal, coulomb.F90:2578-2625, :2690-2711
+void deriv_ewald_pair(const double* rr, const StockLattice& L, double blur, double* out) {
+  const double alpha = L.alpha, vol = L.volume;
+  double d[3] = {0.0, 0.0, 0.0};
+  for (size_t k = 0; k < L.R.size(); k += 3) {
+    const double x[3] = {rr[0] + L.R[k], rr[1] + L.R[k + 1], rr[2] + L.R[k + 2]};
+    const double r = std::sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+    if (r < kTolSameDist2) continue;  // the reference compares r with tolSameDist**2 here
+    double fac = alpha * r;
+    double w = (-2.0 / std::sqrt(kPi) * std::exp(-fac * fac) * fac - std::erfc(fac)) / (r * r * r);
+    if (blur > 0.0 && r < kErfArgLimit * blur) {
+      fac = r / blur;
+      w += (2.0 / std::sqrt(kPi) * std::exp(-fac * fac) * fac + std::erfc(fac)) / (r * r * r);
+    }
+    for (int c = 0; c < 3; ++c) d[c] += x[c] * w;
+  }
+  const double g2f = -1.0 / (4.0 * alpha * alpha);
+  double g[3] = {0.0, 0.0, 0.0};
+  for (size_t k = 0; k < L.G.size(); k += 3) {
+    const double* G = &L.G[k];
+    const double g2 = G[0] * G[0] + G[1] * G[1] + G[2] * G[2];
+    const double gr = G[0] * rr[0] + G[1] * rr[1] + G[2] * rr[2];
+    const double pf = -std::sin(gr) * std::exp(g2f * g2) / g2;
+    for (int c = 0; c < 3; ++c) g[c] += pf * G[c];
+  }
+  for (int c = 0; c < 3; ++c) out[c] = d[c] + 2.0 * g[c] * 4.0 * kPi / vol;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ewo_potential_at(int nt, const double* tcoords, int ns, const double* scoords,
+                     const double* scharges, const double* blur, const double* eps_soften,
+                     const double* lat_cols, double tol_ewald, double alpha, double* pot) {
+  if (nt < 0 || ns < 0) return EWO_ERR_NPARTICLE;
+  StockLattice L;
+  const int rc = stock_lattice(lat_cols, tol_ewald, alpha, L);
+  if (rc) return rc;
+  const double eps2 = eps_soften ? (*eps_soften) * (*eps_soften) : 0.0;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int t = 0; t < nt; ++t) {
+    double acc = 0.0;
+    for (int s = 0; s < ns; ++s) {
+      const double rr[3] = {tcoords[3 * t] - scoords[3 * s], tcoords[3 * t + 1] - scoords[3 * s + 1],
+                            tcoords[3 * t + 2] - scoords[3 * s + 2]};
+      acc += ewald_pair(rr, L, blur ? blur[s] : 0.0, eps2) * scharges[s];
+    }
+    pot[t] = acc;
+  }
+  return EWO_OK;
+}
+
+int ewo_potential_gradient_at(int nt, const double* tcoords, int ns, const double* scoords,
+                              const double* scharges, const double* blur, const double* lat_cols,
+                              double tol_ewald, double alpha, double* grad) {
+  if (nt < 0 || ns < 0) return EWO_ERR_NPARTICLE;
+  StockLattice L;
+  const int rc = stock_lattice(lat_cols, tol_ewald, alpha, L);
+  if (rc) return rc;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int t = 0; t < nt; ++t) {
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int s = 0; s < ns; ++s) {
+      const double rr[3] = {tcoords[3 * t] - scoords[3 * s], tcoords[3 * t + 1] - scoords[3 * s + 1],
+                            tcoords[3 * t + 2] - scoords[3 * s + 2]};
+      double d[3];
+      deriv_ewald_pair(rr, L, blur ? blur[s] : 0.0, d);
+      for (int c = 0; c < 3; ++c) acc[c] += d[c] * scharges[s];
+    }
+    for (int c = 0; c < 3; ++c) grad[3 * t + c] = acc[c];
+  }
+  return EWO_OK;
+}
+
+int ewo_external_pot_grad(int na, const double* acoords, int ne, const double* ecoords,
+                          const double* acharges, const double* echarges, int ham_deriv,
+                          const double* eblur, const double* lat_cols, double tol_ewald,
+                          double alpha, double* agrad, double* egrad) {
+  if (na < 0 || ne < 0) return EWO_ERR_NPARTICLE;
+  StockLattice L;
+  const int rc = stock_lattice(lat_cols, tol_ewald, alpha, L);
+  if (rc) return rc;
+  std::vector<double> d0(3 * static_cast<size_t>(na), 0.0), d1(3 * static_cast<size_t>(ne), 0.0);
+  for (int t = 0; t < na; ++t)
+    for (int s = 0; s < ne; ++s) {
+      const double rr[3] = {acoords[3 * t] - ecoords[3 * s], acoords[3 * t + 1] - ecoords[3 * s + 1],
+                            acoords[3 * t + 2] - ecoords[3 * s + 2]};
+      double d[3];
+      deriv_ewald_pair(rr, L, eblur ? eblur[s] : 0.0, d);
+      const double f = ham_deriv ? echarges[s] : acharges[t] * echarges[s];
+      for (int c = 0; c < 3; ++c) {
+        d0[3 * t + c] += d[c] * f;
+        d1[3 * s + c] -= d[c] * f;
+      }
+    }
+  for (size_t k = 0; k < d0.size(); ++k) agrad[k] += d0[k];
+  if (!ham_deriv)
+    for (size_t k = 0; k < d1.size(); ++k) egrad[k] += d1[k];
+  return EWO_OK;
+}
+
 }  // extern "C"

@@ -82,6 +82,21 @@ int ewo_stock_stress(int n, const double* coords, const double* dq, const double
                      double tol_ewald, double alpha, double* stress_out, double* alpha_out,
                      double* max_r_out, double* max_g_out, int* n_g_out);
 
+/* Source -> target potentials and gradients of TCoulomb (coulomb.F90:3122-3248),
+ * stock Ewald sum with updateLatVecs's setup.  Coordinates (3,n) atom-major,
+ * latVecs one vector per column, alpha <= 0 selects getOptimalAlphaEwald.
+ * blur (per source) and eps_soften may be NULL.  Gradients (3,n). */
+int ewo_potential_at(int nt, const double* tcoords, int ns, const double* scoords,
+                     const double* scharges, const double* blur, const double* eps_soften,
+                     const double* lat_cols, double tol_ewald, double alpha, double* pot);
+int ewo_potential_gradient_at(int nt, const double* tcoords, int ns, const double* scoords,
+                              const double* scharges, const double* blur, const double* lat_cols,
+                              double tol_ewald, double alpha, double* grad);
+int ewo_external_pot_grad(int na, const double* acoords, int ne, const double* ecoords,
+                          const double* acharges, const double* echarges, int ham_deriv,
+                          const double* eblur, const double* lat_cols, double tol_ewald,
+                          double alpha, double* agrad, double* egrad);
+
 /* Building blocks, exposed for the cross-checks. */
 int ewo_fft3d(int n1, int n2, int n3, double* data /* complex interleaved */, int isign);
 int ewo_adjoint_nfft(int n, const double* t1, const double* t2, const double* t3,

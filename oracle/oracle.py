@@ -96,6 +96,12 @@ def lib():
                                          C.POINTER(C.c_int)]
             L.ewo_stock_stress.argtypes = [C.c_int, dp, dp, dp, C.c_double, C.c_double, dp, dp,
                                            dp, dp, C.POINTER(C.c_int)]
+            L.ewo_potential_at.argtypes = [C.c_int, dp, C.c_int, dp, dp, dp, dp, dp, C.c_double,
+                                           C.c_double, dp]
+            L.ewo_potential_gradient_at.argtypes = [C.c_int, dp, C.c_int, dp, dp, dp, dp,
+                                                    C.c_double, C.c_double, dp]
+            L.ewo_external_pot_grad.argtypes = [C.c_int, dp, C.c_int, dp, dp, dp, C.c_int, dp, dp,
+                                                C.c_double, C.c_double, dp, dp]
             L.ewo_fft3d.argtypes = [C.c_int, C.c_int, C.c_int, dp, C.c_int]
             L.ewo_adjoint_nfft.argtypes = [C.c_int, dp, dp, dp, dp, C.c_int, C.c_int, C.c_int,
                                            C.c_int, dp]
@@ -233,6 +239,67 @@ def stock_stress(coords_3n, dq, lat_cols, tol_ewald=1e-9, alpha=0.0):
         raise OracleError(rc, "invRStress")
     return out.reshape(3, 3, order="F"), {"alpha": a.value, "max_r": r.value, "max_g": g.value,
                                           "n_g": ng.value}
+
+
+def _opt(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+def potential_at(targets, sources, charges, lat_cols, tol_ewald=1e-9, alpha=0.0, blur=None,
+                 eps_soften=None):
+    """TCoulomb%getPotential (coulomb.F90:3122-3153), periodic branch: the stock
+    Ewald potential at each target from the charged sources.  Coordinates (N,3)."""
+    t = np.ascontiguousarray(targets, dtype=np.float64)
+    x = np.ascontiguousarray(sources, dtype=np.float64)
+    q = np.ascontiguousarray(charges, dtype=np.float64)
+    lat = np.asfortranarray(np.asarray(lat_cols, dtype=np.float64))
+    b = _opt(blur)
+    eps = None if eps_soften is None else np.array([float(eps_soften)])
+    out = np.zeros(t.shape[0])
+    rc = lib().ewo_potential_at(t.shape[0], _p(t), x.shape[0], _p(x), _p(q),
+                                _p(b) if b is not None else None,
+                                _p(eps) if eps is not None else None, _p(lat), float(tol_ewald),
+                                float(alpha), _p(out))
+    if rc:
+        raise OracleError(rc, "getPotential")
+    return out
+
+
+def potential_gradient_at(targets, sources, charges, lat_cols, tol_ewald=1e-9, alpha=0.0,
+                          blur=None):
+    """TCoulomb%getPotentialGradient (coulomb.F90:3157-3194): (N,3) gradients."""
+    t = np.ascontiguousarray(targets, dtype=np.float64)
+    x = np.ascontiguousarray(sources, dtype=np.float64)
+    q = np.ascontiguousarray(charges, dtype=np.float64)
+    lat = np.asfortranarray(np.asarray(lat_cols, dtype=np.float64))
+    b = _opt(blur)
+    out = np.zeros((t.shape[0], 3))
+    rc = lib().ewo_potential_gradient_at(t.shape[0], _p(t), x.shape[0], _p(x), _p(q),
+                                         _p(b) if b is not None else None, _p(lat),
+                                         float(tol_ewald), float(alpha), _p(out))
+    if rc:
+        raise OracleError(rc, "getPotentialGradient")
+    return out
+
+
+def external_pot_grad(atoms, ext, atom_charges, ext_charges, lat_cols, ham_deriv, tol_ewald=1e-9,
+                      alpha=0.0, ext_blur=None):
+    """TCoulomb%addExternalPotGrad (coulomb.F90:3198-3248) added to zero arrays:
+    returns (atom gradients (N,3), external-charge gradients (M,3))."""
+    a = np.ascontiguousarray(atoms, dtype=np.float64)
+    e = np.ascontiguousarray(ext, dtype=np.float64)
+    qa = np.ascontiguousarray(atom_charges, dtype=np.float64)
+    qe = np.ascontiguousarray(ext_charges, dtype=np.float64)
+    lat = np.asfortranarray(np.asarray(lat_cols, dtype=np.float64))
+    b = _opt(ext_blur)
+    ga = np.zeros((a.shape[0], 3))
+    ge = np.zeros((e.shape[0], 3))
+    rc = lib().ewo_external_pot_grad(a.shape[0], _p(a), e.shape[0], _p(e), _p(qa), _p(qe),
+                                     1 if ham_deriv else 0, _p(b) if b is not None else None,
+                                     _p(lat), float(tol_ewald), float(alpha), _p(ga), _p(ge))
+    if rc:
+        raise OracleError(rc, "addExternalPotGrad")
+    return ga, ge
 
 
 def fft3d(data, isign):

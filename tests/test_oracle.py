@@ -193,3 +193,54 @@ def test_error_statuses(oracle, case, code):
     with pytest.raises(oracle.OracleError) as ei:
         oracle.fft_potential_force(pos, q, lat, tol)
     assert ei.value.code == code
+
+
+# ---- potentials and gradients at arbitrary points (stock Ewald) -------------
+
+def _points_system(seed=3):
+    pos, q, lat = W.c1_small_cubic()
+    rng = np.random.default_rng(seed)
+    targets = rng.uniform(0, 1, (6, 3)) @ lat
+    return pos, q, lat, targets
+
+
+def test_point_potential_at_the_atoms_is_the_shift(oracle):
+    """getPotential at the charges themselves (neutral set) is the Ewald shift:
+    the stock pair sum and the fast NFFT path agree to the tolerance."""
+    pos, q, lat, _ = _points_system()
+    p_stock = oracle.potential_at(pos, pos, q, lat.T, 1e-10)
+    p_fast, _ = oracle.fft_potential_force(pos, q, lat, 1e-10)
+    assert np.abs(p_stock - p_fast).max() / np.abs(p_fast).max() < 1e-9
+
+
+@pytest.mark.parametrize("blur", [None, 0.8])
+def test_point_gradient_is_the_derivative_of_the_potential(oracle, blur):
+    pos, q, lat, tg = _points_system()
+    b = None if blur is None else np.full(len(q), blur)
+    g = oracle.potential_gradient_at(tg, pos, q, lat.T, 1e-10, blur=b)
+    h = 1e-5
+    fd = np.zeros_like(g)
+    for d in range(3):
+        e = np.zeros(3)
+        e[d] = h
+        fd[:, d] = (oracle.potential_at(tg + e, pos, q, lat.T, 1e-10, blur=b)
+                    - oracle.potential_at(tg - e, pos, q, lat.T, 1e-10, blur=b)) / (2 * h)
+    assert np.abs(g - fd).max() / np.abs(g).max() < 1e-8
+
+
+def test_external_gradients_obey_newtons_third_law(oracle):
+    pos, q, lat, tg = _points_system()
+    qt = np.random.default_rng(4).normal(0, 0.3, len(tg))
+    ga, ge = oracle.external_pot_grad(tg, pos, qt, q, lat.T, False, 1e-10)
+    assert np.abs(ga.sum(0) + ge.sum(0)).max() < 1e-14 * np.abs(ga).max() * len(q)
+    gh, _ = oracle.external_pot_grad(tg, pos, qt, q, lat.T, True, 1e-10)
+    assert np.allclose(gh, oracle.potential_gradient_at(tg, pos, q, lat.T, 1e-10), rtol=0,
+                       atol=1e-15)
+    assert np.allclose(ga, qt[:, None] * gh, rtol=1e-13, atol=1e-16)
+
+
+def test_softening_vanishes_far_away(oracle):
+    pos, q, lat, tg = _points_system()
+    p0 = oracle.potential_at(tg, pos, q, lat.T, 1e-10)
+    p1 = oracle.potential_at(tg, pos, q, lat.T, 1e-10, eps_soften=1e-7)
+    assert np.abs(p1 - p0).max() < 1e-10
