@@ -603,6 +603,33 @@ class TCoulomb:
         gradients -= f.T
         return gradients
 
+    # coulomb.F90:3122-3248, periodic branch: stock Ewald between point sets with
+    # this instance's lattice, tolerance and alpha (as updateLatVecs set them up).
+    def getPotential(self, coords, chargeCoords, charges, blurWidths=None, epsSoften=None):
+        """Potential at coords(3, N) from charges at chargeCoords(3, M)."""
+        return self.ctx.potential_at(np.asarray(coords).T, np.asarray(chargeCoords).T, charges,
+                                     self.latVecs, self.tolEwald, self.alpha, blur=blurWidths,
+                                     eps_soften=epsSoften)
+
+    def getPotentialGradient(self, coords, chargeCoords, charges, blurWidths=None):
+        """Potential gradient (3, N) at coords(3, N)."""
+        g = self.ctx.potential_gradient_at(np.asarray(coords).T, np.asarray(chargeCoords).T,
+                                           charges, self.latVecs, self.tolEwald, self.alpha,
+                                           blur=blurWidths)
+        return g.T
+
+    def addExternalPotGrad(self, atomCoords, extChargeCoords, atomCharges, extCharges, atomGrads,
+                           extChargeGrads, tHamDeriv, extChargeBlurWidths=None):
+        """Adds the derivatives into atomGrads(3, N) and extChargeGrads(3, M) in place."""
+        ga = np.ascontiguousarray(np.asarray(atomGrads, dtype=np.float64).T)
+        ge = np.ascontiguousarray(np.asarray(extChargeGrads, dtype=np.float64).T)
+        self.ctx.external_pot_grad(np.asarray(atomCoords).T, np.asarray(extChargeCoords).T,
+                                   atomCharges, extCharges, self.latVecs, tHamDeriv, ga, ge,
+                                   self.tolEwald, self.alpha, ext_blur=extChargeBlurWidths)
+        atomGrads[...] = ga.T
+        extChargeGrads[...] = ge.T
+        return atomGrads, extChargeGrads
+
     def addStress(self, stress):
         """coulomb.F90:721-757: stress -= 0.5 * invRStress(...)."""
         if not (self.coordsUpdated and self.chargesUpdated):

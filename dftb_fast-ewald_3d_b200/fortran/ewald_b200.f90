@@ -17,7 +17,7 @@ module ewald_b200
   public :: TEwaldGpu, ewaldGpuInit, ewaldGpuFinal
   public :: ewaldGpuSetLattice, ewaldGpuSetCoords, ewaldGpuSetCharges
   public :: ewaldGpuShift, ewaldGpuShiftForce, ewaldGpuStress, ewaldGpuStressFast
-  public :: ewaldGpuPotentialForce
+  public :: ewaldGpuPotentialForce, ewaldGpuPotentialAt, ewaldGpuPotentialGradientAt
   public :: EWG_PRECISION_FP64, EWG_PRECISION_MIXED
 
   integer(c_int), parameter :: EWG_PRECISION_FP64 = 0
@@ -110,6 +110,30 @@ module ewald_b200
       real(c_double), intent(out) :: sigma(3, 3)
       integer(c_int) :: rc
     end function ewg_stress_fast
+
+    function ewg_potential_at(ctx, nt, tcoords, ns, scoords, scharges, blur, epsSoften, latVecs,&
+        & tolEwald, alpha, pot) bind(C, name="ewg_potential_at") result(rc)
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: nt, ns
+      real(c_double), intent(in) :: tcoords(3, nt), scoords(3, ns), scharges(ns), latVecs(3, 3)
+      type(c_ptr), value :: blur, epsSoften
+      real(c_double), value :: tolEwald, alpha
+      real(c_double), intent(out) :: pot(nt)
+      integer(c_int) :: rc
+    end function ewg_potential_at
+
+    function ewg_potential_gradient_at(ctx, nt, tcoords, ns, scoords, scharges, blur, latVecs,&
+        & tolEwald, alpha, grad) bind(C, name="ewg_potential_gradient_at") result(rc)
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: nt, ns
+      real(c_double), intent(in) :: tcoords(3, nt), scoords(3, ns), scharges(ns), latVecs(3, 3)
+      type(c_ptr), value :: blur
+      real(c_double), value :: tolEwald, alpha
+      real(c_double), intent(out) :: grad(3, nt)
+      integer(c_int) :: rc
+    end function ewg_potential_gradient_at
 
     function ewg_potential_force(ctx, n, positions, charges, latRows, tol, pot, force, ov) &
         & bind(C, name="ewg_potential_force") result(rc)
@@ -214,6 +238,30 @@ contains
     real(c_double), intent(out) :: sigma(3, 3)
     call check(ewg_stress_fast(this%ctx, tol, sigma))
   end subroutine ewaldGpuStressFast
+
+  !> TCoulomb%getPotential (coulomb.F90:3122-3153) without blur or softening.
+  subroutine ewaldGpuPotentialAt(this, coords, chargeCoords, charges, latVecs, tolEwald, alpha,&
+      & potential)
+    type(TEwaldGpu), intent(in) :: this
+    real(c_double), intent(in) :: coords(:, :), chargeCoords(:, :), charges(:), latVecs(3, 3)
+    real(c_double), intent(in) :: tolEwald, alpha
+    real(c_double), intent(out) :: potential(:)
+    call check(ewg_potential_at(this%ctx, int(size(coords, 2), c_int), coords,&
+        & int(size(chargeCoords, 2), c_int), chargeCoords, charges, c_null_ptr, c_null_ptr,&
+        & latVecs, tolEwald, alpha, potential))
+  end subroutine ewaldGpuPotentialAt
+
+  !> TCoulomb%getPotentialGradient (coulomb.F90:3157-3194) without blur.
+  subroutine ewaldGpuPotentialGradientAt(this, coords, chargeCoords, charges, latVecs, tolEwald,&
+      & alpha, gradient)
+    type(TEwaldGpu), intent(in) :: this
+    real(c_double), intent(in) :: coords(:, :), chargeCoords(:, :), charges(:), latVecs(3, 3)
+    real(c_double), intent(in) :: tolEwald, alpha
+    real(c_double), intent(out) :: gradient(:, :)
+    call check(ewg_potential_gradient_at(this%ctx, int(size(coords, 2), c_int), coords,&
+        & int(size(chargeCoords, 2), c_int), chargeCoords, charges, c_null_ptr, latVecs, tolEwald,&
+        & alpha, gradient))
+  end subroutine ewaldGpuPotentialGradientAt
 
   !> Same argument order as ewald_potential_force (fft/ewald_fft_3d.f90:36).
   subroutine ewaldGpuPotentialForce(this, positions, charges, nParticle, latVecs, tol, pot, force)

@@ -76,3 +76,22 @@ def test_potential_at_the_atoms_matches_the_fast_path(ctx):
     ps = ctx.potential_at(pos, pos, q, lat.T, 1e-10)
     pf = ctx.potential_force(pos, q, lat, 1e-10, want_force=False)
     assert rel_max(ps, pf) < 2e-8
+
+
+def test_tcoulomb_point_methods(ewald_lib, oracle):
+    """The TCoulomb mirror's getPotential / getPotentialGradient / addExternalPotGrad
+    use the instance's lattice, tolerance and alpha (DFTB+'s column layouts)."""
+    src, q, lat, tg = system(seed=11)
+    tc = ewald_lib.TCoulomb(len(q), tolEwald=1e-10)
+    tc.updateLatVecs(lat.T)
+    pot = tc.getPotential(tg.T, src.T, q, epsSoften=0.2)
+    assert rel_max(pot, oracle.potential_at(tg, src, q, lat.T, 1e-10, eps_soften=0.2)) < TOL
+    grad = tc.getPotentialGradient(tg.T, src.T, q)
+    assert rel_max(grad.T, oracle.potential_gradient_at(tg, src, q, lat.T, 1e-10)) < TOL
+    qa = np.linspace(-0.5, 0.5, len(tg))
+    ga = np.zeros((3, len(tg)))
+    ge = np.zeros((3, len(q)))
+    tc.addExternalPotGrad(tg.T, src.T, qa, q, ga, ge, False)
+    da, de = oracle.external_pot_grad(tg, src, qa, q, lat.T, False, 1e-10)
+    assert rel_max(ga.T, da) < TOL
+    assert rel_max(ge.T, de) < TOL
