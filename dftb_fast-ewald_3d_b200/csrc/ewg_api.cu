@@ -957,6 +957,56 @@ int coulomb_eval(ewg_context* c, double tol, double* shift, double* force,
 }
 }  // namespace
 
+int ewg_xlbomd_gradients(ewg_context* c, double tol, const double* dq_out, double* gradients) {
+  if (!c || !dq_out || !gradients) return EWG_ERR_ARG;
+  LaunchScope scope(c);
+  if (!c->has_coords || !c->has_charges) return EWG_ERR_STATE;
+  if (!(tol > 0.0 && tol < 1.0)) tol = 1.0e-9;  // coulomb.F90:348-349
+  const int n = c->natoms;
+  const double* qi = c->dq.data();
+  double q2 = 0.0, q2o = 0.0;
+  int rc = check_charges(n, qi, &q2);
+  if (!rc) rc = check_charges(n, dq_out, &q2o);
+  if (rc) return rc;
+  Cell cell;
+  rc = cell_from_cols(c->lat_cols, cell);
+  if (rc) return rc;
+  // One parameter set (from the input charges) for all three evaluations, so the
+  // combination is the exact gradient of one approximate shadow energy.
+  ewg_params p;
+  rc = choose_parameters(cell, q2, n, tol, nullptr, p);
+  if (rc) return rc;
+  double* dcoords = dbuf<double>(c, B_COORDS, 3 * static_cast<size_t>(n), &rc);
+  double* dq = dbuf<double>(c, B_Q, n, &rc);
+  double* dpot = dbuf<double>(c, B_POT, n, &rc);
+  double* dforce = dbuf<double>(c, B_FORCE, 3 * static_cast<size_t>(n), &rc);
+  if (rc) return rc;
+  if (c->resident.coords_version != c->coords_version)
+    cudaMemcpyAsync(dcoords, c->coords.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice,
+                    c->stream);
+  c->uploaded_charges = -1;  // the charge buffer holds the combinations below
+  // E_XL = E(qi + qo) - E(qo) - 2 E(qi) with E(q) the Coulomb energy of one set:
+  // the cross term sum_{i != j} qo_i qi_j phi_ij is E(qi + qo) - E(qi) - E(qo).
+  std::vector<double> qs(n), f(3 * static_cast<size_t>(n)), acc(3 * static_cast<size_t>(n), 0.0);
+  const double coef[3] = {1.0, -1.0, -2.0};
+  for (int k = 0; k < 3; ++k) {
+    for (int i = 0; i < n; ++i) qs[i] = k == 0 ? qi[i] + dq_out[i] : (k == 1 ? dq_out[i] : qi[i]);
+    cudaMemcpyAsync(dq, qs.data(), sizeof(double) * n, cudaMemcpyHostToDevice, c->stream);
+    rc = evaluate(c, n, dcoords, 3, 1, dq, cell, p, true, dpot, dforce, true);
+    if (rc) {
+      c->resident.coords_version = -1;
+      return rc;
+    }
+    cudaError_t e = cudaMemcpyAsync(f.data(), dforce, sizeof(double) * 3 * n,
+                                    cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_status(e);
+    for (size_t m = 0; m < f.size(); ++m) acc[m] -= coef[k] * f[m];  // gradient = -force
+  }
+  for (size_t m = 0; m < acc.size(); ++m) gradients[m] += acc[m];
+  return EWG_OK;
+}
+
 int ewg_shift(ewg_context* c, double tol, double* shift) { return coulomb_eval(c, tol, shift, nullptr); }
 
 int ewg_stress_fast(ewg_context* c, double tol, double* sigma) {

@@ -51,6 +51,7 @@ EXPORTED = [
     "ewg_stage_name", "ewg_stage_times", "ewg_reset_stage_times", "ewg_set_stream",
     "ewg_direct_potential_force_static", "ewg_fp64_mma_peak", "ewg_potential_force_stress",
     "ewg_stress_fast", "ewg_potential_at", "ewg_potential_gradient_at", "ewg_external_pot_grad",
+    "ewg_xlbomd_gradients",
 ]
 
 
@@ -130,6 +131,7 @@ def lib():
     L.ewg_shift_force.argtypes = [vp, C.c_double, dp, dp]
     L.ewg_stress.argtypes = [vp, C.c_double, C.c_double, dp]
     L.ewg_stress_fast.argtypes = [vp, C.c_double, dp]
+    L.ewg_xlbomd_gradients.argtypes = [vp, C.c_double, dp, dp]
     L.ewg_potential_at.argtypes = [vp, C.c_int, dp, C.c_int, dp, dp, dp, dp, dp, C.c_double,
                                    C.c_double, dp]
     L.ewg_potential_gradient_at.argtypes = [vp, C.c_int, dp, C.c_int, dp, dp, dp, dp, C.c_double,
@@ -393,6 +395,13 @@ class Context:
                                            _dp(ext_grads)))
         return atom_grads, ext_grads
 
+    def xlbomd_gradients(self, tol, dq_out):
+        """Gradient (N,3) of the XLBOMD shadow energy of the resident state."""
+        qo = np.ascontiguousarray(dq_out, dtype=np.float64)
+        g = np.zeros((qo.shape[0], 3))
+        _check(lib().ewg_xlbomd_gradients(self._h, float(tol), _dp(qo), _dp(g)))
+        return g
+
     def stress_fast(self, tol):
         """NFFT-based stress (2/V) dE/d(strain) of the resident state."""
         s = np.empty(9)
@@ -591,10 +600,14 @@ class TCoulomb:
             energies += 0.5 * self.shiftPerAtom * self.deltaQAtom
         return energies
 
-    def addGradients(self, gradients):
-        """coulomb.F90:656-717 with fftEwaldAddGradients (:361-385): deriv -= F."""
+    def addGradients(self, gradients, dQOutAtom=None):
+        """coulomb.F90:656-717 with fftEwaldAddGradients (:361-385): deriv -= F.
+        With dQOutAtom, the XLBOMD shadow-energy gradient (:697-699) instead."""
         if not (self.coordsUpdated and self.chargesUpdated):
             raise EwaldError(16, "addGradients before updateCoords/updateCharges")
+        if dQOutAtom is not None:
+            gradients += self.ctx.xlbomd_gradients(self._tol(), dQOutAtom).T
+            return gradients
         if _env_flag("DFTB_EWALD_DIRECT"):
             _, f = self.ctx.direct_potential_force(self.coords, self.deltaQAtom, self._lat_rows(),
                                                    self._direct_tol(), want_force=True)

@@ -234,6 +234,16 @@ int ewg_external_pot_grad(ewg_context* ctx, int n_atoms, const double* atom_coor
                           const double* lat_cols, double tol_ewald, double alpha,
                           double* atom_grads, double* ext_grads);
 
+/* XLBOMD gradients (addGradients with dQOutAtom, coulomb.F90:697-699): adds to
+ * gradients(3, N) the gradient of the shadow energy
+ * sum_{i<j} (qo_i qi_j + qi_i qo_j - qi_i qi_j) phi(r_ij) with qi the charges set
+ * by ewg_set_charges and qo = dq_out.  The reference sums it with the stock
+ * Ewald engine (addInvRPrimeXlbomdPeriodic, :1823-1894); here it is the fast
+ * path's energy gradient of E(qi + qo) - E(qo) - 2 E(qi), three evaluations on
+ * the resident geometry with one parameter set (tol as in ewg_shift_force).
+ * Both charge sets must be neutral (EWG_ERR_NOT_NEUTRAL otherwise). */
+int ewg_xlbomd_gradients(ewg_context* ctx, double tol, const double* dq_out, double* gradients);
+
 /* The NFFT-based stress of ewg_potential_force_stress on the state set by
  * ewg_set_lattice / ewg_set_coords / ewg_set_charges (the fast path's own alpha
  * and cutoffs at tolerance tol, <= 0 or >= 1 meaning 1e-9 as in fftEwaldShift):

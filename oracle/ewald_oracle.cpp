@@ -1311,4 +1311,67 @@ int ewo_external_pot_grad(int na, const double* acoords, int ne, const double* e
   return EWO_OK;
 }
 
+
+// XLBOMD gradient of the shadow energy with two charge sets,
+// addInvRPrimeXlbomdPeriodic (coulomb.F90:1823-1894) with
+// addNeighbourContribsXl (:1897-1930): over each atom pair and image within
+// the stock cutoff maxR (the half neighbour list, self images skipped) and over
+// all atom pairs in reciprocal space, prefac = qo_i qi_j + qi_i qo_j - qi_i qi_j
+// times derivRTerm (:2752-2773) or derivEwaldReciprocal (:2690-2711).
+int ewo_xlbomd_gradients(int n, const double* coords, const double* dq_in, const double* dq_out,
+                         const double* lat_cols, double tol_ewald, double alpha, double* deriv) {
+  if (n <= 0) return EWO_ERR_NPARTICLE;
+  StockLattice L;
+  int rc = stock_lattice(lat_cols, tol_ewald, alpha, L);
+  if (rc) return rc;
+  double maxR;
+  rc = max_extent([&](double x) { return rTerm(x, L.alpha); }, tol_ewald, maxR);
+  if (rc) return rc;
+  const double cut2 = maxR * maxR;
+  std::vector<double> loc(3 * static_cast<size_t>(n), 0.0);
+  auto prefac = [&](int i, int j) {
+    return dq_out[i] * dq_in[j] + dq_in[i] * dq_out[j] - dq_in[i] * dq_in[j];
+  };
+  // real space; L.R holds the origin first, then the other translations
+  for (int i = 0; i < n; ++i)
+    for (size_t t = 0; t < L.R.size(); t += 3)
+      for (int j = i + 1; j < n; ++j) {
+        const double rr[3] = {coords[3 * i] - coords[3 * j] - L.R[t],
+                              coords[3 * i + 1] - coords[3 * j + 1] - L.R[t + 1],
+                              coords[3 * i + 2] - coords[3 * j + 2] - L.R[t + 2]};
+        const double d2 = rr[0] * rr[0] + rr[1] * rr[1] + rr[2] * rr[2];
+        if (d2 > cut2) continue;
+        const double r = std::sqrt(d2), fac = L.alpha * r;
+        const double w = prefac(i, j) *
+                         (-2.0 * L.alpha / std::sqrt(kPi) * std::exp(-fac * fac) * r - std::erfc(fac)) /
+                         (r * r * r);
+        for (int c = 0; c < 3; ++c) {
+          loc[3 * i + c] += w * rr[c];
+          loc[3 * j + c] -= w * rr[c];
+        }
+      }
+  // reciprocal space
+  const double g2f = -1.0 / (4.0 * L.alpha * L.alpha);
+  for (int i = 0; i < n; ++i)
+    for (int j = i + 1; j < n; ++j) {
+      const double rr[3] = {coords[3 * i] - coords[3 * j], coords[3 * i + 1] - coords[3 * j + 1],
+                            coords[3 * i + 2] - coords[3 * j + 2]};
+      double g[3] = {0.0, 0.0, 0.0};
+      for (size_t k = 0; k < L.G.size(); k += 3) {
+        const double* G = &L.G[k];
+        const double g2 = G[0] * G[0] + G[1] * G[1] + G[2] * G[2];
+        const double pf = -std::sin(G[0] * rr[0] + G[1] * rr[1] + G[2] * rr[2]) *
+                          std::exp(g2f * g2) / g2;
+        for (int c = 0; c < 3; ++c) g[c] += pf * G[c];
+      }
+      const double p = prefac(i, j) * 2.0 * 4.0 * kPi / L.volume;
+      for (int c = 0; c < 3; ++c) {
+        loc[3 * i + c] += p * g[c];
+        loc[3 * j + c] -= p * g[c];
+      }
+    }
+  for (size_t k = 0; k < loc.size(); ++k) deriv[k] += loc[k];
+  return EWO_OK;
+}
+
 }  // extern "C"

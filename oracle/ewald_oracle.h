@@ -97,6 +97,12 @@ int ewo_external_pot_grad(int na, const double* acoords, int ne, const double* e
                           const double* eblur, const double* lat_cols, double tol_ewald,
                           double alpha, double* agrad, double* egrad);
 
+/* XLBOMD gradients of the shadow energy with input and output charges,
+ * addInvRPrimeXlbomdPeriodic (coulomb.F90:1823-1894), stock Ewald; adds to
+ * deriv(3,n). */
+int ewo_xlbomd_gradients(int n, const double* coords, const double* dq_in, const double* dq_out,
+                         const double* lat_cols, double tol_ewald, double alpha, double* deriv);
+
 /* Building blocks, exposed for the cross-checks. */
 int ewo_fft3d(int n1, int n2, int n3, double* data /* complex interleaved */, int isign);
 int ewo_adjoint_nfft(int n, const double* t1, const double* t2, const double* t3,

@@ -102,6 +102,8 @@ def lib():
                                                     C.c_double, C.c_double, dp]
             L.ewo_external_pot_grad.argtypes = [C.c_int, dp, C.c_int, dp, dp, dp, C.c_int, dp, dp,
                                                 C.c_double, C.c_double, dp, dp]
+            L.ewo_xlbomd_gradients.argtypes = [C.c_int, dp, dp, dp, dp, C.c_double, C.c_double,
+                                               dp]
             L.ewo_fft3d.argtypes = [C.c_int, C.c_int, C.c_int, dp, C.c_int]
             L.ewo_adjoint_nfft.argtypes = [C.c_int, dp, dp, dp, dp, C.c_int, C.c_int, C.c_int,
                                            C.c_int, dp]
@@ -300,6 +302,20 @@ def external_pot_grad(atoms, ext, atom_charges, ext_charges, lat_cols, ham_deriv
     if rc:
         raise OracleError(rc, "addExternalPotGrad")
     return ga, ge
+
+
+def xlbomd_gradients(coords_3n, dq_in, dq_out, lat_cols, tol_ewald=1e-9, alpha=0.0):
+    """addInvRPrimeXlbomdPeriodic (coulomb.F90:1823-1894) added to zeros: (N,3)."""
+    x = np.ascontiguousarray(coords_3n, dtype=np.float64)
+    qi = np.ascontiguousarray(dq_in, dtype=np.float64)
+    qo = np.ascontiguousarray(dq_out, dtype=np.float64)
+    lat = np.asfortranarray(np.asarray(lat_cols, dtype=np.float64))
+    out = np.zeros((qi.shape[0], 3))
+    rc = lib().ewo_xlbomd_gradients(qi.shape[0], _p(x), _p(qi), _p(qo), _p(lat), float(tol_ewald),
+                                    float(alpha), _p(out))
+    if rc:
+        raise OracleError(rc, "addInvRPrimeXlbomd")
+    return out
 
 
 def fft3d(data, isign):

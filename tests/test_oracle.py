@@ -244,3 +244,21 @@ def test_softening_vanishes_far_away(oracle):
     p0 = oracle.potential_at(tg, pos, q, lat.T, 1e-10)
     p1 = oracle.potential_at(tg, pos, q, lat.T, 1e-10, eps_soften=1e-7)
     assert np.abs(p1 - p0).max() < 1e-10
+
+
+def test_xlbomd_gradient_restatement(oracle):
+    """addInvRPrimeXlbomdPeriodic: with qo = qi the shadow energy is the energy
+    (gradient = -force of the fast path to the tolerance), and in general it is
+    the gradient of E(qi + qo) - E(qo) - 2 E(qi)."""
+    pos, q, lat = W.c1_small_cubic()
+    g = oracle.xlbomd_gradients(pos, q, q, lat.T, 1e-10)
+    _, f = oracle.fft_potential_force(pos, q, lat, 1e-10)
+    assert np.abs(g + f).max() / np.abs(f).max() < 1e-8
+    rng = np.random.default_rng(1)
+    qo = q + rng.normal(0, 0.05, len(q))
+    qo -= qo.mean()
+    g = oracle.xlbomd_gradients(pos, q, qo, lat.T, 1e-10)
+    f1 = oracle.fft_potential_force(pos, q + qo, lat, 1e-10)[1]
+    f2 = oracle.fft_potential_force(pos, qo, lat, 1e-10)[1]
+    f3 = oracle.fft_potential_force(pos, q, lat, 1e-10)[1]
+    assert np.abs(g + (f1 - f2 - 2 * f3)).max() / np.abs(g).max() < 1e-8
