@@ -79,6 +79,8 @@ struct ewg_context {
   int precision = EWG_PRECISION_FP64;
   cudaStream_t stream = nullptr;
   cudaStream_t own_stream = nullptr;
+  // Charged cells: accept a net charge with a uniform neutralising background.
+  bool background = false;
   // Second stream for the real-space sum, which runs beside the mesh pipeline:
   // forked from `stream` after the atom sort, joined before the final assembly.
   cudaStream_t side = nullptr;
@@ -307,7 +309,8 @@ void stencil_dims(const MeshGeom& g, StencilDims& sd) {
 // later); otherwise the call completes on the GPU before it returns.
 int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const double* q,
              const Cell& cell, const ewg_params& p, bool want_force, double* pot, double* force,
-             bool resident, int* err_flag = nullptr, double* stress12 = nullptr) {
+             bool resident, int* err_flag = nullptr, double* stress12 = nullptr,
+             double pot_shift = 0.0) {
   int rc = EWG_OK;
   cudaStream_t st = c->stream;
   const int mixed = c->precision == EWG_PRECISION_MIXED;
@@ -442,7 +445,7 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
   prof_mark(mp.prof, st, ST_GATHER);
   launch_gather(mp, pairstart, pairs, wtab, outg, nc, part, st);
   if (concurrent) cudaStreamWaitEvent(st, c->join, 0);  // pot_sr, f_sr, err ready
-  launch_gather_final(mp, slot, permmesh, part, nc, n, q, self_coef, pot_sr, f_sr, pot,
+  launch_gather_final(mp, slot, permmesh, part, nc, n, q, self_coef, pot_shift, pot_sr, f_sr, pot,
                       want_force ? force : nullptr, st);
   prof_mark(mp.prof, st, -1);
   if (err_flag && !c->prof.on) {  // deferred: the caller synchronises and reads the flag
@@ -471,11 +474,28 @@ struct LaunchScope {
   ~LaunchScope() { c->launches += g_launches - start; }
 };
 
-int validate_host(int n, const double* pos, const double* q, const double* lat_rows, double tol,
-                  Cell& cell, double& q2) {
+// check_charges, except that with the background convention a net charge is
+// accepted (its sum goes to *qsum).
+int charge_check(const ewg_context* c, int n, const double* q, double* q2, double* qsum) {
+  int rc = check_charges(n, q, q2);
+  double s = 0.0;
+  for (int i = 0; i < n && q; ++i) s += q[i];
+  if (qsum) *qsum = s;
+  if (rc == EWG_ERR_NOT_NEUTRAL && c && c->background) rc = EWG_OK;
+  return rc;
+}
+
+// The background's potential: -pi Q / (V alpha^2) at every atom, the constant
+// the stock pair function ewald carries per unit of charge (coulomb.F90:2338).
+double background_shift(const ewg_context* c, double qsum, const Cell& cell, double alpha) {
+  return c->background ? -kPi * qsum / (cell.volume * alpha * alpha) : 0.0;
+}
+
+int validate_host(const ewg_context* c, int n, const double* pos, const double* q,
+                  const double* lat_rows, double tol, Cell& cell, double& q2, double& qsum) {
   if (n <= 0) return EWG_ERR_NPARTICLE;
   if (!pos || !q || !lat_rows) return EWG_ERR_ARG;
-  int rc = check_charges(n, q, &q2);
+  int rc = charge_check(c, n, q, &q2, &qsum);
   if (rc) return rc;
   rc = cell_from_rows(lat_rows, cell);
   if (rc) return rc;
@@ -568,6 +588,12 @@ int ewg_set_stream(ewg_context* c, void* stream) {
 }
 
 long long ewg_kernel_launches(const ewg_context* c) { return c ? c->launches : 0; }
+
+int ewg_set_background(ewg_context* c, int on) {
+  if (!c) return EWG_ERR_ARG;
+  c->background = on != 0;
+  return EWG_OK;
+}
 
 int ewg_fp64_mma_peak(ewg_context* c, double* tflops) {
   if (!c || !tflops) return EWG_ERR_ARG;
@@ -677,8 +703,8 @@ int ewg_potential_force(ewg_context* c, int n, const double* positions, const do
   c->uploaded_charges = -1;
   c->resident.coords_version = -1;
   Cell cell;
-  double q2 = 0.0;
-  int rc = validate_host(n, positions, charges, lat_rows, tol, cell, q2);
+  double q2 = 0.0, qsum = 0.0;
+  int rc = validate_host(c, n, positions, charges, lat_rows, tol, cell, q2, qsum);
   if (rc) return rc;
   if (!pot) return EWG_ERR_ARG;
   ewg_params p;
@@ -691,7 +717,8 @@ int ewg_potential_force(ewg_context* c, int n, const double* positions, const do
   if (rc) return rc;
   cudaMemcpyAsync(dpos, positions, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream);
   cudaMemcpyAsync(dq, charges, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream);
-  rc = evaluate(c, n, dpos, 1, n, dq, cell, p, force != nullptr, dpot, dforce, false);
+  rc = evaluate(c, n, dpos, 1, n, dq, cell, p, force != nullptr, dpot, dforce, false, nullptr,
+                nullptr, background_shift(c, qsum, cell, p.alpha));
   if (rc) return rc;
   cudaError_t e = cudaMemcpyAsync(pot, dpot, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess && force)
@@ -709,8 +736,8 @@ int ewg_potential_force_stress(ewg_context* c, int n, const double* positions,
   c->uploaded_charges = -1;
   c->resident.coords_version = -1;
   Cell cell;
-  double q2 = 0.0;
-  int rc = validate_host(n, positions, charges, lat_rows, tol, cell, q2);
+  double q2 = 0.0, qsum = 0.0;
+  int rc = validate_host(c, n, positions, charges, lat_rows, tol, cell, q2, qsum);
   if (rc) return rc;
   if (!pot || !sigma) return EWG_ERR_ARG;
   ewg_params p;
@@ -724,7 +751,8 @@ int ewg_potential_force_stress(ewg_context* c, int n, const double* positions,
   if (rc) return rc;
   cudaMemcpyAsync(dpos, positions, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream);
   cudaMemcpyAsync(dq, charges, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream);
-  rc = evaluate(c, n, dpos, 1, n, dq, cell, p, force != nullptr, dpot, dforce, false, nullptr, s12);
+  rc = evaluate(c, n, dpos, 1, n, dq, cell, p, force != nullptr, dpot, dforce, false, nullptr, s12,
+                background_shift(c, qsum, cell, p.alpha));
   if (rc) return rc;
   double h[12];
   cudaError_t e = cudaMemcpyAsync(pot, dpot, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream);
@@ -739,6 +767,9 @@ int ewg_potential_force_stress(ewg_context* c, int n, const double* positions,
   const int map[3][3] = {{0, 3, 4}, {3, 1, 5}, {4, 5, 2}};
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 3; ++j) sigma[i + 3 * j] = (h[map[i][j]] + 2.0 * h[6 + map[i][j]]) / V;
+  // background energy -pi Q^2 / (2 V alpha^2): (2/V) dE/d eps = pi Q^2 / (V alpha)^2 delta
+  if (c->background)
+    for (int i = 0; i < 3; ++i) sigma[4 * i] += kPi * qsum * qsum / (V * V * p.alpha * p.alpha);
   return EWG_OK;
 }
 
@@ -759,6 +790,7 @@ int ewg_potential_force_device(ewg_context* c, int n, const double* coords_devic
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_status(e);
   rc = check_sums(n, h[0], h[1]);
+  if (rc == EWG_ERR_NOT_NEUTRAL && c->background) rc = EWG_OK;
   if (rc) return rc;
   Cell cell;
   rc = cell_from_rows(lat_rows, cell);
@@ -768,7 +800,8 @@ int ewg_potential_force_device(ewg_context* c, int n, const double* coords_devic
   rc = choose_parameters(cell, h[2], n, tol, ov, p);
   if (rc) return rc;
   return evaluate(c, n, coords_device, 3, 1, charges_device, cell, p, force_device != nullptr,
-                  pot_device, force_device, false);
+                  pot_device, force_device, false, nullptr, nullptr,
+                  background_shift(c, h[0], cell, p.alpha));
 }
 
 int ewg_direct_potential_force(ewg_context* c, int n, const double* positions,
@@ -780,8 +813,8 @@ int ewg_direct_potential_force(ewg_context* c, int n, const double* positions,
   c->uploaded_charges = -1;
   c->resident.coords_version = -1;
   Cell cell;
-  double q2 = 0.0;
-  int rc = validate_host(n, positions, charges, lat_rows, tol, cell, q2);
+  double q2 = 0.0, qsum = 0.0;
+  int rc = validate_host(nullptr, n, positions, charges, lat_rows, tol, cell, q2, qsum);
   if (rc) return rc;
   if (!pot) return EWG_ERR_ARG;
   const double alpha = alpha_in ? *alpha_in : balanced_splitting(cell, tol);
@@ -910,8 +943,8 @@ int coulomb_eval(ewg_context* c, double tol, double* shift, double* force,
   if (!c->has_coords || !c->has_charges) return EWG_ERR_STATE;
   if (!(tol > 0.0 && tol < 1.0)) tol = 1.0e-9;  // coulomb.F90:348-349
   const int n = c->natoms;
-  double q2 = 0.0;
-  int rc = check_charges(n, c->dq.data(), &q2);
+  double q2 = 0.0, qsum = 0.0;
+  int rc = charge_check(c, n, c->dq.data(), &q2, &qsum);
   if (rc) return rc;
   Cell cell;
   rc = cell_from_cols(c->lat_cols, cell);
@@ -933,7 +966,7 @@ int coulomb_eval(ewg_context* c, double tol, double* shift, double* force,
     c->uploaded_charges = c->charges_version;
   }
   rc = evaluate(c, n, dcoords, 3, 1, dq, cell, p, force != nullptr, dpot, dforce, true, nullptr,
-                s12);
+                s12, background_shift(c, qsum, cell, p.alpha));
   if (rc) {
     c->resident.coords_version = -1;
     return rc;
@@ -952,6 +985,9 @@ int coulomb_eval(ewg_context* c, double tol, double* shift, double* force,
     for (int i = 0; i < 3; ++i)
       for (int j = 0; j < 3; ++j)
         sigma[i + 3 * j] = (h[map[i][j]] + 2.0 * h[6 + map[i][j]]) / cell.volume;
+    if (c->background)  // background energy -pi Q^2 / (2 V alpha^2)
+      for (int i = 0; i < 3; ++i)
+        sigma[4 * i] += kPi * qsum * qsum / (cell.volume * cell.volume * p.alpha * p.alpha);
   }
   return EWG_OK;
 }

@@ -154,7 +154,7 @@ void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs,
 // Fixed-order sum of each atom's partials with the final assembly
 // (fft/ewald_fft_3d.f90:121-132): pot = (sr + lr) + self, force = sr + q lr.
 void launch_gather_final(const MeshPlan& mp, const int4* slot, const int* mesh_perm,
-                         const double* part, int nc, int n, const double* q_orig, double self_coef,
+                         const double* part, int nc, int n, const double* q_orig, double self_coef, double pot_shift,
                          const double* pot_sr, const double* force_sr, double* pot, double* force,
                          cudaStream_t st);
 

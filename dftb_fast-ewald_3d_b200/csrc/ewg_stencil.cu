@@ -641,7 +641,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma(const int* __r
 template <int NC>
 __global__ void k_gather_final(const int4* __restrict__ slot, const int* __restrict__ perm,
                                const double* __restrict__ part, int n, StencilDims sd,
-                               const double* __restrict__ q, double self_coef,
+                               const double* __restrict__ q, double self_coef, double pot_shift,
                                const double* __restrict__ pot_sr, const double* __restrict__ f_sr,
                                double* __restrict__ pot, double* __restrict__ force) {
   const int k = static_cast<int>((static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
@@ -668,7 +668,7 @@ __global__ void k_gather_final(const int4* __restrict__ slot, const int* __restr
   if (lane != 0) return;
   const int i = perm[k];
   const double qi = q[i];
-  pot[i] = (pot_sr[i] + acc[0]) + self_coef * qi;
+  pot[i] = (pot_sr[i] + acc[0]) + self_coef * qi + pot_shift;
   if (NC == 4 && force) {
 #pragma unroll
     for (int d = 0; d < 3; ++d) force[3 * i + d] = f_sr[3 * i + d] + qi * acc[1 + d];
@@ -774,15 +774,15 @@ void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs,
 }
 
 void launch_gather_final(const MeshPlan& mp, const int4* slot, const int* perm, const double* part,
-                         int nc, int n, const double* q, double self_coef, const double* pot_sr,
+                         int nc, int n, const double* q, double self_coef, double pot_shift, const double* pot_sr,
                          const double* f_sr, double* pot, double* force, cudaStream_t st) {
   if (n == 0) return;
   if (nc == 4)
     k_gather_final<4><<<blocks_for(32L * n, 256), 256, 0, st>>>(
-        slot, perm, part, n, mp.sd, q, self_coef, pot_sr, f_sr, pot, force);
+        slot, perm, part, n, mp.sd, q, self_coef, pot_shift, pot_sr, f_sr, pot, force);
   else
     k_gather_final<1><<<blocks_for(32L * n, 256), 256, 0, st>>>(
-        slot, perm, part, n, mp.sd, q, self_coef, pot_sr, f_sr, pot, nullptr);
+        slot, perm, part, n, mp.sd, q, self_coef, pot_shift, pot_sr, f_sr, pot, nullptr);
   ++g_launches;
 }
 

@@ -51,7 +51,7 @@ EXPORTED = [
     "ewg_stage_name", "ewg_stage_times", "ewg_reset_stage_times", "ewg_set_stream",
     "ewg_direct_potential_force_static", "ewg_fp64_mma_peak", "ewg_potential_force_stress",
     "ewg_stress_fast", "ewg_potential_at", "ewg_potential_gradient_at", "ewg_external_pot_grad",
-    "ewg_xlbomd_gradients",
+    "ewg_xlbomd_gradients", "ewg_set_background",
 ]
 
 
@@ -132,6 +132,7 @@ def lib():
     L.ewg_stress.argtypes = [vp, C.c_double, C.c_double, dp]
     L.ewg_stress_fast.argtypes = [vp, C.c_double, dp]
     L.ewg_xlbomd_gradients.argtypes = [vp, C.c_double, dp, dp]
+    L.ewg_set_background.argtypes = [vp, C.c_int]
     L.ewg_potential_at.argtypes = [vp, C.c_int, dp, C.c_int, dp, dp, dp, dp, dp, C.c_double,
                                    C.c_double, dp]
     L.ewg_potential_gradient_at.argtypes = [vp, C.c_int, dp, C.c_int, dp, dp, dp, dp, C.c_double,
@@ -394,6 +395,10 @@ class Context:
                                            float(tol_ewald), float(alpha), _dp(atom_grads),
                                            _dp(ext_grads)))
         return atom_grads, ext_grads
+
+    def set_background(self, on: bool = True):
+        """Charged cells with a uniform neutralising background (off by default)."""
+        _check(lib().ewg_set_background(self._h, 1 if on else 0))
 
     def xlbomd_gradients(self, tol, dq_out):
         """Gradient (N,3) of the XLBOMD shadow energy of the resident state."""

@@ -91,6 +91,15 @@ const char* ewg_status_string(int status);
 int ewg_set_stream(ewg_context* ctx, void* stream);
 /* Number of this library's kernels launched by the context so far. */
 long long ewg_kernel_launches(const ewg_context* ctx);
+/* Charged cells (on != 0): the fast path then accepts a net charge Q, with the
+ * uniform neutralising background the stock Ewald engine implies (its pair
+ * function carries -pi/(V alpha^2) per unit charge, dftb/coulomb.F90:2338):
+ * every potential gains -pi Q/(V alpha^2) with the evaluation's alpha, forces
+ * are unchanged, and the stresses of ewg_potential_force_stress / ewg_stress_fast
+ * include the background energy -pi Q^2/(2 V alpha^2).  The reference's fast
+ * path refuses charged cells (common/ewald_validation.f90:43-46); this mode
+ * has no counterpart there (fft3d_readme.md:31).  Off by default. */
+int ewg_set_background(ewg_context* ctx, int on);
 /* Parameters the last evaluation on this context used. */
 int ewg_last_params(const ewg_context* ctx, ewg_params* out);
 /* Measured dense FP64 tensor-core rate of the context's GPU (DMMA m8n8k4 on
