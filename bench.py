@@ -13,8 +13,12 @@ Our arm (default):
           the launching stream; L2 flushed between steps (flush not timed).
   e2e     the same through the C ABI with pinned host buffers: every step copies
           positions and charges in and potential and force out.
+  fp64_ad the plain form with forces by window differentiation (one inverse
+          FFT instead of four), with its deviation from the i k forces.
   mixed   the mixed-precision form (FP32 stencils, FFT and pair terms, FP64
-          accumulation) at tol 1e-7, with its error against the FP64 result.
+          accumulation) with force scheme and parameters from the library's
+          autotuner (ewg_tune) for an RMS force error of at most 5e-7 against
+          the FP64 form, with its measured error.
   roofline, cpu_baseline, clocks, gpu_launches as the measurement contract asks.
 Reference arm (--impl reference): the CPU restatement of the reference's own
 algorithm (oracle/), all host threads, one full evaluation per step.
@@ -49,6 +53,7 @@ import workloads  # noqa: E402
 METRIC = "Coulomb shift+force evals/s at 32k atoms, mixed vs FP64; rel. err vs FP64"
 TOL_FP64 = 1e-10
 TOL_MIXED = 1e-7
+MIXED_TARGET = 1e-6  # mixed form: RMS relative force error <= MIXED_TARGET / 2 vs FP64
 L2_FLUSH_BYTES = 256 << 20
 
 
@@ -160,10 +165,11 @@ def stage_flops(params, natoms, nc=4):
 
 
 # DRAM bytes (read + write) per launch from one ncu capture of the 32,769-atom
-# workload (profiles/c3_water_32k_top_kernels.md), keyed by (real bytes, stage).
+# workload (profiles/c3_water_32k_top_kernels.md), keyed by (real bytes, grids
+# through the inverse passes and the gather, stage).
 DRAM_TRAFFIC = {
-    (8, "gather"): 746.37e6 + 62.96e6,
-    (8, "fft_x_c2r"): 356.31e6 + 660.39e6,
+    (8, 4, "gather"): 746.37e6 + 62.96e6,
+    (8, 4, "fft_x_c2r"): 356.31e6 + 660.39e6,
 }
 
 
@@ -231,10 +237,13 @@ def run_reference(args):
 class Arm:
     """One precision form on one device: device-resident and end-to-end timing."""
 
-    def __init__(self, eb, torch, device, precision, tol, pos, q, lat):
+    def __init__(self, eb, torch, device, precision, tol, pos, q, lat, scheme=None, ov=None):
         self.eb, self.torch = eb, torch
         self.tol = tol
+        self.ov = dict(ov or {})
         self.ctx = eb.Context(device, precision)
+        if scheme is not None:
+            self.ctx.set_force_scheme(scheme)
         # A dedicated (non-default) stream: the library launches on it and the
         # CUDA events that time the steps are recorded on it.
         # High priority: the library's real-space side stream (lowest priority)
@@ -259,12 +268,13 @@ class Arm:
         torch.cuda.synchronize()
 
     def step_device(self):
-        self.ctx.potential_force_device(self.x, self.q, self.lat, self.tol, self.pot, self.force)
+        self.ctx.potential_force_device(self.x, self.q, self.lat, self.tol, self.pot, self.force,
+                                        **self.ov)
 
     def step_e2e(self):
         L = self.eb.lib()
         dp = C.POINTER(C.c_double)
-        ov = self.eb.Overrides()
+        ov = self.eb._overrides(**self.ov)
         rc = L.ewg_potential_force(self.ctx.handle, self.n, self.h_pos.ctypes.data_as(dp),
                                    self.h_q.ctypes.data_as(dp), self.lat.ctypes.data_as(dp),
                                    float(self.tol), self.h_pot.ctypes.data_as(dp),
@@ -404,29 +414,43 @@ def run_ours(args):
     if args.profile_only:
         # For profiler captures: warm-up + steps evaluations of one form, nothing
         # timed, no JSON line (numbers taken under a profiler are not results).
-        prec, tol = (eb.FP64, TOL_FP64) if args.profile_only == "fp64" else (eb.MIXED, TOL_MIXED)
-        arm = Arm(eb, torch, device, prec, tol, pos, q, lat)
+        prec, tol = (eb.MIXED, TOL_MIXED) if args.profile_only == "mixed" else (eb.FP64, TOL_FP64)
+        scheme = eb.FORCE_AD if args.profile_only == "fp64_ad" else None
+        arm = Arm(eb, torch, device, prec, tol, pos, q, lat, scheme=scheme)
         for _ in range(args.warmup + args.steps):
             arm.step_device()
         torch.cuda.synchronize()
         print(f"profile-only: {args.warmup + args.steps} {args.profile_only} evaluations", flush=True)
         return 0
 
+    # Three arms on the same inputs:
+    #   fp64     the plain form: FP64, the reference's parameters and its i k forces;
+    #   fp64_ad  the same with forces by window differentiation (one inverse FFT);
+    #   mixed    the mixed form (FP32 stencils, FFT and pair terms), with the
+    #            force scheme and parameters from the library's autotuner for an
+    #            RMS force error of at most MIXED_TARGET / 2 against fp64.
     fp64 = Arm(eb, torch, device, eb.FP64, TOL_FP64, pos, q, lat)
-    mixed = Arm(eb, torch, device, eb.MIXED, TOL_MIXED, pos, q, lat)
+    fp64_ad = Arm(eb, torch, device, eb.FP64, TOL_FP64, pos, q, lat, scheme=eb.FORCE_AD)
+    tuner = eb.Context(device, eb.MIXED)
+    tuned_ov, tuned_scheme, tune_report = tuner.tune(pos, q, lat, MIXED_TARGET)  # untimed, once
+    tuner.close()
+    mixed = Arm(eb, torch, device, eb.MIXED, TOL_MIXED, pos, q, lat, scheme=tuned_scheme,
+                ov=tuned_ov)
+    scheme_name = {eb.FORCE_IK: "ik", eb.FORCE_AD: "window differentiation"}
 
-    # accuracy of the mixed form against the FP64 form (same inputs)
-    fp64.step_device()
-    mixed.step_device()
+    # accuracy of the other arms against the plain form (same inputs)
+    for a in (fp64, fp64_ad, mixed):
+        a.step_device()
     torch.cuda.synchronize()
     p64, f64 = fp64.pot.cpu().numpy(), fp64.force.cpu().numpy()
-    p32, f32 = mixed.pot.cpu().numpy(), mixed.force.cpu().numpy()
 
     def rel(a, b):
         return {"max": float(np.abs(a - b).max() / np.abs(b).max()),
                 "rms": float(np.sqrt(np.mean((a - b) ** 2)) / np.sqrt(np.mean(b ** 2)))}
 
-    err = {"potential": rel(p32, p64), "force": rel(f32, f64)}
+    err = {"potential": rel(mixed.pot.cpu().numpy(), p64), "force": rel(mixed.force.cpu().numpy(), f64)}
+    err_ad = {"potential": rel(fp64_ad.pot.cpu().numpy(), p64),
+              "force": rel(fp64_ad.force.cpu().numpy(), f64)}
     params64 = fp64.ctx.last_params()
     params32 = mixed.ctx.last_params()
 
@@ -442,15 +466,20 @@ def run_ours(args):
     ms64, launches64, _ = fp64.time_device(args.steps, args.warmup)
     clocks = sampler.stop()
     barrier()
+    msad, launchesad, _ = fp64_ad.time_device(args.steps, args.warmup)
+    barrier()
     ms32, launches32, _ = mixed.time_device(args.steps, args.warmup)
     barrier()
     # Per-stage device times come from a separate profiled pass: with stage
     # events on, the library runs the real-space sum in line instead of beside
     # the mesh pipeline, so these stages add up to more than the step time.
     _, _, stages = fp64.time_device(args.steps, 0, profile=True)
+    _, _, stagesad = fp64_ad.time_device(args.steps, 0, profile=True)
     _, _, stages32 = mixed.time_device(args.steps, 0, profile=True)
     barrier()
     e2e64 = fp64.time_e2e(args.steps, args.warmup)
+    barrier()
+    e2ead = fp64_ad.time_e2e(args.steps, args.warmup)
     barrier()
     e2e32 = mixed.time_e2e(args.steps, args.warmup)
     barrier()
@@ -463,8 +492,10 @@ def run_ours(args):
         return float(t.item())
 
     t64 = maxrank(sum(ms64) / 1e3)
+    tad = maxrank(sum(msad) / 1e3)
     t32 = maxrank(sum(ms32) / 1e3)
     te64 = maxrank(e2e64)
+    tead = maxrank(e2ead)
     te32 = maxrank(e2e32)
 
     cpu = None
@@ -484,13 +515,15 @@ def run_ours(args):
     peak, peak_kind = load_peaks()
     natoms = len(q)
 
-    def roofline(stages_ms, params, real_bytes, steps, tensor_peak=None):
+    def roofline(stages_ms, params, real_bytes, steps, tensor_peak=None, nc=4):
         """Per-stage rates; the roofline entry is the stage with the largest time.
         HBM-type stages (the FFT passes; every stage in the FP32 form) use
         algorithmic bytes / time against the measured copy bandwidth.  The FP64
         spread and gather run on the FP64 tensor cores (DMMA): algorithmic FP64
-        flops / time against the FP64 tensor rate measured live on this GPU."""
-        sb = stage_bytes(params, natoms, real_bytes)
+        flops / time against the FP64 tensor rate measured live on this GPU.
+        nc: grids through the inverse passes and the gather (4 for i k, 1 for
+        window differentiation)."""
+        sb = stage_bytes(params, natoms, real_bytes, nc)
         fl = stage_flops(params, natoms) if tensor_peak else {}
         per = {}
         for name, (ms, _) in stages_ms.items():
@@ -506,7 +539,7 @@ def run_ours(args):
                 entry["bytes"] = sb[name]
             per[name] = entry
         top = max((k for k in per if k in sb or k in fl), key=lambda k: per[k]["ms"])
-        traffic = DRAM_TRAFFIC.get((real_bytes, top))
+        traffic = DRAM_TRAFFIC.get((real_bytes, nc, top))
         if top in fl:
             ach = per[top]["tflops"]
             roof = {"bound": "tensor", "kernel": top, "achieved": ach, "peak": tensor_peak,
@@ -519,42 +552,57 @@ def run_ours(args):
                     "frac": ach / peak, "peak_source": f"{peak_kind} hbm_gbs", "traffic": traffic}
         return top, per, roof
 
-    def whole_eval(params, real_bytes, t_step):
-        """B_force = 19 G + 8 N s bytes per evaluation against the measured HBM rate."""
-        n = [2 * m for m in params["n_modes"]]
-        G = n[0] * n[1] * n[2] * real_bytes
-        b = 19 * G + 8 * natoms * real_bytes
+    def whole_eval(params, real_bytes, t_step, nc=4):
+        """Algorithmic bytes of one evaluation (the sum of the stage counts)
+        against the measured HBM rate."""
+        b = sum(stage_bytes(params, natoms, real_bytes, nc).values())
         return {"bytes": b, "achieved_gbs": b / t_step / 1e9, "frac": b / t_step / 1e9 / peak}
 
+    def grid_of(params):
+        return "x".join(str(2 * m) for m in params["n_modes"])
+
     top64, per64, roof64 = roofline(stages, params64, 8, args.steps, tensor_peak)
-    top32, per32, roof32 = roofline(stages32, params32, 4, args.steps)
+    _, perad, roofad = roofline(stagesad, params64, 8, args.steps, tensor_peak, nc=1)
+    nc32 = 1 if tuned_scheme == eb.FORCE_AD else 4
+    top32, per32, roof32 = roofline(stages32, params32, 4, args.steps, nc=nc32)
     h2d = natoms * 3 * 8 + natoms * 8
     d2h = natoms * 8 + natoms * 3 * 8
     value = ws * args.steps / t64
+    e2e_io = {"h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
     line = {
         "metric": metric_for(args.workload, natoms), "value": value, "unit": "evals/s", "n_gpus": ws,
         "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t64 / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": label, "natoms": natoms,
-                   "tol": TOL_FP64, "grid": "x".join(str(2 * m) for m in params64["n_modes"]),
+                   "tol": TOL_FP64, "grid": grid_of(params64),
                    "window_cutoff": params64["window_cutoff"], "alpha": params64["alpha"],
-                   "r_cut_bohr": params64["r_cut"], "parallelism": f"replicas x{ws}",
+                   "r_cut_bohr": params64["r_cut"], "forces": "ik (the reference's scheme)",
+                   "parallelism": f"replicas x{ws}",
                    "l2": "flushed between steps (256 MiB write, untimed); working set > L2"},
-        "e2e": {"value": ws * args.steps / te64, "unit": "evals/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h},
+        "e2e": dict(value=ws * args.steps / te64, unit="evals/s", **e2e_io),
         "roofline": roof64,
         "whole_eval_hbm": whole_eval(params64, 8, t64 / args.steps),
         "stages_ms": per64,
+        "fp64_ad": {
+            "value": ws * args.steps / tad, "unit": "evals/s", "forces": "window differentiation",
+            "speedup_vs_fp64": (ws * args.steps / tad) / value,
+            "e2e": dict(value=ws * args.steps / tead, unit="evals/s", **e2e_io),
+            "rel_err_vs_fp64": err_ad, "roofline": roofad,
+            "whole_eval_hbm": whole_eval(params64, 8, tad / args.steps, nc=1), "stages_ms": perad,
+            "gpu_launches": launchesad,
+        },
         "mixed": {
-            "value": ws * args.steps / t32, "unit": "evals/s", "tol": TOL_MIXED,
-            "grid": "x".join(str(2 * m) for m in params32["n_modes"]),
-            "window_cutoff": params32["window_cutoff"],
+            "value": ws * args.steps / t32, "unit": "evals/s", "forces": scheme_name[tuned_scheme],
+            "params": {"source": f"ewg_tune, target {MIXED_TARGET:g} (RMS force error <= "
+                                 f"{MIXED_TARGET / 2:g} vs the FP64 form)",
+                       "alpha": params32["alpha"], "r_cut_bohr": params32["r_cut"],
+                       "grid": grid_of(params32), "window_cutoff": params32["window_cutoff"],
+                       "tuner_report": tune_report},
             "speedup_vs_fp64": (ws * args.steps / t32) / value,
-            "e2e": {"value": ws * args.steps / te32, "unit": "evals/s",
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": dict(value=ws * args.steps / te32, unit="evals/s", **e2e_io),
             "rel_err_vs_fp64": err, "roofline": roof32,
-            "whole_eval_hbm": whole_eval(params32, 4, t32 / args.steps), "stages_ms": per32,
+            "whole_eval_hbm": whole_eval(params32, 4, t32 / args.steps, nc=nc32), "stages_ms": per32,
             "gpu_launches": launches32,
         },
         "gpu_launches": launches64,
@@ -575,7 +623,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["c3", "c1", "c2", "c5", "c4", "c5_scc"], default="c3",
                     help="c3 (default, the headline) or another configuration of the table")
-    ap.add_argument("--profile-only", choices=["fp64", "mixed"], default=None,
+    ap.add_argument("--profile-only", choices=["fp64", "fp64_ad", "mixed"], default=None,
                     help="run warm-up + steps evaluations of one form for a profiler; no timing")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -26,7 +26,7 @@ enum BufId {
   B_QK, B_GRID, B_A1, B_A2, B_B2, B_B1, B_OUT, B_ERR, B_SUMS, B_PARTIAL, B_KVEC, B_SK, B_WK,
   B_P6, B_O6, B_COORDS, B_SLOT, B_PART, B_PAIRTMP, B_PAIRS, B_PAIRSTART, B_CELLERR, B_ZPART,
   B_BCOUNTS, B_BCURSOR, B_BTMP, B_EXT_T, B_EXT_S, B_EXT_SQ, B_EXT_TQ, B_EXT_BLUR, B_EXT_R,
-  B_EXT_G, B_EXT_SF, B_EXT_SF2, B_EXT_OUT, B_EXT_OUT2, B_COUNT
+  B_EXT_G, B_EXT_SF, B_EXT_SF2, B_EXT_OUT, B_EXT_OUT2, B_X32S, B_TUNE_POT, B_TUNE_FORCE, B_COUNT
 };
 
 struct DevBuf {
@@ -81,6 +81,8 @@ struct ewg_context {
   cudaStream_t own_stream = nullptr;
   // Charged cells: accept a net charge with a uniform neutralising background.
   bool background = false;
+  // Force differentiation scheme (EWG_FORCE_IK / EWG_FORCE_AD).
+  int force_scheme = EWG_FORCE_IK;
   // Second stream for the real-space sum, which runs beside the mesh pipeline:
   // forked from `stream` after the atom sort, joined before the final assembly.
   cudaStream_t side = nullptr;
@@ -103,10 +105,34 @@ struct ewg_context {
     int ng[3] = {0, 0, 0};
     int m = -1;
     int mixed = -1;
+    int ad = -1;
   } resident;
   long long uploaded_charges = -1;
   StockSetup stock;
   bool stock_valid = false;
+  // CUDA graphs of evaluation launch sequences, keyed by everything the
+  // sequence depends on (sizes, device pointers, parameters, cell, buffer
+  // generation).  A key is captured on its second sighting and replayed after.
+  bool graphs_on = true;
+  long long buf_gen = 0;  // bumped whenever a device buffer is reallocated
+  struct GraphEntry {
+    cudaGraphExec_t exec;
+    long long launches;
+  };
+  std::map<std::vector<unsigned long long>, GraphEntry> graphs;
+  std::map<std::vector<unsigned long long>, int> graph_seen;
+  void drop_graphs() {
+    for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);
+    graphs.clear();
+    graph_seen.clear();
+  }
+  // Autotuner results per (atoms, precision, scheme, lattice, target).
+  struct TuneEntry {
+    ewg_overrides ov;
+    int scheme;
+    double report[4];
+  };
+  std::map<std::vector<double>, TuneEntry> tuned;
   int last_ng = 0;
   Profiler prof;
 
@@ -122,6 +148,7 @@ struct ewg_context {
       cudaFree(kv.second.tw32);
     }
     for (auto& kv : corrs) cudaFree(kv.second.dev);
+    drop_graphs();
     for (auto& e : prof.ev)
       if (e) cudaEventDestroy(e);
     if (fork) cudaEventDestroy(fork);
@@ -150,6 +177,8 @@ T* dbuf(ewg_context* c, BufId id, size_t count, int* rc) {
       b.p = nullptr;
       b.cap = 0;
     }
+    ++c->buf_gen;  // recorded launch sequences hold the old address
+    c->drop_graphs();
     const size_t grown = bytes + bytes / 8;
     if (cudaMalloc(&b.p, grown) != cudaSuccess) {
       cudaGetLastError();
@@ -270,7 +299,7 @@ int mesh_geometry(const Cell& cell, const ewg_params& p, MeshGeom& g) {
 // Particle-side tiling: per axis the most tiles one stencil can touch
 // (brute force over start points, so partial last tiles are covered) and the
 // per-atom weight layout.
-void stencil_dims(const MeshGeom& g, StencilDims& sd) {
+void stencil_dims(const MeshGeom& g, bool ad, StencilDims& sd) {
   int off = 0;
   for (int d = 0; d < 3; ++d) {
     const int n = g.n[d], T = kTiles[d], nt = (n + T - 1) / T;
@@ -297,6 +326,9 @@ void stencil_dims(const MeshGeom& g, StencilDims& sd) {
     off += most * T;
   }
   sd.wstride = off;
+  sd.ad = ad ? 1 : 0;
+  sd.dwoff = off;
+  if (ad) sd.wstride = 2 * off;  // derivative rows follow the weight rows
   sd.m = g.m;
   sd.b = g.b;
   sd.pref = g.pref;
@@ -314,7 +346,11 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
   int rc = EWG_OK;
   cudaStream_t st = c->stream;
   const int mixed = c->precision == EWG_PRECISION_MIXED;
-  const int nc = want_force ? 4 : 1;
+  // ik: four grids (potential and the three i k components); ad: the potential
+  // grid alone, the gather differentiating the window.  Four partials either way.
+  const bool ad = want_force && c->force_scheme == EWG_FORCE_AD;
+  const int nc = want_force && !ad ? 4 : 1;
+  const int nparts = want_force ? 4 : 1;
   RealGeom rg;
   real_geometry(cell, p.r_cut, n, rg);
   MeshPlan mp;
@@ -328,13 +364,14 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
     if ((rc = get_corr(c, mp.g.n[d], H, mp.g.m, &mp.corr2[d]))) return rc;
   }
   if ((rc = mesh_check_lengths(mp.g, mixed))) return rc;
-  stencil_dims(mp.g, mp.sd);
+  stencil_dims(mp.g, ad, mp.sd);
   const int nboxes = rg.nb[0] * rg.nb[1] * rg.nb[2];
   const int ntiles = mp.sd.ntiles[0] * mp.sd.ntiles[1] * mp.sd.ntiles[2];
-  const MeshSizes ms = mesh_sizes(mp.g, mp.sd, mixed, nc, n);
+  const MeshSizes ms = mesh_sizes(mp.g, mp.sd, mixed, nc, n, nparts);
 
   double4* s4 = dbuf<double4>(c, B_S4, n, &rc);
   double4* s4s = dbuf<double4>(c, B_S4S, n, &rc);
+  float4* x32s = dbuf<float4>(c, B_X32S, n, &rc);
   int* boxkey = dbuf<int>(c, B_BOXKEY, n, &rc);
   int4* mcv = dbuf<int4>(c, B_MC, n, &rc);
   int4* mcs = dbuf<int4>(c, B_MCS, n, &rc);
@@ -376,77 +413,139 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
                      c->resident.nb[0] == rg.nb[0] && c->resident.nb[1] == rg.nb[1] &&
                      c->resident.nb[2] == rg.nb[2] && c->resident.ng[0] == mp.g.n[0] &&
                      c->resident.ng[1] == mp.g.n[1] && c->resident.ng[2] == mp.g.n[2] &&
-                     c->resident.m == mp.g.m && c->resident.mixed == mixed;
-  if (!err_flag) cudaMemsetAsync(err, 0, sizeof(int), st);
+                     c->resident.m == mp.g.m && c->resident.mixed == mixed &&
+                     c->resident.ad == mp.sd.ad;
+  double* p6 = nullptr;
+  double* zpart = nullptr;
+  const size_t nz = 6 * static_cast<size_t>(mp.g.K1) * mp.g.K2;
+  if (stress12) {
+    p6 = dbuf<double>(c, B_P6, 6 * static_cast<size_t>(n), &rc);
+    zpart = dbuf<double>(c, B_ZPART, nz, &rc);
+    if (rc) return rc;
+  }
   // The real-space branch (box sort, permutation, erfc pair sum; FP64 pipe and
   // issue bound) runs on the low-priority side stream beside the mesh pipeline
   // (memory and tensor bound), forked after the atom preparation and joined
   // before the final assembly.  With stage events on, everything runs in line.
   const bool concurrent = !c->prof.on;
   cudaStream_t rs = concurrent ? c->side : st;
-  prof_mark(mp.prof, st, ST_PREP);
-  if (!reuse) {
-    launch_atom_prep(pos, sa, sd, q, n, cell, rg.nb, mp.g.n, kTiles, mp.sd.ntiles, s4, boxkey, mcv,
-                     fr, tilekey, st);
-    if (concurrent) {
-      cudaEventRecord(c->fork, st);
-      cudaStreamWaitEvent(rs, c->fork, 0);
-    }
-    launch_bucket_sort(boxkey, n, nboxes, bcounts, bcursor, boxstart, btmp, permbox, rs);
-    launch_permute4(s4, permbox, n, s4s, rs);
-    launch_bucket_sort(tilekey, n, ntiles, counts, cursor, tilestart, tmp, permmesh, st);
-    launch_permute_int4(mcv, permmesh, n, mcs, st);
-    launch_permute4(fr, permmesh, n, frs, st);
-    prof_mark(mp.prof, st, ST_WEIGHTS);
-    launch_weights(mp, mcs, frs, n, wtab, qk, slot, st);
-    launch_pair_bins(mp, slot, n, counts, cursor, pairstart, pairtmp, pairs, npairs_max, st);
-    if (resident) {
-      c->resident.coords_version = c->coords_version;
-      for (int d = 0; d < 3; ++d) {
-        c->resident.nb[d] = rg.nb[d];
-        c->resident.ng[d] = mp.g.n[d];
+  const double self_coef = -2.0 * p.alpha / std::sqrt(kPi);
+  // The whole launch sequence of this evaluation (no host synchronisation,
+  // no allocation inside).
+  auto launch_all = [&]() {
+    if (!err_flag) cudaMemsetAsync(err, 0, sizeof(int), st);
+    prof_mark(mp.prof, st, ST_PREP);
+    if (!reuse) {
+      launch_atom_prep(pos, sa, sd, q, n, cell, rg.nb, mp.g.n, kTiles, mp.sd.ntiles, s4, boxkey,
+                       mcv, fr, tilekey, st);
+      if (concurrent) {
+        cudaEventRecord(c->fork, st);
+        cudaStreamWaitEvent(rs, c->fork, 0);
       }
-      c->resident.m = mp.g.m;
-      c->resident.mixed = mixed;
+      launch_bucket_sort(boxkey, n, nboxes, bcounts, bcursor, boxstart, btmp, permbox, rs);
+      launch_permute_box(s4, permbox, n, cell.lat, s4s, x32s, rs);
+      launch_bucket_sort(tilekey, n, ntiles, counts, cursor, tilestart, tmp, permmesh, st);
+      launch_permute_int4(mcv, permmesh, n, mcs, st);
+      launch_permute4(fr, permmesh, n, frs, st);
+      prof_mark(mp.prof, st, ST_WEIGHTS);
+      launch_weights(mp, mcs, frs, n, wtab, qk, slot, st);
+      launch_pair_bins(mp, slot, n, counts, cursor, pairstart, pairtmp, pairs, npairs_max, st);
+    } else {
+      // Geometry unchanged: refresh only the charges in the sorted layouts.
+      launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, nullptr, nullptr, nullptr, s4, nullptr,
+                       nullptr, nullptr, nullptr, st);
+      if (concurrent) {
+        cudaEventRecord(c->fork, st);
+        cudaStreamWaitEvent(rs, c->fork, 0);
+      }
+      launch_permute_box(s4, permbox, n, cell.lat, s4s, x32s, rs);
+      launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, mp.g.n, kTiles, mp.sd.ntiles, nullptr,
+                       nullptr, mcv, fr, tilekey, st);
+      launch_permute4(fr, permmesh, n, frs, st);
+      prof_mark(mp.prof, st, ST_WEIGHTS);
+      launch_weights(mp, mcs, frs, n, wtab, qk, slot, st);
+    }
+    prof_mark(mp.prof, st, ST_REAL);
+    launch_real_space(s4s, x32s, permbox, boxstart, n, rg, p.alpha, p.r_cut, mixed, pot_sr, f_sr,
+                      err, rs);
+    if (stress12) {  // real-space virial over the same pairs, and z-pass partials zeroed
+      launch_real_stress(s4s, x32s, boxstart, n, rg, p.alpha, p.r_cut, p6, stress12, err, rs);
+      cudaMemsetAsync(zpart, 0, sizeof(double) * nz, st);
+    }
+    if (concurrent) cudaEventRecord(c->join, rs);
+    prof_mark(mp.prof, st, ST_SPREAD);
+    launch_spread(mp, pairstart, pairs, wtab, qk, grid, st);
+    launch_forward_and_weight(mp, grid, A1, A2, B2, nc, st, zpart);
+    if (stress12) launch_sum_partials(zpart, mp.g.K1 * mp.g.K2, 6, stress12 + 6, st);
+    launch_inverse(mp, B2, B1, outg, nc, st);
+    prof_mark(mp.prof, st, ST_GATHER);
+    launch_gather(mp, pairstart, pairs, wtab, mcs, outg, nc, part, st);
+    if (concurrent) cudaStreamWaitEvent(st, c->join, 0);  // pot_sr, f_sr, err ready
+    launch_gather_final(mp, slot, permmesh, part, nparts, n, q, self_coef, pot_shift, pot_sr, f_sr,
+                        pot, want_force ? force : nullptr, ad ? cell.rec : nullptr, st);
+  };
+  if (c->graphs_on && concurrent) {
+    // Replay: everything the sequence depends on is in the key.
+    std::vector<unsigned long long> key;
+    auto put = [&key](auto v) {
+      unsigned long long u = 0;
+      static_assert(sizeof(v) <= sizeof(u), "key field");
+      std::memcpy(&u, &v, sizeof(v));
+      key.push_back(u);
+    };
+    put(n), put(sa), put(sd), put(pos), put(q), put(pot), put(want_force ? force : nullptr);
+    put(err), put(err_flag), put(stress12), put(reuse), put(mixed), put(mp.sd.ad), put(nc);
+    put(p.alpha), put(p.r_cut), put(p.k_cut), put(p.window_cutoff);
+    for (int d = 0; d < 3; ++d) put(p.n_modes[d]);
+    for (int i = 0; i < 3; ++i)
+      for (int d = 0; d < 3; ++d) put(cell.lat[i][d]);
+    put(pot_shift), put(c->buf_gen), put(st), put(rs);
+    auto hit = c->graphs.find(key);
+    if (hit != c->graphs.end()) {
+      cudaGraphLaunch(hit->second.exec, st);
+      g_launches += hit->second.launches;
+    } else if (c->graph_seen.count(key)) {
+      // Second sighting: record the sequence once, then replay it from now on.
+      if (c->graphs.size() >= 64) c->drop_graphs();
+      cudaGraph_t graph = nullptr;
+      cudaGraphExec_t exec = nullptr;
+      const long long before = g_launches;
+      bool ok = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      if (ok) {
+        launch_all();
+        ok = cudaStreamEndCapture(st, &graph) == cudaSuccess && graph &&
+             cudaGraphInstantiateWithFlags(&exec, graph, cudaGraphInstantiateFlagUseNodePriority) ==
+                 cudaSuccess;
+      }
+      if (graph) cudaGraphDestroy(graph);
+      const long long recorded = g_launches - before;
+      g_launches = before;
+      if (ok) {
+        c->graphs[key] = ewg_context::GraphEntry{exec, recorded};
+        cudaGraphLaunch(exec, st);
+        g_launches += recorded;
+      } else {  // capture unavailable on this stream: launch directly
+        cudaGetLastError();
+        launch_all();
+      }
+    } else {
+      if (c->graph_seen.size() >= 1024) c->graph_seen.clear();
+      c->graph_seen[key] = 1;
+      launch_all();
     }
   } else {
-    // Geometry unchanged: refresh only the charges in the sorted layouts.
-    launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, nullptr, nullptr, nullptr, s4, nullptr,
-                     nullptr, nullptr, nullptr, st);
-    if (concurrent) {
-      cudaEventRecord(c->fork, st);
-      cudaStreamWaitEvent(rs, c->fork, 0);
+    launch_all();
+  }
+  if (resident && !reuse) {
+    c->resident.coords_version = c->coords_version;
+    for (int d = 0; d < 3; ++d) {
+      c->resident.nb[d] = rg.nb[d];
+      c->resident.ng[d] = mp.g.n[d];
     }
-    launch_permute4(s4, permbox, n, s4s, rs);
-    launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, mp.g.n, kTiles, mp.sd.ntiles, nullptr,
-                     nullptr, mcv, fr, tilekey, st);
-    launch_permute4(fr, permmesh, n, frs, st);
-    prof_mark(mp.prof, st, ST_WEIGHTS);
-    launch_weights(mp, mcs, frs, n, wtab, qk, slot, st);
+    c->resident.m = mp.g.m;
+    c->resident.mixed = mixed;
+    c->resident.ad = mp.sd.ad;
   }
-  prof_mark(mp.prof, st, ST_REAL);
-  launch_real_space(s4s, permbox, boxstart, n, rg, p.alpha, p.r_cut, mixed, pot_sr, f_sr, err, rs);
-  double* zpart = nullptr;
-  if (stress12) {  // real-space virial over the same pairs, and z-pass partials zeroed
-    const size_t nz = 6 * static_cast<size_t>(mp.g.K1) * mp.g.K2;
-    double* p6 = dbuf<double>(c, B_P6, 6 * static_cast<size_t>(n), &rc);
-    zpart = dbuf<double>(c, B_ZPART, nz, &rc);
-    if (rc) return rc;
-    launch_real_stress(s4s, boxstart, n, rg, p.alpha, p.r_cut, p6, stress12, err, rs);
-    cudaMemsetAsync(zpart, 0, sizeof(double) * nz, st);
-  }
-  if (concurrent) cudaEventRecord(c->join, rs);
-  prof_mark(mp.prof, st, ST_SPREAD);
-  launch_spread(mp, pairstart, pairs, wtab, qk, grid, st);
-  launch_forward_and_weight(mp, grid, A1, A2, B2, nc, st, zpart);
-  if (stress12) launch_sum_partials(zpart, mp.g.K1 * mp.g.K2, 6, stress12 + 6, st);
-  launch_inverse(mp, B2, B1, outg, nc, st);
-  const double self_coef = -2.0 * p.alpha / std::sqrt(kPi);
-  prof_mark(mp.prof, st, ST_GATHER);
-  launch_gather(mp, pairstart, pairs, wtab, outg, nc, part, st);
-  if (concurrent) cudaStreamWaitEvent(st, c->join, 0);  // pot_sr, f_sr, err ready
-  launch_gather_final(mp, slot, permmesh, part, nc, n, q, self_coef, pot_shift, pot_sr, f_sr, pot,
-                      want_force ? force : nullptr, st);
   prof_mark(mp.prof, st, -1);
   if (err_flag && !c->prof.on) {  // deferred: the caller synchronises and reads the flag
     const cudaError_t le = cudaGetLastError();
@@ -595,6 +694,20 @@ int ewg_set_background(ewg_context* c, int on) {
   return EWG_OK;
 }
 
+int ewg_set_graphs(ewg_context* c, int on) {
+  if (!c) return EWG_ERR_ARG;
+  c->graphs_on = on != 0;
+  if (!c->graphs_on) c->drop_graphs();
+  return EWG_OK;
+}
+
+int ewg_set_force_scheme(ewg_context* c, int scheme) {
+  if (!c || (scheme != EWG_FORCE_IK && scheme != EWG_FORCE_AD)) return EWG_ERR_ARG;
+  c->force_scheme = scheme;
+  c->resident.coords_version = -1;  // the weight layout depends on the scheme
+  return EWG_OK;
+}
+
 int ewg_fp64_mma_peak(ewg_context* c, double* tflops) {
   if (!c || !tflops) return EWG_ERR_ARG;
   cudaSetDevice(c->device);
@@ -685,9 +798,12 @@ int ewg_device_memory(int n, const double* charges, const double* lat_rows, doub
   MeshGeom g;
   rc = mesh_geometry(cell, p, g);
   if (rc) return rc;
+  // Sizes for the precision's default force scheme (ik for FP64, ad for mixed).
+  const bool mixed = precision == EWG_PRECISION_MIXED;
+  const bool ad = with_force && mixed;
   StencilDims sd;
-  stencil_dims(g, sd);
-  const MeshSizes s = mesh_sizes(g, sd, precision == EWG_PRECISION_MIXED, with_force ? 4 : 1, n);
+  stencil_dims(g, ad, sd);
+  const MeshSizes s = mesh_sizes(g, sd, mixed, with_force && !ad ? 4 : 1, n, with_force ? 4 : 1);
   const double atoms = static_cast<double>(n) * (32 * 4 + 16 * 2 + 4 * 6 + 8 * 6);
   *bytes = static_cast<double>(s.grid + s.A1 + s.A2 + s.B2 + s.B1 + s.out + s.wtab + s.qk + s.slot +
                                s.part) +
@@ -804,6 +920,180 @@ int ewg_potential_force_device(ewg_context* c, int n, const double* coords_devic
                   background_shift(c, h[0], cell, p.alpha));
 }
 
+// Parameter autotuner.  Candidates: both force schemes, and the reference chain
+// (choose_parameters) at tolerances tol = target/10, target/5, target/3, with
+// the real-space cutoff overridden to 1, 1.15, 1.3 or 1.5 times the chain's own
+// (alpha then follows from the real-space budget, k_cut from the Fourier budget,
+// the modes from k_cut) and window half-widths 6 to 9.  Each candidate is
+// evaluated once on the caller's configuration and compared with an FP64 i k
+// evaluation at the reference's parameters for tol = 1e-10; those within the
+// bar are timed with CUDA events over three evaluations, and the fastest is
+// returned.  The context's own force scheme is left as it was.
+int ewg_tune(ewg_context* c, int n, const double* positions, const double* charges,
+             const double* lat_rows, double target, ewg_overrides* out, int* scheme_out,
+             double* report) {
+  if (!c || !out) return EWG_ERR_ARG;
+  if (!(target > 0.0 && target < 1.0)) return EWG_ERR_TOL;
+  LaunchScope scope(c);
+  c->uploaded_charges = -1;
+  c->resident.coords_version = -1;
+  Cell cell;
+  double q2 = 0.0, qsum = 0.0;
+  int rc = validate_host(c, n, positions, charges, lat_rows, 0.5, cell, q2, qsum);
+  if (rc) return rc;
+  std::vector<double> key = {static_cast<double>(n), static_cast<double>(c->precision), target};
+  for (int i = 0; i < 9; ++i) key.push_back(lat_rows[i]);
+  auto hit = c->tuned.find(key);
+  if (hit != c->tuned.end()) {
+    *out = hit->second.ov;
+    if (scheme_out) *scheme_out = hit->second.scheme;
+    if (report)
+      for (int i = 0; i < 4; ++i) report[i] = hit->second.report[i];
+    return EWG_OK;
+  }
+  double* dpos = dbuf<double>(c, B_POS, 3 * static_cast<size_t>(n), &rc);
+  double* dq = dbuf<double>(c, B_Q, n, &rc);
+  double* dpot = dbuf<double>(c, B_POT, n, &rc);
+  double* dforce = dbuf<double>(c, B_FORCE, 3 * static_cast<size_t>(n), &rc);
+  double* rpot = dbuf<double>(c, B_TUNE_POT, n, &rc);
+  double* rforce = dbuf<double>(c, B_TUNE_FORCE, 3 * static_cast<size_t>(n), &rc);
+  if (rc) return rc;
+  cudaStream_t st = c->stream;
+  cudaMemcpyAsync(dpos, positions, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(dq, charges, sizeof(double) * n, cudaMemcpyHostToDevice, st);
+  const double shift_scale = c->background ? qsum : 0.0;
+
+  // Reference: FP64, i k, the reference's parameters for tol = 1e-10.
+  ewg_params pref;
+  if ((rc = choose_parameters(cell, q2, n, 1e-10, nullptr, pref))) return rc;
+  const int precision = c->precision, scheme = c->force_scheme;
+  c->precision = EWG_PRECISION_FP64;
+  c->force_scheme = EWG_FORCE_IK;
+  rc = evaluate(c, n, dpos, 1, n, dq, cell, pref, true, rpot, rforce, false, nullptr, nullptr,
+                background_shift(c, shift_scale, cell, pref.alpha));
+  c->precision = precision;
+  c->force_scheme = scheme;
+  c->resident.coords_version = -1;
+  if (rc) return rc;
+  std::vector<double> ref_pot(n), ref_force(3 * static_cast<size_t>(n)), hp(n),
+      hf(3 * static_cast<size_t>(n));
+  cudaMemcpyAsync(ref_pot.data(), rpot, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(ref_force.data(), rforce, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_status(e);
+  auto rms_rel = [](const std::vector<double>& a, const std::vector<double>& b) {
+    double num = 0.0, den = 0.0;
+    for (size_t i = 0; i < a.size(); ++i) {
+      num += (a[i] - b[i]) * (a[i] - b[i]);
+      den += b[i] * b[i];
+    }
+    return den > 0.0 ? std::sqrt(num / den) : std::sqrt(num);
+  };
+
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    cudaGetLastError();
+    return EWG_ERR_CUDA;
+  }
+  ewg_params base;
+  if ((rc = choose_parameters(cell, q2, n, target / 10.0, nullptr, base))) return rc;
+  struct Best {
+    bool found = false;
+    ewg_params p{};
+    double ms = 0.0, ef = 0.0, ep = 0.0;
+    int scheme = EWG_FORCE_IK;
+  } best, closest;
+  closest.ef = 1e300;
+  // The candidate list: distinct parameter sets, each with both schemes.
+  struct Candidate {
+    ewg_params p;
+    int scheme;
+  };
+  std::vector<Candidate> cands;
+  std::vector<ewg_params> seen;
+  for (double tf : {0.1, 0.2, 1.0 / 3.0})
+    for (double rs : {1.0, 1.15, 1.3, 1.5})
+      for (int m : {6, 7, 8, 9}) {
+        ewg_overrides ov{};
+        ov.has_r_cut = 1;
+        ov.r_cut = base.r_cut * rs;
+        ov.has_window_cutoff = 1;
+        ov.window_cutoff = m;
+        ewg_params p;
+        if (choose_parameters(cell, q2, n, tf * target, &ov, p)) continue;
+        bool dup = false;
+        for (const auto& o : seen)
+          dup = dup || (o.alpha == p.alpha && o.r_cut == p.r_cut && o.window_cutoff == p.window_cutoff &&
+                        o.n_modes[0] == p.n_modes[0] && o.n_modes[1] == p.n_modes[1] &&
+                        o.n_modes[2] == p.n_modes[2]);
+        if (dup) continue;
+        seen.push_back(p);
+        cands.push_back({p, EWG_FORCE_AD});
+        cands.push_back({p, EWG_FORCE_IK});
+      }
+  int tried = 0;
+  for (const Candidate& cd : cands) {
+    const ewg_params& p = cd.p;
+    c->force_scheme = cd.scheme;
+    const double shift = background_shift(c, shift_scale, cell, p.alpha);
+    rc = evaluate(c, n, dpos, 1, n, dq, cell, p, true, dpot, dforce, false, nullptr, nullptr, shift);
+    if (rc == EWG_ERR_OUT_OF_MEMORY || rc == EWG_ERR_GRID_TOO_LARGE) {
+      rc = EWG_OK;  // a grid this device cannot hold: not a candidate
+      continue;
+    }
+    if (rc) break;
+    ++tried;
+    cudaMemcpyAsync(hp.data(), dpot, sizeof(double) * n, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(hf.data(), dforce, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, st);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) {
+      rc = cuda_status(e);
+      break;
+    }
+    const double ef = rms_rel(hf, ref_force), ep = rms_rel(hp, ref_pot);
+    if (ef < closest.ef) closest = Best{true, p, 0.0, ef, ep, cd.scheme};
+    if (!(ef <= 0.5 * target && ep <= target)) continue;
+    cudaEventRecord(e0, st);
+    for (int r = 0; r < 3 && !rc; ++r)
+      rc = evaluate(c, n, dpos, 1, n, dq, cell, p, true, dpot, dforce, false, nullptr, nullptr, shift);
+    cudaEventRecord(e1, st);
+    float ms = 0.0f;
+    if (rc || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+      if (!rc) rc = EWG_ERR_CUDA;
+      break;
+    }
+    if (!best.found || ms / 3.0 < best.ms) best = Best{true, p, ms / 3.0, ef, ep, cd.scheme};
+  }
+  c->force_scheme = scheme;
+  c->resident.coords_version = -1;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  if (!best.found) {
+    if (!closest.found) return EWG_ERR_TOL;
+    best = closest;  // nothing within the bar: the most accurate candidate
+  }
+  ewg_overrides o{};
+  o.has_alpha = o.has_r_cut = o.has_k_cut = o.has_window_cutoff = 1;
+  o.alpha = best.p.alpha;
+  o.r_cut = best.p.r_cut;
+  o.k_cut = best.p.k_cut;
+  o.window_cutoff = best.p.window_cutoff;
+  ewg_context::TuneEntry te;
+  te.ov = o;
+  te.scheme = best.scheme;
+  te.report[0] = best.ef;
+  te.report[1] = best.ep;
+  te.report[2] = best.ms;
+  te.report[3] = tried;
+  c->tuned[key] = te;
+  *out = o;
+  if (scheme_out) *scheme_out = te.scheme;
+  if (report)
+    for (int i = 0; i < 4; ++i) report[i] = te.report[i];
+  return EWG_OK;
+}
+
 int ewg_direct_potential_force(ewg_context* c, int n, const double* positions,
                                const double* charges, const double* lat_rows, double tol,
                                double* pot, double* force, const double* alpha_in,
@@ -854,6 +1144,7 @@ int ewg_direct_potential_force(ewg_context* c, int n, const double* positions,
   double* dforce = dbuf<double>(c, B_FORCE, 3 * static_cast<size_t>(n), &rc);
   double4* s4 = dbuf<double4>(c, B_S4, n, &rc);
   double4* s4s = dbuf<double4>(c, B_S4S, n, &rc);
+  float4* x32s = dbuf<float4>(c, B_X32S, n, &rc);
   int* boxkey = dbuf<int>(c, B_BOXKEY, n, &rc);
   int* counts = dbuf<int>(c, B_COUNTS, nboxes, &rc);
   int* cursor = dbuf<int>(c, B_CURSOR, nboxes, &rc);
@@ -879,8 +1170,8 @@ int ewg_direct_potential_force(ewg_context* c, int n, const double* positions,
   launch_atom_prep(dcoords, 3, 1, dq, n, cell, rg.nb, nullptr, nullptr, nullptr, s4, boxkey, nullptr,
                    nullptr, nullptr, st);
   launch_bucket_sort(boxkey, n, nboxes, counts, cursor, boxstart, tmp, permbox, st);
-  launch_permute4(s4, permbox, n, s4s, st);
-  launch_real_space(s4s, permbox, boxstart, n, rg, alpha, r_cut, 0, dpot, dforce, err, st);
+  launch_permute_box(s4, permbox, n, cell.lat, s4s, x32s, st);
+  launch_real_space(s4s, x32s, permbox, boxstart, n, rg, alpha, r_cut, 0, dpot, dforce, err, st);
   launch_structure_factors(dcoords, dq, n, dk, nk, dsk, st);
   launch_direct_kspace(dcoords, dq, n, dk, dwk, dsk, nk, dpot, dforce, st);
   int herr = 0;
@@ -1230,6 +1521,7 @@ int ewg_stress(ewg_context* c, double tol_ewald, double alpha, double* sigma) {
   double* dq = dbuf<double>(c, B_Q, n, &rc);
   double4* s4 = dbuf<double4>(c, B_S4, n, &rc);
   double4* s4s = dbuf<double4>(c, B_S4S, n, &rc);
+  float4* x32s = dbuf<float4>(c, B_X32S, n, &rc);
   int* boxkey = dbuf<int>(c, B_BOXKEY, n, &rc);
   int* counts = dbuf<int>(c, B_COUNTS, nboxes, &rc);
   int* cursor = dbuf<int>(c, B_CURSOR, nboxes, &rc);
@@ -1253,8 +1545,8 @@ int ewg_stress(ewg_context* c, double tol_ewald, double alpha, double* sigma) {
   launch_atom_prep(dcoords, 3, 1, dq, n, cell, rg.nb, nullptr, nullptr, nullptr, s4, boxkey, nullptr,
                    nullptr, nullptr, st);
   launch_bucket_sort(boxkey, n, nboxes, counts, cursor, boxstart, tmp, permbox, st);
-  launch_permute4(s4, permbox, n, s4s, st);
-  launch_real_stress(s4s, boxstart, n, rg, ss.alpha, ss.max_r, p6, o6, err, st);
+  launch_permute_box(s4, permbox, n, cell.lat, s4s, x32s, st);
+  launch_real_stress(s4s, x32s, boxstart, n, rg, ss.alpha, ss.max_r, p6, o6, err, st);
   launch_structure_factors(dcoords, dq, n, dk, ng, dsk, st);
   launch_recip_stress(dk, dsk, ng, ss.alpha, p6, o6 + 6, st);
   double h[12];

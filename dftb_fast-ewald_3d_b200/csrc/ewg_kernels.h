@@ -54,6 +54,10 @@ void launch_scan(const int* counts, int nkeys, int* starts, cudaStream_t st);
 // out[k] = in[perm[k]]
 void launch_permute4(const double4* in, const int* perm, int n, double4* out, cudaStream_t st);
 void launch_permute_int4(const int4* in, const int* perm, int n, int4* out, cudaStream_t st);
+// Box-sorted atoms: out[k] = in[perm[k]] (fractional s, q) and x32[k] the
+// Cartesian position s . lat with q, in FP32, for the real-space distance test.
+void launch_permute_box(const double4* in, const int* perm, int n, const double (*lat)[3],
+                        double4* out, float4* x32, cudaStream_t st);
 
 // Charge sums for the parameter chain on device-resident charges:
 // out[0] = sum q, out[1] = sum |q|, out[2] = sum q^2 (fixed-order reduction).
@@ -63,17 +67,17 @@ void launch_charge_sums(const double* q, int n, double* partial, double* out, cu
 // direct/ewald_direct_3d.f90:192-309) over box-sorted atoms.  Writes pot and
 // force (3,N) by original atom index.  mixed != 0 evaluates the pair terms in
 // FP32 and accumulates in FP64.
-void launch_real_space(const double4* s4_sorted, const int* perm, const int* box_start, int n,
-                       const RealGeom& g, double alpha, double r_cut, int mixed, double* pot,
-                       double* force, int* err, cudaStream_t st);
+void launch_real_space(const double4* s4_sorted, const float4* x32_sorted, const int* perm,
+                       const int* box_start, int n, const RealGeom& g, double alpha, double r_cut,
+                       int mixed, double* pot, double* force, int* err, cudaStream_t st);
 
 // Real-space virial of invRStress (coulomb.F90:2836-2905): per-atom partial
 // tensors (6 per atom) then a fixed-order sum into out6.
 // Fixed-order sum of np partial vectors of nv doubles (one CTA).
 void launch_sum_partials(const double* partial, int np, int nv, double* out, cudaStream_t st);
-void launch_real_stress(const double4* s4_sorted, const int* box_start, int n, const RealGeom& g,
-                        double alpha, double max_r, double* partial6, double* out6, int* err,
-                        cudaStream_t st);
+void launch_real_stress(const double4* s4_sorted, const float4* x32_sorted, const int* box_start,
+                        int n, const RealGeom& g, double alpha, double max_r, double* partial6,
+                        double* out6, int* err, cudaStream_t st);
 
 // Structure factors S(k) = sum_j q_j exp(i k . x_j) for a list of Cartesian
 // wave vectors; x(3,N) atom-major Cartesian coordinates.  out: 2 per vector.
@@ -107,6 +111,9 @@ struct StencilDims {
   int m;           // window half-width
   double b;        // window shape
   double pref;     // 1/sqrt(pi b)
+  int ad;          // 1: window derivatives stored after the weights (forces by
+                   // analytic differentiation of the window)
+  int dwoff;       // per-atom offset of the derivative rows (woff[d] + dwoff)
 };
 
 // Everything the mesh pipeline needs, resolved on the host.
@@ -148,21 +155,32 @@ void launch_inverse(const MeshPlan& mp, const void* B2, void* B1, void* out, int
 
 // Gather (forward_nfft_3d step 3, nfft/nfft.f90:380-402): per-(atom, tile)
 // partial sums of the nc interleaved real grids into part (nslots * nc per atom).
+// With mp.sd.ad and force wanted, the grid holds the potential alone (nc = 1)
+// and the partials are four: the potential and its derivatives along the three
+// fractional coordinates (window derivatives times the grid).  mesh_c: each
+// mesh-sorted atom's lowest stencil point (the FP32 form's reference value).
 void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs, const void* wtab,
-                   const void* out_grid, int nc, double* part, cudaStream_t st);
+                   const int4* mesh_c, const void* out_grid, int nc, double* part,
+                   cudaStream_t st);
 
 // Fixed-order sum of each atom's partials with the final assembly
 // (fft/ewald_fft_3d.f90:121-132): pot = (sr + lr) + self, force = sr + q lr.
+// nparts = 1 or 4.  rec (nullptr for ik partials): the dual basis rows b_d;
+// the partials are then fractional derivatives D_d and the long-range force
+// is -q sum_d D_d b_d.
 void launch_gather_final(const MeshPlan& mp, const int4* slot, const int* mesh_perm,
-                         const double* part, int nc, int n, const double* q_orig, double self_coef, double pot_shift,
-                         const double* pot_sr, const double* force_sr, double* pot, double* force,
-                         cudaStream_t st);
+                         const double* part, int nparts, int n, const double* q_orig,
+                         double self_coef, double pot_shift, const double* pot_sr,
+                         const double* force_sr, double* pot, double* force,
+                         const double (*rec)[3], cudaStream_t st);
 
-// Device byte sizes of the mesh buffers.
+// Device byte sizes of the mesh buffers (nc grid components, nparts partials
+// per (atom, slot)).
 struct MeshSizes {
   size_t grid, A1, A2, B2, B1, out, wtab, qk, slot, part;
 };
-MeshSizes mesh_sizes(const MeshGeom& g, const StencilDims& sd, int mixed, int nc, int natoms);
+MeshSizes mesh_sizes(const MeshGeom& g, const StencilDims& sd, int mixed, int nc, int natoms,
+                     int nparts);
 
 // Shared-memory limits of the FFT and gather kernels (once per device).
 // Stock Ewald lattice sums for potentials and gradients at arbitrary points

@@ -551,7 +551,8 @@ void prof_collect(Profiler* p) {
   p->n = 0;
 }
 
-MeshSizes mesh_sizes(const MeshGeom& g, const StencilDims& sd, int mixed, int nc, int natoms) {
+MeshSizes mesh_sizes(const MeshGeom& g, const StencilDims& sd, int mixed, int nc, int natoms,
+                     int nparts) {
   const size_t r = mixed ? 4 : 8, c = 2 * r;
   const size_t n1 = g.n[0], n2 = g.n[1], n3 = g.n[2];
   MeshSizes s;
@@ -564,7 +565,7 @@ MeshSizes mesh_sizes(const MeshGeom& g, const StencilDims& sd, int mixed, int nc
   s.wtab = static_cast<size_t>(natoms) * sd.wstride * r;
   s.qk = static_cast<size_t>(natoms) * r;
   s.slot = static_cast<size_t>(natoms) * 16;
-  s.part = static_cast<size_t>(natoms) * sd.S[0] * sd.S[1] * sd.S[2] * nc * 8;
+  s.part = static_cast<size_t>(natoms) * sd.S[0] * sd.S[1] * sd.S[2] * nparts * 8;
   return s;
 }
 

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <type_traits>
 
 #include "ewg_kernels.h"
 
@@ -174,6 +175,24 @@ __global__ void k_permute4(const double4* __restrict__ in, const int* __restrict
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < n) out[k] = in[perm[k]];
 }
+// Box-sorted atoms: fractional coordinates and charge in FP64, and beside them
+// the Cartesian position of the wrapped atom, x = s . lat, with the charge in
+// FP32 for the real-space candidate test.
+struct LatRows {
+  double a[3][3];
+};
+__global__ void k_permute_box(const double4* __restrict__ in, const int* __restrict__ perm, int n,
+                              LatRows lat, double4* __restrict__ out, float4* __restrict__ x32) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double4 v = in[perm[k]];
+  out[k] = v;
+  float c[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    c[d] = static_cast<float>(v.x * lat.a[0][d] + v.y * lat.a[1][d] + v.z * lat.a[2][d]);
+  x32[k] = make_float4(c[0], c[1], c[2], static_cast<float>(v.w));
+}
 __global__ void k_permute_int4(const int4* __restrict__ in, const int* __restrict__ perm, int n,
                                int4* __restrict__ out) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -235,63 +254,114 @@ __global__ void __launch_bounds__(256) k_sum_partials(const double* __restrict__
 
 // ---------------------------------------------------------------------------
 // Real-space pair sums.  One warp per (box-sorted) atom i; lanes take the
-// candidates of each contiguous run of neighbour boxes 32 at a time.  Only
-// about one candidate in eight lies inside the cutoff, so the candidates that
-// pass the distance test are first compacted into a per-warp queue in shared
-// memory; the warp evaluates the pair term (erfc, exp) 32 queued pairs at a
-// time with every lane busy.  The queue order, and so the summation order, is
-// fixed by the candidate order: results are bitwise reproducible.
+// candidates of each contiguous run of neighbour boxes 32 at a time.  The
+// distance test is a prefilter in FP32 on Cartesian positions of the wrapped
+// atoms (x_i - x_j - S lat, with the run's periodic shift S applied once per
+// run), with a margin above its rounding error.  Only about one candidate in
+// eight lies inside the cutoff, so the candidates that pass are first
+// compacted into a per-warp queue in shared memory as (j, S); the warp then
+// redoes, 32 queued pairs at a time with every lane busy, the separation
+// ((s_i - s_j) - S) . lat, the cutoff test and the coincidence test in FP64
+// from the fractional coordinates, as fft/ewald_fft_3d_real.f90:153-160 does,
+// and evaluates the pair term (FP64, or FP32 in the mixed form: an FP32
+// separation computed from Cartesian positions of up to a cell's size would
+// lose too many digits at bonded distances).  The queue order, and so the
+// summation order, is fixed by the candidate order: results are bitwise
+// reproducible.
 // ---------------------------------------------------------------------------
 constexpr int kRealThreads = 256;
 constexpr int kQueue = 64;  // per-warp queue: up to 31 carried over + 32 new
 
-template <class Pair>
-struct PairQueue {
-  double4* q;  // this warp's kQueue entries: separation (x, y, z), q_j
+// One candidate as the scan hands it over.
+struct Candidate {
+  int j, sx, sy, sz;  // sorted index and periodic shift of j's run
+  float r2;           // FP32 |x_i - x_j - S lat|^2
+  bool valid;
+};
+
+template <class Pair, class Entry>
+struct QueueBase {
+  Entry* q;  // this warp's kQueue entries
   Pair& pair;
-  double cut2;
   int count = 0;
-
-  __device__ __forceinline__ PairQueue(double4* qbuf, Pair& p, double c2)
-      : q(qbuf), pair(p), cut2(c2) {}
-
-  // One candidate per lane (valid = false for lanes past the run's end).
-  __device__ __forceinline__ void operator()(const double* sep, double qj, bool valid) {
+  __device__ __forceinline__ QueueBase(Entry* qbuf, Pair& p) : q(qbuf), pair(p) {}
+  // Appends the lanes with take set, in lane order; runs a full batch of 32.
+  template <class Eval>
+  __device__ __forceinline__ void push(bool take, const Entry& e, Eval eval) {
     const int lane = threadIdx.x & 31;
-    const double r2 = sep[0] * sep[0] + sep[1] * sep[1] + sep[2] * sep[2];
-    if (valid && r2 < 1.0e-24) pair.bad = 1;  // coincident charges
-    const bool take = valid && r2 >= 1.0e-24 && r2 <= cut2;
     const unsigned m = __ballot_sync(0xffffffffu, take);
-    if (take) q[count + __popc(m & ((1u << lane) - 1u))] = make_double4(sep[0], sep[1], sep[2], qj);
+    if (take) q[count + __popc(m & ((1u << lane) - 1u))] = e;
     count += __popc(m);
     if (count >= 32) {
       __syncwarp();
-      pair.eval(q[lane]);
+      eval(q[lane]);
       __syncwarp();
       if (lane < count - 32) q[lane] = q[lane + 32];
       count -= 32;
       __syncwarp();
     }
   }
-
-  __device__ __forceinline__ void flush() {
+  template <class Eval>
+  __device__ __forceinline__ void drain(Eval eval) {
     const int lane = threadIdx.x & 31;
     __syncwarp();
-    if (lane < count) pair.eval(q[lane]);
+    if (lane < count) eval(q[lane]);
     count = 0;
   }
 };
 
+// Entries (j, S); at evaluation the separation, the exact cutoff test and the
+// coincidence test are done in FP64.  F32TERM: the pair term then runs in FP32
+// on the FP64 separation rounded once (the mixed form); otherwise in FP64.
+template <class Pair, bool F32TERM>
+struct PairQueue : QueueBase<Pair, int4> {
+  const double4* __restrict__ srt;
+  double4 ai;
+  const RealGeom* g;
+  double cut2;
+  float pre2;  // FP32 prefilter bound: (r_cut + margin)^2
+  __device__ __forceinline__ PairQueue(int4* qbuf, Pair& p, const double4* s, const double4& a,
+                                       const RealGeom& geo, double c2, float p2)
+      : QueueBase<Pair, int4>(qbuf, p), srt(s), ai(a), g(&geo), cut2(c2), pre2(p2) {}
+  __device__ __forceinline__ void eval_entry(const int4& e) {
+    const double4 aj = srt[e.x];
+    const double d1 = (ai.x - aj.x) - e.y, d2 = (ai.y - aj.y) - e.z, d3 = (ai.z - aj.z) - e.w;
+    double sep[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) sep[c] = d1 * g->lat[0][c] + d2 * g->lat[1][c] + d3 * g->lat[2][c];
+    const double r2 = sep[0] * sep[0] + sep[1] * sep[1] + sep[2] * sep[2];
+    if (r2 < 1.0e-24) this->pair.bad = 1;  // coincident charges
+    if (r2 >= 1.0e-24 && r2 <= cut2) {
+      if constexpr (F32TERM)
+        this->pair.eval32(make_float4(static_cast<float>(sep[0]), static_cast<float>(sep[1]),
+                                      static_cast<float>(sep[2]), static_cast<float>(aj.w)));
+      else
+        this->pair.eval(make_double4(sep[0], sep[1], sep[2], aj.w));
+    }
+  }
+  __device__ __forceinline__ void operator()(const Candidate& c) {
+    this->push(c.valid && c.r2 <= pre2, make_int4(c.j, c.sx, c.sy, c.sz),
+               [this](const int4& e) { eval_entry(e); });
+  }
+  __device__ __forceinline__ void flush() {
+    this->drain([this](const int4& e) { eval_entry(e); });
+  }
+};
+
 template <class Visit>
-__device__ __forceinline__ void for_each_candidate(const double4* __restrict__ srt,
+__device__ __forceinline__ void for_each_candidate(const float4* __restrict__ x32,
                                                    const int* __restrict__ box_start, int k,
                                                    const double4& ai, const RealGeom& g,
                                                    Visit& visit) {
   const int lane = threadIdx.x & 31;
   int b[3];
   const double sv[3] = {ai.x, ai.y, ai.z};
+  double xi[3];
 #pragma unroll
-  for (int d = 0; d < 3; ++d) b[d] = min(static_cast<int>(sv[d] * g.nb[d]), g.nb[d] - 1);
+  for (int d = 0; d < 3; ++d) {
+    b[d] = min(static_cast<int>(sv[d] * g.nb[d]), g.nb[d] - 1);
+    xi[d] = sv[0] * g.lat[0][d] + sv[1] * g.lat[1][d] + sv[2] * g.lat[2][d];
+  }
   for (int dz = -g.R[2]; dz <= g.R[2]; ++dz) {
     const int bzr = b[2] + dz;
     const int sz = floor_div(bzr, g.nb[2]);
@@ -309,20 +379,25 @@ __device__ __forceinline__ void for_each_candidate(const double4* __restrict__ s
         const int first = (wz * g.nb[1] + wy) * g.nb[0] + wx;
         const int j0 = box_start[first], j1 = box_start[first + len];
         const bool home_image = (sx == 0 && sy == 0 && sz == 0);
-        for (int jb = j0; jb < j1; jb += 32) {
-          const int j = jb + lane;
-          const bool valid = j < j1 && !(home_image && j == k);
-          double sep[3] = {0.0, 0.0, 0.0};
-          double qj = 0.0;
-          if (valid) {
-            const double4 aj = srt[j];
-            const double d1 = (ai.x - aj.x) - sx, d2 = (ai.y - aj.y) - sy, d3 = (ai.z - aj.z) - sz;
+        // x_i - S lat for this run, rounded once to FP32
+        float base[3];
 #pragma unroll
-            for (int c = 0; c < 3; ++c)
-              sep[c] = d1 * g.lat[0][c] + d2 * g.lat[1][c] + d3 * g.lat[2][c];
-            qj = aj.w;
+        for (int d = 0; d < 3; ++d)
+          base[d] = static_cast<float>(xi[d] - (sx * g.lat[0][d] + sy * g.lat[1][d] + sz * g.lat[2][d]));
+        Candidate c;
+        c.sx = sx;
+        c.sy = sy;
+        c.sz = sz;
+        for (int jb = j0; jb < j1; jb += 32) {
+          c.j = jb + lane;
+          c.valid = c.j < j1 && !(home_image && c.j == k);
+          c.r2 = 3.0e38f;
+          if (c.valid) {
+            const float4 xj = x32[c.j];
+            const float d0 = base[0] - xj.x, d1 = base[1] - xj.y, d2 = base[2] - xj.z;
+            c.r2 = fmaf(d0, d0, fmaf(d1, d1, d2 * d2));
           }
-          visit(sep, qj, valid);
+          visit(c);
         }
         dx += len;
       }
@@ -330,9 +405,22 @@ __device__ __forceinline__ void for_each_candidate(const double4* __restrict__ s
   }
 }
 
-// Pair term of fft/ewald_fft_3d_real.f90:153-172 (FP64), or its FP32 form, for
-// a separation inside the cutoff.
-template <bool MIXED>
+// FP32 prefilter bound for the FP64 cutoff test: the candidate separations
+// carry a rounding error of a few FP32 ulps of the largest coordinate and
+// shift, far below the margin.
+inline float prefilter_bound(const RealGeom& g, double r_cut) {
+  double extent = 0.0;
+  for (int i = 0; i < 3; ++i) {
+    double len = 0.0;
+    for (int d = 0; d < 3; ++d) len += g.lat[i][d] * g.lat[i][d];
+    extent += (2.0 * g.R[i] + 2.0) * std::sqrt(len);
+  }
+  const double r = r_cut + 1.0e-3 + 1.0e-5 * (extent + r_cut);
+  return static_cast<float>(r * r);
+}
+
+// Pair term of fft/ewald_fft_3d_real.f90:153-172: FP64 (eval, FP64 separation),
+// or its FP32 form (eval32, FP32 separation), accumulated in FP64.
 struct EwaldPair {
   double alpha, qi;
   double pot = 0.0, f[3] = {0.0, 0.0, 0.0};
@@ -340,53 +428,53 @@ struct EwaldPair {
   __device__ __forceinline__ void eval(const double4& e) {
     const double r2 = e.x * e.x + e.y * e.y + e.z * e.z;
     const double qj = e.w;
-    if constexpr (!MIXED) {
-      const double r = sqrt(r2);
-      const double rinv = 1.0 / r;
-      const double ecr = erfc(alpha * r) * rinv;  // erfc(alpha r) / r
-      pot += qj * ecr;
-      const double ff =
-          qi * qj * (2.0 * alpha / kSqrtPi * exp(-alpha * alpha * r2) + ecr) * (rinv * rinv);
-      f[0] += ff * e.x;
-      f[1] += ff * e.y;
-      f[2] += ff * e.z;
-    } else {
-      const float r2f = static_cast<float>(r2);
-      const float af = static_cast<float>(alpha);
-      const float rinv = rsqrtf(r2f);
-      const float r = r2f * rinv;
-      const float ec = erfcf(af * r);
-      const float qjf = static_cast<float>(qj);
-      const float pe = qjf * ec * rinv;
-      pot += static_cast<double>(pe);
-      const float ff = static_cast<float>(qi) * qjf *
-                       (2.0f * af * 0.56418958354775628695f * expf(-af * af * r2f) + ec * rinv) *
-                       (rinv * rinv);
-      f[0] += static_cast<double>(ff * static_cast<float>(e.x));
-      f[1] += static_cast<double>(ff * static_cast<float>(e.y));
-      f[2] += static_cast<double>(ff * static_cast<float>(e.z));
-    }
+    const double r = sqrt(r2);
+    const double rinv = 1.0 / r;
+    const double ecr = erfc(alpha * r) * rinv;  // erfc(alpha r) / r
+    pot += qj * ecr;
+    const double ff =
+        qi * qj * (2.0 * alpha / kSqrtPi * exp(-alpha * alpha * r2) + ecr) * (rinv * rinv);
+    f[0] += ff * e.x;
+    f[1] += ff * e.y;
+    f[2] += ff * e.z;
+  }
+  __device__ __forceinline__ void eval32(const float4& e) {
+    const float r2f = fmaf(e.x, e.x, fmaf(e.y, e.y, e.z * e.z));
+    const float af = static_cast<float>(alpha);
+    const float rinv = rsqrtf(r2f);
+    const float r = r2f * rinv;
+    const float ec = erfcf(af * r);
+    const float pe = e.w * ec * rinv;
+    pot += static_cast<double>(pe);
+    const float ff = static_cast<float>(qi) * e.w *
+                     (2.0f * af * 0.56418958354775628695f * expf(-af * af * r2f) + ec * rinv) *
+                     (rinv * rinv);
+    f[0] += static_cast<double>(ff * e.x);
+    f[1] += static_cast<double>(ff * e.y);
+    f[2] += static_cast<double>(ff * e.z);
   }
 };
 
 template <bool MIXED>
 __global__ void __launch_bounds__(kRealThreads) k_real_space(const double4* __restrict__ srt,
+                                                             const float4* __restrict__ x32,
                                                              const int* __restrict__ perm,
                                                              const int* __restrict__ box_start,
                                                              int n, RealGeom g, double alpha,
-                                                             double cut2, double* __restrict__ pot,
+                                                             double cut2, float pre2,
+                                                             double* __restrict__ pot,
                                                              double* __restrict__ force,
                                                              int* __restrict__ err) {
-  __shared__ double4 queue[kRealThreads / 32][kQueue];
+  __shared__ __align__(16) int4 queue[kRealThreads / 32][kQueue];
   const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (k >= n) return;
   const double4 ai = srt[k];
-  EwaldPair<MIXED> pair;
+  EwaldPair pair;
   pair.alpha = alpha;
   pair.qi = ai.w;
-  PairQueue<EwaldPair<MIXED>> pq(queue[threadIdx.x >> 5], pair, cut2);
-  for_each_candidate(srt, box_start, k, ai, g, pq);
+  PairQueue<EwaldPair, MIXED> pq(queue[threadIdx.x >> 5], pair, srt, ai, g, cut2, pre2);
+  for_each_candidate(x32, box_start, k, ai, g, pq);
   pq.flush();
   double v[4] = {pair.pot, pair.f[0], pair.f[1], pair.f[2]};
 #pragma unroll
@@ -426,12 +514,13 @@ struct StressPair {
 };
 
 __global__ void __launch_bounds__(kRealThreads) k_real_stress(const double4* __restrict__ srt,
+                                                              const float4* __restrict__ x32,
                                                               const int* __restrict__ box_start,
                                                               int n, RealGeom g, double alpha,
-                                                              double cut2,
+                                                              double cut2, float pre2,
                                                               double* __restrict__ partial6,
                                                               int* __restrict__ err) {
-  __shared__ double4 queue[kRealThreads / 32][kQueue];
+  __shared__ __align__(16) int4 queue[kRealThreads / 32][kQueue];
   const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (k >= n) return;
@@ -439,8 +528,8 @@ __global__ void __launch_bounds__(kRealThreads) k_real_stress(const double4* __r
   StressPair pair;
   pair.alpha = alpha;
   pair.qi = ai.w;
-  PairQueue<StressPair> pq(queue[threadIdx.x >> 5], pair, cut2);
-  for_each_candidate(srt, box_start, k, ai, g, pq);
+  PairQueue<StressPair, false> pq(queue[threadIdx.x >> 5], pair, srt, ai, g, cut2, pre2);
+  for_each_candidate(x32, box_start, k, ai, g, pq);
   pq.flush();
 #pragma unroll
   for (int j = 0; j < 6; ++j) pair.s[j] = warp_sum(pair.s[j]);
@@ -581,6 +670,16 @@ void launch_permute4(const double4* in, const int* perm, int n, double4* out, cu
   ++g_launches;
 }
 
+void launch_permute_box(const double4* in, const int* perm, int n, const double (*lat)[3],
+                        double4* out, float4* x32, cudaStream_t st) {
+  if (n == 0) return;
+  LatRows L;
+  for (int i = 0; i < 3; ++i)
+    for (int d = 0; d < 3; ++d) L.a[i][d] = lat[i][d];
+  k_permute_box<<<blocks_for(n, 256), 256, 0, st>>>(in, perm, n, L, out, x32);
+  ++g_launches;
+}
+
 void launch_permute_int4(const int4* in, const int* perm, int n, int4* out, cudaStream_t st) {
   if (n == 0) return;
   k_permute_int4<<<blocks_for(n, 256), 256, 0, st>>>(in, perm, n, out);
@@ -594,26 +693,27 @@ void launch_charge_sums(const double* q, int n, double* partial, double* out, cu
   g_launches += 2;
 }
 
-void launch_real_space(const double4* srt, const int* perm, const int* box_start, int n,
-                       const RealGeom& g, double alpha, double r_cut, int mixed, double* pot,
-                       double* force, int* err, cudaStream_t st) {
+void launch_real_space(const double4* srt, const float4* x32, const int* perm,
+                       const int* box_start, int n, const RealGeom& g, double alpha, double r_cut,
+                       int mixed, double* pot, double* force, int* err, cudaStream_t st) {
   if (n == 0) return;
   const int blocks = blocks_for(static_cast<long>(n) * 32, kRealThreads);
+  const float pre2 = prefilter_bound(g, r_cut);
   if (mixed)
-    k_real_space<true><<<blocks, kRealThreads, 0, st>>>(srt, perm, box_start, n, g, alpha,
-                                                        r_cut * r_cut, pot, force, err);
+    k_real_space<true><<<blocks, kRealThreads, 0, st>>>(srt, x32, perm, box_start, n, g, alpha,
+                                                        r_cut * r_cut, pre2, pot, force, err);
   else
-    k_real_space<false><<<blocks, kRealThreads, 0, st>>>(srt, perm, box_start, n, g, alpha,
-                                                         r_cut * r_cut, pot, force, err);
+    k_real_space<false><<<blocks, kRealThreads, 0, st>>>(srt, x32, perm, box_start, n, g, alpha,
+                                                         r_cut * r_cut, pre2, pot, force, err);
   ++g_launches;
 }
 
-void launch_real_stress(const double4* srt, const int* box_start, int n, const RealGeom& g,
-                        double alpha, double max_r, double* partial6, double* out6, int* err,
-                        cudaStream_t st) {
+void launch_real_stress(const double4* srt, const float4* x32, const int* box_start, int n,
+                        const RealGeom& g, double alpha, double max_r, double* partial6,
+                        double* out6, int* err, cudaStream_t st) {
   if (n == 0) return;
   k_real_stress<<<blocks_for(static_cast<long>(n) * 32, kRealThreads), kRealThreads, 0, st>>>(
-      srt, box_start, n, g, alpha, max_r * max_r, partial6, err);
+      srt, x32, box_start, n, g, alpha, max_r * max_r, prefilter_bound(g, max_r), partial6, err);
   k_sum_partials<<<1, 256, 0, st>>>(partial6, n, 6, out6);
   g_launches += 2;
 }

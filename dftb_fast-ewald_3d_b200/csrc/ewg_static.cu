@@ -256,6 +256,7 @@ extern "C" int ewg_direct_potential_force_static(int n, const double* coords_dev
   if (nmodes > (1L << 24)) return EWG_ERR_SCRATCH_LIMIT;
   double4* s4 = cv.take<double4>(n);
   double4* s4s = cv.take<double4>(n);
+  float4* x32s = cv.take<float4>(n);
   int* boxkey = cv.take<int>(n);
   int* counts = cv.take<int>(nboxes);
   int* cursor = cv.take<int>(nboxes);
@@ -270,8 +271,8 @@ extern "C" int ewg_direct_potential_force_static(int n, const double* coords_dev
   launch_atom_prep(coords_device, 3, 1, charges_device, n, cell, rg.nb, nullptr, nullptr, nullptr,
                    s4, boxkey, nullptr, nullptr, nullptr, st);
   launch_bucket_sort(boxkey, n, nboxes, counts, cursor, starts, tmp, perm, st);
-  launch_permute4(s4, perm, n, s4s, st);
-  launch_real_space(s4s, perm, starts, n, rg, alpha, r_cut, 0, pot_device, fbuf, err, st);
+  launch_permute_box(s4, perm, n, cell.lat, s4s, x32s, st);
+  launch_real_space(s4s, x32s, perm, starts, n, rg, alpha, r_cut, 0, pot_device, fbuf, err, st);
   k_modes_box<<<static_cast<unsigned>(nmodes), 256, 0, st>>>(coords_device, charges_device, n, mb,
                                                              modes);
   k_kspace_self<<<(n + 255) / 256, 256, 0, st>>>(coords_device, charges_device, n, modes,

@@ -17,7 +17,8 @@
 //
 // Spread: a CTA owns a tile; each thread owns an x-pencil of 8 points in
 // registers and adds q w1 w2 w3 atom by atom in list order, then writes it
-// once (no atomics, no zeroing, fixed order).
+// once (no atomics, no zeroing, fixed order).  FP64 runs on the tensor cores;
+// FP32 sums groups of 8 atoms in FP32 and the group sums in FP64.
 // Gather: a CTA of one (FP64) or two (FP32) warps stages its tile in shared
 // memory; each warp takes 64 atoms of the tile's list at a time, two per lane,
 // and walks the tile's 512 points in lockstep so every grid value is a
@@ -39,6 +40,7 @@ namespace {
 constexpr int TX = kTileX, TY = kTileY, TZ = kTileZ;
 constexpr int kPencils = TY * TZ;  // spread: one thread per x-pencil
 constexpr int kSpreadChunk = 64;   // atoms whose weights are staged at once
+constexpr int kSpreadGroup = 8;    // FP32 spread: atoms summed in FP32 before the FP64 add
 // Gather: atoms per lane and warps sharing one staged tile, per precision.
 template <typename R>
 struct GatherShape {
@@ -91,21 +93,28 @@ __global__ void k_weights_tiled(const int4* __restrict__ mc, const double4* __re
     count = min(count, nt);
   }
   R* out = wtab + static_cast<size_t>(k) * sd.wstride + sd.woff[d];
+  // Window derivative with respect to the atom's fractional coordinate s_d:
+  // the point sits at u = o - frac grid units from the atom, and
+  // d/ds_d [pref exp(-u^2 / b)] = n_d (2 u / b) pref exp(-u^2 / b).
+  const double dscale = -2.0 * static_cast<double>(nd) / sd.b;
   for (int s = 0; s < S; ++s) {
     const int origin = ((first + s) % nt) * T;
     for (int p = 0; p < T; ++p) {
       const int P = origin + p;
-      double w = 0.0;
+      double w = 0.0, dw = 0.0;
       if (s < count && P < nd) {
         int o = pmod(P - c, nd);  // largest offset <= m congruent to P - c
         while (o > m) o -= nd;
         while (o + nd <= m) o += nd;
         for (; o >= -m; o -= nd) {
           const double dd = frac - static_cast<double>(o);
-          w += sd.pref * exp(-(dd * dd) / sd.b);
+          const double e = sd.pref * exp(-(dd * dd) / sd.b);
+          w += e;
+          dw += dscale * dd * e;
         }
       }
       out[s * T + p] = static_cast<R>(w);
+      if (sd.ad) out[sd.dwoff + s * T + p] = static_cast<R>(dw);
     }
   }
   int* sp = reinterpret_cast<int*>(&slot[k]);
@@ -245,17 +254,22 @@ __global__ void __launch_bounds__(kPencils) k_spread_tiles(const int* __restrict
       for (int z = 0; z < TZ; ++z) sW3[a][z] = t3[z] * qa;
     }
     __syncthreads();
-    for (int a = 0; a < nb; ++a) {
-      const R s = sW2[a][py] * sW3[a][pz];
-      if (s != R(0)) {
+    // Groups of kSpreadGroup atoms are summed in R, each group sum then
+    // added to the FP64 pencil: one FP32 -> FP64 conversion per point and
+    // group instead of per point and atom (the conversions, not the
+    // multiply-adds, bounded the FP32 form).
+    for (int g0 = 0; g0 < nb; g0 += kSpreadGroup) {
+      const int g1 = min(g0 + kSpreadGroup, nb);
+      R part[TX];
 #pragma unroll
-        for (int x = 0; x < TX; ++x) {
-          if constexpr (sizeof(R) == 8)
-            acc[x] = fma(static_cast<double>(s), static_cast<double>(sW1[a][x]), acc[x]);
-          else
-            acc[x] += static_cast<double>(s * sW1[a][x]);
-        }
+      for (int x = 0; x < TX; ++x) part[x] = R(0);
+      for (int a = g0; a < g1; ++a) {
+        const R s = sW2[a][py] * sW3[a][pz];
+#pragma unroll
+        for (int x = 0; x < TX; ++x) part[x] = fma(s, sW1[a][x], part[x]);
       }
+#pragma unroll
+      for (int x = 0; x < TX; ++x) acc[x] += static_cast<double>(part[x]);
     }
   }
   const int ex = min(TX, sd.n[0] - x0), ey = min(TY, sd.n[1] - y0), ez = min(TZ, sd.n[2] - z0);
@@ -285,6 +299,7 @@ __device__ __forceinline__ void dmma_m8n8k4(double& c0, double& c1, double a, do
 
 constexpr int kGatherWarps = 4;   // FP64 gather: warps per tile
 constexpr int kGatherMB = 2;      // FP64 gather: M blocks of 8 atoms per warp and round
+constexpr int kGatherAdWarps = 4;  // FP64 gather with window derivatives: warps per tile
 constexpr int kSpreadAtoms = 64;  // atoms staged per round, one per thread
 constexpr int kWRow = 12;         // doubles per staged weight row: 8 used; the
                                   // padding makes the fragment reads conflict-free
@@ -437,6 +452,12 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles(const int* __restri
       R w3[A];
 #pragma unroll
       for (int a = 0; a < A; ++a) w3[a] = sW3[warp][z][a * 32 + lane];
+      // The plane's rows are summed in R, the plane sum then added in FP64.
+      R pl[A][NC];
+#pragma unroll
+      for (int a = 0; a < A; ++a)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) pl[a][c] = R(0);
 #pragma unroll
       for (int y = 0; y < TY; ++y) {
         R w23[A];
@@ -471,8 +492,12 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles(const int* __restri
 #pragma unroll
         for (int a = 0; a < A; ++a)
 #pragma unroll
-          for (int c = 0; c < NC; ++c) acc[a][c] += static_cast<double>(w23[a] * rs[a][c]);
+          for (int c = 0; c < NC; ++c) pl[a][c] = fma(w23[a], rs[a][c], pl[a][c]);
       }
+#pragma unroll
+      for (int a = 0; a < A; ++a)
+#pragma unroll
+        for (int c = 0; c < NC; ++c) acc[a][c] += static_cast<double>(pl[a][c]);
     }
 #pragma unroll
     for (int a = 0; a < A; ++a) {
@@ -484,6 +509,167 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles(const int* __restri
       for (int c = 0; c < NC; ++c) dst[c] = acc[a][c];
     }
     __syncwarp();  // sW3 is rewritten by the next iteration
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP32 gather with window derivatives (force scheme ad).  The tile holds the
+// potential grid g alone.  With W = w1 w2 w3 and D_d the same product with
+// axis d's weights replaced by their derivatives with respect to s_d, an atom
+// needs phi = sum W g and D_d = sum D_d g.  The derivative weights change sign
+// across the stencil while g carries a large smooth part, so in FP32 the sums
+// would cancel; they run instead on g' = g - c, with c the grid value at the
+// atom's lowest stencil point, and the tile's c terms are added back in FP64
+// from the tile's weight sums:
+//   phi_t = sum_t W g' + c Sx Sy Sz,  D_1,t = sum_t dW_1 g' + c dSx Sy Sz, ...
+// (S, dS: sums over the tile's points of the weights and their derivatives).
+// Per (z, y) row two x sums, r0 = sum_x w1 g' and r1 = sum_x dw1 g', feed all
+// four:  phi += w2 w3 r0, D_1 += w2 w3 r1, D_2 += dw2 w3 r0, D_3 += w2 dw3 r0.
+// Lanes carry A atoms of the tile's list as in k_gather_tiles; products and
+// plane sums in FP32, the sum over planes in FP64; the four partials go to the
+// atom's slot.
+// ---------------------------------------------------------------------------
+template <int A, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_ad(const int* __restrict__ tile_start,
+                                                                const int2* __restrict__ pairs,
+                                                                const float* __restrict__ wtab,
+                                                                const int4* __restrict__ mc,
+                                                                StencilDims sd,
+                                                                const float* __restrict__ grid,
+                                                                double* __restrict__ part) {
+  __shared__ float sG[TZ * TY * TX];
+  __shared__ float sW3[WARPS][TZ][32 * A];  // z weights, lane fastest
+  __shared__ float sD3[WARPS][TZ][32 * A];  // their derivatives
+  const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
+  const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
+  const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
+  const int ex = min(TX, sd.n[0] - x0), ey = min(TY, sd.n[1] - y0), ez = min(TZ, sd.n[2] - z0);
+  const int p0 = tile_start[tile], p1 = tile_start[tile + 1];
+  if (p0 == p1) return;  // no atom reaches this tile
+#pragma unroll 4
+  for (int t = threadIdx.x; t < TX * TY * TZ; t += 32 * WARPS) {
+    const int x = t % TX, y = (t / TX) % TY, z = t / (TX * TY);
+    sG[t] = (x < ex && y < ey && z < ez)
+                ? grid[(static_cast<size_t>(z0 + z) * sd.n[1] + y0 + y) * sd.n[0] + x0 + x]
+                : 0.0f;
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nslots = sd.S[0] * sd.S[1] * sd.S[2];
+  for (int a0 = p0 + warp * 32 * A; a0 < p1; a0 += WARPS * 32 * A) {
+    float w1[A][TX], d1[A][TX], w2[A][TY], d2[A][TY], cg[A];
+    int2 pr[A];
+    bool act[A];
+#pragma unroll
+    for (int a = 0; a < A; ++a) {
+      const int e = a0 + a * 32 + lane;
+      act[a] = e < p1;
+      pr[a] = act[a] ? pairs[e] : make_int2(0, 0);
+      const float* wk = wtab + static_cast<size_t>(pr[a].x) * sd.wstride;
+      const int ox = sd.woff[0] + (pr[a].y & 0xff) * TX;
+      const int oy = sd.woff[1] + ((pr[a].y >> 8) & 0xff) * TY;
+      const int oz = sd.woff[2] + (pr[a].y >> 16) * TZ;
+      cg[a] = 0.0f;
+      if (act[a]) {
+        load8(wk + ox, w1[a]);
+        load8(wk + sd.dwoff + ox, d1[a]);
+        load8(wk + oy, w2[a]);
+        load8(wk + sd.dwoff + oy, d2[a]);
+        const int4 m = mc[pr[a].x];  // the atom's lowest stencil point
+        cg[a] = grid[(static_cast<size_t>(m.z) * sd.n[1] + m.y) * sd.n[0] + m.x];
+      } else {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) w1[a][j] = d1[a][j] = w2[a][j] = d2[a][j] = 0.0f;
+      }
+#pragma unroll
+      for (int z = 0; z < TZ; ++z) {
+        sW3[warp][z][a * 32 + lane] = act[a] ? wk[oz + z] : 0.0f;
+        sD3[warp][z][a * 32 + lane] = act[a] ? wk[sd.dwoff + oz + z] : 0.0f;
+      }
+    }
+    __syncwarp();
+    double acc[A][4];
+    float sz[A], dsz[A];
+#pragma unroll
+    for (int a = 0; a < A; ++a) {
+      sz[a] = dsz[a] = 0.0f;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) acc[a][c] = 0.0;
+    }
+#pragma unroll 1
+    for (int z = 0; z < TZ; ++z) {
+      float w3[A], d3[A], pl[A][4];
+#pragma unroll
+      for (int a = 0; a < A; ++a) {
+        w3[a] = sW3[warp][z][a * 32 + lane];
+        d3[a] = sD3[warp][z][a * 32 + lane];
+        sz[a] += w3[a];
+        dsz[a] += d3[a];
+        pl[a][0] = pl[a][1] = pl[a][2] = pl[a][3] = 0.0f;  // plane sums, FP32
+      }
+#pragma unroll
+      for (int y = 0; y < TY; ++y) {
+        // A zero window product means the row lies outside the atom's stencil
+        // along y or z, where the derivatives vanish as well.
+        float w23[A];
+        bool any = false;
+#pragma unroll
+        for (int a = 0; a < A; ++a) {
+          w23[a] = w2[a][y] * w3[a];
+          any = any || (w23[a] != 0.0f);
+        }
+        if (!__any_sync(0xffffffffu, any)) continue;
+        float r0[A], r1[A];
+#pragma unroll
+        for (int a = 0; a < A; ++a) r0[a] = r1[a] = 0.0f;
+        const float* row = sG + (z * TY + y) * TX;
+#pragma unroll
+        for (int x = 0; x < TX; ++x) {
+          const float g = row[x];
+#pragma unroll
+          for (int a = 0; a < A; ++a) {
+            const float gs = g - cg[a];
+            r0[a] = fmaf(w1[a][x], gs, r0[a]);
+            r1[a] = fmaf(d1[a][x], gs, r1[a]);
+          }
+        }
+#pragma unroll
+        for (int a = 0; a < A; ++a) {
+          pl[a][0] = fmaf(w23[a], r0[a], pl[a][0]);
+          pl[a][1] = fmaf(w23[a], r1[a], pl[a][1]);
+          pl[a][2] = fmaf(d2[a][y] * w3[a], r0[a], pl[a][2]);
+          pl[a][3] = fmaf(w2[a][y] * d3[a], r0[a], pl[a][3]);
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < A; ++a)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) acc[a][c] += static_cast<double>(pl[a][c]);
+    }
+#pragma unroll
+    for (int a = 0; a < A; ++a) {
+      if (!act[a]) continue;
+      // the c terms of this tile: c (S or dS along each axis)
+      double sx = 0.0, dsx = 0.0, sy = 0.0, dsy = 0.0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        sx += w1[a][j];
+        dsx += d1[a][j];
+        sy += w2[a][j];
+        dsy += d2[a][j];
+      }
+      const double c = cg[a];
+      acc[a][0] += c * sx * sy * sz[a];
+      acc[a][1] += c * dsx * sy * sz[a];
+      acc[a][2] += c * sx * dsy * sz[a];
+      acc[a][3] += c * sx * sy * dsz[a];
+      const int ps = pr[a].y;
+      const int sidx = ((ps >> 16) * sd.S[1] + ((ps >> 8) & 0xff)) * sd.S[0] + (ps & 0xff);
+      double* dst = part + (static_cast<size_t>(pr[a].x) * nslots + sidx) * 4;
+#pragma unroll
+      for (int c4 = 0; c4 < 4; ++c4) dst[c4] = acc[a][c4];
+    }
+    __syncwarp();  // sW3 and sD3 are rewritten by the next iteration
   }
 }
 
@@ -634,16 +820,141 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma(const int* __r
   }
 }
 
+// ---------------------------------------------------------------------------
+// FP64 gather with window derivatives (force scheme ad) on the tensor cores.
+// The tile holds the potential grid alone.  Per plane z the x contraction
+// takes two A operands that do not change from plane to plane, w1 and dw1:
+//   C_w[z][m][y] = sum_x w1_m(x) G[z][y][x],  C_d[z][m][y] = sum_x dw1_m(x) G[z][y][x]
+// (four DMMAs per plane for 8 atoms, each plane its own accumulators, so the
+// 32 DMMAs of a tile are independent), and the y and z weights are applied
+// afterwards:
+//   phi = sum_z w3 sum_y w2 C_w,  D_1 = sum_z w3 sum_y w2 C_d,
+//   D_2 = sum_z w3 sum_y dw2 C_w,  D_3 = sum_z dw3 sum_y w2 C_w.
+// One warp per M block of 8 atoms, WARPS warps per round.  Shared layout and
+// fragment mapping as in k_gather_tiles_dmma with NC = 1; six weight rows per
+// atom (w1 w2 w3 dw1 dw2 dw3).
+// ---------------------------------------------------------------------------
+template <int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma_ad(
+    const int* __restrict__ tile_start, const int2* __restrict__ pairs,
+    const double* __restrict__ wtab, StencilDims sd, const double* __restrict__ grid,
+    double* __restrict__ part) {
+  constexpr int RS = GatherRow<1>::value;
+  constexpr int kAtoms = WARPS * 8;  // atoms staged per round
+  __shared__ __align__(16) double sG[TZ * TY * RS];
+  __shared__ __align__(16) double sW[6][kAtoms][kWRow];
+  __shared__ int2 sPair[kAtoms];
+  const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
+  const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
+  const int p0 = tile_start[tile], p1 = tile_start[tile + 1];
+  if (p0 == p1) return;  // no atom reaches this tile
+  const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
+  const int ex = min(TX, sd.n[0] - x0), ey = min(TY, sd.n[1] - y0), ez = min(TZ, sd.n[2] - z0);
+  // Stage the tile: 16-byte chunks of two points.
+  constexpr int kChunksPerRow = TX / 2;
+  for (int t = threadIdx.x; t < TZ * TY * kChunksPerRow; t += blockDim.x) {
+    const int row = t / kChunksPerRow, h = t - row * kChunksPerRow;
+    const int z = row / TY, y = row - z * TY;
+    const int x = 2 * h;
+    double* dst = sG + row * RS + 2 * h;
+    if (z < ez && y < ey && x < ex) {
+      cp_async16(dst, grid + (static_cast<size_t>(z0 + z) * sd.n[1] + y0 + y) * sd.n[0] + x0 + x);
+    } else {
+      dst[0] = 0.0;
+      dst[1] = 0.0;
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int fr = lane >> 2, fk = lane & 3;
+  const int nslots = sd.S[0] * sd.S[1] * sd.S[2];
+  for (int b0 = p0; b0 < p1; b0 += kAtoms) {
+    const int nb = min(kAtoms, p1 - b0);
+    __syncthreads();  // the previous round's weights are no longer read
+    for (int a = threadIdx.x; a < kAtoms; a += blockDim.x) {
+      if (a < nb) {
+        const int2 pr = pairs[b0 + a];
+        sPair[a] = pr;
+        const double* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
+        const int off[3] = {sd.woff[0] + (pr.y & 0xff) * TX, sd.woff[1] + ((pr.y >> 8) & 0xff) * TY,
+                            sd.woff[2] + (pr.y >> 16) * TZ};
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            cp_async16(&sW[d][a][2 * j], wk + off[d] + 2 * j);
+            cp_async16(&sW[3 + d][a][2 * j], wk + sd.dwoff + off[d] + 2 * j);
+          }
+      } else {  // rows past the list: zero weights, results discarded
+#pragma unroll
+        for (int d = 0; d < 6; ++d)
+#pragma unroll
+          for (int j = 0; j < 8; ++j) sW[d][a][j] = 0.0;
+      }
+    }
+    cp_async_wait_all();  // also completes the tile copies on the first round
+    __syncthreads();
+    if (warp * 8 >= nb) continue;
+    const int am = warp * 8 + fr;  // this lane's atom row
+    const double fw0 = sW[0][am][fk], fw1 = sW[0][am][4 + fk];
+    const double fd0 = sW[3][am][fk], fd1 = sW[3][am][4 + fk];
+    double cw[TZ][2], cd[TZ][2];
+#pragma unroll
+    for (int z = 0; z < TZ; ++z) {
+      // B[k][n] = G[z][y = n][x = 4 ks + k] at lane 4n + k.
+      const double* gz = sG + (z * TY + fr) * RS;
+      const double b0v = gz[fk], b1v = gz[4 + fk];
+      cw[z][0] = cw[z][1] = cd[z][0] = cd[z][1] = 0.0;
+      dmma_m8n8k4(cw[z][0], cw[z][1], fw0, b0v);
+      dmma_m8n8k4(cw[z][0], cw[z][1], fw1, b1v);
+      dmma_m8n8k4(cd[z][0], cd[z][1], fd0, b0v);
+      dmma_m8n8k4(cd[z][0], cd[z][1], fd1, b1v);
+    }
+    // This lane holds C for y = 2 fk and 2 fk + 1 of every plane.
+    const double w20 = sW[1][am][2 * fk], w21 = sW[1][am][2 * fk + 1];
+    const double d20 = sW[4][am][2 * fk], d21 = sW[4][am][2 * fk + 1];
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int z = 0; z < TZ; ++z) {
+      const double w3 = sW[2][am][z], d3 = sW[5][am][z];
+      const double pw = fma(w20, cw[z][0], w21 * cw[z][1]);
+      const double pd = fma(w20, cd[z][0], w21 * cd[z][1]);
+      const double qw = fma(d20, cw[z][0], d21 * cw[z][1]);
+      acc[0] = fma(w3, pw, acc[0]);
+      acc[1] = fma(w3, pd, acc[1]);
+      acc[2] = fma(w3, qw, acc[2]);
+      acc[3] = fma(d3, pw, acc[3]);
+    }
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], 1);
+      acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], 2);
+    }
+    if (fk == 0 && am < nb) {
+      const int ps = sPair[am].y;
+      const int sidx = ((ps >> 16) * sd.S[1] + ((ps >> 8) & 0xff)) * sd.S[0] + (ps & 0xff);
+      double* dst = part + (static_cast<size_t>(sPair[am].x) * nslots + sidx) * 4;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) dst[c] = acc[c];
+    }
+  }
+}
+
 // Final per-atom sum of the slot partials in a fixed order, with the assembly
 // of fft/ewald_fft_3d.f90:121-132: pot = (sr + lr) + self, force = sr + q lr.
 // One warp per atom: lanes read the atom's slots (contiguous, coalesced), then
 // a shuffle tree sums them (a fixed order: results are reproducible).
+// Dual basis rows for the ad partials (on = 0: ik partials, Cartesian already).
+struct RecRows {
+  double b[3][3];
+  int on;
+};
+
 template <int NC>
 __global__ void k_gather_final(const int4* __restrict__ slot, const int* __restrict__ perm,
                                const double* __restrict__ part, int n, StencilDims sd,
                                const double* __restrict__ q, double self_coef, double pot_shift,
                                const double* __restrict__ pot_sr, const double* __restrict__ f_sr,
-                               double* __restrict__ pot, double* __restrict__ force) {
+                               double* __restrict__ pot, double* __restrict__ force, RecRows rr) {
   const int k = static_cast<int>((static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
   if (k >= n) return;
@@ -670,8 +981,15 @@ __global__ void k_gather_final(const int4* __restrict__ slot, const int* __restr
   const double qi = q[i];
   pot[i] = (pot_sr[i] + acc[0]) + self_coef * qi + pot_shift;
   if (NC == 4 && force) {
+    if (rr.on) {  // ad: F = -q sum_e D_e b_e, D_e the derivative along s_e
 #pragma unroll
-    for (int d = 0; d < 3; ++d) force[3 * i + d] = f_sr[3 * i + d] + qi * acc[1 + d];
+      for (int d = 0; d < 3; ++d)
+        force[3 * i + d] =
+            f_sr[3 * i + d] - qi * (acc[1] * rr.b[0][d] + acc[2] * rr.b[1][d] + acc[3] * rr.b[2][d]);
+    } else {
+#pragma unroll
+      for (int d = 0; d < 3; ++d) force[3 * i + d] = f_sr[3 * i + d] + qi * acc[1 + d];
+    }
   }
 }
 
@@ -746,13 +1064,23 @@ void launch_spread(const MeshPlan& mp, const int* tile_start, const int2* pairs,
 }
 
 void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs, const void* wtab,
-                   const void* grid, int nc, double* part, cudaStream_t st) {
+                   const int4* mesh_c, const void* grid, int nc, double* part, cudaStream_t st) {
   dim3 grd(mp.sd.ntiles[0], mp.sd.ntiles[1], mp.sd.ntiles[2]);
 #define EWG_GATHER(R, NC)                                                               \
   k_gather_tiles<R, NC, GatherShape<R>::atoms, GatherShape<R>::warps>                      \
       <<<grd, 32 * GatherShape<R>::warps, 0, st>>>(tile_start, pairs, static_cast<const R*>(wtab), \
                                                    mp.sd, static_cast<const R*>(grid), part)
-  if (mp.mixed) {
+  if (mp.sd.ad && nc == 1) {  // force wanted, ad scheme: potential grid, four partials
+    if (mp.mixed)
+      k_gather_tiles_ad<GatherShape<float>::atoms, GatherShape<float>::warps>
+          <<<grd, 32 * GatherShape<float>::warps, 0, st>>>(
+              tile_start, pairs, static_cast<const float*>(wtab), mesh_c,
+              mp.sd, static_cast<const float*>(grid), part);
+    else
+      k_gather_tiles_dmma_ad<kGatherAdWarps><<<grd, 32 * kGatherAdWarps, 0, st>>>(
+          tile_start, pairs, static_cast<const double*>(wtab), mp.sd,
+          static_cast<const double*>(grid), part);
+  } else if (mp.mixed) {
     if (nc == 4)
       EWG_GATHER(float, 4);
     else
@@ -774,15 +1102,22 @@ void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs,
 }
 
 void launch_gather_final(const MeshPlan& mp, const int4* slot, const int* perm, const double* part,
-                         int nc, int n, const double* q, double self_coef, double pot_shift, const double* pot_sr,
-                         const double* f_sr, double* pot, double* force, cudaStream_t st) {
+                         int nparts, int n, const double* q, double self_coef, double pot_shift,
+                         const double* pot_sr, const double* f_sr, double* pot, double* force,
+                         const double (*rec)[3], cudaStream_t st) {
   if (n == 0) return;
-  if (nc == 4)
+  RecRows rr{};
+  if (rec) {
+    rr.on = 1;
+    for (int i = 0; i < 3; ++i)
+      for (int d = 0; d < 3; ++d) rr.b[i][d] = rec[i][d];
+  }
+  if (nparts == 4)
     k_gather_final<4><<<blocks_for(32L * n, 256), 256, 0, st>>>(
-        slot, perm, part, n, mp.sd, q, self_coef, pot_shift, pot_sr, f_sr, pot, force);
+        slot, perm, part, n, mp.sd, q, self_coef, pot_shift, pot_sr, f_sr, pot, force, rr);
   else
     k_gather_final<1><<<blocks_for(32L * n, 256), 256, 0, st>>>(
-        slot, perm, part, n, mp.sd, q, self_coef, pot_shift, pot_sr, f_sr, pot, nullptr);
+        slot, perm, part, n, mp.sd, q, self_coef, pot_shift, pot_sr, f_sr, pot, nullptr, rr);
   ++g_launches;
 }
 

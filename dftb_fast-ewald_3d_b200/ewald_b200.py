@@ -31,6 +31,8 @@ LIB_PATH = os.path.join(HERE, "libewald_b200.so")
 
 FP64 = 0
 MIXED = 1
+FORCE_IK = 0  # the reference's i k differentiation (the default)
+FORCE_AD = 1  # analytic differentiation of the window
 
 STATUS = {
     0: "EWG_OK", 1: "EWG_ERR_NPARTICLE", 2: "EWG_ERR_ARG", 3: "EWG_ERR_NOT_NEUTRAL",
@@ -51,7 +53,7 @@ EXPORTED = [
     "ewg_stage_name", "ewg_stage_times", "ewg_reset_stage_times", "ewg_set_stream",
     "ewg_direct_potential_force_static", "ewg_fp64_mma_peak", "ewg_potential_force_stress",
     "ewg_stress_fast", "ewg_potential_at", "ewg_potential_gradient_at", "ewg_external_pot_grad",
-    "ewg_xlbomd_gradients", "ewg_set_background",
+    "ewg_xlbomd_gradients", "ewg_set_background", "ewg_set_force_scheme", "ewg_tune", "ewg_set_graphs",
 ]
 
 
@@ -118,6 +120,8 @@ def lib():
     L.ewg_potential_force_stress.argtypes = [vp, C.c_int, dp, dp, dp, C.c_double, dp, dp, dp,
                                              C.POINTER(Overrides)]
     L.ewg_parameters.argtypes = [C.c_int, dp, dp, C.c_double, C.POINTER(Overrides), C.POINTER(Params)]
+    L.ewg_tune.argtypes = [vp, C.c_int, dp, dp, dp, C.c_double, C.POINTER(Overrides),
+                           C.POINTER(C.c_int), dp]
     L.ewg_grid_memory.argtypes = [C.c_int, dp, dp, C.c_double, C.POINTER(Overrides), dp]
     L.ewg_device_memory.argtypes = [C.c_int, dp, dp, C.c_double, C.POINTER(Overrides), C.c_int,
                                     C.c_int, dp]
@@ -133,6 +137,8 @@ def lib():
     L.ewg_stress_fast.argtypes = [vp, C.c_double, dp]
     L.ewg_xlbomd_gradients.argtypes = [vp, C.c_double, dp, dp]
     L.ewg_set_background.argtypes = [vp, C.c_int]
+    L.ewg_set_force_scheme.argtypes = [vp, C.c_int]
+    L.ewg_set_graphs.argtypes = [vp, C.c_int]
     L.ewg_potential_at.argtypes = [vp, C.c_int, dp, C.c_int, dp, dp, dp, dp, dp, C.c_double,
                                    C.c_double, dp]
     L.ewg_potential_gradient_at.argtypes = [vp, C.c_int, dp, C.c_int, dp, dp, dp, dp, C.c_double,
@@ -262,6 +268,26 @@ class Context:
         _check(lib().ewg_potential_force(self._h, n, _dp(pos), _dp(q), _dp(lat), float(tol), _dp(pot),
                                          _dp(force) if want_force else None, C.byref(o)))
         return (pot, force) if want_force else pot
+
+    def tune(self, positions, charges, latVecs, target=1e-6):
+        """Fastest parameter set and force scheme of this form whose RMS
+        relative force error against the FP64 i k form at tol 1e-10 is at most
+        target/2 (potential: target) on this configuration.  Returns
+        (overrides, scheme, report): overrides as keyword arguments for
+        potential_force & co., scheme for set_force_scheme."""
+        q = np.ascontiguousarray(charges, dtype=np.float64)
+        n = q.shape[0]
+        pos = _positions_fortran(positions, n)
+        lat = _lat_fortran(latVecs)
+        o = Overrides()
+        scheme = C.c_int()
+        rep = np.zeros(4)
+        _check(lib().ewg_tune(self._h, n, _dp(pos), _dp(q), _dp(lat), float(target), C.byref(o),
+                              C.byref(scheme), _dp(rep)))
+        ov = dict(alpha_in=o.alpha, r_cut_in=o.r_cut, k_cut_in=o.k_cut,
+                  windowCutoff_in=o.window_cutoff)
+        return ov, int(scheme.value), dict(force_rms=float(rep[0]), pot_rms=float(rep[1]),
+                                           ms=float(rep[2]), candidates=int(rep[3]))
 
     def potential_force_stress(self, positions, charges, latVecs, tol=1e-10, **ov):
         """Potential, force and the NFFT-based stress sigma = (2/V) dE/d(strain)
@@ -399,6 +425,14 @@ class Context:
     def set_background(self, on: bool = True):
         """Charged cells with a uniform neutralising background (off by default)."""
         _check(lib().ewg_set_background(self._h, 1 if on else 0))
+
+    def set_graphs(self, on: bool = True):
+        """Record repeated evaluations as CUDA graphs and replay them (default on)."""
+        _check(lib().ewg_set_graphs(self._h, 1 if on else 0))
+
+    def set_force_scheme(self, scheme: int):
+        """FORCE_IK (the reference's scheme) or FORCE_AD (window derivatives)."""
+        _check(lib().ewg_set_force_scheme(self._h, int(scheme)))
 
     def xlbomd_gradients(self, tol, dq_out):
         """Gradient (N,3) of the XLBOMD shadow energy of the resident state."""

@@ -63,6 +63,16 @@ enum {
                               self term, reductions and lattice setup                 */
 };
 
+/* ---- force differentiation schemes --------------------------------------- */
+enum {
+  EWG_FORCE_IK = 0, /* the reference's scheme: the potential spectrum times i k per
+                       Cartesian component, four inverse transforms and gathers
+                       (fft/ewald_fft_3d_fourier.f90:130-151)                    */
+  EWG_FORCE_AD = 1  /* analytic differentiation of the window: one inverse
+                       transform; the gather applies the window and its
+                       derivative along each fractional axis                     */
+};
+
 /* Optional arguments of ewald_potential_force (fft/ewald_fft_3d.f90:36-77):
  * alpha_in, r_cut_in, k_cut_in, nModes_in, windowCutoff_in.  A member counts
  * only when its has_ flag is non-zero. */
@@ -89,6 +99,12 @@ const char* ewg_status_string(int status);
  * void*); NULL returns to the context's own stream.  Calls still complete on
  * the GPU before they return. */
 int ewg_set_stream(ewg_context* ctx, void* stream);
+/* CUDA graphs (on by default): an evaluation whose launch sequence -- sizes,
+ * device pointers, parameters, cell, stream -- repeats is recorded as a CUDA
+ * graph on its second call and replayed from the third, one graph launch in
+ * place of some thirty kernel launches.  Off with on = 0 (recorded graphs are
+ * released).  Not used while stage profiling is on. */
+int ewg_set_graphs(ewg_context* ctx, int on);
 /* Number of this library's kernels launched by the context so far. */
 long long ewg_kernel_launches(const ewg_context* ctx);
 /* Charged cells (on != 0): the fast path then accepts a net charge Q, with the
@@ -100,6 +116,19 @@ long long ewg_kernel_launches(const ewg_context* ctx);
  * path refuses charged cells (common/ewald_validation.f90:43-46); this mode
  * has no counterpart there (fft3d_readme.md:31).  Off by default. */
 int ewg_set_background(ewg_context* ctx, int on);
+/* Force differentiation scheme of the context's force evaluations
+ * (EWG_FORCE_IK or EWG_FORCE_AD).  Default: IK, the reference's own scheme,
+ * in both precision forms.  AD computes the
+ * reciprocal force as -q sum_d b_d sum_l g_l dW/ds_d, with g the potential grid
+ * and W the product of the three Gaussian windows; it spends one inverse
+ * transform where IK spends four.  Both converge to the same Ewald force; at
+ * the reference's parameters for tol = 1e-10 they differ by about 1e-12
+ * relative.  Potentials, energies and stresses do not depend on the scheme.
+ * In FP32 (the mixed form) ad is less robust: the derivative sums cancel, and
+ * in strongly anisotropic cells its error can exceed the i k form's by an
+ * order of magnitude; ewg_tune measures both and picks.
+ * No counterpart in the reference. */
+int ewg_set_force_scheme(ewg_context* ctx, int scheme);
 /* Parameters the last evaluation on this context used. */
 int ewg_last_params(const ewg_context* ctx, ewg_params* out);
 /* Measured dense FP64 tensor-core rate of the context's GPU (DMMA m8n8k4 on
@@ -142,6 +171,26 @@ int ewg_potential_force_stress(ewg_context* ctx, int n, const double* positions,
                                const double* charges, const double* lat_rows, double tol,
                                double* pot, double* force, double* sigma,
                                const ewg_overrides* ov);
+
+/* Parameter autotuner for the context's precision form (the mixed form in
+ * practice).  On the caller's configuration it evaluates candidates -- both
+ * force schemes, with the reference chain at tol = target/10, /5, /3, the
+ * real-space cutoff scaled by 1, 1.15, 1.3 or 1.5 (alpha, k_cut and the modes
+ * following from it) and window half-widths 6..9 -- against an FP64 i k
+ * evaluation at the reference's parameters for tol = 1e-10, times those whose
+ * RMS relative force error is at most target/2 and RMS relative potential
+ * error at most target, and returns the fastest: its parameters as overrides
+ * (alpha, r_cut, k_cut, window_cutoff; any tol in (0,1) may accompany them)
+ * and its force scheme in *scheme (may be NULL; apply it with
+ * ewg_set_force_scheme).  If no candidate meets the bar, the most accurate one
+ * is returned.  report (optional, 4 doubles): its force and potential RMS
+ * errors, its device milliseconds per force evaluation, and the number of
+ * candidates evaluated.  Results are cached in the context per (atoms, form,
+ * lattice, target); the context's force scheme is left as it was.
+ * No counterpart in the reference. */
+int ewg_tune(ewg_context* ctx, int n, const double* positions, const double* charges,
+             const double* lat_rows, double target, ewg_overrides* out, int* scheme,
+             double* report);
 
 /* ewald_parameters (fft/ewald_fft_3d.f90:142-191); host only. */
 int ewg_parameters(int n, const double* charges, const double* lat_rows, double tol,
