@@ -91,8 +91,17 @@ struct MeshGeom {
 struct RealGeom {
   int nb[3];       // boxes per axis
   int R[3];        // neighbour box range per axis
+  int flat;        // 1: the neighbourhood has at most 32 rows (dy, dz) and each
+                   // row is at most two contiguous runs of boxes (see set_scan_mode)
   double lat[3][3];
   double rec[3][3];
 };
+
+// The flat candidate scan needs every x row of 2R+1 boxes to split into at
+// most two runs (nb_x >= 2R_x + 1) and at most 32 rows.
+inline void set_scan_mode(RealGeom& g) {
+  const int rows = (2 * g.R[1] + 1) * (2 * g.R[2] + 1);
+  g.flat = (g.nb[0] >= 2 * g.R[0] + 1 && rows <= 32) ? 1 : 0;
+}
 
 }  // namespace ewg

@@ -157,11 +157,9 @@ void launch_inverse(const MeshPlan& mp, const void* B2, void* B1, void* out, int
 // partial sums of the nc interleaved real grids into part (nslots * nc per atom).
 // With mp.sd.ad and force wanted, the grid holds the potential alone (nc = 1)
 // and the partials are four: the potential and its derivatives along the three
-// fractional coordinates (window derivatives times the grid).  mesh_c: each
-// mesh-sorted atom's lowest stencil point (the FP32 form's reference value).
+// fractional coordinates (window derivatives times the grid).
 void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs, const void* wtab,
-                   const int4* mesh_c, const void* out_grid, int nc, double* part,
-                   cudaStream_t st);
+                   const void* out_grid, int nc, double* part, cudaStream_t st);
 
 // Fixed-order sum of each atom's partials with the final assembly
 // (fft/ewald_fft_3d.f90:121-132): pot = (sr + lr) + self, force = sr + q lr.

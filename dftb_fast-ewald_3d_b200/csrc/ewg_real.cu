@@ -405,6 +405,128 @@ __device__ __forceinline__ void for_each_candidate(const float4* __restrict__ x3
   }
 }
 
+// Flat scan (RealGeom::flat).  The neighbourhood's rows (dy, dz) are laid out
+// one per lane; each row is one or two contiguous runs of boxes (two when it
+// wraps around the cell in x).  The non-empty runs go to a per-warp table in
+// row order -- sorted index of the first atom, offset in the concatenated
+// candidate list, the run's x_i - S lat in FP32 and its shift S -- and the warp
+// then walks the concatenated list 32 candidates at a time, so that a warp
+// iteration is filled across run ends.  Candidate order (and with it the
+// summation order) is the same as the row-by-row scan's.
+constexpr int kRuns = 64;
+struct RunTable {
+  int j0[kRuns];
+  int start[kRuns + 1];  // offset of each run in the concatenated list; start[nrun] = total
+  int shift[kRuns];      // (sx + 512) | (sy + 512) << 10 | (sz + 512) << 20
+  float base[kRuns][3];  // x_i - S lat
+};
+
+template <class Visit>
+__device__ __forceinline__ void for_each_candidate_flat(const float4* __restrict__ x32,
+                                                        const int* __restrict__ box_start, int k,
+                                                        const double4& ai, const RealGeom& g,
+                                                        RunTable& t, Visit& visit) {
+  const int lane = threadIdx.x & 31;
+  int b[3];
+  const double sv[3] = {ai.x, ai.y, ai.z};
+  double xi[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    b[d] = min(static_cast<int>(sv[d] * g.nb[d]), g.nb[d] - 1);
+    xi[d] = sv[0] * g.lat[0][d] + sv[1] * g.lat[1][d] + sv[2] * g.lat[2][d];
+  }
+  const int wdy = 2 * g.R[1] + 1;
+  const int rows = wdy * (2 * g.R[2] + 1);
+  // This lane's row: up to two runs.
+  int j0[2] = {0, 0}, cnt[2] = {0, 0}, sx[2] = {0, 0}, sy = 0, sz = 0;
+  if (lane < rows) {
+    const int byr = b[1] + lane % wdy - g.R[1], bzr = b[2] + lane / wdy - g.R[2];
+    sy = floor_div(byr, g.nb[1]);
+    sz = floor_div(bzr, g.nb[2]);
+    const int wy = byr - sy * g.nb[1], wz = bzr - sz * g.nb[2];
+    int dx = -g.R[0];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (dx <= g.R[0]) {
+        const int bxr = b[0] + dx;
+        const int s = floor_div(bxr, g.nb[0]);
+        const int wx = bxr - s * g.nb[0];
+        const int len = min(g.R[0] - dx + 1, g.nb[0] - wx);
+        const int first = (wz * g.nb[1] + wy) * g.nb[0] + wx;
+        j0[h] = box_start[first];
+        cnt[h] = box_start[first + len] - j0[h];
+        sx[h] = s;
+        dx += len;
+      }
+    }
+  }
+  // Compact the non-empty runs into the table in (row, run) order.
+  const unsigned below = (1u << lane) - 1u;
+  const unsigned m0 = __ballot_sync(0xffffffffu, cnt[0] > 0);
+  const unsigned m1 = __ballot_sync(0xffffffffu, cnt[1] > 0);
+  const int nrun = __popc(m0) + __popc(m1);
+  int pos = __popc(m0 & below) + __popc(m1 & below);
+  __syncwarp();
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    if (cnt[h] > 0) {
+      t.j0[pos] = j0[h];
+      t.start[pos] = cnt[h];  // counts for now; turned into offsets below
+      t.shift[pos] = (sx[h] + 512) | ((sy + 512) << 10) | ((sz + 512) << 20);
+#pragma unroll
+      for (int d = 0; d < 3; ++d)
+        t.base[pos][d] = static_cast<float>(
+            xi[d] - (sx[h] * g.lat[0][d] + sy * g.lat[1][d] + sz * g.lat[2][d]));
+      ++pos;
+    }
+  }
+  __syncwarp();
+  // Exclusive prefix of the counts (entries lane and lane + 32).
+  const int c0 = lane < nrun ? t.start[lane] : 0, c1 = lane + 32 < nrun ? t.start[lane + 32] : 0;
+  int s0 = c0, s1 = c1;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const int u0 = __shfl_up_sync(0xffffffffu, s0, off), u1 = __shfl_up_sync(0xffffffffu, s1, off);
+    if (lane >= off) {
+      s0 += u0;
+      s1 += u1;
+    }
+  }
+  const int half = __shfl_sync(0xffffffffu, s0, 31);
+  const int total = half + __shfl_sync(0xffffffffu, s1, 31);
+  __syncwarp();
+  if (lane < nrun) t.start[lane] = s0 - c0;
+  if (lane + 32 < nrun) t.start[lane + 32] = half + s1 - c1;
+  if (lane == 0) t.start[nrun] = total;
+  __syncwarp();
+  int rc = 0;  // the run holding the iteration's first candidate
+  for (int v0 = 0; v0 < total; v0 += 32) {
+    const int v = v0 + lane;
+    Candidate c;
+    c.j = 0;
+    c.sx = c.sy = c.sz = 0;
+    c.valid = false;
+    c.r2 = 3.0e38f;
+    if (v < total) {
+      int r = rc;
+      while (t.start[r + 1] <= v) ++r;
+      c.j = t.j0[r] + (v - t.start[r]);
+      const int sh = t.shift[r];
+      c.sx = (sh & 0x3ff) - 512;
+      c.sy = ((sh >> 10) & 0x3ff) - 512;
+      c.sz = (sh >> 20) - 512;
+      c.valid = !(c.sx == 0 && c.sy == 0 && c.sz == 0 && c.j == k);
+      if (c.valid) {
+        const float4 xj = x32[c.j];
+        const float d0 = t.base[r][0] - xj.x, d1 = t.base[r][1] - xj.y, d2 = t.base[r][2] - xj.z;
+        c.r2 = fmaf(d0, d0, fmaf(d1, d1, d2 * d2));
+      }
+    }
+    visit(c);
+    while (rc + 1 < nrun && t.start[rc + 1] <= v0 + 32) ++rc;
+  }
+}
+
 // FP32 prefilter bound for the FP64 cutoff test: the candidate separations
 // carry a rounding error of a few FP32 ulps of the largest coordinate and
 // shift, far below the margin.
@@ -455,8 +577,10 @@ struct EwaldPair {
   }
 };
 
+// Four CTAs of 256 threads per SM (64 registers): the candidate loads and the
+// pair terms' dependent FP64 chains want the warps.
 template <bool MIXED>
-__global__ void __launch_bounds__(kRealThreads) k_real_space(const double4* __restrict__ srt,
+__global__ void __launch_bounds__(kRealThreads, 4) k_real_space(const double4* __restrict__ srt,
                                                              const float4* __restrict__ x32,
                                                              const int* __restrict__ perm,
                                                              const int* __restrict__ box_start,
@@ -466,6 +590,7 @@ __global__ void __launch_bounds__(kRealThreads) k_real_space(const double4* __re
                                                              double* __restrict__ force,
                                                              int* __restrict__ err) {
   __shared__ __align__(16) int4 queue[kRealThreads / 32][kQueue];
+  __shared__ RunTable runs[kRealThreads / 32];
   const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (k >= n) return;
@@ -474,7 +599,10 @@ __global__ void __launch_bounds__(kRealThreads) k_real_space(const double4* __re
   pair.alpha = alpha;
   pair.qi = ai.w;
   PairQueue<EwaldPair, MIXED> pq(queue[threadIdx.x >> 5], pair, srt, ai, g, cut2, pre2);
-  for_each_candidate(x32, box_start, k, ai, g, pq);
+  if (g.flat)
+    for_each_candidate_flat(x32, box_start, k, ai, g, runs[threadIdx.x >> 5], pq);
+  else
+    for_each_candidate(x32, box_start, k, ai, g, pq);
   pq.flush();
   double v[4] = {pair.pot, pair.f[0], pair.f[1], pair.f[2]};
 #pragma unroll
@@ -521,6 +649,7 @@ __global__ void __launch_bounds__(kRealThreads) k_real_stress(const double4* __r
                                                               double* __restrict__ partial6,
                                                               int* __restrict__ err) {
   __shared__ __align__(16) int4 queue[kRealThreads / 32][kQueue];
+  __shared__ RunTable runs[kRealThreads / 32];
   const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (k >= n) return;
@@ -529,7 +658,10 @@ __global__ void __launch_bounds__(kRealThreads) k_real_stress(const double4* __r
   pair.alpha = alpha;
   pair.qi = ai.w;
   PairQueue<StressPair, false> pq(queue[threadIdx.x >> 5], pair, srt, ai, g, cut2, pre2);
-  for_each_candidate(x32, box_start, k, ai, g, pq);
+  if (g.flat)
+    for_each_candidate_flat(x32, box_start, k, ai, g, runs[threadIdx.x >> 5], pq);
+  else
+    for_each_candidate(x32, box_start, k, ai, g, pq);
   pq.flush();
 #pragma unroll
   for (int j = 0; j < 6; ++j) pair.s[j] = warp_sum(pair.s[j]);

@@ -240,6 +240,7 @@ extern "C" int ewg_direct_potential_force_static(int n, const double* coords_dev
       rg.rec[d][f] = cell.rec[d][f];
     }
   }
+  set_scan_mode(rg);
   const int nboxes = rg.nb[0] * rg.nb[1] * rg.nb[2];
   ModeBox mb;
   long nmodes = 1;

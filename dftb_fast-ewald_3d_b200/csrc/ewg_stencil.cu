@@ -299,7 +299,7 @@ __device__ __forceinline__ void dmma_m8n8k4(double& c0, double& c1, double a, do
 
 constexpr int kGatherWarps = 4;   // FP64 gather: warps per tile
 constexpr int kGatherMB = 2;      // FP64 gather: M blocks of 8 atoms per warp and round
-constexpr int kGatherAdWarps = 4;  // FP64 gather with window derivatives: warps per tile
+constexpr int kGatherAdWarps = 2;  // FP64 gather with window derivatives: warps per tile
 constexpr int kSpreadAtoms = 64;  // atoms staged per round, one per thread
 constexpr int kWRow = 12;         // doubles per staged weight row: 8 used; the
                                   // padding makes the fragment reads conflict-free
@@ -519,45 +519,49 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles(const int* __restri
 // needs phi = sum W g and D_d = sum D_d g.  The derivative weights change sign
 // across the stencil while g carries a large smooth part, so in FP32 the sums
 // would cancel; they run instead on g' = g - c, with c the grid value at the
-// atom's lowest stencil point, and the tile's c terms are added back in FP64
-// from the tile's weight sums:
+// tile's first point (subtracted once, when the tile is staged), and the
+// tile's c terms are added back in FP64 from the tile's weight sums:
 //   phi_t = sum_t W g' + c Sx Sy Sz,  D_1,t = sum_t dW_1 g' + c dSx Sy Sz, ...
 // (S, dS: sums over the tile's points of the weights and their derivatives).
 // Per (z, y) row two x sums, r0 = sum_x w1 g' and r1 = sum_x dw1 g', feed all
 // four:  phi += w2 w3 r0, D_1 += w2 w3 r1, D_2 += dw2 w3 r0, D_3 += w2 dw3 r0.
-// Lanes carry A atoms of the tile's list as in k_gather_tiles; products and
-// plane sums in FP32, the sum over planes in FP64; the four partials go to the
-// atom's slot.
+// Lanes carry A atoms of the tile's list as in k_gather_tiles (x weights in
+// registers, y and z rows staged in shared memory); products and plane sums in
+// FP32, the sum over planes in FP64; the four partials go to the atom's slot.
 // ---------------------------------------------------------------------------
 template <int A, int WARPS>
 __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_ad(const int* __restrict__ tile_start,
                                                                 const int2* __restrict__ pairs,
                                                                 const float* __restrict__ wtab,
-                                                                const int4* __restrict__ mc,
                                                                 StencilDims sd,
                                                                 const float* __restrict__ grid,
                                                                 double* __restrict__ part) {
   __shared__ float sG[TZ * TY * TX];
-  __shared__ float sW3[WARPS][TZ][32 * A];  // z weights, lane fastest
-  __shared__ float sD3[WARPS][TZ][32 * A];  // their derivatives
+  // y and z weights and their derivatives, lane fastest: [kind][row][lane]
+  // with kind 0 = w2, 1 = dw2, 2 = w3, 3 = dw3.
+  __shared__ float sYZ[WARPS][4][TY][32 * A];
+  static_assert(TY == TZ, "y and z rows share one staging layout");
   const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
   const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
   const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
   const int ex = min(TX, sd.n[0] - x0), ey = min(TY, sd.n[1] - y0), ez = min(TZ, sd.n[2] - z0);
   const int p0 = tile_start[tile], p1 = tile_start[tile + 1];
   if (p0 == p1) return;  // no atom reaches this tile
+  const float cg = grid[(static_cast<size_t>(z0) * sd.n[1] + y0) * sd.n[0] + x0];
 #pragma unroll 4
   for (int t = threadIdx.x; t < TX * TY * TZ; t += 32 * WARPS) {
     const int x = t % TX, y = (t / TX) % TY, z = t / (TX * TY);
+    // points past the grid's end carry zero weight for every atom
     sG[t] = (x < ex && y < ey && z < ez)
-                ? grid[(static_cast<size_t>(z0 + z) * sd.n[1] + y0 + y) * sd.n[0] + x0 + x]
+                ? grid[(static_cast<size_t>(z0 + z) * sd.n[1] + y0 + y) * sd.n[0] + x0 + x] - cg
                 : 0.0f;
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nslots = sd.S[0] * sd.S[1] * sd.S[2];
+  float(*YZ)[TY][32 * A] = sYZ[warp];
   for (int a0 = p0 + warp * 32 * A; a0 < p1; a0 += WARPS * 32 * A) {
-    float w1[A][TX], d1[A][TX], w2[A][TY], d2[A][TY], cg[A];
+    float w1[A][TX], d1[A][TX];
     int2 pr[A];
     bool act[A];
 #pragma unroll
@@ -569,23 +573,22 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_ad(const int* __res
       const int ox = sd.woff[0] + (pr[a].y & 0xff) * TX;
       const int oy = sd.woff[1] + ((pr[a].y >> 8) & 0xff) * TY;
       const int oz = sd.woff[2] + (pr[a].y >> 16) * TZ;
-      cg[a] = 0.0f;
+      float t[4][8];
       if (act[a]) {
         load8(wk + ox, w1[a]);
         load8(wk + sd.dwoff + ox, d1[a]);
-        load8(wk + oy, w2[a]);
-        load8(wk + sd.dwoff + oy, d2[a]);
-        const int4 m = mc[pr[a].x];  // the atom's lowest stencil point
-        cg[a] = grid[(static_cast<size_t>(m.z) * sd.n[1] + m.y) * sd.n[0] + m.x];
+        load8(wk + oy, t[0]);
+        load8(wk + sd.dwoff + oy, t[1]);
+        load8(wk + oz, t[2]);
+        load8(wk + sd.dwoff + oz, t[3]);
       } else {
 #pragma unroll
-        for (int j = 0; j < 8; ++j) w1[a][j] = d1[a][j] = w2[a][j] = d2[a][j] = 0.0f;
+        for (int j = 0; j < 8; ++j) w1[a][j] = d1[a][j] = t[0][j] = t[1][j] = t[2][j] = t[3][j] = 0.0f;
       }
 #pragma unroll
-      for (int z = 0; z < TZ; ++z) {
-        sW3[warp][z][a * 32 + lane] = act[a] ? wk[oz + z] : 0.0f;
-        sD3[warp][z][a * 32 + lane] = act[a] ? wk[sd.dwoff + oz + z] : 0.0f;
-      }
+      for (int kd = 0; kd < 4; ++kd)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) YZ[kd][j][a * 32 + lane] = t[kd][j];
     }
     __syncwarp();
     double acc[A][4];
@@ -601,8 +604,8 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_ad(const int* __res
       float w3[A], d3[A], pl[A][4];
 #pragma unroll
       for (int a = 0; a < A; ++a) {
-        w3[a] = sW3[warp][z][a * 32 + lane];
-        d3[a] = sD3[warp][z][a * 32 + lane];
+        w3[a] = YZ[2][z][a * 32 + lane];
+        d3[a] = YZ[3][z][a * 32 + lane];
         sz[a] += w3[a];
         dsz[a] += d3[a];
         pl[a][0] = pl[a][1] = pl[a][2] = pl[a][3] = 0.0f;  // plane sums, FP32
@@ -611,11 +614,13 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_ad(const int* __res
       for (int y = 0; y < TY; ++y) {
         // A zero window product means the row lies outside the atom's stencil
         // along y or z, where the derivatives vanish as well.
-        float w23[A];
+        float w2[A], d2[A], w23[A];
         bool any = false;
 #pragma unroll
         for (int a = 0; a < A; ++a) {
-          w23[a] = w2[a][y] * w3[a];
+          w2[a] = YZ[0][y][a * 32 + lane];
+          d2[a] = YZ[1][y][a * 32 + lane];
+          w23[a] = w2[a] * w3[a];
           any = any || (w23[a] != 0.0f);
         }
         if (!__any_sync(0xffffffffu, any)) continue;
@@ -628,17 +633,16 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_ad(const int* __res
           const float g = row[x];
 #pragma unroll
           for (int a = 0; a < A; ++a) {
-            const float gs = g - cg[a];
-            r0[a] = fmaf(w1[a][x], gs, r0[a]);
-            r1[a] = fmaf(d1[a][x], gs, r1[a]);
+            r0[a] = fmaf(w1[a][x], g, r0[a]);
+            r1[a] = fmaf(d1[a][x], g, r1[a]);
           }
         }
 #pragma unroll
         for (int a = 0; a < A; ++a) {
           pl[a][0] = fmaf(w23[a], r0[a], pl[a][0]);
           pl[a][1] = fmaf(w23[a], r1[a], pl[a][1]);
-          pl[a][2] = fmaf(d2[a][y] * w3[a], r0[a], pl[a][2]);
-          pl[a][3] = fmaf(w2[a][y] * d3[a], r0[a], pl[a][3]);
+          pl[a][2] = fmaf(d2[a] * w3[a], r0[a], pl[a][2]);
+          pl[a][3] = fmaf(w2[a] * d3[a], r0[a], pl[a][3]);
         }
       }
 #pragma unroll
@@ -655,10 +659,10 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_ad(const int* __res
       for (int j = 0; j < 8; ++j) {
         sx += w1[a][j];
         dsx += d1[a][j];
-        sy += w2[a][j];
-        dsy += d2[a][j];
+        sy += YZ[0][j][a * 32 + lane];
+        dsy += YZ[1][j][a * 32 + lane];
       }
-      const double c = cg[a];
+      const double c = cg;
       acc[a][0] += c * sx * sy * sz[a];
       acc[a][1] += c * dsx * sy * sz[a];
       acc[a][2] += c * sx * dsy * sz[a];
@@ -669,7 +673,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_ad(const int* __res
 #pragma unroll
       for (int c4 = 0; c4 < 4; ++c4) dst[c4] = acc[a][c4];
     }
-    __syncwarp();  // sW3 and sD3 are rewritten by the next iteration
+    __syncwarp();  // the staged rows are rewritten by the next iteration
   }
 }
 
@@ -830,9 +834,9 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma(const int* __r
 // afterwards:
 //   phi = sum_z w3 sum_y w2 C_w,  D_1 = sum_z w3 sum_y w2 C_d,
 //   D_2 = sum_z w3 sum_y dw2 C_w,  D_3 = sum_z dw3 sum_y w2 C_w.
-// One warp per M block of 8 atoms, WARPS warps per round.  Shared layout and
-// fragment mapping as in k_gather_tiles_dmma with NC = 1; six weight rows per
-// atom (w1 w2 w3 dw1 dw2 dw3).
+// WARPS warps per tile, each taking blocks of 8 atoms (one M block) on its own.
+// Shared layout and fragment mapping as in k_gather_tiles_dmma with NC = 1; six
+// weight rows per atom (w1 w2 w3 dw1 dw2 dw3).
 // ---------------------------------------------------------------------------
 template <int WARPS>
 __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma_ad(
@@ -840,10 +844,8 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma_ad(
     const double* __restrict__ wtab, StencilDims sd, const double* __restrict__ grid,
     double* __restrict__ part) {
   constexpr int RS = GatherRow<1>::value;
-  constexpr int kAtoms = WARPS * 8;  // atoms staged per round
   __shared__ __align__(16) double sG[TZ * TY * RS];
-  __shared__ __align__(16) double sW[6][kAtoms][kWRow];
-  __shared__ int2 sPair[kAtoms];
+  __shared__ __align__(16) double sW[WARPS][6][8][kWRow];  // per warp: its 8 atoms' rows
   const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
   const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
   const int p0 = tile_start[tile], p1 = tile_start[tile + 1];
@@ -867,36 +869,34 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma_ad(
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int fr = lane >> 2, fk = lane & 3;
   const int nslots = sd.S[0] * sd.S[1] * sd.S[2];
-  for (int b0 = p0; b0 < p1; b0 += kAtoms) {
-    const int nb = min(kAtoms, p1 - b0);
-    __syncthreads();  // the previous round's weights are no longer read
-    for (int a = threadIdx.x; a < kAtoms; a += blockDim.x) {
-      if (a < nb) {
-        const int2 pr = pairs[b0 + a];
-        sPair[a] = pr;
-        const double* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
-        const int off[3] = {sd.woff[0] + (pr.y & 0xff) * TX, sd.woff[1] + ((pr.y >> 8) & 0xff) * TY,
-                            sd.woff[2] + (pr.y >> 16) * TZ};
+  double(*W)[8][kWRow] = sW[warp];
+  cp_async_wait_all();
+  __syncthreads();  // the tile, staged by all warps; the only CTA barrier
+  // Each warp takes blocks of 8 atoms of the tile's list on its own.  Lane
+  // (fr, fk) stages 16-byte chunk fk of atom fr's six rows and later holds
+  // that atom's fragments.
+  for (int b0 = p0 + warp * 8; b0 < p1; b0 += WARPS * 8) {
+    const int nb = min(8, p1 - b0);
+    __syncwarp();  // the previous block's rows are no longer read
+    int2 pr = make_int2(0, 0);
+    if (fr < nb) {
+      pr = pairs[b0 + fr];
+      const double* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
+      const int off[3] = {sd.woff[0] + (pr.y & 0xff) * TX, sd.woff[1] + ((pr.y >> 8) & 0xff) * TY,
+                          sd.woff[2] + (pr.y >> 16) * TZ};
 #pragma unroll
-        for (int d = 0; d < 3; ++d)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            cp_async16(&sW[d][a][2 * j], wk + off[d] + 2 * j);
-            cp_async16(&sW[3 + d][a][2 * j], wk + sd.dwoff + off[d] + 2 * j);
-          }
-      } else {  // rows past the list: zero weights, results discarded
-#pragma unroll
-        for (int d = 0; d < 6; ++d)
-#pragma unroll
-          for (int j = 0; j < 8; ++j) sW[d][a][j] = 0.0;
+      for (int d = 0; d < 3; ++d) {
+        cp_async16(&W[d][fr][2 * fk], wk + off[d] + 2 * fk);
+        cp_async16(&W[3 + d][fr][2 * fk], wk + sd.dwoff + off[d] + 2 * fk);
       }
+    } else {  // rows past the list: zero weights, results discarded
+#pragma unroll
+      for (int d = 0; d < 6; ++d) W[d][fr][2 * fk] = W[d][fr][2 * fk + 1] = 0.0;
     }
-    cp_async_wait_all();  // also completes the tile copies on the first round
-    __syncthreads();
-    if (warp * 8 >= nb) continue;
-    const int am = warp * 8 + fr;  // this lane's atom row
-    const double fw0 = sW[0][am][fk], fw1 = sW[0][am][4 + fk];
-    const double fd0 = sW[3][am][fk], fd1 = sW[3][am][4 + fk];
+    cp_async_wait_all();
+    __syncwarp();
+    const double fw0 = W[0][fr][fk], fw1 = W[0][fr][4 + fk];
+    const double fd0 = W[3][fr][fk], fd1 = W[3][fr][4 + fk];
     double cw[TZ][2], cd[TZ][2];
 #pragma unroll
     for (int z = 0; z < TZ; ++z) {
@@ -910,12 +910,12 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma_ad(
       dmma_m8n8k4(cd[z][0], cd[z][1], fd1, b1v);
     }
     // This lane holds C for y = 2 fk and 2 fk + 1 of every plane.
-    const double w20 = sW[1][am][2 * fk], w21 = sW[1][am][2 * fk + 1];
-    const double d20 = sW[4][am][2 * fk], d21 = sW[4][am][2 * fk + 1];
+    const double w20 = W[1][fr][2 * fk], w21 = W[1][fr][2 * fk + 1];
+    const double d20 = W[4][fr][2 * fk], d21 = W[4][fr][2 * fk + 1];
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int z = 0; z < TZ; ++z) {
-      const double w3 = sW[2][am][z], d3 = sW[5][am][z];
+      const double w3 = W[2][fr][z], d3 = W[5][fr][z];
       const double pw = fma(w20, cw[z][0], w21 * cw[z][1]);
       const double pd = fma(w20, cd[z][0], w21 * cd[z][1]);
       const double qw = fma(d20, cw[z][0], d21 * cw[z][1]);
@@ -929,10 +929,10 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma_ad(
       acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], 1);
       acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], 2);
     }
-    if (fk == 0 && am < nb) {
-      const int ps = sPair[am].y;
+    if (fk == 0 && fr < nb) {
+      const int ps = pr.y;
       const int sidx = ((ps >> 16) * sd.S[1] + ((ps >> 8) & 0xff)) * sd.S[0] + (ps & 0xff);
-      double* dst = part + (static_cast<size_t>(sPair[am].x) * nslots + sidx) * 4;
+      double* dst = part + (static_cast<size_t>(pr.x) * nslots + sidx) * 4;
 #pragma unroll
       for (int c = 0; c < 4; ++c) dst[c] = acc[c];
     }
@@ -1064,7 +1064,7 @@ void launch_spread(const MeshPlan& mp, const int* tile_start, const int2* pairs,
 }
 
 void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs, const void* wtab,
-                   const int4* mesh_c, const void* grid, int nc, double* part, cudaStream_t st) {
+                   const void* grid, int nc, double* part, cudaStream_t st) {
   dim3 grd(mp.sd.ntiles[0], mp.sd.ntiles[1], mp.sd.ntiles[2]);
 #define EWG_GATHER(R, NC)                                                               \
   k_gather_tiles<R, NC, GatherShape<R>::atoms, GatherShape<R>::warps>                      \
@@ -1074,8 +1074,8 @@ void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs,
     if (mp.mixed)
       k_gather_tiles_ad<GatherShape<float>::atoms, GatherShape<float>::warps>
           <<<grd, 32 * GatherShape<float>::warps, 0, st>>>(
-              tile_start, pairs, static_cast<const float*>(wtab), mesh_c,
-              mp.sd, static_cast<const float*>(grid), part);
+              tile_start, pairs, static_cast<const float*>(wtab), mp.sd,
+              static_cast<const float*>(grid), part);
     else
       k_gather_tiles_dmma_ad<kGatherAdWarps><<<grd, 32 * kGatherAdWarps, 0, st>>>(
           tile_start, pairs, static_cast<const double*>(wtab), mp.sd,

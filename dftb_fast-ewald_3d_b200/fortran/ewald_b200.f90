@@ -18,10 +18,13 @@ module ewald_b200
   public :: ewaldGpuSetLattice, ewaldGpuSetCoords, ewaldGpuSetCharges
   public :: ewaldGpuShift, ewaldGpuShiftForce, ewaldGpuStress, ewaldGpuStressFast
   public :: ewaldGpuPotentialForce, ewaldGpuPotentialAt, ewaldGpuPotentialGradientAt
-  public :: EWG_PRECISION_FP64, EWG_PRECISION_MIXED
+  public :: ewaldGpuSetForceScheme
+  public :: EWG_PRECISION_FP64, EWG_PRECISION_MIXED, EWG_FORCE_IK, EWG_FORCE_AD
 
   integer(c_int), parameter :: EWG_PRECISION_FP64 = 0
   integer(c_int), parameter :: EWG_PRECISION_MIXED = 1
+  integer(c_int), parameter :: EWG_FORCE_IK = 0
+  integer(c_int), parameter :: EWG_FORCE_AD = 1
 
   !> Handle of one device context.
   type :: TEwaldGpu
@@ -102,6 +105,13 @@ module ewald_b200
       real(c_double), intent(out) :: sigma(3, 3)
       integer(c_int) :: rc
     end function ewg_stress
+
+    function ewg_set_force_scheme(ctx, scheme) bind(C, name="ewg_set_force_scheme") result(rc)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: scheme
+      integer(c_int) :: rc
+    end function ewg_set_force_scheme
 
     function ewg_stress_fast(ctx, tol, sigma) bind(C, name="ewg_stress_fast") result(rc)
       import :: c_ptr, c_int, c_double
@@ -229,6 +239,14 @@ contains
     real(c_double), intent(out) :: sigma(3, 3)
     call check(ewg_stress(this%ctx, tolEwald, alpha, sigma))
   end subroutine ewaldGpuStress
+
+  !> Force differentiation scheme: EWG_FORCE_IK, the reference's i k (default),
+  !> or EWG_FORCE_AD, window derivatives (one inverse transform instead of four).
+  subroutine ewaldGpuSetForceScheme(this, scheme)
+    type(TEwaldGpu), intent(inout) :: this
+    integer(c_int), intent(in) :: scheme
+    call check(ewg_set_force_scheme(this%ctx, scheme))
+  end subroutine ewaldGpuSetForceScheme
 
   !> NFFT-based stress of the fast engine on the resident state; same convention as
   !> ewaldGpuStress (the caller does stress = stress - 0.5 * sigma).

@@ -1,7 +1,8 @@
 """Replay of evaluation launch sequences as CUDA graphs (ewg_set_graphs): the
-replayed evaluations give bitwise the results of direct launches, follow new
-input values behind the same device pointers, count their kernels, and survive
-buffer reallocation by a larger system in between."""
+replayed evaluations give bitwise the results of direct launches through the
+same entry point, follow new input values behind the same device pointers,
+count their kernels, and survive buffer reallocation by a larger system in
+between."""
 
 import numpy as np
 import pytest
@@ -29,7 +30,10 @@ def test_replay_matches_direct_launches(ewald_lib, precision):
     direct.set_graphs(False)
     try:
         x, qq, pot, force = _device_inputs(pos, q)
-        ref_pot, ref_force = direct.potential_force(pos, q, lat, 1e-10)
+        _, _, rpot, rforce = _device_inputs(pos, q)
+        direct.potential_force_device(x, qq, lat, 1e-10, rpot, rforce)
+        torch.cuda.synchronize()
+        ref_pot, ref_force = rpot.cpu().numpy(), rforce.cpu().numpy()
         counts = []
         for _ in range(4):  # direct, record + replay, replay, replay
             before = graphs.kernel_launches
@@ -43,10 +47,10 @@ def test_replay_matches_direct_launches(ewald_lib, precision):
         pos2 = np.asarray(pos) + np.array([0.3, -0.2, 0.1])
         x.copy_(torch.tensor(pos2, dtype=torch.float64, device="cuda"))
         graphs.potential_force_device(x, qq, lat, 1e-10, pot, force)
+        direct.potential_force_device(x, qq, lat, 1e-10, rpot, rforce)
         torch.cuda.synchronize()
-        p2, f2 = direct.potential_force(pos2, q, lat, 1e-10)
-        assert np.array_equal(pot.cpu().numpy(), p2)
-        assert np.array_equal(force.cpu().numpy(), f2)
+        assert torch.equal(pot, rpot) and torch.equal(force, rforce)
+        assert not np.array_equal(pot.cpu().numpy(), ref_pot)  # the new positions took effect
     finally:
         graphs.close()
         direct.close()
