@@ -165,7 +165,7 @@ def stage_flops(params, natoms, nc=4):
 
 
 # DRAM bytes (read + write) per launch from one ncu capture of the 32,769-atom
-# workload (profiles/c3_water_32k_top_kernels.md), keyed by (real bytes, grids
+# workload (profiles/c3_water_32k_fp64_top_kernels.md), keyed by (real bytes, grids
 # through the inverse passes and the gather, stage).
 DRAM_TRAFFIC = {
     (8, 4, "gather"): 746.37e6 + 62.96e6,
@@ -416,7 +416,14 @@ def run_ours(args):
         # timed, no JSON line (numbers taken under a profiler are not results).
         prec, tol = (eb.MIXED, TOL_MIXED) if args.profile_only == "mixed" else (eb.FP64, TOL_FP64)
         scheme = eb.FORCE_AD if args.profile_only == "fp64_ad" else None
-        arm = Arm(eb, torch, device, prec, tol, pos, q, lat, scheme=scheme)
+        ov = None
+        if args.profile_only == "mixed" and args.mixed_params:
+            # the tuned parameters of a previous bench line: mixed.params
+            mp = json.loads(args.mixed_params)
+            ov = {"alpha_in": mp["alpha"], "r_cut_in": mp["r_cut_bohr"], "k_cut_in": mp["k_cut"],
+                  "windowCutoff_in": mp["window_cutoff"]}
+            scheme = eb.FORCE_AD if mp["forces"] == "window differentiation" else eb.FORCE_IK
+        arm = Arm(eb, torch, device, prec, tol, pos, q, lat, scheme=scheme, ov=ov)
         for _ in range(args.warmup + args.steps):
             arm.step_device()
         torch.cuda.synchronize()
@@ -596,7 +603,8 @@ def run_ours(args):
             "value": ws * args.steps / t32, "unit": "evals/s", "forces": scheme_name[tuned_scheme],
             "params": {"source": f"ewg_tune, target {MIXED_TARGET:g} (RMS force error <= "
                                  f"{MIXED_TARGET / 2:g} vs the FP64 form)",
-                       "alpha": params32["alpha"], "r_cut_bohr": params32["r_cut"],
+                       "forces": scheme_name[tuned_scheme], "alpha": params32["alpha"],
+                       "r_cut_bohr": params32["r_cut"], "k_cut": params32["k_cut"],
                        "grid": grid_of(params32), "window_cutoff": params32["window_cutoff"],
                        "tuner_report": tune_report},
             "speedup_vs_fp64": (ws * args.steps / t32) / value,
@@ -625,6 +633,9 @@ def main():
                     help="c3 (default, the headline) or another configuration of the table")
     ap.add_argument("--profile-only", choices=["fp64", "fp64_ad", "mixed"], default=None,
                     help="run warm-up + steps evaluations of one form for a profiler; no timing")
+    ap.add_argument("--mixed-params", default=None,
+                    help="with --profile-only mixed: a bench line's mixed.params (JSON) to run "
+                         "the tuned parameters instead of the reference chain at tol 1e-7")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -21,7 +21,7 @@ constexpr int kTiles[3] = {kTileX, kTileY, kTileZ};
 
 // Device buffers owned by a context, grown on demand and reused across calls.
 enum BufId {
-  B_POS, B_Q, B_POT, B_FORCE, B_POT_SR, B_F_SR, B_S4, B_S4S, B_BOXKEY, B_MC, B_MCS, B_FR, B_FRS,
+  B_POS, B_Q, B_POT, B_FORCE, B_POT_SR, B_F_SR, B_S4, B_S4S, B_BOXKEY, B_MC, B_FR,
   B_TILEKEY, B_COUNTS, B_CURSOR, B_BOXSTART, B_TILESTART, B_TMP, B_PERMBOX, B_PERMMESH, B_WTAB,
   B_QK, B_GRID, B_A1, B_A2, B_B2, B_B1, B_OUT, B_ERR, B_SUMS, B_PARTIAL, B_KVEC, B_SK, B_WK,
   B_P6, B_O6, B_COORDS, B_SLOT, B_PART, B_PAIRTMP, B_PAIRS, B_PAIRSTART, B_CELLERR, B_ZPART,
@@ -378,9 +378,7 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
   float4* x32s = dbuf<float4>(c, B_X32S, n, &rc);
   int* boxkey = dbuf<int>(c, B_BOXKEY, n, &rc);
   int4* mcv = dbuf<int4>(c, B_MC, n, &rc);
-  int4* mcs = dbuf<int4>(c, B_MCS, n, &rc);
   double4* fr = dbuf<double4>(c, B_FR, n, &rc);
-  double4* frs = dbuf<double4>(c, B_FRS, n, &rc);
   int* tilekey = dbuf<int>(c, B_TILEKEY, n, &rc);
   int* counts = dbuf<int>(c, B_COUNTS, std::max(nboxes, ntiles), &rc);
   int* cursor = dbuf<int>(c, B_CURSOR, std::max(nboxes, ntiles), &rc);
@@ -449,10 +447,8 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
       launch_bucket_sort(boxkey, n, nboxes, bcounts, bcursor, boxstart, btmp, permbox, rs);
       launch_permute_box(s4, permbox, n, cell.lat, s4s, x32s, rs);
       launch_bucket_sort(tilekey, n, ntiles, counts, cursor, tilestart, tmp, permmesh, st);
-      launch_permute_int4(mcv, permmesh, n, mcs, st);
-      launch_permute4(fr, permmesh, n, frs, st);
       prof_mark(mp.prof, st, ST_WEIGHTS);
-      launch_weights(mp, mcs, frs, n, wtab, qk, slot, st);
+      launch_weights(mp, mcv, fr, permmesh, n, wtab, qk, slot, st);
       launch_pair_bins(mp, slot, n, counts, cursor, pairstart, pairtmp, pairs, npairs_max, st);
     } else {
       // Geometry unchanged: refresh only the charges in the sorted layouts.
@@ -465,9 +461,8 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
       launch_permute_box(s4, permbox, n, cell.lat, s4s, x32s, rs);
       launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, mp.g.n, kTiles, mp.sd.ntiles, nullptr,
                        nullptr, mcv, fr, tilekey, st);
-      launch_permute4(fr, permmesh, n, frs, st);
       prof_mark(mp.prof, st, ST_WEIGHTS);
-      launch_weights(mp, mcs, frs, n, wtab, qk, slot, st);
+      launch_weights(mp, mcv, fr, permmesh, n, wtab, qk, slot, st);
     }
     prof_mark(mp.prof, st, ST_REAL);
     launch_real_space(s4s, x32s, permbox, boxstart, n, rg, p.alpha, p.r_cut, mixed, pot_sr, f_sr,

@@ -128,9 +128,10 @@ struct MeshPlan {
 
 // Tiled window weights per mesh-sorted atom (wtab: wstride values per atom),
 // slot origin and count per axis (slot: first | count << 16 in x, y, z), and
-// the charges in mesh order (qk).
-void launch_weights(const MeshPlan& mp, const int4* mesh_c_sorted, const double4* mesh_fr_sorted,
-                    int n, void* wtab, void* qk, int4* slot, cudaStream_t st);
+// the charges in mesh order (qk).  mesh_c / mesh_fr are in atom order and are
+// read through the mesh permutation (sorted atom k is atom perm[k]).
+void launch_weights(const MeshPlan& mp, const int4* mesh_c, const double4* mesh_fr,
+                    const int* perm, int n, void* wtab, void* qk, int4* slot, cudaStream_t st);
 
 // Bins every (atom, tile) pair by tile, buckets ordered by atom index:
 // pairs[tile_start[t] .. tile_start[t+1]) = (atom, packed slot).  Scratch:

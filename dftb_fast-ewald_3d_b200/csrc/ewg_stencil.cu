@@ -60,14 +60,16 @@ __device__ __forceinline__ int slot_count(int packed) { return packed >> 16; }
 // Tiled window weights, one thread per (atom, axis).
 // ---------------------------------------------------------------------------
 template <typename R>
-__global__ void k_weights_tiled(const int4* __restrict__ mc, const double4* __restrict__ fr, int n,
-                                StencilDims sd, R* __restrict__ wtab, R* __restrict__ qk,
+__global__ void k_weights_tiled(const int4* __restrict__ mc, const double4* __restrict__ fr,
+                                const int* __restrict__ perm, int n, StencilDims sd,
+                                R* __restrict__ wtab, R* __restrict__ qk,
                                 int4* __restrict__ slot) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= 3 * n) return;
   const int k = idx / 3, d = idx - 3 * k;
-  const int4 c4 = mc[k];
-  const double4 f4 = fr[k];
+  const int i = perm[k];
+  const int4 c4 = mc[i];
+  const double4 f4 = fr[i];
   const int c = d == 0 ? c4.x : (d == 1 ? c4.y : c4.z);
   const double frac = d == 0 ? f4.x : (d == 1 ? f4.y : f4.z);
   const int nd = sd.n[d], T = sd.T[d], nt = sd.ntiles[d], S = sd.S[d];
@@ -300,6 +302,9 @@ __device__ __forceinline__ void dmma_m8n8k4(double& c0, double& c1, double a, do
 constexpr int kGatherWarps = 4;   // FP64 gather: warps per tile
 constexpr int kGatherMB = 2;      // FP64 gather: M blocks of 8 atoms per warp and round
 constexpr int kGatherAdWarps = 2;  // FP64 gather with window derivatives: warps per tile
+// FP32 gather with window derivatives: one atom per lane (74 registers, so
+// about 13 CTAs per SM) and two warps per tile.
+constexpr int kGatherAdF32Atoms = 1, kGatherAdF32Warps = 2;
 constexpr int kSpreadAtoms = 64;  // atoms staged per round, one per thread
 constexpr int kWRow = 12;         // doubles per staged weight row: 8 used; the
                                   // padding makes the fragment reads conflict-free
@@ -1015,15 +1020,15 @@ inline int blocks_for(long n, int threads) { return static_cast<int>((n + thread
 
 }  // namespace
 
-void launch_weights(const MeshPlan& mp, const int4* mc, const double4* fr, int n, void* wtab,
-                    void* qk, int4* slot, cudaStream_t st) {
+void launch_weights(const MeshPlan& mp, const int4* mc, const double4* fr, const int* perm, int n,
+                    void* wtab, void* qk, int4* slot, cudaStream_t st) {
   if (n == 0) return;
   if (mp.mixed)
     k_weights_tiled<float><<<blocks_for(3L * n, 128), 128, 0, st>>>(
-        mc, fr, n, mp.sd, static_cast<float*>(wtab), static_cast<float*>(qk), slot);
+        mc, fr, perm, n, mp.sd, static_cast<float*>(wtab), static_cast<float*>(qk), slot);
   else
     k_weights_tiled<double><<<blocks_for(3L * n, 128), 128, 0, st>>>(
-        mc, fr, n, mp.sd, static_cast<double*>(wtab), static_cast<double*>(qk), slot);
+        mc, fr, perm, n, mp.sd, static_cast<double*>(wtab), static_cast<double*>(qk), slot);
   ++g_launches;
 }
 
@@ -1072,8 +1077,8 @@ void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs,
                                                    mp.sd, static_cast<const R*>(grid), part)
   if (mp.sd.ad && nc == 1) {  // force wanted, ad scheme: potential grid, four partials
     if (mp.mixed)
-      k_gather_tiles_ad<GatherShape<float>::atoms, GatherShape<float>::warps>
-          <<<grd, 32 * GatherShape<float>::warps, 0, st>>>(
+      k_gather_tiles_ad<kGatherAdF32Atoms, kGatherAdF32Warps>
+          <<<grd, 32 * kGatherAdF32Warps, 0, st>>>(
               tile_start, pairs, static_cast<const float*>(wtab), mp.sd,
               static_cast<const float*>(grid), part);
     else
