@@ -126,6 +126,12 @@ struct ewg_context {
     graphs.clear();
     graph_seen.clear();
   }
+  // Batched calls: cells are spread over `batch_lanes` lanes, each a context
+  // of its own (buffers, streams), so that independent cells run concurrently.
+  int batch_lanes = 4;
+  std::vector<ewg_context*> lanes;
+  cudaEvent_t lanes_ready = nullptr;
+  std::vector<cudaEvent_t> lane_done;
   // Autotuner results per (atoms, precision, scheme, lattice, target).
   struct TuneEntry {
     ewg_overrides ov;
@@ -149,6 +155,9 @@ struct ewg_context {
     }
     for (auto& kv : corrs) cudaFree(kv.second.dev);
     drop_graphs();
+    for (ewg_context* l : lanes) delete l;
+    if (lanes_ready) cudaEventDestroy(lanes_ready);
+    for (cudaEvent_t e : lane_done) cudaEventDestroy(e);
     for (auto& e : prof.ev)
       if (e) cudaEventDestroy(e);
     if (fork) cudaEventDestroy(fork);
@@ -505,7 +514,7 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
       g_launches += hit->second.launches;
     } else if (c->graph_seen.count(key)) {
       // Second sighting: record the sequence once, then replay it from now on.
-      if (c->graphs.size() >= 64) c->drop_graphs();
+      if (c->graphs.size() >= 512) c->drop_graphs();
       cudaGraph_t graph = nullptr;
       cudaGraphExec_t exec = nullptr;
       const long long before = g_launches;
@@ -1579,9 +1588,23 @@ int ewg_last_stress_setup(const ewg_context* c, double* alpha, double* max_r, do
 
 // ---- batched form ----------------------------------------------------------
 
+int ewg_set_batch_lanes(ewg_context* c, int lanes) {
+  if (!c || lanes < 1 || lanes > 16) return EWG_ERR_ARG;
+  c->batch_lanes = lanes;
+  return EWG_OK;
+}
+
 int ewg_batch_potential_force(ewg_context* c, int n_cells, const int* offsets, const double* coords,
                               const double* charges, const double* lat_rows, double tol,
                               double* pot, double* force, int* cell_status) {
+  return ewg_batch_potential_force_ov(c, n_cells, offsets, coords, charges, lat_rows, tol, pot,
+                                      force, cell_status, nullptr);
+}
+
+int ewg_batch_potential_force_ov(ewg_context* c, int n_cells, const int* offsets,
+                                 const double* coords, const double* charges,
+                                 const double* lat_rows, double tol, double* pot, double* force,
+                                 int* cell_status, const ewg_overrides* ov) {
   if (!c || n_cells < 0 || !offsets || !coords || !charges || !lat_rows || !pot) return EWG_ERR_ARG;
   LaunchScope scope(c);
   c->uploaded_charges = -1;
@@ -1594,14 +1617,41 @@ int ewg_batch_potential_force(ewg_context* c, int n_cells, const int* offsets, c
   double* dpot = dbuf<double>(c, B_POT, std::max(total, 1), &rc);
   double* dforce = dbuf<double>(c, B_FORCE, 3 * static_cast<size_t>(std::max(total, 1)), &rc);
   // One coincident-charge flag per cell, read once at the end: the cells'
-  // evaluations are queued back to back on the stream with no host wait.
+  // evaluations are queued with no host wait.
   int* cellerr = dbuf<int>(c, B_CELLERR, std::max(n_cells, 1), &rc);
   if (rc) return rc;
+  // The lanes: the context itself when one lane is asked for (or profiling is
+  // on, which times stages on the context's own stream), else sub-contexts of
+  // the same device, form and settings, each with its own buffers and streams.
+  const int nl = c->prof.on ? 1 : std::min(c->batch_lanes, std::max(n_cells, 1));
+  if (nl > 1) {
+    while (static_cast<int>(c->lanes.size()) < nl) {
+      ewg_context* l = nullptr;
+      if ((rc = ewg_create(&l, c->device, c->precision))) return rc;
+      c->lanes.push_back(l);
+      cudaEvent_t e;
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return EWG_ERR_CUDA;
+      c->lane_done.push_back(e);
+    }
+    if (!c->lanes_ready &&
+        cudaEventCreateWithFlags(&c->lanes_ready, cudaEventDisableTiming) != cudaSuccess)
+      return EWG_ERR_CUDA;
+    for (int l = 0; l < nl; ++l) {
+      c->lanes[l]->force_scheme = c->force_scheme;
+      c->lanes[l]->background = c->background;
+      c->lanes[l]->graphs_on = c->graphs_on;
+    }
+  }
   cudaMemsetAsync(cellerr, 0, sizeof(int) * std::max(n_cells, 1), c->stream);
   cudaMemcpyAsync(dcoords, coords, sizeof(double) * 3 * total, cudaMemcpyHostToDevice, c->stream);
   cudaMemcpyAsync(dq, charges, sizeof(double) * total, cudaMemcpyHostToDevice, c->stream);
+  if (nl > 1) {
+    cudaEventRecord(c->lanes_ready, c->stream);
+    for (int l = 0; l < nl; ++l) cudaStreamWaitEvent(c->lanes[l]->stream, c->lanes_ready, 0);
+  }
   std::vector<int> status(n_cells, EWG_OK);
   for (int cidx = 0; cidx < n_cells; ++cidx) {
+    ewg_context* lc = nl > 1 ? c->lanes[cidx % nl] : c;
     const int a0 = offsets[cidx], na = offsets[cidx + 1] - a0;
     Cell cell;
     double q2 = 0.0;
@@ -1609,12 +1659,18 @@ int ewg_batch_potential_force(ewg_context* c, int n_cells, const int* offsets, c
     if (!s) s = cell_from_rows(lat_rows + 9 * static_cast<size_t>(cidx), cell);
     if (!s && !(tol > 0.0 && tol < 1.0)) s = EWG_ERR_TOL;
     ewg_params p;
-    if (!s) s = choose_parameters(cell, q2, na, tol, nullptr, p);
+    if (!s) s = choose_parameters(cell, q2, na, tol, ov, p);
     if (!s)
-      s = evaluate(c, na, dcoords + 3 * static_cast<size_t>(a0), 3, 1, dq + a0, cell, p,
+      s = evaluate(lc, na, dcoords + 3 * static_cast<size_t>(a0), 3, 1, dq + a0, cell, p,
                    force != nullptr, dpot + a0, dforce + 3 * static_cast<size_t>(a0), false,
                    cellerr + cidx);
     status[cidx] = s;
+  }
+  if (nl > 1) {
+    for (int l = 0; l < nl; ++l) {
+      cudaEventRecord(c->lane_done[l], c->lanes[l]->stream);
+      cudaStreamWaitEvent(c->stream, c->lane_done[l], 0);
+    }
   }
   std::vector<int> herr(std::max(n_cells, 1), 0);
   cudaError_t e = cudaMemcpyAsync(pot, dpot, sizeof(double) * total, cudaMemcpyDeviceToHost, c->stream);

@@ -408,17 +408,17 @@ __device__ __forceinline__ void for_each_candidate(const float4* __restrict__ x3
 // Flat scan (RealGeom::flat).  The neighbourhood's rows (dy, dz) are laid out
 // one per lane; each row is one or two contiguous runs of boxes (two when it
 // wraps around the cell in x).  The non-empty runs go to a per-warp table in
-// row order -- sorted index of the first atom, offset in the concatenated
-// candidate list, the run's x_i - S lat in FP32 and its shift S -- and the warp
+// row order -- offset in the concatenated candidate list, sorted index of the
+// first atom less that offset, the shift S and the run's x_i - S lat in FP32 --
+// and the warp
 // then walks the concatenated list 32 candidates at a time, so that a warp
 // iteration is filled across run ends.  Candidate order (and with it the
 // summation order) is the same as the row-by-row scan's.
 constexpr int kRuns = 64;
 struct RunTable {
-  int j0[kRuns];
   int start[kRuns + 1];  // offset of each run in the concatenated list; start[nrun] = total
-  int shift[kRuns];      // (sx + 512) | (sy + 512) << 10 | (sz + 512) << 20
-  float base[kRuns][3];  // x_i - S lat
+  int4 info[kRuns];      // (j0 - start, sx, sy, sz): candidate v of run r is atom v + info.x
+  float4 base[kRuns];    // x_i - S lat (w unused)
 };
 
 template <class Visit>
@@ -470,13 +470,14 @@ __device__ __forceinline__ void for_each_candidate_flat(const float4* __restrict
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
     if (cnt[h] > 0) {
-      t.j0[pos] = j0[h];
+      t.info[pos] = make_int4(j0[h], sx[h], sy, sz);  // .x becomes j0 - start below
       t.start[pos] = cnt[h];  // counts for now; turned into offsets below
-      t.shift[pos] = (sx[h] + 512) | ((sy + 512) << 10) | ((sz + 512) << 20);
+      float b3[3];
 #pragma unroll
       for (int d = 0; d < 3; ++d)
-        t.base[pos][d] = static_cast<float>(
+        b3[d] = static_cast<float>(
             xi[d] - (sx[h] * g.lat[0][d] + sy * g.lat[1][d] + sz * g.lat[2][d]));
+      t.base[pos] = make_float4(b3[0], b3[1], b3[2], 0.0f);
       ++pos;
     }
   }
@@ -495,8 +496,14 @@ __device__ __forceinline__ void for_each_candidate_flat(const float4* __restrict
   const int half = __shfl_sync(0xffffffffu, s0, 31);
   const int total = half + __shfl_sync(0xffffffffu, s1, 31);
   __syncwarp();
-  if (lane < nrun) t.start[lane] = s0 - c0;
-  if (lane + 32 < nrun) t.start[lane + 32] = half + s1 - c1;
+  if (lane < nrun) {
+    t.start[lane] = s0 - c0;
+    t.info[lane].x -= s0 - c0;
+  }
+  if (lane + 32 < nrun) {
+    t.start[lane + 32] = half + s1 - c1;
+    t.info[lane + 32].x -= half + s1 - c1;
+  }
   if (lane == 0) t.start[nrun] = total;
   __syncwarp();
   int rc = 0;  // the run holding the iteration's first candidate
@@ -510,15 +517,16 @@ __device__ __forceinline__ void for_each_candidate_flat(const float4* __restrict
     if (v < total) {
       int r = rc;
       while (t.start[r + 1] <= v) ++r;
-      c.j = t.j0[r] + (v - t.start[r]);
-      const int sh = t.shift[r];
-      c.sx = (sh & 0x3ff) - 512;
-      c.sy = ((sh >> 10) & 0x3ff) - 512;
-      c.sz = (sh >> 20) - 512;
-      c.valid = !(c.sx == 0 && c.sy == 0 && c.sz == 0 && c.j == k);
+      const int4 e = t.info[r];
+      c.j = v + e.x;
+      c.sx = e.y;
+      c.sy = e.z;
+      c.sz = e.w;
+      c.valid = !((e.y | e.z | e.w) == 0 && c.j == k);
       if (c.valid) {
         const float4 xj = x32[c.j];
-        const float d0 = t.base[r][0] - xj.x, d1 = t.base[r][1] - xj.y, d2 = t.base[r][2] - xj.z;
+        const float4 bs = t.base[r];
+        const float d0 = bs.x - xj.x, d1 = bs.y - xj.y, d2 = bs.z - xj.z;
         c.r2 = fmaf(d0, d0, fmaf(d1, d1, d2 * d2));
       }
     }

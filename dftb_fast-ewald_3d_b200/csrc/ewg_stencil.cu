@@ -15,10 +15,10 @@
 // counting sort whose buckets are ordered by atom index, so each tile owns an
 // exact, deterministic list of the atoms that reach it.
 //
-// Spread: a CTA owns a tile; each thread owns an x-pencil of 8 points in
-// registers and adds q w1 w2 w3 atom by atom in list order, then writes it
-// once (no atomics, no zeroing, fixed order).  FP64 runs on the tensor cores;
-// FP32 sums groups of 8 atoms in FP32 and the group sums in FP64.
+// Spread: a CTA owns a tile.  FP64 runs on the tensor cores.  FP32: each lane
+// owns two x-pencils of 8 points in registers and adds q w1 w2 w3 atom by atom
+// in list order (groups of 8 atoms in FP32, the group sums in FP64), then
+// writes them once (no atomics, no zeroing, fixed order).
 // Gather: a CTA of one (FP64) or two (FP32) warps stages its tile in shared
 // memory; each warp takes 64 atoms of the tile's list at a time, two per lane,
 // and walks the tile's 512 points in lockstep so every grid value is a
@@ -38,7 +38,7 @@ namespace ewg {
 namespace {
 
 constexpr int TX = kTileX, TY = kTileY, TZ = kTileZ;
-constexpr int kPencils = TY * TZ;  // spread: one thread per x-pencil
+constexpr int kSpreadLanes = TY * TZ / 2;  // FP32 spread: one warp, two x-pencils per lane
 constexpr int kSpreadChunk = 64;   // atoms whose weights are staged at once
 constexpr int kSpreadGroup = 8;    // FP32 spread: atoms summed in FP32 before the FP64 add
 // Gather: atoms per lane and warps sharing one staged tile, per precision.
@@ -57,22 +57,27 @@ __device__ __forceinline__ int slot_first(int packed) { return packed & 0xffff; 
 __device__ __forceinline__ int slot_count(int packed) { return packed >> 16; }
 
 // ---------------------------------------------------------------------------
-// Tiled window weights, one thread per (atom, axis).
+// Tiled window weights, one thread per (atom, axis, tile slot): eight points
+// each, so an atom's S_x + S_y + S_z rows are computed in parallel.
 // ---------------------------------------------------------------------------
 template <typename R>
 __global__ void k_weights_tiled(const int4* __restrict__ mc, const double4* __restrict__ fr,
                                 const int* __restrict__ perm, int n, StencilDims sd,
                                 R* __restrict__ wtab, R* __restrict__ qk,
                                 int4* __restrict__ slot) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= 3 * n) return;
-  const int k = idx / 3, d = idx - 3 * k;
+  const int SS = sd.S[0] + sd.S[1] + sd.S[2];
+  const long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= static_cast<long>(SS) * n) return;
+  const int k = static_cast<int>(idx / SS);
+  int r = static_cast<int>(idx - static_cast<long>(k) * SS);
+  const int d = r < sd.S[0] ? 0 : (r < sd.S[0] + sd.S[1] ? 1 : 2);
+  const int s = r - (d == 0 ? 0 : (d == 1 ? sd.S[0] : sd.S[0] + sd.S[1]));
   const int i = perm[k];
   const int4 c4 = mc[i];
   const double4 f4 = fr[i];
   const int c = d == 0 ? c4.x : (d == 1 ? c4.y : c4.z);
   const double frac = d == 0 ? f4.x : (d == 1 ? f4.y : f4.z);
-  const int nd = sd.n[d], T = sd.T[d], nt = sd.ntiles[d], S = sd.S[d];
+  const int nd = sd.n[d], T = sd.T[d], nt = sd.ntiles[d];
   const int m = sd.m;
   // Tiles the stencil [c - m, c + m] (mod n) runs through, starting at `first`;
   // a stencil that comes back into its first tile, or covers the whole axis,
@@ -94,31 +99,39 @@ __global__ void k_weights_tiled(const int4* __restrict__ mc, const double4* __re
     }
     count = min(count, nt);
   }
-  R* out = wtab + static_cast<size_t>(k) * sd.wstride + sd.woff[d];
+  R* out = wtab + static_cast<size_t>(k) * sd.wstride + sd.woff[d] + s * T;
   // Window derivative with respect to the atom's fractional coordinate s_d:
   // the point sits at u = o - frac grid units from the atom, and
   // d/ds_d [pref exp(-u^2 / b)] = n_d (2 u / b) pref exp(-u^2 / b).
   const double dscale = -2.0 * static_cast<double>(nd) / sd.b;
-  for (int s = 0; s < S; ++s) {
-    const int origin = ((first + s) % nt) * T;
-    for (int p = 0; p < T; ++p) {
-      const int P = origin + p;
-      double w = 0.0, dw = 0.0;
-      if (s < count && P < nd) {
-        int o = pmod(P - c, nd);  // largest offset <= m congruent to P - c
-        while (o > m) o -= nd;
-        while (o + nd <= m) o += nd;
-        for (; o >= -m; o -= nd) {
-          const double dd = frac - static_cast<double>(o);
-          const double e = sd.pref * exp(-(dd * dd) / sd.b);
-          w += e;
-          dw += dscale * dd * e;
-        }
+  const int origin = ((first + s) % nt) * T;
+  R wv[TX], dv[TX];
+  static_assert(TX == TY && TY == TZ, "one row length for all axes");
+#pragma unroll
+  for (int p = 0; p < TX; ++p) {
+    const int P = origin + p;
+    double w = 0.0, dw = 0.0;
+    if (s < count && P < nd) {
+      int o = pmod(P - c, nd);  // largest offset <= m congruent to P - c
+      while (o > m) o -= nd;
+      while (o + nd <= m) o += nd;
+      for (; o >= -m; o -= nd) {
+        const double dd = frac - static_cast<double>(o);
+        const double e = sd.pref * exp(-(dd * dd) / sd.b);
+        w += e;
+        dw += dscale * dd * e;
       }
-      out[s * T + p] = static_cast<R>(w);
-      if (sd.ad) out[sd.dwoff + s * T + p] = static_cast<R>(dw);
     }
+    wv[p] = static_cast<R>(w);
+    dv[p] = static_cast<R>(dw);
   }
+#pragma unroll
+  for (int p = 0; p < TX; ++p) out[p] = wv[p];
+  if (sd.ad) {
+#pragma unroll
+    for (int p = 0; p < TX; ++p) out[sd.dwoff + p] = dv[p];
+  }
+  if (s != 0) return;  // the axis' first slot thread writes the slot record
   int* sp = reinterpret_cast<int*>(&slot[k]);
   sp[d] = first | (count << 16);
   if (d == 0) {
@@ -217,30 +230,32 @@ __device__ __forceinline__ void load8(const float* __restrict__ p, float* out) {
 // ---------------------------------------------------------------------------
 // Spread
 // ---------------------------------------------------------------------------
+// FP32 form: one warp per tile; each lane owns two x-pencils, (py, pz) and
+// (py + 4, pz), so every pair of shared-memory reads of an atom's x weights
+// feeds 16 multiply-adds.
 template <typename R>
-__global__ void __launch_bounds__(kPencils) k_spread_tiles(const int* __restrict__ tile_start,
-                                                           const int2* __restrict__ pairs,
-                                                           const R* __restrict__ wtab,
-                                                           const R* __restrict__ qk, StencilDims sd,
-                                                           R* __restrict__ grid) {
+__global__ void __launch_bounds__(kSpreadLanes) k_spread_tiles(const int* __restrict__ tile_start,
+                                                               const int2* __restrict__ pairs,
+                                                               const R* __restrict__ wtab,
+                                                               const R* __restrict__ qk,
+                                                               StencilDims sd, R* __restrict__ grid) {
   __shared__ R sW1[kSpreadChunk][TX];
   __shared__ R sW2[kSpreadChunk][TY];
   __shared__ R sW3[kSpreadChunk][TZ];
   const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
   const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
   const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
-  const int py = threadIdx.x % TY, pz = threadIdx.x / TY;
-  double acc[TX];
+  const int py = threadIdx.x % (TY / 2), pz = threadIdx.x / (TY / 2);
+  double acc[2][TX];
 #pragma unroll
-  for (int x = 0; x < TX; ++x) acc[x] = 0.0;
+  for (int x = 0; x < TX; ++x) acc[0][x] = acc[1][x] = 0.0;
   const int p0 = tile_start[tile], p1 = tile_start[tile + 1];
   for (int b0 = p0; b0 < p1; b0 += kSpreadChunk) {
     const int nb = min(kSpreadChunk, p1 - b0);
     __syncthreads();  // the previous chunk's weights are no longer read
-    // One thread per atom of the chunk: its pair, charge and the 3 x 8 weights
-    // for this tile, loaded in one round of independent vector loads.
-    if (threadIdx.x < nb) {
-      const int a = threadIdx.x;
+    // Each lane stages whole atoms of the chunk: its pair, charge and the
+    // 3 x 8 weights for this tile, in independent vector loads.
+    for (int a = threadIdx.x; a < nb; a += kSpreadLanes) {
       const int2 pr = pairs[b0 + a];
       const R* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
       R t1[TX], t2[TY], t3[TZ];
@@ -262,24 +277,36 @@ __global__ void __launch_bounds__(kPencils) k_spread_tiles(const int* __restrict
     // multiply-adds, bounded the FP32 form).
     for (int g0 = 0; g0 < nb; g0 += kSpreadGroup) {
       const int g1 = min(g0 + kSpreadGroup, nb);
-      R part[TX];
+      R part[2][TX];
 #pragma unroll
-      for (int x = 0; x < TX; ++x) part[x] = R(0);
+      for (int x = 0; x < TX; ++x) part[0][x] = part[1][x] = R(0);
       for (int a = g0; a < g1; ++a) {
-        const R s = sW2[a][py] * sW3[a][pz];
+        const R w3 = sW3[a][pz];
+        const R s0 = sW2[a][py] * w3, s1 = sW2[a][py + TY / 2] * w3;
 #pragma unroll
-        for (int x = 0; x < TX; ++x) part[x] = fma(s, sW1[a][x], part[x]);
+        for (int x = 0; x < TX; ++x) {
+          const R w1 = sW1[a][x];
+          part[0][x] = fma(s0, w1, part[0][x]);
+          part[1][x] = fma(s1, w1, part[1][x]);
+        }
       }
 #pragma unroll
-      for (int x = 0; x < TX; ++x) acc[x] += static_cast<double>(part[x]);
+      for (int x = 0; x < TX; ++x) {
+        acc[0][x] += static_cast<double>(part[0][x]);
+        acc[1][x] += static_cast<double>(part[1][x]);
+      }
     }
   }
   const int ex = min(TX, sd.n[0] - x0), ey = min(TY, sd.n[1] - y0), ez = min(TZ, sd.n[2] - z0);
-  if (py < ey && pz < ez) {
-    R* row = grid + (static_cast<size_t>(z0 + pz) * sd.n[1] + y0 + py) * sd.n[0] + x0;
 #pragma unroll
-    for (int x = 0; x < TX; ++x)
-      if (x < ex) row[x] = static_cast<R>(acc[x]);
+  for (int h = 0; h < 2; ++h) {
+    const int y = py + h * (TY / 2);
+    if (y < ey && pz < ez) {
+      R* row = grid + (static_cast<size_t>(z0 + pz) * sd.n[1] + y0 + y) * sd.n[0] + x0;
+#pragma unroll
+      for (int x = 0; x < TX; ++x)
+        if (x < ex) row[x] = static_cast<R>(acc[h][x]);
+    }
   }
 }
 
@@ -946,42 +973,48 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma_ad(
 
 // Final per-atom sum of the slot partials in a fixed order, with the assembly
 // of fft/ewald_fft_3d.f90:121-132: pot = (sr + lr) + self, force = sr + q lr.
-// One warp per atom: lanes read the atom's slots (contiguous, coalesced), then
-// a shuffle tree sums them (a fixed order: results are reproducible).
+// A group of lanes per atom (a warp, or 8 lanes when the atom has at most 32
+// slots) reads the atom's slots (contiguous, coalesced), then a shuffle tree
+// sums them (a fixed order: results are reproducible).
 // Dual basis rows for the ad partials (on = 0: ik partials, Cartesian already).
 struct RecRows {
   double b[3][3];
   int on;
 };
 
-template <int NC>
+// LPA lanes per atom (32, or 8 when an atom has at most 32 slots: four atoms
+// per warp).
+template <int NC, int LPA>
 __global__ void k_gather_final(const int4* __restrict__ slot, const int* __restrict__ perm,
                                const double* __restrict__ part, int n, StencilDims sd,
                                const double* __restrict__ q, double self_coef, double pot_shift,
                                const double* __restrict__ pot_sr, const double* __restrict__ f_sr,
                                double* __restrict__ pot, double* __restrict__ force, RecRows rr) {
-  const int k = static_cast<int>((static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (k >= n) return;
-  const int4 si = slot[k];
+  const long t = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int k = static_cast<int>(t / LPA);
+  const int lane = static_cast<int>(t % LPA);
+  // Lanes past the last atom stay to the end: the shuffles below take the whole warp.
+  const bool live = k < n;
+  const int4 si = live ? slot[k] : make_int4(0, 0, 0, 0);
   const int cx = slot_count(si.x), cy = slot_count(si.y), cz = slot_count(si.z);
   const int nslots = sd.S[0] * sd.S[1] * sd.S[2];
-  const double* pk = part + static_cast<size_t>(k) * nslots * NC;
+  const double* pk = part + static_cast<size_t>(live ? k : 0) * nslots * NC;
   double acc[NC];
 #pragma unroll
   for (int c = 0; c < NC; ++c) acc[c] = 0.0;
-  for (int s = lane; s < nslots; s += 32) {
+  for (int s = lane; s < (live ? nslots : 0); s += LPA) {
     const int sx = s % sd.S[0], sy = (s / sd.S[0]) % sd.S[1], sz = s / (sd.S[0] * sd.S[1]);
     if (sx < cx && sy < cy && sz < cz) {  // slots past the atom's tiles hold no partial
 #pragma unroll
       for (int c = 0; c < NC; ++c) acc[c] += pk[s * NC + c];
     }
   }
+  // A fixed shuffle tree within the atom's LPA lanes.
 #pragma unroll
   for (int c = 0; c < NC; ++c)
 #pragma unroll
-    for (int off = 16; off > 0; off >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
-  if (lane != 0) return;
+    for (int off = LPA / 2; off > 0; off >>= 1) acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
+  if (lane != 0 || !live) return;
   const int i = perm[k];
   const double qi = q[i];
   pot[i] = (pot_sr[i] + acc[0]) + self_coef * qi + pot_shift;
@@ -1023,11 +1056,12 @@ inline int blocks_for(long n, int threads) { return static_cast<int>((n + thread
 void launch_weights(const MeshPlan& mp, const int4* mc, const double4* fr, const int* perm, int n,
                     void* wtab, void* qk, int4* slot, cudaStream_t st) {
   if (n == 0) return;
+  const long threads = static_cast<long>(mp.sd.S[0] + mp.sd.S[1] + mp.sd.S[2]) * n;
   if (mp.mixed)
-    k_weights_tiled<float><<<blocks_for(3L * n, 128), 128, 0, st>>>(
+    k_weights_tiled<float><<<blocks_for(threads, 128), 128, 0, st>>>(
         mc, fr, perm, n, mp.sd, static_cast<float*>(wtab), static_cast<float*>(qk), slot);
   else
-    k_weights_tiled<double><<<blocks_for(3L * n, 128), 128, 0, st>>>(
+    k_weights_tiled<double><<<blocks_for(threads, 128), 128, 0, st>>>(
         mc, fr, perm, n, mp.sd, static_cast<double*>(wtab), static_cast<double*>(qk), slot);
   ++g_launches;
 }
@@ -1057,7 +1091,7 @@ void launch_spread(const MeshPlan& mp, const int* tile_start, const int2* pairs,
                    const void* qk, void* grid, cudaStream_t st) {
   dim3 grd(mp.sd.ntiles[0], mp.sd.ntiles[1], mp.sd.ntiles[2]);
   if (mp.mixed)
-    k_spread_tiles<float><<<grd, kPencils, 0, st>>>(tile_start, pairs,
+    k_spread_tiles<float><<<grd, kSpreadLanes, 0, st>>>(tile_start, pairs,
                                                      static_cast<const float*>(wtab),
                                                      static_cast<const float*>(qk), mp.sd,
                                                      static_cast<float*>(grid));
@@ -1117,12 +1151,22 @@ void launch_gather_final(const MeshPlan& mp, const int4* slot, const int* perm, 
     for (int i = 0; i < 3; ++i)
       for (int d = 0; d < 3; ++d) rr.b[i][d] = rec[i][d];
   }
-  if (nparts == 4)
-    k_gather_final<4><<<blocks_for(32L * n, 256), 256, 0, st>>>(
-        slot, perm, part, n, mp.sd, q, self_coef, pot_shift, pot_sr, f_sr, pot, force, rr);
-  else
-    k_gather_final<1><<<blocks_for(32L * n, 256), 256, 0, st>>>(
-        slot, perm, part, n, mp.sd, q, self_coef, pot_shift, pot_sr, f_sr, pot, nullptr, rr);
+  const bool narrow = mp.sd.S[0] * mp.sd.S[1] * mp.sd.S[2] <= 32;
+  if (nparts == 4) {
+    if (narrow)
+      k_gather_final<4, 8><<<blocks_for(8L * n, 256), 256, 0, st>>>(
+          slot, perm, part, n, mp.sd, q, self_coef, pot_shift, pot_sr, f_sr, pot, force, rr);
+    else
+      k_gather_final<4, 32><<<blocks_for(32L * n, 256), 256, 0, st>>>(
+          slot, perm, part, n, mp.sd, q, self_coef, pot_shift, pot_sr, f_sr, pot, force, rr);
+  } else {
+    if (narrow)
+      k_gather_final<1, 8><<<blocks_for(8L * n, 256), 256, 0, st>>>(
+          slot, perm, part, n, mp.sd, q, self_coef, pot_shift, pot_sr, f_sr, pot, nullptr, rr);
+    else
+      k_gather_final<1, 32><<<blocks_for(32L * n, 256), 256, 0, st>>>(
+          slot, perm, part, n, mp.sd, q, self_coef, pot_shift, pot_sr, f_sr, pot, nullptr, rr);
+  }
   ++g_launches;
 }
 

@@ -53,7 +53,8 @@ EXPORTED = [
     "ewg_stage_name", "ewg_stage_times", "ewg_reset_stage_times", "ewg_set_stream",
     "ewg_direct_potential_force_static", "ewg_fp64_mma_peak", "ewg_potential_force_stress",
     "ewg_stress_fast", "ewg_potential_at", "ewg_potential_gradient_at", "ewg_external_pot_grad",
-    "ewg_xlbomd_gradients", "ewg_set_background", "ewg_set_force_scheme", "ewg_tune", "ewg_set_graphs",
+    "ewg_xlbomd_gradients", "ewg_set_background", "ewg_set_force_scheme", "ewg_tune", "ewg_set_graphs", "ewg_set_batch_lanes",
+    "ewg_batch_potential_force_ov",
 ]
 
 
@@ -147,6 +148,9 @@ def lib():
                                         C.c_double, C.c_double, dp, dp]
     L.ewg_last_stress_setup.argtypes = [vp, dp, dp, dp, ip]
     L.ewg_batch_potential_force.argtypes = [vp, C.c_int, ip, dp, dp, dp, C.c_double, dp, dp, ip]
+    L.ewg_batch_potential_force_ov.argtypes = [vp, C.c_int, ip, dp, dp, dp, C.c_double, dp, dp, ip,
+                                               C.POINTER(Overrides)]
+    L.ewg_set_batch_lanes.argtypes = [vp, C.c_int]
     L.ewg_set_profiling.argtypes = [vp, C.c_int]
     L.ewg_stage_count.argtypes = []
     L.ewg_stage_name.argtypes = [C.c_int]
@@ -328,8 +332,13 @@ class Context:
                                                 _dp(pot), _dp(force) if want_force else None, *opt))
         return (pot, force) if want_force else pot
 
-    def batch_potential_force(self, cells, tol=1e-10, want_force=True):
-        """cells: list of (positions (N_c,3), charges, lat_rows).  Returns lists."""
+    def set_batch_lanes(self, lanes: int):
+        """Concurrent lanes of batched calls (1..16, default 4)."""
+        _check(lib().ewg_set_batch_lanes(self._h, int(lanes)))
+
+    def batch_potential_force(self, cells, tol=1e-10, want_force=True, **ov):
+        """cells: list of (positions (N_c,3), charges, lat_rows).  Returns lists.
+        Keyword overrides (alpha_in, ...) apply to every cell."""
         offsets = np.zeros(len(cells) + 1, dtype=np.int32)
         for i, (p, q, _) in enumerate(cells):
             offsets[i + 1] = offsets[i] + len(q)
@@ -341,10 +350,11 @@ class Context:
         pot = np.empty(total)
         force = np.empty((total, 3)) if want_force else None
         status = np.zeros(len(cells), dtype=np.int32)
-        rc = lib().ewg_batch_potential_force(
+        o = _overrides(**ov)
+        rc = lib().ewg_batch_potential_force_ov(
             self._h, len(cells), offsets.ctypes.data_as(C.POINTER(C.c_int)), _dp(coords), _dp(charges),
             _dp(lat), float(tol), _dp(pot), _dp(force) if want_force else None,
-            status.ctypes.data_as(C.POINTER(C.c_int)))
+            status.ctypes.data_as(C.POINTER(C.c_int)), C.byref(o))
         _check(rc)
         pots = [pot[offsets[i]:offsets[i + 1]] for i in range(len(cells))]
         forces = [force[offsets[i]:offsets[i + 1]] for i in range(len(cells))] if want_force else None
