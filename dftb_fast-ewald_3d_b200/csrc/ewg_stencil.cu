@@ -332,7 +332,7 @@ constexpr int kGatherAdWarps = 2;  // FP64 gather with window derivatives: warps
 // FP32 gather with window derivatives: one atom per lane (74 registers, so
 // about 13 CTAs per SM) and two warps per tile.
 constexpr int kGatherAdF32Atoms = 1, kGatherAdF32Warps = 2;
-constexpr int kSpreadAtoms = 64;  // atoms staged per round, one per thread
+constexpr int kSpreadAtoms = 32;  // FP64 spread: atoms staged per round, one per lane
 constexpr int kWRow = 12;         // doubles per staged weight row: 8 used; the
                                   // padding makes the fragment reads conflict-free
 
@@ -344,9 +344,10 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
-// Two warps per tile, each owning four z-planes; the 64 threads stage up to 64
-// atoms' weight rows with asynchronous 16-byte copies in one round.
-__global__ void __launch_bounds__(64) k_spread_tiles_dmma(const int* __restrict__ tile_start,
+// One warp per tile owning all eight z-planes, so each step's x and y weights
+// are read from shared memory once for the eight planes; the lanes stage up to
+// 32 atoms' weight rows per round with asynchronous 16-byte copies.
+__global__ void __launch_bounds__(32) k_spread_tiles_dmma(const int* __restrict__ tile_start,
                                                           const int2* __restrict__ pairs,
                                                           const double* __restrict__ wtab,
                                                           const double* __restrict__ qk,
@@ -357,16 +358,16 @@ __global__ void __launch_bounds__(64) k_spread_tiles_dmma(const int* __restrict_
   const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
   const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
   const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
-  const int lane = threadIdx.x & 31, zb = (threadIdx.x >> 5) * (TZ / 2);
+  const int lane = threadIdx.x;
   const int fr = lane >> 2, fk = lane & 3;  // fragment row (y, or x for B) and k
-  double acc[TZ / 2][2];
+  double acc[TZ][2];
 #pragma unroll
-  for (int z = 0; z < TZ / 2; ++z) acc[z][0] = acc[z][1] = 0.0;
+  for (int z = 0; z < TZ; ++z) acc[z][0] = acc[z][1] = 0.0;
   const int p0 = tile_start[tile], p1 = tile_start[tile + 1];
   for (int b0 = p0; b0 < p1; b0 += kSpreadAtoms) {
     const int nb = min(kSpreadAtoms, p1 - b0);
-    __syncthreads();  // the previous round's weights are no longer read
-    const int a = threadIdx.x;
+    __syncwarp();  // the previous round's weights are no longer read
+    const int a = lane;
     if (a < nb) {
       const int2 pr = pairs[b0 + a];
       const double* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
@@ -386,24 +387,22 @@ __global__ void __launch_bounds__(64) k_spread_tiles_dmma(const int* __restrict_
       sQ[a] = 0.0;
     }
     cp_async_wait_all();
-    __syncthreads();
+    __syncwarp();
     for (int k0 = 0; k0 < nb; k0 += 4) {
       const int aa = k0 + fk;
       const double bw = sW[0][aa][fr];            // B[k][x = fr]
       const double w2q = sW[1][aa][fr] * sQ[aa];  // A[y = fr][k] = q w2(y) w3(z)
 #pragma unroll
-      for (int z = 0; z < TZ / 2; ++z)
-        dmma_m8n8k4(acc[z][0], acc[z][1], w2q * sW[2][aa][zb + z], bw);
+      for (int z = 0; z < TZ; ++z) dmma_m8n8k4(acc[z][0], acc[z][1], w2q * sW[2][aa][z], bw);
     }
   }
   const int ex = min(TX, sd.n[0] - x0), ey = min(TY, sd.n[1] - y0), ez = min(TZ, sd.n[2] - z0);
   const int y = fr, x = 2 * fk;
   if (y < ey) {
 #pragma unroll
-    for (int z = 0; z < TZ / 2; ++z) {
-      if (zb + z >= ez) break;
-      double* row =
-          grid + (static_cast<size_t>(z0 + zb + z) * sd.n[1] + y0 + y) * sd.n[0] + x0 + x;
+    for (int z = 0; z < TZ; ++z) {
+      if (z >= ez) break;
+      double* row = grid + (static_cast<size_t>(z0 + z) * sd.n[1] + y0 + y) * sd.n[0] + x0 + x;
       if (x + 1 < ex) {
         row[0] = acc[z][0];
         row[1] = acc[z][1];
@@ -1096,7 +1095,7 @@ void launch_spread(const MeshPlan& mp, const int* tile_start, const int2* pairs,
                                                      static_cast<const float*>(qk), mp.sd,
                                                      static_cast<float*>(grid));
   else
-    k_spread_tiles_dmma<<<grd, 64, 0, st>>>(tile_start, pairs, static_cast<const double*>(wtab),
+    k_spread_tiles_dmma<<<grd, 32, 0, st>>>(tile_start, pairs, static_cast<const double*>(wtab),
                                              static_cast<const double*>(qk), mp.sd,
                                              static_cast<double*>(grid));
   ++g_launches;
