@@ -51,9 +51,6 @@ void launch_bucket_sort(const int* key, int n, int nkeys, int* counts, int* curs
 // Exclusive scan of counts[0..nkeys) into starts[0..nkeys] (one CTA).
 void launch_scan(const int* counts, int nkeys, int* starts, cudaStream_t st);
 
-// out[k] = in[perm[k]]
-void launch_permute4(const double4* in, const int* perm, int n, double4* out, cudaStream_t st);
-void launch_permute_int4(const int4* in, const int* perm, int n, int4* out, cudaStream_t st);
 // Box-sorted atoms: out[k] = in[perm[k]] (fractional s, q) and x32[k] the
 // Cartesian position s . lat with q, in FP32, for the real-space distance test.
 void launch_permute_box(const double4* in, const int* perm, int n, const double (*lat)[3],

@@ -170,11 +170,6 @@ __global__ void k_rank(const int* __restrict__ key, int n, const int* __restrict
   perm[b + r] = i;
 }
 
-__global__ void k_permute4(const double4* __restrict__ in, const int* __restrict__ perm, int n,
-                           double4* __restrict__ out) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) out[k] = in[perm[k]];
-}
 // Box-sorted atoms: fractional coordinates and charge in FP64, and beside them
 // the Cartesian position of the wrapped atom, x = s . lat, with the charge in
 // FP32 for the real-space candidate test.
@@ -192,11 +187,6 @@ __global__ void k_permute_box(const double4* __restrict__ in, const int* __restr
   for (int d = 0; d < 3; ++d)
     c[d] = static_cast<float>(v.x * lat.a[0][d] + v.y * lat.a[1][d] + v.z * lat.a[2][d]);
   x32[k] = make_float4(c[0], c[1], c[2], static_cast<float>(v.w));
-}
-__global__ void k_permute_int4(const int4* __restrict__ in, const int* __restrict__ perm, int n,
-                               int4* __restrict__ out) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) out[k] = in[perm[k]];
 }
 
 // ---------------------------------------------------------------------------
@@ -804,12 +794,6 @@ void launch_scan(const int* counts, int nkeys, int* starts, cudaStream_t st) {
   ++g_launches;
 }
 
-void launch_permute4(const double4* in, const int* perm, int n, double4* out, cudaStream_t st) {
-  if (n == 0) return;
-  k_permute4<<<blocks_for(n, 256), 256, 0, st>>>(in, perm, n, out);
-  ++g_launches;
-}
-
 void launch_permute_box(const double4* in, const int* perm, int n, const double (*lat)[3],
                         double4* out, float4* x32, cudaStream_t st) {
   if (n == 0) return;
@@ -817,12 +801,6 @@ void launch_permute_box(const double4* in, const int* perm, int n, const double 
   for (int i = 0; i < 3; ++i)
     for (int d = 0; d < 3; ++d) L.a[i][d] = lat[i][d];
   k_permute_box<<<blocks_for(n, 256), 256, 0, st>>>(in, perm, n, L, out, x32);
-  ++g_launches;
-}
-
-void launch_permute_int4(const int4* in, const int* perm, int n, int4* out, cudaStream_t st) {
-  if (n == 0) return;
-  k_permute_int4<<<blocks_for(n, 256), 256, 0, st>>>(in, perm, n, out);
   ++g_launches;
 }
 
