@@ -22,7 +22,7 @@ constexpr int kTiles[3] = {kTileX, kTileY, kTileZ};
 // Device buffers owned by a context, grown on demand and reused across calls.
 enum BufId {
   B_POS, B_Q, B_POT, B_FORCE, B_POT_SR, B_F_SR, B_S4, B_S4S, B_BOXKEY, B_MC, B_FR,
-  B_TILEKEY, B_COUNTS, B_CURSOR, B_BOXSTART, B_TILESTART, B_TMP, B_PERMBOX, B_PERMMESH, B_WTAB,
+  B_COUNTS, B_CURSOR, B_BOXSTART, B_TMP, B_PERMBOX, B_WTAB,
   B_QK, B_GRID, B_A1, B_A2, B_B2, B_B1, B_OUT, B_ERR, B_SUMS, B_PARTIAL, B_KVEC, B_SK, B_WK,
   B_P6, B_O6, B_COORDS, B_SLOT, B_PART, B_PAIRTMP, B_PAIRS, B_PAIRSTART, B_CELLERR, B_ZPART,
   B_BCOUNTS, B_BCURSOR, B_BTMP, B_EXT_T, B_EXT_S, B_EXT_SQ, B_EXT_TQ, B_EXT_BLUR, B_EXT_R,
@@ -388,15 +388,10 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
   int* boxkey = dbuf<int>(c, B_BOXKEY, n, &rc);
   int4* mcv = dbuf<int4>(c, B_MC, n, &rc);
   double4* fr = dbuf<double4>(c, B_FR, n, &rc);
-  int* tilekey = dbuf<int>(c, B_TILEKEY, n, &rc);
-  int* counts = dbuf<int>(c, B_COUNTS, std::max(nboxes, ntiles), &rc);
-  int* cursor = dbuf<int>(c, B_CURSOR, std::max(nboxes, ntiles), &rc);
+  int* counts = dbuf<int>(c, B_COUNTS, ntiles, &rc);
+  int* cursor = dbuf<int>(c, B_CURSOR, ntiles, &rc);
   int* boxstart = dbuf<int>(c, B_BOXSTART, nboxes + 1, &rc);
-  int* tilestart = dbuf<int>(c, B_TILESTART, ntiles + 1, &rc);
-  int* tmp = dbuf<int>(c, B_TMP, n, &rc);
   int* permbox = dbuf<int>(c, B_PERMBOX, n, &rc);
-  int* permmesh = dbuf<int>(c, B_PERMMESH, n, &rc);
-  // the box sort runs on the side stream: scratch of its own
   int* bcounts = dbuf<int>(c, B_BCOUNTS, nboxes, &rc);
   int* bcursor = dbuf<int>(c, B_BCURSOR, nboxes, &rc);
   int* btmp = dbuf<int>(c, B_BTMP, n, &rc);
@@ -434,10 +429,12 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
     zpart = dbuf<double>(c, B_ZPART, nz, &rc);
     if (rc) return rc;
   }
-  // The real-space branch (box sort, permutation, erfc pair sum; FP64 pipe and
+  // One box sort orders the atoms for both sums: the real-space cell list and
+  // the mesh side (weights rows, pair lists; boxes are about one mesh tile
+  // wide).  The real-space branch (permutation, erfc pair sum; FP64 pipe and
   // issue bound) runs on the low-priority side stream beside the mesh pipeline
-  // (memory and tensor bound), forked after the atom preparation and joined
-  // before the final assembly.  With stage events on, everything runs in line.
+  // (memory and tensor bound), forked after the sort and joined before the
+  // final assembly.  With stage events on, everything runs in line.
   const bool concurrent = !c->prof.on;
   cudaStream_t rs = concurrent ? c->side : st;
   const double self_coef = -2.0 * p.alpha / std::sqrt(kPi);
@@ -447,31 +444,28 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
     if (!err_flag) cudaMemsetAsync(err, 0, sizeof(int), st);
     prof_mark(mp.prof, st, ST_PREP);
     if (!reuse) {
-      launch_atom_prep(pos, sa, sd, q, n, cell, rg.nb, mp.g.n, kTiles, mp.sd.ntiles, s4, boxkey,
-                       mcv, fr, tilekey, st);
+      launch_atom_prep(pos, sa, sd, q, n, cell, rg.nb, mp.g.n, s4, boxkey, mcv, fr, st);
+      launch_bucket_sort(boxkey, n, nboxes, bcounts, bcursor, boxstart, btmp, permbox, st);
       if (concurrent) {
         cudaEventRecord(c->fork, st);
         cudaStreamWaitEvent(rs, c->fork, 0);
       }
-      launch_bucket_sort(boxkey, n, nboxes, bcounts, bcursor, boxstart, btmp, permbox, rs);
       launch_permute_box(s4, permbox, n, cell.lat, s4s, x32s, rs);
-      launch_bucket_sort(tilekey, n, ntiles, counts, cursor, tilestart, tmp, permmesh, st);
       prof_mark(mp.prof, st, ST_WEIGHTS);
-      launch_weights(mp, mcv, fr, permmesh, n, wtab, qk, slot, st);
+      launch_weights(mp, mcv, fr, permbox, n, wtab, qk, slot, st);
       launch_pair_bins(mp, slot, n, counts, cursor, pairstart, pairtmp, pairs, npairs_max, st);
     } else {
       // Geometry unchanged: refresh only the charges in the sorted layouts.
-      launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, nullptr, nullptr, nullptr, s4, nullptr,
-                       nullptr, nullptr, nullptr, st);
+      launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, nullptr, s4, nullptr, nullptr, nullptr,
+                       st);
       if (concurrent) {
         cudaEventRecord(c->fork, st);
         cudaStreamWaitEvent(rs, c->fork, 0);
       }
       launch_permute_box(s4, permbox, n, cell.lat, s4s, x32s, rs);
-      launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, mp.g.n, kTiles, mp.sd.ntiles, nullptr,
-                       nullptr, mcv, fr, tilekey, st);
+      launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, mp.g.n, nullptr, nullptr, mcv, fr, st);
       prof_mark(mp.prof, st, ST_WEIGHTS);
-      launch_weights(mp, mcv, fr, permmesh, n, wtab, qk, slot, st);
+      launch_weights(mp, mcv, fr, permbox, n, wtab, qk, slot, st);
     }
     prof_mark(mp.prof, st, ST_REAL);
     launch_real_space(s4s, x32s, permbox, boxstart, n, rg, p.alpha, p.r_cut, mixed, pot_sr, f_sr,
@@ -489,7 +483,7 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
     prof_mark(mp.prof, st, ST_GATHER);
     launch_gather(mp, pairstart, pairs, wtab, outg, nc, part, st);
     if (concurrent) cudaStreamWaitEvent(st, c->join, 0);  // pot_sr, f_sr, err ready
-    launch_gather_final(mp, slot, permmesh, part, nparts, n, q, self_coef, pot_shift, pot_sr, f_sr,
+    launch_gather_final(mp, slot, permbox, part, nparts, n, q, self_coef, pot_shift, pot_sr, f_sr,
                         pot, want_force ? force : nullptr, ad ? cell.rec : nullptr, st);
   };
   if (c->graphs_on && concurrent) {
@@ -806,16 +800,19 @@ int ewg_device_memory(int n, const double* charges, const double* lat_rows, doub
   MeshGeom g;
   rc = mesh_geometry(cell, p, g);
   if (rc) return rc;
-  // Sizes for the precision's default force scheme (ik for FP64, ad for mixed).
+  // The larger of the two force schemes: i k keeps four transform channels,
+  // window derivatives one channel and twice the weight rows.
   const bool mixed = precision == EWG_PRECISION_MIXED;
-  const bool ad = with_force && mixed;
-  StencilDims sd;
-  stencil_dims(g, ad, sd);
-  const MeshSizes s = mesh_sizes(g, sd, mixed, with_force && !ad ? 4 : 1, n, with_force ? 4 : 1);
   const double atoms = static_cast<double>(n) * (32 * 4 + 16 * 2 + 4 * 6 + 8 * 6);
-  *bytes = static_cast<double>(s.grid + s.A1 + s.A2 + s.B2 + s.B1 + s.out + s.wtab + s.qk + s.slot +
-                               s.part) +
-           atoms;
+  double most = 0.0;
+  for (int ad = 0; ad < (with_force ? 2 : 1); ++ad) {
+    StencilDims sd;
+    stencil_dims(g, ad != 0, sd);
+    const MeshSizes s = mesh_sizes(g, sd, mixed, with_force && !ad ? 4 : 1, n, with_force ? 4 : 1);
+    most = std::max(most, static_cast<double>(s.grid + s.A1 + s.A2 + s.B2 + s.B1 + s.out + s.wtab +
+                                              s.qk + s.slot + s.part));
+  }
+  *bytes = most + atoms;
   return EWG_OK;
 }
 
@@ -1179,8 +1176,7 @@ int ewg_direct_potential_force(ewg_context* c, int n, const double* positions,
     cudaMemcpyAsync(dwk, wk.data(), sizeof(double) * nk, cudaMemcpyHostToDevice, st);
   }
   cudaMemsetAsync(err, 0, sizeof(int), st);
-  launch_atom_prep(dcoords, 3, 1, dq, n, cell, rg.nb, nullptr, nullptr, nullptr, s4, boxkey, nullptr,
-                   nullptr, nullptr, st);
+  launch_atom_prep(dcoords, 3, 1, dq, n, cell, rg.nb, nullptr, s4, boxkey, nullptr, nullptr, st);
   launch_bucket_sort(boxkey, n, nboxes, counts, cursor, boxstart, tmp, permbox, st);
   launch_permute_box(s4, permbox, n, cell.lat, s4s, x32s, st);
   launch_real_space(s4s, x32s, permbox, boxstart, n, rg, alpha, r_cut, 0, dpot, dforce, err, st);
@@ -1554,8 +1550,7 @@ int ewg_stress(ewg_context* c, double tol_ewald, double alpha, double* sigma) {
   if (ng) cudaMemcpyAsync(dk, ss.g.data(), sizeof(double) * ss.g.size(), cudaMemcpyHostToDevice, st);
   cudaMemsetAsync(err, 0, sizeof(int), st);
   c->resident.coords_version = -1;  // the sorted layout below is for max_r
-  launch_atom_prep(dcoords, 3, 1, dq, n, cell, rg.nb, nullptr, nullptr, nullptr, s4, boxkey, nullptr,
-                   nullptr, nullptr, st);
+  launch_atom_prep(dcoords, 3, 1, dq, n, cell, rg.nb, nullptr, s4, boxkey, nullptr, nullptr, st);
   launch_bucket_sort(boxkey, n, nboxes, counts, cursor, boxstart, tmp, permbox, st);
   launch_permute_box(s4, permbox, n, cell.lat, s4s, x32s, st);
   launch_real_stress(s4s, x32s, boxstart, n, rg, ss.alpha, ss.max_r, p6, o6, err, st);

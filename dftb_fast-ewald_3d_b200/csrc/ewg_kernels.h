@@ -35,12 +35,12 @@ void prof_collect(Profiler* p);
 // ---- atoms: fractional coordinates, keys, sorting (ewg_real.cu) ----------
 
 // Per atom: wrapped fractional coordinates s and charge (double4), real-space
-// box key, mesh lowest point and fraction (nfft/nfft.f90:122-159), mesh tile key.
+// box key, mesh lowest point and fraction (nfft/nfft.f90:122-159).  Null
+// outputs (and null nb / ngrid) are skipped.
 // positions: element (i, d) at pos[i * sa + d * sd].
 void launch_atom_prep(const double* pos, long sa, long sd, const double* q, int n, const Cell& cell,
-                      const int nb[3], const int ngrid[3], const int tile[3], const int ntiles[3],
-                      double4* s4, int* box_key, int4* mesh_c, double4* mesh_fr, int* tile_key,
-                      cudaStream_t st);
+                      const int nb[3], const int ngrid[3], double4* s4, int* box_key, int4* mesh_c,
+                      double4* mesh_fr, cudaStream_t st);
 
 // Stable counting sort by key: perm[k] = atom with the k-th key in (key, index)
 // order; starts[nkeys + 1] are bucket offsets.  Scratch: counts/cursor (nkeys),
@@ -123,10 +123,11 @@ struct MeshPlan {
   const double* corr2[3] = {nullptr, nullptr, nullptr};  // squared deconvolution factors, index k + H
 };
 
-// Tiled window weights per mesh-sorted atom (wtab: wstride values per atom),
-// slot origin and count per axis (slot: first | count << 16 in x, y, z), and
-// the charges in mesh order (qk).  mesh_c / mesh_fr are in atom order and are
-// read through the mesh permutation (sorted atom k is atom perm[k]).
+// Tiled window weights per sorted atom (wtab: wstride values per atom), slot
+// origin and count per axis (slot: first | count << 16 in x, y, z), and the
+// charges in sorted order (qk).  mesh_c / mesh_fr are in atom order and are
+// read through the permutation (sorted atom k is atom perm[k]; the cell-list
+// box order, which keeps neighbouring atoms close in the tables).
 void launch_weights(const MeshPlan& mp, const int4* mesh_c, const double4* mesh_fr,
                     const int* perm, int n, void* wtab, void* qk, int4* slot, cudaStream_t st);
 

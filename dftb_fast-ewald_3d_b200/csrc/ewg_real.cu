@@ -41,20 +41,17 @@ struct PrepArgs {
   double rec[3][3];
   int nb[3];
   int ng[3];
-  int tile[3];
-  int ntiles[3];
 };
 
 __global__ void k_atom_prep(const double* __restrict__ pos, long sa, long sd,
                             const double* __restrict__ q, int n, PrepArgs a,
                             double4* __restrict__ s4, int* __restrict__ box_key,
-                            int4* __restrict__ mesh_c, double4* __restrict__ mesh_fr,
-                            int* __restrict__ tile_key) {
+                            int4* __restrict__ mesh_c, double4* __restrict__ mesh_fr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double x[3] = {pos[i * sa], pos[i * sa + sd], pos[i * sa + 2 * sd]};
   double s[3];
-  int bx[3], c[3], tk[3];
+  int bx[3], c[3];
   double fr[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -67,7 +64,6 @@ __global__ void k_atom_prep(const double* __restrict__ pos, long sa, long sd,
       fr[d] = scaled - static_cast<double>(lowest);
       if (lowest >= a.ng[d]) lowest -= a.ng[d];
       c[d] = lowest;
-      tk[d] = lowest / a.tile[d];
     }
   }
   const double qi = q[i];
@@ -76,7 +72,6 @@ __global__ void k_atom_prep(const double* __restrict__ pos, long sa, long sd,
   if (mesh_c) {
     mesh_c[i] = make_int4(c[0], c[1], c[2], 0);
     mesh_fr[i] = make_double4(fr[0], fr[1], fr[2], qi);
-    tile_key[i] = (tk[2] * a.ntiles[1] + tk[1]) * a.ntiles[0] + tk[0];
   }
 }
 
@@ -755,20 +750,17 @@ inline int blocks_for(long n, int threads) { return static_cast<int>((n + thread
 }  // namespace
 
 void launch_atom_prep(const double* pos, long sa, long sd, const double* q, int n, const Cell& cell,
-                      const int nb[3], const int ngrid[3], const int tile[3], const int ntiles[3],
-                      double4* s4, int* box_key, int4* mesh_c, double4* mesh_fr, int* tile_key,
-                      cudaStream_t st) {
+                      const int nb[3], const int ngrid[3], double4* s4, int* box_key,
+                      int4* mesh_c, double4* mesh_fr, cudaStream_t st) {
   if (n == 0) return;
   PrepArgs a;
   for (int i = 0; i < 3; ++i) {
     for (int d = 0; d < 3; ++d) a.rec[i][d] = cell.rec[i][d];
     a.nb[i] = nb ? nb[i] : 0;
     a.ng[i] = ngrid ? ngrid[i] : 0;
-    a.ntiles[i] = ntiles ? ntiles[i] : 0;
-    a.tile[i] = tile ? tile[i] : 1;
   }
   k_atom_prep<<<blocks_for(n, 256), 256, 0, st>>>(pos, sa, sd, q, n, a, s4, box_key, mesh_c,
-                                                  mesh_fr, tile_key);
+                                                  mesh_fr);
   ++g_launches;
 }
 

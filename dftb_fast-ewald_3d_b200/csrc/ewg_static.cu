@@ -269,8 +269,8 @@ extern "C" int ewg_direct_potential_force_static(int n, const double* coords_dev
   if (!cv.fits()) return EWG_ERR_SCRATCH_LIMIT;
 
   cudaMemsetAsync(err, 0, sizeof(int), st);
-  launch_atom_prep(coords_device, 3, 1, charges_device, n, cell, rg.nb, nullptr, nullptr, nullptr,
-                   s4, boxkey, nullptr, nullptr, nullptr, st);
+  launch_atom_prep(coords_device, 3, 1, charges_device, n, cell, rg.nb, nullptr, s4, boxkey,
+                   nullptr, nullptr, st);
   launch_bucket_sort(boxkey, n, nboxes, counts, cursor, starts, tmp, perm, st);
   launch_permute_box(s4, perm, n, cell.lat, s4s, x32s, st);
   launch_real_space(s4s, x32s, perm, starts, n, rg, alpha, r_cut, 0, pot_device, fbuf, err, st);

@@ -53,6 +53,17 @@ __device__ __forceinline__ int pmod(int a, int n) {
   return r < 0 ? r + n : r;
 }
 
+// One tile row of eight weights, 16-byte aligned.
+__device__ __forceinline__ void store_row(float* out, const float (&v)[8]) {
+  reinterpret_cast<float4*>(out)[0] = make_float4(v[0], v[1], v[2], v[3]);
+  reinterpret_cast<float4*>(out)[1] = make_float4(v[4], v[5], v[6], v[7]);
+}
+__device__ __forceinline__ void store_row(double* out, const double (&v)[8]) {
+#pragma unroll
+  for (int p = 0; p < 8; p += 2)
+    reinterpret_cast<double2*>(out)[p / 2] = make_double2(v[p], v[p + 1]);
+}
+
 __device__ __forceinline__ int slot_first(int packed) { return packed & 0xffff; }
 __device__ __forceinline__ int slot_count(int packed) { return packed >> 16; }
 
@@ -107,30 +118,44 @@ __global__ void k_weights_tiled(const int4* __restrict__ mc, const double4* __re
   const int origin = ((first + s) % nt) * T;
   R wv[TX], dv[TX];
   static_assert(TX == TY && TY == TZ, "one row length for all axes");
+  if (2 * m + 1 < nd) {
+    // Every point has at most one image in [-m, m]: the offsets of the row are
+    // consecutive (one wrap at most) and the eight terms are independent.
+    const int o0 = pmod(origin - c, nd);
 #pragma unroll
-  for (int p = 0; p < TX; ++p) {
-    const int P = origin + p;
-    double w = 0.0, dw = 0.0;
-    if (s < count && P < nd) {
-      int o = pmod(P - c, nd);  // largest offset <= m congruent to P - c
-      while (o > m) o -= nd;
-      while (o + nd <= m) o += nd;
-      for (; o >= -m; o -= nd) {
-        const double dd = frac - static_cast<double>(o);
-        const double e = sd.pref * exp(-(dd * dd) / sd.b);
-        w += e;
-        dw += dscale * dd * e;
-      }
+    for (int p = 0; p < TX; ++p) {
+      int o = o0 + p;
+      if (o >= nd) o -= nd;
+      if (o > m) o -= nd;  // largest offset <= m congruent to P - c
+      const bool live = s < count && origin + p < nd && o >= -m;
+      const double dd = frac - static_cast<double>(o);
+      const double e = sd.pref * exp(-(dd * dd) / sd.b);
+      wv[p] = static_cast<R>(live ? e : 0.0);
+      dv[p] = static_cast<R>(live ? dscale * dd * e : 0.0);
     }
-    wv[p] = static_cast<R>(w);
-    dv[p] = static_cast<R>(dw);
-  }
+  } else {
 #pragma unroll
-  for (int p = 0; p < TX; ++p) out[p] = wv[p];
-  if (sd.ad) {
-#pragma unroll
-    for (int p = 0; p < TX; ++p) out[sd.dwoff + p] = dv[p];
+    for (int p = 0; p < TX; ++p) {
+      const int P = origin + p;
+      double w = 0.0, dw = 0.0;
+      if (s < count && P < nd) {
+        int o = pmod(P - c, nd);  // largest offset <= m congruent to P - c
+        while (o > m) o -= nd;
+        while (o + nd <= m) o += nd;
+        for (; o >= -m; o -= nd) {
+          const double dd = frac - static_cast<double>(o);
+          const double e = sd.pref * exp(-(dd * dd) / sd.b);
+          w += e;
+          dw += dscale * dd * e;
+        }
+      }
+      wv[p] = static_cast<R>(w);
+      dv[p] = static_cast<R>(dw);
+    }
   }
+  // Rows start on multiples of eight values: whole 16-byte stores.
+  store_row(out, wv);
+  if (sd.ad) store_row(out + sd.dwoff, dv);
   if (s != 0) return;  // the axis' first slot thread writes the slot record
   int* sp = reinterpret_cast<int*>(&slot[k]);
   sp[d] = first | (count << 16);
