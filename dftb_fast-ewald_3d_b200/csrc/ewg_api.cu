@@ -441,7 +441,10 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
   // The whole launch sequence of this evaluation (no host synchronisation,
   // no allocation inside).
   auto launch_all = [&]() {
+    // Memsets first, so that the spread follows a kernel (programmatic
+    // dependent launch).
     if (!err_flag) cudaMemsetAsync(err, 0, sizeof(int), st);
+    if (stress12) cudaMemsetAsync(zpart, 0, sizeof(double) * nz, st);  // z-pass partials
     prof_mark(mp.prof, st, ST_PREP);
     if (!reuse) {
       launch_atom_prep(pos, sa, sd, q, n, cell, rg.nb, mp.g.n, s4, boxkey, mcv, fr, st);
@@ -470,10 +473,8 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
     prof_mark(mp.prof, st, ST_REAL);
     launch_real_space(s4s, x32s, permbox, boxstart, n, rg, p.alpha, p.r_cut, mixed, pot_sr, f_sr,
                       err, rs);
-    if (stress12) {  // real-space virial over the same pairs, and z-pass partials zeroed
+    if (stress12)  // real-space virial over the same pairs
       launch_real_stress(s4s, x32s, boxstart, n, rg, p.alpha, p.r_cut, p6, stress12, err, rs);
-      cudaMemsetAsync(zpart, 0, sizeof(double) * nz, st);
-    }
     if (concurrent) cudaEventRecord(c->join, rs);
     prof_mark(mp.prof, st, ST_SPREAD);
     launch_spread(mp, pairstart, pairs, wtab, qk, grid, st);

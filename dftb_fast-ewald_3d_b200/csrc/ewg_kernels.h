@@ -10,6 +10,35 @@ namespace ewg {
 // Launch counter shared by every launcher (the context copies it out).
 extern thread_local long long g_launches;
 
+// Programmatic dependent launch along the evaluation's chain of short kernels.
+// A chained kernel starts with chain_enter(): griddepcontrol.wait holds every
+// thread until the previous grid on the stream has completed and its writes
+// are visible (a no-op for a kernel launched without the attribute), so the
+// kernel touches no global memory before its predecessor is done; then
+// launch_dependents lets the next grid's CTAs be placed on the SMs this grid's
+// last wave leaves idle, instead of after a launch gap.
+__device__ __forceinline__ void chain_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Launch a chained kernel; the stream's previous operation must be a kernel.
+template <typename... P, typename... A>
+void launch_chained(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                    A&&... args) {
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, static_cast<A&&>(args)...);
+}
+
 // Stages of one evaluation, for the per-stage device timing.
 enum Stage {
   ST_PREP, ST_REAL, ST_WEIGHTS, ST_SPREAD, ST_FFT_X_R2C, ST_FFT_Y_FWD, ST_FFT_Z_INFL,
@@ -48,8 +77,9 @@ void launch_atom_prep(const double* pos, long sa, long sd, const double* q, int 
 void launch_bucket_sort(const int* key, int n, int nkeys, int* counts, int* cursor, int* starts,
                         int* tmp, int* perm, cudaStream_t st);
 
-// Exclusive scan of counts[0..nkeys) into starts[0..nkeys] (one CTA).
-void launch_scan(const int* counts, int nkeys, int* starts, cudaStream_t st);
+// Exclusive scan of counts[0..nkeys) into starts[0..nkeys] (one CTA), chained
+// to the stream's previous kernel when after_kernel.
+void launch_scan(const int* counts, int nkeys, int* starts, bool after_kernel, cudaStream_t st);
 
 // Box-sorted atoms: out[k] = in[perm[k]] (fractional s, q) and x32[k] the
 // Cartesian position s . lat with q, in FP32, for the real-space distance test.

@@ -54,6 +54,7 @@ template <typename R, int L>
 __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_r2c(const R* __restrict__ grid,
                                                                cx<R>* __restrict__ A1, int n1,
                                                                int npairs, int K1, FftPlan plan) {
+  chain_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
   cx<R>* b = a + static_cast<size_t>(n1) * L;
@@ -90,6 +91,7 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_fwd(const cx<R>* __re
                                                                cx<R>* __restrict__ A2, int n2,
                                                                int K1, int K2, int H2,
                                                                FftPlan plan) {
+  chain_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
   cx<R>* b = a + static_cast<size_t>(n2) * L;
@@ -133,6 +135,7 @@ template <typename R, int L, bool STRESS>
 __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
     const cx<R>* __restrict__ A2, cx<R>* __restrict__ B2, int n3, int K1, int K2, int K3, int nc,
     InfluenceArgs ia, FftPlan plan) {
+  chain_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
   cx<R>* b = a + static_cast<size_t>(n3) * L;
@@ -254,6 +257,7 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_inv(const cx<R>* __re
                                                                cx<R>* __restrict__ B1, int n2,
                                                                int n3, int K1, int K2, int H2,
                                                                FftPlan plan) {
+  chain_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
   cx<R>* b = a + static_cast<size_t>(n2) * L;
@@ -293,6 +297,7 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_c2r(const cx<R>* __re
                                                                R* __restrict__ out, int n1,
                                                                int nrows, int K1, int nc,
                                                                FftPlan plan) {
+  chain_enter();
   constexpr int NP = L / NCG;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
@@ -383,7 +388,7 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
     const int blocks = (npairs + L - 1) / L;
     with_lines(L, [&](auto lc) {
       constexpr int LL = decltype(lc)::value;
-      k_fft_x_r2c<R, LL><<<blocks, pass_threads(LL), sm, st>>>(static_cast<const R*>(grid), A1, n1, npairs,
+      launch_chained(k_fft_x_r2c<R, LL>, blocks, pass_threads(LL), sm, st, static_cast<const R*>(grid), A1, n1, npairs,
                                                        g.K1, mp.fft[0]);
     });
     ++g_launches;
@@ -396,7 +401,7 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
     const int H2 = (g.K2 - 1) / 2;
     with_lines(L, [&](auto lc) {
       constexpr int LL = decltype(lc)::value;
-      k_fft_y_fwd<R, LL><<<grd, pass_threads(LL), sm, st>>>(A1, A2, n2, g.K1, g.K2, H2, mp.fft[1]);
+      launch_chained(k_fft_y_fwd<R, LL>, grd, pass_threads(LL), sm, st, A1, A2, n2, g.K1, g.K2, H2, mp.fft[1]);
     });
     ++g_launches;
   }
@@ -420,10 +425,10 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
     with_lines(L, [&](auto lc) {
       constexpr int LL = decltype(lc)::value;
       if (stress_part)
-        k_fft_z_influence<R, LL, true><<<grd, pass_threads(LL), sm, st>>>(
+        launch_chained(k_fft_z_influence<R, LL, true>, grd, pass_threads(LL), sm, st,
             A2, B2, n3, g.K1, g.K2, g.K3, nc, ia, mp.fft[2]);
       else
-        k_fft_z_influence<R, LL, false><<<grd, pass_threads(LL), sm, st>>>(
+        launch_chained(k_fft_z_influence<R, LL, false>, grd, pass_threads(LL), sm, st,
             A2, B2, n3, g.K1, g.K2, g.K3, nc, ia, mp.fft[2]);
     });
     ++g_launches;
@@ -446,7 +451,7 @@ void inverse_impl(const MeshPlan& mp, const void* B2v, void* B1v, void* out, int
     const int H2 = (g.K2 - 1) / 2;
     with_lines(L, [&](auto lc) {
       constexpr int LL = decltype(lc)::value;
-      k_fft_y_inv<R, LL><<<grd, pass_threads(LL), sm, st>>>(B2, B1, n2, n3, g.K1, g.K2, H2, mp.fft[1]);
+      launch_chained(k_fft_y_inv<R, LL>, grd, pass_threads(LL), sm, st, B2, B1, n2, n3, g.K1, g.K2, H2, mp.fft[1]);
     });
     ++g_launches;
   }
@@ -460,14 +465,14 @@ void inverse_impl(const MeshPlan& mp, const void* B2v, void* B1v, void* out, int
       const int NP = L / 4;
       dim3 grd((nrows / 2 + NP - 1) / NP, 1);
       if (L == 8)
-        k_fft_x_c2r<R, 8, 4><<<grd, pass_threads(8), sm, st>>>(B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
+        launch_chained(k_fft_x_c2r<R, 8, 4>, grd, pass_threads(8), sm, st, B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
       else
-        k_fft_x_c2r<R, 4, 4><<<grd, pass_threads(4), sm, st>>>(B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
+        launch_chained(k_fft_x_c2r<R, 4, 4>, grd, pass_threads(4), sm, st, B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
     } else {  // one component per CTA row (grid.y = component)
       dim3 grd((nrows / 2 + L - 1) / L, nc);
       with_lines(L, [&](auto lc) {
         constexpr int LL = decltype(lc)::value;
-        k_fft_x_c2r<R, LL, 1><<<grd, pass_threads(LL), sm, st>>>(B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
+        launch_chained(k_fft_x_c2r<R, LL, 1>, grd, pass_threads(LL), sm, st, B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
       });
     }
     ++g_launches;

@@ -89,6 +89,7 @@ __global__ void k_count(const int* __restrict__ key, int n, int* __restrict__ co
 // consecutive entries per thread and writes the starts back coalesced.
 __global__ void __launch_bounds__(1024) k_scan(const int* __restrict__ counts, int nkeys,
                                                int* __restrict__ starts) {
+  chain_enter();
   constexpr int kItems = 8, kRound = 1024 * kItems;
   __shared__ int buf[kRound + kRound / 32];  // padded: entry i at i + i / 32
   __shared__ int warp_sums[32];
@@ -148,6 +149,7 @@ __global__ void __launch_bounds__(1024) k_scan(const int* __restrict__ counts, i
 
 __global__ void k_scatter(const int* __restrict__ key, int n, const int* __restrict__ starts,
                           int* __restrict__ cursor, int* __restrict__ tmp) {
+  chain_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int k = key[i];
@@ -156,6 +158,7 @@ __global__ void k_scatter(const int* __restrict__ key, int n, const int* __restr
 
 __global__ void k_rank(const int* __restrict__ key, int n, const int* __restrict__ starts,
                        const int* __restrict__ tmp, int* __restrict__ perm) {
+  chain_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int k = key[i];
@@ -772,17 +775,23 @@ void launch_bucket_sort(const int* key, int n, int nkeys, int* counts, int* curs
     k_count<<<blocks_for(n, 256), 256, 0, st>>>(key, n, counts);
     ++g_launches;
   }
-  k_scan<<<1, 1024, 0, st>>>(counts, nkeys, starts);
+  if (n > 0)
+    launch_chained(k_scan, 1, 1024, 0, st, counts, nkeys, starts);
+  else  // the stream's previous operation is a memset
+    k_scan<<<1, 1024, 0, st>>>(counts, nkeys, starts);
   ++g_launches;
   if (n > 0) {
-    k_scatter<<<blocks_for(n, 256), 256, 0, st>>>(key, n, starts, cursor, tmp);
-    k_rank<<<blocks_for(n, 256), 256, 0, st>>>(key, n, starts, tmp, perm);
+    launch_chained(k_scatter, blocks_for(n, 256), 256, 0, st, key, n, starts, cursor, tmp);
+    launch_chained(k_rank, blocks_for(n, 256), 256, 0, st, key, n, starts, tmp, perm);
     g_launches += 2;
   }
 }
 
-void launch_scan(const int* counts, int nkeys, int* starts, cudaStream_t st) {
-  k_scan<<<1, 1024, 0, st>>>(counts, nkeys, starts);
+void launch_scan(const int* counts, int nkeys, int* starts, bool after_kernel, cudaStream_t st) {
+  if (after_kernel)
+    launch_chained(k_scan, 1, 1024, 0, st, counts, nkeys, starts);
+  else
+    k_scan<<<1, 1024, 0, st>>>(counts, nkeys, starts);
   ++g_launches;
 }
 

@@ -76,6 +76,7 @@ __global__ void k_weights_tiled(const int4* __restrict__ mc, const double4* __re
                                 const int* __restrict__ perm, int n, StencilDims sd,
                                 R* __restrict__ wtab, R* __restrict__ qk,
                                 int4* __restrict__ slot) {
+  chain_enter();
   const int SS = sd.S[0] + sd.S[1] + sd.S[2];
   const long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (idx >= static_cast<long>(SS) * n) return;
@@ -214,6 +215,7 @@ __global__ void k_pair_count(const int4* __restrict__ slot, int n, StencilDims s
 __global__ void k_pair_scatter(const int4* __restrict__ slot, int n, StencilDims sd,
                                const int* __restrict__ starts, int* __restrict__ cursor,
                                int2* __restrict__ tmp) {
+  chain_enter();
   int tile, k, packed;
   if (pair_of_thread(slot, n, sd, &tile, &k, &packed))
     tmp[starts[tile] + atomicAdd(&cursor[tile], 1)] = make_int2(k, packed);
@@ -225,6 +227,7 @@ __global__ void k_pair_scatter(const int4* __restrict__ slot, int n, StencilDims
 __global__ void k_pair_rank(const int2* __restrict__ tmp, const int* __restrict__ starts,
                             int ntiles, const int4* __restrict__ slot, StencilDims sd,
                             int2* __restrict__ pairs) {
+  chain_enter();
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= starts[ntiles]) return;
   const int2 v = tmp[e];
@@ -264,6 +267,7 @@ __global__ void __launch_bounds__(kSpreadLanes) k_spread_tiles(const int* __rest
                                                                const R* __restrict__ wtab,
                                                                const R* __restrict__ qk,
                                                                StencilDims sd, R* __restrict__ grid) {
+  chain_enter();
   __shared__ R sW1[kSpreadChunk][TX];
   __shared__ R sW2[kSpreadChunk][TY];
   __shared__ R sW3[kSpreadChunk][TZ];
@@ -378,6 +382,7 @@ __global__ void __launch_bounds__(32) k_spread_tiles_dmma(const int* __restrict_
                                                           const double* __restrict__ qk,
                                                           StencilDims sd,
                                                           double* __restrict__ grid) {
+  chain_enter();
   __shared__ __align__(16) double sW[3][kSpreadAtoms][kWRow];
   __shared__ double sQ[kSpreadAtoms];
   const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
@@ -450,6 +455,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles(const int* __restri
                                                              StencilDims sd,
                                                              const R* __restrict__ grid,
                                                              double* __restrict__ part) {
+  chain_enter();
   using V = typename std::conditional<
       NC == 4, typename std::conditional<sizeof(R) == 8, double4, float4>::type, R>::type;
   __shared__ V sG[TZ * TY * TX];
@@ -592,6 +598,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_ad(const int* __res
                                                                 StencilDims sd,
                                                                 const float* __restrict__ grid,
                                                                 double* __restrict__ part) {
+  chain_enter();
   __shared__ float sG[TZ * TY * TX];
   // y and z weights and their derivatives, lane fastest: [kind][row][lane]
   // with kind 0 = w2, 1 = dw2, 2 = w3, 3 = dw3.
@@ -761,6 +768,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma(const int* __r
                                                           StencilDims sd,
                                                           const double* __restrict__ grid,
                                                           double* __restrict__ part) {
+  chain_enter();
   constexpr int RS = GatherRow<NC>::value;
   constexpr int kGatherAtoms = WARPS * MB * 8;  // atoms staged per round
   __shared__ __align__(16) double sG[TZ * TY * RS];
@@ -899,6 +907,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma_ad(
     const int* __restrict__ tile_start, const int2* __restrict__ pairs,
     const double* __restrict__ wtab, StencilDims sd, const double* __restrict__ grid,
     double* __restrict__ part) {
+  chain_enter();
   constexpr int RS = GatherRow<1>::value;
   __shared__ __align__(16) double sG[TZ * TY * RS];
   __shared__ __align__(16) double sW[WARPS][6][8][kWRow];  // per warp: its 8 atoms' rows
@@ -1082,10 +1091,10 @@ void launch_weights(const MeshPlan& mp, const int4* mc, const double4* fr, const
   if (n == 0) return;
   const long threads = static_cast<long>(mp.sd.S[0] + mp.sd.S[1] + mp.sd.S[2]) * n;
   if (mp.mixed)
-    k_weights_tiled<float><<<blocks_for(threads, 128), 128, 0, st>>>(
+    launch_chained(k_weights_tiled<float>, blocks_for(threads, 128), 128, 0, st,
         mc, fr, perm, n, mp.sd, static_cast<float*>(wtab), static_cast<float*>(qk), slot);
   else
-    k_weights_tiled<double><<<blocks_for(threads, 128), 128, 0, st>>>(
+    launch_chained(k_weights_tiled<double>, blocks_for(threads, 128), 128, 0, st,
         mc, fr, perm, n, mp.sd, static_cast<double*>(wtab), static_cast<double*>(qk), slot);
   ++g_launches;
 }
@@ -1101,11 +1110,11 @@ void launch_pair_bins(const MeshPlan& mp, const int4* slot, int n, int* counts, 
     k_pair_count<<<blocks_for(nthreads, 256), 256, 0, st>>>(slot, n, mp.sd, counts);
     ++g_launches;
   }
-  launch_scan(counts, ntiles, tile_start, st);
+  launch_scan(counts, ntiles, tile_start, n > 0, st);
   if (n > 0) {
-    k_pair_scatter<<<blocks_for(nthreads, 256), 256, 0, st>>>(slot, n, mp.sd, tile_start, cursor,
+    launch_chained(k_pair_scatter, blocks_for(nthreads, 256), 256, 0, st, slot, n, mp.sd, tile_start, cursor,
                                                                t2);
-    k_pair_rank<<<blocks_for(npairs_max, 256), 256, 0, st>>>(t2, tile_start, ntiles, slot, mp.sd,
+    launch_chained(k_pair_rank, blocks_for(npairs_max, 256), 256, 0, st, t2, tile_start, ntiles, slot, mp.sd,
                                                               pairs);
     g_launches += 2;
   }
@@ -1115,12 +1124,12 @@ void launch_spread(const MeshPlan& mp, const int* tile_start, const int2* pairs,
                    const void* qk, void* grid, cudaStream_t st) {
   dim3 grd(mp.sd.ntiles[0], mp.sd.ntiles[1], mp.sd.ntiles[2]);
   if (mp.mixed)
-    k_spread_tiles<float><<<grd, kSpreadLanes, 0, st>>>(tile_start, pairs,
+    launch_chained(k_spread_tiles<float>, grd, kSpreadLanes, 0, st, tile_start, pairs,
                                                      static_cast<const float*>(wtab),
                                                      static_cast<const float*>(qk), mp.sd,
                                                      static_cast<float*>(grid));
   else
-    k_spread_tiles_dmma<<<grd, 32, 0, st>>>(tile_start, pairs, static_cast<const double*>(wtab),
+    launch_chained(k_spread_tiles_dmma, grd, 32, 0, st, tile_start, pairs, static_cast<const double*>(wtab),
                                              static_cast<const double*>(qk), mp.sd,
                                              static_cast<double*>(grid));
   ++g_launches;
@@ -1129,18 +1138,17 @@ void launch_spread(const MeshPlan& mp, const int* tile_start, const int2* pairs,
 void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs, const void* wtab,
                    const void* grid, int nc, double* part, cudaStream_t st) {
   dim3 grd(mp.sd.ntiles[0], mp.sd.ntiles[1], mp.sd.ntiles[2]);
-#define EWG_GATHER(R, NC)                                                               \
-  k_gather_tiles<R, NC, GatherShape<R>::atoms, GatherShape<R>::warps>                      \
-      <<<grd, 32 * GatherShape<R>::warps, 0, st>>>(tile_start, pairs, static_cast<const R*>(wtab), \
-                                                   mp.sd, static_cast<const R*>(grid), part)
+#define EWG_GATHER(R, NC)                                                                \
+  launch_chained(k_gather_tiles<R, NC, GatherShape<R>::atoms, GatherShape<R>::warps>, grd,  \
+                 32 * GatherShape<R>::warps, 0, st, tile_start, pairs,                       \
+                 static_cast<const R*>(wtab), mp.sd, static_cast<const R*>(grid), part)
   if (mp.sd.ad && nc == 1) {  // force wanted, ad scheme: potential grid, four partials
     if (mp.mixed)
-      k_gather_tiles_ad<kGatherAdF32Atoms, kGatherAdF32Warps>
-          <<<grd, 32 * kGatherAdF32Warps, 0, st>>>(
-              tile_start, pairs, static_cast<const float*>(wtab), mp.sd,
-              static_cast<const float*>(grid), part);
+      launch_chained(k_gather_tiles_ad<kGatherAdF32Atoms, kGatherAdF32Warps>, grd,
+                     32 * kGatherAdF32Warps, 0, st, tile_start, pairs,
+                     static_cast<const float*>(wtab), mp.sd, static_cast<const float*>(grid), part);
     else
-      k_gather_tiles_dmma_ad<kGatherAdWarps><<<grd, 32 * kGatherAdWarps, 0, st>>>(
+      launch_chained(k_gather_tiles_dmma_ad<kGatherAdWarps>, grd, 32 * kGatherAdWarps, 0, st,
           tile_start, pairs, static_cast<const double*>(wtab), mp.sd,
           static_cast<const double*>(grid), part);
   } else if (mp.mixed) {
@@ -1150,12 +1158,12 @@ void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs,
       EWG_GATHER(float, 1);
   } else {
     if (nc == 4)
-      k_gather_tiles_dmma<4, kGatherWarps, kGatherMB><<<grd, 32 * kGatherWarps, 0, st>>>(
+      launch_chained(k_gather_tiles_dmma<4, kGatherWarps, kGatherMB>, grd, 32 * kGatherWarps, 0, st,
           tile_start, pairs,
                                                  static_cast<const double*>(wtab), mp.sd,
                                                  static_cast<const double*>(grid), part);
     else
-      k_gather_tiles_dmma<1, kGatherWarps, kGatherMB><<<grd, 32 * kGatherWarps, 0, st>>>(
+      launch_chained(k_gather_tiles_dmma<1, kGatherWarps, kGatherMB>, grd, 32 * kGatherWarps, 0, st,
           tile_start, pairs,
                                                  static_cast<const double*>(wtab), mp.sd,
                                                  static_cast<const double*>(grid), part);
