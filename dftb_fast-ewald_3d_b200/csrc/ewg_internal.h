@@ -3,6 +3,7 @@
 // public interface.
 #pragma once
 
+#include <cmath>
 #include <cstddef>
 #include <cstdint>
 #include <vector>
@@ -95,13 +96,26 @@ struct RealGeom {
                    // row is at most two contiguous runs of boxes (see set_scan_mode)
   double lat[3][3];
   double rec[3][3];
+  double rl[3];    // |rec_d|: fractional extent per Bohr normal to the planes s_d = const
+  int ortho;       // 1: the three plane normals are mutually orthogonal
 };
 
 // The flat candidate scan needs every x row of 2R+1 boxes to split into at
-// most two runs (nb_x >= 2R_x + 1) and at most 32 rows.
+// most two runs (nb_x >= 2R_x + 1) and at most 32 rows.  Also fills rl and
+// ortho, which the scan uses to skip rows and trim runs beyond the cutoff.
 inline void set_scan_mode(RealGeom& g) {
   const int rows = (2 * g.R[1] + 1) * (2 * g.R[2] + 1);
   g.flat = (g.nb[0] >= 2 * g.R[0] + 1 && rows <= 32) ? 1 : 0;
+  for (int d = 0; d < 3; ++d)
+    g.rl[d] = std::sqrt(g.rec[d][0] * g.rec[d][0] + g.rec[d][1] * g.rec[d][1] +
+                        g.rec[d][2] * g.rec[d][2]);
+  g.ortho = 1;
+  for (int d = 0; d < 3; ++d)
+    for (int e = d + 1; e < 3; ++e) {
+      const double dot = g.rec[d][0] * g.rec[e][0] + g.rec[d][1] * g.rec[e][1] +
+                         g.rec[d][2] * g.rec[e][2];
+      if (std::fabs(dot) > 1e-12 * g.rl[d] * g.rl[e]) g.ortho = 0;
+    }
 }
 
 }  // namespace ewg

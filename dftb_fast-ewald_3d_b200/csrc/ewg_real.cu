@@ -400,8 +400,10 @@ __device__ __forceinline__ void for_each_candidate(const float4* __restrict__ x3
 // first atom less that offset, the shift S and the run's x_i - S lat in FP32 --
 // and the warp
 // then walks the concatenated list 32 candidates at a time, so that a warp
-// iteration is filled across run ends.  Candidate order (and with it the
-// summation order) is the same as the row-by-row scan's.
+// iteration is filled across run ends.  Rows, and the ends of rows, that lie
+// wholly beyond the cutoff from atom i (by the distance from i to the boxes'
+// slabs) are left out; the candidates visited keep the row-by-row scan's
+// order, and the pairs inside the cutoff are the same.
 constexpr int kRuns = 64;
 struct RunTable {
   int start[kRuns + 1];  // offset of each run in the concatenated list; start[nrun] = total
@@ -409,11 +411,21 @@ struct RunTable {
   float4 base[kRuns];    // x_i - S lat (w unused)
 };
 
+// Fractional distance from s to the slab [b / nb, (b + 1) / nb) of the
+// unwrapped box index b (0 inside).
+__device__ __forceinline__ double slab_gap(double s, int b, int nb) {
+  const double lo = static_cast<double>(b) / nb, hi = static_cast<double>(b + 1) / nb;
+  return s < lo ? lo - s : (s > hi ? s - hi : 0.0);
+}
+
+// reach2: squared cutoff with a relative margin far above the rounding of the
+// slab distances; rows and boxes wholly beyond it are not visited.
 template <class Visit>
 __device__ __forceinline__ void for_each_candidate_flat(const float4* __restrict__ x32,
                                                         const int* __restrict__ box_start, int k,
                                                         const double4& ai, const RealGeom& g,
-                                                        RunTable& t, Visit& visit) {
+                                                        double reach2, RunTable& t,
+                                                        Visit& visit) {
   const int lane = threadIdx.x & 31;
   int b[3];
   const double sv[3] = {ai.x, ai.y, ai.z};
@@ -432,14 +444,30 @@ __device__ __forceinline__ void for_each_candidate_flat(const float4* __restrict
     sy = floor_div(byr, g.nb[1]);
     sz = floor_div(bzr, g.nb[2]);
     const int wy = byr - sy * g.nb[1], wz = bzr - sz * g.nb[2];
-    int dx = -g.R[0];
+    // Distances from atom i to the row's y and z box slabs (normal to the
+    // planes of constant s_y, s_z); the row region is the slabs' intersection.
+    // With orthogonal plane normals its distance is sqrt(dy^2 + dz^2) and a
+    // box of the row is reached when its x slab lies within
+    // sqrt(reach^2 - dy^2 - dz^2); otherwise max(dy, dz) and reach bound them.
+    const double dyz_y = slab_gap(sv[1], byr, g.nb[1]) / g.rl[1];
+    const double dyz_z = slab_gap(sv[2], bzr, g.nb[2]) / g.rl[2];
+    const double dperp2 = g.ortho ? dyz_y * dyz_y + dyz_z * dyz_z
+                                  : fmax(dyz_y, dyz_z) * fmax(dyz_y, dyz_z);
+    int dx = -g.R[0], dx_hi = g.R[0];
+    if (dperp2 > reach2) {
+      dx_hi = dx - 1;  // the whole row lies beyond the cutoff
+    } else {
+      const double fx = sqrt(g.ortho ? reach2 - dperp2 : reach2) * g.rl[0];
+      dx = max(dx, static_cast<int>(floor((sv[0] - fx) * g.nb[0])) - b[0]);
+      dx_hi = min(dx_hi, static_cast<int>(floor((sv[0] + fx) * g.nb[0])) - b[0]);
+    }
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      if (dx <= g.R[0]) {
+      if (dx <= dx_hi) {
         const int bxr = b[0] + dx;
         const int s = floor_div(bxr, g.nb[0]);
         const int wx = bxr - s * g.nb[0];
-        const int len = min(g.R[0] - dx + 1, g.nb[0] - wx);
+        const int len = min(dx_hi - dx + 1, g.nb[0] - wx);
         const int first = (wz * g.nb[1] + wy) * g.nb[0] + wx;
         j0[h] = box_start[first];
         cnt[h] = box_start[first + len] - j0[h];
@@ -596,7 +624,8 @@ __global__ void __launch_bounds__(kRealThreads, 4) k_real_space(const double4* _
   pair.qi = ai.w;
   PairQueue<EwaldPair, MIXED> pq(queue[threadIdx.x >> 5], pair, srt, ai, g, cut2, pre2);
   if (g.flat)
-    for_each_candidate_flat(x32, box_start, k, ai, g, runs[threadIdx.x >> 5], pq);
+    for_each_candidate_flat(x32, box_start, k, ai, g, cut2 * (1.0 + 1e-9), runs[threadIdx.x >> 5],
+                              pq);
   else
     for_each_candidate(x32, box_start, k, ai, g, pq);
   pq.flush();
@@ -655,7 +684,8 @@ __global__ void __launch_bounds__(kRealThreads) k_real_stress(const double4* __r
   pair.qi = ai.w;
   PairQueue<StressPair, false> pq(queue[threadIdx.x >> 5], pair, srt, ai, g, cut2, pre2);
   if (g.flat)
-    for_each_candidate_flat(x32, box_start, k, ai, g, runs[threadIdx.x >> 5], pq);
+    for_each_candidate_flat(x32, box_start, k, ai, g, cut2 * (1.0 + 1e-9), runs[threadIdx.x >> 5],
+                              pq);
   else
     for_each_candidate(x32, box_start, k, ai, g, pq);
   pq.flush();
