@@ -130,6 +130,9 @@ struct ewg_context {
   // of its own (buffers, streams), so that independent cells run concurrently.
   int batch_lanes = 4;
   std::vector<ewg_context*> lanes;
+  // Pinned host copy of the device charge sums (sum q, sum |q|, sum q^2) for
+  // checks deferred to the end of a call.
+  double* host_sums = nullptr;
   cudaEvent_t lanes_ready = nullptr;
   std::vector<cudaEvent_t> lane_done;
   // Autotuner results per (atoms, precision, scheme, lattice, target).
@@ -154,6 +157,7 @@ struct ewg_context {
       cudaFree(kv.second.tw32);
     }
     for (auto& kv : corrs) cudaFree(kv.second.dev);
+    if (host_sums) cudaFreeHost(host_sums);
     drop_graphs();
     for (ewg_context* l : lanes) delete l;
     if (lanes_ready) cudaEventDestroy(lanes_ready);
@@ -906,15 +910,38 @@ int ewg_potential_force_device(ewg_context* c, int n, const double* coords_devic
   double* partial = dbuf<double>(c, B_PARTIAL, 3 * 148, &rc);
   double* sums = dbuf<double>(c, B_SUMS, 4, &rc);
   if (rc) return rc;
+  if (!c->host_sums && cudaMallocHost(&c->host_sums, 4 * sizeof(double)) != cudaSuccess) {
+    c->host_sums = nullptr;
+    return EWG_ERR_OUT_OF_MEMORY;
+  }
+  double* h = c->host_sums;
+  Cell cell;
+  if (ov && ov->has_alpha && ov->has_k_cut && !c->background) {
+    // The parameters do not depend on the charges (sum q^2 enters only alpha
+    // and k_cut): the evaluation is queued behind the sums without a host
+    // wait, and the neutrality check reads them after the call's own
+    // synchronisation (it then reports after the cell and tolerance checks).
+    if ((rc = cell_from_rows(lat_rows, cell))) return rc;
+    if (!(tol > 0.0 && tol < 1.0)) return EWG_ERR_TOL;
+    ewg_params p;
+    if ((rc = choose_parameters(cell, 0.0, n, tol, ov, p))) return rc;
+    launch_charge_sums(charges_device, n, partial, sums, c->stream);
+    cudaError_t e = cudaMemcpyAsync(h, sums, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) return cuda_status(e);
+    const int erc = evaluate(c, n, coords_device, 3, 1, charges_device, cell, p,
+                             force_device != nullptr, pot_device, force_device, false, nullptr,
+                             nullptr, 0.0);
+    if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return cuda_status(e);
+    if ((rc = check_sums(n, h[0], h[1]))) return rc;
+    return erc;
+  }
   launch_charge_sums(charges_device, n, partial, sums, c->stream);
-  double h[3];
-  cudaError_t e = cudaMemcpyAsync(h, sums, sizeof(h), cudaMemcpyDeviceToHost, c->stream);
+  cudaError_t e = cudaMemcpyAsync(h, sums, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
   if (e != cudaSuccess) return cuda_status(e);
   rc = check_sums(n, h[0], h[1]);
   if (rc == EWG_ERR_NOT_NEUTRAL && c->background) rc = EWG_OK;
   if (rc) return rc;
-  Cell cell;
   rc = cell_from_rows(lat_rows, cell);
   if (rc) return rc;
   if (!(tol > 0.0 && tol < 1.0)) return EWG_ERR_TOL;
