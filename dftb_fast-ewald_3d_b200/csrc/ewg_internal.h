@@ -97,6 +97,8 @@ struct RealGeom {
   double lat[3][3];
   double rec[3][3];
   double rl[3];    // |rec_d|: fractional extent per Bohr normal to the planes s_d = const
+  double h[3];     // 1 / rl[d]: spacing of the planes s_d = 0 and s_d = 1
+  double inb[3];   // 1 / nb[d]
   int ortho;       // 1: the three plane normals are mutually orthogonal
 };
 
@@ -106,9 +108,12 @@ struct RealGeom {
 inline void set_scan_mode(RealGeom& g) {
   const int rows = (2 * g.R[1] + 1) * (2 * g.R[2] + 1);
   g.flat = (g.nb[0] >= 2 * g.R[0] + 1 && rows <= 32) ? 1 : 0;
-  for (int d = 0; d < 3; ++d)
+  for (int d = 0; d < 3; ++d) {
     g.rl[d] = std::sqrt(g.rec[d][0] * g.rec[d][0] + g.rec[d][1] * g.rec[d][1] +
                         g.rec[d][2] * g.rec[d][2]);
+    g.h[d] = 1.0 / g.rl[d];
+    g.inb[d] = 1.0 / g.nb[d];
+  }
   g.ortho = 1;
   for (int d = 0; d < 3; ++d)
     for (int e = d + 1; e < 3; ++e) {

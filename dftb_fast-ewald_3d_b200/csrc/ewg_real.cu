@@ -412,9 +412,9 @@ struct RunTable {
 };
 
 // Fractional distance from s to the slab [b / nb, (b + 1) / nb) of the
-// unwrapped box index b (0 inside).
-__device__ __forceinline__ double slab_gap(double s, int b, int nb) {
-  const double lo = static_cast<double>(b) / nb, hi = static_cast<double>(b + 1) / nb;
+// unwrapped box index b (0 inside); inb = 1 / nb.
+__device__ __forceinline__ double slab_gap(double s, int b, double inb) {
+  const double lo = b * inb, hi = (b + 1) * inb;
   return s < lo ? lo - s : (s > hi ? s - hi : 0.0);
 }
 
@@ -449,8 +449,8 @@ __device__ __forceinline__ void for_each_candidate_flat(const float4* __restrict
     // With orthogonal plane normals its distance is sqrt(dy^2 + dz^2) and a
     // box of the row is reached when its x slab lies within
     // sqrt(reach^2 - dy^2 - dz^2); otherwise max(dy, dz) and reach bound them.
-    const double dyz_y = slab_gap(sv[1], byr, g.nb[1]) / g.rl[1];
-    const double dyz_z = slab_gap(sv[2], bzr, g.nb[2]) / g.rl[2];
+    const double dyz_y = slab_gap(sv[1], byr, g.inb[1]) * g.h[1];
+    const double dyz_z = slab_gap(sv[2], bzr, g.inb[2]) * g.h[2];
     const double dperp2 = g.ortho ? dyz_y * dyz_y + dyz_z * dyz_z
                                   : fmax(dyz_y, dyz_z) * fmax(dyz_y, dyz_z);
     int dx = -g.R[0], dx_hi = g.R[0];

@@ -209,7 +209,11 @@ int ewg_device_memory(int n, const double* charges, const double* lat_rows, doub
 /* Same as ewg_potential_force with every array already in device memory:
  * coords(3,N), charges(N), pot(N), force(3,N) all device pointers; lat_rows on
  * the host.  The charge sums the parameter chain needs are reduced on the GPU
- * and read back (24 bytes). */
+ * and read back (24 bytes).  When ov fixes alpha and k_cut (as ewg_tune's
+ * result does) and the background convention is off, the parameters do not
+ * depend on the charges: the evaluation is queued without waiting for the
+ * sums, and the neutrality check (EWG_ERR_NOT_NEUTRAL) is made after it, once
+ * the call has synchronised. */
 int ewg_potential_force_device(ewg_context* ctx, int n, const double* coords_device,
                                const double* charges_device, const double* lat_rows, double tol,
                                double* pot_device, double* force_device, const ewg_overrides* ov);
