@@ -100,6 +100,7 @@ struct RealGeom {
   double h[3];     // 1 / rl[d]: spacing of the planes s_d = 0 and s_d = 1
   double inb[3];   // 1 / nb[d]
   int ortho;       // 1: the three plane normals are mutually orthogonal
+  int rowmul;      // ceil(2^16 / (2 R_y + 1)): row / (2 R_y + 1) as (row * rowmul) >> 16, exact for rows < 32
 };
 
 // The flat candidate scan needs every x row of 2R+1 boxes to split into at
@@ -114,6 +115,7 @@ inline void set_scan_mode(RealGeom& g) {
     g.h[d] = 1.0 / g.rl[d];
     g.inb[d] = 1.0 / g.nb[d];
   }
+  g.rowmul = (65536 + 2 * g.R[1]) / (2 * g.R[1] + 1);
   g.ortho = 1;
   for (int d = 0; d < 3; ++d)
     for (int e = d + 1; e < 3; ++e) {

@@ -27,7 +27,12 @@ namespace {
 
 constexpr double kSqrtPi = 1.77245385090551602730;  // sqrt(pi)
 
+// floor(a / n) for n > 0.  Box indices of a neighbourhood lie within one
+// image of the cell almost always, which needs no division.
 __device__ __forceinline__ int floor_div(int a, int n) {
+  if (a >= 0 && a < n) return 0;
+  if (a < 0 && a >= -n) return -1;
+  if (a >= n && a < 2 * n) return 1;
   return a >= 0 ? a / n : -((-a + n - 1) / n);
 }
 
@@ -440,7 +445,8 @@ __device__ __forceinline__ void for_each_candidate_flat(const float4* __restrict
   // This lane's row: up to two runs.
   int j0[2] = {0, 0}, cnt[2] = {0, 0}, sx[2] = {0, 0}, sy = 0, sz = 0;
   if (lane < rows) {
-    const int byr = b[1] + lane % wdy - g.R[1], bzr = b[2] + lane / wdy - g.R[2];
+    const int rz = (lane * g.rowmul) >> 16, ry = lane - rz * wdy;
+    const int byr = b[1] + ry - g.R[1], bzr = b[2] + rz - g.R[2];
     sy = floor_div(byr, g.nb[1]);
     sz = floor_div(bzr, g.nb[2]);
     const int wy = byr - sy * g.nb[1], wz = bzr - sz * g.nb[2];
