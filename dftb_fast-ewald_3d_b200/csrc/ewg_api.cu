@@ -583,9 +583,8 @@ struct LaunchScope {
 // check_charges, except that with the background convention a net charge is
 // accepted (its sum goes to *qsum).
 int charge_check(const ewg_context* c, int n, const double* q, double* q2, double* qsum) {
-  int rc = check_charges(n, q, q2);
   double s = 0.0;
-  for (int i = 0; i < n && q; ++i) s += q[i];
+  int rc = check_charges(n, q, q2, &s);
   if (qsum) *qsum = s;
   if (rc == EWG_ERR_NOT_NEUTRAL && c && c->background) rc = EWG_OK;
   return rc;
@@ -828,14 +827,12 @@ int ewg_potential_force(ewg_context* c, int n, const double* positions, const do
   LaunchScope scope(c);
   c->uploaded_charges = -1;
   c->resident.coords_version = -1;
-  Cell cell;
-  double q2 = 0.0, qsum = 0.0;
-  int rc = validate_host(c, n, positions, charges, lat_rows, tol, cell, q2, qsum);
-  if (rc) return rc;
-  if (!pot) return EWG_ERR_ARG;
-  ewg_params p;
-  rc = choose_parameters(cell, q2, n, tol, ov, p);
-  if (rc) return rc;
+  if (n <= 0) return EWG_ERR_NPARTICLE;
+  if (!positions || !charges || !lat_rows || !pot) return EWG_ERR_ARG;
+  // The uploads go first and run while the host checks the charges and the
+  // cell; every return after them waits for them (the caller's arrays must
+  // outlive the copies).
+  int rc = EWG_OK;
   double* dpos = dbuf<double>(c, B_POS, 3 * static_cast<size_t>(n), &rc);
   double* dq = dbuf<double>(c, B_Q, n, &rc);
   double* dpot = dbuf<double>(c, B_POT, n, &rc);
@@ -843,9 +840,21 @@ int ewg_potential_force(ewg_context* c, int n, const double* positions, const do
   if (rc) return rc;
   cudaMemcpyAsync(dpos, positions, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream);
   cudaMemcpyAsync(dq, charges, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream);
+  Cell cell;
+  double q2 = 0.0, qsum = 0.0;
+  ewg_params p;
+  rc = validate_host(c, n, positions, charges, lat_rows, tol, cell, q2, qsum);
+  if (!rc) rc = choose_parameters(cell, q2, n, tol, ov, p);
+  if (rc) {
+    cudaStreamSynchronize(c->stream);
+    return rc;
+  }
   rc = evaluate(c, n, dpos, 1, n, dq, cell, p, force != nullptr, dpot, dforce, false, nullptr,
                 nullptr, background_shift(c, qsum, cell, p.alpha));
-  if (rc) return rc;
+  if (rc) {
+    cudaStreamSynchronize(c->stream);
+    return rc;
+  }
   cudaError_t e = cudaMemcpyAsync(pot, dpot, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream);
   if (e == cudaSuccess && force)
     e = cudaMemcpyAsync(force, dforce, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->stream);

@@ -85,14 +85,19 @@ int check_sums(int n, double sum_q, double sum_abs_q) {
   return EWG_OK;
 }
 
-int check_charges(int n, const double* q, double* q2sum) {
+int check_charges(int n, const double* q, double* q2sum, double* qsum) {
   if (n <= 0) return EWG_ERR_NPARTICLE;
   if (!q) return EWG_ERR_ARG;
+  // One pass, three independent chains, each summed in index order.
   double s = 0.0, a = 0.0, s2 = 0.0;
-  for (int i = 0; i < n; ++i) s += q[i];
-  for (int i = 0; i < n; ++i) a += std::fabs(q[i]);
-  for (int i = 0; i < n; ++i) s2 += q[i] * q[i];
+  for (int i = 0; i < n; ++i) {
+    const double v = q[i];
+    s += v;
+    a += std::fabs(v);
+    s2 += v * v;
+  }
   if (q2sum) *q2sum = s2;
+  if (qsum) *qsum = s;
   return check_sums(n, s, a);
 }
 

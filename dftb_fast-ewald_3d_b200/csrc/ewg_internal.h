@@ -33,7 +33,7 @@ int cell_from_cols(const double* lat_cols, Cell& cell);
 
 // check_configuration (common/ewald_validation.f90:26-48) on host charges;
 // also returns sum q^2 for the parameter chain.
-int check_charges(int n, const double* q, double* q2sum);
+int check_charges(int n, const double* q, double* q2sum, double* qsum = nullptr);
 // The same test on the three sums (sum q, sum |q|, sum q^2).
 int check_sums(int n, double sum_q, double sum_abs_q);
 
