@@ -635,17 +635,27 @@ __global__ void __launch_bounds__(kRealThreads, 4) k_real_space(const double4* _
   else
     for_each_candidate(x32, box_start, k, ai, g, pq);
   pq.flush();
-  double v[4] = {pair.pot, pair.f[0], pair.f[1], pair.f[2]};
-#pragma unroll
-  for (int j = 0; j < 4; ++j) v[j] = warp_sum(v[j]);
+  // Transposed reduction of (pot, f_x, f_y, f_z): halves and quarters of the
+  // warp each keep some of the four sums and pass the others on (6 shuffles of
+  // doubles instead of 20); lanes 0, 8, 16, 24 end with the four totals.
+  const bool hi16 = lane & 16, hi8 = lane & 8;
+  const double s0 = hi16 ? pair.pot : pair.f[1], s1 = hi16 ? pair.f[0] : pair.f[2];
+  const double k0 = hi16 ? pair.f[1] : pair.pot, k1 = hi16 ? pair.f[2] : pair.f[0];
+  const double a0 = k0 + __shfl_xor_sync(0xffffffffu, s0, 16);
+  const double a1 = k1 + __shfl_xor_sync(0xffffffffu, s1, 16);
+  double t = (hi8 ? a1 : a0) + __shfl_xor_sync(0xffffffffu, hi8 ? a0 : a1, 8);
+  t += __shfl_xor_sync(0xffffffffu, t, 4);
+  t += __shfl_xor_sync(0xffffffffu, t, 2);
+  t += __shfl_xor_sync(0xffffffffu, t, 1);
   const int bad = __any_sync(0xffffffffu, pair.bad);
-  if (lane == 0) {
+  if ((lane & 7) == 0) {
     const int i = perm[k];
-    pot[i] = v[0];
-    force[3 * i] = v[1];
-    force[3 * i + 1] = v[2];
-    force[3 * i + 2] = v[3];
-    if (bad) atomicOr(err, 1);
+    const int c = lane >> 3;  // 0: pot, 1..3: force component c - 1
+    if (c == 0)
+      pot[i] = t;
+    else
+      force[3 * i + c - 1] = t;
+    if (c == 0 && bad) atomicOr(err, 1);
   }
 }
 
