@@ -131,8 +131,10 @@ struct ewg_context {
   int batch_lanes = 4;
   std::vector<ewg_context*> lanes;
   // Pinned host copy of the device charge sums (sum q, sum |q|, sum q^2) for
-  // checks deferred to the end of a call.
+  // checks deferred to the end of a call, and the event that orders those sums
+  // on the side stream after the caller's work on `stream`.
   double* host_sums = nullptr;
+  cudaEvent_t sums_after = nullptr;
   cudaEvent_t lanes_ready = nullptr;
   std::vector<cudaEvent_t> lane_done;
   // Autotuner results per (atoms, precision, scheme, lattice, target).
@@ -158,6 +160,7 @@ struct ewg_context {
     }
     for (auto& kv : corrs) cudaFree(kv.second.dev);
     if (host_sums) cudaFreeHost(host_sums);
+    if (sums_after) cudaEventDestroy(sums_after);
     drop_graphs();
     for (ewg_context* l : lanes) delete l;
     if (lanes_ready) cudaEventDestroy(lanes_ready);
@@ -934,12 +937,22 @@ int ewg_potential_force_device(ewg_context* c, int n, const double* coords_devic
     if (!(tol > 0.0 && tol < 1.0)) return EWG_ERR_TOL;
     ewg_params p;
     if ((rc = choose_parameters(cell, 0.0, n, tol, ov, p))) return rc;
-    launch_charge_sums(charges_device, n, partial, sums, c->stream);
-    cudaError_t e = cudaMemcpyAsync(h, sums, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    // The sums run on the side stream, after the caller's work on `stream`
+    // and beside the evaluation.
+    if (!c->sums_after &&
+        cudaEventCreateWithFlags(&c->sums_after, cudaEventDisableTiming) != cudaSuccess) {
+      c->sums_after = nullptr;
+      return EWG_ERR_CUDA;
+    }
+    cudaEventRecord(c->sums_after, c->stream);
+    cudaStreamWaitEvent(c->side, c->sums_after, 0);
+    launch_charge_sums(charges_device, n, partial, sums, c->side);
+    cudaError_t e = cudaMemcpyAsync(h, sums, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->side);
     if (e != cudaSuccess) return cuda_status(e);
     const int erc = evaluate(c, n, coords_device, 3, 1, charges_device, cell, p,
                              force_device != nullptr, pot_device, force_device, false, nullptr,
                              nullptr, 0.0);
+    if ((e = cudaStreamSynchronize(c->side)) != cudaSuccess) return cuda_status(e);
     if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return cuda_status(e);
     if ((rc = check_sums(n, h[0], h[1]))) return rc;
     return erc;
