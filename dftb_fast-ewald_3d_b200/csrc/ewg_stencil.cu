@@ -17,7 +17,7 @@
 //
 // Spread: a CTA owns a tile.  FP64 runs on the tensor cores.  FP32: each lane
 // owns two x-pencils of 8 points in registers and adds q w1 w2 w3 atom by atom
-// in list order (groups of 8 atoms in FP32, the group sums in FP64), then
+// in list order (groups of 16 atoms in FP32, the group sums in FP64), then
 // writes them once (no atomics, no zeroing, fixed order).
 // Gather: a CTA of one (FP64) or two (FP32) warps stages its tile in shared
 // memory; each warp takes 64 atoms of the tile's list at a time, two per lane,
@@ -40,7 +40,7 @@ namespace {
 constexpr int TX = kTileX, TY = kTileY, TZ = kTileZ;
 constexpr int kSpreadLanes = TY * TZ / 2;  // FP32 spread: one warp, two x-pencils per lane
 constexpr int kSpreadChunk = 64;   // atoms whose weights are staged at once
-constexpr int kSpreadGroup = 8;    // FP32 spread: atoms summed in FP32 before the FP64 add
+constexpr int kSpreadGroup = 16;   // FP32 spread: atoms summed in FP32 before the FP64 add
 // Gather: atoms per lane and warps sharing one staged tile, per precision.
 template <typename R>
 struct GatherShape {
