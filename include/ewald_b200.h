@@ -102,7 +102,7 @@ int ewg_set_stream(ewg_context* ctx, void* stream);
 /* CUDA graphs (on by default): an evaluation whose launch sequence -- sizes,
  * device pointers, parameters, cell, stream -- repeats is recorded as a CUDA
  * graph on its second call and replayed from the third, one graph launch in
- * place of some thirty kernel launches.  Off with on = 0 (recorded graphs are
+ * place of some twenty kernel launches.  Off with on = 0 (recorded graphs are
  * released).  Not used while stage profiling is on. */
 int ewg_set_graphs(ewg_context* ctx, int on);
 /* Number of this library's kernels launched by the context so far. */
