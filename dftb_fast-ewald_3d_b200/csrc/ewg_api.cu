@@ -846,6 +846,38 @@ int ewg_potential_force(ewg_context* c, int n, const double* positions, const do
   Cell cell;
   double q2 = 0.0, qsum = 0.0;
   ewg_params p;
+  if (ov && ov->has_alpha && ov->has_k_cut && !c->background) {
+    // Parameters independent of the charges: the evaluation is queued first
+    // and the host checks the charges while it runs (a net charge is then
+    // reported after the cell and tolerance checks).
+    if ((rc = cell_from_rows(lat_rows, cell)) == EWG_OK && !(tol > 0.0 && tol < 1.0))
+      rc = EWG_ERR_TOL;
+    if (!rc) rc = choose_parameters(cell, 0.0, n, tol, ov, p);
+    if (!c->host_sums && cudaMallocHost(&c->host_sums, 4 * sizeof(double)) != cudaSuccess) {
+      c->host_sums = nullptr;
+      rc = rc ? rc : EWG_ERR_OUT_OF_MEMORY;
+    }
+    int* flag = rc ? nullptr : dbuf<int>(c, B_ERR, 1, &rc);
+    if (!rc) {
+      cudaMemsetAsync(flag, 0, sizeof(int), c->stream);
+      rc = evaluate(c, n, dpos, 1, n, dq, cell, p, force != nullptr, dpot, dforce, false, flag,
+                    nullptr, 0.0);
+    }
+    int* hflag = reinterpret_cast<int*>(c->host_sums ? c->host_sums + 3 : nullptr);
+    if (!rc) {
+      cudaMemcpyAsync(pot, dpot, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream);
+      if (force)
+        cudaMemcpyAsync(force, dforce, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->stream);
+      cudaMemcpyAsync(hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    }
+    const int qrc = charge_check(c, n, charges, &q2, &qsum);  // beside the GPU work
+    const cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (qrc) return qrc;
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_status(e);
+    if (*hflag) return EWG_ERR_COINCIDENT;
+    return EWG_OK;
+  }
   rc = validate_host(c, n, positions, charges, lat_rows, tol, cell, q2, qsum);
   if (!rc) rc = choose_parameters(cell, q2, n, tol, ov, p);
   if (rc) {

@@ -153,7 +153,10 @@ int ewg_reset_stage_times(ewg_context* ctx);
 
 /* ewald_potential_force (fft/ewald_fft_3d.f90:36-134).  force may be NULL:
  * potential-only evaluation with one forward transform instead of four.
- * ov may be NULL (no overrides). */
+ * ov may be NULL (no overrides).  When ov fixes alpha and k_cut and the
+ * background convention is off, the parameters do not depend on the charges:
+ * the evaluation is queued first and the charges are checked while it runs
+ * (EWG_ERR_NOT_NEUTRAL is then reported after the cell and tolerance checks). */
 int ewg_potential_force(ewg_context* ctx, int n, const double* positions, const double* charges,
                         const double* lat_rows, double tol, double* pot, double* force,
                         const ewg_overrides* ov);

@@ -77,3 +77,26 @@ def test_background_with_fixed_parameters(ewald_lib):
         assert np.max(np.abs(force.cpu().numpy() - hf)) <= 1e-12 * np.max(np.abs(hf))
     finally:
         ctx.close()
+
+
+def test_host_entry_with_fixed_parameters(ewald_lib, oracle):
+    """The host-array entry point with alpha and k_cut fixed checks the charges
+    while the evaluation runs: results match the oracle at those parameters,
+    and a net charge still fails with EWG_ERR_NOT_NEUTRAL."""
+    pos, q, lat = W.c1_small_cubic()
+    ov = {"alpha_in": 0.30, "r_cut_in": 11.0, "k_cut_in": 2.4, "windowCutoff_in": 10}
+    ctx = ewald_lib.Context(0, ewald_lib.FP64)
+    try:
+        for _ in range(3):  # direct, record + replay, replay
+            pot, force = ctx.potential_force(pos, q, lat, 1e-10, **ov)
+        po, fo = oracle.fft_potential_force(pos, q, lat, 1e-10, alpha=0.30, r_cut=11.0, k_cut=2.4,
+                                            window_cutoff=10)
+        assert np.max(np.abs(pot - po)) <= 1e-10 * np.max(np.abs(po))
+        assert np.max(np.abs(force - fo)) <= 1e-10 * np.max(np.abs(fo))
+        bad = np.asarray(q).copy()
+        bad[0] += 0.5
+        with pytest.raises(ewald_lib.EwaldError) as ei:
+            ctx.potential_force(pos, bad, lat, 1e-10, **ov)
+        assert ei.value.code == 3  # EWG_ERR_NOT_NEUTRAL
+    finally:
+        ctx.close()
