@@ -319,27 +319,52 @@ class Arm:
         return time.perf_counter() - t0
 
 
-def run_batched(args, eb, torch, device):
+def run_batched(args, eb, torch, device, dist, ws, rank):
     """Batched cells through ewg_batch_potential_force from host arrays (copies
     inside the timed region), the cells spread over the context's concurrent
-    lanes (default 4; the one-lane figure beside it).
-    c4:       256 independent triclinic cells (50-2000 atoms each), reference chain
-              per cell (FP64 tol 1e-10, mixed tol 1e-7);
-    c3_batch: 8 independent 32,769-atom water boxes (seeds 3..10); FP64 with the
+    lanes (default 4; the one-lane figure beside it).  Weak scaling: the job
+    holds 256 cells (c4) or 8 boxes (c3_batch) per GPU, partitioned over the
+    ranks by sharding.shard_of (LPT on the cost model; no collective in the
+    data path), and each rank times its own share with CUDA events on the
+    library's stream; the step time is the max over ranks.  The one gather of
+    the results (sharding.gather_results) follows the timed region.
+    c4:       independent triclinic cells (50-2000 atoms each), reference chain
+              per cell (FP64 tol 1e-10, mixed tol 1e-7); N = 1 is C4's 256 cells;
+    c3_batch: independent 32,769-atom water boxes (seeds 3, 4, ...); FP64 with the
               reference chain at tol 1e-10, mixed with the autotuner's parameters
-              and force scheme for the first box applied to all eight."""
+              and force scheme for the first box applied to all."""
+    import sharding
+
     if args.workload == "c4":
-        cells = workloads.c4_batched_cells()
-        metric = "C4 batched cells: cell shift+force evals/s (256 cells, 50-2000 atoms)"
-        label = "c4_256_triclinic_cells"
+        cells = workloads.c4_batched_cells(256 * ws)
+        metric = "C4 batched cells: cell shift+force evals/s (256 cells per GPU, 50-2000 atoms)"
+        label = "c4_256_triclinic_cells_per_gpu"
     else:
-        cells = [workloads.water_box(10923, seed=3 + k) for k in range(8)]
-        metric = "batched 32k-atom cells: shift+force evals/s (8 water boxes of 32,769 atoms)"
-        label = "c3_batch_8_water_32769"
+        cells = [workloads.water_box(10923, seed=3 + k) for k in range(8 * ws)]
+        metric = "batched 32k-atom cells: shift+force evals/s (8 water boxes of 32,769 atoms per GPU)"
+        label = "c3_batch_8_water_32769_per_gpu"
     natoms = sum(len(c[1]) for c in cells)
+    mine = sharding.shard_of(cells, TOL_FP64, sharding.library_parameters, rank, ws)
+    my_cells = [cells[i] for i in mine]
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def maxrank(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     out = {}
+    gather_s = None
     for name, prec, tol in (("fp64", eb.FP64, TOL_FP64), ("mixed", eb.MIXED, TOL_MIXED)):
         ctx = eb.Context(device, prec)
+        stream = torch.cuda.Stream(device=device)
+        ctx.set_stream(stream.cuda_stream)
         kw, note = {}, None
         if name == "mixed" and args.workload == "c3_batch":
             kw, scheme, rep = ctx.tune(*cells[0], MIXED_TARGET)
@@ -348,67 +373,126 @@ def run_batched(args, eb, torch, device):
                     "r_cut_bohr": kw["r_cut_in"], "window_cutoff": kw["windowCutoff_in"],
                     "tuner_force_rms": rep["force_rms"]}
         res = {}
+        launches = 0
         for lanes in (4, 1):
             ctx.set_batch_lanes(lanes)
             for _ in range(args.warmup):
-                ctx.batch_potential_force(cells, tol, **kw)
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
+                ctx.batch_potential_force(my_cells, tol, **kw)
+            barrier()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            l0 = ctx.kernel_launches
+            e0.record(stream)
             for _ in range(args.steps):
-                ctx.batch_potential_force(cells, tol, **kw)
+                ctx.batch_potential_force(my_cells, tol, **kw)
+            e1.record(stream)
             torch.cuda.synchronize()
-            res[lanes] = (time.perf_counter() - t0) / args.steps
+            if lanes == 4:
+                launches = ctx.kernel_launches - l0
+            res[lanes] = maxrank(e0.elapsed_time(e1) / 1e3) / args.steps
+        if name == "fp64":
+            pots, forces = ctx.batch_potential_force(my_cells, tol)
+            barrier()
+            t0 = time.perf_counter()
+            sharding.gather_results(mine, pots, forces, len(cells), ws)
+            gather_s = maxrank(time.perf_counter() - t0)
         out[name] = {"value": len(cells) / res[4], "ms_per_step": 1e3 * res[4],
-                     "one_lane_value": len(cells) / res[1]}
+                     "one_lane_value": len(cells) / res[1], "gpu_launches": launches}
         if note:
             out[name]["params"] = note
         ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    h2d = sum(len(c[1]) * 4 * 8 + 9 * 8 for c in cells)
+    d2h = natoms * 4 * 8
     line = {"metric": metric,
-            "value": out["fp64"]["value"], "unit": "cells/s", "n_gpus": 1, "steps": args.steps,
+            "value": out["fp64"]["value"], "unit": "cells/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": out["fp64"]["ms_per_step"],
-            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-            "timing": "host wall clock around the batch call, host arrays in and out; 4 lanes",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "timing": "CUDA events on the library's stream around each rank's batched calls from "
+                      "host arrays (packing and copies inside), max over ranks; 4 lanes",
             "config": {"workload": label, "cells": len(cells), "natoms_total": natoms,
-                       "tol": TOL_FP64},
+                       "tol": TOL_FP64, "parallelism": f"cells sharded over {ws} ranks (LPT)",
+                       "l2": "working set of a batch > L2 for c3_batch; c4 cells fit in L2"},
+            "e2e": {"value": out["fp64"]["value"], "unit": "cells/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": out["fp64"]["gpu_launches"],
             "one_lane_value": out["fp64"]["one_lane_value"],
+            "result_gather_s": gather_s,
             "mixed": dict(out["mixed"], unit="cells/s", tol=TOL_MIXED,
                           speedup_vs_fp64=out["mixed"]["value"] / out["fp64"]["value"])}
     print(json.dumps(line), flush=True)
     return 0
 
 
-def run_scc(args, eb, torch, device):
+def run_scc(args, eb, torch, device, dist, ws, rank):
     """C5 SCC: 216,000-site rock salt, geometry fixed, 30 charge updates per step,
     each followed by a shift (potential) evaluation through the TCoulomb-style
-    resident calls (ewg_set_charges + ewg_shift, host arrays)."""
+    resident calls (ewg_set_charges + ewg_shift, host arrays).  One cell does
+    not shard: under torchrun every rank runs a replica, each timed with CUDA
+    events on the library's stream, max over ranks."""
     pos, q, lat = workloads.c5_rock_salt_216k()
     charges = [workloads.c5_charge_update(q, k) for k in range(30)]
+
+    def maxrank(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     out = {}
     for name, prec, tol in (("fp64", eb.FP64, TOL_FP64), ("mixed", eb.MIXED, TOL_MIXED)):
         ctx = eb.Context(device, prec)
+        stream = torch.cuda.Stream(device=device)
+        ctx.set_stream(stream.cuda_stream)
         ctx.set_lattice(np.asarray(lat).T)
         ctx.set_coords(np.ascontiguousarray(np.asarray(pos)))
         for k in range(min(args.warmup, 30)):
             ctx.set_charges(charges[k])
             ctx.shift(tol, len(q))
+        if dist:
+            dist.barrier()
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        l0 = ctx.kernel_launches
+        e0.record(stream)
         nev = 0
         for _ in range(args.steps):
             for k in range(30):
                 ctx.set_charges(charges[k])
                 ctx.shift(tol, len(q))
                 nev += 1
+        e1.record(stream)
         torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
-        out[name] = {"value": nev / dt, "ms_per_eval": 1e3 * dt / nev}
+        dt = maxrank(e0.elapsed_time(e1) / 1e3)
+        out[name] = {"value": ws * nev / dt, "ms_per_eval": 1e3 * dt / nev,
+                     "gpu_launches": ctx.kernel_launches - l0}
         ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    n = len(q)
     line = {"metric": "C5 SCC: shift evals/s at 216,000 sites, fixed geometry, 30 charge updates",
-            "value": out["fp64"]["value"], "unit": "evals/s", "n_gpus": 1, "steps": args.steps,
+            "value": out["fp64"]["value"], "unit": "evals/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 30 * out["fp64"]["ms_per_eval"],
-            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-            "timing": "host wall clock around set_charges + shift, host arrays in and out",
-            "config": {"workload": "c5_rock_salt_216000_scc30", "natoms": len(q), "tol": TOL_FP64},
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "timing": "CUDA events on the library's stream around set_charges + shift, host arrays "
+                      "in and out, max over ranks",
+            "config": {"workload": "c5_rock_salt_216000_scc30", "natoms": n, "tol": TOL_FP64,
+                       "parallelism": f"replicas x{ws}",
+                       "l2": "working set (512^3 grids) > L2"},
+            "e2e": {"value": out["fp64"]["value"], "unit": "evals/s", "h2d_bytes_per_step": 30 * n * 8,
+                    "d2h_bytes_per_step": 30 * n * 8},
+            "gpu_launches": out["fp64"]["gpu_launches"],
             "mixed": {"value": out["mixed"]["value"], "unit": "evals/s", "tol": TOL_MIXED}}
     print(json.dumps(line), flush=True)
     return 0
@@ -431,9 +515,9 @@ def run_ours(args):
     torch.cuda.set_device(device)
     eb.lib()
     if args.workload in ("c4", "c3_batch"):
-        return run_batched(args, eb, torch, device)
+        return run_batched(args, eb, torch, device, dist, ws, rank)
     if args.workload == "c5_scc":
-        return run_scc(args, eb, torch, device)
+        return run_scc(args, eb, torch, device, dist, ws, rank)
     gen, label = SINGLE_CELL[args.workload]
     pos, q, lat = gen()
 
@@ -484,6 +568,13 @@ def run_ours(args):
     err = {"potential": rel(mixed.pot.cpu().numpy(), p64), "force": rel(mixed.force.cpu().numpy(), f64)}
     err_ad = {"potential": rel(fp64_ad.pot.cpu().numpy(), p64),
               "force": rel(fp64_ad.force.cpu().numpy(), f64)}
+    # FP64 direct-Ewald ground truth (the direct engine with its splitting
+    # pinned: cell-list real space, structure-factor sum over the k sphere),
+    # against which the mixed form's bar (RMS force <= 1e-6) is defined.
+    pd, fd = fp64.ctx.direct_ground_truth(pos, q, lat)
+    err_direct = {"potential": rel(mixed.pot.cpu().numpy(), pd),
+                  "force": rel(mixed.force.cpu().numpy(), fd)}
+    err64_direct = {"potential": rel(p64, pd), "force": rel(f64, fd)}
     params64 = fp64.ctx.last_params()
     params32 = mixed.ctx.last_params()
 
@@ -615,6 +706,7 @@ def run_ours(args):
                    "parallelism": f"replicas x{ws}",
                    "l2": "flushed between steps (256 MiB write, untimed); working set > L2"},
         "e2e": dict(value=ws * args.steps / te64, unit="evals/s", **e2e_io),
+        "rel_err_vs_direct": err64_direct,
         "roofline": roof64,
         "whole_eval_hbm": whole_eval(params64, 8, t64 / args.steps),
         "stages_ms": per64,
@@ -636,7 +728,7 @@ def run_ours(args):
                        "tuner_report": tune_report},
             "speedup_vs_fp64": (ws * args.steps / t32) / value,
             "e2e": dict(value=ws * args.steps / te32, unit="evals/s", **e2e_io),
-            "rel_err_vs_fp64": err, "roofline": roof32,
+            "rel_err_vs_fp64": err, "rel_err_vs_direct": err_direct, "roofline": roof32,
             "whole_eval_hbm": whole_eval(params32, 4, t32 / args.steps, nc=nc32), "stages_ms": per32,
             "gpu_launches": launches32,
         },

@@ -863,14 +863,18 @@ int ewg_potential_force(ewg_context* c, int n, const double* positions, const do
       rc = evaluate(c, n, dpos, 1, n, dq, cell, p, force != nullptr, dpot, dforce, false, flag,
                     nullptr, 0.0);
     }
+    // The charge check runs on the host while the evaluation runs on the GPU;
+    // it comes before the result copies, which wait for the evaluation when
+    // the caller's arrays are pageable, and a failed check leaves the caller's
+    // pot and force untouched.
+    const int qrc = charge_check(c, n, charges, &q2, &qsum);
     int* hflag = reinterpret_cast<int*>(c->host_sums ? c->host_sums + 3 : nullptr);
-    if (!rc) {
+    if (!rc && !qrc) {
       cudaMemcpyAsync(pot, dpot, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream);
       if (force)
         cudaMemcpyAsync(force, dforce, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->stream);
       cudaMemcpyAsync(hflag, flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
     }
-    const int qrc = charge_check(c, n, charges, &q2, &qsum);  // beside the GPU work
     const cudaError_t e = cudaStreamSynchronize(c->stream);
     if (qrc) return qrc;
     if (rc) return rc;

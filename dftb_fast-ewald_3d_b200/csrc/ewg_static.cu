@@ -25,7 +25,12 @@
 // Set-up: the device address of the array is looked up once per device, with
 // that device current, on the first call made on it (cudaGetSymbolAddress);
 // later calls reuse it.  Make that first call on each device before any stream
-// capture begins.
+// capture begins.  With CUDA's lazy module loading (the default since CUDA
+// 12.2) the 16 MiB array is only reserved on a device when this file's module
+// first loads there, which is that same first call.  A program that hands all
+// device memory to its own pool at start-up must therefore make one call on
+// each device (any small system will do) before its pool takes the memory;
+// otherwise the first call can fail with EWG_ERR_OUT_OF_MEMORY.
 
 #include <cuda_runtime.h>
 
@@ -60,7 +65,9 @@ int scratch_address(unsigned char** out) {
     const cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
     if (e != cudaSuccess || !p) {
       cudaGetLastError();
-      return EWG_ERR_CUDA;
+      // Under lazy module loading this lookup is what loads the module and
+      // reserves the array; with the device memory already taken it fails here.
+      return e == cudaErrorMemoryAllocation ? EWG_ERR_OUT_OF_MEMORY : EWG_ERR_CUDA;
     }
     g_scratch_ptr[dev] = static_cast<unsigned char*>(p);
   }

@@ -10,7 +10,7 @@
 !> one lattice vector per column, force(3,N).  No transposes are needed.
 module ewald_b200
   use, intrinsic :: iso_c_binding, only : c_int, c_double, c_ptr, c_null_ptr, c_char, &
-      & c_associated, c_f_pointer, c_long_long
+      & c_associated, c_f_pointer, c_long_long, c_loc
   implicit none
   private
 
@@ -18,7 +18,8 @@ module ewald_b200
   public :: ewaldGpuSetLattice, ewaldGpuSetCoords, ewaldGpuSetCharges
   public :: ewaldGpuShift, ewaldGpuShiftForce, ewaldGpuStress, ewaldGpuStressFast
   public :: ewaldGpuPotentialForce, ewaldGpuPotentialAt, ewaldGpuPotentialGradientAt
-  public :: ewaldGpuSetForceScheme
+  public :: ewaldGpuSetForceScheme, ewaldGpuSetBackground, ewaldGpuXlbomdGradients
+  public :: ewaldGpuExternalPotGrad, ewaldGpuPotentialForceStress, ewaldGpuBatchPotentialForce
   public :: EWG_PRECISION_FP64, EWG_PRECISION_MIXED, EWG_FORCE_IK, EWG_FORCE_AD
 
   integer(c_int), parameter :: EWG_PRECISION_FP64 = 0
@@ -120,6 +121,63 @@ module ewald_b200
       real(c_double), intent(out) :: sigma(3, 3)
       integer(c_int) :: rc
     end function ewg_stress_fast
+
+    function ewg_set_background(ctx, on) bind(C, name="ewg_set_background") result(rc)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: on
+      integer(c_int) :: rc
+    end function ewg_set_background
+
+    function ewg_xlbomd_gradients(ctx, tol, dqOut, gradients) &
+        & bind(C, name="ewg_xlbomd_gradients") result(rc)
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), value :: tol
+      real(c_double), intent(in) :: dqOut(*)
+      real(c_double), intent(inout) :: gradients(3, *)
+      integer(c_int) :: rc
+    end function ewg_xlbomd_gradients
+
+    function ewg_external_pot_grad(ctx, na, acoords, ne, ecoords, acharges, echarges, hamDeriv,&
+        & blur, latVecs, tolEwald, alpha, atomGrads, extGrads)&
+        & bind(C, name="ewg_external_pot_grad") result(rc)
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: na, ne, hamDeriv
+      real(c_double), intent(in) :: acoords(3, na), ecoords(3, ne), latVecs(3, 3)
+      type(c_ptr), value :: acharges, blur, extGrads
+      real(c_double), intent(in) :: echarges(ne)
+      real(c_double), value :: tolEwald, alpha
+      real(c_double), intent(inout) :: atomGrads(3, na)
+      integer(c_int) :: rc
+    end function ewg_external_pot_grad
+
+    function ewg_potential_force_stress(ctx, n, positions, charges, latRows, tol, pot, force,&
+        & sigma, ov) bind(C, name="ewg_potential_force_stress") result(rc)
+      import :: c_ptr, c_int, c_double, TEwgOverrides
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: n
+      real(c_double), intent(in) :: positions(n, 3), charges(n), latRows(3, 3)
+      real(c_double), value :: tol
+      real(c_double), intent(out) :: pot(n), force(3, n), sigma(3, 3)
+      type(TEwgOverrides), intent(in) :: ov
+      integer(c_int) :: rc
+    end function ewg_potential_force_stress
+
+    function ewg_batch_potential_force_ov(ctx, nCells, offsets, coords, charges, latRows, tol,&
+        & pot, force, cellStatus, ov) bind(C, name="ewg_batch_potential_force_ov") result(rc)
+      import :: c_ptr, c_int, c_double, TEwgOverrides
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: nCells
+      integer(c_int), intent(in) :: offsets(nCells + 1)
+      real(c_double), intent(in) :: coords(3, *), charges(*), latRows(9, nCells)
+      real(c_double), value :: tol
+      real(c_double), intent(out) :: pot(*), force(3, *)
+      integer(c_int), intent(out) :: cellStatus(nCells)
+      type(TEwgOverrides), intent(in) :: ov
+      integer(c_int) :: rc
+    end function ewg_batch_potential_force_ov
 
     function ewg_potential_at(ctx, nt, tcoords, ns, scoords, scharges, blur, epsSoften, latVecs,&
         & tolEwald, alpha, pot) bind(C, name="ewg_potential_at") result(rc)
@@ -257,29 +315,123 @@ contains
     call check(ewg_stress_fast(this%ctx, tol, sigma))
   end subroutine ewaldGpuStressFast
 
-  !> TCoulomb%getPotential (coulomb.F90:3122-3153) without blur or softening.
+  !> TCoulomb%getPotential (coulomb.F90:3122-3153), with the optional Gaussian
+  !> blur of each charge and the softening length.
   subroutine ewaldGpuPotentialAt(this, coords, chargeCoords, charges, latVecs, tolEwald, alpha,&
-      & potential)
+      & potential, blurWidths, epsSoften)
     type(TEwaldGpu), intent(in) :: this
     real(c_double), intent(in) :: coords(:, :), chargeCoords(:, :), charges(:), latVecs(3, 3)
     real(c_double), intent(in) :: tolEwald, alpha
     real(c_double), intent(out) :: potential(:)
+    real(c_double), intent(in), optional, target, contiguous :: blurWidths(:)
+    real(c_double), intent(in), optional, target :: epsSoften
+    type(c_ptr) :: pBlur, pEps
+    pBlur = c_null_ptr
+    pEps = c_null_ptr
+    if (present(blurWidths)) pBlur = c_loc(blurWidths)
+    if (present(epsSoften)) pEps = c_loc(epsSoften)
     call check(ewg_potential_at(this%ctx, int(size(coords, 2), c_int), coords,&
-        & int(size(chargeCoords, 2), c_int), chargeCoords, charges, c_null_ptr, c_null_ptr,&
+        & int(size(chargeCoords, 2), c_int), chargeCoords, charges, pBlur, pEps,&
         & latVecs, tolEwald, alpha, potential))
   end subroutine ewaldGpuPotentialAt
 
-  !> TCoulomb%getPotentialGradient (coulomb.F90:3157-3194) without blur.
+  !> TCoulomb%getPotentialGradient (coulomb.F90:3157-3194), with the optional blur.
   subroutine ewaldGpuPotentialGradientAt(this, coords, chargeCoords, charges, latVecs, tolEwald,&
-      & alpha, gradient)
+      & alpha, gradient, blurWidths)
     type(TEwaldGpu), intent(in) :: this
     real(c_double), intent(in) :: coords(:, :), chargeCoords(:, :), charges(:), latVecs(3, 3)
     real(c_double), intent(in) :: tolEwald, alpha
     real(c_double), intent(out) :: gradient(:, :)
+    real(c_double), intent(in), optional, target, contiguous :: blurWidths(:)
+    type(c_ptr) :: pBlur
+    pBlur = c_null_ptr
+    if (present(blurWidths)) pBlur = c_loc(blurWidths)
     call check(ewg_potential_gradient_at(this%ctx, int(size(coords, 2), c_int), coords,&
-        & int(size(chargeCoords, 2), c_int), chargeCoords, charges, c_null_ptr, latVecs, tolEwald,&
+        & int(size(chargeCoords, 2), c_int), chargeCoords, charges, pBlur, latVecs, tolEwald,&
         & alpha, gradient))
   end subroutine ewaldGpuPotentialGradientAt
+
+  !> TCoulomb%addExternalPotGrad (coulomb.F90:3198-3248).  Adds to atomGrads and,
+  !> unless tHamDeriv, to extGrads (intent inout, like the reference); with
+  !> tHamDeriv the atom charges are not used (pass any array) and extGrads is
+  !> left untouched.
+  subroutine ewaldGpuExternalPotGrad(this, atomCoords, extCoords, atomCharges, extCharges,&
+      & tHamDeriv, latVecs, tolEwald, alpha, atomGrads, extGrads, extBlurWidths)
+    type(TEwaldGpu), intent(in) :: this
+    real(c_double), intent(in) :: atomCoords(:, :), extCoords(:, :), extCharges(:), latVecs(3, 3)
+    real(c_double), intent(in), target, contiguous :: atomCharges(:)
+    logical, intent(in) :: tHamDeriv
+    real(c_double), intent(in) :: tolEwald, alpha
+    real(c_double), intent(inout) :: atomGrads(:, :)
+    real(c_double), intent(inout), target, contiguous :: extGrads(:, :)
+    real(c_double), intent(in), optional, target, contiguous :: extBlurWidths(:)
+    type(c_ptr) :: pBlur, pAtomQ, pExtGrads
+    integer(c_int) :: hamDeriv
+    pBlur = c_null_ptr
+    if (present(extBlurWidths)) pBlur = c_loc(extBlurWidths)
+    hamDeriv = 0
+    pAtomQ = c_loc(atomCharges)
+    pExtGrads = c_loc(extGrads)
+    if (tHamDeriv) then
+      hamDeriv = 1
+      pAtomQ = c_null_ptr
+      pExtGrads = c_null_ptr
+    end if
+    call check(ewg_external_pot_grad(this%ctx, int(size(atomCoords, 2), c_int), atomCoords,&
+        & int(size(extCoords, 2), c_int), extCoords, pAtomQ, extCharges, hamDeriv, pBlur,&
+        & latVecs, tolEwald, alpha, atomGrads, pExtGrads))
+  end subroutine ewaldGpuExternalPotGrad
+
+  !> Charged cells on the fast path with the stock engine's neutralising
+  !> background (on = .true.); see ewg_set_background in the C header.
+  subroutine ewaldGpuSetBackground(this, on)
+    type(TEwaldGpu), intent(in) :: this
+    logical, intent(in) :: on
+    integer(c_int) :: flag
+    flag = 0
+    if (on) flag = 1
+    call check(ewg_set_background(this%ctx, flag))
+  end subroutine ewaldGpuSetBackground
+
+  !> addGradients with dQOutAtom (coulomb.F90:697-699): adds the XLBOMD shadow
+  !> energy's gradient to gradients(3, N), for the charges set by
+  !> ewaldGpuSetCharges and dQOutAtom.
+  subroutine ewaldGpuXlbomdGradients(this, tol, dQOutAtom, gradients)
+    type(TEwaldGpu), intent(in) :: this
+    real(c_double), intent(in) :: tol
+    real(c_double), intent(in) :: dQOutAtom(:)
+    real(c_double), intent(inout) :: gradients(:, :)
+    call check(ewg_xlbomd_gradients(this%ctx, tol, dQOutAtom, gradients))
+  end subroutine ewaldGpuXlbomdGradients
+
+  !> ewald_potential_force plus the NFFT-based stress of the same evaluation
+  !> (sigma in the invRStress convention: the caller does stress - 0.5 * sigma).
+  subroutine ewaldGpuPotentialForceStress(this, positions, charges, nParticle, latVecs, tol, pot,&
+      & force, sigma)
+    type(TEwaldGpu), intent(in) :: this
+    real(c_double), intent(in) :: positions(:, :), charges(:), latVecs(3, 3), tol
+    integer, intent(in) :: nParticle
+    real(c_double), intent(out) :: pot(:), force(:, :), sigma(3, 3)
+    type(TEwgOverrides) :: ov
+    call check(ewg_potential_force_stress(this%ctx, int(nParticle, c_int), positions, charges,&
+        & latVecs, tol, pot, force, sigma, ov))
+  end subroutine ewaldGpuPotentialForceStress
+
+  !> ewald_potential_force on many independent cells in one submission: cell c
+  !> holds atoms offsets(c)+1 .. offsets(c+1) (0-based CSR offsets, size nCells+1)
+  !> of coords(3, :), latRows(:, c) its lattice in the rows layout of
+  !> ewald_potential_force (column-major 3 x 3).  Stops on the first failing cell.
+  subroutine ewaldGpuBatchPotentialForce(this, offsets, coords, charges, latRows, tol, pot, force)
+    type(TEwaldGpu), intent(in) :: this
+    integer(c_int), intent(in) :: offsets(:)
+    real(c_double), intent(in) :: coords(:, :), charges(:), latRows(:, :), tol
+    real(c_double), intent(out) :: pot(:), force(:, :)
+    integer(c_int), allocatable :: cellStatus(:)
+    type(TEwgOverrides) :: ov
+    allocate(cellStatus(size(offsets) - 1))
+    call check(ewg_batch_potential_force_ov(this%ctx, int(size(offsets) - 1, c_int), offsets,&
+        & coords, charges, latRows, tol, pot, force, cellStatus, ov))
+  end subroutine ewaldGpuBatchPotentialForce
 
   !> Same argument order as ewald_potential_force (fft/ewald_fft_3d.f90:36).
   subroutine ewaldGpuPotentialForce(this, positions, charges, nParticle, latVecs, tol, pot, force)

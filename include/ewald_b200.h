@@ -156,7 +156,8 @@ int ewg_reset_stage_times(ewg_context* ctx);
  * ov may be NULL (no overrides).  When ov fixes alpha and k_cut and the
  * background convention is off, the parameters do not depend on the charges:
  * the evaluation is queued first and the charges are checked while it runs
- * (EWG_ERR_NOT_NEUTRAL is then reported after the cell and tolerance checks). */
+ * (EWG_ERR_NOT_NEUTRAL is then reported after the cell and tolerance checks).
+ * On every error return pot and force are left as they were. */
 int ewg_potential_force(ewg_context* ctx, int n, const double* positions, const double* charges,
                         const double* lat_rows, double tol, double* pot, double* force,
                         const ewg_overrides* ov);
@@ -247,8 +248,12 @@ int ewg_direct_potential_force(ewg_context* ctx, int n, const double* positions,
  * cudaFree or other allocating routine.  All calls share that array, so calls
  * that overlap on the GPU race; run them one at a time.  The first call on a
  * device looks up the array's device address for that device; make that first
- * call before any stream capture begins.  stream is a cudaStream_t (NULL: the
- * default stream); the call returns after the work has finished. */
+ * call before any stream capture begins.  Under CUDA's lazy module loading (the
+ * default since CUDA 12.2) that first call is also what reserves the 16 MiB on
+ * the device, so a program that gives all device memory to its own pool must
+ * make one small call on each device before its pool takes the memory (else
+ * the first call can return EWG_ERR_OUT_OF_MEMORY).  stream is a cudaStream_t
+ * (NULL: the default stream); the call returns after the work has finished. */
 int ewg_direct_potential_force_static(int n, const double* coords_device,
                                       const double* charges_device, const double* lat_rows,
                                       double tol, double* pot_device, double* force_device,

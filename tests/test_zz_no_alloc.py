@@ -38,20 +38,21 @@ def _static_entry(ewald_lib):
     return fn
 
 
-def _call_static(ewald_lib, pos, q, lat, tol):
+def _call_static(ewald_lib, pos, q, lat, tol, want_force=True):
     import torch
 
     fn = _static_entry(ewald_lib)
     x = torch.tensor(np.asarray(pos), dtype=torch.float64, device="cuda").contiguous()
     qq = torch.tensor(np.asarray(q), dtype=torch.float64, device="cuda").contiguous()
     pot = torch.empty(len(q), dtype=torch.float64, device="cuda")
-    force = torch.empty((len(q), 3), dtype=torch.float64, device="cuda")
+    force = torch.empty((len(q), 3), dtype=torch.float64, device="cuda") if want_force else None
     lat_f = np.asfortranarray(np.asarray(lat, dtype=np.float64))
     torch.cuda.synchronize()
     rc = fn(len(q), x.data_ptr(), qq.data_ptr(), lat_f.ctypes.data_as(C.POINTER(C.c_double)),
-            float(tol), pot.data_ptr(), force.data_ptr(), None, None, None, None)
+            float(tol), pot.data_ptr(), force.data_ptr() if want_force else None, None, None, None,
+            None)
     torch.cuda.synchronize()
-    return rc, pot.cpu().numpy(), force.cpu().numpy()
+    return rc, pot.cpu().numpy(), force.cpu().numpy() if want_force else None
 
 
 def _triclinic(seed, n):
@@ -72,6 +73,21 @@ def test_static_matches_regular_direct_engine_on_two_calls(ewald_lib):
             ref_pot, ref_force = ctx.direct_potential_force(pos, q, lat, 1e-12)
             assert rel_max(pot, ref_pot) < TOL_REL
             assert rel_max(force, ref_force) < TOL_REL
+    finally:
+        ctx.close()
+
+
+def test_static_potential_only_matches_regular_direct_engine(ewald_lib):
+    # Without a force array the call takes its force workspace from the fixed
+    # array too; the potential must not change.
+    pos, q, lat = _triclinic(32, 500)
+    ctx = ewald_lib.Context(0, ewald_lib.FP64)
+    try:
+        for _ in range(2):
+            rc, pot, _ = _call_static(ewald_lib, pos, q, lat, 1e-12, want_force=False)
+            assert rc == 0, ewald_lib.status_string(rc)
+            ref_pot, _ = ctx.direct_potential_force(pos, q, lat, 1e-12)
+            assert rel_max(pot, ref_pot) < TOL_REL
     finally:
         ctx.close()
 
