@@ -146,13 +146,16 @@ def stage_bytes(params, natoms, real_bytes, nc=4):
     K1, K2, K3 = H[0] + 1, 2 * H[1] + 1, 2 * H[2] + 1
     s, c = real_bytes, 2 * real_bytes
     G = n[0] * n[1] * n[2] * s
+    # force grids in the fractional-derivative basis: the z pass writes 2
+    # spectra, the y inverse 3, the x C2R 4 real grids
+    nz, ny = (2, 3) if nc == 4 else (1, 1)
     return {
         "spread": G,
         "fft_x_r2c": G + n[1] * n[2] * K1 * c,
         "fft_y_fwd": n[2] * n[1] * K1 * c + n[2] * K2 * K1 * c,
-        "fft_z_influence": n[2] * K2 * K1 * c * (1 + nc),
-        "fft_y_inv": nc * n[2] * K2 * K1 * c + nc * n[2] * n[1] * K1 * c,
-        "fft_x_c2r": nc * n[2] * n[1] * K1 * c + nc * G,
+        "fft_z_influence": n[2] * K2 * K1 * c * (1 + nz),
+        "fft_y_inv": nz * n[2] * K2 * K1 * c + ny * n[2] * n[1] * K1 * c,
+        "fft_x_c2r": ny * n[2] * n[1] * K1 * c + nc * G,
         "gather": nc * G + natoms * (8 * 4 + 8 * 4),
     }
 
@@ -169,7 +172,6 @@ def stage_flops(params, natoms, nc=4):
 # through the inverse passes and the gather, stage).
 DRAM_TRAFFIC = {
     (8, 4, "gather"): 746.37e6 + 62.96e6,
-    (8, 4, "fft_x_c2r"): 356.31e6 + 660.39e6,
 }
 
 

@@ -23,7 +23,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libewald_b200.so")
 
 SOURCES = ["ewg_chain.cpp", "ewg_real.cu", "ewg_mesh.cu", "ewg_stencil.cu", "ewg_api.cu",
-           "ewg_static.cu", "ewg_external.cu"]
+           "ewg_static.cu", "ewg_external.cu", "ewg_points.cu"]
 HEADERS = ["ewg_internal.h", "ewg_kernels.h", "ewg_fft.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -26,7 +26,13 @@ enum BufId {
   B_QK, B_GRID, B_A1, B_A2, B_B2, B_B1, B_OUT, B_ERR, B_SUMS, B_PARTIAL, B_KVEC, B_SK, B_WK,
   B_P6, B_O6, B_COORDS, B_SLOT, B_PART, B_PAIRTMP, B_PAIRS, B_PAIRSTART, B_CELLERR, B_ZPART,
   B_BCOUNTS, B_BCURSOR, B_BTMP, B_EXT_T, B_EXT_S, B_EXT_SQ, B_EXT_TQ, B_EXT_BLUR, B_EXT_R,
-  B_EXT_G, B_EXT_SF, B_EXT_SF2, B_EXT_OUT, B_EXT_OUT2, B_X32S, B_TUNE_POT, B_TUNE_FORCE, B_COUNT
+  B_EXT_G, B_EXT_SF, B_EXT_SF2, B_EXT_OUT, B_EXT_OUT2, B_X32S, B_TUNE_POT, B_TUNE_FORCE,
+  // mesh-based point potentials: source (S) and target (T) tables
+  B_PT_S4, B_PT_S4S, B_PT_X32, B_PT_SKEY, B_PT_SPERM, B_PT_SBOX, B_PT_SMC, B_PT_SFR, B_PT_SWT,
+  B_PT_SQK, B_PT_SSLOT, B_PT_SPAIRS, B_PT_SPSTART, B_PT_TKEY, B_PT_TPERM, B_PT_TBOX, B_PT_TMC,
+  B_PT_TFR, B_PT_TWT, B_PT_TQK, B_PT_TSLOT, B_PT_TPAIRS, B_PT_TPSTART, B_PT_BCNT, B_PT_BCUR,
+  B_PT_BTMP, B_PT_KCNT, B_PT_KCUR, B_PT_PTMP, B_PT_QNEG, B_PT_PART, B_PT_POTSR, B_PT_GRADSR,
+  B_PT_GRAD, B_PT_POTOUT, B_COUNT
 };
 
 struct DevBuf {
@@ -129,6 +135,8 @@ struct ewg_context {
   // Batched calls: cells are spread over `batch_lanes` lanes, each a context
   // of its own (buffers, streams), so that independent cells run concurrently.
   int batch_lanes = 4;
+  // Engine of the point potentials (ewg_potential_at & co.).
+  int point_engine = EWG_POINTS_AUTO;
   std::vector<ewg_context*> lanes;
   // Pinned host copy of the device charge sums (sum q, sum |q|, sum q^2) for
   // checks deferred to the end of a call, and the event that orders those sums
@@ -491,8 +499,9 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
     prof_mark(mp.prof, st, ST_GATHER);
     launch_gather(mp, pairstart, pairs, wtab, outg, nc, part, st);
     if (concurrent) cudaStreamWaitEvent(st, c->join, 0);  // pot_sr, f_sr, err ready
+    // Both force schemes deliver the fractional derivatives D_d = dphi/ds_d.
     launch_gather_final(mp, slot, permbox, part, nparts, n, q, self_coef, pot_shift, pot_sr, f_sr,
-                        pot, want_force ? force : nullptr, ad ? cell.rec : nullptr, st);
+                        pot, want_force ? force : nullptr, want_force ? cell.rec : nullptr, st);
   };
   if (c->graphs_on && concurrent) {
     // Replay: everything the sequence depends on is in the key.
@@ -504,7 +513,7 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
       key.push_back(u);
     };
     put(n), put(sa), put(sd), put(pos), put(q), put(pot), put(want_force ? force : nullptr);
-    put(err), put(err_flag), put(stress12), put(reuse), put(mixed), put(mp.sd.ad), put(nc);
+    put(err), put(err_flag), put(stress12), put(reuse), put(mixed), put(mp.sd.ad), put(nc), put(ad);
     put(p.alpha), put(p.r_cut), put(p.k_cut), put(p.window_cutoff);
     for (int d = 0; d < 3; ++d) put(p.n_modes[d]);
     for (int i = 0; i < 3; ++i)
@@ -707,6 +716,13 @@ int ewg_set_graphs(ewg_context* c, int on) {
   if (!c) return EWG_ERR_ARG;
   c->graphs_on = on != 0;
   if (!c->graphs_on) c->drop_graphs();
+  return EWG_OK;
+}
+
+int ewg_set_point_engine(ewg_context* c, int engine) {
+  if (!c || (engine != EWG_POINTS_AUTO && engine != EWG_POINTS_STOCK && engine != EWG_POINTS_MESH))
+    return EWG_ERR_ARG;
+  c->point_engine = engine;
   return EWG_OK;
 }
 
@@ -1507,6 +1523,147 @@ int finish(ewg_context* c) {
   if (e == cudaSuccess) e = cudaGetLastError();
   return cuda_status(e);
 }
+
+// AUTO takes the mesh form from this many (target, source) pairs on.
+constexpr double kPointsMeshPairs = 1048576.0;
+
+bool use_mesh(const ewg_context* c, int nt, int ns, bool softened) {
+  if (softened) return false;  // softening is defined on the stock splitting
+  if (c->point_engine == EWG_POINTS_MESH) return true;
+  if (c->point_engine == EWG_POINTS_STOCK) return false;
+  return static_cast<double>(nt) * static_cast<double>(ns) >= kPointsMeshPairs;
+}
+
+// Mesh form of the point potentials (FP64): the potential (dpot, nt) and/or its
+// gradient (dgrad, 3 x nt) at the targets dt from the sources ds (charges dq,
+// optional Gaussian widths sblur per source or tblur per target), all device
+// arrays, written (not accumulated).  Parameters from the fast path's chain for
+// the sources at tolerance tol; the Fourier sum through the NFFT (sources
+// spread, targets gathered; window derivatives for the gradient), the real
+// sum over a source cell list (ewg_points.cu) with the cutoff widened to
+// wmax sqrt(-ln(tol/5)) for the widest blur, the background -pi Q/(V alpha^2).
+int points_mesh(ewg_context* c, const Cell& cell, double tol, int nt, const double* dt,
+                const double* tblur, int ns, const double* ds, const double* dq,
+                const double* sblur, double qsum, double q2sum, double wmax, double* dpot,
+                double* dgrad) {
+  int rc = EWG_OK;
+  cudaStream_t st = c->stream;
+  if (nt == 0) return EWG_OK;
+  if (ns == 0) {  // no sources: the reference's sums are zero
+    if (dpot) cudaMemsetAsync(dpot, 0, sizeof(double) * nt, st);
+    if (dgrad) cudaMemsetAsync(dgrad, 0, sizeof(double) * 3 * nt, st);
+    return EWG_OK;
+  }
+  if (!(tol > 0.0 && tol < 1.0)) return EWG_ERR_TOL;
+  ewg_params p;
+  if ((rc = choose_parameters(cell, q2sum, ns, tol, nullptr, p))) return rc;
+  const double r_pair = std::max(p.r_cut, wmax * std::sqrt(-std::log(0.2 * tol)));
+  RealGeom rg;
+  real_geometry(cell, r_pair, ns, rg);
+  const bool want_grad = dgrad != nullptr;
+  MeshPlan src, tgt;
+  if ((rc = mesh_geometry(cell, p, src.g))) return rc;
+  src.mixed = 0;
+  src.prof = nullptr;
+  for (int d = 0; d < 3; ++d) {
+    if ((rc = get_fft(c, src.g.n[d], src.fft[d]))) return rc;
+    const int H = src.g.M[d] - src.g.M[d] / 2;
+    if ((rc = get_corr(c, src.g.n[d], H, src.g.m, &src.corr2[d]))) return rc;
+  }
+  if ((rc = mesh_check_lengths(src.g, false))) return rc;
+  stencil_dims(src.g, false, src.sd);
+  tgt = src;
+  stencil_dims(tgt.g, want_grad, tgt.sd);
+  const int nboxes = rg.nb[0] * rg.nb[1] * rg.nb[2];
+  const int ntiles = src.sd.ntiles[0] * src.sd.ntiles[1] * src.sd.ntiles[2];
+  const int nmax = std::max(nt, ns);
+  const MeshSizes ms = mesh_sizes(src.g, src.sd, 0, 1, ns, 1);
+  const MeshSizes mt = mesh_sizes(tgt.g, tgt.sd, 0, 1, nt, want_grad ? 4 : 1);
+  const int spairs = ns * src.sd.S[0] * src.sd.S[1] * src.sd.S[2];
+  const int tpairs = nt * tgt.sd.S[0] * tgt.sd.S[1] * tgt.sd.S[2];
+  double4* s4 = dbuf<double4>(c, B_PT_S4, ns, &rc);
+  double4* s4s = dbuf<double4>(c, B_PT_S4S, ns, &rc);
+  float4* x32 = dbuf<float4>(c, B_PT_X32, ns, &rc);
+  int* skey = dbuf<int>(c, B_PT_SKEY, ns, &rc);
+  int* sperm = dbuf<int>(c, B_PT_SPERM, ns, &rc);
+  int* sbox = dbuf<int>(c, B_PT_SBOX, nboxes + 1, &rc);
+  int4* smc = dbuf<int4>(c, B_PT_SMC, ns, &rc);
+  double4* sfr = dbuf<double4>(c, B_PT_SFR, ns, &rc);
+  void* swt = dbuf<char>(c, B_PT_SWT, ms.wtab, &rc);
+  void* sqk = dbuf<char>(c, B_PT_SQK, ms.qk, &rc);
+  int4* sslot = dbuf<int4>(c, B_PT_SSLOT, ns, &rc);
+  int2* spairs_d = dbuf<int2>(c, B_PT_SPAIRS, spairs, &rc);
+  int* spstart = dbuf<int>(c, B_PT_SPSTART, ntiles + 1, &rc);
+  int* tkey = dbuf<int>(c, B_PT_TKEY, nt, &rc);
+  int* tperm = dbuf<int>(c, B_PT_TPERM, nt, &rc);
+  int* tbox = dbuf<int>(c, B_PT_TBOX, nboxes + 1, &rc);
+  int4* tmc = dbuf<int4>(c, B_PT_TMC, nt, &rc);
+  double4* tfr = dbuf<double4>(c, B_PT_TFR, nt, &rc);
+  void* twt = dbuf<char>(c, B_PT_TWT, mt.wtab, &rc);
+  void* tqk = dbuf<char>(c, B_PT_TQK, mt.qk, &rc);
+  int4* tslot = dbuf<int4>(c, B_PT_TSLOT, nt, &rc);
+  int2* tpairs_d = dbuf<int2>(c, B_PT_TPAIRS, tpairs, &rc);
+  int* tpstart = dbuf<int>(c, B_PT_TPSTART, ntiles + 1, &rc);
+  int* bcnt = dbuf<int>(c, B_PT_BCNT, nboxes, &rc);
+  int* bcur = dbuf<int>(c, B_PT_BCUR, nboxes, &rc);
+  int* btmp = dbuf<int>(c, B_PT_BTMP, nmax, &rc);
+  int* kcnt = dbuf<int>(c, B_PT_KCNT, ntiles, &rc);
+  int* kcur = dbuf<int>(c, B_PT_KCUR, ntiles, &rc);
+  int4* ptmp = dbuf<int4>(c, B_PT_PTMP, std::max(spairs, tpairs), &rc);
+  double* qneg = dbuf<double>(c, B_PT_QNEG, nt, &rc);
+  double* part = dbuf<double>(c, B_PT_PART, mt.part / 8, &rc);
+  double* potsr = dbuf<double>(c, B_PT_POTSR, nt, &rc);
+  double* gradsr = dbuf<double>(c, B_PT_GRADSR, 3 * static_cast<size_t>(nt), &rc);
+  void* grid = dbuf<char>(c, B_GRID, ms.grid, &rc);
+  void* A1 = dbuf<char>(c, B_A1, ms.A1, &rc);
+  void* A2 = dbuf<char>(c, B_A2, ms.A2, &rc);
+  void* B2 = dbuf<char>(c, B_B2, ms.B2, &rc);
+  void* B1 = dbuf<char>(c, B_B1, ms.B1, &rc);
+  void* outg = dbuf<char>(c, B_OUT, ms.out, &rc);
+  if (rc) return rc;
+  double* pot_out = dpot ? dpot : dbuf<double>(c, B_PT_POTOUT, nt, &rc);
+  if (rc) return rc;
+
+  // The targets carry charge -1 in the final assembly: it then returns
+  // pot = real + mesh + shift and grad = real + sum_d D_d b_d.
+  launch_fill(qneg, nt, -1.0, st);
+  // Sources: box order for the real-space cell list and the mesh tables.
+  launch_atom_prep(ds, 3, 1, dq, ns, cell, rg.nb, src.g.n, s4, skey, smc, sfr, st);
+  launch_bucket_sort(skey, ns, nboxes, bcnt, bcur, sbox, btmp, sperm, st);
+  launch_permute_box(s4, sperm, ns, cell.lat, s4s, x32, st);
+  // Targets: the same box order, for locality in the gather.
+  launch_atom_prep(dt, 3, 1, qneg, nt, cell, rg.nb, tgt.g.n, nullptr, tkey, tmc, tfr, st);
+  launch_bucket_sort(tkey, nt, nboxes, bcnt, bcur, tbox, btmp, tperm, st);
+  // Fourier sum: spread the sources, transform, weight, invert, gather.
+  launch_weights(src, smc, sfr, sperm, ns, swt, sqk, sslot, st);
+  launch_pair_bins(src, sslot, ns, kcnt, kcur, spstart, ptmp, spairs_d, spairs, st);
+  launch_spread(src, spstart, spairs_d, swt, sqk, grid, st);
+  launch_forward_and_weight(src, grid, A1, A2, B2, 1, st, nullptr);
+  launch_inverse(src, B2, B1, outg, 1, st);
+  launch_weights(tgt, tmc, tfr, tperm, nt, twt, tqk, tslot, st);
+  launch_pair_bins(tgt, tslot, nt, kcnt, kcur, tpstart, ptmp, tpairs_d, tpairs, st);
+  launch_gather(tgt, tpstart, tpairs_d, twt, outg, 1, part, st);
+  // Real-space sum over the source cell list.
+  PointsReal pr;
+  for (int d = 0; d < 3; ++d) {
+    pr.nb[d] = rg.nb[d];
+    pr.R[d] = rg.R[d];
+    for (int e = 0; e < 3; ++e) {
+      pr.lat[d][e] = cell.lat[d][e];
+      pr.rec[d][e] = cell.rec[d][e];
+    }
+  }
+  pr.r_cut2 = r_pair * r_pair;
+  pr.alpha = p.alpha;
+  pr.want_pot = 1;
+  pr.want_grad = want_grad ? 1 : 0;
+  launch_points_real(nt, dt, tblur, ns, s4s, sperm, ds, sblur, sbox, pr, potsr, gradsr, st);
+  const double shift = -kPi * qsum / (cell.volume * p.alpha * p.alpha);
+  launch_gather_final(tgt, tslot, tperm, part, want_grad ? 4 : 1, nt, qneg, 0.0, shift, potsr,
+                      gradsr, pot_out, dgrad, want_grad ? cell.rec : nullptr, st);
+  c->last = p;
+  return EWG_OK;
+}
 }  // namespace
 
 int ewg_potential_at(ewg_context* c, int nt, const double* tcoords, int ns, const double* scoords,
@@ -1518,7 +1675,33 @@ int ewg_potential_at(ewg_context* c, int nt, const double* tcoords, int ns, cons
   LaunchScope scope(c);
   Cell cell;
   ExtLattice L;
-  int rc = ext_setup(c, lat_cols, tol_ewald, alpha, cell, L);
+  int rc = EWG_OK;
+  if (use_mesh(c, nt, ns, eps_soften && *eps_soften != 0.0)) {
+    if ((rc = cell_from_cols(lat_cols, cell))) return rc;
+    if (!(tol_ewald > 0.0 && tol_ewald < 1.0)) return EWG_ERR_TOL;
+    if (nt == 0) return EWG_OK;
+    const double* dt = upload(c, B_EXT_T, tcoords, 3 * static_cast<size_t>(nt), &rc);
+    const double* ds = upload(c, B_EXT_S, scoords, 3 * static_cast<size_t>(ns), &rc);
+    const double* dq = upload(c, B_EXT_SQ, scharges, ns, &rc);
+    const double* db = upload(c, B_EXT_BLUR, blur, ns, &rc);
+    double* dpot = dbuf<double>(c, B_EXT_OUT, nt, &rc);
+    if (rc) return rc;
+    double qs = 0.0, q2 = 0.0, wmax = 0.0;
+    for (int i = 0; i < ns; ++i) {
+      qs += scharges[i];
+      q2 += scharges[i] * scharges[i];
+      if (blur) wmax = std::max(wmax, blur[i]);
+    }
+    rc = points_mesh(c, cell, tol_ewald, nt, dt, nullptr, ns, ds, dq, db, qs, q2, wmax, dpot,
+                     nullptr);
+    if (rc) {
+      cudaStreamSynchronize(c->stream);
+      return rc;
+    }
+    cudaMemcpyAsync(pot, dpot, sizeof(double) * nt, cudaMemcpyDeviceToHost, c->stream);
+    return finish(c);
+  }
+  rc = ext_setup(c, lat_cols, tol_ewald, alpha, cell, L);
   if (rc) return rc;
   if (nt == 0) return finish(c);
   const double* dt = upload(c, B_EXT_T, tcoords, 3 * static_cast<size_t>(nt), &rc);
@@ -1547,7 +1730,33 @@ int ewg_potential_gradient_at(ewg_context* c, int nt, const double* tcoords, int
   LaunchScope scope(c);
   Cell cell;
   ExtLattice L;
-  int rc = ext_setup(c, lat_cols, tol_ewald, alpha, cell, L);
+  int rc = EWG_OK;
+  if (use_mesh(c, nt, ns, false)) {
+    if ((rc = cell_from_cols(lat_cols, cell))) return rc;
+    if (!(tol_ewald > 0.0 && tol_ewald < 1.0)) return EWG_ERR_TOL;
+    if (nt == 0) return EWG_OK;
+    const double* dt = upload(c, B_EXT_T, tcoords, 3 * static_cast<size_t>(nt), &rc);
+    const double* ds = upload(c, B_EXT_S, scoords, 3 * static_cast<size_t>(ns), &rc);
+    const double* dq = upload(c, B_EXT_SQ, scharges, ns, &rc);
+    const double* db = upload(c, B_EXT_BLUR, blur, ns, &rc);
+    double* dg = dbuf<double>(c, B_EXT_OUT, 3 * static_cast<size_t>(nt), &rc);
+    if (rc) return rc;
+    double qs = 0.0, q2 = 0.0, wmax = 0.0;
+    for (int i = 0; i < ns; ++i) {
+      qs += scharges[i];
+      q2 += scharges[i] * scharges[i];
+      if (blur) wmax = std::max(wmax, blur[i]);
+    }
+    rc = points_mesh(c, cell, tol_ewald, nt, dt, nullptr, ns, ds, dq, db, qs, q2, wmax, nullptr,
+                     dg);
+    if (rc) {
+      cudaStreamSynchronize(c->stream);
+      return rc;
+    }
+    cudaMemcpyAsync(gradient, dg, sizeof(double) * 3 * nt, cudaMemcpyDeviceToHost, c->stream);
+    return finish(c);
+  }
+  rc = ext_setup(c, lat_cols, tol_ewald, alpha, cell, L);
   if (rc) return rc;
   if (nt == 0) return finish(c);
   const double* dt = upload(c, B_EXT_T, tcoords, 3 * static_cast<size_t>(nt), &rc);
@@ -1573,7 +1782,53 @@ int ewg_external_pot_grad(ewg_context* c, int na, const double* acoords, int ne,
   LaunchScope scope(c);
   Cell cell;
   ExtLattice L;
-  int rc = ext_setup(c, lat_cols, tol_ewald, alpha, cell, L);
+  int rc = EWG_OK;
+  if (use_mesh(c, na, ne, false)) {
+    if ((rc = cell_from_cols(lat_cols, cell))) return rc;
+    if (!(tol_ewald > 0.0 && tol_ewald < 1.0)) return EWG_ERR_TOL;
+    const double* da = upload(c, B_EXT_T, acoords, 3 * static_cast<size_t>(na), &rc);
+    const double* de = upload(c, B_EXT_S, ecoords, 3 * static_cast<size_t>(ne), &rc);
+    const double* deq = upload(c, B_EXT_SQ, echarges, ne, &rc);
+    const double* daq = ham_deriv ? nullptr : upload(c, B_EXT_TQ, acharges, na, &rc);
+    const double* db = upload(c, B_EXT_BLUR, eblur, ne, &rc);
+    double* dga = upload(c, B_EXT_OUT, agrad, 3 * static_cast<size_t>(na), &rc);
+    double* dge = ham_deriv ? nullptr : upload(c, B_EXT_OUT2, egrad, 3 * static_cast<size_t>(ne), &rc);
+    double* tmp = dbuf<double>(c, B_PT_GRAD, 3 * static_cast<size_t>(std::max(std::max(na, ne), 1)), &rc);
+    if (rc) return rc;
+    double qe = 0.0, qe2 = 0.0, wmax = 0.0, qa = 0.0, qa2 = 0.0;
+    for (int e = 0; e < ne; ++e) {
+      qe += echarges[e];
+      qe2 += echarges[e] * echarges[e];
+      if (eblur) wmax = std::max(wmax, eblur[e]);
+    }
+    // atoms: deriv0 += (ham_deriv ? 1 : q_a) sum_e q_e d(r_a - r_e), the gradient
+    // at the atoms of the external charges' potential
+    if (na) {
+      rc = points_mesh(c, cell, tol_ewald, na, da, nullptr, ne, de, deq, db, qe, qe2, wmax,
+                       nullptr, tmp);
+      if (!rc) launch_add_scaled3(na, daq, tmp, dga, c->stream);
+    }
+    // external charges: deriv1 -= q_e sum_a q_a d(r_a - r_e) = q_e times the
+    // gradient at r_e of the atoms' potential, each pair with the blur of e
+    if (!rc && !ham_deriv && ne) {
+      for (int a = 0; a < na; ++a) {
+        qa += acharges[a];
+        qa2 += acharges[a] * acharges[a];
+      }
+      rc = points_mesh(c, cell, tol_ewald, ne, de, db, na, da, daq, nullptr, qa, qa2, wmax,
+                       nullptr, tmp);
+      if (!rc) launch_add_scaled3(ne, deq, tmp, dge, c->stream);
+    }
+    if (rc) {
+      cudaStreamSynchronize(c->stream);
+      return rc;
+    }
+    if (na) cudaMemcpyAsync(agrad, dga, sizeof(double) * 3 * na, cudaMemcpyDeviceToHost, c->stream);
+    if (!ham_deriv && ne)
+      cudaMemcpyAsync(egrad, dge, sizeof(double) * 3 * ne, cudaMemcpyDeviceToHost, c->stream);
+    return finish(c);
+  }
+  rc = ext_setup(c, lat_cols, tol_ewald, alpha, cell, L);
   if (rc) return rc;
   const double* da = upload(c, B_EXT_T, acoords, 3 * static_cast<size_t>(na), &rc);
   const double* de = upload(c, B_EXT_S, ecoords, 3 * static_cast<size_t>(ne), &rc);

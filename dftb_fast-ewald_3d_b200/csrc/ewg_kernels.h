@@ -173,7 +173,8 @@ void launch_spread(const MeshPlan& mp, const int* tile_start, const int2* pairs,
 
 // Pruned forward transform of the real grid to the compact spectrum, fused with
 // the influence weights and the first inverse pass: grid -> A1 -> A2 -> B2.
-// nc = 1 (potential) or 4 (potential and three force components).
+// nc = 1 (potential) or 4 (potential and its three fractional derivatives
+// d/ds_d; B2 then holds two spectra, B1 three, the output four real grids).
 // stress_part (optional, K1 x K2 x 6 doubles, zeroed): per-CTA partials of the
 // reciprocal strain derivative, accumulated by the z pass.
 void launch_forward_and_weight(const MeshPlan& mp, const void* grid, void* A1, void* A2, void* B2,
@@ -231,6 +232,30 @@ void launch_ext_gradient(int nt, const double* tc, int ns, const double* sc, con
 void launch_ext_source_gradient(int nt, const double* tc, const double* tq, int ns,
                                 const double* sc, const double* sq, const double* blur,
                                 const ExtLattice& L, double* grad, cudaStream_t st);
+
+// Real-space half of the mesh-based point potentials (ewg_points.cu): per
+// target, the pair terms of ewaldReal / derivEwaldReal (dftb/coulomb.F90:2520-2625)
+// with splitting alpha over the sources within r_cut (cell list of the
+// sources in box order, periodic images included), plus the self term of
+// coincident points.  Writes pot (nt) and/or grad (3, nt) when asked.
+struct PointsReal {
+  int nb[3];        // source boxes per axis
+  int R[3];         // neighbour box range per axis
+  double lat[3][3];
+  double rec[3][3];
+  double r_cut2;
+  double alpha;
+  int want_pot, want_grad;
+};
+void launch_points_real(int nt, const double* tc, const double* tblur, int ns, const double4* s4s,
+                        const int* sperm, const double* sc, const double* sblur,
+                        const int* box_start, const PointsReal& g, double* pot, double* grad,
+                        cudaStream_t st);
+// x[0..n) = v.
+void launch_fill(double* x, int n, double v, cudaStream_t st);
+// dst(3, n) += scale_i src(3, n) (scale NULL: 1).
+void launch_add_scaled3(int n, const double* scale, const double* src, double* dst,
+                        cudaStream_t st);
 
 int mesh_configure_kernels();
 // Dense FP64 tensor-core (DMMA m8n8k4) rate of this GPU in TFLOP/s, timed on `st`.

@@ -16,8 +16,19 @@
 // per-axis deconvolution factors, the real part the reference takes of its
 // forward NFFT equals the standard inverse transform of c(k) Q(k) over the
 // closed box |k_d| <= M_d/2, where c(k) = ([k in S] + [-k in S]) / 2 and S is
-// the reference's mode set [-M/2, M/2-1]^3 (nfft/nfft.f90:61-75).  The force
-// components use -i k_c c(k) Q(k).  Only k1 >= 0 is stored (Hermitian half).
+// the reference's mode set [-M/2, M/2-1]^3 (nfft/nfft.f90:61-75).  Only k1 >= 0
+// is stored (Hermitian half).
+//
+// Force grids.  The reference differentiates in Fourier space along each
+// Cartesian axis, -i k_c c(k) Q(k) with k_c = 2 pi sum_d k_d b_dc
+// (fft/ewald_fft_3d_fourier.f90:130-151).  The same force follows from the
+// three fractional derivatives D_d = d(phi)/d(s_d), spectra 2 pi i k_d c Q, as
+// F = -q sum_d D_d b_d.  In that basis each multiplication by k_d commutes with
+// the transforms along the other axes, so fewer transforms are needed:
+//   z inverse  P = IFFT_z(cQ), T3 = IFFT_z(2 pi i k3 cQ)                    (2, not 4)
+//   y inverse  Y0 = IFFT_y(P), Y2 = IFFT_y(2 pi i k2 P), Y3 = IFFT_y(T3)     (3, not 4)
+//   x C2R      phi = C2R(Y0), D1 = C2R(2 pi i k1 Y0), D2 = C2R(Y2), D3 = C2R(Y3).
+// The result equals the Cartesian form up to rounding.
 
 #include <cuda_runtime.h>
 
@@ -131,9 +142,10 @@ struct InfluenceArgs {
   double* stress;
 };
 
+// nz = 1 (potential) or 2 (also T3, the spectrum times 2 pi i k3).
 template <typename R, int L, bool STRESS>
 __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
-    const cx<R>* __restrict__ A2, cx<R>* __restrict__ B2, int n3, int K1, int K2, int K3, int nc,
+    const cx<R>* __restrict__ A2, cx<R>* __restrict__ B2, int n3, int K1, int K2, int K3, int nz,
     InfluenceArgs ia, FftPlan plan) {
   chain_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -217,13 +229,7 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
       ia.stress[(static_cast<size_t>(blockIdx.y) * gridDim.x + blockIdx.x) * 6 + threadIdx.x] = t;
     }
   }
-  for (int c = 0; c < nc; ++c) {
-    R kc1 = R(0), kc2 = R(0), kc3 = R(0);
-    if (c > 0) {
-      kc1 = static_cast<R>(twoPi * ia.rec[0][c - 1]);
-      kc2 = static_cast<R>(twoPi * ia.rec[1][c - 1]);
-      kc3 = static_cast<R>(twoPi * ia.rec[2][c - 1]);
-    }
+  for (int c = 0; c < nz; ++c) {
     auto load_inv = [&](int l, int i3) {
       int k3;
       if (i3 <= h3)
@@ -234,9 +240,8 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
         return mk(R(0), R(0));
       cx<R> v = q[(k3 + h3) * L + l];
       if (c > 0) {
-        const R kc = static_cast<R>(k0 + l) * kc1 + static_cast<R>(k2) * kc2 +
-                     static_cast<R>(k3) * kc3;
-        v = mk(kc * v.y, -kc * v.x);  // -i kc v
+        const R t = static_cast<R>(twoPi * k3);
+        v = mk(-t * v.y, t * v.x);  // 2 pi i k3 v
       }
       return v;
     };
@@ -251,6 +256,8 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
 
 // ---------------------------------------------------------------------------
 // y pass inverse: zero-padded k2 box -> i2, for (k1-block, i3, component).
+// Components: 0 = IFFT_y(P) and, for forces, 1 = IFFT_y(2 pi i k2 P),
+// 2 = IFFT_y(T3), with P and T3 the z pass's two outputs.
 // ---------------------------------------------------------------------------
 template <typename R, int L>
 __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_inv(const cx<R>* __restrict__ B2,
@@ -265,10 +272,12 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_inv(const cx<R>* __re
   const int k0 = blockIdx.x * L;
   const int i3 = blockIdx.y;
   const int c = blockIdx.z;
+  const int cs = c == 2 ? 1 : 0;  // source component in B2
+  const bool dk2 = c == 1;        // times 2 pi i k2
   const int kl = k0 + static_cast<int>(threadIdx.x & (L - 1));  // this thread's k1
   const bool kin = kl < K1;
   // src points at the k2 = 0 row of this line's (i3, k1) column.
-  const cx<R>* src = B2 + ((static_cast<size_t>(c) * n3 + i3) * K2 + H2) * K1 + kl;
+  const cx<R>* src = B2 + ((static_cast<size_t>(cs) * n3 + i3) * K2 + H2) * K1 + kl;
   cx<R>* dst = B1 + (static_cast<size_t>(c) * n3 + i3) * n2 * K1 + kl;
   auto load = [&](int, int i2) {
     int k2;
@@ -278,7 +287,12 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_inv(const cx<R>* __re
       k2 = i2 - n2;
     else
       return mk(R(0), R(0));
-    return kin ? src[k2 * K1] : mk(R(0), R(0));
+    cx<R> v = kin ? src[k2 * K1] : mk(R(0), R(0));
+    if (dk2) {
+      const R t = static_cast<R>(2.0 * 3.14159265358979323846 * k2);
+      v = mk(-t * v.y, t * v.x);
+    }
+    return v;
   };
   auto store = [&](int, int i2, cx<R> v, cx<R>*) {
     if (kin) dst[i2 * K1] = v;
@@ -290,7 +304,9 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_inv(const cx<R>* __re
 // x pass, complex to real.  Lines are (row pair, component) with the component
 // fastest: line = l * NCG + cc, NP = L / NCG pairs and NCG components per CTA,
 // so neighbouring threads write the components of one grid point; output
-// interleaved with nc components per grid point.
+// interleaved with nc components per grid point.  With nc = 4 the outputs are
+// phi = C2R(Y0), D1 = C2R(2 pi i k1 Y0), D2 = C2R(Y2), D3 = C2R(Y3), Y0, Y2, Y3
+// the y pass's three components.
 // ---------------------------------------------------------------------------
 template <typename R, int L, int NCG>
 __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_c2r(const cx<R>* __restrict__ B1,
@@ -310,7 +326,10 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_c2r(const cx<R>* __re
   const int line = static_cast<int>(threadIdx.x & (L - 1));
   const int cc = line % NCG, pr = pair0 + line / NCG;
   const bool valid = pr < npairs;
-  const cx<R>* sa = B1 + (static_cast<size_t>(c0 + cc) * nrows + 2 * static_cast<size_t>(pr)) * K1;
+  const int co = c0 + cc;               // output component
+  const int cs = co <= 1 ? 0 : co - 1;  // its source component in B1
+  const bool dk1 = co == 1;             // times 2 pi i k1
+  const cx<R>* sa = B1 + (static_cast<size_t>(cs) * nrows + 2 * static_cast<size_t>(pr)) * K1;
   const cx<R>* sb = sa + K1;
   R* oa = out + 2 * static_cast<size_t>(pr) * n1 * nc + c0 + cc;
   R* ob = oa + static_cast<size_t>(n1) * nc;
@@ -322,6 +341,11 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_c2r(const cx<R>* __re
       const int kx = lo ? x : n1 - x;
       fa = sa[kx];
       fb = sb[kx];
+      if (dk1) {
+        const R t = static_cast<R>(2.0 * 3.14159265358979323846 * kx);
+        fa = mk(-t * fa.y, t * fa.x);
+        fb = mk(-t * fb.y, t * fb.x);
+      }
       if (x == 0) {
         fa.y = R(0);
         fb.y = R(0);
@@ -407,6 +431,7 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
   }
   {  // z forward + influence + z inverse
     prof_mark(mp.prof, st, ST_FFT_Z_INFL);
+    const int nz = nc == 4 ? 2 : 1;
     InfluenceArgs ia;
     for (int d = 0; d < 3; ++d) {
       ia.H[d] = g.M[d] - g.M[d] / 2;
@@ -426,10 +451,10 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
       constexpr int LL = decltype(lc)::value;
       if (stress_part)
         launch_chained(k_fft_z_influence<R, LL, true>, grd, pass_threads(LL), sm, st,
-            A2, B2, n3, g.K1, g.K2, g.K3, nc, ia, mp.fft[2]);
+            A2, B2, n3, g.K1, g.K2, g.K3, nz, ia, mp.fft[2]);
       else
         launch_chained(k_fft_z_influence<R, LL, false>, grd, pass_threads(LL), sm, st,
-            A2, B2, n3, g.K1, g.K2, g.K3, nc, ia, mp.fft[2]);
+            A2, B2, n3, g.K1, g.K2, g.K3, nz, ia, mp.fft[2]);
     });
     ++g_launches;
   }
@@ -447,7 +472,7 @@ void inverse_impl(const MeshPlan& mp, const void* B2v, void* B1v, void* out, int
     prof_mark(mp.prof, st, ST_FFT_Y_INV);
     const int L = pick_lines(n2, cb);
     const size_t sm = pass_smem(n2, L, cb, 0);
-    dim3 grd((g.K1 + L - 1) / L, n3, nc);
+    dim3 grd((g.K1 + L - 1) / L, n3, nc == 4 ? 3 : 1);
     const int H2 = (g.K2 - 1) / 2;
     with_lines(L, [&](auto lc) {
       constexpr int LL = decltype(lc)::value;
@@ -564,8 +589,9 @@ MeshSizes mesh_sizes(const MeshGeom& g, const StencilDims& sd, int mixed, int nc
   s.grid = n1 * n2 * n3 * r;
   s.A1 = n3 * n2 * g.K1 * c;
   s.A2 = n3 * g.K2 * g.K1 * c;
-  s.B2 = nc * n3 * g.K2 * g.K1 * c;
-  s.B1 = nc * n3 * n2 * g.K1 * c;
+  const size_t nz = nc == 4 ? 2 : 1, ny = nc == 4 ? 3 : 1;  // force grids in the fractional basis
+  s.B2 = nz * n3 * g.K2 * g.K1 * c;
+  s.B1 = ny * n3 * n2 * g.K1 * c;
   s.out = nc * n1 * n2 * n3 * r;
   s.wtab = static_cast<size_t>(natoms) * sd.wstride * r;
   s.qk = static_cast<size_t>(natoms) * r;

@@ -33,6 +33,9 @@ FP64 = 0
 MIXED = 1
 FORCE_IK = 0  # the reference's i k differentiation (the default)
 FORCE_AD = 1  # analytic differentiation of the window
+POINTS_AUTO = 0   # point potentials: mesh from 2^20 pairs on, stock below
+POINTS_STOCK = 1  # the reference's stock pair sum, O(N_t N_s)
+POINTS_MESH = 2   # NFFT + cell list, O(N_t + N_s)
 
 STATUS = {
     0: "EWG_OK", 1: "EWG_ERR_NPARTICLE", 2: "EWG_ERR_ARG", 3: "EWG_ERR_NOT_NEUTRAL",
@@ -54,7 +57,7 @@ EXPORTED = [
     "ewg_direct_potential_force_static", "ewg_fp64_mma_peak", "ewg_potential_force_stress",
     "ewg_stress_fast", "ewg_potential_at", "ewg_potential_gradient_at", "ewg_external_pot_grad",
     "ewg_xlbomd_gradients", "ewg_set_background", "ewg_set_force_scheme", "ewg_tune", "ewg_set_graphs", "ewg_set_batch_lanes",
-    "ewg_batch_potential_force_ov",
+    "ewg_batch_potential_force_ov", "ewg_set_point_engine",
 ]
 
 
@@ -139,6 +142,7 @@ def lib():
     L.ewg_xlbomd_gradients.argtypes = [vp, C.c_double, dp, dp]
     L.ewg_set_background.argtypes = [vp, C.c_int]
     L.ewg_set_force_scheme.argtypes = [vp, C.c_int]
+    L.ewg_set_point_engine.argtypes = [vp, C.c_int]
     L.ewg_set_graphs.argtypes = [vp, C.c_int]
     L.ewg_potential_at.argtypes = [vp, C.c_int, dp, C.c_int, dp, dp, dp, dp, dp, C.c_double,
                                    C.c_double, dp]
@@ -453,6 +457,11 @@ class Context:
     def set_graphs(self, on: bool = True):
         """Record repeated evaluations as CUDA graphs and replay them (default on)."""
         _check(lib().ewg_set_graphs(self._h, 1 if on else 0))
+
+    def set_point_engine(self, engine: int):
+        """Engine of potential_at / potential_gradient_at / external_pot_grad:
+        POINTS_AUTO (default), POINTS_STOCK or POINTS_MESH."""
+        _check(lib().ewg_set_point_engine(self._h, int(engine)))
 
     def set_force_scheme(self, scheme: int):
         """FORCE_IK (the reference's scheme) or FORCE_AD (window derivatives)."""

@@ -73,6 +73,15 @@ enum {
                        derivative along each fractional axis                     */
 };
 
+/* ---- engines of the potentials at arbitrary points ----------------------- */
+enum {
+  EWG_POINTS_AUTO = 0,  /* mesh from 2^20 (target, source) pairs on, stock below    */
+  EWG_POINTS_STOCK = 1, /* the reference's stock pair sum, O(N_t N_s) (default for
+                           small inputs)                                           */
+  EWG_POINTS_MESH = 2   /* NFFT reciprocal sum plus a cell-list real-space sum,
+                           O(N_t + N_s)                                            */
+};
+
 /* Optional arguments of ewald_potential_force (fft/ewald_fft_3d.f90:36-77):
  * alpha_in, r_cut_in, k_cut_in, nModes_in, windowCutoff_in.  A member counts
  * only when its has_ flag is non-zero. */
@@ -129,6 +138,24 @@ int ewg_set_background(ewg_context* ctx, int on);
  * order of magnitude; ewg_tune measures both and picks.
  * No counterpart in the reference. */
 int ewg_set_force_scheme(ewg_context* ctx, int scheme);
+/* Engine of ewg_potential_at, ewg_potential_gradient_at and
+ * ewg_external_pot_grad (EWG_POINTS_AUTO, _STOCK or _MESH; default AUTO).
+ * STOCK evaluates the reference's pair function ewald (dftb/coulomb.F90:2311-2343)
+ * for every (target, source) pair with DFTB+'s own splitting: O(N_t N_s) with a
+ * real-space sum over every cell translation.  MESH computes the same periodic
+ * sum, which does not depend on the splitting, at cost O(N_t + N_s): alpha,
+ * cutoffs, window and grid from the fast path's parameter chain for the
+ * sources at tol_ewald, the Fourier part through the NFFT (sources spread,
+ * targets gathered, gradients by window differentiation), the real-space part
+ * (with each source's Gaussian blur) over a cell list within the chain's
+ * cutoff widened to the widest blur, all in FP64.  The two agree to the
+ * truncation of either method at tol_ewald (about 1e-9 relative at 1e-10).
+ * The alpha argument of those calls then plays no part.  A softening length
+ * is defined on the stock splitting (the reference softens only its
+ * real-space part), so a call with eps_soften != 0 always takes the stock sum.
+ * The reference's own next step for these routines is such an operator
+ * (fft3d_readme.md:36). */
+int ewg_set_point_engine(ewg_context* ctx, int engine);
 /* Parameters the last evaluation on this context used. */
 int ewg_last_params(const ewg_context* ctx, ewg_params* out);
 /* Measured dense FP64 tensor-core rate of the context's GPU (DMMA m8n8k4 on
