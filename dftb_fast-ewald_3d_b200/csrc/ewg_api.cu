@@ -131,12 +131,21 @@ struct ewg_context {
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second.exec);
     graphs.clear();
     graph_seen.clear();
+    for (auto& kv : batch_graphs) cudaGraphExecDestroy(kv.second.exec);
+    batch_graphs.clear();
+    batch_seen.clear();
   }
   // Batched calls: cells are spread over `batch_lanes` lanes, each a context
   // of its own (buffers, streams), so that independent cells run concurrently.
   int batch_lanes = 4;
   // Engine of the point potentials (ewg_potential_at & co.).
   int point_engine = EWG_POINTS_AUTO;
+  // Batched calls: the whole batch (every lane's cells) recorded as one CUDA
+  // graph, keyed like single evaluations; on while a lane is being recorded
+  // into it (its evaluations then launch directly).
+  bool in_batch_capture = false;
+  std::map<std::vector<unsigned long long>, GraphEntry> batch_graphs;
+  std::map<std::vector<unsigned long long>, int> batch_seen;
   std::vector<ewg_context*> lanes;
   // Pinned host copy of the device charge sums (sum q, sum |q|, sum q^2) for
   // checks deferred to the end of a call, and the event that orders those sums
@@ -503,7 +512,7 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
     launch_gather_final(mp, slot, permbox, part, nparts, n, q, self_coef, pot_shift, pot_sr, f_sr,
                         pot, want_force ? force : nullptr, want_force ? cell.rec : nullptr, st);
   };
-  if (c->graphs_on && concurrent) {
+  if (c->graphs_on && concurrent && !c->in_batch_capture) {
     // Replay: everything the sequence depends on is in the key.
     std::vector<unsigned long long> key;
     auto put = [&key](auto v) {
@@ -1990,35 +1999,116 @@ int ewg_batch_potential_force_ov(ewg_context* c, int n_cells, const int* offsets
       c->lanes[l]->graphs_on = c->graphs_on;
     }
   }
-  cudaMemsetAsync(cellerr, 0, sizeof(int) * std::max(n_cells, 1), c->stream);
+  // Host side first: each cell's checks and parameters (the reference chain).
+  std::vector<int> status(n_cells, EWG_OK);
+  std::vector<Cell> cells(n_cells);
+  std::vector<ewg_params> params(n_cells);
+  for (int cidx = 0; cidx < n_cells; ++cidx) {
+    const int a0 = offsets[cidx], na = offsets[cidx + 1] - a0;
+    double q2 = 0.0;
+    int st = check_charges(na, charges + a0, &q2);
+    if (!st) st = cell_from_rows(lat_rows + 9 * static_cast<size_t>(cidx), cells[cidx]);
+    if (!st && !(tol > 0.0 && tol < 1.0)) st = EWG_ERR_TOL;
+    if (!st) st = choose_parameters(cells[cidx], q2, na, tol, ov, params[cidx]);
+    status[cidx] = st;
+  }
   cudaMemcpyAsync(dcoords, coords, sizeof(double) * 3 * total, cudaMemcpyHostToDevice, c->stream);
   cudaMemcpyAsync(dq, charges, sizeof(double) * total, cudaMemcpyHostToDevice, c->stream);
-  if (nl > 1) {
-    cudaEventRecord(c->lanes_ready, c->stream);
-    for (int l = 0; l < nl; ++l) cudaStreamWaitEvent(c->lanes[l]->stream, c->lanes_ready, 0);
-  }
-  std::vector<int> status(n_cells, EWG_OK);
-  for (int cidx = 0; cidx < n_cells; ++cidx) {
-    ewg_context* lc = nl > 1 ? c->lanes[cidx % nl] : c;
-    const int a0 = offsets[cidx], na = offsets[cidx + 1] - a0;
-    Cell cell;
-    double q2 = 0.0;
-    int s = check_charges(na, charges + a0, &q2);
-    if (!s) s = cell_from_rows(lat_rows + 9 * static_cast<size_t>(cidx), cell);
-    if (!s && !(tol > 0.0 && tol < 1.0)) s = EWG_ERR_TOL;
-    ewg_params p;
-    if (!s) s = choose_parameters(cell, q2, na, tol, ov, p);
-    if (!s)
-      s = evaluate(lc, na, dcoords + 3 * static_cast<size_t>(a0), 3, 1, dq + a0, cell, p,
-                   force != nullptr, dpot + a0, dforce + 3 * static_cast<size_t>(a0), false,
-                   cellerr + cidx);
-    status[cidx] = s;
-  }
-  if (nl > 1) {
-    for (int l = 0; l < nl; ++l) {
-      cudaEventRecord(c->lane_done[l], c->lanes[l]->stream);
-      cudaStreamWaitEvent(c->stream, c->lane_done[l], 0);
+  // The device work of the whole batch: the cells round-robin on the lanes,
+  // forked from and joined back to the context's stream.
+  auto launch_batch = [&]() -> int {
+    int bad = EWG_OK;
+    cudaMemsetAsync(cellerr, 0, sizeof(int) * std::max(n_cells, 1), c->stream);
+    if (nl > 1) {
+      cudaEventRecord(c->lanes_ready, c->stream);
+      for (int l = 0; l < nl; ++l) cudaStreamWaitEvent(c->lanes[l]->stream, c->lanes_ready, 0);
     }
+    for (int cidx = 0; cidx < n_cells; ++cidx) {
+      if (status[cidx]) continue;
+      ewg_context* lc = nl > 1 ? c->lanes[cidx % nl] : c;
+      const int a0 = offsets[cidx], na = offsets[cidx + 1] - a0;
+      const int er = evaluate(lc, na, dcoords + 3 * static_cast<size_t>(a0), 3, 1, dq + a0,
+                              cells[cidx], params[cidx], force != nullptr, dpot + a0,
+                              dforce + 3 * static_cast<size_t>(a0), false, cellerr + cidx);
+      if (er) {
+        status[cidx] = er;
+        bad = er;
+      }
+    }
+    if (nl > 1) {
+      for (int l = 0; l < nl; ++l) {
+        cudaEventRecord(c->lane_done[l], c->lanes[l]->stream);
+        cudaStreamWaitEvent(c->stream, c->lane_done[l], 0);
+      }
+    }
+    return bad;
+  };
+  // A repeated batch (same cells, parameters, buffers and settings) is
+  // recorded as one CUDA graph on its second call and replayed from the
+  // third: one graph launch in place of every cell's launches and host work.
+  const bool graphed = c->graphs_on && !c->prof.on;
+  if (graphed) {
+    std::vector<unsigned long long> key;
+    auto put = [&key](auto v) {
+      unsigned long long u = 0;
+      static_assert(sizeof(v) <= sizeof(u), "key field");
+      std::memcpy(&u, &v, sizeof(v));
+      key.push_back(u);
+    };
+    put(n_cells), put(nl), put(tol), put(force != nullptr), put(c->precision);
+    put(c->force_scheme), put(c->background), put(c->buf_gen), put(c->stream);
+    for (int l = 0; l < nl && nl > 1; ++l) put(c->lanes[l]->buf_gen), put(c->lanes[l]->stream);
+    for (int cidx = 0; cidx < n_cells; ++cidx) {
+      const ewg_params& p = params[cidx];
+      put(offsets[cidx]), put(status[cidx]), put(p.alpha), put(p.r_cut), put(p.k_cut);
+      put(p.window_cutoff), put(p.n_modes[0]), put(p.n_modes[1]), put(p.n_modes[2]);
+      for (int i = 0; i < 9; ++i) put(lat_rows[9 * static_cast<size_t>(cidx) + i]);
+    }
+    put(offsets[n_cells]);
+    auto hit = c->batch_graphs.find(key);
+    if (hit != c->batch_graphs.end()) {
+      cudaGraphLaunch(hit->second.exec, c->stream);
+      g_launches += hit->second.launches;
+    } else if (c->batch_seen.count(key)) {
+      if (c->batch_graphs.size() >= 16) {
+        for (auto& kv : c->batch_graphs) cudaGraphExecDestroy(kv.second.exec);
+        c->batch_graphs.clear();
+      }
+      const long long before = g_launches;
+      auto set_capture = [&](bool on) {
+        c->in_batch_capture = on;
+        for (int l = 0; l < nl && nl > 1; ++l) c->lanes[l]->in_batch_capture = on;
+      };
+      cudaGraph_t graph = nullptr;
+      cudaGraphExec_t exec = nullptr;
+      bool ok = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+      if (ok) {
+        set_capture(true);
+        const int bad = launch_batch();
+        set_capture(false);
+        ok = cudaStreamEndCapture(c->stream, &graph) == cudaSuccess && graph && bad == EWG_OK &&
+             cudaGraphInstantiateWithFlags(&exec, graph, cudaGraphInstantiateFlagUseNodePriority) ==
+                 cudaSuccess;
+      }
+      if (graph) cudaGraphDestroy(graph);
+      const long long recorded = g_launches - before;
+      g_launches = before;
+      if (ok) {
+        c->batch_graphs[key] = ewg_context::GraphEntry{exec, recorded};
+        cudaGraphLaunch(exec, c->stream);
+        g_launches += recorded;
+      } else {  // recording failed: run the batch directly
+        if (exec) cudaGraphExecDestroy(exec);
+        cudaGetLastError();
+        launch_batch();
+      }
+    } else {
+      if (c->batch_seen.size() >= 64) c->batch_seen.clear();
+      c->batch_seen[key] = 1;
+      launch_batch();
+    }
+  } else {
+    launch_batch();
   }
   std::vector<int> herr(std::max(n_cells, 1), 0);
   cudaError_t e = cudaMemcpyAsync(pot, dpot, sizeof(double) * total, cudaMemcpyDeviceToHost, c->stream);
