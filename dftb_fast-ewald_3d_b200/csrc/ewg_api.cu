@@ -32,7 +32,9 @@ enum BufId {
   B_PT_SQK, B_PT_SSLOT, B_PT_SPAIRS, B_PT_SPSTART, B_PT_TKEY, B_PT_TPERM, B_PT_TBOX, B_PT_TMC,
   B_PT_TFR, B_PT_TWT, B_PT_TQK, B_PT_TSLOT, B_PT_TPAIRS, B_PT_TPSTART, B_PT_BCNT, B_PT_BCUR,
   B_PT_BTMP, B_PT_KCNT, B_PT_KCUR, B_PT_PTMP, B_PT_QNEG, B_PT_PART, B_PT_POTSR, B_PT_GRADSR,
-  B_PT_GRAD, B_PT_POTOUT, B_COUNT
+  B_PT_GRAD, B_PT_POTOUT,
+  // segmented batches: cell table and launch prefixes
+  B_BT_CELLS, B_BT_PREFIX, B_COUNT
 };
 
 struct DevBuf {
@@ -137,7 +139,7 @@ struct ewg_context {
   }
   // Batched calls: cells are spread over `batch_lanes` lanes, each a context
   // of its own (buffers, streams), so that independent cells run concurrently.
-  int batch_lanes = 4;
+  int batch_lanes = 0;  // 0: segmented launches (one per stage for all cells)
   // Engine of the point potentials (ewg_potential_at & co.).
   int point_engine = EWG_POINTS_AUTO;
   // Batched calls: the whole batch (every lane's cells) recorded as one CUDA
@@ -363,6 +365,7 @@ void stencil_dims(const MeshGeom& g, bool ad, StencilDims& sd) {
     off += most * T;
   }
   sd.wstride = off;
+  sd.pstride = sd.S[0] * sd.S[1] * sd.S[2];
   sd.ad = ad ? 1 : 0;
   sd.dwoff = off;
   if (ad) sd.wstride = 2 * off;  // derivative rows follow the weight rows
@@ -630,6 +633,267 @@ int validate_host(const ewg_context* c, int n, const double* pos, const double* 
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------------------
+// Segmented batches.  Every cell of a batched call in one launch per stage:
+// the host builds the cell table (geometry, parameters, FFT plans, buffer
+// pointers) and each launch's prefix array, uploads them on the context's
+// stream, and the stage kernels map their global index to (cell, local).
+// Buffers: the per-atom arrays over all atoms, one box and one tile key space
+// over all cells, and each cell's grids at its offset in the shared buffers.
+// ---------------------------------------------------------------------------
+struct SegPlan {
+  BatchLaunch b;
+  std::vector<BatchCell> cells;
+  std::vector<int> prefix;  // 11 arrays of ncells + 1
+  size_t wstride = 0;       // common weight stride (values per atom)
+  int pstride = 0;          // common partial slots per atom
+  size_t pairs_max = 0;
+  size_t grid = 0, A1 = 0, A2 = 0, B2 = 0, B1 = 0, out = 0;  // total bytes
+};
+
+// Offsets of the 11 prefix arrays inside SegPlan::prefix.
+enum { SP_ATOMS, SP_WEIGHTS, SP_SLOTS, SP_TILES, SP_R2C, SP_YFWD, SP_Z, SP_YINV, SP_C2R, SP_BOXES,
+       SP_COUNT };
+
+inline size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+// Host part: per cell its real-space and mesh geometry (from the parameters
+// the reference chain gave), plans, and the batch's common launch shapes.
+int seg_plan(ewg_context* c, int n_cells, const int* offsets, const std::vector<Cell>& cells,
+             const std::vector<ewg_params>& params, bool want_force, SegPlan& sp) {
+  const int mixed = c->precision == EWG_PRECISION_MIXED;
+  const bool ad = want_force && c->force_scheme == EWG_FORCE_AD;
+  const int nc = want_force && !ad ? 4 : 1;
+  const int nparts = want_force ? 4 : 1;
+  const size_t rs = mixed ? 4 : 8;
+  sp.cells.assign(n_cells, BatchCell{});
+  int L = 8, nmax[3] = {0, 0, 0}, lpa = 8;
+  std::vector<int> nboxes(n_cells);
+  for (int ci = 0; ci < n_cells; ++ci) {
+    BatchCell& bc = sp.cells[ci];
+    const ewg_params& p = params[ci];
+    const int na = offsets[ci + 1] - offsets[ci];
+    bc.atom0 = offsets[ci];
+    bc.natoms = na;
+    for (int i = 0; i < 3; ++i)
+      for (int d = 0; d < 3; ++d) {
+        bc.lat[i][d] = cells[ci].lat[i][d];
+        bc.rec[i][d] = cells[ci].rec[i][d];
+      }
+    real_geometry(cells[ci], p.r_cut, na, bc.rg);
+    bc.alpha = p.alpha;
+    bc.cut2 = p.r_cut * p.r_cut;
+    bc.pre2 = real_prefilter_bound(bc.rg, p.r_cut);
+    bc.self_coef = -2.0 * p.alpha / std::sqrt(kPi);
+    int rc = mesh_geometry(cells[ci], p, bc.g);
+    if (rc) return rc;
+    if ((rc = mesh_check_lengths(bc.g, mixed))) return rc;
+    for (int d = 0; d < 3; ++d) {
+      FftPlan fp;
+      if ((rc = get_fft(c, bc.g.n[d], fp))) return rc;
+      bc.fft[d] = fp;
+      const int H = bc.g.M[d] - bc.g.M[d] / 2;
+      if ((rc = get_corr(c, bc.g.n[d], H, bc.g.m, &bc.corr2[d]))) return rc;
+      nmax[d] = std::max(nmax[d], bc.g.n[d]);
+    }
+    stencil_dims(bc.g, ad, bc.sd);
+    sp.wstride = std::max<size_t>(sp.wstride, bc.sd.wstride);
+    sp.pstride = std::max(sp.pstride, bc.sd.pstride);
+    if (bc.sd.pstride > 32) lpa = 32;
+    L = std::min(L, mesh_batch_lines(bc.g.n[0], mixed, 0));
+    L = std::min(L, mesh_batch_lines(bc.g.n[1], mixed, 0));
+    L = std::min(L, mesh_batch_lines(bc.g.n[2], mixed, bc.g.K3));
+    nboxes[ci] = bc.rg.nb[0] * bc.rg.nb[1] * bc.rg.nb[2];
+  }
+  if (L < 1) return EWG_ERR_GRID_TOO_LARGE;
+  // Prefixes, key offsets, buffer offsets.
+  sp.prefix.assign(static_cast<size_t>(SP_COUNT) * (n_cells + 1), 0);
+  auto pre = [&](int a) { return sp.prefix.data() + static_cast<size_t>(a) * (n_cells + 1); };
+  size_t og = 0, oA1 = 0, oA2 = 0, oB2 = 0, oB1 = 0, oout = 0;
+  const int nz = nc == 4 ? 2 : 1, ny = nc == 4 ? 3 : 1;
+  size_t smz = 0;
+  for (int ci = 0; ci < n_cells; ++ci) {
+    BatchCell& bc = sp.cells[ci];
+    bc.sd.wstride = static_cast<int>(sp.wstride);
+    bc.sd.pstride = sp.pstride;
+    const StencilDims& sd = bc.sd;
+    const MeshGeom& g = bc.g;
+    const int na = bc.natoms;
+    const int ntiles = sd.ntiles[0] * sd.ntiles[1] * sd.ntiles[2];
+    const int SS = sd.S[0] + sd.S[1] + sd.S[2], S3 = sd.S[0] * sd.S[1] * sd.S[2];
+    int blk[5];
+    mesh_pass_blocks(g, L, nc, blk);
+    bc.box0 = pre(SP_BOXES)[ci];
+    bc.tile0 = pre(SP_TILES)[ci];
+    pre(SP_ATOMS)[ci + 1] = pre(SP_ATOMS)[ci] + na;
+    pre(SP_WEIGHTS)[ci + 1] = pre(SP_WEIGHTS)[ci] + na * SS;
+    pre(SP_SLOTS)[ci + 1] = pre(SP_SLOTS)[ci] + na * S3;
+    pre(SP_TILES)[ci + 1] = pre(SP_TILES)[ci] + ntiles;
+    pre(SP_R2C)[ci + 1] = pre(SP_R2C)[ci] + blk[0];
+    pre(SP_YFWD)[ci + 1] = pre(SP_YFWD)[ci] + blk[1];
+    pre(SP_Z)[ci + 1] = pre(SP_Z)[ci] + blk[2];
+    pre(SP_YINV)[ci + 1] = pre(SP_YINV)[ci] + blk[3];
+    pre(SP_C2R)[ci + 1] = pre(SP_C2R)[ci] + blk[4];
+    pre(SP_BOXES)[ci + 1] = pre(SP_BOXES)[ci] + nboxes[ci];
+    const size_t G = static_cast<size_t>(g.n[0]) * g.n[1] * g.n[2];
+    const size_t cb = 2 * rs;
+    // offsets for now; turned into pointers once the buffers exist
+    bc.grid = reinterpret_cast<void*>(og);
+    bc.A1 = reinterpret_cast<void*>(oA1);
+    bc.A2 = reinterpret_cast<void*>(oA2);
+    bc.B2 = reinterpret_cast<void*>(oB2);
+    bc.B1 = reinterpret_cast<void*>(oB1);
+    bc.out = reinterpret_cast<void*>(oout);
+    og += align256(G * rs);
+    oA1 += align256(static_cast<size_t>(g.n[2]) * g.n[1] * g.K1 * cb);
+    oA2 += align256(static_cast<size_t>(g.n[2]) * g.K2 * g.K1 * cb);
+    oB2 += align256(nz * static_cast<size_t>(g.n[2]) * g.K2 * g.K1 * cb);
+    oB1 += align256(ny * static_cast<size_t>(g.n[2]) * g.n[1] * g.K1 * cb);
+    oout += align256(nc * G * rs);
+    smz = std::max(smz, mesh_pass_smem(g.n[2], L, mixed, g.K3));
+  }
+  sp.grid = og, sp.A1 = oA1, sp.A2 = oA2, sp.B2 = oB2, sp.B1 = oB1, sp.out = oout;
+  BatchLaunch& b = sp.b;
+  b.ncells = n_cells;
+  b.mixed = mixed;
+  b.nc = nc;
+  b.nparts = nparts;
+  b.ad = ad ? 1 : 0;
+  b.L = L;
+  b.lpa = lpa;
+  for (int d = 0; d < 3; ++d) b.smem[d] = mesh_pass_smem(nmax[d], L, mixed, 0);
+  b.smem_z = smz;
+  b.n_atoms = pre(SP_ATOMS)[n_cells];
+  b.n_weights = pre(SP_WEIGHTS)[n_cells];
+  b.n_slots = pre(SP_SLOTS)[n_cells];
+  b.n_tiles = pre(SP_TILES)[n_cells];
+  b.n_r2c = pre(SP_R2C)[n_cells];
+  b.n_yfwd = pre(SP_YFWD)[n_cells];
+  b.n_z = pre(SP_Z)[n_cells];
+  b.n_yinv = pre(SP_YINV)[n_cells];
+  b.n_c2r = pre(SP_C2R)[n_cells];
+  b.n_boxes = pre(SP_BOXES)[n_cells];
+  b.n_final = static_cast<long>(lpa) * b.n_atoms;
+  sp.pairs_max = static_cast<size_t>(b.n_slots);
+  return EWG_OK;
+}
+
+// Device buffers of a segmented batch.
+struct SegBufs {
+  double4 *s4, *s4s, *fr;
+  float4* x32;
+  int *boxkey, *perm, *boxstart, *bcounts, *bcursor, *btmp;
+  int4 *mc, *slot, *pairtmp;
+  int *tcounts, *tcursor, *pairstart;
+  int2* pairs;
+  void *wtab, *qk;
+  double *part, *pot_sr, *f_sr;
+};
+
+// Sizes the buffers, turns the table's offsets into pointers and uploads the
+// table and prefixes on the context's stream (outside any graph capture).
+int seg_prepare(ewg_context* c, SegPlan& sp, SegBufs& sb) {
+  int rc = EWG_OK;
+  const BatchLaunch& b = sp.b;
+  const size_t rs = b.mixed ? 4 : 8;
+  const size_t na = std::max(b.n_atoms, 1);
+  sb.s4 = dbuf<double4>(c, B_S4, na, &rc);
+  sb.s4s = dbuf<double4>(c, B_S4S, na, &rc);
+  sb.x32 = dbuf<float4>(c, B_X32S, na, &rc);
+  sb.boxkey = dbuf<int>(c, B_BOXKEY, na, &rc);
+  sb.perm = dbuf<int>(c, B_PERMBOX, na, &rc);
+  sb.mc = dbuf<int4>(c, B_MC, na, &rc);
+  sb.fr = dbuf<double4>(c, B_FR, na, &rc);
+  sb.slot = dbuf<int4>(c, B_SLOT, na, &rc);
+  sb.btmp = dbuf<int>(c, B_BTMP, na, &rc);
+  sb.boxstart = dbuf<int>(c, B_BOXSTART, b.n_boxes + 1, &rc);
+  sb.bcounts = dbuf<int>(c, B_BCOUNTS, std::max(b.n_boxes, 1), &rc);
+  sb.bcursor = dbuf<int>(c, B_BCURSOR, std::max(b.n_boxes, 1), &rc);
+  sb.tcounts = dbuf<int>(c, B_COUNTS, std::max(b.n_tiles, 1), &rc);
+  sb.tcursor = dbuf<int>(c, B_CURSOR, std::max(b.n_tiles, 1), &rc);
+  sb.pairstart = dbuf<int>(c, B_PAIRSTART, b.n_tiles + 1, &rc);
+  sb.pairtmp = dbuf<int4>(c, B_PAIRTMP, std::max<size_t>(sp.pairs_max, 1), &rc);
+  sb.pairs = dbuf<int2>(c, B_PAIRS, std::max<size_t>(sp.pairs_max, 1), &rc);
+  sb.wtab = dbuf<char>(c, B_WTAB, na * sp.wstride * rs, &rc);
+  sb.qk = dbuf<char>(c, B_QK, na * rs, &rc);
+  sb.part = dbuf<double>(c, B_PART, na * sp.pstride * b.nparts, &rc);
+  sb.pot_sr = dbuf<double>(c, B_POT_SR, na, &rc);
+  sb.f_sr = dbuf<double>(c, B_F_SR, 3 * na, &rc);
+  char* grid = dbuf<char>(c, B_GRID, sp.grid, &rc);
+  char* A1 = dbuf<char>(c, B_A1, sp.A1, &rc);
+  char* A2 = dbuf<char>(c, B_A2, sp.A2, &rc);
+  char* B2 = dbuf<char>(c, B_B2, sp.B2, &rc);
+  char* B1 = dbuf<char>(c, B_B1, sp.B1, &rc);
+  char* out = dbuf<char>(c, B_OUT, sp.out, &rc);
+  BatchCell* dcells = dbuf<BatchCell>(c, B_BT_CELLS, sp.cells.size(), &rc);
+  int* dpre = dbuf<int>(c, B_BT_PREFIX, sp.prefix.size(), &rc);
+  if (rc) return rc;
+  for (BatchCell& bc : sp.cells) {
+    bc.grid = grid + reinterpret_cast<size_t>(bc.grid);
+    bc.A1 = A1 + reinterpret_cast<size_t>(bc.A1);
+    bc.A2 = A2 + reinterpret_cast<size_t>(bc.A2);
+    bc.B2 = B2 + reinterpret_cast<size_t>(bc.B2);
+    bc.B1 = B1 + reinterpret_cast<size_t>(bc.B1);
+    bc.out = out + reinterpret_cast<size_t>(bc.out);
+  }
+  cudaMemcpyAsync(dcells, sp.cells.data(), sizeof(BatchCell) * sp.cells.size(),
+                  cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(dpre, sp.prefix.data(), sizeof(int) * sp.prefix.size(), cudaMemcpyHostToDevice,
+                  c->stream);
+  const int n1 = b.ncells + 1;
+  BatchLaunch& bl = sp.b;
+  bl.cells = dcells;
+  bl.p_atoms = dpre + SP_ATOMS * n1;
+  bl.p_weights = dpre + SP_WEIGHTS * n1;
+  bl.p_slots = dpre + SP_SLOTS * n1;
+  bl.p_tiles = dpre + SP_TILES * n1;
+  bl.p_r2c = dpre + SP_R2C * n1;
+  bl.p_yfwd = dpre + SP_YFWD * n1;
+  bl.p_z = dpre + SP_Z * n1;
+  bl.p_yinv = dpre + SP_YINV * n1;
+  bl.p_c2r = dpre + SP_C2R * n1;
+  bl.p_final = bl.p_atoms;
+  return EWG_OK;
+}
+
+// The stage sequence of a segmented batch (no host synchronisation, no
+// allocation): the real-space branch on the side stream beside the mesh chain.
+void seg_kernels(ewg_context* c, const SegPlan& sp, const SegBufs& sb, const double* coords,
+                 const double* q, double* pot, double* force, int* cellerr) {
+  const BatchLaunch& b = sp.b;
+  // With stage timing on, everything runs in line on the context's stream.
+  Profiler* prof = &c->prof;
+  const bool concurrent = !prof->on;
+  cudaStream_t st = c->stream, rs = concurrent ? c->side : c->stream;
+  cudaMemsetAsync(cellerr, 0, sizeof(int) * std::max(b.ncells, 1), st);
+  prof_mark(prof, st, ST_PREP);
+  launch_atom_prep_seg(b, coords, q, sb.s4, sb.boxkey, sb.mc, sb.fr, st);
+  launch_bucket_sort(sb.boxkey, b.n_atoms, b.n_boxes, sb.bcounts, sb.bcursor, sb.boxstart, sb.btmp,
+                     sb.perm, st);
+  if (concurrent) {
+    cudaEventRecord(c->fork, st);
+    cudaStreamWaitEvent(rs, c->fork, 0);
+  }
+  launch_permute_box_seg(b, sb.s4, sb.perm, sb.s4s, sb.x32, rs);
+  prof_mark(prof, st, ST_REAL);
+  launch_real_space_seg(b, sb.s4s, sb.x32, sb.perm, sb.boxstart, sb.pot_sr, sb.f_sr, cellerr, rs);
+  if (concurrent) cudaEventRecord(c->join, rs);
+  prof_mark(prof, st, ST_WEIGHTS);
+  launch_weights_seg(b, sb.mc, sb.fr, sb.perm, sb.wtab, sb.qk, sb.slot, st);
+  launch_pair_bins_seg(b, sb.slot, sb.tcounts, sb.tcursor, sb.pairstart, sb.pairtmp, sb.pairs, st);
+  prof_mark(prof, st, ST_SPREAD);
+  launch_spread_seg(b, sb.pairstart, sb.pairs, sb.wtab, sb.qk, st);
+  prof_mark(prof, st, ST_FFT_X_R2C);  // the three forward passes together
+  launch_forward_and_weight_seg(b, st);
+  prof_mark(prof, st, ST_FFT_Y_INV);  // both inverse passes together
+  launch_inverse_seg(b, st);
+  prof_mark(prof, st, ST_GATHER);
+  launch_gather_seg(b, sb.pairstart, sb.pairs, sb.wtab, sb.part, st);
+  if (concurrent) cudaStreamWaitEvent(st, c->join, 0);
+  launch_gather_final_seg(b, sb.slot, sb.perm, sb.part, q, sb.pot_sr, sb.f_sr, pot, force, st);
+  prof_mark(prof, st, -1);
+}
 
 // ===========================================================================
 // C ABI
@@ -1946,7 +2210,7 @@ int ewg_last_stress_setup(const ewg_context* c, double* alpha, double* max_r, do
 // ---- batched form ----------------------------------------------------------
 
 int ewg_set_batch_lanes(ewg_context* c, int lanes) {
-  if (!c || lanes < 1 || lanes > 16) return EWG_ERR_ARG;
+  if (!c || lanes < 0 || lanes > 16) return EWG_ERR_ARG;
   c->batch_lanes = lanes;
   return EWG_OK;
 }
@@ -1980,7 +2244,33 @@ int ewg_batch_potential_force_ov(ewg_context* c, int n_cells, const int* offsets
   // The lanes: the context itself when one lane is asked for (or profiling is
   // on, which times stages on the context's own stream), else sub-contexts of
   // the same device, form and settings, each with its own buffers and streams.
-  const int nl = c->prof.on ? 1 : std::min(c->batch_lanes, std::max(n_cells, 1));
+  // Host side first: each cell's checks and parameters (the reference chain).
+  std::vector<int> status(n_cells, EWG_OK);
+  std::vector<Cell> cells(n_cells);
+  std::vector<ewg_params> params(n_cells);
+  bool all_ok = n_cells > 0;
+  for (int cidx = 0; cidx < n_cells; ++cidx) {
+    const int a0 = offsets[cidx], na = offsets[cidx + 1] - a0;
+    double q2 = 0.0;
+    int st = na > 0 ? check_charges(na, charges + a0, &q2) : EWG_ERR_NPARTICLE;
+    if (!st) st = cell_from_rows(lat_rows + 9 * static_cast<size_t>(cidx), cells[cidx]);
+    if (!st && !(tol > 0.0 && tol < 1.0)) st = EWG_ERR_TOL;
+    if (!st) st = choose_parameters(cells[cidx], q2, na, tol, ov, params[cidx]);
+    status[cidx] = st;
+    all_ok = all_ok && st == EWG_OK;
+  }
+  // Segmented launches (one per stage over every cell) unless lanes were asked
+  // for, stage timing is on, or a cell failed its checks.
+  const bool segmented = c->batch_lanes == 0 && all_ok;
+  SegPlan sp;
+  SegBufs sb{};
+  if (segmented) {
+    if ((rc = seg_plan(c, n_cells, offsets, cells, params, force != nullptr, sp))) return rc;
+    if ((rc = seg_prepare(c, sp, sb))) return rc;
+  }
+  const int nl = segmented ? 1
+                 : c->prof.on ? 1
+                              : std::min(std::max(c->batch_lanes, 1), std::max(n_cells, 1));
   if (nl > 1) {
     while (static_cast<int>(c->lanes.size()) < nl) {
       ewg_context* l = nullptr;
@@ -1999,24 +2289,15 @@ int ewg_batch_potential_force_ov(ewg_context* c, int n_cells, const int* offsets
       c->lanes[l]->graphs_on = c->graphs_on;
     }
   }
-  // Host side first: each cell's checks and parameters (the reference chain).
-  std::vector<int> status(n_cells, EWG_OK);
-  std::vector<Cell> cells(n_cells);
-  std::vector<ewg_params> params(n_cells);
-  for (int cidx = 0; cidx < n_cells; ++cidx) {
-    const int a0 = offsets[cidx], na = offsets[cidx + 1] - a0;
-    double q2 = 0.0;
-    int st = check_charges(na, charges + a0, &q2);
-    if (!st) st = cell_from_rows(lat_rows + 9 * static_cast<size_t>(cidx), cells[cidx]);
-    if (!st && !(tol > 0.0 && tol < 1.0)) st = EWG_ERR_TOL;
-    if (!st) st = choose_parameters(cells[cidx], q2, na, tol, ov, params[cidx]);
-    status[cidx] = st;
-  }
   cudaMemcpyAsync(dcoords, coords, sizeof(double) * 3 * total, cudaMemcpyHostToDevice, c->stream);
   cudaMemcpyAsync(dq, charges, sizeof(double) * total, cudaMemcpyHostToDevice, c->stream);
   // The device work of the whole batch: the cells round-robin on the lanes,
   // forked from and joined back to the context's stream.
   auto launch_batch = [&]() -> int {
+    if (segmented) {
+      seg_kernels(c, sp, sb, dcoords, dq, dpot, force ? dforce : nullptr, cellerr);
+      return EWG_OK;
+    }
     int bad = EWG_OK;
     cudaMemsetAsync(cellerr, 0, sizeof(int) * std::max(n_cells, 1), c->stream);
     if (nl > 1) {
@@ -2055,7 +2336,7 @@ int ewg_batch_potential_force_ov(ewg_context* c, int n_cells, const int* offsets
       std::memcpy(&u, &v, sizeof(v));
       key.push_back(u);
     };
-    put(n_cells), put(nl), put(tol), put(force != nullptr), put(c->precision);
+    put(n_cells), put(nl), put(segmented), put(tol), put(force != nullptr), put(c->precision);
     put(c->force_scheme), put(c->background), put(c->buf_gen), put(c->stream);
     for (int l = 0; l < nl && nl > 1; ++l) put(c->lanes[l]->buf_gen), put(c->lanes[l]->stream);
     for (int cidx = 0; cidx < n_cells; ++cidx) {
@@ -2118,6 +2399,7 @@ int ewg_batch_potential_force_ov(ewg_context* c, int n_cells, const int* offsets
     e = cudaMemcpyAsync(herr.data(), cellerr, sizeof(int) * n_cells, cudaMemcpyDeviceToHost,
                         c->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (segmented) prof_collect(&c->prof);
   if (e != cudaSuccess) return cuda_status(e);
   for (int cidx = 0; cidx < n_cells; ++cidx) {
     if (status[cidx] == EWG_OK && herr[cidx]) status[cidx] = EWG_ERR_COINCIDENT;

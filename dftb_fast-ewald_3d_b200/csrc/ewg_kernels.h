@@ -141,6 +141,8 @@ struct StencilDims {
   int ad;          // 1: window derivatives stored after the weights (forces by
                    // analytic differentiation of the window)
   int dwoff;       // per-atom offset of the derivative rows (woff[d] + dwoff)
+  int pstride;     // gather partials per atom: S_x S_y S_z slots (or more, when
+                   // cells of a batch share one layout)
 };
 
 // Everything the mesh pipeline needs, resolved on the host.
@@ -152,6 +154,100 @@ struct MeshPlan {
   Profiler* prof = nullptr;
   const double* corr2[3] = {nullptr, nullptr, nullptr};  // squared deconvolution factors, index k + H
 };
+
+// ---- segmented launches of the batched form --------------------------------
+// The cells of a batch lie end to end: their atoms in global arrays (the
+// caller's CSR order, and after the global box sort, cell by cell in box
+// order), their cell-list boxes and mesh tiles as consecutive key ranges of
+// global counting sorts, their grids in separate buffers.  One launch per
+// stage covers every cell; its global index (atom, work item or block) maps to
+// its cell through the launch's prefix array (prefix[c] = first index of cell
+// c, prefix[ncells] = total), and the cell's parameters come from the device
+// table below.
+struct BatchCell {
+  int atom0, natoms;  // global atom range
+  int box0, tile0;    // first key of the cell in the global box and tile sorts
+  double lat[3][3], rec[3][3];
+  RealGeom rg;
+  double alpha, cut2;
+  float pre2;
+  double self_coef;
+  MeshGeom g;
+  StencilDims sd;
+  FftPlan fft[3];
+  const double* corr2[3];
+  void *grid, *A1, *A2, *B2, *B1, *out;
+};
+
+// The cell holding global index idx: the last c with prefix[c] <= idx (cells
+// with no work in a launch have prefix[c] == prefix[c + 1] and are skipped).
+__device__ __forceinline__ int seg_cell(const int* __restrict__ prefix, int ncells, long idx) {
+  int lo = 0, hi = ncells - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (prefix[mid] <= idx)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// Host description of one segmented batch: the device table, the prefix
+// array of every launch (device) and the totals (host).
+struct BatchLaunch {
+  const BatchCell* cells = nullptr;
+  int ncells = 0;
+  int mixed = 0, nc = 1, nparts = 1, ad = 0;
+  int L = 1;           // FFT lines per CTA, one value for every cell
+  size_t smem[3] = {0, 0, 0};  // FFT pass shared memory per axis (the largest cell's)
+  size_t smem_z = 0;
+  int lpa = 32;        // lanes per atom of the final sum
+  // prefix arrays (device) and totals
+  const int* p_atoms = nullptr;   int n_atoms = 0;
+  const int* p_weights = nullptr; long n_weights = 0;  // natoms (S_x + S_y + S_z)
+  const int* p_slots = nullptr;   long n_slots = 0;    // natoms S_x S_y S_z
+  const int* p_tiles = nullptr;   int n_tiles = 0;
+  const int* p_r2c = nullptr;     int n_r2c = 0;
+  const int* p_yfwd = nullptr;    int n_yfwd = 0;
+  const int* p_z = nullptr;       int n_z = 0;
+  const int* p_yinv = nullptr;    int n_yinv = 0;
+  const int* p_c2r = nullptr;     int n_c2r = 0;
+  const int* p_final = nullptr;   long n_final = 0;    // natoms lpa
+  int n_boxes = 0;
+};
+
+// Segmented counterparts of the single-cell launchers (same work per cell).
+void launch_atom_prep_seg(const BatchLaunch& b, const double* coords3n, const double* q,
+                          double4* s4, int* box_key, int4* mesh_c, double4* mesh_fr,
+                          cudaStream_t st);
+void launch_permute_box_seg(const BatchLaunch& b, const double4* in, const int* perm,
+                            double4* out, float4* x32, cudaStream_t st);
+void launch_real_space_seg(const BatchLaunch& b, const double4* s4s, const float4* x32,
+                           const int* perm, const int* box_start, double* pot, double* force,
+                           int* cell_err, cudaStream_t st);
+void launch_weights_seg(const BatchLaunch& b, const int4* mesh_c, const double4* mesh_fr,
+                        const int* perm, void* wtab, void* qk, int4* slot, cudaStream_t st);
+void launch_pair_bins_seg(const BatchLaunch& b, const int4* slot, int* counts, int* cursor,
+                          int* tile_start, int4* tmp, int2* pairs, cudaStream_t st);
+void launch_spread_seg(const BatchLaunch& b, const int* tile_start, const int2* pairs,
+                       const void* wtab, const void* qk, cudaStream_t st);
+void launch_forward_and_weight_seg(const BatchLaunch& b, cudaStream_t st);
+void launch_inverse_seg(const BatchLaunch& b, cudaStream_t st);
+void launch_gather_seg(const BatchLaunch& b, const int* tile_start, const int2* pairs,
+                       const void* wtab, double* part, cudaStream_t st);
+void launch_gather_final_seg(const BatchLaunch& b, const int4* slot, const int* perm,
+                             const double* part, const double* q, const double* pot_sr,
+                             const double* f_sr, double* pot, double* force, cudaStream_t st);
+// FP32 prefilter bound of the real-space distance test for this geometry.
+float real_prefilter_bound(const RealGeom& g, double r_cut);
+// FFT lines per CTA a pass of length n (plus `extra` elements per line) would
+// take alone, and the shared bytes of such a pass at L lines.
+int mesh_batch_lines(int n, bool mixed, int extra);
+// Blocks per cell of each pass (x R2C, y forward, z, y inverse, x C2R) at L
+// lines per CTA and nc grids through the inverse passes.
+void mesh_pass_blocks(const MeshGeom& g, int L, int nc, int out[5]);
+size_t mesh_pass_smem(int n, int L, bool mixed, int extra);
 
 // Tiled window weights per sorted atom (wtab: wstride values per atom), slot
 // origin and count per axis (slot: first | count << 16 in x, y, z), and the

@@ -62,7 +62,7 @@ __device__ __forceinline__ cx<R>* spare_buffer(cx<R>* a, cx<R>* b, const FftPlan
 // k1 = 0..K1-1 of each row.
 // ---------------------------------------------------------------------------
 template <typename R, int L>
-__global__ void __launch_bounds__(pass_threads(L)) k_fft_x_r2c(const R* __restrict__ grid,
+__device__ __forceinline__ void fft_x_r2c_body(int bx, const R* __restrict__ grid,
                                                                cx<R>* __restrict__ A1, int n1,
                                                                int npairs, int K1, FftPlan plan) {
   chain_enter();
@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_r2c(const R* __restri
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
   cx<R>* b = a + static_cast<size_t>(n1) * L;
   const cx<R>* tw = plan_twiddles<R>(plan);
-  const int pair0 = blockIdx.x * L;
+  const int pair0 = bx * L;
   // Each thread serves one line (its lane in the group): resolve its rows once.
   const bool valid = pair0 + static_cast<int>(threadIdx.x & (L - 1)) < npairs;
   const R* ra = grid + static_cast<size_t>(2 * (pair0 + (threadIdx.x & (L - 1)))) * n1;
@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_r2c(const R* __restri
 // y pass, forward: lines over i2 for (i3, k1-block); keep k2 in [-H2, H2].
 // ---------------------------------------------------------------------------
 template <typename R, int L>
-__global__ void __launch_bounds__(pass_threads(L)) k_fft_y_fwd(const cx<R>* __restrict__ A1,
+__device__ __forceinline__ void fft_y_fwd_body(int bx, int by, const cx<R>* __restrict__ A1,
                                                                cx<R>* __restrict__ A2, int n2,
                                                                int K1, int K2, int H2,
                                                                FftPlan plan) {
@@ -107,8 +107,8 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_fwd(const cx<R>* __re
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
   cx<R>* b = a + static_cast<size_t>(n2) * L;
   const cx<R>* tw = plan_twiddles<R>(plan);
-  const int k0 = blockIdx.x * L;
-  const int i3 = blockIdx.y;
+  const int k0 = bx * L;
+  const int i3 = by;
   const int kl = k0 + static_cast<int>(threadIdx.x & (L - 1));  // this thread's k1
   const bool kin = kl < K1;
   const cx<R>* src = A1 + static_cast<size_t>(i3) * n2 * K1 + kl;
@@ -144,8 +144,8 @@ struct InfluenceArgs {
 
 // nz = 1 (potential) or 2 (also T3, the spectrum times 2 pi i k3).
 template <typename R, int L, bool STRESS>
-__global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
-    const cx<R>* __restrict__ A2, cx<R>* __restrict__ B2, int n3, int K1, int K2, int K3, int nz,
+__device__ __forceinline__ void fft_z_influence_body(
+    int bx, int by, int gx, const cx<R>* __restrict__ A2, cx<R>* __restrict__ B2, int n3, int K1, int K2, int K3, int nz,
     InfluenceArgs ia, FftPlan plan) {
   chain_enter();
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -153,8 +153,8 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
   cx<R>* b = a + static_cast<size_t>(n3) * L;
   cx<R>* q = b + static_cast<size_t>(n3) * L;  // K3 weighted modes per line
   const cx<R>* tw = plan_twiddles<R>(plan);
-  const int k0 = blockIdx.x * L;
-  const int k2i = blockIdx.y;
+  const int k0 = bx * L;
+  const int k2i = by;
   const int h1 = ia.H[0], h2 = ia.H[1], h3 = ia.H[2];
   const int k2 = k2i - h2;
   const double twoPi = 2.0 * 3.14159265358979323846;
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
     if (threadIdx.x < 6) {
       double t = 0.0;
       for (int w = 0; w < static_cast<int>(blockDim.x >> 5); ++w) t += sred[w][threadIdx.x];
-      ia.stress[(static_cast<size_t>(blockIdx.y) * gridDim.x + blockIdx.x) * 6 + threadIdx.x] = t;
+      ia.stress[(static_cast<size_t>(by) * gx + bx) * 6 + threadIdx.x] = t;
     }
   }
   for (int c = 0; c < nz; ++c) {
@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
 // 2 = IFFT_y(T3), with P and T3 the z pass's two outputs.
 // ---------------------------------------------------------------------------
 template <typename R, int L>
-__global__ void __launch_bounds__(pass_threads(L)) k_fft_y_inv(const cx<R>* __restrict__ B2,
+__device__ __forceinline__ void fft_y_inv_body(int bx, int by, int bz, const cx<R>* __restrict__ B2,
                                                                cx<R>* __restrict__ B1, int n2,
                                                                int n3, int K1, int K2, int H2,
                                                                FftPlan plan) {
@@ -269,9 +269,9 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_inv(const cx<R>* __re
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
   cx<R>* b = a + static_cast<size_t>(n2) * L;
   const cx<R>* tw = plan_twiddles<R>(plan);
-  const int k0 = blockIdx.x * L;
-  const int i3 = blockIdx.y;
-  const int c = blockIdx.z;
+  const int k0 = bx * L;
+  const int i3 = by;
+  const int c = bz;
   const int cs = c == 2 ? 1 : 0;  // source component in B2
   const bool dk2 = c == 1;        // times 2 pi i k2
   const int kl = k0 + static_cast<int>(threadIdx.x & (L - 1));  // this thread's k1
@@ -309,7 +309,7 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_inv(const cx<R>* __re
 // the y pass's three components.
 // ---------------------------------------------------------------------------
 template <typename R, int L, int NCG>
-__global__ void __launch_bounds__(pass_threads(L)) k_fft_x_c2r(const cx<R>* __restrict__ B1,
+__device__ __forceinline__ void fft_x_c2r_body(int bx, int by, const cx<R>* __restrict__ B1,
                                                                R* __restrict__ out, int n1,
                                                                int nrows, int K1, int nc,
                                                                FftPlan plan) {
@@ -319,8 +319,8 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_c2r(const cx<R>* __re
   cx<R>* a = reinterpret_cast<cx<R>*>(smem_raw);
   cx<R>* b = a + static_cast<size_t>(n1) * L;
   const cx<R>* tw = plan_twiddles<R>(plan);
-  const int pair0 = blockIdx.x * NP;
-  const int c0 = blockIdx.y * NCG;
+  const int pair0 = bx * NP;
+  const int c0 = by * NCG;
   const int npairs = nrows / 2;
   // Each thread serves one line: resolve its rows and output columns once.
   const int line = static_cast<int>(threadIdx.x & (L - 1));
@@ -362,6 +362,131 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_c2r(const cx<R>* __re
     ob[x * nc] = v.y;
   };
   fft_edges<R, 1, L>(a, b, n1, plan, tw, load, store);
+}
+
+// ---- pass kernels: one cell (blockIdx = the pass's block), or every cell of a
+// batch (blockIdx.x over the cells' blocks end to end; the cell's lengths,
+// plans and buffers from the batch table; the lines per CTA are common).
+template <typename R, int L>
+__global__ void __launch_bounds__(pass_threads(L)) k_fft_x_r2c(const R* __restrict__ grid,
+                                                               cx<R>* __restrict__ A1, int n1,
+                                                               int npairs, int K1, FftPlan plan) {
+  fft_x_r2c_body<R, L>(blockIdx.x, grid, A1, n1, npairs, K1, plan);
+}
+template <typename R, int L>
+__global__ void __launch_bounds__(pass_threads(L)) k_fft_y_fwd(const cx<R>* __restrict__ A1,
+                                                               cx<R>* __restrict__ A2, int n2,
+                                                               int K1, int K2, int H2,
+                                                               FftPlan plan) {
+  fft_y_fwd_body<R, L>(blockIdx.x, blockIdx.y, A1, A2, n2, K1, K2, H2, plan);
+}
+template <typename R, int L, bool STRESS>
+__global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
+    const cx<R>* __restrict__ A2, cx<R>* __restrict__ B2, int n3, int K1, int K2, int K3, int nz,
+    InfluenceArgs ia, FftPlan plan) {
+  fft_z_influence_body<R, L, STRESS>(blockIdx.x, blockIdx.y, gridDim.x, A2, B2, n3, K1, K2, K3, nz,
+                                     ia, plan);
+}
+template <typename R, int L>
+__global__ void __launch_bounds__(pass_threads(L)) k_fft_y_inv(const cx<R>* __restrict__ B2,
+                                                               cx<R>* __restrict__ B1, int n2,
+                                                               int n3, int K1, int K2, int H2,
+                                                               FftPlan plan) {
+  fft_y_inv_body<R, L>(blockIdx.x, blockIdx.y, blockIdx.z, B2, B1, n2, n3, K1, K2, H2, plan);
+}
+template <typename R, int L, int NCG>
+__global__ void __launch_bounds__(pass_threads(L)) k_fft_x_c2r(const cx<R>* __restrict__ B1,
+                                                               R* __restrict__ out, int n1,
+                                                               int nrows, int K1, int nc,
+                                                               FftPlan plan) {
+  fft_x_c2r_body<R, L, NCG>(blockIdx.x, blockIdx.y, B1, out, n1, nrows, K1, nc, plan);
+}
+
+// Blocks per cell of each pass (r2c, y forward, z, y inverse, c2r) at L lines
+// per CTA, nc grids through the inverse passes.
+__host__ __device__ inline void pass_blocks(const MeshGeom& g, int L, int nc, int out[5]) {
+  const int npairs = g.n[1] * g.n[2] / 2, kb = (g.K1 + L - 1) / L;
+  out[0] = (npairs + L - 1) / L;
+  out[1] = kb * g.n[2];
+  out[2] = kb * g.K2;
+  out[3] = kb * g.n[2] * (nc == 4 ? 3 : 1);
+  out[4] = (nc == 4 && L >= 4) ? (npairs + L / 4 - 1) / (L / 4) : ((npairs + L - 1) / L) * nc;
+}
+
+__device__ __forceinline__ const BatchCell& pass_cell(const BatchCell* __restrict__ cells,
+                                                      const int* __restrict__ prefix, int ncells,
+                                                      int* local) {
+  const int c = seg_cell(prefix, ncells, blockIdx.x);
+  *local = static_cast<int>(blockIdx.x) - prefix[c];
+  return cells[c];
+}
+
+template <typename R, int L>
+__global__ void __launch_bounds__(pass_threads(L)) k_fft_x_r2c_seg(
+    const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells) {
+  int local;
+  const BatchCell& bc = pass_cell(cells, prefix, ncells, &local);
+  const FftPlan plan = bc.fft[0];
+  fft_x_r2c_body<R, L>(local, static_cast<const R*>(bc.grid), static_cast<cx<R>*>(bc.A1),
+                       bc.g.n[0], bc.g.n[1] * bc.g.n[2] / 2, bc.g.K1, plan);
+}
+template <typename R, int L>
+__global__ void __launch_bounds__(pass_threads(L)) k_fft_y_fwd_seg(
+    const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells) {
+  int local;
+  const BatchCell& bc = pass_cell(cells, prefix, ncells, &local);
+  const int kb = (bc.g.K1 + L - 1) / L;
+  const FftPlan plan = bc.fft[1];
+  fft_y_fwd_body<R, L>(local % kb, local / kb, static_cast<const cx<R>*>(bc.A1),
+                       static_cast<cx<R>*>(bc.A2), bc.g.n[1], bc.g.K1, bc.g.K2,
+                       (bc.g.K2 - 1) / 2, plan);
+}
+template <typename R, int L>
+__global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence_seg(
+    const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells, int nz) {
+  int local;
+  const BatchCell& bc = pass_cell(cells, prefix, ncells, &local);
+  const int kb = (bc.g.K1 + L - 1) / L;
+  InfluenceArgs ia;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    ia.H[d] = bc.g.M[d] - bc.g.M[d] / 2;
+    ia.slo[d] = bc.g.M[d] / 2 - bc.g.M[d];
+    ia.shi[d] = bc.g.M[d] / 2 - 1;
+    ia.corr2[d] = bc.corr2[d];
+#pragma unroll
+    for (int e = 0; e < 3; ++e) ia.rec[d][e] = bc.g.rec[d][e];
+  }
+  ia.prefactor = 4.0 * 3.14159265358979323846 / bc.g.volume;
+  ia.inv4a2 = 1.0 / (4.0 * (bc.g.alpha * bc.g.alpha));
+  ia.stress = nullptr;
+  const FftPlan plan = bc.fft[2];
+  fft_z_influence_body<R, L, false>(local % kb, local / kb, kb, static_cast<const cx<R>*>(bc.A2),
+                                    static_cast<cx<R>*>(bc.B2), bc.g.n[2], bc.g.K1, bc.g.K2,
+                                    bc.g.K3, nz, ia, plan);
+}
+template <typename R, int L>
+__global__ void __launch_bounds__(pass_threads(L)) k_fft_y_inv_seg(
+    const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells) {
+  int local;
+  const BatchCell& bc = pass_cell(cells, prefix, ncells, &local);
+  const int kb = (bc.g.K1 + L - 1) / L, n3 = bc.g.n[2];
+  const int t = local / kb;
+  const FftPlan plan = bc.fft[1];
+  fft_y_inv_body<R, L>(local % kb, t % n3, t / n3, static_cast<const cx<R>*>(bc.B2),
+                       static_cast<cx<R>*>(bc.B1), bc.g.n[1], n3, bc.g.K1, bc.g.K2,
+                       (bc.g.K2 - 1) / 2, plan);
+}
+template <typename R, int L, int NCG>
+__global__ void __launch_bounds__(pass_threads(L)) k_fft_x_c2r_seg(
+    const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells, int nc) {
+  int local;
+  const BatchCell& bc = pass_cell(cells, prefix, ncells, &local);
+  const int nrows = bc.g.n[1] * bc.g.n[2];
+  const int nbx = (nrows / 2 + L / NCG - 1) / (L / NCG);
+  const FftPlan plan = bc.fft[0];
+  fft_x_c2r_body<R, L, NCG>(local % nbx, local / nbx, static_cast<const cx<R>*>(bc.B1),
+                            static_cast<R*>(bc.out), bc.g.n[0], nrows, bc.g.K1, nc, plan);
 }
 
 template <typename R>
@@ -516,6 +641,8 @@ void allow_lines() {
   allow_smem(k_fft_x_r2c<R, L>, k_fft_y_fwd<R, L>, k_fft_z_influence<R, L, false>,
              k_fft_z_influence<R, L, true>, k_fft_y_inv<R, L>,
              k_fft_x_c2r<R, L, 1>);
+  allow_smem(k_fft_x_r2c_seg<R, L>, k_fft_y_fwd_seg<R, L>, k_fft_z_influence_seg<R, L>,
+             k_fft_y_inv_seg<R, L>, k_fft_x_c2r_seg<R, L, 1>);
 }
 
 template <typename R>
@@ -525,9 +652,76 @@ void allow_all() {
   allow_lines<R, 2>();
   allow_lines<R, 1>();
   allow_smem(k_fft_x_c2r<R, 8, 4>, k_fft_x_c2r<R, 4, 4>);
+  allow_smem(k_fft_x_c2r_seg<R, 8, 4>, k_fft_x_c2r_seg<R, 4, 4>);
+}
+
+// Segmented passes of a batch: lines per CTA b.L for every cell, shared
+// memory for the batch's largest length per axis.
+template <typename R>
+void forward_seg_impl(const BatchLaunch& b, cudaStream_t st) {
+  const int nz = b.nc == 4 ? 2 : 1;
+  with_lines(b.L, [&](auto lc) {
+    constexpr int LL = decltype(lc)::value;
+    if (b.n_r2c)
+      launch_chained(k_fft_x_r2c_seg<R, LL>, b.n_r2c, pass_threads(LL), b.smem[0], st, b.cells,
+                     b.p_r2c, b.ncells);
+    if (b.n_yfwd)
+      launch_chained(k_fft_y_fwd_seg<R, LL>, b.n_yfwd, pass_threads(LL), b.smem[1], st, b.cells,
+                     b.p_yfwd, b.ncells);
+    if (b.n_z)
+      launch_chained(k_fft_z_influence_seg<R, LL>, b.n_z, pass_threads(LL), b.smem_z, st, b.cells,
+                     b.p_z, b.ncells, nz);
+  });
+  g_launches += 3;
+}
+
+template <typename R>
+void inverse_seg_impl(const BatchLaunch& b, cudaStream_t st) {
+  with_lines(b.L, [&](auto lc) {
+    constexpr int LL = decltype(lc)::value;
+    if (b.n_yinv)
+      launch_chained(k_fft_y_inv_seg<R, LL>, b.n_yinv, pass_threads(LL), b.smem[1], st, b.cells,
+                     b.p_yinv, b.ncells);
+    if (b.n_c2r) {
+      if constexpr (LL >= 4) {
+        if (b.nc == 4) {
+          launch_chained(k_fft_x_c2r_seg<R, LL, 4>, b.n_c2r, pass_threads(LL), b.smem[0], st,
+                         b.cells, b.p_c2r, b.ncells, b.nc);
+          return;
+        }
+      }
+      launch_chained(k_fft_x_c2r_seg<R, LL, 1>, b.n_c2r, pass_threads(LL), b.smem[0], st, b.cells,
+                     b.p_c2r, b.ncells, b.nc);
+    }
+  });
+  g_launches += 2;
 }
 
 }  // namespace
+
+void mesh_pass_blocks(const MeshGeom& g, int L, int nc, int out[5]) { pass_blocks(g, L, nc, out); }
+
+int mesh_batch_lines(int n, bool mixed, int extra) {
+  return pick_lines(n, mixed ? sizeof(cx<float>) : sizeof(cx<double>), extra);
+}
+
+size_t mesh_pass_smem(int n, int L, bool mixed, int extra) {
+  return pass_smem(n, L, mixed ? sizeof(cx<float>) : sizeof(cx<double>), extra);
+}
+
+void launch_forward_and_weight_seg(const BatchLaunch& b, cudaStream_t st) {
+  if (b.mixed)
+    forward_seg_impl<float>(b, st);
+  else
+    forward_seg_impl<double>(b, st);
+}
+
+void launch_inverse_seg(const BatchLaunch& b, cudaStream_t st) {
+  if (b.mixed)
+    inverse_seg_impl<float>(b, st);
+  else
+    inverse_seg_impl<double>(b, st);
+}
 
 int mesh_check_lengths(const MeshGeom& g, bool mixed) {
   const size_t cb = mixed ? sizeof(cx<float>) : sizeof(cx<double>);

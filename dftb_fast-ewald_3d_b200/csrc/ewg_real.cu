@@ -48,13 +48,12 @@ struct PrepArgs {
   int ng[3];
 };
 
-__global__ void k_atom_prep(const double* __restrict__ pos, long sa, long sd,
-                            const double* __restrict__ q, int n, PrepArgs a,
-                            double4* __restrict__ s4, int* __restrict__ box_key,
-                            int4* __restrict__ mesh_c, double4* __restrict__ mesh_fr) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double x[3] = {pos[i * sa], pos[i * sa + sd], pos[i * sa + 2 * sd]};
+// One atom of k_atom_prep (key: its box in the cell's own numbering).
+__device__ __forceinline__ void atom_prep_one(const double (&x)[3], double qi, const PrepArgs& a,
+                                              int i, int key0, double4* __restrict__ s4,
+                                              int* __restrict__ box_key,
+                                              int4* __restrict__ mesh_c,
+                                              double4* __restrict__ mesh_fr) {
   double s[3];
   int bx[3], c[3];
   double fr[3];
@@ -71,13 +70,44 @@ __global__ void k_atom_prep(const double* __restrict__ pos, long sa, long sd,
       c[d] = lowest;
     }
   }
-  const double qi = q[i];
   if (s4) s4[i] = make_double4(s[0], s[1], s[2], qi);
-  if (box_key) box_key[i] = (bx[2] * a.nb[1] + bx[1]) * a.nb[0] + bx[0];
+  if (box_key) box_key[i] = key0 + (bx[2] * a.nb[1] + bx[1]) * a.nb[0] + bx[0];
   if (mesh_c) {
     mesh_c[i] = make_int4(c[0], c[1], c[2], 0);
     mesh_fr[i] = make_double4(fr[0], fr[1], fr[2], qi);
   }
+}
+
+__global__ void k_atom_prep(const double* __restrict__ pos, long sa, long sd,
+                            const double* __restrict__ q, int n, PrepArgs a,
+                            double4* __restrict__ s4, int* __restrict__ box_key,
+                            int4* __restrict__ mesh_c, double4* __restrict__ mesh_fr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double x[3] = {pos[i * sa], pos[i * sa + sd], pos[i * sa + 2 * sd]};
+  atom_prep_one(x, q[i], a, i, 0, s4, box_key, mesh_c, mesh_fr);
+}
+
+// Every cell of a batch at once: atom i of the global arrays (coords(3, total)),
+// its cell's reciprocal rows, boxes and grid; box keys offset by the cell's box0.
+__global__ void k_atom_prep_seg(const BatchCell* __restrict__ cells, const int* __restrict__ prefix,
+                                int ncells, int n, const double* __restrict__ pos,
+                                const double* __restrict__ q, double4* __restrict__ s4,
+                                int* __restrict__ box_key, int4* __restrict__ mesh_c,
+                                double4* __restrict__ mesh_fr) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const BatchCell& bc = cells[seg_cell(prefix, ncells, i)];
+  PrepArgs a;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+#pragma unroll
+    for (int e = 0; e < 3; ++e) a.rec[d][e] = bc.rec[d][e];
+    a.nb[d] = bc.rg.nb[d];
+    a.ng[d] = bc.g.n[d];
+  }
+  const double x[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+  atom_prep_one(x, q[i], a, i, bc.box0, s4, box_key, mesh_c, mesh_fr);
 }
 
 // ---------------------------------------------------------------------------
@@ -179,6 +209,22 @@ __global__ void k_rank(const int* __restrict__ key, int n, const int* __restrict
 struct LatRows {
   double a[3][3];
 };
+__global__ void k_permute_box_seg(const BatchCell* __restrict__ cells,
+                                  const int* __restrict__ prefix, int ncells, int n,
+                                  const double4* __restrict__ in, const int* __restrict__ perm,
+                                  double4* __restrict__ out, float4* __restrict__ x32) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const BatchCell& bc = cells[seg_cell(prefix, ncells, k)];  // sorted ranges = atom ranges
+  const double4 v = in[perm[k]];
+  out[k] = v;
+  float c[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    c[d] = static_cast<float>(v.x * bc.lat[0][d] + v.y * bc.lat[1][d] + v.z * bc.lat[2][d]);
+  x32[k] = make_float4(c[0], c[1], c[2], static_cast<float>(v.w));
+}
+
 __global__ void k_permute_box(const double4* __restrict__ in, const int* __restrict__ perm, int n,
                               LatRows lat, double4* __restrict__ out, float4* __restrict__ x32) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -609,21 +655,19 @@ struct EwaldPair {
 
 // Four CTAs of 256 threads per SM (64 registers): the candidate loads and the
 // pair terms' dependent FP64 chains want the warps.
+// The warp of sorted atom k (box_start: the cell's own box numbering).
 template <bool MIXED>
-__global__ void __launch_bounds__(kRealThreads, 4) k_real_space(const double4* __restrict__ srt,
-                                                             const float4* __restrict__ x32,
-                                                             const int* __restrict__ perm,
-                                                             const int* __restrict__ box_start,
-                                                             int n, RealGeom g, double alpha,
-                                                             double cut2, float pre2,
-                                                             double* __restrict__ pot,
-                                                             double* __restrict__ force,
-                                                             int* __restrict__ err) {
+__device__ __forceinline__ void real_space_body(const double4* __restrict__ srt,
+                                                const float4* __restrict__ x32,
+                                                const int* __restrict__ perm,
+                                                const int* __restrict__ box_start, int k,
+                                                const RealGeom& g, double alpha, double cut2,
+                                                float pre2, double* __restrict__ pot,
+                                                double* __restrict__ force,
+                                                int* __restrict__ err) {
   __shared__ __align__(16) int4 queue[kRealThreads / 32][kQueue];
   __shared__ RunTable runs[kRealThreads / 32];
-  const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (k >= n) return;
   const double4 ai = srt[k];
   EwaldPair pair;
   pair.alpha = alpha;
@@ -657,6 +701,38 @@ __global__ void __launch_bounds__(kRealThreads, 4) k_real_space(const double4* _
       force[3 * i + c - 1] = t;
     if (c == 0 && bad) atomicOr(err, 1);
   }
+}
+
+template <bool MIXED>
+__global__ void __launch_bounds__(kRealThreads, 4) k_real_space(const double4* __restrict__ srt,
+                                                             const float4* __restrict__ x32,
+                                                             const int* __restrict__ perm,
+                                                             const int* __restrict__ box_start,
+                                                             int n, RealGeom g, double alpha,
+                                                             double cut2, float pre2,
+                                                             double* __restrict__ pot,
+                                                             double* __restrict__ force,
+                                                             int* __restrict__ err) {
+  const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (k >= n) return;
+  real_space_body<MIXED>(srt, x32, perm, box_start, k, g, alpha, cut2, pre2, pot, force, err);
+}
+
+// Every cell of a batch: the warp's atom k picks its cell's cell-list geometry,
+// splitting and cutoff; a coincident pair flags the cell (err[cell]).
+template <bool MIXED>
+__global__ void __launch_bounds__(kRealThreads, 4) k_real_space_seg(
+    const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells,
+    const double4* __restrict__ srt, const float4* __restrict__ x32, const int* __restrict__ perm,
+    const int* __restrict__ box_start, int n, double* __restrict__ pot,
+    double* __restrict__ force, int* __restrict__ err) {
+  const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (k >= n) return;
+  const int c = seg_cell(prefix, ncells, k);
+  const BatchCell& bc = cells[c];
+  const RealGeom g = bc.rg;
+  real_space_body<MIXED>(srt, x32, perm, box_start + bc.box0, k, g, bc.alpha, bc.cut2, bc.pre2,
+                         pot, force, err + c);
 }
 
 // Real-space virial of invRStress with addNeighbourContribsStress
@@ -872,6 +948,41 @@ void launch_real_space(const double4* srt, const float4* x32, const int* perm,
                                                          r_cut * r_cut, pre2, pot, force, err);
   ++g_launches;
 }
+
+void launch_atom_prep_seg(const BatchLaunch& b, const double* coords3n, const double* q,
+                          double4* s4, int* box_key, int4* mesh_c, double4* mesh_fr,
+                          cudaStream_t st) {
+  if (b.n_atoms == 0) return;
+  k_atom_prep_seg<<<blocks_for(b.n_atoms, 256), 256, 0, st>>>(
+      b.cells, b.p_atoms, b.ncells, b.n_atoms, coords3n, q, s4, box_key, mesh_c, mesh_fr);
+  ++g_launches;
+}
+
+void launch_permute_box_seg(const BatchLaunch& b, const double4* in, const int* perm,
+                            double4* out, float4* x32, cudaStream_t st) {
+  if (b.n_atoms == 0) return;
+  k_permute_box_seg<<<blocks_for(b.n_atoms, 256), 256, 0, st>>>(b.cells, b.p_atoms, b.ncells,
+                                                                b.n_atoms, in, perm, out, x32);
+  ++g_launches;
+}
+
+void launch_real_space_seg(const BatchLaunch& b, const double4* s4s, const float4* x32,
+                           const int* perm, const int* box_start, double* pot, double* force,
+                           int* cell_err, cudaStream_t st) {
+  if (b.n_atoms == 0) return;
+  const int blocks = blocks_for(static_cast<long>(b.n_atoms) * 32, kRealThreads);
+  if (b.mixed)
+    k_real_space_seg<true><<<blocks, kRealThreads, 0, st>>>(b.cells, b.p_atoms, b.ncells, s4s, x32,
+                                                            perm, box_start, b.n_atoms, pot,
+                                                            force, cell_err);
+  else
+    k_real_space_seg<false><<<blocks, kRealThreads, 0, st>>>(b.cells, b.p_atoms, b.ncells, s4s,
+                                                             x32, perm, box_start, b.n_atoms, pot,
+                                                             force, cell_err);
+  ++g_launches;
+}
+
+float real_prefilter_bound(const RealGeom& g, double r_cut) { return prefilter_bound(g, r_cut); }
 
 void launch_real_stress(const double4* srt, const float4* x32, const int* box_start, int n,
                         const RealGeom& g, double alpha, double max_r, double* partial6,

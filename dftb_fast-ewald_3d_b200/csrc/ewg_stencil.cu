@@ -71,17 +71,13 @@ __device__ __forceinline__ int slot_count(int packed) { return packed >> 16; }
 // Tiled window weights, one thread per (atom, axis, tile slot): eight points
 // each, so an atom's S_x + S_y + S_z rows are computed in parallel.
 // ---------------------------------------------------------------------------
+// Row r (axis and slot) of sorted atom k.
 template <typename R>
-__global__ void k_weights_tiled(const int4* __restrict__ mc, const double4* __restrict__ fr,
-                                const int* __restrict__ perm, int n, StencilDims sd,
-                                R* __restrict__ wtab, R* __restrict__ qk,
-                                int4* __restrict__ slot) {
-  chain_enter();
-  const int SS = sd.S[0] + sd.S[1] + sd.S[2];
-  const long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (idx >= static_cast<long>(SS) * n) return;
-  const int k = static_cast<int>(idx / SS);
-  int r = static_cast<int>(idx - static_cast<long>(k) * SS);
+__device__ __forceinline__ void weights_row(const int4* __restrict__ mc,
+                                            const double4* __restrict__ fr,
+                                            const int* __restrict__ perm, int k, int r,
+                                            const StencilDims& sd, R* __restrict__ wtab,
+                                            R* __restrict__ qk, int4* __restrict__ slot) {
   const int d = r < sd.S[0] ? 0 : (r < sd.S[0] + sd.S[1] ? 1 : 2);
   const int s = r - (d == 0 ? 0 : (d == 1 ? sd.S[0] : sd.S[0] + sd.S[1]));
   const int i = perm[k];
@@ -166,6 +162,40 @@ __global__ void k_weights_tiled(const int4* __restrict__ mc, const double4* __re
   }
 }
 
+template <typename R>
+__global__ void k_weights_tiled(const int4* __restrict__ mc, const double4* __restrict__ fr,
+                                const int* __restrict__ perm, int n, StencilDims sd,
+                                R* __restrict__ wtab, R* __restrict__ qk,
+                                int4* __restrict__ slot) {
+  chain_enter();
+  const int SS = sd.S[0] + sd.S[1] + sd.S[2];
+  const long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= static_cast<long>(SS) * n) return;
+  const int k = static_cast<int>(idx / SS);
+  weights_row<R>(mc, fr, perm, k, static_cast<int>(idx - static_cast<long>(k) * SS), sd, wtab, qk,
+                 slot);
+}
+
+// Every cell of a batch: item idx is (atom, row) of its cell (prefix over the
+// cells' natoms (S_x + S_y + S_z)); the weight rows keep the batch's common
+// per-atom stride.
+template <typename R>
+__global__ void k_weights_seg(const BatchCell* __restrict__ cells, const int* __restrict__ prefix,
+                              int ncells, long nitems, const int4* __restrict__ mc,
+                              const double4* __restrict__ fr, const int* __restrict__ perm,
+                              R* __restrict__ wtab, R* __restrict__ qk, int4* __restrict__ slot) {
+  chain_enter();
+  const long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= nitems) return;
+  const int c = seg_cell(prefix, ncells, idx);
+  const BatchCell& bc = cells[c];
+  const StencilDims sd = bc.sd;
+  const int SS = sd.S[0] + sd.S[1] + sd.S[2];
+  const int local = static_cast<int>(idx - prefix[c]);
+  const int kl = local / SS;
+  weights_row<R>(mc, fr, perm, bc.atom0 + kl, local - kl * SS, sd, wtab, qk, slot);
+}
+
 // ---------------------------------------------------------------------------
 // (atom, tile) pair binning.
 // ---------------------------------------------------------------------------
@@ -187,6 +217,82 @@ __device__ __forceinline__ void for_each_tile(const int4& si, const StencilDims&
 
 // One thread per (atom, slot of the S_x x S_y x S_z block); slots past the
 // atom's own tile counts are skipped.
+// Slot s of sorted atom k: its tile (the cell's own numbering) and packed
+// slot, false for slots past the atom's tile counts.
+__device__ __forceinline__ bool pair_of(const int4* __restrict__ slot, int k, int s,
+                                        const StencilDims& sd, int* tile, int* packed) {
+  const int sx = s % sd.S[0], sy = (s / sd.S[0]) % sd.S[1], sz = s / (sd.S[0] * sd.S[1]);
+  const int4 si = slot[k];
+  if (sx >= slot_count(si.x) || sy >= slot_count(si.y) || sz >= slot_count(si.z)) return false;
+  const int tx = (slot_first(si.x) + sx) % sd.ntiles[0];
+  const int ty = (slot_first(si.y) + sy) % sd.ntiles[1];
+  const int tz = (slot_first(si.z) + sz) % sd.ntiles[2];
+  *tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
+  *packed = sx | (sy << 8) | (sz << 16);
+  return true;
+}
+
+// Item idx of a batch's (atom, slot) launch: its cell, sorted atom, tile
+// (global numbering: the cell's tile0 added) and packed slot.
+__device__ __forceinline__ bool pair_of_seg(const BatchCell* __restrict__ cells,
+                                            const int* __restrict__ prefix, int ncells, long idx,
+                                            const int4* __restrict__ slot, int* tile, int* k,
+                                            int* packed) {
+  const int c = seg_cell(prefix, ncells, idx);
+  const BatchCell& bc = cells[c];
+  const int S = bc.sd.S[0] * bc.sd.S[1] * bc.sd.S[2];
+  const int local = static_cast<int>(idx - prefix[c]);
+  const int kl = local / S;
+  *k = bc.atom0 + kl;
+  const StencilDims sd = bc.sd;
+  if (!pair_of(slot, *k, local - kl * S, sd, tile, packed)) return false;
+  *tile += bc.tile0;
+  return true;
+}
+
+__global__ void k_pair_count_seg(const BatchCell* __restrict__ cells,
+                                 const int* __restrict__ prefix, int ncells, long nitems,
+                                 const int4* __restrict__ slot, int* __restrict__ counts) {
+  const long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  int tile, k, packed;
+  if (idx < nitems && pair_of_seg(cells, prefix, ncells, idx, slot, &tile, &k, &packed))
+    atomicAdd(&counts[tile], 1);
+}
+
+__global__ void k_pair_scatter_seg(const BatchCell* __restrict__ cells,
+                                   const int* __restrict__ prefix, int ncells, long nitems,
+                                   const int4* __restrict__ slot, const int* __restrict__ starts,
+                                   int* __restrict__ cursor, int2* __restrict__ tmp) {
+  chain_enter();
+  const long idx = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  int tile, k, packed;
+  if (idx < nitems && pair_of_seg(cells, prefix, ncells, idx, slot, &tile, &k, &packed))
+    tmp[starts[tile] + atomicAdd(&cursor[tile], 1)] = make_int2(k, packed);
+}
+
+// As k_pair_rank, the entry's cell found from its atom (sorted ranges follow
+// the cells' atom ranges).
+__global__ void k_pair_rank_seg(const BatchCell* __restrict__ cells,
+                                const int* __restrict__ atom_prefix, int ncells,
+                                const int2* __restrict__ tmp, const int* __restrict__ starts,
+                                int ntiles, const int4* __restrict__ slot,
+                                int2* __restrict__ pairs) {
+  chain_enter();
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= starts[ntiles]) return;
+  const int2 v = tmp[e];
+  const BatchCell& bc = cells[seg_cell(atom_prefix, ncells, v.x)];
+  const int4 si = slot[v.x];
+  const int tx = (slot_first(si.x) + (v.y & 0xff)) % bc.sd.ntiles[0];
+  const int ty = (slot_first(si.y) + ((v.y >> 8) & 0xff)) % bc.sd.ntiles[1];
+  const int tz = (slot_first(si.z) + (v.y >> 16)) % bc.sd.ntiles[2];
+  const int tile = bc.tile0 + (tz * bc.sd.ntiles[1] + ty) * bc.sd.ntiles[0] + tx;
+  const int b = starts[tile], end = starts[tile + 1];
+  int r = 0;
+  for (int j = b; j < end; ++j) r += tmp[j].x < v.x;
+  pairs[b + r] = v;
+}
+
 __device__ __forceinline__ bool pair_of_thread(const int4* __restrict__ slot, int n,
                                                const StencilDims& sd, int* tile, int* k,
                                                int* packed) {
@@ -195,15 +301,7 @@ __device__ __forceinline__ bool pair_of_thread(const int4* __restrict__ slot, in
   if (t >= static_cast<long>(n) * S) return false;
   *k = static_cast<int>(t / S);
   const int s = static_cast<int>(t - static_cast<long>(*k) * S);
-  const int sx = s % sd.S[0], sy = (s / sd.S[0]) % sd.S[1], sz = s / (sd.S[0] * sd.S[1]);
-  const int4 si = slot[*k];
-  if (sx >= slot_count(si.x) || sy >= slot_count(si.y) || sz >= slot_count(si.z)) return false;
-  const int tx = (slot_first(si.x) + sx) % sd.ntiles[0];
-  const int ty = (slot_first(si.y) + sy) % sd.ntiles[1];
-  const int tz = (slot_first(si.z) + sz) % sd.ntiles[2];
-  *tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
-  *packed = sx | (sy << 8) | (sz << 16);
-  return true;
+  return pair_of(slot, *k, s, sd, tile, packed);
 }
 
 __global__ void k_pair_count(const int4* __restrict__ slot, int n, StencilDims sd,
@@ -262,7 +360,8 @@ __device__ __forceinline__ void load8(const float* __restrict__ p, float* out) {
 // (py + 4, pz), so every pair of shared-memory reads of an atom's x weights
 // feeds 16 multiply-adds.
 template <typename R>
-__global__ void __launch_bounds__(kSpreadLanes) k_spread_tiles(const int* __restrict__ tile_start,
+__device__ __forceinline__ void spread_tiles_body(int tx, int ty, int tz,
+                                                  const int* __restrict__ tile_start,
                                                                const int2* __restrict__ pairs,
                                                                const R* __restrict__ wtab,
                                                                const R* __restrict__ qk,
@@ -271,7 +370,6 @@ __global__ void __launch_bounds__(kSpreadLanes) k_spread_tiles(const int* __rest
   __shared__ R sW1[kSpreadChunk][TX];
   __shared__ R sW2[kSpreadChunk][TY];
   __shared__ R sW3[kSpreadChunk][TZ];
-  const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
   const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
   const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
   const int py = threadIdx.x % (TY / 2), pz = threadIdx.x / (TY / 2);
@@ -376,7 +474,8 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // One warp per tile owning all eight z-planes, so each step's x and y weights
 // are read from shared memory once for the eight planes; the lanes stage up to
 // 32 atoms' weight rows per round with asynchronous 16-byte copies.
-__global__ void __launch_bounds__(32) k_spread_tiles_dmma(const int* __restrict__ tile_start,
+__device__ __forceinline__ void spread_tiles_dmma_body(int tx, int ty, int tz,
+                                                       const int* __restrict__ tile_start,
                                                           const int2* __restrict__ pairs,
                                                           const double* __restrict__ wtab,
                                                           const double* __restrict__ qk,
@@ -385,7 +484,6 @@ __global__ void __launch_bounds__(32) k_spread_tiles_dmma(const int* __restrict_
   chain_enter();
   __shared__ __align__(16) double sW[3][kSpreadAtoms][kWRow];
   __shared__ double sQ[kSpreadAtoms];
-  const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
   const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
   const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
   const int lane = threadIdx.x;
@@ -449,7 +547,8 @@ __global__ void __launch_bounds__(32) k_spread_tiles_dmma(const int* __restrict_
 // same point) feeds A atoms.
 // ---------------------------------------------------------------------------
 template <typename R, int NC, int A, int WARPS>
-__global__ void __launch_bounds__(32 * WARPS) k_gather_tiles(const int* __restrict__ tile_start,
+__device__ __forceinline__ void gather_tiles_body(int tx, int ty, int tz,
+                                                  const int* __restrict__ tile_start,
                                                              const int2* __restrict__ pairs,
                                                              const R* __restrict__ wtab,
                                                              StencilDims sd,
@@ -460,7 +559,6 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles(const int* __restri
       NC == 4, typename std::conditional<sizeof(R) == 8, double4, float4>::type, R>::type;
   __shared__ V sG[TZ * TY * TX];
   __shared__ R sW3[WARPS][TZ][32 * A];  // z weights, lane fastest
-  const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
   const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
   const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
   const int ex = min(TX, sd.n[0] - x0), ey = min(TY, sd.n[1] - y0), ez = min(TZ, sd.n[2] - z0);
@@ -483,7 +581,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles(const int* __restri
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nslots = sd.S[0] * sd.S[1] * sd.S[2];
+  const int nslots = sd.pstride;
   for (int a0 = p0 + warp * 32 * A; a0 < p1; a0 += WARPS * 32 * A) {
     R w1[A][TX], w2[A][TY];
     int2 pr[A];
@@ -592,7 +690,8 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles(const int* __restri
 // FP32, the sum over planes in FP64; the four partials go to the atom's slot.
 // ---------------------------------------------------------------------------
 template <int A, int WARPS>
-__global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_ad(const int* __restrict__ tile_start,
+__device__ __forceinline__ void gather_tiles_ad_body(int tx, int ty, int tz,
+                                                     const int* __restrict__ tile_start,
                                                                 const int2* __restrict__ pairs,
                                                                 const float* __restrict__ wtab,
                                                                 StencilDims sd,
@@ -604,7 +703,6 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_ad(const int* __res
   // with kind 0 = w2, 1 = dw2, 2 = w3, 3 = dw3.
   __shared__ float sYZ[WARPS][4][TY][32 * A];
   static_assert(TY == TZ, "y and z rows share one staging layout");
-  const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
   const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
   const int x0 = tx * TX, y0 = ty * TY, z0 = tz * TZ;
   const int ex = min(TX, sd.n[0] - x0), ey = min(TY, sd.n[1] - y0), ez = min(TZ, sd.n[2] - z0);
@@ -621,7 +719,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_ad(const int* __res
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int nslots = sd.S[0] * sd.S[1] * sd.S[2];
+  const int nslots = sd.pstride;
   float(*YZ)[TY][32 * A] = sYZ[warp];
   for (int a0 = p0 + warp * 32 * A; a0 < p1; a0 += WARPS * 32 * A) {
     float w1[A][TX], d1[A][TX];
@@ -762,7 +860,8 @@ struct GatherRow {
 };
 // WARPS warps per CTA, MB M blocks of 8 atoms per warp and round.
 template <int NC, int WARPS, int MB>
-__global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma(const int* __restrict__ tile_start,
+__device__ __forceinline__ void gather_tiles_dmma_body(int tx, int ty, int tz,
+                                                       const int* __restrict__ tile_start,
                                                           const int2* __restrict__ pairs,
                                                           const double* __restrict__ wtab,
                                                           StencilDims sd,
@@ -774,7 +873,6 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma(const int* __r
   __shared__ __align__(16) double sG[TZ * TY * RS];
   __shared__ __align__(16) double sW[3][kGatherAtoms][kWRow];
   __shared__ int2 sPair[kGatherAtoms];
-  const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
   const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
   const int p0 = tile_start[tile], p1 = tile_start[tile + 1];
   if (p0 == p1) return;  // no atom reaches this tile
@@ -797,7 +895,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma(const int* __r
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int fr = lane >> 2, fk = lane & 3;
-  const int nslots = sd.S[0] * sd.S[1] * sd.S[2];
+  const int nslots = sd.pstride;
   for (int b0 = p0; b0 < p1; b0 += kGatherAtoms) {
     const int nb = min(kGatherAtoms, p1 - b0);
     __syncthreads();  // the previous round's weights are no longer read
@@ -903,15 +1001,14 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma(const int* __r
 // weight rows per atom (w1 w2 w3 dw1 dw2 dw3).
 // ---------------------------------------------------------------------------
 template <int WARPS>
-__global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma_ad(
-    const int* __restrict__ tile_start, const int2* __restrict__ pairs,
+__device__ __forceinline__ void gather_tiles_dmma_ad_body(
+    int tx, int ty, int tz, const int* __restrict__ tile_start, const int2* __restrict__ pairs,
     const double* __restrict__ wtab, StencilDims sd, const double* __restrict__ grid,
     double* __restrict__ part) {
   chain_enter();
   constexpr int RS = GatherRow<1>::value;
   __shared__ __align__(16) double sG[TZ * TY * RS];
   __shared__ __align__(16) double sW[WARPS][6][8][kWRow];  // per warp: its 8 atoms' rows
-  const int tx = blockIdx.x, ty = blockIdx.y, tz = blockIdx.z;
   const int tile = (tz * sd.ntiles[1] + ty) * sd.ntiles[0] + tx;
   const int p0 = tile_start[tile], p1 = tile_start[tile + 1];
   if (p0 == p1) return;  // no atom reaches this tile
@@ -933,7 +1030,7 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma_ad(
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int fr = lane >> 2, fk = lane & 3;
-  const int nslots = sd.S[0] * sd.S[1] * sd.S[2];
+  const int nslots = sd.pstride;
   double(*W)[8][kWRow] = sW[warp];
   cp_async_wait_all();
   __syncthreads();  // the tile, staged by all warps; the only CTA barrier
@@ -1018,20 +1115,20 @@ struct RecRows {
 // LPA lanes per atom (32, or 8 when an atom has at most 32 slots: four atoms
 // per warp).
 template <int NC, int LPA>
-__global__ void k_gather_final(const int4* __restrict__ slot, const int* __restrict__ perm,
-                               const double* __restrict__ part, int n, StencilDims sd,
-                               const double* __restrict__ q, double self_coef, double pot_shift,
-                               const double* __restrict__ pot_sr, const double* __restrict__ f_sr,
-                               double* __restrict__ pot, double* __restrict__ force, RecRows rr) {
-  const long t = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  const int k = static_cast<int>(t / LPA);
-  const int lane = static_cast<int>(t % LPA);
-  // Lanes past the last atom stay to the end: the shuffles below take the whole warp.
-  const bool live = k < n;
+__device__ __forceinline__ void gather_final_body(const int4* __restrict__ slot,
+                                                  const int* __restrict__ perm,
+                                                  const double* __restrict__ part, int k,
+                                                  int lane, bool live, const StencilDims& sd,
+                                                  const double* __restrict__ q, double self_coef,
+                                                  double pot_shift,
+                                                  const double* __restrict__ pot_sr,
+                                                  const double* __restrict__ f_sr,
+                                                  double* __restrict__ pot,
+                                                  double* __restrict__ force, const RecRows& rr) {
   const int4 si = live ? slot[k] : make_int4(0, 0, 0, 0);
   const int cx = slot_count(si.x), cy = slot_count(si.y), cz = slot_count(si.z);
   const int nslots = sd.S[0] * sd.S[1] * sd.S[2];
-  const double* pk = part + static_cast<size_t>(live ? k : 0) * nslots * NC;
+  const double* pk = part + static_cast<size_t>(live ? k : 0) * sd.pstride * NC;
   double acc[NC];
 #pragma unroll
   for (int c = 0; c < NC; ++c) acc[c] = 0.0;
@@ -1064,6 +1161,44 @@ __global__ void k_gather_final(const int4* __restrict__ slot, const int* __restr
   }
 }
 
+template <int NC, int LPA>
+__global__ void k_gather_final(const int4* __restrict__ slot, const int* __restrict__ perm,
+                               const double* __restrict__ part, int n, StencilDims sd,
+                               const double* __restrict__ q, double self_coef, double pot_shift,
+                               const double* __restrict__ pot_sr, const double* __restrict__ f_sr,
+                               double* __restrict__ pot, double* __restrict__ force, RecRows rr) {
+  const long t = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int k = static_cast<int>(t / LPA);
+  // Lanes past the last atom stay to the end: the shuffles below take the whole warp.
+  gather_final_body<NC, LPA>(slot, perm, part, k, static_cast<int>(t % LPA), k < n, sd, q,
+                             self_coef, pot_shift, pot_sr, f_sr, pot, force, rr);
+}
+
+// Every cell of a batch: the atom's cell gives its slot layout, self term and
+// dual basis (window-derivative partials are fractional derivatives).
+template <int NC, int LPA>
+__global__ void k_gather_final_seg(const BatchCell* __restrict__ cells,
+                                   const int* __restrict__ prefix, int ncells,
+                                   const int4* __restrict__ slot, const int* __restrict__ perm,
+                                   const double* __restrict__ part, int n,
+                                   const double* __restrict__ q, const double* __restrict__ pot_sr,
+                                   const double* __restrict__ f_sr, double* __restrict__ pot,
+                                   double* __restrict__ force) {
+  const long t = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int k = static_cast<int>(t / LPA);
+  const bool live = k < n;
+  const BatchCell& bc = cells[seg_cell(prefix, ncells, live ? k : n - 1)];
+  RecRows rr;
+  rr.on = 1;
+#pragma unroll
+  for (int a = 0; a < 3; ++a)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) rr.b[a][d] = bc.rec[a][d];
+  const StencilDims sd = bc.sd;
+  gather_final_body<NC, LPA>(slot, perm, part, k, static_cast<int>(t % LPA), live, sd, q,
+                             bc.self_coef, 0.0, pot_sr, f_sr, pot, force, rr);
+}
+
 // FP64 tensor-core throughput probe: every warp issues independent DMMAs on
 // register operands (eight accumulator pairs, no memory traffic), so the
 // measured rate is the m8n8k4 FP64 pipe's own.
@@ -1080,6 +1215,140 @@ __global__ void __launch_bounds__(128) k_dmma_peak(int iters, double seed, doubl
 #pragma unroll
   for (int i = 0; i < 8; ++i) t += acc[i][0] + acc[i][1];
   if (t == -1.0) sink[threadIdx.x] = t;  // never true; keeps the work live
+}
+
+// ---- the tile kernels: one tile per CTA (blockIdx = tile), or, for a batch,
+// the tiles of every cell (blockIdx.x over the cells' tiles end to end; the
+// cell's tile list, weights layout and grid from the batch table).
+__device__ __forceinline__ const BatchCell& tile_of_block(const BatchCell* __restrict__ cells,
+                                                          const int* __restrict__ prefix,
+                                                          int ncells, int* tx, int* ty, int* tz) {
+  const int c = seg_cell(prefix, ncells, blockIdx.x);
+  const BatchCell& bc = cells[c];
+  const int local = static_cast<int>(blockIdx.x) - prefix[c];
+  *tx = local % bc.sd.ntiles[0];
+  *ty = (local / bc.sd.ntiles[0]) % bc.sd.ntiles[1];
+  *tz = local / (bc.sd.ntiles[0] * bc.sd.ntiles[1]);
+  return bc;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kSpreadLanes) k_spread_tiles(const int* __restrict__ tile_start,
+                                                               const int2* __restrict__ pairs,
+                                                               const R* __restrict__ wtab,
+                                                               const R* __restrict__ qk,
+                                                               StencilDims sd, R* __restrict__ grid) {
+  spread_tiles_body<R>(blockIdx.x, blockIdx.y, blockIdx.z, tile_start, pairs, wtab, qk, sd, grid);
+}
+template <typename R>
+__global__ void __launch_bounds__(kSpreadLanes) k_spread_tiles_seg(
+    const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells,
+    const int* __restrict__ tile_start, const int2* __restrict__ pairs, const R* __restrict__ wtab,
+    const R* __restrict__ qk) {
+  int tx, ty, tz;
+  const BatchCell& bc = tile_of_block(cells, prefix, ncells, &tx, &ty, &tz);
+  spread_tiles_body<R>(tx, ty, tz, tile_start + bc.tile0, pairs, wtab, qk, bc.sd,
+                       static_cast<R*>(bc.grid));
+}
+
+__global__ void __launch_bounds__(32) k_spread_tiles_dmma(const int* __restrict__ tile_start,
+                                                          const int2* __restrict__ pairs,
+                                                          const double* __restrict__ wtab,
+                                                          const double* __restrict__ qk,
+                                                          StencilDims sd,
+                                                          double* __restrict__ grid) {
+  spread_tiles_dmma_body(blockIdx.x, blockIdx.y, blockIdx.z, tile_start, pairs, wtab, qk, sd, grid);
+}
+__global__ void __launch_bounds__(32) k_spread_tiles_dmma_seg(
+    const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells,
+    const int* __restrict__ tile_start, const int2* __restrict__ pairs,
+    const double* __restrict__ wtab, const double* __restrict__ qk) {
+  int tx, ty, tz;
+  const BatchCell& bc = tile_of_block(cells, prefix, ncells, &tx, &ty, &tz);
+  spread_tiles_dmma_body(tx, ty, tz, tile_start + bc.tile0, pairs, wtab, qk, bc.sd,
+                         static_cast<double*>(bc.grid));
+}
+
+template <typename R, int NC, int A, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) k_gather_tiles(const int* __restrict__ tile_start,
+                                                             const int2* __restrict__ pairs,
+                                                             const R* __restrict__ wtab,
+                                                             StencilDims sd,
+                                                             const R* __restrict__ grid,
+                                                             double* __restrict__ part) {
+  gather_tiles_body<R, NC, A, WARPS>(blockIdx.x, blockIdx.y, blockIdx.z, tile_start, pairs, wtab,
+                                     sd, grid, part);
+}
+template <typename R, int NC, int A, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_seg(
+    const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells,
+    const int* __restrict__ tile_start, const int2* __restrict__ pairs, const R* __restrict__ wtab,
+    double* __restrict__ part) {
+  int tx, ty, tz;
+  const BatchCell& bc = tile_of_block(cells, prefix, ncells, &tx, &ty, &tz);
+  gather_tiles_body<R, NC, A, WARPS>(tx, ty, tz, tile_start + bc.tile0, pairs, wtab, bc.sd,
+                                     static_cast<const R*>(bc.out), part);
+}
+
+template <int A, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_ad(const int* __restrict__ tile_start,
+                                                                const int2* __restrict__ pairs,
+                                                                const float* __restrict__ wtab,
+                                                                StencilDims sd,
+                                                                const float* __restrict__ grid,
+                                                                double* __restrict__ part) {
+  gather_tiles_ad_body<A, WARPS>(blockIdx.x, blockIdx.y, blockIdx.z, tile_start, pairs, wtab, sd,
+                                 grid, part);
+}
+template <int A, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_ad_seg(
+    const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells,
+    const int* __restrict__ tile_start, const int2* __restrict__ pairs,
+    const float* __restrict__ wtab, double* __restrict__ part) {
+  int tx, ty, tz;
+  const BatchCell& bc = tile_of_block(cells, prefix, ncells, &tx, &ty, &tz);
+  gather_tiles_ad_body<A, WARPS>(tx, ty, tz, tile_start + bc.tile0, pairs, wtab, bc.sd,
+                                 static_cast<const float*>(bc.out), part);
+}
+
+template <int NC, int WARPS, int MB>
+__global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma(const int* __restrict__ tile_start,
+                                                                  const int2* __restrict__ pairs,
+                                                                  const double* __restrict__ wtab,
+                                                                  StencilDims sd,
+                                                                  const double* __restrict__ grid,
+                                                                  double* __restrict__ part) {
+  gather_tiles_dmma_body<NC, WARPS, MB>(blockIdx.x, blockIdx.y, blockIdx.z, tile_start, pairs,
+                                        wtab, sd, grid, part);
+}
+template <int NC, int WARPS, int MB>
+__global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma_seg(
+    const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells,
+    const int* __restrict__ tile_start, const int2* __restrict__ pairs,
+    const double* __restrict__ wtab, double* __restrict__ part) {
+  int tx, ty, tz;
+  const BatchCell& bc = tile_of_block(cells, prefix, ncells, &tx, &ty, &tz);
+  gather_tiles_dmma_body<NC, WARPS, MB>(tx, ty, tz, tile_start + bc.tile0, pairs, wtab, bc.sd,
+                                        static_cast<const double*>(bc.out), part);
+}
+
+template <int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma_ad(
+    const int* __restrict__ tile_start, const int2* __restrict__ pairs,
+    const double* __restrict__ wtab, StencilDims sd, const double* __restrict__ grid,
+    double* __restrict__ part) {
+  gather_tiles_dmma_ad_body<WARPS>(blockIdx.x, blockIdx.y, blockIdx.z, tile_start, pairs, wtab, sd,
+                                   grid, part);
+}
+template <int WARPS>
+__global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma_ad_seg(
+    const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells,
+    const int* __restrict__ tile_start, const int2* __restrict__ pairs,
+    const double* __restrict__ wtab, double* __restrict__ part) {
+  int tx, ty, tz;
+  const BatchCell& bc = tile_of_block(cells, prefix, ncells, &tx, &ty, &tz);
+  gather_tiles_dmma_ad_body<WARPS>(tx, ty, tz, tile_start + bc.tile0, pairs, wtab, bc.sd,
+                                   static_cast<const double*>(bc.out), part);
 }
 
 inline int blocks_for(long n, int threads) { return static_cast<int>((n + threads - 1) / threads); }
@@ -1199,6 +1468,114 @@ void launch_gather_final(const MeshPlan& mp, const int4* slot, const int* perm, 
       k_gather_final<1, 32><<<blocks_for(32L * n, 256), 256, 0, st>>>(
           slot, perm, part, n, mp.sd, q, self_coef, pot_shift, pot_sr, f_sr, pot, nullptr, rr);
   }
+  ++g_launches;
+}
+
+void launch_weights_seg(const BatchLaunch& b, const int4* mc, const double4* fr, const int* perm,
+                        void* wtab, void* qk, int4* slot, cudaStream_t st) {
+  if (b.n_weights == 0) return;
+  if (b.mixed)
+    launch_chained(k_weights_seg<float>, blocks_for(b.n_weights, 128), 128, 0, st, b.cells,
+                   b.p_weights, b.ncells, b.n_weights, mc, fr, perm, static_cast<float*>(wtab),
+                   static_cast<float*>(qk), slot);
+  else
+    launch_chained(k_weights_seg<double>, blocks_for(b.n_weights, 128), 128, 0, st, b.cells,
+                   b.p_weights, b.ncells, b.n_weights, mc, fr, perm, static_cast<double*>(wtab),
+                   static_cast<double*>(qk), slot);
+  ++g_launches;
+}
+
+void launch_pair_bins_seg(const BatchLaunch& b, const int4* slot, int* counts, int* cursor,
+                          int* tile_start, int4* tmp, int2* pairs, cudaStream_t st) {
+  int2* t2 = reinterpret_cast<int2*>(tmp);
+  cudaMemsetAsync(counts, 0, sizeof(int) * b.n_tiles, st);
+  cudaMemsetAsync(cursor, 0, sizeof(int) * b.n_tiles, st);
+  if (b.n_slots > 0) {
+    k_pair_count_seg<<<blocks_for(b.n_slots, 256), 256, 0, st>>>(b.cells, b.p_slots, b.ncells,
+                                                                 b.n_slots, slot, counts);
+    ++g_launches;
+  }
+  launch_scan(counts, b.n_tiles, tile_start, b.n_slots > 0, st);
+  if (b.n_slots > 0) {
+    launch_chained(k_pair_scatter_seg, blocks_for(b.n_slots, 256), 256, 0, st, b.cells, b.p_slots,
+                   b.ncells, b.n_slots, slot, tile_start, cursor, t2);
+    launch_chained(k_pair_rank_seg, blocks_for(b.n_slots, 256), 256, 0, st, b.cells, b.p_atoms,
+                   b.ncells, t2, tile_start, b.n_tiles, slot, pairs);
+    g_launches += 2;
+  }
+}
+
+void launch_spread_seg(const BatchLaunch& b, const int* tile_start, const int2* pairs,
+                       const void* wtab, const void* qk, cudaStream_t st) {
+  if (b.n_tiles == 0) return;
+  if (b.mixed)
+    launch_chained(k_spread_tiles_seg<float>, b.n_tiles, kSpreadLanes, 0, st, b.cells, b.p_tiles,
+                   b.ncells, tile_start, pairs, static_cast<const float*>(wtab),
+                   static_cast<const float*>(qk));
+  else
+    launch_chained(k_spread_tiles_dmma_seg, b.n_tiles, 32, 0, st, b.cells, b.p_tiles, b.ncells,
+                   tile_start, pairs, static_cast<const double*>(wtab),
+                   static_cast<const double*>(qk));
+  ++g_launches;
+}
+
+void launch_gather_seg(const BatchLaunch& b, const int* tile_start, const int2* pairs,
+                       const void* wtab, double* part, cudaStream_t st) {
+  if (b.n_tiles == 0) return;
+  const int nb = b.n_tiles;
+  if (b.ad && b.nc == 1 && b.nparts == 4) {  // window-differentiated forces
+    if (b.mixed)
+      launch_chained(k_gather_tiles_ad_seg<kGatherAdF32Atoms, kGatherAdF32Warps>, nb,
+                     32 * kGatherAdF32Warps, 0, st, b.cells, b.p_tiles, b.ncells, tile_start, pairs,
+                     static_cast<const float*>(wtab), part);
+    else
+      launch_chained(k_gather_tiles_dmma_ad_seg<kGatherAdWarps>, nb, 32 * kGatherAdWarps, 0, st,
+                     b.cells, b.p_tiles, b.ncells, tile_start, pairs,
+                     static_cast<const double*>(wtab), part);
+  } else if (b.mixed) {
+    const float* w = static_cast<const float*>(wtab);
+    if (b.nc == 4)
+      launch_chained(k_gather_tiles_seg<float, 4, GatherShape<float>::atoms, GatherShape<float>::warps>,
+                     nb, 32 * GatherShape<float>::warps, 0, st, b.cells, b.p_tiles, b.ncells,
+                     tile_start, pairs, w, part);
+    else
+      launch_chained(k_gather_tiles_seg<float, 1, GatherShape<float>::atoms, GatherShape<float>::warps>,
+                     nb, 32 * GatherShape<float>::warps, 0, st, b.cells, b.p_tiles, b.ncells,
+                     tile_start, pairs, w, part);
+  } else {
+    const double* w = static_cast<const double*>(wtab);
+    if (b.nc == 4)
+      launch_chained(k_gather_tiles_dmma_seg<4, kGatherWarps, kGatherMB>, nb, 32 * kGatherWarps, 0,
+                     st, b.cells, b.p_tiles, b.ncells, tile_start, pairs, w, part);
+    else
+      launch_chained(k_gather_tiles_dmma_seg<1, kGatherWarps, kGatherMB>, nb, 32 * kGatherWarps, 0,
+                     st, b.cells, b.p_tiles, b.ncells, tile_start, pairs, w, part);
+  }
+  ++g_launches;
+}
+
+void launch_gather_final_seg(const BatchLaunch& b, const int4* slot, const int* perm,
+                             const double* part, const double* q, const double* pot_sr,
+                             const double* f_sr, double* pot, double* force, cudaStream_t st) {
+  if (b.n_atoms == 0) return;
+  const int n = b.n_atoms;
+  const int blocks = blocks_for(static_cast<long>(b.lpa) * n, 256);
+#define EWG_FINAL(NC, LPA)                                                                   \
+  k_gather_final_seg<NC, LPA><<<blocks, 256, 0, st>>>(b.cells, b.p_atoms, b.ncells, slot, perm, \
+                                                      part, n, q, pot_sr, f_sr, pot,         \
+                                                      NC == 4 ? force : nullptr)
+  if (b.nparts == 4) {
+    if (b.lpa == 8)
+      EWG_FINAL(4, 8);
+    else
+      EWG_FINAL(4, 32);
+  } else {
+    if (b.lpa == 8)
+      EWG_FINAL(1, 8);
+    else
+      EWG_FINAL(1, 32);
+  }
+#undef EWG_FINAL
   ++g_launches;
 }
 

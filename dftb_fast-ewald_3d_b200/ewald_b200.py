@@ -351,7 +351,8 @@ class Context:
                                            alpha_in=alpha)
 
     def set_batch_lanes(self, lanes: int):
-        """Concurrent lanes of batched calls (1..16, default 4)."""
+        """Batched calls: 0 (default) runs every stage of all cells in one
+        segmented launch; 1..16 runs the cells on that many concurrent lanes."""
         _check(lib().ewg_set_batch_lanes(self._h, int(lanes)))
 
     def batch_potential_force(self, cells, tol=1e-10, want_force=True, **ov):

@@ -367,9 +367,11 @@ int ewg_last_stress_setup(const ewg_context* ctx, double* alpha, double* max_r, 
  * lat_rows 9 doubles per cell (Fortran rows layout); pot(total), force(3,total).
  * Each cell gets its own parameters from the reference chain.  Status of
  * cell c goes to cell_status[c] when cell_status is not NULL; the return value
- * is the first non-zero cell status.  The cells are spread round-robin over the
- * context's batch lanes (ewg_set_batch_lanes) and run concurrently; results do
- * not depend on the number of lanes. */
+ * is the first non-zero cell status.  By default every stage of every cell
+ * runs in one segmented launch (the cells' parameters, FFT plans and buffers
+ * in a device table), and a repeated batch is recorded as one CUDA graph and
+ * replayed; with ewg_set_batch_lanes(ctx, 1..16) the cells run instead on that
+ * many concurrent lanes.  Results are bitwise the same either way. */
 int ewg_batch_potential_force(ewg_context* ctx, int n_cells, const int* offsets,
                               const double* coords, const double* charges, const double* lat_rows,
                               double tol, double* pot, double* force, int* cell_status);
@@ -382,11 +384,13 @@ int ewg_batch_potential_force_ov(ewg_context* ctx, int n_cells, const int* offse
                                  const double* lat_rows, double tol, double* pot, double* force,
                                  int* cell_status, const ewg_overrides* ov);
 
-/* Batch lanes (1..16, default 4): independent cells of a batched call run
- * concurrently on this many lanes, each a sub-context of the same device, form
- * and settings with its own device buffers and streams (so each lane holds
- * the buffers of the largest cell it has run).  One lane runs the cells back to
- * back on the context itself.  No counterpart in the reference. */
+/* Batch lanes (0..16, default 0).  0: segmented launches, one per stage for
+ * all cells of a batched call (cells that fail their checks send the whole
+ * call to the lane path).  1..16: independent cells run concurrently on this
+ * many lanes, each a sub-context of the same device, form and settings with
+ * its own device buffers and streams (so each lane holds the buffers of the
+ * largest cell it has run); one lane runs the cells back to back on the
+ * context itself.  No counterpart in the reference. */
 int ewg_set_batch_lanes(ewg_context* ctx, int lanes);
 
 #ifdef __cplusplus

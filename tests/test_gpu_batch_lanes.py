@@ -48,7 +48,7 @@ def test_lanes_with_overrides_and_oracle(ewald_lib, oracle):
 def test_lane_count_range(ewald_lib):
     ctx = ewald_lib.Context(0, ewald_lib.FP64)
     try:
-        for bad in (0, 17):
+        for bad in (-1, 17):
             with pytest.raises(ewald_lib.EwaldError) as e:
                 ctx.set_batch_lanes(bad)
             assert e.value.code == 2  # EWG_ERR_ARG
