@@ -301,6 +301,78 @@ __device__ void edge_pass_generic(const cx<R>* __restrict__ in, cx<R>* __restric
   }
 }
 
+// ---------------------------------------------------------------------------
+// The same passes with the length, the radix schedule, the sub-length p and
+// the CTA size known at compile time: every index, loop bound and twiddle
+// offset folds to a constant and the butterfly loops unroll.  Arithmetic and
+// order are those of edge_pass, so results are bitwise the same.
+// ---------------------------------------------------------------------------
+template <typename R, int SIGN, int RR, int L, int T, int N, int P, bool FIRST, bool LAST,
+          class Load, class Store>
+__device__ __forceinline__ void edge_pass_s(const cx<R>* __restrict__ in, cx<R>* __restrict__ out,
+                                            cx<R>* spare, const cx<R>* __restrict__ tw,
+                                            Load& load, Store& store) {
+  constexpr int NR = N / RR;
+  constexpr int STEP = N / (P * RR);
+  constexpr int ISTEP = T / L;
+  constexpr int ITERS = (NR + ISTEP - 1) / ISTEP;
+  const int line = threadIdx.x & (L - 1);
+  const int i0 = threadIdx.x / L;
+#pragma unroll
+  for (int it = 0; it < ITERS; ++it) {
+    const int i = i0 + it * ISTEP;
+    if (NR % ISTEP != 0 && i >= NR) break;
+    const int j = i / P, k = i - j * P;
+    cx<R> u[RR];
+    if (FIRST) {
+#pragma unroll
+      for (int jj = 0; jj < RR; ++jj) u[jj] = load(line, i + jj * NR);
+    } else {
+      const cx<R>* src = in + i * L + line;
+#pragma unroll
+      for (int jj = 0; jj < RR; ++jj) u[jj] = src[jj * NR * L];
+      if (P > 1) {
+        if constexpr (sizeof(R) == 8) {
+          const cx<R> w1 = twiddle(tw, k * STEP, SIGN);
+          cx<R> w = w1;
+#pragma unroll
+          for (int jj = 1; jj < RR; ++jj) {
+            u[jj] = mul(u[jj], w);
+            if (jj + 1 < RR) w = mul(w, w1);
+          }
+        } else {
+#pragma unroll
+          for (int jj = 1; jj < RR; ++jj) u[jj] = mul(u[jj], twiddle(tw, jj * k * STEP, SIGN));
+        }
+      }
+    }
+    dft_fixed<R, SIGN, RR>(u, tw, N);
+    const int e0 = j * P * RR + k;
+    if (LAST) {
+#pragma unroll
+      for (int jj = 0; jj < RR; ++jj) store(line, e0 + jj * P, u[jj], spare);
+    } else {
+      cx<R>* dst = out + e0 * L + line;
+#pragma unroll
+      for (int jj = 0; jj < RR; ++jj) dst[jj * P * L] = u[jj];
+    }
+  }
+}
+
+// Three passes of radices R0, R1, R2 (N = R0 R1 R2, in the host factorisation's
+// order) on T threads; buffers as in fft_edges: the last pass's spare is a.
+template <typename R, int SIGN, int L, int T, int N, int R0, int R1, int R2, class Load,
+          class Store>
+__device__ __forceinline__ void fft_static3(cx<R>* a, cx<R>* b, const cx<R>* __restrict__ tw,
+                                            Load load, Store store) {
+  static_assert(R0 * R1 * R2 == N, "radix schedule");
+  edge_pass_s<R, SIGN, R0, L, T, N, 1, true, false>(b, a, a, tw, load, store);
+  __syncthreads();
+  edge_pass_s<R, SIGN, R1, L, T, N, R0, false, false>(a, b, b, tw, load, store);
+  __syncthreads();
+  edge_pass_s<R, SIGN, R2, L, T, N, R0 * R1, false, true>(b, a, a, tw, load, store);
+}
+
 template <typename R, int SIGN, int L, class Load, class Store>
 __device__ void fft_edges(cx<R>* a, cx<R>* b, int n, const FftPlan& plan,
                           const cx<R>* __restrict__ tw, Load load, Store store) {

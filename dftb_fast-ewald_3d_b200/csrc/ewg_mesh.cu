@@ -57,11 +57,30 @@ __device__ __forceinline__ cx<R>* spare_buffer(cx<R>* a, cx<R>* b, const FftPlan
   return (plan.nstages & 1) ? a : b;
 }
 
+// Transform shapes: the generic runtime schedule, or a length and three-radix
+// schedule fixed at compile time (fft_static3) for the lengths the benchmark
+// configurations use most.
+struct DynShape {
+  template <typename R, int SIGN, int L, class Ld, class St>
+  __device__ __forceinline__ static void run(cx<R>* a, cx<R>* b, int n, const FftPlan& plan,
+                                             const cx<R>* __restrict__ tw, Ld ld, St st) {
+    fft_edges<R, SIGN, L>(a, b, n, plan, tw, ld, st);
+  }
+};
+template <int N, int R0, int R1, int R2>
+struct StatShape {
+  template <typename R, int SIGN, int L, class Ld, class St>
+  __device__ __forceinline__ static void run(cx<R>* a, cx<R>* b, int, const FftPlan&,
+                                             const cx<R>* __restrict__ tw, Ld ld, St st) {
+    fft_static3<R, SIGN, L, pass_threads(L), N, R0, R1, R2>(a, b, tw, ld, st);
+  }
+};
+
 // ---------------------------------------------------------------------------
 // x pass, real to complex: row pairs (2p, 2p+1) form one complex line; keep
 // k1 = 0..K1-1 of each row.
 // ---------------------------------------------------------------------------
-template <typename R, int L>
+template <typename R, int L, class SH>
 __device__ __forceinline__ void fft_x_r2c_body(int bx, const R* __restrict__ grid,
                                                                cx<R>* __restrict__ A1, int n1,
                                                                int npairs, int K1, FftPlan plan) {
@@ -77,7 +96,7 @@ __device__ __forceinline__ void fft_x_r2c_body(int bx, const R* __restrict__ gri
   const R* rb = ra + n1;
   auto load = [&](int, int x) { return valid ? mk(ra[x], rb[x]) : mk(R(0), R(0)); };
   auto store = [&](int l, int k, cx<R> v, cx<R>* spare) { spare[k * L + l] = v; };
-  fft_edges<R, -1, L>(a, b, n1, plan, tw, load, store);
+  SH::template run<R, -1, L>(a, b, n1, plan, tw, load, store);
   __syncthreads();
   const cx<R>* res = spare_buffer(a, b, plan);
   const R h = R(0.5);
@@ -97,7 +116,7 @@ __device__ __forceinline__ void fft_x_r2c_body(int bx, const R* __restrict__ gri
 // ---------------------------------------------------------------------------
 // y pass, forward: lines over i2 for (i3, k1-block); keep k2 in [-H2, H2].
 // ---------------------------------------------------------------------------
-template <typename R, int L>
+template <typename R, int L, class SH>
 __device__ __forceinline__ void fft_y_fwd_body(int bx, int by, const cx<R>* __restrict__ A1,
                                                                cx<R>* __restrict__ A2, int n2,
                                                                int K1, int K2, int H2,
@@ -124,7 +143,7 @@ __device__ __forceinline__ void fft_y_fwd_body(int bx, int by, const cx<R>* __re
       return;
     if (kin) dst[k2i * K1] = v;
   };
-  fft_edges<R, -1, L>(a, b, n2, plan, tw, load, store);
+  SH::template run<R, -1, L>(a, b, n2, plan, tw, load, store);
 }
 
 // ---------------------------------------------------------------------------
@@ -143,7 +162,7 @@ struct InfluenceArgs {
 };
 
 // nz = 1 (potential) or 2 (also T3, the spectrum times 2 pi i k3).
-template <typename R, int L, bool STRESS>
+template <typename R, int L, bool STRESS, class SH>
 __device__ __forceinline__ void fft_z_influence_body(
     int bx, int by, int gx, const cx<R>* __restrict__ A2, cx<R>* __restrict__ B2, int n3, int K1, int K2, int K3, int nz,
     InfluenceArgs ia, FftPlan plan) {
@@ -211,7 +230,7 @@ __device__ __forceinline__ void fft_z_influence_body(
     q[(k3 + h3) * L + l] = mk(static_cast<R>(wt * static_cast<double>(g.x)),
                               static_cast<R>(wt * static_cast<double>(g.y)));
   };
-  fft_edges<R, -1, L>(a, b, n3, plan, tw, load_fwd, store_weighted);
+  SH::template run<R, -1, L>(a, b, n3, plan, tw, load_fwd, store_weighted);
   __syncthreads();
   if constexpr (STRESS) {  // fixed-order CTA sum: shuffle tree per warp, then warps in order
     __shared__ double sred[32][6];
@@ -249,7 +268,7 @@ __device__ __forceinline__ void fft_z_influence_body(
     auto store = [&](int, int i3, cx<R> v, cx<R>*) {
       if (kin) dst[i3 * zstride] = v;
     };
-    fft_edges<R, 1, L>(a, b, n3, plan, tw, load_inv, store);
+    SH::template run<R, 1, L>(a, b, n3, plan, tw, load_inv, store);
     __syncthreads();
   }
 }
@@ -259,7 +278,7 @@ __device__ __forceinline__ void fft_z_influence_body(
 // Components: 0 = IFFT_y(P) and, for forces, 1 = IFFT_y(2 pi i k2 P),
 // 2 = IFFT_y(T3), with P and T3 the z pass's two outputs.
 // ---------------------------------------------------------------------------
-template <typename R, int L>
+template <typename R, int L, class SH>
 __device__ __forceinline__ void fft_y_inv_body(int bx, int by, int bz, const cx<R>* __restrict__ B2,
                                                                cx<R>* __restrict__ B1, int n2,
                                                                int n3, int K1, int K2, int H2,
@@ -297,7 +316,7 @@ __device__ __forceinline__ void fft_y_inv_body(int bx, int by, int bz, const cx<
   auto store = [&](int, int i2, cx<R> v, cx<R>*) {
     if (kin) dst[i2 * K1] = v;
   };
-  fft_edges<R, 1, L>(a, b, n2, plan, tw, load, store);
+  SH::template run<R, 1, L>(a, b, n2, plan, tw, load, store);
 }
 
 // ---------------------------------------------------------------------------
@@ -308,7 +327,7 @@ __device__ __forceinline__ void fft_y_inv_body(int bx, int by, int bz, const cx<
 // phi = C2R(Y0), D1 = C2R(2 pi i k1 Y0), D2 = C2R(Y2), D3 = C2R(Y3), Y0, Y2, Y3
 // the y pass's three components.
 // ---------------------------------------------------------------------------
-template <typename R, int L, int NCG>
+template <typename R, int L, int NCG, class SH>
 __device__ __forceinline__ void fft_x_c2r_body(int bx, int by, const cx<R>* __restrict__ B1,
                                                                R* __restrict__ out, int n1,
                                                                int nrows, int K1, int nc,
@@ -361,45 +380,45 @@ __device__ __forceinline__ void fft_x_c2r_body(int bx, int by, const cx<R>* __re
     oa[x * nc] = v.x;
     ob[x * nc] = v.y;
   };
-  fft_edges<R, 1, L>(a, b, n1, plan, tw, load, store);
+  SH::template run<R, 1, L>(a, b, n1, plan, tw, load, store);
 }
 
 // ---- pass kernels: one cell (blockIdx = the pass's block), or every cell of a
 // batch (blockIdx.x over the cells' blocks end to end; the cell's lengths,
 // plans and buffers from the batch table; the lines per CTA are common).
-template <typename R, int L>
+template <typename R, int L, class SH = DynShape>
 __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_r2c(const R* __restrict__ grid,
                                                                cx<R>* __restrict__ A1, int n1,
                                                                int npairs, int K1, FftPlan plan) {
-  fft_x_r2c_body<R, L>(blockIdx.x, grid, A1, n1, npairs, K1, plan);
+  fft_x_r2c_body<R, L, SH>(blockIdx.x, grid, A1, n1, npairs, K1, plan);
 }
-template <typename R, int L>
+template <typename R, int L, class SH = DynShape>
 __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_fwd(const cx<R>* __restrict__ A1,
                                                                cx<R>* __restrict__ A2, int n2,
                                                                int K1, int K2, int H2,
                                                                FftPlan plan) {
-  fft_y_fwd_body<R, L>(blockIdx.x, blockIdx.y, A1, A2, n2, K1, K2, H2, plan);
+  fft_y_fwd_body<R, L, SH>(blockIdx.x, blockIdx.y, A1, A2, n2, K1, K2, H2, plan);
 }
-template <typename R, int L, bool STRESS>
+template <typename R, int L, bool STRESS, class SH = DynShape>
 __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
     const cx<R>* __restrict__ A2, cx<R>* __restrict__ B2, int n3, int K1, int K2, int K3, int nz,
     InfluenceArgs ia, FftPlan plan) {
-  fft_z_influence_body<R, L, STRESS>(blockIdx.x, blockIdx.y, gridDim.x, A2, B2, n3, K1, K2, K3, nz,
-                                     ia, plan);
+  fft_z_influence_body<R, L, STRESS, SH>(blockIdx.x, blockIdx.y, gridDim.x, A2, B2, n3, K1, K2,
+                                         K3, nz, ia, plan);
 }
-template <typename R, int L>
+template <typename R, int L, class SH = DynShape>
 __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_inv(const cx<R>* __restrict__ B2,
                                                                cx<R>* __restrict__ B1, int n2,
                                                                int n3, int K1, int K2, int H2,
                                                                FftPlan plan) {
-  fft_y_inv_body<R, L>(blockIdx.x, blockIdx.y, blockIdx.z, B2, B1, n2, n3, K1, K2, H2, plan);
+  fft_y_inv_body<R, L, SH>(blockIdx.x, blockIdx.y, blockIdx.z, B2, B1, n2, n3, K1, K2, H2, plan);
 }
-template <typename R, int L, int NCG>
+template <typename R, int L, int NCG, class SH = DynShape>
 __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_c2r(const cx<R>* __restrict__ B1,
                                                                R* __restrict__ out, int n1,
                                                                int nrows, int K1, int nc,
                                                                FftPlan plan) {
-  fft_x_c2r_body<R, L, NCG>(blockIdx.x, blockIdx.y, B1, out, n1, nrows, K1, nc, plan);
+  fft_x_c2r_body<R, L, NCG, SH>(blockIdx.x, blockIdx.y, B1, out, n1, nrows, K1, nc, plan);
 }
 
 // Blocks per cell of each pass (r2c, y forward, z, y inverse, c2r) at L lines
@@ -427,7 +446,7 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_r2c_seg(
   int local;
   const BatchCell& bc = pass_cell(cells, prefix, ncells, &local);
   const FftPlan plan = bc.fft[0];
-  fft_x_r2c_body<R, L>(local, static_cast<const R*>(bc.grid), static_cast<cx<R>*>(bc.A1),
+  fft_x_r2c_body<R, L, DynShape>(local, static_cast<const R*>(bc.grid), static_cast<cx<R>*>(bc.A1),
                        bc.g.n[0], bc.g.n[1] * bc.g.n[2] / 2, bc.g.K1, plan);
 }
 template <typename R, int L>
@@ -437,7 +456,7 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_fwd_seg(
   const BatchCell& bc = pass_cell(cells, prefix, ncells, &local);
   const int kb = (bc.g.K1 + L - 1) / L;
   const FftPlan plan = bc.fft[1];
-  fft_y_fwd_body<R, L>(local % kb, local / kb, static_cast<const cx<R>*>(bc.A1),
+  fft_y_fwd_body<R, L, DynShape>(local % kb, local / kb, static_cast<const cx<R>*>(bc.A1),
                        static_cast<cx<R>*>(bc.A2), bc.g.n[1], bc.g.K1, bc.g.K2,
                        (bc.g.K2 - 1) / 2, plan);
 }
@@ -461,7 +480,7 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence_seg(
   ia.inv4a2 = 1.0 / (4.0 * (bc.g.alpha * bc.g.alpha));
   ia.stress = nullptr;
   const FftPlan plan = bc.fft[2];
-  fft_z_influence_body<R, L, false>(local % kb, local / kb, kb, static_cast<const cx<R>*>(bc.A2),
+  fft_z_influence_body<R, L, false, DynShape>(local % kb, local / kb, kb, static_cast<const cx<R>*>(bc.A2),
                                     static_cast<cx<R>*>(bc.B2), bc.g.n[2], bc.g.K1, bc.g.K2,
                                     bc.g.K3, nz, ia, plan);
 }
@@ -473,7 +492,7 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_y_inv_seg(
   const int kb = (bc.g.K1 + L - 1) / L, n3 = bc.g.n[2];
   const int t = local / kb;
   const FftPlan plan = bc.fft[1];
-  fft_y_inv_body<R, L>(local % kb, t % n3, t / n3, static_cast<const cx<R>*>(bc.B2),
+  fft_y_inv_body<R, L, DynShape>(local % kb, t % n3, t / n3, static_cast<const cx<R>*>(bc.B2),
                        static_cast<cx<R>*>(bc.B1), bc.g.n[1], n3, bc.g.K1, bc.g.K2,
                        (bc.g.K2 - 1) / 2, plan);
 }
@@ -485,7 +504,7 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_x_c2r_seg(
   const int nrows = bc.g.n[1] * bc.g.n[2];
   const int nbx = (nrows / 2 + L / NCG - 1) / (L / NCG);
   const FftPlan plan = bc.fft[0];
-  fft_x_c2r_body<R, L, NCG>(local % nbx, local / nbx, static_cast<const cx<R>*>(bc.B1),
+  fft_x_c2r_body<R, L, NCG, DynShape>(local % nbx, local / nbx, static_cast<const cx<R>*>(bc.B1),
                             static_cast<R*>(bc.out), bc.g.n[0], nrows, bc.g.K1, nc, plan);
 }
 
@@ -520,6 +539,30 @@ void with_lines(int L, F&& f) {
   }
 }
 
+// Calls f(shape) with the compile-time shape of the plan's length when one is
+// specialised for this precision and lines per CTA (and the plan's radix
+// schedule is the one specialised), else f(DynShape{}).
+template <int N, int R0, int R1, int R2>
+bool is_schedule(const FftPlan& p) {
+  return p.n == N && p.nstages == 3 && p.radix[0] == R0 && p.radix[1] == R1 && p.radix[2] == R2;
+}
+template <typename R, int L, typename F>
+void with_shape(const FftPlan& p, F&& f) {
+  if constexpr (sizeof(R) == 8 && L == 4) {
+    if (is_schedule<280, 7, 5, 8>(p)) return f(StatShape<280, 7, 5, 8>{});
+    if (is_schedule<512, 8, 8, 8>(p)) return f(StatShape<512, 8, 8, 8>{});
+  }
+  if constexpr (sizeof(R) == 8 && L == 8) {
+    if (is_schedule<128, 8, 8, 2>(p)) return f(StatShape<128, 8, 8, 2>{});
+  }
+  if constexpr (sizeof(R) == 4 && L == 8) {
+    if (is_schedule<140, 7, 5, 4>(p)) return f(StatShape<140, 7, 5, 4>{});
+    if (is_schedule<160, 5, 8, 4>(p)) return f(StatShape<160, 5, 8, 4>{});
+    if (is_schedule<280, 7, 5, 8>(p)) return f(StatShape<280, 7, 5, 8>{});
+  }
+  f(DynShape{});
+}
+
 template <typename R>
 void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, void* B2v, int nc,
                   double* stress_part, cudaStream_t st) {
@@ -537,8 +580,10 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
     const int blocks = (npairs + L - 1) / L;
     with_lines(L, [&](auto lc) {
       constexpr int LL = decltype(lc)::value;
-      launch_chained(k_fft_x_r2c<R, LL>, blocks, pass_threads(LL), sm, st, static_cast<const R*>(grid), A1, n1, npairs,
-                                                       g.K1, mp.fft[0]);
+      with_shape<R, LL>(mp.fft[0], [&](auto sh) {
+        launch_chained(k_fft_x_r2c<R, LL, decltype(sh)>, blocks, pass_threads(LL), sm, st,
+                       static_cast<const R*>(grid), A1, n1, npairs, g.K1, mp.fft[0]);
+      });
     });
     ++g_launches;
   }
@@ -550,7 +595,10 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
     const int H2 = (g.K2 - 1) / 2;
     with_lines(L, [&](auto lc) {
       constexpr int LL = decltype(lc)::value;
-      launch_chained(k_fft_y_fwd<R, LL>, grd, pass_threads(LL), sm, st, A1, A2, n2, g.K1, g.K2, H2, mp.fft[1]);
+      with_shape<R, LL>(mp.fft[1], [&](auto sh) {
+        launch_chained(k_fft_y_fwd<R, LL, decltype(sh)>, grd, pass_threads(LL), sm, st, A1, A2, n2,
+                       g.K1, g.K2, H2, mp.fft[1]);
+      });
     });
     ++g_launches;
   }
@@ -574,12 +622,15 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
     dim3 grd((g.K1 + L - 1) / L, g.K2);
     with_lines(L, [&](auto lc) {
       constexpr int LL = decltype(lc)::value;
-      if (stress_part)
-        launch_chained(k_fft_z_influence<R, LL, true>, grd, pass_threads(LL), sm, st,
-            A2, B2, n3, g.K1, g.K2, g.K3, nz, ia, mp.fft[2]);
-      else
-        launch_chained(k_fft_z_influence<R, LL, false>, grd, pass_threads(LL), sm, st,
-            A2, B2, n3, g.K1, g.K2, g.K3, nz, ia, mp.fft[2]);
+      with_shape<R, LL>(mp.fft[2], [&](auto sh) {
+        using SH = decltype(sh);
+        if (stress_part)
+          launch_chained(k_fft_z_influence<R, LL, true, SH>, grd, pass_threads(LL), sm, st, A2, B2,
+                         n3, g.K1, g.K2, g.K3, nz, ia, mp.fft[2]);
+        else
+          launch_chained(k_fft_z_influence<R, LL, false, SH>, grd, pass_threads(LL), sm, st, A2, B2,
+                         n3, g.K1, g.K2, g.K3, nz, ia, mp.fft[2]);
+      });
     });
     ++g_launches;
   }
@@ -601,7 +652,10 @@ void inverse_impl(const MeshPlan& mp, const void* B2v, void* B1v, void* out, int
     const int H2 = (g.K2 - 1) / 2;
     with_lines(L, [&](auto lc) {
       constexpr int LL = decltype(lc)::value;
-      launch_chained(k_fft_y_inv<R, LL>, grd, pass_threads(LL), sm, st, B2, B1, n2, n3, g.K1, g.K2, H2, mp.fft[1]);
+      with_shape<R, LL>(mp.fft[1], [&](auto sh) {
+        launch_chained(k_fft_y_inv<R, LL, decltype(sh)>, grd, pass_threads(LL), sm, st, B2, B1, n2,
+                       n3, g.K1, g.K2, H2, mp.fft[1]);
+      });
     });
     ++g_launches;
   }
@@ -614,15 +668,22 @@ void inverse_impl(const MeshPlan& mp, const void* B2v, void* B1v, void* out, int
     if (nc == 4 && L >= 4) {  // the four components of a row pair in one CTA
       const int NP = L / 4;
       dim3 grd((nrows / 2 + NP - 1) / NP, 1);
-      if (L == 8)
-        launch_chained(k_fft_x_c2r<R, 8, 4>, grd, pass_threads(8), sm, st, B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
-      else
-        launch_chained(k_fft_x_c2r<R, 4, 4>, grd, pass_threads(4), sm, st, B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
+      with_lines(L, [&](auto lc) {
+        constexpr int LL = decltype(lc)::value;
+        if constexpr (LL >= 4)
+          with_shape<R, LL>(mp.fft[0], [&](auto sh) {
+            launch_chained(k_fft_x_c2r<R, LL, 4, decltype(sh)>, grd, pass_threads(LL), sm, st, B1,
+                           o, n1, nrows, g.K1, nc, mp.fft[0]);
+          });
+      });
     } else {  // one component per CTA row (grid.y = component)
       dim3 grd((nrows / 2 + L - 1) / L, nc);
       with_lines(L, [&](auto lc) {
         constexpr int LL = decltype(lc)::value;
-        launch_chained(k_fft_x_c2r<R, LL, 1>, grd, pass_threads(LL), sm, st, B1, o, n1, nrows, g.K1, nc, mp.fft[0]);
+        with_shape<R, LL>(mp.fft[0], [&](auto sh) {
+          launch_chained(k_fft_x_c2r<R, LL, 1, decltype(sh)>, grd, pass_threads(LL), sm, st, B1, o,
+                         n1, nrows, g.K1, nc, mp.fft[0]);
+        });
       });
     }
     ++g_launches;
@@ -645,8 +706,24 @@ void allow_lines() {
              k_fft_y_inv_seg<R, L>, k_fft_x_c2r_seg<R, L, 1>);
 }
 
+template <typename R, int L, class SH>
+void allow_shape() {
+  allow_smem(k_fft_x_r2c<R, L, SH>, k_fft_y_fwd<R, L, SH>, k_fft_z_influence<R, L, false, SH>,
+             k_fft_z_influence<R, L, true, SH>, k_fft_y_inv<R, L, SH>, k_fft_x_c2r<R, L, 1, SH>,
+             k_fft_x_c2r<R, L, 4, SH>);
+}
+
 template <typename R>
 void allow_all() {
+  if constexpr (sizeof(R) == 8) {
+    allow_shape<R, 4, StatShape<280, 7, 5, 8>>();
+    allow_shape<R, 4, StatShape<512, 8, 8, 8>>();
+    allow_shape<R, 8, StatShape<128, 8, 8, 2>>();
+  } else {
+    allow_shape<R, 8, StatShape<140, 7, 5, 4>>();
+    allow_shape<R, 8, StatShape<160, 5, 8, 4>>();
+    allow_shape<R, 8, StatShape<280, 7, 5, 8>>();
+  }
   allow_lines<R, 8>();
   allow_lines<R, 4>();
   allow_lines<R, 2>();

@@ -115,12 +115,16 @@ def test_mesh_potential_at_the_charges_equals_the_fast_path_at_32k(ewald_lib, ct
 
 def test_mesh_cost_is_linear_in_the_points(ctx):
     def timed(n_mol):
+        # best of several calls: a host or allocation hiccup in one call must
+        # not decide the comparison
         pos, q, lat = W.water_box(n_mol, seed=17)
         ctx.potential_at(pos, pos, q, lat.T, 1e-10)  # first call: buffers and plans
-        t0 = time.perf_counter()
-        for _ in range(3):
+        best = float("inf")
+        for _ in range(7):
+            t0 = time.perf_counter()
             ctx.potential_at(pos, pos, q, lat.T, 1e-10)
-        return (time.perf_counter() - t0) / 3
+            best = min(best, time.perf_counter() - t0)
+        return best
 
     t_small = timed(2731)   # 8,193 points on 8,193 charges
     t_large = timed(10923)  # 32,769 on 32,769: four times the points
