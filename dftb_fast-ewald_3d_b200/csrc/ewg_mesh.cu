@@ -61,18 +61,24 @@ __device__ __forceinline__ cx<R>* spare_buffer(cx<R>* a, cx<R>* b, const FftPlan
 // schedule fixed at compile time (fft_static3) for the lengths the benchmark
 // configurations use most.
 struct DynShape {
+  template <int L>
+  static constexpr int threads() { return pass_threads(L); }
   template <typename R, int SIGN, int L, class Ld, class St>
   __device__ __forceinline__ static void run(cx<R>* a, cx<R>* b, int n, const FftPlan& plan,
                                              const cx<R>* __restrict__ tw, Ld ld, St st) {
     fft_edges<R, SIGN, L>(a, b, n, plan, tw, ld, st);
   }
 };
-template <int N, int R0, int R1, int R2>
+// TPL threads per line: the butterflies of a pass per line are N / radix, so a
+// count that divides them (or just exceeds them) saves rounds over 32.
+template <int N, int R0, int R1, int R2, int TPL = 32>
 struct StatShape {
+  template <int L>
+  static constexpr int threads() { return L * TPL; }
   template <typename R, int SIGN, int L, class Ld, class St>
   __device__ __forceinline__ static void run(cx<R>* a, cx<R>* b, int, const FftPlan&,
                                              const cx<R>* __restrict__ tw, Ld ld, St st) {
-    fft_static3<R, SIGN, L, pass_threads(L), N, R0, R1, R2>(a, b, tw, ld, st);
+    fft_static3<R, SIGN, L, L * TPL, N, R0, R1, R2>(a, b, tw, ld, st);
   }
 };
 
@@ -387,34 +393,34 @@ __device__ __forceinline__ void fft_x_c2r_body(int bx, int by, const cx<R>* __re
 // batch (blockIdx.x over the cells' blocks end to end; the cell's lengths,
 // plans and buffers from the batch table; the lines per CTA are common).
 template <typename R, int L, class SH = DynShape>
-__global__ void __launch_bounds__(pass_threads(L)) k_fft_x_r2c(const R* __restrict__ grid,
+__global__ void __launch_bounds__(SH::template threads<L>()) k_fft_x_r2c(const R* __restrict__ grid,
                                                                cx<R>* __restrict__ A1, int n1,
                                                                int npairs, int K1, FftPlan plan) {
   fft_x_r2c_body<R, L, SH>(blockIdx.x, grid, A1, n1, npairs, K1, plan);
 }
 template <typename R, int L, class SH = DynShape>
-__global__ void __launch_bounds__(pass_threads(L)) k_fft_y_fwd(const cx<R>* __restrict__ A1,
+__global__ void __launch_bounds__(SH::template threads<L>()) k_fft_y_fwd(const cx<R>* __restrict__ A1,
                                                                cx<R>* __restrict__ A2, int n2,
                                                                int K1, int K2, int H2,
                                                                FftPlan plan) {
   fft_y_fwd_body<R, L, SH>(blockIdx.x, blockIdx.y, A1, A2, n2, K1, K2, H2, plan);
 }
 template <typename R, int L, bool STRESS, class SH = DynShape>
-__global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence(
+__global__ void __launch_bounds__(SH::template threads<L>()) k_fft_z_influence(
     const cx<R>* __restrict__ A2, cx<R>* __restrict__ B2, int n3, int K1, int K2, int K3, int nz,
     InfluenceArgs ia, FftPlan plan) {
   fft_z_influence_body<R, L, STRESS, SH>(blockIdx.x, blockIdx.y, gridDim.x, A2, B2, n3, K1, K2,
                                          K3, nz, ia, plan);
 }
 template <typename R, int L, class SH = DynShape>
-__global__ void __launch_bounds__(pass_threads(L)) k_fft_y_inv(const cx<R>* __restrict__ B2,
+__global__ void __launch_bounds__(SH::template threads<L>()) k_fft_y_inv(const cx<R>* __restrict__ B2,
                                                                cx<R>* __restrict__ B1, int n2,
                                                                int n3, int K1, int K2, int H2,
                                                                FftPlan plan) {
   fft_y_inv_body<R, L, SH>(blockIdx.x, blockIdx.y, blockIdx.z, B2, B1, n2, n3, K1, K2, H2, plan);
 }
 template <typename R, int L, int NCG, class SH = DynShape>
-__global__ void __launch_bounds__(pass_threads(L)) k_fft_x_c2r(const cx<R>* __restrict__ B1,
+__global__ void __launch_bounds__(SH::template threads<L>()) k_fft_x_c2r(const cx<R>* __restrict__ B1,
                                                                R* __restrict__ out, int n1,
                                                                int nrows, int K1, int nc,
                                                                FftPlan plan) {
@@ -549,16 +555,16 @@ bool is_schedule(const FftPlan& p) {
 template <typename R, int L, typename F>
 void with_shape(const FftPlan& p, F&& f) {
   if constexpr (sizeof(R) == 8 && L == 4) {
-    if (is_schedule<280, 7, 5, 8>(p)) return f(StatShape<280, 7, 5, 8>{});
-    if (is_schedule<512, 8, 8, 8>(p)) return f(StatShape<512, 8, 8, 8>{});
+    if (is_schedule<280, 7, 5, 8>(p)) return f(StatShape<280, 7, 5, 8, 40>{});
+    if (is_schedule<512, 8, 8, 8>(p)) return f(StatShape<512, 8, 8, 8, 64>{});
   }
   if constexpr (sizeof(R) == 8 && L == 8) {
     if (is_schedule<128, 8, 8, 2>(p)) return f(StatShape<128, 8, 8, 2>{});
   }
   if constexpr (sizeof(R) == 4 && L == 8) {
-    if (is_schedule<140, 7, 5, 4>(p)) return f(StatShape<140, 7, 5, 4>{});
-    if (is_schedule<160, 5, 8, 4>(p)) return f(StatShape<160, 5, 8, 4>{});
-    if (is_schedule<280, 7, 5, 8>(p)) return f(StatShape<280, 7, 5, 8>{});
+    if (is_schedule<140, 7, 5, 4>(p)) return f(StatShape<140, 7, 5, 4, 36>{});
+    if (is_schedule<160, 5, 8, 4>(p)) return f(StatShape<160, 5, 8, 4, 40>{});
+    if (is_schedule<280, 7, 5, 8>(p)) return f(StatShape<280, 7, 5, 8, 40>{});
   }
   f(DynShape{});
 }
@@ -581,7 +587,7 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
     with_lines(L, [&](auto lc) {
       constexpr int LL = decltype(lc)::value;
       with_shape<R, LL>(mp.fft[0], [&](auto sh) {
-        launch_chained(k_fft_x_r2c<R, LL, decltype(sh)>, blocks, pass_threads(LL), sm, st,
+        launch_chained(k_fft_x_r2c<R, LL, decltype(sh)>, blocks, decltype(sh)::template threads<LL>(), sm, st,
                        static_cast<const R*>(grid), A1, n1, npairs, g.K1, mp.fft[0]);
       });
     });
@@ -596,7 +602,7 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
     with_lines(L, [&](auto lc) {
       constexpr int LL = decltype(lc)::value;
       with_shape<R, LL>(mp.fft[1], [&](auto sh) {
-        launch_chained(k_fft_y_fwd<R, LL, decltype(sh)>, grd, pass_threads(LL), sm, st, A1, A2, n2,
+        launch_chained(k_fft_y_fwd<R, LL, decltype(sh)>, grd, decltype(sh)::template threads<LL>(), sm, st, A1, A2, n2,
                        g.K1, g.K2, H2, mp.fft[1]);
       });
     });
@@ -625,10 +631,10 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
       with_shape<R, LL>(mp.fft[2], [&](auto sh) {
         using SH = decltype(sh);
         if (stress_part)
-          launch_chained(k_fft_z_influence<R, LL, true, SH>, grd, pass_threads(LL), sm, st, A2, B2,
+          launch_chained(k_fft_z_influence<R, LL, true, SH>, grd, SH::template threads<LL>(), sm, st, A2, B2,
                          n3, g.K1, g.K2, g.K3, nz, ia, mp.fft[2]);
         else
-          launch_chained(k_fft_z_influence<R, LL, false, SH>, grd, pass_threads(LL), sm, st, A2, B2,
+          launch_chained(k_fft_z_influence<R, LL, false, SH>, grd, SH::template threads<LL>(), sm, st, A2, B2,
                          n3, g.K1, g.K2, g.K3, nz, ia, mp.fft[2]);
       });
     });
@@ -653,7 +659,7 @@ void inverse_impl(const MeshPlan& mp, const void* B2v, void* B1v, void* out, int
     with_lines(L, [&](auto lc) {
       constexpr int LL = decltype(lc)::value;
       with_shape<R, LL>(mp.fft[1], [&](auto sh) {
-        launch_chained(k_fft_y_inv<R, LL, decltype(sh)>, grd, pass_threads(LL), sm, st, B2, B1, n2,
+        launch_chained(k_fft_y_inv<R, LL, decltype(sh)>, grd, decltype(sh)::template threads<LL>(), sm, st, B2, B1, n2,
                        n3, g.K1, g.K2, H2, mp.fft[1]);
       });
     });
@@ -672,7 +678,7 @@ void inverse_impl(const MeshPlan& mp, const void* B2v, void* B1v, void* out, int
         constexpr int LL = decltype(lc)::value;
         if constexpr (LL >= 4)
           with_shape<R, LL>(mp.fft[0], [&](auto sh) {
-            launch_chained(k_fft_x_c2r<R, LL, 4, decltype(sh)>, grd, pass_threads(LL), sm, st, B1,
+            launch_chained(k_fft_x_c2r<R, LL, 4, decltype(sh)>, grd, decltype(sh)::template threads<LL>(), sm, st, B1,
                            o, n1, nrows, g.K1, nc, mp.fft[0]);
           });
       });
@@ -681,7 +687,7 @@ void inverse_impl(const MeshPlan& mp, const void* B2v, void* B1v, void* out, int
       with_lines(L, [&](auto lc) {
         constexpr int LL = decltype(lc)::value;
         with_shape<R, LL>(mp.fft[0], [&](auto sh) {
-          launch_chained(k_fft_x_c2r<R, LL, 1, decltype(sh)>, grd, pass_threads(LL), sm, st, B1, o,
+          launch_chained(k_fft_x_c2r<R, LL, 1, decltype(sh)>, grd, decltype(sh)::template threads<LL>(), sm, st, B1, o,
                          n1, nrows, g.K1, nc, mp.fft[0]);
         });
       });
@@ -716,13 +722,13 @@ void allow_shape() {
 template <typename R>
 void allow_all() {
   if constexpr (sizeof(R) == 8) {
-    allow_shape<R, 4, StatShape<280, 7, 5, 8>>();
-    allow_shape<R, 4, StatShape<512, 8, 8, 8>>();
+    allow_shape<R, 4, StatShape<280, 7, 5, 8, 40>>();
+    allow_shape<R, 4, StatShape<512, 8, 8, 8, 64>>();
     allow_shape<R, 8, StatShape<128, 8, 8, 2>>();
   } else {
-    allow_shape<R, 8, StatShape<140, 7, 5, 4>>();
-    allow_shape<R, 8, StatShape<160, 5, 8, 4>>();
-    allow_shape<R, 8, StatShape<280, 7, 5, 8>>();
+    allow_shape<R, 8, StatShape<140, 7, 5, 4, 36>>();
+    allow_shape<R, 8, StatShape<160, 5, 8, 4, 40>>();
+    allow_shape<R, 8, StatShape<280, 7, 5, 8, 40>>();
   }
   allow_lines<R, 8>();
   allow_lines<R, 4>();
