@@ -762,6 +762,11 @@ int seg_plan(ewg_context* c, int n_cells, const int* offsets, const std::vector<
   b.ad = ad ? 1 : 0;
   b.L = L;
   b.lpa = lpa;
+  for (int d = 0; d < 3; ++d) {
+    b.uniform[d] = 1;
+    for (int ci = 1; ci < n_cells; ++ci) b.uniform[d] &= sp.cells[ci].g.n[d] == sp.cells[0].g.n[d];
+    b.plan[d] = sp.cells[0].fft[d];
+  }
   for (int d = 0; d < 3; ++d) b.smem[d] = mesh_pass_smem(nmax[d], L, mixed, 0);
   b.smem_z = smz;
   b.n_atoms = pre(SP_ATOMS)[n_cells];

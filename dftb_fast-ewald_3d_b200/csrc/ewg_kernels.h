@@ -200,6 +200,8 @@ struct BatchLaunch {
   int ncells = 0;
   int mixed = 0, nc = 1, nparts = 1, ad = 0;
   int L = 1;           // FFT lines per CTA, one value for every cell
+  int uniform[3] = {0, 0, 0};  // every cell has the same length along this axis
+  FftPlan plan[3];             // that length's plan (when uniform)
   size_t smem[3] = {0, 0, 0};  // FFT pass shared memory per axis (the largest cell's)
   size_t smem_z = 0;
   int lpa = 32;        // lanes per atom of the final sum

@@ -446,28 +446,28 @@ __device__ __forceinline__ const BatchCell& pass_cell(const BatchCell* __restric
   return cells[c];
 }
 
-template <typename R, int L>
-__global__ void __launch_bounds__(pass_threads(L)) k_fft_x_r2c_seg(
+template <typename R, int L, class SH = DynShape>
+__global__ void __launch_bounds__(SH::template threads<L>()) k_fft_x_r2c_seg(
     const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells) {
   int local;
   const BatchCell& bc = pass_cell(cells, prefix, ncells, &local);
   const FftPlan plan = bc.fft[0];
-  fft_x_r2c_body<R, L, DynShape>(local, static_cast<const R*>(bc.grid), static_cast<cx<R>*>(bc.A1),
+  fft_x_r2c_body<R, L, SH>(local, static_cast<const R*>(bc.grid), static_cast<cx<R>*>(bc.A1),
                        bc.g.n[0], bc.g.n[1] * bc.g.n[2] / 2, bc.g.K1, plan);
 }
-template <typename R, int L>
-__global__ void __launch_bounds__(pass_threads(L)) k_fft_y_fwd_seg(
+template <typename R, int L, class SH = DynShape>
+__global__ void __launch_bounds__(SH::template threads<L>()) k_fft_y_fwd_seg(
     const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells) {
   int local;
   const BatchCell& bc = pass_cell(cells, prefix, ncells, &local);
   const int kb = (bc.g.K1 + L - 1) / L;
   const FftPlan plan = bc.fft[1];
-  fft_y_fwd_body<R, L, DynShape>(local % kb, local / kb, static_cast<const cx<R>*>(bc.A1),
+  fft_y_fwd_body<R, L, SH>(local % kb, local / kb, static_cast<const cx<R>*>(bc.A1),
                        static_cast<cx<R>*>(bc.A2), bc.g.n[1], bc.g.K1, bc.g.K2,
                        (bc.g.K2 - 1) / 2, plan);
 }
-template <typename R, int L>
-__global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence_seg(
+template <typename R, int L, class SH = DynShape>
+__global__ void __launch_bounds__(SH::template threads<L>()) k_fft_z_influence_seg(
     const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells, int nz) {
   int local;
   const BatchCell& bc = pass_cell(cells, prefix, ncells, &local);
@@ -486,31 +486,31 @@ __global__ void __launch_bounds__(pass_threads(L)) k_fft_z_influence_seg(
   ia.inv4a2 = 1.0 / (4.0 * (bc.g.alpha * bc.g.alpha));
   ia.stress = nullptr;
   const FftPlan plan = bc.fft[2];
-  fft_z_influence_body<R, L, false, DynShape>(local % kb, local / kb, kb, static_cast<const cx<R>*>(bc.A2),
+  fft_z_influence_body<R, L, false, SH>(local % kb, local / kb, kb, static_cast<const cx<R>*>(bc.A2),
                                     static_cast<cx<R>*>(bc.B2), bc.g.n[2], bc.g.K1, bc.g.K2,
                                     bc.g.K3, nz, ia, plan);
 }
-template <typename R, int L>
-__global__ void __launch_bounds__(pass_threads(L)) k_fft_y_inv_seg(
+template <typename R, int L, class SH = DynShape>
+__global__ void __launch_bounds__(SH::template threads<L>()) k_fft_y_inv_seg(
     const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells) {
   int local;
   const BatchCell& bc = pass_cell(cells, prefix, ncells, &local);
   const int kb = (bc.g.K1 + L - 1) / L, n3 = bc.g.n[2];
   const int t = local / kb;
   const FftPlan plan = bc.fft[1];
-  fft_y_inv_body<R, L, DynShape>(local % kb, t % n3, t / n3, static_cast<const cx<R>*>(bc.B2),
+  fft_y_inv_body<R, L, SH>(local % kb, t % n3, t / n3, static_cast<const cx<R>*>(bc.B2),
                        static_cast<cx<R>*>(bc.B1), bc.g.n[1], n3, bc.g.K1, bc.g.K2,
                        (bc.g.K2 - 1) / 2, plan);
 }
-template <typename R, int L, int NCG>
-__global__ void __launch_bounds__(pass_threads(L)) k_fft_x_c2r_seg(
+template <typename R, int L, int NCG, class SH = DynShape>
+__global__ void __launch_bounds__(SH::template threads<L>()) k_fft_x_c2r_seg(
     const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells, int nc) {
   int local;
   const BatchCell& bc = pass_cell(cells, prefix, ncells, &local);
   const int nrows = bc.g.n[1] * bc.g.n[2];
   const int nbx = (nrows / 2 + L / NCG - 1) / (L / NCG);
   const FftPlan plan = bc.fft[0];
-  fft_x_c2r_body<R, L, NCG, DynShape>(local % nbx, local / nbx, static_cast<const cx<R>*>(bc.B1),
+  fft_x_c2r_body<R, L, NCG, SH>(local % nbx, local / nbx, static_cast<const cx<R>*>(bc.B1),
                             static_cast<R*>(bc.out), bc.g.n[0], nrows, bc.g.K1, nc, plan);
 }
 
@@ -717,6 +717,8 @@ void allow_shape() {
   allow_smem(k_fft_x_r2c<R, L, SH>, k_fft_y_fwd<R, L, SH>, k_fft_z_influence<R, L, false, SH>,
              k_fft_z_influence<R, L, true, SH>, k_fft_y_inv<R, L, SH>, k_fft_x_c2r<R, L, 1, SH>,
              k_fft_x_c2r<R, L, 4, SH>);
+  allow_smem(k_fft_x_r2c_seg<R, L, SH>, k_fft_y_fwd_seg<R, L, SH>, k_fft_z_influence_seg<R, L, SH>,
+             k_fft_y_inv_seg<R, L, SH>, k_fft_x_c2r_seg<R, L, 1, SH>, k_fft_x_c2r_seg<R, L, 4, SH>);
 }
 
 template <typename R>
@@ -740,20 +742,39 @@ void allow_all() {
 
 // Segmented passes of a batch: lines per CTA b.L for every cell, shared
 // memory for the batch's largest length per axis.
+// The shape of axis d for a segmented launch: the compile-time one when every
+// cell has the same length along d (and it is specialised), else generic.
+template <typename R, int L, typename F>
+void with_seg_shape(const BatchLaunch& b, int d, F&& f) {
+  if (b.uniform[d])
+    with_shape<R, L>(b.plan[d], f);
+  else
+    f(DynShape{});
+}
+
 template <typename R>
 void forward_seg_impl(const BatchLaunch& b, cudaStream_t st) {
   const int nz = b.nc == 4 ? 2 : 1;
   with_lines(b.L, [&](auto lc) {
     constexpr int LL = decltype(lc)::value;
     if (b.n_r2c)
-      launch_chained(k_fft_x_r2c_seg<R, LL>, b.n_r2c, pass_threads(LL), b.smem[0], st, b.cells,
-                     b.p_r2c, b.ncells);
+      with_seg_shape<R, LL>(b, 0, [&](auto sh) {
+        using SH = decltype(sh);
+        launch_chained(k_fft_x_r2c_seg<R, LL, SH>, b.n_r2c, SH::template threads<LL>(), b.smem[0],
+                       st, b.cells, b.p_r2c, b.ncells);
+      });
     if (b.n_yfwd)
-      launch_chained(k_fft_y_fwd_seg<R, LL>, b.n_yfwd, pass_threads(LL), b.smem[1], st, b.cells,
-                     b.p_yfwd, b.ncells);
+      with_seg_shape<R, LL>(b, 1, [&](auto sh) {
+        using SH = decltype(sh);
+        launch_chained(k_fft_y_fwd_seg<R, LL, SH>, b.n_yfwd, SH::template threads<LL>(), b.smem[1],
+                       st, b.cells, b.p_yfwd, b.ncells);
+      });
     if (b.n_z)
-      launch_chained(k_fft_z_influence_seg<R, LL>, b.n_z, pass_threads(LL), b.smem_z, st, b.cells,
-                     b.p_z, b.ncells, nz);
+      with_seg_shape<R, LL>(b, 2, [&](auto sh) {
+        using SH = decltype(sh);
+        launch_chained(k_fft_z_influence_seg<R, LL, SH>, b.n_z, SH::template threads<LL>(),
+                       b.smem_z, st, b.cells, b.p_z, b.ncells, nz);
+      });
   });
   g_launches += 3;
 }
@@ -763,19 +784,24 @@ void inverse_seg_impl(const BatchLaunch& b, cudaStream_t st) {
   with_lines(b.L, [&](auto lc) {
     constexpr int LL = decltype(lc)::value;
     if (b.n_yinv)
-      launch_chained(k_fft_y_inv_seg<R, LL>, b.n_yinv, pass_threads(LL), b.smem[1], st, b.cells,
-                     b.p_yinv, b.ncells);
-    if (b.n_c2r) {
-      if constexpr (LL >= 4) {
-        if (b.nc == 4) {
-          launch_chained(k_fft_x_c2r_seg<R, LL, 4>, b.n_c2r, pass_threads(LL), b.smem[0], st,
-                         b.cells, b.p_c2r, b.ncells, b.nc);
-          return;
+      with_seg_shape<R, LL>(b, 1, [&](auto sh) {
+        using SH = decltype(sh);
+        launch_chained(k_fft_y_inv_seg<R, LL, SH>, b.n_yinv, SH::template threads<LL>(), b.smem[1],
+                       st, b.cells, b.p_yinv, b.ncells);
+      });
+    if (b.n_c2r)
+      with_seg_shape<R, LL>(b, 0, [&](auto sh) {
+        using SH = decltype(sh);
+        if constexpr (LL >= 4) {
+          if (b.nc == 4) {
+            launch_chained(k_fft_x_c2r_seg<R, LL, 4, SH>, b.n_c2r, SH::template threads<LL>(),
+                           b.smem[0], st, b.cells, b.p_c2r, b.ncells, b.nc);
+            return;
+          }
         }
-      }
-      launch_chained(k_fft_x_c2r_seg<R, LL, 1>, b.n_c2r, pass_threads(LL), b.smem[0], st, b.cells,
-                     b.p_c2r, b.ncells, b.nc);
-    }
+        launch_chained(k_fft_x_c2r_seg<R, LL, 1, SH>, b.n_c2r, SH::template threads<LL>(),
+                       b.smem[0], st, b.cells, b.p_c2r, b.ncells, b.nc);
+      });
   });
   g_launches += 2;
 }

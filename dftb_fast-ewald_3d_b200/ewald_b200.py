@@ -492,6 +492,48 @@ class Context:
         return {"alpha": a.value, "max_r": r.value, "max_g": g.value, "n_g": n.value}
 
 
+class PackedCells:
+    """A batch of cells packed once in the C ABI's host layout (CSR offsets,
+    coords (3, total) atom-major, charges, 9 lattice values per cell, outputs),
+    for repeated batched calls on the same cells (an MD or SCC loop over a set
+    of structures): each call then passes these arrays straight to
+    ewg_batch_potential_force_ov.  alloc(shape) makes the host arrays
+    (np.empty by default; page-locked arrays make the call's copies faster)."""
+
+    def __init__(self, cells, want_force=True, alloc=None):
+        alloc = alloc or (lambda shape: np.empty(shape, dtype=np.float64))
+        n = len(cells)
+        self.offsets = np.zeros(n + 1, dtype=np.int32)
+        for i, (_, q, _) in enumerate(cells):
+            self.offsets[i + 1] = self.offsets[i] + len(q)
+        total = int(self.offsets[-1])
+        self.coords = alloc((total, 3))
+        self.charges = alloc((total,))
+        self.lat = alloc((n, 9))
+        for i, (p, q, lat) in enumerate(cells):
+            a, b = self.offsets[i], self.offsets[i + 1]
+            self.coords[a:b] = np.asarray(p)
+            self.charges[a:b] = np.asarray(q)
+            self.lat[i] = np.asarray(lat, dtype=np.float64).ravel(order="F")
+        self.pot = alloc((total,))
+        self.force = alloc((total, 3)) if want_force else None
+        self.status = np.zeros(n, dtype=np.int32)
+
+    def set_charges(self, i, q):
+        """New charges for cell i (same atom count)."""
+        self.charges[self.offsets[i]:self.offsets[i + 1]] = q
+
+    def evaluate(self, ctx, tol=1e-10, **ov):
+        """One batched call on ctx; results in self.pot and self.force."""
+        o = _overrides(**ov)
+        _check(lib().ewg_batch_potential_force_ov(
+            ctx.handle, len(self.status), self.offsets.ctypes.data_as(C.POINTER(C.c_int)),
+            _dp(self.coords), _dp(self.charges), _dp(self.lat), float(tol), _dp(self.pot),
+            _dp(self.force) if self.force is not None else None,
+            self.status.ctypes.data_as(C.POINTER(C.c_int)), C.byref(o)))
+        return self
+
+
 _default = {}
 
 
