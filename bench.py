@@ -200,6 +200,7 @@ def cpu_evals(pos, q, lat, tol, steps, warmup, threads):
         t0 = time.perf_counter()
         oracle.fft_potential_force(pos, q, lat, tol)
         times.append(time.perf_counter() - t0)
+    cpu_evals.split = oracle.last_stage_seconds()  # of the last evaluation
     return times
 
 
@@ -226,7 +227,8 @@ def run_reference(args):
         "config": {"workload": label, "natoms": len(q), "tol": TOL_FP64},
         "cpu_baseline": {"value": value, "unit": "evals/s", "cores": threads, "kind": "port",
                          "sample": f"{args.steps} full {args.workload} shift+force evaluations (oracle/ C++ "
-                                   f"restatement, OpenMP, project FFT in place of FFTW)"},
+                                   f"restatement, OpenMP, project FFT in place of FFTW)",
+                         "split_s": cpu_evals.split},
         "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -637,7 +639,8 @@ def run_ours(args):
         times = cpu_evals(pos, q, lat, TOL_FP64, 1, 0, threads)
         cpu = {"value": 1.0 / times[0], "unit": "evals/s", "cores": threads, "kind": "port",
                "sample": f"1 full {len(q)}-atom shift+force evaluation at tol 1e-10 (oracle/ C++ "
-                         "restatement of the reference, OpenMP, project FFT in place of FFTW)"}
+                         "restatement of the reference, OpenMP, project FFT in place of FFTW)",
+               "split_s": cpu_evals.split}
 
     if dist:
         dist.barrier()

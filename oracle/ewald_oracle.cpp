@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <complex>
 #include <cstdint>
@@ -360,6 +361,21 @@ void deconvolution_table(int M, int n, double b, std::vector<int>& idx, std::vec
   }
 }
 
+// Wall-clock split of the last ewo_fft_potential_force call (seconds): real
+// space, spread, FFTs, gathers, everything else (deconvolution, embedding,
+// influence weights).  Reported beside the CPU baseline so that a reader can
+// bound how much of the timing depends on the FFT used in place of FFTW.
+enum { ST_REAL, ST_SPREAD, ST_FFT, ST_GATHER, ST_OTHER, ST_N };
+double g_stage_s[ST_N] = {0, 0, 0, 0, 0};
+struct StageTimer {
+  int st;
+  std::chrono::steady_clock::time_point t0;
+  explicit StageTimer(int s) : st(s), t0(std::chrono::steady_clock::now()) {}
+  ~StageTimer() {
+    g_stage_s[st] += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  }
+};
+
 // adjoint_nfft_3d, nfft/nfft.f90:196-305
 void adjoint_nfft(int N, const double* t1, const double* t2, const double* t3, const double* q,
                   int M1, int M2, int M3, int m, cplx* Shat) {
@@ -369,6 +385,7 @@ void adjoint_nfft(int N, const double* t1, const double* t2, const double* t3, c
   double* g = reinterpret_cast<double*>(grid.data());
   const int W = 2 * m + 1;
   // Step 1: spread, atomic updates on the real part (:256-278).
+  StageTimer* spread_timer = new StageTimer(ST_SPREAD);
 #pragma omp parallel
   {
     std::vector<double> w1(W), w2(W), w3(W);
@@ -394,9 +411,14 @@ void adjoint_nfft(int N, const double* t1, const double* t2, const double* t3, c
       }
     }
   }
+  delete spread_timer;
   // Step 2: one transform with sign +1 (:282).
-  fft3d(grid.data(), n1, n2, n3, 1);
+  {
+    StageTimer t(ST_FFT);
+    fft3d(grid.data(), n1, n2, n3, 1);
+  }
   // Step 3: keep the low modes and divide out the window (:286-298).
+  StageTimer other(ST_OTHER);
   std::vector<int> i1v, i2v, i3v;
   std::vector<double> f1, f2, f3;
   deconvolution_table(M1, n1, b, i1v, f1);
@@ -415,6 +437,7 @@ void forward_nfft(int N, const double* t1, const double* t2, const double* t3, i
                   int m, const cplx* fhat, cplx* f) {
   const int n1 = kOversampling * M1, n2 = kOversampling * M2, n3 = kOversampling * M3;
   const double b = window_shape(m);
+  StageTimer* embed_timer = new StageTimer(ST_OTHER);
   std::vector<cplx> grid(static_cast<size_t>(n1) * n2 * n3, cplx(0.0, 0.0));
   std::vector<int> i1v, i2v, i3v;
   std::vector<double> f1, f2, f3;
@@ -427,8 +450,13 @@ void forward_nfft(int N, const double* t1, const double* t2, const double* t3, i
         size_t dst = (static_cast<size_t>(i3v[a3]) * n2 + i2v[a2]) * n1 + i1v[a1];
         grid[dst] = fhat[(static_cast<size_t>(a3) * M2 + a2) * M1 + a1] * f1[a1] * f2[a2] * f3[a3];
       }
-  fft3d(grid.data(), n1, n2, n3, -1);
+  delete embed_timer;
+  {
+    StageTimer t(ST_FFT);
+    fft3d(grid.data(), n1, n2, n3, -1);
+  }
   const int W = 2 * m + 1;
+  StageTimer gather_timer(ST_GATHER);
 #pragma omp parallel
   {
     std::vector<double> w1(W), w2(W), w3(W);
@@ -897,13 +925,23 @@ int ewo_fft_potential_force(int n, const double* positions, const double* charge
   rc = choose_parameters(cell, q2, n, tol, ov, p);
   if (rc) return rc;
   std::vector<double> sp(n), lp(n), sf(3 * static_cast<size_t>(n)), lf(3 * static_cast<size_t>(n));
-  rc = short_range(n, positions, charges, cell, p.alpha, p.r_cut, sp.data(), sf.data(), nullptr);
+  for (double& t : g_stage_s) t = 0.0;
+  {
+    StageTimer t(ST_REAL);
+    rc = short_range(n, positions, charges, cell, p.alpha, p.r_cut, sp.data(), sf.data(), nullptr);
+  }
   if (rc) return rc;
   long_range(n, positions, charges, cell, p.alpha, p.n_modes, p.window_cutoff, lp.data(),
              force ? lf.data() : nullptr);
   for (int i = 0; i < n; ++i) pot[i] = sp[i] + lp[i] + (-2.0 * p.alpha / kSqrtPi * charges[i]);
   if (force)
     for (size_t k = 0; k < 3 * static_cast<size_t>(n); ++k) force[k] = sf[k] + lf[k];
+  return EWO_OK;
+}
+
+int ewo_stage_seconds(double* out) {
+  if (!out) return EWO_ERR_ARG;
+  for (int i = 0; i < ST_N; ++i) out[i] = g_stage_s[i];
   return EWO_OK;
 }
 

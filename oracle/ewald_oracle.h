@@ -71,6 +71,9 @@ int ewo_direct_potential_force(int n, const double* positions, const double* cha
                                const double* lat, double tol, double* pot, double* force,
                                const double* alpha_in, const double* r_cut_in,
                                const double* k_cut_in);
+/* Wall-clock seconds of the last ewo_fft_potential_force: real space, spread,
+ * FFTs, gathers, other (out: 5 doubles). */
+int ewo_stage_seconds(double* out);
 int ewo_real_space(int n, const double* positions, const double* charges, const double* lat,
                    double alpha, double r_cut, double* pot, double* force, int* used_cell_list);
 

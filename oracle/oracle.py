@@ -209,6 +209,14 @@ def direct_potential_force(positions, charges, lat_rows, tol=1e-12, want_force=T
     return (pot, force) if want_force else pot
 
 
+def last_stage_seconds():
+    """Wall-clock split of the last fft_potential_force: real space, spread,
+    FFTs, gathers, other (deconvolution, embedding, influence weights)."""
+    out = np.zeros(5)
+    lib().ewo_stage_seconds(_p(out))
+    return dict(zip(("real_space", "spread", "fft", "gather", "other"), map(float, out)))
+
+
 def real_space(positions, charges, lat_rows, alpha, r_cut):
     pos = _fortran_positions(positions)
     q = np.ascontiguousarray(charges, dtype=np.float64)
