@@ -20,12 +20,17 @@ module ewald_b200
   public :: ewaldGpuPotentialForce, ewaldGpuPotentialAt, ewaldGpuPotentialGradientAt
   public :: ewaldGpuSetForceScheme, ewaldGpuSetBackground, ewaldGpuXlbomdGradients
   public :: ewaldGpuExternalPotGrad, ewaldGpuPotentialForceStress, ewaldGpuBatchPotentialForce
+  public :: ewaldGpuSetPointEngine
   public :: EWG_PRECISION_FP64, EWG_PRECISION_MIXED, EWG_FORCE_IK, EWG_FORCE_AD
+  public :: EWG_POINTS_AUTO, EWG_POINTS_STOCK, EWG_POINTS_MESH
 
   integer(c_int), parameter :: EWG_PRECISION_FP64 = 0
   integer(c_int), parameter :: EWG_PRECISION_MIXED = 1
   integer(c_int), parameter :: EWG_FORCE_IK = 0
   integer(c_int), parameter :: EWG_FORCE_AD = 1
+  integer(c_int), parameter :: EWG_POINTS_AUTO = 0
+  integer(c_int), parameter :: EWG_POINTS_STOCK = 1
+  integer(c_int), parameter :: EWG_POINTS_MESH = 2
 
   !> Handle of one device context.
   type :: TEwaldGpu
@@ -113,6 +118,13 @@ module ewald_b200
       integer(c_int), value :: scheme
       integer(c_int) :: rc
     end function ewg_set_force_scheme
+
+    function ewg_set_point_engine(ctx, engine) bind(C, name="ewg_set_point_engine") result(rc)
+      import :: c_ptr, c_int
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: engine
+      integer(c_int) :: rc
+    end function ewg_set_point_engine
 
     function ewg_stress_fast(ctx, tol, sigma) bind(C, name="ewg_stress_fast") result(rc)
       import :: c_ptr, c_int, c_double
@@ -305,6 +317,17 @@ contains
     integer(c_int), intent(in) :: scheme
     call check(ewg_set_force_scheme(this%ctx, scheme))
   end subroutine ewaldGpuSetForceScheme
+
+  !> Engine of ewaldGpuPotentialAt, ewaldGpuPotentialGradientAt and
+  !> ewaldGpuExternalPotGrad: EWG_POINTS_STOCK (the stock pair sum of
+  !> coulomb.F90:2311-2343), EWG_POINTS_MESH (NFFT plus a cell-list real-space
+  !> sum, linear in the number of points) or EWG_POINTS_AUTO (mesh from 2**20
+  !> target-source pairs on). Softened calls always take the stock sum.
+  subroutine ewaldGpuSetPointEngine(this, engine)
+    type(TEwaldGpu), intent(inout) :: this
+    integer(c_int), intent(in) :: engine
+    call check(ewg_set_point_engine(this%ctx, engine))
+  end subroutine ewaldGpuSetPointEngine
 
   !> NFFT-based stress of the fast engine on the resident state; same convention as
   !> ewaldGpuStress (the caller does stress = stress - 0.5 * sigma).
