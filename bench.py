@@ -168,10 +168,11 @@ def stage_flops(params, natoms, nc=4):
 
 
 # DRAM bytes (read + write) per launch from one ncu capture of the 32,769-atom
-# workload (profiles/c3_water_32k_fp64_top_kernels.md), keyed by (real bytes, grids
-# through the inverse passes and the gather, stage).
+# workload (profiles/c3_water_32k_fp64_top_kernels.md), keyed by (workload, real
+# bytes, grids through the inverse passes and the gather, stage); other
+# workloads report null.
 DRAM_TRAFFIC = {
-    (8, 4, "gather"): 746.37e6 + 62.96e6,
+    ("c3", 8, 4, "gather"): 746.37e6 + 62.96e6,
 }
 
 
@@ -675,7 +676,7 @@ def run_ours(args):
                 entry["bytes"] = sb[name]
             per[name] = entry
         top = max((k for k in per if k in sb or k in fl), key=lambda k: per[k]["ms"])
-        traffic = DRAM_TRAFFIC.get((real_bytes, nc, top))
+        traffic = DRAM_TRAFFIC.get((args.workload, real_bytes, nc, top))
         if top in fl:
             ach = per[top]["tflops"]
             roof = {"bound": "tensor", "kernel": top, "achieved": ach, "peak": tensor_peak,

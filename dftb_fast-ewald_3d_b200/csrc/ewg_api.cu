@@ -2227,6 +2227,10 @@ int ewg_batch_potential_force(ewg_context* c, int n_cells, const int* offsets, c
                                       force, cell_status, nullptr);
 }
 
+// Mean real-grid bytes per cell above which a batch runs cell by cell (about
+// half the B200's 126 MB L2).
+constexpr double kSegGridBytes = 64.0 * 1024 * 1024;
+
 int ewg_batch_potential_force_ov(ewg_context* c, int n_cells, const int* offsets,
                                  const double* coords, const double* charges,
                                  const double* lat_rows, double tol, double* pot, double* force,
@@ -2265,8 +2269,17 @@ int ewg_batch_potential_force_ov(ewg_context* c, int n_cells, const int* offsets
     all_ok = all_ok && st == EWG_OK;
   }
   // Segmented launches (one per stage over every cell) unless lanes were asked
-  // for, stage timing is on, or a cell failed its checks.
-  const bool segmented = c->batch_lanes == 0 && all_ok;
+  // for, a cell failed its checks, or the cells are large: when the cells' real
+  // grids average more than kSegGridBytes, one cell alone fills the GPU and its
+  // middle FFT passes run from L2, which interleaving the cells would give up;
+  // such a batch runs cell by cell on the context's stream.
+  double grid_bytes = 0.0;
+  for (int cidx = 0; cidx < n_cells && all_ok; ++cidx)
+    grid_bytes += 8.0 * params[cidx].n_modes[0] * params[cidx].n_modes[1] *
+                  params[cidx].n_modes[2] *
+                  (c->precision == EWG_PRECISION_MIXED ? sizeof(float) : sizeof(double));
+  const bool large = all_ok && grid_bytes > kSegGridBytes * n_cells;
+  const bool segmented = c->batch_lanes == 0 && all_ok && !large;
   SegPlan sp;
   SegBufs sb{};
   if (segmented) {

@@ -370,8 +370,10 @@ int ewg_last_stress_setup(const ewg_context* ctx, double* alpha, double* max_r, 
  * is the first non-zero cell status.  By default every stage of every cell
  * runs in one segmented launch (the cells' parameters, FFT plans and buffers
  * in a device table), and a repeated batch is recorded as one CUDA graph and
- * replayed; with ewg_set_batch_lanes(ctx, 1..16) the cells run instead on that
- * many concurrent lanes.  Results are bitwise the same either way. */
+ * replayed; cells whose real FFT grids average more than 64 MiB run one after
+ * another instead (one such cell fills the GPU on its own).  With
+ * ewg_set_batch_lanes(ctx, 1..16) the cells run on that many concurrent lanes.
+ * Results are bitwise the same either way. */
 int ewg_batch_potential_force(ewg_context* ctx, int n_cells, const int* offsets,
                               const double* coords, const double* charges, const double* lat_rows,
                               double tol, double* pot, double* force, int* cell_status);
@@ -386,7 +388,8 @@ int ewg_batch_potential_force_ov(ewg_context* ctx, int n_cells, const int* offse
 
 /* Batch lanes (0..16, default 0).  0: segmented launches, one per stage for
  * all cells of a batched call (cells that fail their checks send the whole
- * call to the lane path).  1..16: independent cells run concurrently on this
+ * call to the lane path, and cells whose real grids average more than 64 MiB
+ * run one after another on the context).  1..16: independent cells run concurrently on this
  * many lanes, each a sub-context of the same device, form and settings with
  * its own device buffers and streams (so each lane holds the buffers of the
  * largest cell it has run); one lane runs the cells back to back on the
