@@ -242,9 +242,11 @@ def run_reference(args):
 class Arm:
     """One precision form on one device: device-resident and end-to-end timing."""
 
-    def __init__(self, eb, torch, device, precision, tol, pos, q, lat, scheme=None, ov=None):
+    def __init__(self, eb, torch, device, precision, tol, pos, q, lat, scheme=None, ov=None,
+                 want_force=True):
         self.eb, self.torch = eb, torch
         self.tol = tol
+        self.want_force = want_force  # False: SCC-style shift (potential) only
         self.ov = dict(ov or {})
         self.ctx = eb.Context(device, precision)
         if scheme is not None:
@@ -273,8 +275,8 @@ class Arm:
         torch.cuda.synchronize()
 
     def step_device(self):
-        self.ctx.potential_force_device(self.x, self.q, self.lat, self.tol, self.pot, self.force,
-                                        **self.ov)
+        self.ctx.potential_force_device(self.x, self.q, self.lat, self.tol, self.pot,
+                                        self.force if self.want_force else None, **self.ov)
 
     def step_e2e(self):
         L = self.eb.lib()
@@ -283,7 +285,8 @@ class Arm:
         rc = L.ewg_potential_force(self.ctx.handle, self.n, self.h_pos.ctypes.data_as(dp),
                                    self.h_q.ctypes.data_as(dp), self.lat.ctypes.data_as(dp),
                                    float(self.tol), self.h_pot.ctypes.data_as(dp),
-                                   self.h_force.ctypes.data_as(dp), C.byref(ov))
+                                   self.h_force.ctypes.data_as(dp) if self.want_force else None,
+                                   C.byref(ov))
         if rc:
             raise self.eb.EwaldError(rc, self.eb.status_string(rc))
 
@@ -564,6 +567,11 @@ def run_ours(args):
     tuner.close()
     mixed = Arm(eb, torch, device, eb.MIXED, TOL_MIXED, pos, q, lat, scheme=tuned_scheme,
                 ov=tuned_ov)
+    # SCC-style shift evaluations (potential only: one spread, one inverse
+    # transform, one gather), reported beside the force evaluations.
+    shift64 = Arm(eb, torch, device, eb.FP64, TOL_FP64, pos, q, lat, want_force=False)
+    shift32 = Arm(eb, torch, device, eb.MIXED, TOL_MIXED, pos, q, lat, ov=tuned_ov,
+                  want_force=False)
     scheme_name = {eb.FORCE_IK: "ik", eb.FORCE_AD: "window differentiation"}
 
     # accuracy of the other arms against the plain form (same inputs)
@@ -604,6 +612,10 @@ def run_ours(args):
     msad, launchesad, _ = fp64_ad.time_device(args.steps, args.warmup)
     barrier()
     ms32, launches32, _ = mixed.time_device(args.steps, args.warmup)
+    barrier()
+    mss64, _, _ = shift64.time_device(args.steps, args.warmup)
+    barrier()
+    mss32, _, _ = shift32.time_device(args.steps, args.warmup)
     clocks = sampler.stop()
     barrier()
     # Per-stage device times come from a separate profiled pass: with stage
@@ -619,6 +631,10 @@ def run_ours(args):
     barrier()
     e2e32 = mixed.time_e2e(args.steps, args.warmup)
     barrier()
+    e2es64 = shift64.time_e2e(args.steps, args.warmup)
+    barrier()
+    e2es32 = shift32.time_e2e(args.steps, args.warmup)
+    barrier()
 
     def maxrank(x):
         if not dist:
@@ -633,6 +649,8 @@ def run_ours(args):
     te64 = maxrank(e2e64)
     tead = maxrank(e2ead)
     te32 = maxrank(e2e32)
+    ts64, ts32 = maxrank(sum(mss64) / 1e3), maxrank(sum(mss32) / 1e3)
+    tes64, tes32 = maxrank(e2es64), maxrank(e2es32)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -743,6 +761,16 @@ def run_ours(args):
             "rel_err_vs_fp64": err, "rel_err_vs_direct": err_direct, "roofline": roof32,
             "whole_eval_hbm": whole_eval(params32, 4, t32 / args.steps, nc=nc32), "stages_ms": per32,
             "gpu_launches": launches32,
+        },
+        "shift_only": {
+            "what": "SCC-style shift evaluations: potential only (one spread, one inverse "
+                    "transform, one gather) plus the real-space potential",
+            "fp64": {"value": ws * args.steps / ts64, "unit": "evals/s",
+                     "e2e": {"value": ws * args.steps / tes64, "unit": "evals/s",
+                             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": natoms * 8}},
+            "mixed": {"value": ws * args.steps / ts32, "unit": "evals/s",
+                      "e2e": {"value": ws * args.steps / tes32, "unit": "evals/s",
+                              "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": natoms * 8}},
         },
         "gpu_launches": launches64,
         "clocks": clocks,

@@ -121,7 +121,8 @@ __global__ void k_count(const int* __restrict__ key, int n, int* __restrict__ co
 
 // Exclusive scan of counts into starts[0..nkeys]; one CTA of 1024 threads.
 // Each round stages 8192 counts in shared memory with coalesced loads, scans 8
-// consecutive entries per thread and writes the starts back coalesced.
+// consecutive entries per thread and writes the starts back coalesced.  The
+// next round's counts are loaded into registers while this round is scanned.
 __global__ void __launch_bounds__(1024) k_scan(const int* __restrict__ counts, int nkeys,
                                                int* __restrict__ starts) {
   chain_enter();
@@ -131,11 +132,24 @@ __global__ void __launch_bounds__(1024) k_scan(const int* __restrict__ counts, i
   __shared__ int carry_s;
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   int carry = 0;
+  int next[kItems];
+#pragma unroll
+  for (int j = 0; j < kItems; ++j) {
+    const int e = j * 1024 + tid;
+    next[j] = e < nkeys ? counts[e] : 0;
+  }
   for (int base = 0; base < nkeys; base += kRound) {
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
       const int e = j * 1024 + tid;
-      buf[e + (e >> 5)] = base + e < nkeys ? counts[base + e] : 0;
+      buf[e + (e >> 5)] = next[j];
+    }
+    if (base + kRound < nkeys) {
+#pragma unroll
+      for (int j = 0; j < kItems; ++j) {
+        const int e = base + kRound + j * 1024 + tid;
+        next[j] = e < nkeys ? counts[e] : 0;
+      }
     }
     __syncthreads();
     int v[kItems];
