@@ -34,7 +34,9 @@ enum BufId {
   B_PT_BTMP, B_PT_KCNT, B_PT_KCUR, B_PT_PTMP, B_PT_QNEG, B_PT_PART, B_PT_POTSR, B_PT_GRADSR,
   B_PT_GRAD, B_PT_POTOUT,
   // segmented batches: cell table and launch prefixes
-  B_BT_CELLS, B_BT_PREFIX, B_COUNT
+  B_BT_CELLS, B_BT_PREFIX,
+  // batched SCC updates: charges and shifts of k updates
+  B_SCC_Q, B_SCC_POT, B_COUNT
 };
 
 struct DevBuf {
@@ -485,7 +487,8 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
       launch_weights(mp, mcv, fr, permbox, n, wtab, qk, slot, st);
       launch_pair_bins(mp, slot, n, counts, cursor, pairstart, pairtmp, pairs, npairs_max, st);
     } else {
-      // Geometry unchanged: refresh only the charges in the sorted layouts.
+      // Geometry unchanged: refresh only the charges in the sorted layouts; the
+      // window weights, slots and pair lists stay.
       launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, nullptr, s4, nullptr, nullptr, nullptr,
                        st);
       if (concurrent) {
@@ -493,9 +496,8 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
         cudaStreamWaitEvent(rs, c->fork, 0);
       }
       launch_permute_box(s4, permbox, n, cell.lat, s4s, x32s, rs);
-      launch_atom_prep(pos, sa, sd, q, n, cell, nullptr, mp.g.n, nullptr, nullptr, mcv, fr, st);
       prof_mark(mp.prof, st, ST_WEIGHTS);
-      launch_weights(mp, mcv, fr, permbox, n, wtab, qk, slot, st);
+      launch_sorted_charges(mp, q, permbox, n, qk, st);
     }
     prof_mark(mp.prof, st, ST_REAL);
     launch_real_space(s4s, x32s, permbox, boxstart, n, rg, p.alpha, p.r_cut, mixed, pot_sr, f_sr,
@@ -1731,6 +1733,63 @@ int ewg_xlbomd_gradients(ewg_context* c, double tol, const double* dq_out, doubl
 }
 
 int ewg_shift(ewg_context* c, double tol, double* shift) { return coulomb_eval(c, tol, shift, nullptr); }
+
+int ewg_shift_batch(ewg_context* c, double tol, int k, const double* charges, double* shifts) {
+  if (!c || k < 0 || (k > 0 && (!charges || !shifts))) return EWG_ERR_ARG;
+  LaunchScope scope(c);
+  if (!c->has_coords) return EWG_ERR_STATE;
+  if (k == 0) return EWG_OK;
+  if (!(tol > 0.0 && tol < 1.0)) tol = 1.0e-9;  // coulomb.F90:348-349
+  const int n = c->natoms;
+  const size_t kn = static_cast<size_t>(k) * n;
+  Cell cell;
+  int rc = cell_from_cols(c->lat_cols, cell);
+  if (rc) return rc;
+  // Host side first: every update's checks and its parameters (the reference
+  // chain depends on the charges through sum q^2).
+  std::vector<ewg_params> ps(k);
+  std::vector<double> bg(k);
+  for (int j = 0; j < k; ++j) {
+    double q2 = 0.0, qsum = 0.0;
+    const double* qj = charges + static_cast<size_t>(j) * n;
+    if ((rc = charge_check(c, n, qj, &q2, &qsum))) return rc;
+    if ((rc = choose_parameters(cell, q2, n, tol, nullptr, ps[j]))) return rc;
+    bg[j] = background_shift(c, qsum, cell, ps[j].alpha);
+  }
+  double* dcoords = dbuf<double>(c, B_COORDS, 3 * static_cast<size_t>(n), &rc);
+  double* dq = dbuf<double>(c, B_SCC_Q, kn, &rc);
+  double* dpot = dbuf<double>(c, B_SCC_POT, kn, &rc);
+  int* flags = dbuf<int>(c, B_CELLERR, k, &rc);
+  if (rc) return rc;
+  if (c->resident.coords_version != c->coords_version)
+    cudaMemcpyAsync(dcoords, c->coords.data(), sizeof(double) * 3 * n, cudaMemcpyHostToDevice,
+                    c->stream);
+  cudaMemcpyAsync(dq, charges, sizeof(double) * kn, cudaMemcpyHostToDevice, c->stream);
+  cudaMemsetAsync(flags, 0, sizeof(int) * k, c->stream);
+  for (int j = 0; j < k; ++j) {
+    rc = evaluate(c, n, dcoords, 3, 1, dq + static_cast<size_t>(j) * n, cell, ps[j], false,
+                  dpot + static_cast<size_t>(j) * n, nullptr, true, flags + j, nullptr, bg[j]);
+    if (rc) {
+      c->resident.coords_version = -1;
+      return rc;
+    }
+  }
+  std::vector<int> hflags(k);
+  cudaError_t e = cudaMemcpyAsync(shifts, dpot, sizeof(double) * kn, cudaMemcpyDeviceToHost,
+                                  c->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(hflags.data(), flags, sizeof(int) * k, cudaMemcpyDeviceToHost, c->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+  if (e != cudaSuccess) return cuda_status(e);
+  // As after k ewg_set_charges calls: the resident charges are the last update's.
+  const double* last = charges + static_cast<size_t>(k - 1) * n;
+  c->dq.assign(last, last + n);
+  c->has_charges = true;
+  ++c->charges_version;
+  for (int j = 0; j < k; ++j)
+    if (hflags[j]) return EWG_ERR_COINCIDENT;
+  return EWG_OK;
+}
 
 int ewg_stress_fast(ewg_context* c, double tol, double* sigma) {
   if (!sigma) return EWG_ERR_ARG;

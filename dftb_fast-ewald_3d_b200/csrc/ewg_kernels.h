@@ -259,6 +259,12 @@ size_t mesh_pass_smem(int n, int L, bool mixed, int extra);
 void launch_weights(const MeshPlan& mp, const int4* mesh_c, const double4* mesh_fr,
                     const int* perm, int n, void* wtab, void* qk, int4* slot, cudaStream_t st);
 
+// Only the charges in sorted order, qk[k] = q[perm[k]] (FP32 in the mixed form):
+// the resident path's refresh when the geometry and so the weights and the
+// pair lists are unchanged.
+void launch_sorted_charges(const MeshPlan& mp, const double* q, const int* perm, int n, void* qk,
+                           cudaStream_t st);
+
 // Bins every (atom, tile) pair by tile, buckets ordered by atom index:
 // pairs[tile_start[t] .. tile_start[t+1]) = (atom, packed slot).  Scratch:
 // counts/cursor (ntiles), tmp (npairs_max); npairs_max = n * S_x * S_y * S_z.

@@ -1351,6 +1351,13 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma_ad_seg(
                                    static_cast<const double*>(bc.out), part);
 }
 
+template <typename R>
+__global__ void k_sorted_charges(const double* __restrict__ q, const int* __restrict__ perm, int n,
+                                 R* __restrict__ qk) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) qk[k] = static_cast<R>(q[perm[k]]);
+}
+
 inline int blocks_for(long n, int threads) { return static_cast<int>((n + threads - 1) / threads); }
 
 }  // namespace
@@ -1365,6 +1372,16 @@ void launch_weights(const MeshPlan& mp, const int4* mc, const double4* fr, const
   else
     launch_chained(k_weights_tiled<double>, blocks_for(threads, 128), 128, 0, st,
         mc, fr, perm, n, mp.sd, static_cast<double*>(wtab), static_cast<double*>(qk), slot);
+  ++g_launches;
+}
+
+void launch_sorted_charges(const MeshPlan& mp, const double* q, const int* perm, int n, void* qk,
+                           cudaStream_t st) {
+  if (n == 0) return;
+  if (mp.mixed)
+    k_sorted_charges<float><<<blocks_for(n, 256), 256, 0, st>>>(q, perm, n, static_cast<float*>(qk));
+  else
+    k_sorted_charges<double><<<blocks_for(n, 256), 256, 0, st>>>(q, perm, n, static_cast<double*>(qk));
   ++g_launches;
 }
 

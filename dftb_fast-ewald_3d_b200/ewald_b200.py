@@ -51,7 +51,8 @@ EXPORTED = [
     "ewg_create", "ewg_destroy", "ewg_status_string", "ewg_kernel_launches", "ewg_last_params",
     "ewg_potential_force", "ewg_parameters", "ewg_grid_memory", "ewg_device_memory",
     "ewg_potential_force_device", "ewg_direct_potential_force", "ewg_set_lattice",
-    "ewg_set_coords", "ewg_set_charges", "ewg_shift", "ewg_shift_force", "ewg_stress",
+    "ewg_set_coords", "ewg_set_charges", "ewg_shift", "ewg_shift_force", "ewg_shift_batch",
+    "ewg_stress",
     "ewg_last_stress_setup", "ewg_batch_potential_force", "ewg_set_profiling", "ewg_stage_count",
     "ewg_stage_name", "ewg_stage_times", "ewg_reset_stage_times", "ewg_set_stream",
     "ewg_direct_potential_force_static", "ewg_fp64_mma_peak", "ewg_potential_force_stress",
@@ -137,6 +138,7 @@ def lib():
     L.ewg_set_charges.argtypes = [vp, dp]
     L.ewg_shift.argtypes = [vp, C.c_double, dp]
     L.ewg_shift_force.argtypes = [vp, C.c_double, dp, dp]
+    L.ewg_shift_batch.argtypes = [vp, C.c_double, C.c_int, dp, dp]
     L.ewg_stress.argtypes = [vp, C.c_double, C.c_double, dp]
     L.ewg_stress_fast.argtypes = [vp, C.c_double, dp]
     L.ewg_xlbomd_gradients.argtypes = [vp, C.c_double, dp, dp]
@@ -402,6 +404,18 @@ class Context:
         f = np.empty((n, 3))
         _check(lib().ewg_shift_force(self._h, float(tol), _dp(out), _dp(f)))
         return out, f
+
+    def shift_batch(self, tol, charges, out=None):
+        """k charge updates on the resident geometry in one submission
+        (ewg_shift_batch): charges (k, N) -> shifts (k, N), each row what
+        set_charges(row) then shift() would give."""
+        q = np.ascontiguousarray(charges, dtype=np.float64)
+        if q.ndim != 2:
+            raise EwaldError(2, "ewald_b200: charges must be (k, N)")
+        if out is None:
+            out = np.empty_like(q)
+        _check(lib().ewg_shift_batch(self._h, float(tol), q.shape[0], _dp(q), _dp(out)))
+        return out
 
     # -- potentials and gradients at arbitrary points (stock Ewald) -----------
     def potential_at(self, targets, sources, charges, lat_cols, tol_ewald=1e-9, alpha=0.0,

@@ -17,6 +17,7 @@ module ewald_b200
   public :: TEwaldGpu, ewaldGpuInit, ewaldGpuFinal
   public :: ewaldGpuSetLattice, ewaldGpuSetCoords, ewaldGpuSetCharges
   public :: ewaldGpuShift, ewaldGpuShiftForce, ewaldGpuStress, ewaldGpuStressFast
+  public :: ewaldGpuShiftBatch
   public :: ewaldGpuPotentialForce, ewaldGpuPotentialAt, ewaldGpuPotentialGradientAt
   public :: ewaldGpuSetForceScheme, ewaldGpuSetBackground, ewaldGpuXlbomdGradients
   public :: ewaldGpuExternalPotGrad, ewaldGpuPotentialForceStress, ewaldGpuBatchPotentialForce
@@ -103,6 +104,17 @@ module ewald_b200
       real(c_double), intent(out) :: force(3, *)
       integer(c_int) :: rc
     end function ewg_shift_force
+
+    function ewg_shift_batch(ctx, tol, k, charges, shifts) bind(C, name="ewg_shift_batch") &
+        & result(rc)
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), value :: tol
+      integer(c_int), value :: k
+      real(c_double), intent(in) :: charges(*)
+      real(c_double), intent(out) :: shifts(*)
+      integer(c_int) :: rc
+    end function ewg_shift_batch
 
     function ewg_stress(ctx, tolEwald, alpha, sigma) bind(C, name="ewg_stress") result(rc)
       import :: c_ptr, c_int, c_double
@@ -300,6 +312,16 @@ contains
     real(c_double), intent(out) :: shift(:), force(:, :)
     call check(ewg_shift_force(this%ctx, tol, shift, force))
   end subroutine ewaldGpuShiftForce
+
+  !> k charge updates on the resident geometry in one submission: column j of
+  !> shifts is what ewaldGpuSetCharges(charges(:, j)) and ewaldGpuShift would give.
+  subroutine ewaldGpuShiftBatch(this, tol, charges, shifts)
+    type(TEwaldGpu), intent(inout) :: this
+    real(c_double), intent(in) :: tol
+    real(c_double), intent(in) :: charges(:, :)
+    real(c_double), intent(out) :: shifts(:, :)
+    call check(ewg_shift_batch(this%ctx, tol, int(size(charges, 2), c_int), charges, shifts))
+  end subroutine ewaldGpuShiftBatch
 
   !> Replaces invRStress in TCoulomb%addStress (coulomb.F90:752); the caller
   !> keeps stress = stress - 0.5 * sigma.

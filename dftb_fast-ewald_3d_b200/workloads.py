@@ -158,6 +158,14 @@ def c5_charge_update(base_charges, k: int):
     return _neutral(0.8 * sign + rng.normal(0.0, 0.05, size=sign.shape))
 
 
+def charge_update(base_charges, k: int, seed: int, scale: float = 0.05):
+    """k-th SCC-style charge update of a workload (seed + k): each charge
+    moves by N(0, scale) relative to its own size, neutrality kept."""
+    rng = np.random.default_rng(seed + k)
+    q = np.asarray(base_charges, dtype=np.float64)
+    return _neutral(q * (1.0 + rng.normal(0.0, scale, size=q.shape)))
+
+
 def reference_pair_fixture():
     """The 2-atom periodic fixture of the reference's unit test
     (test/src/dftbp/unit/dftb/coulomb.F90:104-195): lattice diag(2,1,1) Bohr,

@@ -304,6 +304,17 @@ int ewg_shift(ewg_context* ctx, double tol, double* shift);
 /* fftEwaldAddGradients (coulomb.F90:361-385): shift(N) and the physical force
  * F(3,N); the adapter subtracts F from DFTB+'s gradient array. */
 int ewg_shift_force(ewg_context* ctx, double tol, double* shift, double* force);
+/* k charge updates on the resident geometry in one submission: for each j,
+ * the result of ewg_set_charges(charges + j N) then ewg_shift(tol, shifts + j N)
+ * (updateCharges, coulomb.F90:760-781, then fftEwaldShift, :336-357), bitwise,
+ * each update with its own parameters from its own charges.  charges and
+ * shifts are (N, k) column-major (update-major); one upload, one download and
+ * no host wait between the updates.  Afterwards the context's charges are the
+ * last update's.  Returns the first failing check (every update is checked
+ * before any work is queued; nothing is written then) or EWG_ERR_COINCIDENT
+ * (shifts written all the same).  No counterpart in the reference, whose SCC
+ * loop calls the shift once per iteration. */
+int ewg_shift_batch(ewg_context* ctx, double tol, int k, const double* charges, double* shifts);
 /* ---- potentials and gradients at arbitrary points ---------------------- */
 /* TCoulomb%getPotential / getPotentialGradient / addExternalPotGrad
  * (dftb/coulomb.F90:3122-3248), periodic branch: the stock Ewald sum of
