@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -55,7 +56,9 @@ struct CorrEntry {
   double* dev = nullptr;
 };
 
-bool factor_length(int n, FftPlan& plan) {
+// Radix schedule of length n: odd radices first, then radix 8 (or, with
+// radix4, radix 4 in its place), 4 and 2.
+bool factor_length(int n, FftPlan& plan, bool radix4 = false) {
   plan.n = n;
   plan.nstages = 0;
   int rem = n;
@@ -73,7 +76,7 @@ bool factor_length(int n, FftPlan& plan) {
   for (int r = 11; r <= 31 && rem > 1; r += 2)
     while (rem % r == 0)
       if (!push(r)) return false;
-  while (rem % 8 == 0)
+  while (!radix4 && rem % 8 == 0)
     if (!push(8)) return false;
   while (rem % 4 == 0)
     if (!push(4)) return false;
@@ -165,6 +168,10 @@ struct ewg_context {
     double report[4];
   };
   std::map<std::vector<double>, TuneEntry> tuned;
+  // Kernel shapes: tuned per bucket (ewg_tune_kernels), or pinned by the caller.
+  std::map<std::array<int, 7>, ewg_kernel_shape> shapes;
+  bool shape_pinned = false;
+  ewg_kernel_shape pinned{};
   int last_ng = 0;
   Profiler prof;
 
@@ -227,12 +234,14 @@ T* dbuf(ewg_context* c, BufId id, size_t count, int* rc) {
   return static_cast<T*>(b.p);
 }
 
-int get_fft(ewg_context* c, int n, FftPlan& out) {
-  auto it = c->ffts.find(n);
+// The plan of length n with radix schedule sched (ewg_kernel_shape.fft_sched).
+int get_fft(ewg_context* c, int n, FftPlan& out, int sched = 1) {
+  const int key = 4 * n + sched;
+  auto it = c->ffts.find(key);
   if (it == c->ffts.end()) {
     FftEntry e;
-    if (n > kMaxFftLength || !factor_length(n, e.plan)) {
-      c->ffts[n] = e;
+    if (n > kMaxFftLength || !factor_length(n, e.plan, sched == 2)) {
+      c->ffts[key] = e;
       return EWG_ERR_GRID_TOO_LARGE;
     }
     std::vector<double> t64(2 * n);
@@ -256,7 +265,7 @@ int get_fft(ewg_context* c, int n, FftPlan& out) {
     e.plan.tw64 = static_cast<const double*>(e.tw64);
     e.plan.tw32 = static_cast<const float*>(e.tw32);
     e.ok = true;
-    it = c->ffts.emplace(n, e).first;
+    it = c->ffts.emplace(key, e).first;
   }
   if (!it->second.ok) return EWG_ERR_GRID_TOO_LARGE;
   out = it->second.plan;
@@ -288,12 +297,13 @@ int get_corr(ewg_context* c, int n, int H, int m, const double** out) {
   return EWG_OK;
 }
 
-// Boxes half as wide as the reference's (box_count gives boxes at least r_cut
-// wide): the 5 x 5 x 5 neighbourhood of half-width boxes holds about 40% fewer
-// candidates than 3 x 3 x 3 full-width ones.  The pairs found are the same.
-void real_geometry(const Cell& cell, double r_cut, int natoms, RealGeom& g) {
+// div boxes per reference box width along each axis (box_count gives boxes at
+// least r_cut wide).  By default half-width boxes: their 5 x 5 x 5
+// neighbourhood holds about 40% fewer candidates than 3 x 3 x 3 full-width
+// ones.  The pairs found are the same for every div.
+void real_geometry(const Cell& cell, double r_cut, int natoms, RealGeom& g, int div = 2) {
   for (int d = 0; d < 3; ++d) {
-    int nb = 2 * box_count(r_cut, cell.recLen[d]);
+    int nb = div * box_count(r_cut, cell.recLen[d]);
     g.nb[d] = std::max(1, std::min(nb, 1 << 10));
   }
   const long cap = std::max<long>(64, 4L * natoms);
@@ -311,6 +321,31 @@ void real_geometry(const Cell& cell, double r_cut, int natoms, RealGeom& g) {
     }
   }
   set_scan_mode(g);
+}
+
+// Kernel shapes: the zero (or out-of-range) fields of s take the defaults.
+ewg_kernel_shape resolve_shape(ewg_kernel_shape s) {
+  if (s.box_div < 1 || s.box_div > 3) s.box_div = 2;
+  if (s.fft_lines != 1 && s.fft_lines != 2 && s.fft_lines != 4 && s.fft_lines != 8)
+    s.fft_lines = 0;  // the most that fit
+  if (s.fft_sched != 2) s.fft_sched = 1;
+  if (s.gather_warps != 2 && s.gather_warps != 8) s.gather_warps = 4;
+  return s;
+}
+
+// Bucket of an evaluation for the kernel-shape cache: precision form, force
+// grids (0 potential only, 1 i k, 2 window derivatives), atom octave
+// (2^k <= n < 2^(k+1)), fine grid and window half-width.
+std::array<int, 7> shape_bucket(int precision, int grids, int n, const MeshGeom& g) {
+  int oct = 0;
+  while (oct < 30 && (2L << oct) <= n) ++oct;
+  return {precision, grids, oct, g.n[0], g.n[1], g.n[2], g.m};
+}
+
+ewg_kernel_shape shape_for(const ewg_context* c, const std::array<int, 7>& bucket) {
+  if (c->shape_pinned) return resolve_shape(c->pinned);
+  auto it = c->shapes.find(bucket);
+  return resolve_shape(it == c->shapes.end() ? ewg_kernel_shape{} : it->second);
 }
 
 int mesh_geometry(const Cell& cell, const ewg_params& p, MeshGeom& g) {
@@ -393,15 +428,19 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
   const bool ad = want_force && c->force_scheme == EWG_FORCE_AD;
   const int nc = want_force && !ad ? 4 : 1;
   const int nparts = want_force ? 4 : 1;
-  RealGeom rg;
-  real_geometry(cell, p.r_cut, n, rg);
   MeshPlan mp;
   rc = mesh_geometry(cell, p, mp.g);
   if (rc) return rc;
+  const ewg_kernel_shape ks =
+      shape_for(c, shape_bucket(c->precision, want_force ? (ad ? 2 : 1) : 0, n, mp.g));
+  RealGeom rg;
+  real_geometry(cell, p.r_cut, n, rg, ks.box_div);
   mp.mixed = mixed;
   mp.prof = &c->prof;
+  mp.lines_cap = ks.fft_lines;
+  mp.gather_warps = ks.gather_warps;
   for (int d = 0; d < 3; ++d) {
-    if ((rc = get_fft(c, mp.g.n[d], mp.fft[d]))) return rc;
+    if ((rc = get_fft(c, mp.g.n[d], mp.fft[d], ks.fft_sched))) return rc;
     const int H = mp.g.M[d] - mp.g.M[d] / 2;
     if ((rc = get_corr(c, mp.g.n[d], H, mp.g.m, &mp.corr2[d]))) return rc;
   }
@@ -533,6 +572,7 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
     for (int i = 0; i < 3; ++i)
       for (int d = 0; d < 3; ++d) put(cell.lat[i][d]);
     put(pot_shift), put(c->buf_gen), put(st), put(rs);
+    put(ks.box_div), put(ks.fft_lines), put(ks.fft_sched), put(ks.gather_warps);
     auto hit = c->graphs.find(key);
     if (hit != c->graphs.end()) {
       cudaGraphLaunch(hit->second.exec, st);
@@ -1319,6 +1359,127 @@ int ewg_potential_force_device(ewg_context* c, int n, const double* coords_devic
 // scheme is left as it was.
 constexpr int kTuneRuns = 7;  // timed evaluations per candidate within the bar
 
+// Median device milliseconds of kTuneRuns evaluations of p with kernel shape ks
+// pinned (two untimed evaluations first: with graphs on, the second records
+// the sequence and the timed ones are replays).
+int time_shape(ewg_context* c, int n, const double* dpos, const double* dq, const Cell& cell,
+               const ewg_params& p, double* dpot, double* dforce, double shift,
+               const ewg_kernel_shape& ks, cudaEvent_t e0, cudaEvent_t e1, double* ms) {
+  const bool was_pinned = c->shape_pinned;
+  const ewg_kernel_shape saved = c->pinned;
+  c->shape_pinned = true;
+  c->pinned = ks;
+  const bool want_force = dforce != nullptr;
+  int rc = EWG_OK;
+  for (int r = 0; r < 2 && !rc; ++r)
+    rc = evaluate(c, n, dpos, 1, n, dq, cell, p, want_force, dpot, dforce, false, nullptr, nullptr,
+                  shift);
+  float runs[kTuneRuns];
+  for (int r = 0; r < kTuneRuns && !rc; ++r) {
+    cudaEventRecord(e0, c->stream);
+    rc = evaluate(c, n, dpos, 1, n, dq, cell, p, want_force, dpot, dforce, false, nullptr, nullptr,
+                  shift);
+    cudaEventRecord(e1, c->stream);
+    if (!rc && (cudaEventSynchronize(e1) != cudaSuccess ||
+                cudaEventElapsedTime(&runs[r], e0, e1) != cudaSuccess))
+      rc = EWG_ERR_CUDA;
+  }
+  c->shape_pinned = was_pinned;
+  c->pinned = saved;
+  if (rc) return rc;
+  std::sort(runs, runs + kTuneRuns);
+  *ms = runs[kTuneRuns / 2];
+  return EWG_OK;
+}
+
+// Kernel-shape search for the bucket of one evaluation (ewg_tune_kernels):
+// one field at a time from the defaults, a change kept when it is more than 1%
+// faster.  Fields that cannot change this evaluation's kernels are skipped.
+int tune_shapes(ewg_context* c, int n, const double* dpos, const double* dq, const Cell& cell,
+                const ewg_params& p, double* dpot, double* dforce, double shift,
+                ewg_kernel_shape* out, double* ms_out) {
+  MeshGeom g;
+  int rc = mesh_geometry(cell, p, g);
+  if (rc) return rc;
+  const bool want_force = dforce != nullptr;
+  const bool ad = want_force && c->force_scheme == EWG_FORCE_AD;
+  const auto bucket = shape_bucket(c->precision, want_force ? (ad ? 2 : 1) : 0, n, g);
+  auto hit = c->shapes.find(bucket);
+  if (hit != c->shapes.end()) {
+    if (out) *out = hit->second;
+    if (ms_out) ms_out[0] = ms_out[1] = 0.0;
+    return EWG_OK;
+  }
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    cudaGetLastError();
+    return EWG_ERR_CUDA;
+  }
+  ewg_kernel_shape best = resolve_shape(ewg_kernel_shape{});
+  double best_ms = 0.0;
+  rc = time_shape(c, n, dpos, dq, cell, p, dpot, dforce, shift, best, e0, e1, &best_ms);
+  const double ms_default = best_ms;
+  auto consider = [&](const ewg_kernel_shape& cand) {
+    if (rc) return;
+    double t = 0.0;
+    const int r = time_shape(c, n, dpos, dq, cell, p, dpot, dforce, shift, cand, e0, e1, &t);
+    if (r == EWG_ERR_OUT_OF_MEMORY) {  // a shape this device cannot hold: not a candidate
+      cudaGetLastError();
+      return;
+    }
+    if (r) {
+      rc = r;
+      return;
+    }
+    if (t < 0.99 * best_ms) {
+      best = cand;
+      best_ms = t;
+    }
+  };
+  const bool mixed = c->precision == EWG_PRECISION_MIXED;
+  for (int v : {1, 3}) {  // neighbour-cell blocking of the real-space sum
+    ewg_kernel_shape s = best;
+    s.box_div = v;
+    consider(s);
+  }
+  if (want_force && !ad && !mixed)  // FP64 i k gather CTA
+    for (int v : {2, 8}) {
+      ewg_kernel_shape s = best;
+      s.gather_warps = v;
+      consider(s);
+    }
+  int lmax = 0;  // the most lines per CTA any pass takes by default
+  for (int d = 0; d < 3; ++d)
+    lmax = std::max(lmax, mesh_batch_lines(g.n[d], mixed, d == 2 ? g.K3 : 0));
+  for (int v : {4, 2, 1}) {
+    if (v >= lmax) continue;
+    ewg_kernel_shape s = best;
+    s.fft_lines = v;
+    consider(s);
+  }
+  bool has8 = false;  // the radix-4 schedule differs only where radix 8 is used
+  for (int d = 0; d < 3; ++d) {
+    FftPlan fp;
+    if (factor_length(g.n[d], fp))
+      for (int i = 0; i < fp.nstages; ++i) has8 = has8 || fp.radix[i] == 8;
+  }
+  if (has8) {
+    ewg_kernel_shape s = best;
+    s.fft_sched = 2;
+    consider(s);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  c->shapes[bucket] = best;
+  if (out) *out = best;
+  if (ms_out) {
+    ms_out[0] = ms_default;
+    ms_out[1] = best_ms;
+  }
+  return EWG_OK;
+}
+
 int ewg_tune(ewg_context* c, int n, const double* positions, const double* charges,
              const double* lat_rows, double target, ewg_overrides* out, int* scheme_out,
              double* report) {
@@ -1478,6 +1639,13 @@ int ewg_tune(ewg_context* c, int n, const double* positions, const double* charg
   o.r_cut = best.p.r_cut;
   o.k_cut = best.p.k_cut;
   o.window_cutoff = best.p.window_cutoff;
+  // The winner's kernel shapes, for later evaluations with these overrides.
+  c->force_scheme = best.scheme;
+  rc = tune_shapes(c, n, dpos, dq, cell, best.p, dpot, dforce,
+                   background_shift(c, shift_scale, cell, best.p.alpha), nullptr, nullptr);
+  c->force_scheme = scheme;
+  c->resident.coords_version = -1;
+  if (rc) return rc;
   ewg_context::TuneEntry te;
   te.ov = o;
   te.scheme = best.scheme;
@@ -1490,6 +1658,50 @@ int ewg_tune(ewg_context* c, int n, const double* positions, const double* charg
   if (scheme_out) *scheme_out = te.scheme;
   if (report)
     for (int i = 0; i < 4; ++i) report[i] = te.report[i];
+  return EWG_OK;
+}
+
+int ewg_tune_kernels(ewg_context* c, int n, const double* positions, const double* charges,
+                     const double* lat_rows, double tol, const ewg_overrides* ov, int want_force,
+                     ewg_kernel_shape* out, double* ms) {
+  if (!c) return EWG_ERR_ARG;
+  LaunchScope scope(c);
+  c->uploaded_charges = -1;
+  c->resident.coords_version = -1;
+  Cell cell;
+  double q2 = 0.0, qsum = 0.0;
+  int rc = validate_host(c, n, positions, charges, lat_rows, tol, cell, q2, qsum);
+  if (rc) return rc;
+  ewg_params p;
+  if ((rc = choose_parameters(cell, q2, n, tol, ov, p))) return rc;
+  double* dpos = dbuf<double>(c, B_POS, 3 * static_cast<size_t>(n), &rc);
+  double* dq = dbuf<double>(c, B_Q, n, &rc);
+  double* dpot = dbuf<double>(c, B_POT, n, &rc);
+  double* dforce = dbuf<double>(c, B_FORCE, 3 * static_cast<size_t>(n), &rc);
+  if (rc) return rc;
+  cudaMemcpyAsync(dpos, positions, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(dq, charges, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream);
+  rc = tune_shapes(c, n, dpos, dq, cell, p, dpot, want_force ? dforce : nullptr,
+                   background_shift(c, qsum, cell, p.alpha), out, ms);
+  c->resident.coords_version = -1;
+  return rc;
+}
+
+int ewg_set_kernel_shape(ewg_context* c, const ewg_kernel_shape* s) {
+  if (!c) return EWG_ERR_ARG;
+  if (!s) {
+    c->shape_pinned = false;
+    return EWG_OK;
+  }
+  const bool ok = s->box_div >= 0 && s->box_div <= 3 &&
+                  (s->fft_lines == 0 || s->fft_lines == 1 || s->fft_lines == 2 ||
+                   s->fft_lines == 4 || s->fft_lines == 8) &&
+                  s->fft_sched >= 0 && s->fft_sched <= 2 &&
+                  (s->gather_warps == 0 || s->gather_warps == 2 || s->gather_warps == 4 ||
+                   s->gather_warps == 8);
+  if (!ok) return EWG_ERR_ARG;
+  c->pinned = *s;
+  c->shape_pinned = true;
   return EWG_OK;
 }
 

@@ -534,6 +534,13 @@ int pick_lines(int n, size_t cb, int extra = 0) {
   return 0;
 }
 
+// Lines per CTA of one single-cell pass: pick_lines, capped by the plan's
+// kernel shape (the cap only lowers L, so the buffers still fit).
+int plan_lines(const MeshPlan& mp, int n, size_t cb, int extra = 0) {
+  const int L = pick_lines(n, cb, extra);
+  return mp.lines_cap > 0 && mp.lines_cap < L ? mp.lines_cap : L;
+}
+
 // Calls f(std::integral_constant<int, L>) for L in {1, 2, 4, 8}.
 template <typename F>
 void with_lines(int L, F&& f) {
@@ -581,7 +588,7 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
   {  // x, real to complex
     prof_mark(mp.prof, st, ST_FFT_X_R2C);
     const int npairs = n2 * n3 / 2;
-    const int L = pick_lines(n1, cb);
+    const int L = plan_lines(mp, n1, cb);
     const size_t sm = pass_smem(n1, L, cb, 0);
     const int blocks = (npairs + L - 1) / L;
     with_lines(L, [&](auto lc) {
@@ -595,7 +602,7 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
   }
   {  // y forward
     prof_mark(mp.prof, st, ST_FFT_Y_FWD);
-    const int L = pick_lines(n2, cb);
+    const int L = plan_lines(mp, n2, cb);
     const size_t sm = pass_smem(n2, L, cb, 0);
     dim3 grd((g.K1 + L - 1) / L, n3);
     const int H2 = (g.K2 - 1) / 2;
@@ -623,7 +630,7 @@ void forward_impl(const MeshPlan& mp, const void* grid, void* A1v, void* A2v, vo
     ia.inv4a2 = 1.0 / (4.0 * (g.alpha * g.alpha));
     for (int d = 0; d < 3; ++d) ia.corr2[d] = mp.corr2[d];
     ia.stress = stress_part;
-    const int L = pick_lines(n3, cb, g.K3);
+    const int L = plan_lines(mp, n3, cb, g.K3);
     const size_t sm = pass_smem(n3, L, cb, g.K3);
     dim3 grd((g.K1 + L - 1) / L, g.K2);
     with_lines(L, [&](auto lc) {
@@ -652,7 +659,7 @@ void inverse_impl(const MeshPlan& mp, const void* B2v, void* B1v, void* out, int
   const size_t cb = cbytes<R>();
   {
     prof_mark(mp.prof, st, ST_FFT_Y_INV);
-    const int L = pick_lines(n2, cb);
+    const int L = plan_lines(mp, n2, cb);
     const size_t sm = pass_smem(n2, L, cb, 0);
     dim3 grd((g.K1 + L - 1) / L, n3, nc == 4 ? 3 : 1);
     const int H2 = (g.K2 - 1) / 2;
@@ -668,7 +675,7 @@ void inverse_impl(const MeshPlan& mp, const void* B2v, void* B1v, void* out, int
   {
     prof_mark(mp.prof, st, ST_FFT_X_C2R);
     const int nrows = n2 * n3;
-    const int L = pick_lines(n1, cb);
+    const int L = plan_lines(mp, n1, cb);
     const size_t sm = pass_smem(n1, L, cb, 0);
     R* o = static_cast<R*>(out);
     if (nc == 4 && L >= 4) {  // the four components of a row pair in one CTA

@@ -1443,16 +1443,30 @@ void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs,
     else
       EWG_GATHER(float, 1);
   } else {
-    if (nc == 4)
-      launch_chained(k_gather_tiles_dmma<4, kGatherWarps, kGatherMB>, grd, 32 * kGatherWarps, 0, st,
-          tile_start, pairs,
-                                                 static_cast<const double*>(wtab), mp.sd,
-                                                 static_cast<const double*>(grid), part);
-    else
-      launch_chained(k_gather_tiles_dmma<1, kGatherWarps, kGatherMB>, grd, 32 * kGatherWarps, 0, st,
-          tile_start, pairs,
-                                                 static_cast<const double*>(wtab), mp.sd,
-                                                 static_cast<const double*>(grid), part);
+    // The kernel shape's warps per tile; every shape stages 64 atoms per round
+    // (warps x blocks of 8 atoms per warp) and gives bitwise the same partials.
+    const double* w = static_cast<const double*>(wtab);
+    const double* gv = static_cast<const double*>(grid);
+#define EWG_GATHER64(NC, WARPS, MB)                                                             \
+  launch_chained(k_gather_tiles_dmma<NC, WARPS, MB>, grd, 32 * WARPS, 0, st, tile_start, pairs, w, \
+                 mp.sd, gv, part)
+    static_assert(kGatherWarps * kGatherMB == 8, "64 atoms per round");
+    if (nc == 4) {
+      if (mp.gather_warps == 2)
+        EWG_GATHER64(4, 2, 4);
+      else if (mp.gather_warps == 8)
+        EWG_GATHER64(4, 8, 1);
+      else
+        EWG_GATHER64(4, kGatherWarps, kGatherMB);
+    } else {
+      if (mp.gather_warps == 2)
+        EWG_GATHER64(1, 2, 4);
+      else if (mp.gather_warps == 8)
+        EWG_GATHER64(1, 8, 1);
+      else
+        EWG_GATHER64(1, kGatherWarps, kGatherMB);
+    }
+#undef EWG_GATHER64
   }
 #undef EWG_GATHER
   ++g_launches;

@@ -58,7 +58,8 @@ EXPORTED = [
     "ewg_direct_potential_force_static", "ewg_fp64_mma_peak", "ewg_potential_force_stress",
     "ewg_stress_fast", "ewg_potential_at", "ewg_potential_gradient_at", "ewg_external_pot_grad",
     "ewg_xlbomd_gradients", "ewg_set_background", "ewg_set_force_scheme", "ewg_tune", "ewg_set_graphs", "ewg_set_batch_lanes",
-    "ewg_batch_potential_force_ov", "ewg_set_point_engine",
+    "ewg_batch_potential_force_ov", "ewg_set_point_engine", "ewg_tune_kernels",
+    "ewg_set_kernel_shape",
 ]
 
 
@@ -77,6 +78,16 @@ class Overrides(C.Structure):
         ("alpha", C.c_double), ("r_cut", C.c_double), ("k_cut", C.c_double),
         ("n_modes", C.c_int), ("window_cutoff", C.c_int),
     ]
+
+
+class KernelShape(C.Structure):
+    """ewg_kernel_shape: kernel shapes of an evaluation (0 = the default)."""
+
+    _fields_ = [("box_div", C.c_int), ("fft_lines", C.c_int), ("fft_sched", C.c_int),
+                ("gather_warps", C.c_int)]
+
+    def as_dict(self):
+        return {f: int(getattr(self, f)) for f, _ in self._fields_}
 
 
 class Params(C.Structure):
@@ -127,6 +138,9 @@ def lib():
     L.ewg_parameters.argtypes = [C.c_int, dp, dp, C.c_double, C.POINTER(Overrides), C.POINTER(Params)]
     L.ewg_tune.argtypes = [vp, C.c_int, dp, dp, dp, C.c_double, C.POINTER(Overrides),
                            C.POINTER(C.c_int), dp]
+    L.ewg_tune_kernels.argtypes = [vp, C.c_int, dp, dp, dp, C.c_double, C.POINTER(Overrides),
+                                   C.c_int, C.POINTER(KernelShape), dp]
+    L.ewg_set_kernel_shape.argtypes = [vp, C.POINTER(KernelShape)]
     L.ewg_grid_memory.argtypes = [C.c_int, dp, dp, C.c_double, C.POINTER(Overrides), dp]
     L.ewg_device_memory.argtypes = [C.c_int, dp, dp, C.c_double, C.POINTER(Overrides), C.c_int,
                                     C.c_int, dp]
@@ -298,6 +312,32 @@ class Context:
                   windowCutoff_in=o.window_cutoff)
         return ov, int(scheme.value), dict(force_rms=float(rep[0]), pot_rms=float(rep[1]),
                                            ms=float(rep[2]), candidates=int(rep[3]))
+
+    def tune_kernels(self, positions, charges, latVecs, tol=1e-10, want_force=True, **ov):
+        """Kernel shapes for this configuration's bucket (precision form, force
+        grids, atom octave, grid, window), searched by timing when the bucket is
+        new and cached in the context; later evaluations in the bucket run
+        them.  Returns (shape dict, (default ms, tuned ms)), the times 0 when the
+        bucket was already tuned."""
+        q = np.ascontiguousarray(charges, dtype=np.float64)
+        n = q.shape[0]
+        pos = _positions_fortran(positions, n)
+        lat = _lat_fortran(latVecs)
+        o = _overrides(**ov)
+        ks = KernelShape()
+        ms = np.zeros(2)
+        _check(lib().ewg_tune_kernels(self._h, n, _dp(pos), _dp(q), _dp(lat), float(tol),
+                                      C.byref(o), int(bool(want_force)), C.byref(ks), _dp(ms)))
+        return ks.as_dict(), (float(ms[0]), float(ms[1]))
+
+    def set_kernel_shape(self, shape=None):
+        """Pin kernel shapes (a dict of KernelShape fields, 0 or missing =
+        default) for every later evaluation; None returns to the tuned buckets."""
+        if shape is None:
+            _check(lib().ewg_set_kernel_shape(self._h, None))
+            return
+        ks = KernelShape(**{k: int(v) for k, v in shape.items()})
+        _check(lib().ewg_set_kernel_shape(self._h, C.byref(ks)))
 
     def potential_force_stress(self, positions, charges, latVecs, tol=1e-10, **ov):
         """Potential, force and the NFFT-based stress sigma = (2/V) dE/d(strain)

@@ -21,7 +21,7 @@ module ewald_b200
   public :: ewaldGpuPotentialForce, ewaldGpuPotentialAt, ewaldGpuPotentialGradientAt
   public :: ewaldGpuSetForceScheme, ewaldGpuSetBackground, ewaldGpuXlbomdGradients
   public :: ewaldGpuExternalPotGrad, ewaldGpuPotentialForceStress, ewaldGpuBatchPotentialForce
-  public :: ewaldGpuSetPointEngine
+  public :: ewaldGpuSetPointEngine, ewaldGpuTuneKernels, ewaldGpuSetKernelShape, TEwgKernelShape
   public :: EWG_PRECISION_FP64, EWG_PRECISION_MIXED, EWG_FORCE_IK, EWG_FORCE_AD
   public :: EWG_POINTS_AUTO, EWG_POINTS_STOCK, EWG_POINTS_MESH
 
@@ -45,6 +45,11 @@ module ewald_b200
     real(c_double) :: alpha = 0.0_c_double, r_cut = 0.0_c_double, k_cut = 0.0_c_double
     integer(c_int) :: n_modes = 0, window_cutoff = 0
   end type TEwgOverrides
+
+  !> ewg_kernel_shape of the C header (0 = the library's default).
+  type, bind(C) :: TEwgKernelShape
+    integer(c_int) :: box_div = 0, fft_lines = 0, fft_sched = 0, gather_warps = 0
+  end type TEwgKernelShape
 
   interface
     function ewg_create(ctx, device, precision) bind(C, name="ewg_create") result(rc)
@@ -130,6 +135,26 @@ module ewald_b200
       integer(c_int), value :: scheme
       integer(c_int) :: rc
     end function ewg_set_force_scheme
+
+    function ewg_tune_kernels(ctx, n, positions, charges, latRows, tol, ov, wantForce, shape, ms) &
+        & bind(C, name="ewg_tune_kernels") result(rc)
+      import :: c_ptr, c_int, c_double, TEwgOverrides, TEwgKernelShape
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: n, wantForce
+      real(c_double), intent(in) :: positions(n, 3), charges(n), latRows(3, 3)
+      real(c_double), value :: tol
+      type(TEwgOverrides), intent(in) :: ov
+      type(TEwgKernelShape), intent(out) :: shape
+      real(c_double), intent(out) :: ms(2)
+      integer(c_int) :: rc
+    end function ewg_tune_kernels
+
+    function ewg_set_kernel_shape(ctx, shape) bind(C, name="ewg_set_kernel_shape") result(rc)
+      import :: c_ptr, c_int, TEwgKernelShape
+      type(c_ptr), value :: ctx
+      type(TEwgKernelShape), intent(in) :: shape
+      integer(c_int) :: rc
+    end function ewg_set_kernel_shape
 
     function ewg_set_point_engine(ctx, engine) bind(C, name="ewg_set_point_engine") result(rc)
       import :: c_ptr, c_int
@@ -339,6 +364,33 @@ contains
     integer(c_int), intent(in) :: scheme
     call check(ewg_set_force_scheme(this%ctx, scheme))
   end subroutine ewaldGpuSetForceScheme
+
+  !> Kernel-shape autotuner for the bucket of this configuration (precision
+  !> form, force grids, atom octave, grid, window); called once, for example
+  !> after the first updateCoords, so that the SCC loop's evaluations run the
+  !> fastest shapes. ms (optional) gets the default and tuned milliseconds.
+  subroutine ewaldGpuTuneKernels(this, positions, charges, latRows, tol, wantForce, shape, ms)
+    type(TEwaldGpu), intent(inout) :: this
+    real(c_double), intent(in) :: positions(:, :), charges(:), latRows(3, 3), tol
+    logical, intent(in) :: wantForce
+    type(TEwgKernelShape), intent(out) :: shape
+    real(c_double), intent(out), optional :: ms(2)
+    type(TEwgOverrides) :: ov
+    real(c_double) :: msLoc(2)
+    integer(c_int) :: wf
+    wf = 0
+    if (wantForce) wf = 1
+    call check(ewg_tune_kernels(this%ctx, int(size(charges), c_int), positions, charges, latRows, &
+        & tol, ov, wf, shape, msLoc))
+    if (present(ms)) ms = msLoc
+  end subroutine ewaldGpuTuneKernels
+
+  !> Pin kernel shapes for every later evaluation (zero fields: defaults).
+  subroutine ewaldGpuSetKernelShape(this, shape)
+    type(TEwaldGpu), intent(inout) :: this
+    type(TEwgKernelShape), intent(in) :: shape
+    call check(ewg_set_kernel_shape(this%ctx, shape))
+  end subroutine ewaldGpuSetKernelShape
 
   !> Engine of ewaldGpuPotentialAt, ewaldGpuPotentialGradientAt and
   !> ewaldGpuExternalPotGrad: EWG_POINTS_STOCK (the stock pair sum of

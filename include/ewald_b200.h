@@ -217,11 +217,49 @@ int ewg_potential_force_stress(ewg_context* ctx, int n, const double* positions,
  * is returned.  report (optional, 4 doubles): its force and potential RMS
  * errors, its device milliseconds per force evaluation, and the number of
  * candidates evaluated.  Results are cached in the context per (atoms, form,
- * lattice, target); the context's force scheme is left as it was.
+ * lattice, target); the context's force scheme is left as it was.  The
+ * winner's kernel shapes are then tuned as by ewg_tune_kernels, so later
+ * evaluations with the returned overrides run them.
  * No counterpart in the reference. */
 int ewg_tune(ewg_context* ctx, int n, const double* positions, const double* charges,
              const double* lat_rows, double target, ewg_overrides* out, int* scheme,
              double* report);
+
+/* Kernel shapes of an evaluation.  A field left 0 takes the library's default.
+ * Results do not depend on gather_warps or fft_lines (bitwise); box_div and
+ * fft_sched change the order of the sums, so results move by rounding only.
+ * No counterpart in the reference (its kernels are fixed CPU loops). */
+typedef struct {
+  int box_div;      /* real-space cell list: boxes per reference box width
+                       (box_count_3d, common/ewald_cell_list.f90:56-73) along
+                       each axis, 1, 2 or 3 (default 2: 5 x 5 x 5 neighbourhoods) */
+  int fft_lines;    /* most FFT lines per CTA: 1, 2, 4 or 8 (default: the most
+                       whose buffers fit the CTA's shared-memory budget) */
+  int fft_sched;    /* FFT radix schedule: 1 odd radices, then radix 8 (default);
+                       2 odd radices, then radix 4 in place of 8 */
+  int gather_warps; /* FP64 i k gather: warps per tile, 2, 4 or 8, each with
+                       64 / (8 warps) blocks of 8 atoms per round (default 4) */
+} ewg_kernel_shape;
+
+/* Kernel-shape autotuner.  Evaluates the caller's configuration (the
+ * parameters the reference chain gives for tol, or the overrides) with the
+ * context's form and force scheme, and searches the kernel shapes one field
+ * at a time (box_div, gather_warps, fft_lines, fft_sched), keeping a change
+ * only when the median of seven timed evaluations (graph replays) improves by
+ * more than 1%.  The result is cached in the context per bucket -- precision
+ * form, force grids (i k, window derivatives or potential only), atom count
+ * by octave (2^k <= n < 2^(k+1)), fine grid and window half-width -- and every
+ * later evaluation that falls in the bucket runs it.  out (may be NULL) gets the
+ * shape; ms (optional, 2 doubles) the median milliseconds per evaluation with
+ * the default shapes and with the chosen ones.  A bucket already tuned returns
+ * its cached shape with ms[0] = ms[1] = 0 and evaluates nothing.
+ * No counterpart in the reference. */
+int ewg_tune_kernels(ewg_context* ctx, int n, const double* positions, const double* charges,
+                     const double* lat_rows, double tol, const ewg_overrides* ov,
+                     int want_force, ewg_kernel_shape* out, double* ms);
+/* Pin the kernel shapes of every later evaluation of the context (zero fields:
+ * defaults); NULL returns to the tuned buckets and the defaults. */
+int ewg_set_kernel_shape(ewg_context* ctx, const ewg_kernel_shape* shape);
 
 /* ewald_parameters (fft/ewald_fft_3d.f90:142-191); host only. */
 int ewg_parameters(int n, const double* charges, const double* lat_rows, double tol,
