@@ -330,6 +330,7 @@ ewg_kernel_shape resolve_shape(ewg_kernel_shape s) {
     s.fft_lines = 0;  // the most that fit
   if (s.fft_sched != 2) s.fft_sched = 1;
   if (s.gather_warps != 2 && s.gather_warps != 8) s.gather_warps = 4;
+  if (s.stencil != 2) s.stencil = 1;
   return s;
 }
 
@@ -439,6 +440,7 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
   mp.prof = &c->prof;
   mp.lines_cap = ks.fft_lines;
   mp.gather_warps = ks.gather_warps;
+  mp.stencil = ks.stencil;
   for (int d = 0; d < 3; ++d) {
     if ((rc = get_fft(c, mp.g.n[d], mp.fft[d], ks.fft_sched))) return rc;
     const int H = mp.g.M[d] - mp.g.M[d] / 2;
@@ -572,7 +574,7 @@ int evaluate(ewg_context* c, int n, const double* pos, long sa, long sd, const d
     for (int i = 0; i < 3; ++i)
       for (int d = 0; d < 3; ++d) put(cell.lat[i][d]);
     put(pot_shift), put(c->buf_gen), put(st), put(rs);
-    put(ks.box_div), put(ks.fft_lines), put(ks.fft_sched), put(ks.gather_warps);
+    put(ks.box_div), put(ks.fft_lines), put(ks.fft_sched), put(ks.gather_warps), put(ks.stencil);
     auto hit = c->graphs.find(key);
     if (hit != c->graphs.end()) {
       cudaGraphLaunch(hit->second.exec, st);
@@ -1442,7 +1444,12 @@ int tune_shapes(ewg_context* c, int n, const double* dpos, const double* dq, con
     s.box_div = v;
     consider(s);
   }
-  if (want_force && !ad && !mixed)  // FP64 i k gather CTA
+  if (mixed) {  // the mixed form's stencils on the FP32 CUDA cores
+    ewg_kernel_shape s = best;
+    s.stencil = 2;
+    consider(s);
+  }
+  if (want_force && !ad && !(mixed && best.stencil == 2))  // i k gather CTA (tensor cores)
     for (int v : {2, 8}) {
       ewg_kernel_shape s = best;
       s.gather_warps = v;
@@ -1698,7 +1705,8 @@ int ewg_set_kernel_shape(ewg_context* c, const ewg_kernel_shape* s) {
                    s->fft_lines == 4 || s->fft_lines == 8) &&
                   s->fft_sched >= 0 && s->fft_sched <= 2 &&
                   (s->gather_warps == 0 || s->gather_warps == 2 || s->gather_warps == 4 ||
-                   s->gather_warps == 8);
+                   s->gather_warps == 8) &&
+                  s->stencil >= 0 && s->stencil <= 2;
   if (!ok) return EWG_ERR_ARG;
   c->pinned = *s;
   c->shape_pinned = true;

@@ -153,6 +153,8 @@ struct MeshPlan {
   int mixed;                      // 0: FP64, 1: FP32 storage/products
   int lines_cap = 0;              // most FFT lines per CTA (0: the most that fit)
   int gather_warps = 4;           // FP64 i k gather CTA: 2, 4 or 8 warps
+  int stencil = 1;                // mixed form's spread and gather: 1 FP64 tensor
+                                  // cores on FP32 data, 2 FP32 CUDA cores
   Profiler* prof = nullptr;
   const double* corr2[3] = {nullptr, nullptr, nullptr};  // squared deconvolution factors, index k + H
 };

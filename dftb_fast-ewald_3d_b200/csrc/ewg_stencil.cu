@@ -471,16 +471,26 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
+// Two consecutive elements from global into shared memory as doubles: a
+// 16-byte cp.async for FP64 data; for the mixed form's FP32 tiles and weight
+// rows an 8-byte load widened to FP64, so the same DMMA code contracts them.
+__device__ __forceinline__ void stage2(double* dst, const double* src) { cp_async16(dst, src); }
+__device__ __forceinline__ void stage2(double* dst, const float* src) {
+  const float2 v = __ldg(reinterpret_cast<const float2*>(src));
+  dst[0] = v.x;
+  dst[1] = v.y;
+}
+
 // One warp per tile owning all eight z-planes, so each step's x and y weights
 // are read from shared memory once for the eight planes; the lanes stage up to
 // 32 atoms' weight rows per round with asynchronous 16-byte copies.
+template <typename R>
 __device__ __forceinline__ void spread_tiles_dmma_body(int tx, int ty, int tz,
                                                        const int* __restrict__ tile_start,
-                                                          const int2* __restrict__ pairs,
-                                                          const double* __restrict__ wtab,
-                                                          const double* __restrict__ qk,
-                                                          StencilDims sd,
-                                                          double* __restrict__ grid) {
+                                                       const int2* __restrict__ pairs,
+                                                       const R* __restrict__ wtab,
+                                                       const R* __restrict__ qk, StencilDims sd,
+                                                       R* __restrict__ grid) {
   chain_enter();
   __shared__ __align__(16) double sW[3][kSpreadAtoms][kWRow];
   __shared__ double sQ[kSpreadAtoms];
@@ -498,14 +508,14 @@ __device__ __forceinline__ void spread_tiles_dmma_body(int tx, int ty, int tz,
     const int a = lane;
     if (a < nb) {
       const int2 pr = pairs[b0 + a];
-      const double* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
-      const double* src[3] = {wk + sd.woff[0] + (pr.y & 0xff) * TX,
-                              wk + sd.woff[1] + ((pr.y >> 8) & 0xff) * TY,
-                              wk + sd.woff[2] + (pr.y >> 16) * TZ};
+      const R* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
+      const R* src[3] = {wk + sd.woff[0] + (pr.y & 0xff) * TX,
+                         wk + sd.woff[1] + ((pr.y >> 8) & 0xff) * TY,
+                         wk + sd.woff[2] + (pr.y >> 16) * TZ};
 #pragma unroll
       for (int d = 0; d < 3; ++d)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) cp_async16(&sW[d][a][2 * j], src[d] + 2 * j);
+        for (int j = 0; j < 4; ++j) stage2(&sW[d][a][2 * j], src[d] + 2 * j);
       sQ[a] = qk[pr.x];
     } else if (a < ((nb + 3) & ~3)) {  // padding atoms of the last group of four
 #pragma unroll
@@ -530,12 +540,12 @@ __device__ __forceinline__ void spread_tiles_dmma_body(int tx, int ty, int tz,
 #pragma unroll
     for (int z = 0; z < TZ; ++z) {
       if (z >= ez) break;
-      double* row = grid + (static_cast<size_t>(z0 + z) * sd.n[1] + y0 + y) * sd.n[0] + x0 + x;
+      R* row = grid + (static_cast<size_t>(z0 + z) * sd.n[1] + y0 + y) * sd.n[0] + x0 + x;
       if (x + 1 < ex) {
-        row[0] = acc[z][0];
-        row[1] = acc[z][1];
+        row[0] = static_cast<R>(acc[z][0]);
+        row[1] = static_cast<R>(acc[z][1]);
       } else if (x < ex) {
-        row[0] = acc[z][0];
+        row[0] = static_cast<R>(acc[z][0]);
       }
     }
   }
@@ -859,14 +869,13 @@ struct GatherRow {
   static constexpr int value = NC == 4 ? 34 : 12;  // 16-byte multiples
 };
 // WARPS warps per CTA, MB M blocks of 8 atoms per warp and round.
-template <int NC, int WARPS, int MB>
+template <typename R, int NC, int WARPS, int MB>
 __device__ __forceinline__ void gather_tiles_dmma_body(int tx, int ty, int tz,
                                                        const int* __restrict__ tile_start,
-                                                          const int2* __restrict__ pairs,
-                                                          const double* __restrict__ wtab,
-                                                          StencilDims sd,
-                                                          const double* __restrict__ grid,
-                                                          double* __restrict__ part) {
+                                                       const int2* __restrict__ pairs,
+                                                       const R* __restrict__ wtab, StencilDims sd,
+                                                       const R* __restrict__ grid,
+                                                       double* __restrict__ part) {
   chain_enter();
   constexpr int RS = GatherRow<NC>::value;
   constexpr int kGatherAtoms = WARPS * MB * 8;  // atoms staged per round
@@ -886,8 +895,8 @@ __device__ __forceinline__ void gather_tiles_dmma_body(int tx, int ty, int tz,
     const int x = NC == 4 ? h / 2 : 2 * h;  // first point of the chunk
     double* dst = sG + row * RS + 2 * h;
     if (z < ez && y < ey && x < ex) {
-      const double* src = grid + ((static_cast<size_t>(z0 + z) * sd.n[1] + y0 + y) * sd.n[0] + x0) * NC + 2 * h;
-      cp_async16(dst, src);
+      const R* src = grid + ((static_cast<size_t>(z0 + z) * sd.n[1] + y0 + y) * sd.n[0] + x0) * NC + 2 * h;
+      stage2(dst, src);
     } else {
       dst[0] = 0.0;
       dst[1] = 0.0;
@@ -903,14 +912,14 @@ __device__ __forceinline__ void gather_tiles_dmma_body(int tx, int ty, int tz,
       if (a < nb) {
         const int2 pr = pairs[b0 + a];
         sPair[a] = pr;
-        const double* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
-        const double* src[3] = {wk + sd.woff[0] + (pr.y & 0xff) * TX,
-                                wk + sd.woff[1] + ((pr.y >> 8) & 0xff) * TY,
-                                wk + sd.woff[2] + (pr.y >> 16) * TZ};
+        const R* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
+        const R* src[3] = {wk + sd.woff[0] + (pr.y & 0xff) * TX,
+                           wk + sd.woff[1] + ((pr.y >> 8) & 0xff) * TY,
+                           wk + sd.woff[2] + (pr.y >> 16) * TZ};
 #pragma unroll
         for (int d = 0; d < 3; ++d)
 #pragma unroll
-          for (int j = 0; j < 4; ++j) cp_async16(&sW[d][a][2 * j], src[d] + 2 * j);
+          for (int j = 0; j < 4; ++j) stage2(&sW[d][a][2 * j], src[d] + 2 * j);
       } else {  // rows past the list: zero weights, results discarded
 #pragma unroll
         for (int d = 0; d < 3; ++d)
@@ -1000,10 +1009,10 @@ __device__ __forceinline__ void gather_tiles_dmma_body(int tx, int ty, int tz,
 // Shared layout and fragment mapping as in k_gather_tiles_dmma with NC = 1; six
 // weight rows per atom (w1 w2 w3 dw1 dw2 dw3).
 // ---------------------------------------------------------------------------
-template <int WARPS>
+template <typename R, int WARPS>
 __device__ __forceinline__ void gather_tiles_dmma_ad_body(
     int tx, int ty, int tz, const int* __restrict__ tile_start, const int2* __restrict__ pairs,
-    const double* __restrict__ wtab, StencilDims sd, const double* __restrict__ grid,
+    const R* __restrict__ wtab, StencilDims sd, const R* __restrict__ grid,
     double* __restrict__ part) {
   chain_enter();
   constexpr int RS = GatherRow<1>::value;
@@ -1022,7 +1031,7 @@ __device__ __forceinline__ void gather_tiles_dmma_ad_body(
     const int x = 2 * h;
     double* dst = sG + row * RS + 2 * h;
     if (z < ez && y < ey && x < ex) {
-      cp_async16(dst, grid + (static_cast<size_t>(z0 + z) * sd.n[1] + y0 + y) * sd.n[0] + x0 + x);
+      stage2(dst, grid + (static_cast<size_t>(z0 + z) * sd.n[1] + y0 + y) * sd.n[0] + x0 + x);
     } else {
       dst[0] = 0.0;
       dst[1] = 0.0;
@@ -1043,13 +1052,13 @@ __device__ __forceinline__ void gather_tiles_dmma_ad_body(
     int2 pr = make_int2(0, 0);
     if (fr < nb) {
       pr = pairs[b0 + fr];
-      const double* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
+      const R* wk = wtab + static_cast<size_t>(pr.x) * sd.wstride;
       const int off[3] = {sd.woff[0] + (pr.y & 0xff) * TX, sd.woff[1] + ((pr.y >> 8) & 0xff) * TY,
                           sd.woff[2] + (pr.y >> 16) * TZ};
 #pragma unroll
       for (int d = 0; d < 3; ++d) {
-        cp_async16(&W[d][fr][2 * fk], wk + off[d] + 2 * fk);
-        cp_async16(&W[3 + d][fr][2 * fk], wk + sd.dwoff + off[d] + 2 * fk);
+        stage2(&W[d][fr][2 * fk], wk + off[d] + 2 * fk);
+        stage2(&W[3 + d][fr][2 * fk], wk + sd.dwoff + off[d] + 2 * fk);
       }
     } else {  // rows past the list: zero weights, results discarded
 #pragma unroll
@@ -1241,32 +1250,23 @@ __global__ void __launch_bounds__(kSpreadLanes) k_spread_tiles(const int* __rest
   spread_tiles_body<R>(blockIdx.x, blockIdx.y, blockIdx.z, tile_start, pairs, wtab, qk, sd, grid);
 }
 template <typename R>
-__global__ void __launch_bounds__(kSpreadLanes) k_spread_tiles_seg(
-    const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells,
-    const int* __restrict__ tile_start, const int2* __restrict__ pairs, const R* __restrict__ wtab,
-    const R* __restrict__ qk) {
-  int tx, ty, tz;
-  const BatchCell& bc = tile_of_block(cells, prefix, ncells, &tx, &ty, &tz);
-  spread_tiles_body<R>(tx, ty, tz, tile_start + bc.tile0, pairs, wtab, qk, bc.sd,
-                       static_cast<R*>(bc.grid));
-}
-
 __global__ void __launch_bounds__(32) k_spread_tiles_dmma(const int* __restrict__ tile_start,
                                                           const int2* __restrict__ pairs,
-                                                          const double* __restrict__ wtab,
-                                                          const double* __restrict__ qk,
-                                                          StencilDims sd,
-                                                          double* __restrict__ grid) {
-  spread_tiles_dmma_body(blockIdx.x, blockIdx.y, blockIdx.z, tile_start, pairs, wtab, qk, sd, grid);
+                                                          const R* __restrict__ wtab,
+                                                          const R* __restrict__ qk,
+                                                          StencilDims sd, R* __restrict__ grid) {
+  spread_tiles_dmma_body<R>(blockIdx.x, blockIdx.y, blockIdx.z, tile_start, pairs, wtab, qk, sd,
+                            grid);
 }
+template <typename R>
 __global__ void __launch_bounds__(32) k_spread_tiles_dmma_seg(
     const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells,
     const int* __restrict__ tile_start, const int2* __restrict__ pairs,
-    const double* __restrict__ wtab, const double* __restrict__ qk) {
+    const R* __restrict__ wtab, const R* __restrict__ qk) {
   int tx, ty, tz;
   const BatchCell& bc = tile_of_block(cells, prefix, ncells, &tx, &ty, &tz);
-  spread_tiles_dmma_body(tx, ty, tz, tile_start + bc.tile0, pairs, wtab, qk, bc.sd,
-                         static_cast<double*>(bc.grid));
+  spread_tiles_dmma_body<R>(tx, ty, tz, tile_start + bc.tile0, pairs, wtab, qk, bc.sd,
+                            static_cast<R*>(bc.grid));
 }
 
 template <typename R, int NC, int A, int WARPS>
@@ -1279,17 +1279,6 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles(const int* __restri
   gather_tiles_body<R, NC, A, WARPS>(blockIdx.x, blockIdx.y, blockIdx.z, tile_start, pairs, wtab,
                                      sd, grid, part);
 }
-template <typename R, int NC, int A, int WARPS>
-__global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_seg(
-    const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells,
-    const int* __restrict__ tile_start, const int2* __restrict__ pairs, const R* __restrict__ wtab,
-    double* __restrict__ part) {
-  int tx, ty, tz;
-  const BatchCell& bc = tile_of_block(cells, prefix, ncells, &tx, &ty, &tz);
-  gather_tiles_body<R, NC, A, WARPS>(tx, ty, tz, tile_start + bc.tile0, pairs, wtab, bc.sd,
-                                     static_cast<const R*>(bc.out), part);
-}
-
 template <int A, int WARPS>
 __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_ad(const int* __restrict__ tile_start,
                                                                 const int2* __restrict__ pairs,
@@ -1300,55 +1289,44 @@ __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_ad(const int* __res
   gather_tiles_ad_body<A, WARPS>(blockIdx.x, blockIdx.y, blockIdx.z, tile_start, pairs, wtab, sd,
                                  grid, part);
 }
-template <int A, int WARPS>
-__global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_ad_seg(
-    const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells,
-    const int* __restrict__ tile_start, const int2* __restrict__ pairs,
-    const float* __restrict__ wtab, double* __restrict__ part) {
-  int tx, ty, tz;
-  const BatchCell& bc = tile_of_block(cells, prefix, ncells, &tx, &ty, &tz);
-  gather_tiles_ad_body<A, WARPS>(tx, ty, tz, tile_start + bc.tile0, pairs, wtab, bc.sd,
-                                 static_cast<const float*>(bc.out), part);
-}
-
-template <int NC, int WARPS, int MB>
+template <typename R, int NC, int WARPS, int MB>
 __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma(const int* __restrict__ tile_start,
                                                                   const int2* __restrict__ pairs,
-                                                                  const double* __restrict__ wtab,
+                                                                  const R* __restrict__ wtab,
                                                                   StencilDims sd,
-                                                                  const double* __restrict__ grid,
+                                                                  const R* __restrict__ grid,
                                                                   double* __restrict__ part) {
-  gather_tiles_dmma_body<NC, WARPS, MB>(blockIdx.x, blockIdx.y, blockIdx.z, tile_start, pairs,
-                                        wtab, sd, grid, part);
+  gather_tiles_dmma_body<R, NC, WARPS, MB>(blockIdx.x, blockIdx.y, blockIdx.z, tile_start, pairs,
+                                           wtab, sd, grid, part);
 }
-template <int NC, int WARPS, int MB>
+template <typename R, int NC, int WARPS, int MB>
 __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma_seg(
     const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells,
     const int* __restrict__ tile_start, const int2* __restrict__ pairs,
-    const double* __restrict__ wtab, double* __restrict__ part) {
+    const R* __restrict__ wtab, double* __restrict__ part) {
   int tx, ty, tz;
   const BatchCell& bc = tile_of_block(cells, prefix, ncells, &tx, &ty, &tz);
-  gather_tiles_dmma_body<NC, WARPS, MB>(tx, ty, tz, tile_start + bc.tile0, pairs, wtab, bc.sd,
-                                        static_cast<const double*>(bc.out), part);
+  gather_tiles_dmma_body<R, NC, WARPS, MB>(tx, ty, tz, tile_start + bc.tile0, pairs, wtab, bc.sd,
+                                           static_cast<const R*>(bc.out), part);
 }
 
-template <int WARPS>
+template <typename R, int WARPS>
 __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma_ad(
     const int* __restrict__ tile_start, const int2* __restrict__ pairs,
-    const double* __restrict__ wtab, StencilDims sd, const double* __restrict__ grid,
+    const R* __restrict__ wtab, StencilDims sd, const R* __restrict__ grid,
     double* __restrict__ part) {
-  gather_tiles_dmma_ad_body<WARPS>(blockIdx.x, blockIdx.y, blockIdx.z, tile_start, pairs, wtab, sd,
-                                   grid, part);
+  gather_tiles_dmma_ad_body<R, WARPS>(blockIdx.x, blockIdx.y, blockIdx.z, tile_start, pairs, wtab,
+                                      sd, grid, part);
 }
-template <int WARPS>
+template <typename R, int WARPS>
 __global__ void __launch_bounds__(32 * WARPS) k_gather_tiles_dmma_ad_seg(
     const BatchCell* __restrict__ cells, const int* __restrict__ prefix, int ncells,
     const int* __restrict__ tile_start, const int2* __restrict__ pairs,
-    const double* __restrict__ wtab, double* __restrict__ part) {
+    const R* __restrict__ wtab, double* __restrict__ part) {
   int tx, ty, tz;
   const BatchCell& bc = tile_of_block(cells, prefix, ncells, &tx, &ty, &tz);
-  gather_tiles_dmma_ad_body<WARPS>(tx, ty, tz, tile_start + bc.tile0, pairs, wtab, bc.sd,
-                                   static_cast<const double*>(bc.out), part);
+  gather_tiles_dmma_ad_body<R, WARPS>(tx, ty, tz, tile_start + bc.tile0, pairs, wtab, bc.sd,
+                                      static_cast<const R*>(bc.out), part);
 }
 
 template <typename R>
@@ -1409,15 +1387,18 @@ void launch_pair_bins(const MeshPlan& mp, const int4* slot, int n, int* counts, 
 void launch_spread(const MeshPlan& mp, const int* tile_start, const int2* pairs, const void* wtab,
                    const void* qk, void* grid, cudaStream_t st) {
   dim3 grd(mp.sd.ntiles[0], mp.sd.ntiles[1], mp.sd.ntiles[2]);
-  if (mp.mixed)
+  if (mp.mixed && mp.stencil == 2)  // FP32 CUDA-core spread
     launch_chained(k_spread_tiles<float>, grd, kSpreadLanes, 0, st, tile_start, pairs,
-                                                     static_cast<const float*>(wtab),
-                                                     static_cast<const float*>(qk), mp.sd,
-                                                     static_cast<float*>(grid));
+                   static_cast<const float*>(wtab), static_cast<const float*>(qk), mp.sd,
+                   static_cast<float*>(grid));
+  else if (mp.mixed)  // FP32 weights and grid, FP64 products on the tensor cores
+    launch_chained(k_spread_tiles_dmma<float>, grd, 32, 0, st, tile_start, pairs,
+                   static_cast<const float*>(wtab), static_cast<const float*>(qk), mp.sd,
+                   static_cast<float*>(grid));
   else
-    launch_chained(k_spread_tiles_dmma, grd, 32, 0, st, tile_start, pairs, static_cast<const double*>(wtab),
-                                             static_cast<const double*>(qk), mp.sd,
-                                             static_cast<double*>(grid));
+    launch_chained(k_spread_tiles_dmma<double>, grd, 32, 0, st, tile_start, pairs,
+                   static_cast<const double*>(wtab), static_cast<const double*>(qk), mp.sd,
+                   static_cast<double*>(grid));
   ++g_launches;
 }
 
@@ -1428,16 +1409,21 @@ void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs,
   launch_chained(k_gather_tiles<R, NC, GatherShape<R>::atoms, GatherShape<R>::warps>, grd,  \
                  32 * GatherShape<R>::warps, 0, st, tile_start, pairs,                       \
                  static_cast<const R*>(wtab), mp.sd, static_cast<const R*>(grid), part)
+  const bool cores = mp.mixed && mp.stencil == 2;  // FP32 CUDA-core stencils
   if (mp.sd.ad && nc == 1) {  // force wanted, ad scheme: potential grid, four partials
-    if (mp.mixed)
+    if (cores)
       launch_chained(k_gather_tiles_ad<kGatherAdF32Atoms, kGatherAdF32Warps>, grd,
                      32 * kGatherAdF32Warps, 0, st, tile_start, pairs,
                      static_cast<const float*>(wtab), mp.sd, static_cast<const float*>(grid), part);
+    else if (mp.mixed)
+      launch_chained(k_gather_tiles_dmma_ad<float, kGatherAdWarps>, grd, 32 * kGatherAdWarps, 0,
+                     st, tile_start, pairs, static_cast<const float*>(wtab), mp.sd,
+                     static_cast<const float*>(grid), part);
     else
-      launch_chained(k_gather_tiles_dmma_ad<kGatherAdWarps>, grd, 32 * kGatherAdWarps, 0, st,
-          tile_start, pairs, static_cast<const double*>(wtab), mp.sd,
-          static_cast<const double*>(grid), part);
-  } else if (mp.mixed) {
+      launch_chained(k_gather_tiles_dmma_ad<double, kGatherAdWarps>, grd, 32 * kGatherAdWarps, 0,
+                     st, tile_start, pairs, static_cast<const double*>(wtab), mp.sd,
+                     static_cast<const double*>(grid), part);
+  } else if (cores) {
     if (nc == 4)
       EWG_GATHER(float, 4);
     else
@@ -1445,27 +1431,31 @@ void launch_gather(const MeshPlan& mp, const int* tile_start, const int2* pairs,
   } else {
     // The kernel shape's warps per tile; every shape stages 64 atoms per round
     // (warps x blocks of 8 atoms per warp) and gives bitwise the same partials.
-    const double* w = static_cast<const double*>(wtab);
-    const double* gv = static_cast<const double*>(grid);
-#define EWG_GATHER64(NC, WARPS, MB)                                                             \
-  launch_chained(k_gather_tiles_dmma<NC, WARPS, MB>, grd, 32 * WARPS, 0, st, tile_start, pairs, w, \
-                 mp.sd, gv, part)
+#define EWG_GATHER64(R, NC, WARPS, MB)                                                          \
+  launch_chained(k_gather_tiles_dmma<R, NC, WARPS, MB>, grd, 32 * WARPS, 0, st, tile_start, pairs, \
+                 static_cast<const R*>(wtab), mp.sd, static_cast<const R*>(grid), part)
+#define EWG_GATHER64_SHAPES(R, NC)          \
+  do {                                      \
+    if (mp.gather_warps == 2)               \
+      EWG_GATHER64(R, NC, 2, 4);            \
+    else if (mp.gather_warps == 8)          \
+      EWG_GATHER64(R, NC, 8, 1);            \
+    else                                    \
+      EWG_GATHER64(R, NC, kGatherWarps, kGatherMB); \
+  } while (0)
     static_assert(kGatherWarps * kGatherMB == 8, "64 atoms per round");
-    if (nc == 4) {
-      if (mp.gather_warps == 2)
-        EWG_GATHER64(4, 2, 4);
-      else if (mp.gather_warps == 8)
-        EWG_GATHER64(4, 8, 1);
+    if (mp.mixed) {  // FP32 tiles and weights, FP64 products on the tensor cores
+      if (nc == 4)
+        EWG_GATHER64_SHAPES(float, 4);
       else
-        EWG_GATHER64(4, kGatherWarps, kGatherMB);
+        EWG_GATHER64_SHAPES(float, 1);
     } else {
-      if (mp.gather_warps == 2)
-        EWG_GATHER64(1, 2, 4);
-      else if (mp.gather_warps == 8)
-        EWG_GATHER64(1, 8, 1);
+      if (nc == 4)
+        EWG_GATHER64_SHAPES(double, 4);
       else
-        EWG_GATHER64(1, kGatherWarps, kGatherMB);
+        EWG_GATHER64_SHAPES(double, 1);
     }
+#undef EWG_GATHER64_SHAPES
 #undef EWG_GATHER64
   }
 #undef EWG_GATHER
@@ -1540,12 +1530,12 @@ void launch_spread_seg(const BatchLaunch& b, const int* tile_start, const int2* 
                        const void* wtab, const void* qk, cudaStream_t st) {
   if (b.n_tiles == 0) return;
   if (b.mixed)
-    launch_chained(k_spread_tiles_seg<float>, b.n_tiles, kSpreadLanes, 0, st, b.cells, b.p_tiles,
+    launch_chained(k_spread_tiles_dmma_seg<float>, b.n_tiles, 32, 0, st, b.cells, b.p_tiles,
                    b.ncells, tile_start, pairs, static_cast<const float*>(wtab),
                    static_cast<const float*>(qk));
   else
-    launch_chained(k_spread_tiles_dmma_seg, b.n_tiles, 32, 0, st, b.cells, b.p_tiles, b.ncells,
-                   tile_start, pairs, static_cast<const double*>(wtab),
+    launch_chained(k_spread_tiles_dmma_seg<double>, b.n_tiles, 32, 0, st, b.cells, b.p_tiles,
+                   b.ncells, tile_start, pairs, static_cast<const double*>(wtab),
                    static_cast<const double*>(qk));
   ++g_launches;
 }
@@ -1556,31 +1546,33 @@ void launch_gather_seg(const BatchLaunch& b, const int* tile_start, const int2* 
   const int nb = b.n_tiles;
   if (b.ad && b.nc == 1 && b.nparts == 4) {  // window-differentiated forces
     if (b.mixed)
-      launch_chained(k_gather_tiles_ad_seg<kGatherAdF32Atoms, kGatherAdF32Warps>, nb,
-                     32 * kGatherAdF32Warps, 0, st, b.cells, b.p_tiles, b.ncells, tile_start, pairs,
+      launch_chained(k_gather_tiles_dmma_ad_seg<float, kGatherAdWarps>, nb, 32 * kGatherAdWarps, 0,
+                     st, b.cells, b.p_tiles, b.ncells, tile_start, pairs,
                      static_cast<const float*>(wtab), part);
     else
-      launch_chained(k_gather_tiles_dmma_ad_seg<kGatherAdWarps>, nb, 32 * kGatherAdWarps, 0, st,
-                     b.cells, b.p_tiles, b.ncells, tile_start, pairs,
+      launch_chained(k_gather_tiles_dmma_ad_seg<double, kGatherAdWarps>, nb, 32 * kGatherAdWarps,
+                     0, st, b.cells, b.p_tiles, b.ncells, tile_start, pairs,
                      static_cast<const double*>(wtab), part);
   } else if (b.mixed) {
     const float* w = static_cast<const float*>(wtab);
     if (b.nc == 4)
-      launch_chained(k_gather_tiles_seg<float, 4, GatherShape<float>::atoms, GatherShape<float>::warps>,
-                     nb, 32 * GatherShape<float>::warps, 0, st, b.cells, b.p_tiles, b.ncells,
-                     tile_start, pairs, w, part);
+      launch_chained(k_gather_tiles_dmma_seg<float, 4, kGatherWarps, kGatherMB>, nb,
+                     32 * kGatherWarps, 0, st, b.cells, b.p_tiles, b.ncells, tile_start, pairs, w,
+                     part);
     else
-      launch_chained(k_gather_tiles_seg<float, 1, GatherShape<float>::atoms, GatherShape<float>::warps>,
-                     nb, 32 * GatherShape<float>::warps, 0, st, b.cells, b.p_tiles, b.ncells,
-                     tile_start, pairs, w, part);
+      launch_chained(k_gather_tiles_dmma_seg<float, 1, kGatherWarps, kGatherMB>, nb,
+                     32 * kGatherWarps, 0, st, b.cells, b.p_tiles, b.ncells, tile_start, pairs, w,
+                     part);
   } else {
     const double* w = static_cast<const double*>(wtab);
     if (b.nc == 4)
-      launch_chained(k_gather_tiles_dmma_seg<4, kGatherWarps, kGatherMB>, nb, 32 * kGatherWarps, 0,
-                     st, b.cells, b.p_tiles, b.ncells, tile_start, pairs, w, part);
+      launch_chained(k_gather_tiles_dmma_seg<double, 4, kGatherWarps, kGatherMB>, nb,
+                     32 * kGatherWarps, 0, st, b.cells, b.p_tiles, b.ncells, tile_start, pairs, w,
+                     part);
     else
-      launch_chained(k_gather_tiles_dmma_seg<1, kGatherWarps, kGatherMB>, nb, 32 * kGatherWarps, 0,
-                     st, b.cells, b.p_tiles, b.ncells, tile_start, pairs, w, part);
+      launch_chained(k_gather_tiles_dmma_seg<double, 1, kGatherWarps, kGatherMB>, nb,
+                     32 * kGatherWarps, 0, st, b.cells, b.p_tiles, b.ncells, tile_start, pairs, w,
+                     part);
   }
   ++g_launches;
 }

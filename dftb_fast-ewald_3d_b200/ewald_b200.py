@@ -84,7 +84,7 @@ class KernelShape(C.Structure):
     """ewg_kernel_shape: kernel shapes of an evaluation (0 = the default)."""
 
     _fields_ = [("box_div", C.c_int), ("fft_lines", C.c_int), ("fft_sched", C.c_int),
-                ("gather_warps", C.c_int)]
+                ("gather_warps", C.c_int), ("stencil", C.c_int)]
 
     def as_dict(self):
         return {f: int(getattr(self, f)) for f, _ in self._fields_}

@@ -48,7 +48,7 @@ module ewald_b200
 
   !> ewg_kernel_shape of the C header (0 = the library's default).
   type, bind(C) :: TEwgKernelShape
-    integer(c_int) :: box_div = 0, fft_lines = 0, fft_sched = 0, gather_warps = 0
+    integer(c_int) :: box_div = 0, fft_lines = 0, fft_sched = 0, gather_warps = 0, stencil = 0
   end type TEwgKernelShape
 
   interface

@@ -59,7 +59,9 @@ enum {
 /* ---- precision forms ---------------------------------------------------- */
 enum {
   EWG_PRECISION_FP64 = 0,  /* plain form: FP64 throughout, parity with the reference  */
-  EWG_PRECISION_MIXED = 1  /* FP32 stencils, FFT and pair terms; FP64 accumulation,
+  EWG_PRECISION_MIXED = 1  /* FP32 window weights, grids, FFT and pair terms; the
+                              stencil contractions on the FP64 tensor cores (or FP32
+                              CUDA cores, ewg_kernel_shape.stencil); FP64 accumulation,
                               self term, reductions and lattice setup                 */
 };
 
@@ -226,8 +228,9 @@ int ewg_tune(ewg_context* ctx, int n, const double* positions, const double* cha
              double* report);
 
 /* Kernel shapes of an evaluation.  A field left 0 takes the library's default.
- * Results do not depend on gather_warps or fft_lines (bitwise); box_div and
- * fft_sched change the order of the sums, so results move by rounding only.
+ * Results do not depend on gather_warps or fft_lines (bitwise); box_div,
+ * fft_sched and stencil change the order or the precision of the sums, so
+ * results move by rounding only.
  * No counterpart in the reference (its kernels are fixed CPU loops). */
 typedef struct {
   int box_div;      /* real-space cell list: boxes per reference box width
@@ -237,14 +240,17 @@ typedef struct {
                        whose buffers fit the CTA's shared-memory budget) */
   int fft_sched;    /* FFT radix schedule: 1 odd radices, then radix 8 (default);
                        2 odd radices, then radix 4 in place of 8 */
-  int gather_warps; /* FP64 i k gather: warps per tile, 2, 4 or 8, each with
-                       64 / (8 warps) blocks of 8 atoms per round (default 4) */
+  int gather_warps; /* FP64-contraction i k gather: warps per tile, 2, 4 or 8,
+                       each with 64 / (8 warps) blocks of 8 atoms per round
+                       (default 4) */
+  int stencil;      /* mixed form's spread and gathers: 1 the FP64 tensor cores
+                       on its FP32 weights and grids (default), 2 FP32 CUDA cores */
 } ewg_kernel_shape;
 
 /* Kernel-shape autotuner.  Evaluates the caller's configuration (the
  * parameters the reference chain gives for tol, or the overrides) with the
  * context's form and force scheme, and searches the kernel shapes one field
- * at a time (box_div, gather_warps, fft_lines, fft_sched), keeping a change
+ * at a time (box_div, stencil, gather_warps, fft_lines, fft_sched), keeping a change
  * only when the median of seven timed evaluations (graph replays) improves by
  * more than 1%.  The result is cached in the context per bucket -- precision
  * form, force grids (i k, window derivatives or potential only), atom count

@@ -10,7 +10,7 @@ applied to every later evaluation in that bucket."""
 
 import numpy as np
 import pytest
-from conftest import rel_max
+from conftest import rel_max, rel_rms
 
 import workloads as W
 
@@ -101,8 +101,33 @@ def test_tune_kernels_caches_per_bucket(ewald_lib, ctx, oracle):
     assert ms3 > 0.0
 
 
+@pytest.mark.parametrize("scheme", [0, 1], ids=["ik", "ad"])
+def test_mixed_stencil_engines(ewald_lib, ctx, scheme):
+    """The mixed form's spread and gathers on the FP64 tensor cores (default)
+    and on the FP32 CUDA cores both stay within the mixed bar of the FP64 form."""
+    pos, q, lat = W.water_box(1365, seed=3)
+    p64, f64 = ctx.potential_force(pos, q, lat, 1e-10)
+    cm = ewald_lib.Context(0, ewald_lib.MIXED)
+    try:
+        cm.set_force_scheme(scheme)
+        out = {}
+        for st in (1, 2):
+            cm.set_kernel_shape({"stencil": st})
+            out[st] = cm.potential_force(pos, q, lat, 1e-7)
+            out[st, "pot"] = cm.potential_force(pos, q, lat, 1e-7, want_force=False)
+    finally:
+        cm.close()
+    for st in (1, 2):
+        pm, fm = out[st]
+        assert rel_rms(fm, f64) < 1e-6 and rel_rms(pm, p64) < 1e-6
+        assert rel_rms(out[st, "pot"], p64) < 1e-6
+    # the tensor-core contraction is the more accurate of the two
+    assert rel_rms(out[1][1], f64) <= 1.5 * rel_rms(out[2][1], f64)
+
+
 def test_set_kernel_shape_rejects_bad_fields(ewald_lib, ctx):
-    for bad in ({"box_div": 4}, {"fft_lines": 3}, {"fft_sched": 3}, {"gather_warps": 16}):
+    for bad in ({"box_div": 4}, {"fft_lines": 3}, {"fft_sched": 3}, {"gather_warps": 16},
+                {"stencil": 3}):
         with pytest.raises(ewald_lib.EwaldError) as e:
             ctx.set_kernel_shape(bad)
         assert e.value.code == 2  # EWG_ERR_ARG
