@@ -1351,9 +1351,9 @@ int ewg_potential_force_device(ewg_context* c, int n, const double* coords_devic
 
 // Parameter autotuner.  Candidates: both force schemes, and the reference chain
 // (choose_parameters) at tolerances tol = target/10, target/5, target/3, with
-// the real-space cutoff overridden to 1, 1.15, 1.3 or 1.5 times the chain's own
-// (alpha then follows from the real-space budget, k_cut from the Fourier budget,
-// the modes from k_cut) and window half-widths 6 to 9.  Each candidate is
+// the real-space cutoff overridden to 0.7, 0.85, 1, 1.15, 1.3 or 1.5 times the
+// chain's own (alpha then follows from the real-space budget, k_cut from the
+// Fourier budget, the modes from k_cut) and window half-widths 5 to 9.  Each candidate is
 // evaluated once on the caller's configuration and compared with an FP64 i k
 // evaluation at the reference's parameters for tol = 1e-10; those within the
 // bar are timed with CUDA events, evaluation by evaluation, and ranked by the
@@ -1570,8 +1570,8 @@ int ewg_tune(ewg_context* c, int n, const double* positions, const double* charg
   std::vector<Candidate> cands;
   std::vector<ewg_params> seen;
   for (double tf : {0.1, 0.2, 1.0 / 3.0})
-    for (double rs : {1.0, 1.15, 1.3, 1.5})
-      for (int m : {6, 7, 8, 9}) {
+    for (double rs : {0.7, 0.85, 1.0, 1.15, 1.3, 1.5})
+      for (int m : {5, 6, 7, 8, 9}) {
         ewg_overrides ov{};
         ov.has_r_cut = 1;
         ov.r_cut = base.r_cut * rs;

@@ -208,8 +208,8 @@ int ewg_potential_force_stress(ewg_context* ctx, int n, const double* positions,
 /* Parameter autotuner for the context's precision form (the mixed form in
  * practice).  On the caller's configuration it evaluates candidates -- both
  * force schemes, with the reference chain at tol = target/10, /5, /3, the
- * real-space cutoff scaled by 1, 1.15, 1.3 or 1.5 (alpha, k_cut and the modes
- * following from it) and window half-widths 6..9 -- against an FP64 i k
+ * real-space cutoff scaled by 0.7, 0.85, 1, 1.15, 1.3 or 1.5 (alpha, k_cut and
+ * the modes following from it) and window half-widths 5..9 -- against an FP64 i k
  * evaluation at the reference's parameters for tol = 1e-10, times those whose
  * RMS relative force error is at most target/2 and RMS relative potential
  * error at most target, and returns the fastest: its parameters as overrides
