@@ -15,16 +15,19 @@
 // counting sort whose buckets are ordered by atom index, so each tile owns an
 // exact, deterministic list of the atoms that reach it.
 //
-// Spread: a CTA owns a tile.  FP64 runs on the tensor cores.  FP32: each lane
-// owns two x-pencils of 8 points in registers and adds q w1 w2 w3 atom by atom
-// in list order (groups of 16 atoms in FP32, the group sums in FP64), then
-// writes them once (no atomics, no zeroing, fixed order).
-// Gather: a CTA of one (FP64) or two (FP32) warps stages its tile in shared
-// memory; each warp takes 64 atoms of the tile's list at a time, two per lane,
-// and walks the tile's 512 points in lockstep so every grid value is a
-// shared-memory broadcast, skipping the rows none of its atoms reach.  Each lane writes its atom's partial to the atom's slot for
-// this tile; a final kernel sums each atom's slots in a fixed order.  Results
-// are bitwise reproducible.
+// Spread: a CTA owns a tile and writes it once (no atomics, no zeroing, fixed
+// order).  Both precision forms contract on the FP64 tensor cores (DMMA); the
+// mixed form's FP32 weight rows are widened to FP64 as they are staged and its
+// grid is written in FP32.  The FP32 CUDA-core spread (a kernel shape of the
+// mixed form) keeps two x-pencils of 8 points per lane in registers and adds
+// q w1 w2 w3 atom by atom in list order (groups of 16 atoms in FP32, the group
+// sums in FP64).
+// Gather: a CTA stages its tile in shared memory and contracts it with the
+// weight rows of its atoms on the tensor cores (FP32 tiles widened as they are
+// staged), or, on the FP32 CUDA cores, walks the tile's points in lockstep so
+// every grid value is a shared-memory broadcast.  Each atom's partial goes to
+// its slot for this tile; a final kernel sums each atom's slots in a fixed
+// order.  Results are bitwise reproducible.
 
 #include <cuda_runtime.h>
 
@@ -453,13 +456,13 @@ __device__ __forceinline__ void dmma_m8n8k4(double& c0, double& c1, double a, do
                : "d"(a), "d"(b));
 }
 
-constexpr int kGatherWarps = 4;   // FP64 gather: warps per tile
-constexpr int kGatherMB = 2;      // FP64 gather: M blocks of 8 atoms per warp and round
-constexpr int kGatherAdWarps = 2;  // FP64 gather with window derivatives: warps per tile
-// FP32 gather with window derivatives: one atom per lane (74 registers, so
+constexpr int kGatherWarps = 4;   // tensor-core i k gather: warps per tile
+constexpr int kGatherMB = 2;      // tensor-core i k gather: M blocks of 8 atoms per warp and round
+constexpr int kGatherAdWarps = 2;  // tensor-core gather with window derivatives: warps per tile
+// FP32 CUDA-core gather with window derivatives: one atom per lane (74 registers, so
 // about 13 CTAs per SM) and two warps per tile.
 constexpr int kGatherAdF32Atoms = 1, kGatherAdF32Warps = 2;
-constexpr int kSpreadAtoms = 32;  // FP64 spread: atoms staged per round, one per lane
+constexpr int kSpreadAtoms = 32;  // tensor-core spread: atoms staged per round, one per lane
 constexpr int kWRow = 12;         // doubles per staged weight row: 8 used; the
                                   // padding makes the fragment reads conflict-free
 
