@@ -46,7 +46,8 @@ def triclinic(seed=21, n=300):
     return pos, q - q.mean(), lat
 
 
-SYSTEMS = [("c2", W.c2_random_4096), ("triclinic", triclinic)]
+# C1 is the image-sum regime (one reference-width box per axis, cutoff beyond half the cell).
+SYSTEMS = [("c1", W.c1_small_cubic), ("c2", W.c2_random_4096), ("triclinic", triclinic)]
 
 
 @pytest.mark.parametrize("sys_name,gen", SYSTEMS, ids=[s[0] for s in SYSTEMS])
