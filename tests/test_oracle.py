@@ -1,5 +1,5 @@
 """Pins of the CPU oracle (no GPU): the oracle must be right before the CUDA
-library is judged against it.  The reference ships no golden vectors for this
+library is checked against it.  The reference ships no golden vectors for this
 path, so the oracle is pinned against numpy's FFT, an independent numpy
 restatement, the direct engine, the rock-salt Madelung constant, finite
 differences and the reference's own parameter values quoted for the benchmark
