@@ -5,6 +5,8 @@ matches the oracle exactly (integers bit for bit)."""
 import ctypes as C
 import os
 import re
+import shutil
+import subprocess
 
 import numpy as np
 import pytest
@@ -27,6 +29,52 @@ def test_library_exports_every_declared_symbol(ewald_lib):
     L = ewald_lib.lib()
     for name in declared_symbols():
         assert hasattr(L, name), name
+
+
+def _cc():
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    return cc
+
+
+def test_header_is_c99_and_the_c_driver_links(tmp_path, ewald_lib):
+    """The plain C caller (tests/c_driver) builds against the header alone and
+    links every entry point it uses; it is run by the GPU tests."""
+    ewald_lib.lib()
+    libdir = os.path.join(ROOT, "dftb_fast-ewald_3d_b200")
+    subprocess.run([_cc(), "-std=c99", "-O2", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "c_driver", "tcoulomb_sequence.c"), "-L", libdir,
+                    "-lewald_b200", f"-Wl,-rpath,{libdir}", "-o", str(tmp_path / "driver")],
+                   check=True)
+
+
+def test_struct_layouts_match_the_python_mirror(tmp_path, ewald_lib):
+    """Sizes and member offsets of the header's structs as a C compiler lays
+    them out, against the ctypes structures of the Python mirror."""
+    members = {"ewg_overrides": ("Overrides", ["has_alpha", "has_window_cutoff", "alpha", "r_cut",
+                                               "k_cut", "n_modes", "window_cutoff"]),
+               "ewg_params": ("Params", ["alpha", "k_cut", "window_cutoff", "n_modes"]),
+               "ewg_kernel_shape": ("KernelShape", ["box_div", "fft_lines", "fft_sched",
+                                                    "gather_warps", "stencil"])}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "ewald_b200.h"', 'int main(void) {']
+    for cname, (_, fields) in members.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f in fields:
+            lines.append(f'  printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ['  return 0;', '}']
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = str(tmp_path / "layout")
+    subprocess.run([_cc(), "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    str(src), "-o", exe], check=True)
+    out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, (pyname, fields) in members.items():
+        py = getattr(ewald_lib, pyname)
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for f in fields:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
 
 
 def test_status_strings(ewald_lib):
