@@ -22,6 +22,8 @@ module ewald_b200
   public :: ewaldGpuSetForceScheme, ewaldGpuSetBackground, ewaldGpuXlbomdGradients
   public :: ewaldGpuExternalPotGrad, ewaldGpuPotentialForceStress, ewaldGpuBatchPotentialForce
   public :: ewaldGpuSetPointEngine, ewaldGpuTuneKernels, ewaldGpuSetKernelShape, TEwgKernelShape
+  public :: ewaldGpuParameters, ewaldGpuGridMemory, ewaldGpuLastParams, ewaldGpuTune
+  public :: ewaldGpuDirectPotentialForce, TEwgParams, TEwgOverrides
   public :: EWG_PRECISION_FP64, EWG_PRECISION_MIXED, EWG_FORCE_IK, EWG_FORCE_AD
   public :: EWG_POINTS_AUTO, EWG_POINTS_STOCK, EWG_POINTS_MESH
 
@@ -45,6 +47,14 @@ module ewald_b200
     real(c_double) :: alpha = 0.0_c_double, r_cut = 0.0_c_double, k_cut = 0.0_c_double
     integer(c_int) :: n_modes = 0, window_cutoff = 0
   end type TEwgOverrides
+
+  !> ewg_params of the C header: TEwaldParameters3d
+  !> (fft/ewald_fft_3d_parameters.f90:24-42).
+  type, bind(C) :: TEwgParams
+    real(c_double) :: alpha = 0.0_c_double, r_cut = 0.0_c_double, k_cut = 0.0_c_double
+    integer(c_int) :: window_cutoff = 0
+    integer(c_int) :: n_modes(3) = 0
+  end type TEwgParams
 
   !> ewg_kernel_shape of the C header (0 = the library's default).
   type, bind(C) :: TEwgKernelShape
@@ -155,6 +165,60 @@ module ewald_b200
       type(TEwgKernelShape), intent(in) :: shape
       integer(c_int) :: rc
     end function ewg_set_kernel_shape
+
+    function ewg_parameters(n, charges, latRows, tol, ov, params) &
+        & bind(C, name="ewg_parameters") result(rc)
+      import :: c_int, c_double, TEwgOverrides, TEwgParams
+      integer(c_int), value :: n
+      real(c_double), intent(in) :: charges(n), latRows(3, 3)
+      real(c_double), value :: tol
+      type(TEwgOverrides), intent(in) :: ov
+      type(TEwgParams), intent(out) :: params
+      integer(c_int) :: rc
+    end function ewg_parameters
+
+    function ewg_grid_memory(n, charges, latRows, tol, ov, gigabytes) &
+        & bind(C, name="ewg_grid_memory") result(rc)
+      import :: c_int, c_double, TEwgOverrides
+      integer(c_int), value :: n
+      real(c_double), intent(in) :: charges(n), latRows(3, 3)
+      real(c_double), value :: tol
+      type(TEwgOverrides), intent(in) :: ov
+      real(c_double), intent(out) :: gigabytes
+      integer(c_int) :: rc
+    end function ewg_grid_memory
+
+    function ewg_last_params(ctx, params) bind(C, name="ewg_last_params") result(rc)
+      import :: c_ptr, c_int, TEwgParams
+      type(c_ptr), value :: ctx
+      type(TEwgParams), intent(out) :: params
+      integer(c_int) :: rc
+    end function ewg_last_params
+
+    function ewg_direct_potential_force(ctx, n, positions, charges, latRows, tol, pot, force, &
+        & alphaIn, rCutIn, kCutIn) bind(C, name="ewg_direct_potential_force") result(rc)
+      import :: c_ptr, c_int, c_double
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: n
+      real(c_double), intent(in) :: positions(n, 3), charges(n), latRows(3, 3)
+      real(c_double), value :: tol
+      real(c_double), intent(out) :: pot(n), force(3, n)
+      type(c_ptr), value :: alphaIn, rCutIn, kCutIn
+      integer(c_int) :: rc
+    end function ewg_direct_potential_force
+
+    function ewg_tune(ctx, n, positions, charges, latRows, target, ov, scheme, report) &
+        & bind(C, name="ewg_tune") result(rc)
+      import :: c_ptr, c_int, c_double, TEwgOverrides
+      type(c_ptr), value :: ctx
+      integer(c_int), value :: n
+      real(c_double), intent(in) :: positions(n, 3), charges(n), latRows(3, 3)
+      real(c_double), value :: target
+      type(TEwgOverrides), intent(out) :: ov
+      integer(c_int), intent(out) :: scheme
+      real(c_double), intent(out) :: report(4)
+      integer(c_int) :: rc
+    end function ewg_tune
 
     function ewg_set_point_engine(ctx, engine) bind(C, name="ewg_set_point_engine") result(rc)
       import :: c_ptr, c_int
@@ -391,6 +455,70 @@ contains
     type(TEwgKernelShape), intent(in) :: shape
     call check(ewg_set_kernel_shape(this%ctx, shape))
   end subroutine ewaldGpuSetKernelShape
+
+  !> ewald_parameters (fft/ewald_fft_3d.f90:142-191): the parameter set the
+  !> reference chain selects for these charges, cell and tolerance (host only).
+  subroutine ewaldGpuParameters(charges, nParticle, latVecs, tol, params)
+    real(c_double), intent(in) :: charges(:), latVecs(3, 3), tol
+    integer, intent(in) :: nParticle
+    type(TEwgParams), intent(out) :: params
+    type(TEwgOverrides) :: ov
+    call check(ewg_parameters(int(nParticle, c_int), charges, latVecs, tol, ov, params))
+  end subroutine ewaldGpuParameters
+
+  !> ewald_grid_memory (fft/ewald_fft_3d.f90:197-244): GiB in the reference's
+  !> own accounting (host only).
+  function ewaldGpuGridMemory(charges, nParticle, latVecs, tol) result(gib)
+    real(c_double), intent(in) :: charges(:), latVecs(3, 3), tol
+    integer, intent(in) :: nParticle
+    real(c_double) :: gib
+    type(TEwgOverrides) :: ov
+    call check(ewg_grid_memory(int(nParticle, c_int), charges, latVecs, tol, ov, gib))
+  end function ewaldGpuGridMemory
+
+  !> Parameters of the context's last evaluation (alpha, cutoffs, window, modes).
+  subroutine ewaldGpuLastParams(this, params)
+    type(TEwaldGpu), intent(in) :: this
+    type(TEwgParams), intent(out) :: params
+    call check(ewg_last_params(this%ctx, params))
+  end subroutine ewaldGpuLastParams
+
+  !> The direct engine (direct/ewald_direct_3d.f90:37-182), which the adapter
+  !> takes under DFTB_EWALD_DIRECT=1; alpha, rCut and kCut default to the
+  !> engine's own balance when absent.
+  subroutine ewaldGpuDirectPotentialForce(this, positions, charges, nParticle, latVecs, tol, pot, &
+      & force, alpha, rCut, kCut)
+    type(TEwaldGpu), intent(in) :: this
+    real(c_double), intent(in) :: positions(:, :), charges(:), latVecs(3, 3), tol
+    integer, intent(in) :: nParticle
+    real(c_double), intent(out) :: pot(:), force(:, :)
+    real(c_double), intent(in), optional, target :: alpha, rCut, kCut
+    type(c_ptr) :: pAlpha, pRCut, pKCut
+    pAlpha = c_null_ptr
+    pRCut = c_null_ptr
+    pKCut = c_null_ptr
+    if (present(alpha)) pAlpha = c_loc(alpha)
+    if (present(rCut)) pRCut = c_loc(rCut)
+    if (present(kCut)) pKCut = c_loc(kCut)
+    call check(ewg_direct_potential_force(this%ctx, int(nParticle, c_int), positions, charges, &
+        & latVecs, tol, pot, force, pAlpha, pRCut, pKCut))
+  end subroutine ewaldGpuDirectPotentialForce
+
+  !> Parameter autotuner of the context's form: the overrides and force scheme
+  !> of the fastest candidate within the RMS error bar set by target; report
+  !> (optional) gets its force and potential RMS errors, milliseconds per
+  !> evaluation and the number of candidates evaluated.
+  subroutine ewaldGpuTune(this, positions, charges, latVecs, target, ov, scheme, report)
+    type(TEwaldGpu), intent(inout) :: this
+    real(c_double), intent(in) :: positions(:, :), charges(:), latVecs(3, 3), target
+    type(TEwgOverrides), intent(out) :: ov
+    integer(c_int), intent(out) :: scheme
+    real(c_double), intent(out), optional :: report(4)
+    real(c_double) :: rep(4)
+    call check(ewg_tune(this%ctx, int(size(charges), c_int), positions, charges, latVecs, target, &
+        & ov, scheme, rep))
+    if (present(report)) report = rep
+  end subroutine ewaldGpuTune
 
   !> Engine of ewaldGpuPotentialAt, ewaldGpuPotentialGradientAt and
   !> ewaldGpuExternalPotGrad: EWG_POINTS_STOCK (the stock pair sum of

@@ -101,3 +101,50 @@ def test_every_interface_matches_its_c_prototype():
                                   "ewg_xlbomd_gradients", "ewg_external_pot_grad"])
 def test_binding_covers(name):
     assert name in fortran_interfaces()
+
+
+def c_structs():
+    """{typedef name: [(member, C type, count)]} of the header's plain structs."""
+    text = re.sub(r"/\*.*?\*/", " ", open(HEADER).read(), flags=re.S)
+    out = {}
+    for m in re.finditer(r"typedef struct\s*\{([^}]*)\}\s*(\w+)\s*;", text):
+        members = []
+        for decl in m.group(1).split(";"):
+            decl = decl.strip()
+            if not decl:
+                continue
+            ctype, rest = decl.split(None, 1)
+            for item in rest.split(","):
+                item = item.strip()
+                mm = re.match(r"(\w+)(?:\[(\d+)\])?", item)
+                members.append((mm.group(1), ctype, int(mm.group(2) or 1)))
+        out[m.group(2)] = members
+    return out
+
+
+def fortran_types():
+    """{type name (lower case): [(component, Fortran type, count)]} of bind(C) types."""
+    text = re.sub(r"&\s*\n\s*&?", " ", open(F90).read())
+    out = {}
+    for m in re.finditer(r"type,\s*bind\(C\)\s*::\s*(\w+)(.*?)end type", text, re.S | re.I):
+        comps = []
+        for line in m.group(2).split("\n"):
+            if "::" not in line:
+                continue
+            spec, names = line.split("::", 1)
+            for item in re.findall(r"(\w+)\s*(?:\((\d+)\))?\s*(?:=\s*[^,]+)?", names):
+                if item[0]:
+                    comps.append((item[0].lower(), spec.strip().lower(), int(item[1] or 1)))
+        out[m.group(1).lower()] = comps
+    return out
+
+
+@pytest.mark.parametrize("cname,ftype", [("ewg_overrides", "tewgoverrides"),
+                                          ("ewg_params", "tewgparams"),
+                                          ("ewg_kernel_shape", "tewgkernelshape")])
+def test_derived_types_match_the_c_structs(cname, ftype):
+    ctype = {"int": "integer(c_int)", "double": "real(c_double)"}
+    c = [(n.lower(), ctype[t], k) for n, t, k in c_structs()[cname]]
+    f = fortran_types()[ftype]
+    assert f == c
+
